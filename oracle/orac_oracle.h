@@ -1,0 +1,149 @@
+/*
+ * ORACLE — test infrastructure only.
+ *
+ * FP64 CPU restatement of ORAC's nonbonded force path (procacci/orac-porting,
+ * ORAC 5).  Only the tests, the smoke check and the bench's CPU-baseline leg
+ * load this library, and only as the checker.  The product (liborac_gpu.so)
+ * never links, loads or calls it.
+ *
+ * Parity status: UNPINNED against reference outputs.  The reference ships no
+ * force- or energy-per-call vectors (its tests are four chaotic full MD runs)
+ * and it cannot be built here (Fortran + FFTW + MPI, none installed).  The
+ * restatement is instead checked by properties the reference's algorithm must
+ * satisfy: forces = -dE/dx by finite differences, PME against a direct Ewald
+ * k-sum, the NaCl Madelung constant, the FFT against numpy.fft, and the
+ * linked-cell list against a brute-force pair search.
+ *
+ * Conventions follow the Fortran arguments: every array is column-major,
+ * every index stored in an array (grppt, atomp, mapnl, list entries, type
+ * tables, bond lists) is 1-based.  co/oc/stress are 3x3 column-major
+ * (co[i + 3*j] = co(i+1, j+1)).  Coordinates in force routines are ORAC
+ * scaled box coordinates in [-1,1) (box length 2); PME, fnb14, fnbgrp and ferrf
+ * take Cartesian coordinates, as the reference does.
+ */
+#ifndef ORAC_ORACLE_H
+#define ORAC_ORACLE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* A&S 7.1.26 erfc as evaluated throughout ORAC (src/force.f:123-125,444-447). */
+double orc_erfc_as(double x);
+
+/* decide_force, src/mts_forces.f:212-241 */
+int orc_decide_force(double rinn, double alphal);
+
+/* appbou, src/appbou.f:57-69: group centres sum pmass*x */
+void orc_appbou(const double* xp0, const double* yp0, const double* zp0,
+                double* xpg, double* ypg, double* zpg,
+                const double* pmass, int ngrp, const int* grppt);
+
+/* change_frame, src/change_frame.f: way=1 x1 = co x0, way=-1 x1 = oc x0 */
+void orc_change_frame(const double* co, const double* oc, int way, int nato,
+                      const double* xp0, const double* yp0, const double* zp0,
+                      double* xp1, double* yp1, double* zp1);
+
+/* lc_index, src/lc_index.f:3-125 (+ dist_ijk, src/dist_ijk.f).
+ * Returns the full-stencil count nind(2) or -1 (INDMAX overflow) or -2
+ * (a cell would be visited twice: the reference stops). */
+int orc_lc_index(int indmax, int ncx, int ncy, int ncz, double ctoff,
+                 const double* co, int* indxi, int* indxj, int* indxk);
+
+/* lc_list, src/lc_list.f:1-237, serial layout nnlpp = [nv, l1..lnv] per
+ * group.  Returns total length written or -1 on overflow of cap. */
+long orc_lc_list(int ncx, int ncy, int ncz, int nind, const int* indxi,
+                 const int* indxj, const int* indxk, double rcut,
+                 const double* co, const double* xp, const double* yp,
+                 const double* zp, int natp, int* nnlpp, long cap);
+
+/* force, src/force.f:1-917 (standard LJ + Ewald-erfc real-space kernel).
+ * Energies are set (not accumulated); forces and stress are accumulated.
+ * nnlpp/nnlpp1 use the serial layout; when rinn > 1e-5 the next inner
+ * shell list is written to nnlpp1 (capacity cap1).  Returns the length of
+ * nnlpp1 written (0 when none) or -1 on overflow. */
+long orc_force(const int* ss_index, const double* xp0, const double* yp0,
+               const double* zp0, const double* xpg, const double* ypg,
+               const double* zpg, const double* charge, const int* nbtype,
+               const int* type, int ma, int nato, const int* atomg,
+               const double* xpcm, const double* ypcm, const double* zpcm,
+               const int* atomp, const double* co, const double* ecc12,
+               const double* ecc6, double alphal, const int* mapnl,
+               int ngrp, const int* grppt, double* ue /* [6]: uconf slt,slv,ss
+               ucoul slt,slv,ss */, double* fpx, double* fpy, double* fpz,
+               double* stress, const int* nnlpp, int* nnlpp1, long cap1,
+               double rneigh, double rinn, double rout, double rtolinn,
+               double rtolout, const double* gmass, int iz,
+               const double* mass, double massinfty, int lskip_ewald,
+               int ewald, int nthreads);
+
+/* PME (FFTW build): load_bsp_moduli + DFTMOD, src/pme_fftw3.f90:165-230 */
+void orc_load_bsp_moduli(double* bsp_mod1, double* bsp_mod2, double* bsp_mod3,
+                         int nfft1, int nfft2, int nfft3, int order);
+
+/* fill_bspline, src/pme_fftw3.f90:518-576 */
+void orc_fill_bspline(double w, int order, double* array, double* darray);
+
+/* 3D transforms with FFTW's conventions for Q(n1,n2,n3) column-major:
+ * r2c forward (exp(-i..)), output FQ(1+n1/2,n2,n3) interleaved complex;
+ * c2r backward (exp(+i..)), unnormalised. */
+void orc_fft1d(int n, double* data, int sign);
+void orc_fft3d_r2c(int n1, int n2, int n3, const double* Q, double* FQ);
+void orc_fft3d_c2r(int n1, int n2, int n3, const double* FQ, double* Q);
+
+/* scalar_sum FFTW branch, src/scalar_sum.f:2-135 (in place on FQ). */
+void orc_scalar_sum(double* FQ, double ewaldcof, double volume,
+                    const double* recip, const double* bsp_mod1,
+                    const double* bsp_mod2, const double* bsp_mod3,
+                    int nfft1, int nfft2, int nfft3, double* eer, double* vir,
+                    double rkcut);
+
+/* do_pmesh_kspace FFTW branch, src/pme_fftw3.f90:56-130.
+ * x,y,z Cartesian; dx,dy,dz accumulated; vir set. */
+void orc_do_pmesh_kspace(int numatoms, const double* x, const double* y,
+                         const double* z, const double* charge,
+                         const double* recip, double volume,
+                         double ewald_coeff, int order, int nfft1, int nfft2,
+                         int nfft3, double* eer, double* dx, double* dy,
+                         double* dz, double* vir, double rkcut, int nthreads);
+
+/* fft_pme, src/fft_pme.f:1-115.  xp scaled, xpcm scaled; forces accumulated;
+ * stressc accumulated (-vir + molecular correction) when pressure != 0. */
+void orc_fft_pme(int ntap, const double* xp, const double* yp, const double* zp,
+                 const double* xpcm, const double* ypcm, const double* zpcm,
+                 const double* pmechg, const double* co, const double* oc,
+                 double volume, double alphal, int order, int nfft1, int nfft2,
+                 int nfft3, double* eer, double* fpx, double* fpy, double* fpz,
+                 double* stressc, const int* atomp, int pressure, double rkcut,
+                 int nthreads);
+
+/* ferrf, src/ferrf.f:1-244 (erf_corr = .false. branches).  x Cartesian.
+ * fs[2] = (slt, slv) set. iz=1 forces + energy, iz=0 energy only. */
+void orc_ferrf(const int* ss_index, double alphal, const double* charge,
+               double fudge, const double* x0, const double* y0,
+               const double* z0, int iz, const int* list, int nlist,
+               double* fs, double* fpx, double* fpy, double* fpz);
+
+/* cself, src/cself.f:1-64 */
+void orc_cself(const int* ss_index, const double* charge, int nato,
+               double alphal, double kcut, double* self_slt, double* self_slv);
+
+/* fnb14, src/fnb14.f:1-219.  ue[4] = uconf slt, slv, ucoul slt, slv (set). */
+void orc_fnb14(const int* ss_index, const double* xp0, const double* yp0,
+               const double* zp0, const double* charge, int nato,
+               const double* ecc12, const double* ecc6, int cut, int ewald,
+               double alphal, const int* int14, int int14p,
+               const int* type14, double fudge, double lj_fudge, double* fpx,
+               double* fpy, double* fpz, double* ue);
+
+/* fnbgrp, src/fnbgrp.f:1-213.  ue[4] as fnb14. */
+void orc_fnbgrp(const int* ss_index, const double* xp0, const double* yp0,
+                const double* zp0, const double* charge, const int* type,
+                const double* ecc12, const double* ecc6, int ewald,
+                double alphal, const int* ingrp, int ingrpp, double* fpx,
+                double* fpy, double* fpz, double* ue);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,296 @@
+"""ORACLE — test infrastructure only.
+
+ctypes front end of liborac_oracle.so (the FP64 CPU restatement of ORAC's
+nonbonded force path).  Only tests/, __graft_entry__.smoke() and bench.py's
+CPU-baseline leg import this module, as the checker.  Parity status: unpinned
+against reference outputs (see orac_oracle.h).
+
+The Oracle class drives the restated routines in the order ORAC's r-RESPA
+driver does (src/mtsmd.f:2403-2470 for the list update, :3030/:3185/:3263 for
+the shell evaluations, :3287-3295 for the phony M-list refresh).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liborac_oracle.so")
+
+_D = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_I = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+_lib = None
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = C.CDLL(LIB_PATH)
+        L.orc_erfc_as.restype = C.c_double
+        L.orc_erfc_as.argtypes = [C.c_double]
+        L.orc_decide_force.restype = C.c_int
+        L.orc_decide_force.argtypes = [C.c_double, C.c_double]
+        L.orc_lc_index.restype = C.c_int
+        L.orc_lc_index.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, _D, _I, _I, _I]
+        L.orc_lc_list.restype = C.c_long
+        L.orc_lc_list.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, _I, _I, _I, C.c_double, _D, _D, _D, _D,
+                                  C.c_int, _I, C.c_long]
+        L.orc_force.restype = C.c_long
+        L.orc_force.argtypes = [_I, _D, _D, _D, _D, _D, _D, _D, _I, _I, C.c_int, C.c_int, _I, _D, _D, _D, _I, _D,
+                                _D, _D, C.c_double, _I, C.c_int, _I, _D, _D, _D, _D, _D, _I, _I, C.c_long,
+                                C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, _D, C.c_int, _D,
+                                C.c_double, C.c_int, C.c_int, C.c_int]
+        L.orc_load_bsp_moduli.argtypes = [_D, _D, _D, C.c_int, C.c_int, C.c_int, C.c_int]
+        L.orc_fill_bspline.argtypes = [C.c_double, C.c_int, _D, _D]
+        L.orc_fft1d.argtypes = [C.c_int, _D, C.c_int]
+        L.orc_fft3d_r2c.argtypes = [C.c_int, C.c_int, C.c_int, _D, _D]
+        L.orc_fft3d_c2r.argtypes = [C.c_int, C.c_int, C.c_int, _D, _D]
+        L.orc_scalar_sum.argtypes = [_D, C.c_double, C.c_double, _D, _D, _D, _D, C.c_int, C.c_int, C.c_int, _D,
+                                     _D, C.c_double]
+        L.orc_do_pmesh_kspace.argtypes = [C.c_int, _D, _D, _D, _D, _D, C.c_double, C.c_double, C.c_int, C.c_int,
+                                          C.c_int, C.c_int, _D, _D, _D, _D, _D, C.c_double, C.c_int]
+        L.orc_fft_pme.argtypes = [C.c_int, _D, _D, _D, _D, _D, _D, _D, _D, _D, C.c_double, C.c_double, C.c_int,
+                                  C.c_int, C.c_int, C.c_int, _D, _D, _D, _D, _D, _I, C.c_int, C.c_double, C.c_int]
+        L.orc_ferrf.argtypes = [_I, C.c_double, _D, C.c_double, _D, _D, _D, C.c_int, _I, C.c_int, _D, _D, _D, _D]
+        L.orc_cself.argtypes = [_I, _D, C.c_int, C.c_double, C.c_double, _D, _D]
+        L.orc_fnb14.argtypes = [_I, _D, _D, _D, _D, C.c_int, _D, _D, C.c_int, C.c_int, C.c_double, _I, C.c_int,
+                                _I, C.c_double, C.c_double, _D, _D, _D, _D]
+        L.orc_fnbgrp.argtypes = [_I, _D, _D, _D, _D, _I, _D, _D, C.c_int, C.c_double, _I, C.c_int, _D, _D, _D, _D]
+        _lib = L
+    return _lib
+
+
+def _f(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _i(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def _colmajor(m):
+    return np.ascontiguousarray(np.asarray(m, dtype=np.float64).T).ravel()
+
+
+def default_threads():
+    return max(1, os.cpu_count() or 1)
+
+
+class Oracle:
+    """CPU restatement of ORAC's force path for one System."""
+
+    def __init__(self, s, nthreads=None, ewald=True):
+        self.s = s
+        self.nthreads = nthreads or default_threads()
+        self.ewald = ewald
+        self.L = lib()
+        self.lists = {}
+        self._prep()
+
+    def _prep(self):
+        s = self.s
+        self.co = _colmajor(s.co)
+        self.oc = _colmajor(s.oc)
+        self.type_cm = _i(np.asarray(s.type_table).T.ravel())
+        self.grppt = _i(s.grppt.ravel())
+        self.xp0, self.yp0, self.zp0 = _f(s.xp0), _f(s.yp0), _f(s.zp0)
+        xg, yg, zg = s.group_centres()
+        self.xpg, self.ypg, self.zpg = _f(xg), _f(yg), _f(zg)
+        xm, ym, zm = s.molecule_centres()
+        self.xpcm, self.ypcm, self.zpcm = _f(xm), _f(ym), _f(zm)
+
+    def set_coords(self, xp0, yp0, zp0):
+        self.s.xp0, self.s.yp0, self.s.zp0 = _f(xp0), _f(yp0), _f(zp0)
+        self._prep()
+
+    # ------------------------------------------------------------ lists
+    def lc_list(self, rcut):
+        s = self.s
+        ncx, ncy, ncz = s.ncell
+        indmax = (2 * ncx) * (2 * ncy) * (2 * ncz) + 1
+        ii = np.zeros(indmax, np.int32)
+        jj = np.zeros(indmax, np.int32)
+        kk = np.zeros(indmax, np.int32)
+        nind = self.L.orc_lc_index(indmax, ncx, ncy, ncz, rcut, self.co, ii, jj, kk)
+        if nind < 0:
+            raise RuntimeError(f"lc_index failed ({nind})")
+        cap = s.ngrp * (s.ngrp + 1) // 2 + s.ngrp + 16
+        cap = min(cap, 400_000_000)
+        out = np.zeros(cap, np.int32)
+        n = self.L.orc_lc_list(ncx, ncy, ncz, nind, ii, jj, kk, rcut, self.co, self.xpg, self.ypg, self.zpg, s.ngrp,
+                               out, cap)
+        if n < 0:
+            raise RuntimeError("lc_list overflow")
+        return out[:n].copy()
+
+    def full_list(self):
+        """ORAC's 'u' list for the brute-force update (iz = 0): one shared
+        list [ngrp, 1..ngrp] read from mbeg = i+1."""
+        return np.concatenate([[self.s.ngrp], np.arange(1, self.s.ngrp + 1)]).astype(np.int32)
+
+    # ------------------------------------------------------------ force
+    def force(self, nnlpp, rneigh, rinn, rout, rtolinn, rtolout, iz=1, lskip=None):
+        """One call of force (src/force.f).  Returns (F (3,N), ue[6], stress
+        (3,3), next list or None)."""
+        s = self.s
+        if lskip is None:
+            lskip = bool(self.L.orc_decide_force(rinn, s.alphal)) if self.ewald else True
+        fx = np.zeros(s.ntap)
+        fy = np.zeros(s.ntap)
+        fz = np.zeros(s.ntap)
+        ue = np.zeros(6)
+        st = np.zeros(9)
+        nnlpp = _i(nnlpp)
+        cap1 = len(nnlpp) + s.ngrp + 16
+        if iz == 0:  # one shared list read from i+1: up to ngrp(ngrp-1)/2 pairs
+            cap1 = s.ngrp * (s.ngrp + 1) // 2 + s.ngrp + 16
+        nxt = np.zeros(cap1, np.int32)
+        n1 = self.L.orc_force(_i(s.ss_index), self.xp0, self.yp0, self.zp0, self.xpg, self.ypg, self.zpg,
+                              _f(s.charge), _i(s.nbtype), self.type_cm, s.ntype, s.ntap, _i(s.atomg), self.xpcm,
+                              self.ypcm, self.zpcm, _i(s.atomp), self.co, _f(s.ecc12), _f(s.ecc6), s.alphal,
+                              _i(s.mapnl), s.ngrp, self.grppt, ue, fx, fy, fz, st, nnlpp, nxt, cap1, rneigh, rinn,
+                              rout, rtolinn, rtolout, _f(s.pmass), iz, _f(s.mass), s.massinfty, int(lskip),
+                              int(self.ewald), self.nthreads)
+        if n1 < 0:
+            raise RuntimeError("next list overflow")
+        nxt = nxt[:n1].copy() if rinn > 1e-5 else None
+        return np.stack([fx, fy, fz]), ue, st.reshape(3, 3, order="F"), nxt
+
+    def shell_params(self, shell, sh=None):
+        """mts_forces radius selection, src/mts_forces.f:57-93:
+        returns (ro, ri, rto, rti, rni, iz)."""
+        sh = sh or self.s.shells
+        if shell == "h":
+            return sh.rcuth, sh.rcutl, sh.rtolh, sh.rtoll, sh.rneil, (1 if sh.rneih >= 1e-10 else 0)
+        if shell == "l":
+            return sh.rcutl, sh.rcutm, sh.rtoll, sh.rtolm, sh.rneim, 1
+        if shell == "m":
+            return sh.rcutm, 0.0, sh.rtolm, 0.0, 0.0, 1
+        raise ValueError(shell)
+
+    def mts_forces(self, shell, nnlpp, sh=None):
+        ro, ri, rto, rti, rni, iz = self.shell_params(shell, sh)
+        return self.force(nnlpp, rni, ri, ro, rti, rto, iz=iz)
+
+    def update_lists(self):
+        """Linked-cell H list plus the two phony calls that derive the L and
+        M lists (src/mtsmd.f:2403-2470)."""
+        import dataclasses
+
+        sh = self.s.shells
+        if self.s.ncell is None:
+            # no LINKED_CELL: the 'u' shell over the all-pairs list (iz = 0),
+            # src/mtsmd.f:2409-2418 with src/mts_forces.f:57-65
+            _, _, _, self.lists["h"] = self.force(self.full_list(), sh.rneih, sh.rcuth, sh.rcuth, sh.rtolh, 0.0,
+                                                  iz=0)
+        else:
+            self.lists["h"] = self.lc_list(sh.rcuth + sh.rtolh + sh.rneih)
+        sh1 = dataclasses.replace(sh, rcuth=sh.rcutl, rtolh=0.0)
+        _, _, _, self.lists["l"] = self.mts_forces("h", self.lists["h"], sh1)
+        sh2 = dataclasses.replace(sh1, rcutl=sh.rcutm, rtoll=0.0)
+        _, _, _, self.lists["m"] = self.mts_forces("l", self.lists["l"], sh2)
+
+    def shell(self, shell):
+        """Evaluate one shell with the current lists; H and L calls refresh
+        the next inner list as ORAC's do."""
+        F, ue, st, nxt = self.mts_forces(shell, self.lists[shell])
+        if shell == "h":
+            self.lists["l"] = nxt
+        elif shell == "l":
+            self.lists["m"] = nxt
+        return F, ue, st
+
+    def refresh_m_list(self):
+        """Phony 'l' call after the H shell (src/mtsmd.f:3287-3295)."""
+        import dataclasses
+
+        sh = self.s.shells
+        sh2 = dataclasses.replace(sh, rcutl=sh.rcutm)
+        _, _, _, self.lists["m"] = self.mts_forces("l", self.lists["l"], sh2)
+
+    # -------------------------------------------------------------- PME
+    def fft_pme(self, pressure=True):
+        s = self.s
+        fx = np.zeros(s.ntap)
+        fy = np.zeros(s.ntap)
+        fz = np.zeros(s.ntap)
+        eer = np.zeros(1)
+        st = np.zeros(9)
+        n1, n2, n3 = s.nfft
+        self.L.orc_fft_pme(s.ntap, self.xp0, self.yp0, self.zp0, self.xpcm, self.ypcm, self.zpcm, _f(s.charge),
+                           self.co, self.oc, s.volume, s.alphal, s.order, n1, n2, n3, eer, fx, fy, fz, st,
+                           _i(s.atomp), int(pressure), s.rkcut, self.nthreads)
+        return np.stack([fx, fy, fz]), float(eer[0]), st.reshape(3, 3, order="F")
+
+    def do_pmesh_kspace(self, x, y, z, charge, recip, volume, alpha, order, nfft, rkcut=1e9):
+        n = len(x)
+        dx = np.zeros(n)
+        dy = np.zeros(n)
+        dz = np.zeros(n)
+        eer = np.zeros(1)
+        vir = np.zeros(9)
+        self.L.orc_do_pmesh_kspace(n, _f(x), _f(y), _f(z), _f(charge), _colmajor(recip), volume, alpha, order,
+                                   nfft[0], nfft[1], nfft[2], eer, dx, dy, dz, vir, rkcut, self.nthreads)
+        return np.stack([dx, dy, dz]), float(eer[0]), vir.reshape(3, 3, order="F")
+
+    # ------------------------------------------------------ corrections
+    def cartesian(self):
+        return self.s.cartesian()
+
+    def ferrf(self, pairs, fudge, iz=1):
+        s = self.s
+        r = self.cartesian()
+        fx = np.zeros(s.ntap)
+        fy = np.zeros(s.ntap)
+        fz = np.zeros(s.ntap)
+        fs = np.zeros(2)
+        p = _i(np.asarray(pairs).reshape(-1, 2).ravel())
+        self.L.orc_ferrf(_i(s.ss_index), s.alphal, _f(s.charge), fudge, _f(r[0]), _f(r[1]), _f(r[2]), iz, p,
+                         len(p) // 2, fs, fx, fy, fz)
+        return np.stack([fx, fy, fz]), fs
+
+    def cself(self):
+        s = self.s
+        a = np.zeros(1)
+        b = np.zeros(1)
+        self.L.orc_cself(_i(s.ss_index), _f(s.charge), s.ntap, s.alphal, s.rkcut, a, b)
+        return float(a[0]), float(b[0])
+
+    def fnb14(self, cut=True):
+        s = self.s
+        r = self.cartesian()
+        fx = np.zeros(s.ntap)
+        fy = np.zeros(s.ntap)
+        fz = np.zeros(s.ntap)
+        ue = np.zeros(4)
+        p = _i(s.int14.ravel())
+        self.L.orc_fnb14(_i(s.ss_index), _f(r[0]), _f(r[1]), _f(r[2]), _f(s.charge), s.ntap, _f(s.ecc1412),
+                         _f(s.ecc146), int(cut), int(self.ewald), s.alphal, p, len(p) // 2, _i(s.type14), s.fudge,
+                         1.0, fx, fy, fz, ue)
+        return np.stack([fx, fy, fz]), ue
+
+    def fnbgrp(self):
+        s = self.s
+        r = self.cartesian()
+        fx = np.zeros(s.ntap)
+        fy = np.zeros(s.ntap)
+        fz = np.zeros(s.ntap)
+        ue = np.zeros(4)
+        p = _i(s.ingrp.ravel())
+        self.L.orc_fnbgrp(_i(s.ss_index), _f(r[0]), _f(r[1]), _f(r[2]), _f(s.charge), _i(s.nbtype), _f(s.ecc12),
+                          _f(s.ecc6), int(self.ewald), s.alphal, p, len(p) // 2, fx, fy, fz, ue)
+        return np.stack([fx, fy, fz]), ue
+
+
+def rel_rms(F, Fref):
+    """ORAC's check_force metric (src/pme_code.f:378-396)."""
+    return float(np.sqrt(((F - Fref) ** 2).sum() / (Fref ** 2).sum()))
