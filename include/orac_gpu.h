@@ -1,0 +1,202 @@
+/*
+ * orac_gpu.h — C ABI of the B200 implementation of ORAC's nonbonded force
+ * path (liborac_gpu.so).
+ *
+ * The entry points replace, one for one, the Fortran routines ORAC's r-RESPA
+ * driver calls on this path (file:line are positions in procacci/orac-porting):
+ *
+ *   orac_gpu_mts_forces       mts_forces   src/mts_forces.f:2-209
+ *   orac_gpu_lc_list          lc_list      src/lc_list.f:1-237 (+ lc_index)
+ *   orac_gpu_fft_pme          fft_pme      src/fft_pme.f:1-115
+ *   orac_gpu_do_pmesh_kspace  do_pmesh_kspace src/pme_fftw3.f90:56-130
+ *                             (argument meaning of src/pme_code.f:65-72)
+ *   orac_gpu_fnb14            fnb14        src/fnb14.f:1-219
+ *   orac_gpu_fnbgrp           fnbgrp       src/fnbgrp.f:1-213
+ *   orac_gpu_ferrf            ferrf        src/ferrf.f:1-244
+ *   orac_gpu_cself            cself        src/cself.f:1-64
+ *
+ * ORAC reads most inputs of these routines from Fortran module globals
+ * (parst, cpropar, unit, spme).  Those are uploaded once per context with
+ * orac_gpu_set_topology / _set_ewald / _set_shells / _set_box.
+ *
+ * Conventions (same as the Fortran arrays, so the iso_c_binding interface
+ * passes them unchanged):
+ *   - reals are double, integers int32; arrays are column-major;
+ *   - every index stored in an array (grppt, atomp, atomg, mapnl, int14,
+ *     list entries, type tables) is 1-based;
+ *   - co, oc, stress, virial, recip are 3x3 column-major (a[i + 3*j] = a(i+1,j+1));
+ *   - coordinates passed to mts_forces / fft_pme / lc_list are ORAC scaled box
+ *     coordinates (box length 2, r = co s); do_pmesh_kspace, fnb14, fnbgrp and
+ *     ferrf take Cartesian coordinates, as their Fortran counterparts do;
+ *   - forces are ACCUMULATED into the caller's arrays (src/force.f:460-471);
+ *     energies and the mts_forces stress are zeroed then set
+ *     (src/mts_forces.f:96-107); fft_pme adds into stressc.
+ *
+ * Every entry point returns an int status (ORAC_OK = 0) and never aborts the
+ * process; orac_gpu_last_error() gives a text for the last failure.  A context
+ * owns one CUDA stream; entry points on one context are not reentrant,
+ * distinct contexts may be driven from distinct host threads.
+ */
+#ifndef ORAC_GPU_H
+#define ORAC_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  ORAC_OK = 0,
+  ORAC_ERR_PARAM = 1,    /* invalid argument or unsupported configuration */
+  ORAC_ERR_CUDA = 2,     /* CUDA runtime failure */
+  ORAC_ERR_CAPACITY = 3, /* list or table capacity exceeded (ORAC: xerror) */
+  ORAC_ERR_STATE = 4,    /* call order violated (e.g. no topology yet) */
+  ORAC_ERR_TIMEOUT = 5,  /* a device-side wait ran out of its budget */
+  ORAC_ERR_NODEVICE = 6  /* no CUDA device / the library cannot run */
+};
+
+typedef struct orac_gpu_ctx orac_gpu_ctx;
+
+/* Context life cycle ------------------------------------------------------ */
+int orac_gpu_create(int device, orac_gpu_ctx** out);
+int orac_gpu_destroy(orac_gpu_ctx* ctx);
+const char* orac_gpu_last_error(const orac_gpu_ctx* ctx);
+/* Library version and build (sm_100a) string. */
+const char* orac_gpu_version(void);
+
+/* Module globals read by mts_forces (src/mts_forces.f:120-152) and by the
+ * routines it calls.  type_table is ORAC's type(ma,ma) (column-major, values
+ * 1-based into ecc12/ecc6 of length ntype*(ntype+1)/2).  mapnl is the serial
+ * exclusion map built by mappa (src/mappa.f): for each atom i in order,
+ * [n, j_1 .. j_n] with j > i.  pmass is the mass fraction of each atom in its
+ * group (ORAC's pmass/gmass, src/redmss.f:15). */
+int orac_gpu_set_topology(orac_gpu_ctx* ctx, int ntap, int ngrp, int nprot,
+                          const int* grppt, const int* atomp, const int* atomg,
+                          const int* ss_index, const double* chrge,
+                          const int* nbtype, int ntype, const int* type_table,
+                          const double* ecc12, const double* ecc6,
+                          const double* mass, const double* pmass,
+                          double massinfty, const int* mapnl, int64_t nmapnl);
+
+/* EWALD PME alpha n1 n2 n3 order (src/read_potential.f:133-150); clewld = 0
+ * selects plain Coulomb in the real-space shells; rkcut as in blkdta.f90:386. */
+int orac_gpu_set_ewald(orac_gpu_ctx* ctx, int clewld, double alphal, int order,
+                       int nfft1, int nfft2, int nfft3, double rkcut);
+
+/* r-RESPA shell radii rcut/rtol/rnei of the M, L and H shells (cpropar
+ * rcutm..rneih, src/read_integrator.f:152-230).  The driver's temporary
+ * swaps of these globals for the list-update calls (src/mtsmd.f:2436-2469,
+ * :3287-3295) become calls to this function. */
+int orac_gpu_set_shells(orac_gpu_ctx* ctx, double rcutm, double rtolm,
+                        double rneim, double rcutl, double rtoll, double rneil,
+                        double rcuth, double rtolh, double rneih);
+
+/* LINKED_CELL ncx ncy ncz (src/read_potential.f:210-230). */
+int orac_gpu_set_linked_cell(orac_gpu_ctx* ctx, int ncx, int ncy, int ncz);
+
+/* Box: co (scaled -> Cartesian, upper triangular as ORAC keeps it) and its
+ * inverse oc; volume = det(co) * 8. */
+int orac_gpu_set_box(orac_gpu_ctx* ctx, const double* co, const double* oc);
+
+/* lc_list: rebuild the H-shell group neighbour list from group centres
+ * (scaled), radius rcut (ORAC passes rcuth+rtolh+rneih, src/mtsmd.f:2420).
+ * The list stays on the device (ORAC's nnlpp0).  *npairs receives the
+ * number of group pairs (may be NULL). */
+int orac_gpu_lc_list(orac_gpu_ctx* ctx, double rcut, const double* xpga,
+                     const double* ypga, const double* zpga, int64_t* npairs);
+
+/* mts_forces(nstep, rshell, ...): evaluate shell rshell ('m', 'l', 'h') of
+ * the standard (non-alchemical, non-REM) real-space kernel with the device
+ * lists, exactly as src/mts_forces.f selects radii and lskip_ewald.  As in
+ * ORAC, the 'h' call rebuilds the L list and the 'l' call the M list; a call
+ * whose inner radius plus tolerance exceeds its outer radius (the phony
+ * list-update calls) computes no forces.  'u' with no linked cell rebuilds
+ * the H list from all pairs (src/mts_forces.f:57-65).
+ * Energies: ucnp/ucns/ucnsp = LJ solute/solvent/mixed, ucop/ucos/ucosp =
+ * Coulomb solute/solvent/mixed; virs, virsp are zeroed (force does not set
+ * them).  Forces are accumulated into fpx/fpy/fpz, stress is set. */
+int orac_gpu_mts_forces(orac_gpu_ctx* ctx, int nstep, char rshell,
+                        const double* xp0, const double* yp0, const double* zp0,
+                        const double* xpg, const double* ypg, const double* zpg,
+                        const double* xpcm, const double* ypcm,
+                        const double* zpcm, double* ucns, double* ucos,
+                        double* virs, double* virsp, double* ucnp, double* ucop,
+                        double* ucnsp, double* ucosp, double* fpx, double* fpy,
+                        double* fpz, double* stress);
+
+/* fft_pme (src/fft_pme.f): SPME reciprocal energy, forces and stress for
+ * scaled coordinates xp and molecule centres xpcm; forces accumulated,
+ * stressc accumulated (-virial + molecular correction) when pressure != 0. */
+int orac_gpu_fft_pme(orac_gpu_ctx* ctx, const double* xp, const double* yp,
+                     const double* zp, const double* xpcm, const double* ypcm,
+                     const double* zpcm, double* eer, double* fpx, double* fpy,
+                     double* fpz, double* stressc, int pressure);
+
+/* do_pmesh_kspace: the SPME core on Cartesian coordinates with an explicit
+ * recip (= 0.5 oc^T in ORAC), volume, alpha, order and grid.  dx/dy/dz are
+ * accumulated, eer and virial set.  Uses the context's stream and buffers but
+ * not its topology (charges are passed). */
+int orac_gpu_do_pmesh_kspace(orac_gpu_ctx* ctx, int numatoms, const double* x,
+                             const double* y, const double* z,
+                             const double* charge, const double* recip,
+                             double volume, double ewald_coeff, int order,
+                             int nfft1, int nfft2, int nfft3, double* eer,
+                             double* dx, double* dy, double* dz,
+                             double* virial);
+
+/* fnb14 (src/fnb14.f): 1-4 pairs int14(2,int14p), LJ tables ecc1412/ecc146
+ * indexed by type14, lj_fudge and fudge; Cartesian coordinates.
+ * ue[4] = LJ slt, LJ slv, Coulomb slt, Coulomb slv (set). */
+int orac_gpu_fnb14(orac_gpu_ctx* ctx, const double* xp0, const double* yp0,
+                   const double* zp0, int cut, const int* int14, int int14p,
+                   const int* type14, const double* ecc1412,
+                   const double* ecc146, int ntab, double fudge,
+                   double lj_fudge, double* fpx, double* fpy, double* fpz,
+                   double* ue);
+
+/* fnbgrp (src/fnbgrp.f): non-excluded intra-group pairs ingrp(2,ingrpp);
+ * Cartesian coordinates; ue[4] as fnb14. */
+int orac_gpu_fnbgrp(orac_gpu_ctx* ctx, const double* xp0, const double* yp0,
+                    const double* zp0, const int* ingrp, int ingrpp,
+                    double* fpx, double* fpy, double* fpz, double* ue);
+
+/* ferrf (src/ferrf.f, erf_corr off): subtract fudge*q_i q_j erf(alpha r)/r for
+ * the pairs list(2,nlist); iz = 1 forces + energy, iz = 0 energy only.
+ * fs[2] = (solute, solvent) energies (set). Cartesian coordinates. */
+int orac_gpu_ferrf(orac_gpu_ctx* ctx, double fudge, const double* x0,
+                   const double* y0, const double* z0, int iz, const int* list,
+                   int nlist, double* fs, double* fpx, double* fpy,
+                   double* fpz);
+
+/* cself (src/cself.f): self energy of the context's charges. */
+int orac_gpu_cself(orac_gpu_ctx* ctx, double kcut, double* self_slt,
+                   double* self_slv);
+
+/* Device-resident entry points -------------------------------------------
+ * The same computations on device pointers (CUDA global memory, FP64 SoA),
+ * for drivers that keep the state in HBM.  Forces are accumulated into the
+ * device arrays fdev[0..3*ntap) laid out x|y|z; energies[8] and stress[9]
+ * are device pointers that receive the shell's results (set). */
+int orac_gpu_mts_forces_dev(orac_gpu_ctx* ctx, char rshell,
+                            const double* xyz_scaled /* 3*ntap, x|y|z */,
+                            const double* grp_scaled /* 3*ngrp */,
+                            const double* mol_scaled /* 3*nprot */,
+                            double* fdev, double* energies, double* stress);
+
+int orac_gpu_fft_pme_dev(orac_gpu_ctx* ctx, const double* xyz_scaled,
+                         const double* mol_scaled, double* fdev,
+                         double* eer_dev, double* stress_dev);
+
+/* Synchronise the context's stream. */
+int orac_gpu_sync(orac_gpu_ctx* ctx);
+
+/* Counters of the last calls (for measurement): number of group pairs in
+ * the H/L/M lists, number of kernel launches issued by the context so far. */
+int orac_gpu_stats(orac_gpu_ctx* ctx, int64_t* list_pairs /* [3] h,l,m */,
+                   int64_t* launches);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ORAC_GPU_H */

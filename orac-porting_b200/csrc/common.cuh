@@ -1,0 +1,254 @@
+// Internal definitions shared by the translation units of liborac_gpu.so.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "orac_gpu.h"
+
+// Maximum atoms per charge group handled by the pair kernel.  Exclusion and
+// skip masks are stored with a fixed stride of 8 bits per i-atom.
+#define ORAC_MAXG 8
+
+// Fixed-point scale of the force accumulators: 2^40 per internal force unit
+// (amu A fs^-2).  Resolution 9.1e-13, range +-8.4e6 internal units.
+#define ORAC_FSCALE 1099511627776.0
+#define ORAC_FSCALE_INV (1.0 / 1099511627776.0)
+
+// Fixed-point scale of the PME charge grid: 2^40 per internal charge unit.
+#define ORAC_QSCALE 1099511627776.0
+
+// Accumulator slots (double) of one force evaluation.
+enum {
+  ACC_CONF = 0,   // [3] LJ by type pair: slt-slt, slt-slv, slv-slv
+  ACC_COUL = 3,   // [3] Coulomb by type pair
+  ACC_VIMG = 6,   // [9] image term of the molecular virial, row-major
+  ACC_STR = 15,   // [9] sum_a F_a (x) co.Rm_a, row-major
+  ACC_N = 24
+};
+
+// A group-pair list in CSR form with fixed row capacities: row i occupies
+// [off[i], off[i+1]) and holds cnt[i] entries.  Nested shell lists reuse the
+// rows of their parent list.
+struct GList {
+  int* off = nullptr;   // [ngrp+1]
+  int* cnt = nullptr;   // [ngrp]
+  int* j = nullptr;     // [cap] partner group, 0-based, > row group
+  unsigned long long* mask = nullptr;  // [cap] skipped atom pairs, bit a*8+b
+  int64_t cap = 0;
+  int64_t npairs = 0;   // host copy, updated when read back
+  bool valid = false;
+};
+
+struct ShellRadii {
+  double rcutm, rtolm, rneim, rcutl, rtoll, rneil, rcuth, rtolh, rneih;
+};
+
+// Arguments of one pair-kernel launch (passed by value).
+struct PairArgs {
+  // topology
+  const double4* gpos;   // [G] scaled group centres (.w unused)
+  const int2* gmeta;     // [G] (first atom, natoms | ss_type << 8)
+  const float4* aoff;    // [N] Cartesian offset from group centre, charge
+  const int* atype;      // [N] 0-based LJ type
+  const float* apm;      // [N] mass fraction in group
+  const float2* lj;      // [ntype*ntype] (ecc12, ecc6), 0 when ecc6 <= 1e-12
+  int ntype;
+  int ngrp;
+  // box (upper triangular co)
+  double c11, c12, c13, c22, c23, c33;
+  // radii of this call (src/force.f:145-167)
+  double r2inn, r2inn0, r2out, r2out0, rinn0, rout0, r2neigh;
+  double arsout1, arsout2, arsinn1, arsinn2;
+  float alphal, twrtpi;
+  int forces_on, next_on, lskip, ewald;
+  // lists
+  const int* off;
+  const int* cnt;
+  const int* lj_;
+  const unsigned long long* lmask;
+  int* cnt_out;
+  int* j_out;
+  unsigned long long* mask_out;
+  // outputs
+  unsigned long long* ffix;  // [3N] x|y|z fixed point
+  double* acc;               // [ACC_N]
+  int natom;
+};
+
+struct PmePlan {
+  int n1 = 0, n2 = 0, n3 = 0, order = 0;
+  int h1 = 0;
+  float2* tw1 = nullptr;  // twiddles exp(-2 pi i k / n) per axis
+  float2* tw2 = nullptr;
+  float2* tw3 = nullptr;
+  float* bsp1 = nullptr;  // |DFT(B-spline)|^2 moduli (double -> float)
+  float* bsp2 = nullptr;
+  float* bsp3 = nullptr;
+  unsigned long long* qfix = nullptr;  // [n1*n2*n3] fixed-point charge grid
+  float2* cgrid = nullptr;             // [h1*n2*n3] complex grid
+  float* rgrid = nullptr;              // [n1*n2*n3] real grid after c2r
+  float4* theta = nullptr;             // per atom spline data cache
+  int natom_cap = 0;
+};
+
+// grow-only device scratch of the short-list and SPME host entry points
+struct ApiScratch {
+  double* cart = nullptr;
+  size_t cart_n = 0;
+  double* eout = nullptr;
+  int* ipairs = nullptr;
+  size_t ipairs_n = 0;
+  int* itype = nullptr;
+  size_t itype_n = 0;
+  double* t12 = nullptr;
+  double* t6 = nullptr;
+  size_t tab_n = 0;
+  int* ss = nullptr;
+  double* e4 = nullptr;
+  double* q = nullptr;
+  size_t q_n = 0;
+};
+
+struct orac_gpu_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  char err[1024] = {0};
+  int64_t launches = 0;
+
+  // sizes
+  int N = 0, G = 0, P = 0, ntype = 0, maxg = 0;
+  bool have_topo = false, have_box = false, have_ewald = false,
+       have_shells = false;
+
+  // host copies needed by the drivers
+  std::vector<int> h_gfirst, h_gn, h_amol, h_gmol;
+  std::vector<double> h_charge, h_mass;
+  std::vector<int> h_ss, h_nbtype;
+  std::vector<double> h_ecc12, h_ecc6;
+  ApiScratch api;
+
+  // device topology
+  int2* d_gmeta = nullptr;
+  int* d_atype = nullptr;
+  float* d_apm = nullptr;
+  float* d_aq = nullptr;
+  double* d_aqd = nullptr;
+  int* d_amol = nullptr;
+  int* d_agrp = nullptr;
+  int* d_gmol = nullptr;
+  unsigned char* d_amassinf = nullptr;
+  float2* d_lj = nullptr;
+  int* d_exoff = nullptr;  // [N+1]
+  int* d_exj = nullptr;    // 0-based partners j > i
+
+  // box and parameters
+  double co[9] = {0}, oc[9] = {0}, volume = 0;
+  ShellRadii sh{};
+  int clewld = 1;
+  double alphal = 0.35;
+  int order = 4, nfft1 = 0, nfft2 = 0, nfft3 = 0;
+  double rkcut = 1e9;
+  int ncx = 0, ncy = 0, ncz = 0;
+  double massinfty = 1e20;
+
+  // per-call device buffers
+  double* d_xyz = nullptr;  // [3N] scaled x|y|z
+  double* d_grp = nullptr;  // [3G]
+  double* d_mol = nullptr;  // [3P]
+  double4* d_gpos = nullptr;
+  float4* d_aoff = nullptr;
+  unsigned long long* d_ffix = nullptr;  // [3N]
+  double* d_acc = nullptr;               // [ACC_N]
+  double* d_fout = nullptr;              // [3N] double forces of one call
+  double* d_red = nullptr;               // [32] reduction scratch
+
+  // pinned host staging
+  double* h_stage = nullptr;
+  size_t h_stage_bytes = 0;
+
+  // lists: 0 = H (nnlpp0), 1 = L (nnlpp), 2 = M (nnlpp1)
+  GList lists[3];
+  int* d_scan_tmp = nullptr;
+  int64_t* d_total = nullptr;
+  int* d_flag = nullptr;
+
+  // cell list
+  int* d_cell_of = nullptr;   // [G]
+  int* d_cell_cnt = nullptr;  // [ncell+1]
+  int* d_cell_start = nullptr;
+  int* d_cell_grp = nullptr;  // [G]
+  int ncell_cap = 0;
+  int* d_stencil = nullptr;   // [3*nsten]
+  int nsten = 0;
+  double sten_rcut = -1, sten_co[9] = {0};
+  int sten_nc[3] = {0, 0, 0};
+
+  // PME
+  PmePlan pme;
+};
+
+// ---------------------------------------------------------------- errors
+int ctx_fail(orac_gpu_ctx* c, int code, const char* fmt, ...);
+
+#define CK(call)                                                            \
+  do {                                                                      \
+    cudaError_t e_ = (call);                                                \
+    if (e_ != cudaSuccess)                                                  \
+      return ctx_fail(ctx, ORAC_ERR_CUDA, "%s:%d %s: %s", __FILE__,        \
+                      __LINE__, #call, cudaGetErrorString(e_));             \
+  } while (0)
+
+#define CKL()                                                               \
+  do {                                                                      \
+    ctx->launches++;                                                        \
+    cudaError_t e_ = cudaGetLastError();                                    \
+    if (e_ != cudaSuccess)                                                  \
+      return ctx_fail(ctx, ORAC_ERR_CUDA, "%s:%d launch: %s", __FILE__,    \
+                      __LINE__, cudaGetErrorString(e_));                    \
+  } while (0)
+
+template <typename T>
+static inline int dev_alloc(orac_gpu_ctx* ctx, T** p, size_t n) {
+  if (*p) cudaFree(*p);
+  *p = nullptr;
+  if (n == 0) n = 1;
+  CK(cudaMalloc((void**)p, n * sizeof(T)));
+  return ORAC_OK;
+}
+
+// ------------------------------------------------------ internal drivers
+// k_list.cu
+int list_build_cells(orac_gpu_ctx* ctx, double rcut, GList* out);
+int list_build_allpairs(orac_gpu_ctx* ctx, double rcut, GList* out);
+int list_ensure_rows(orac_gpu_ctx* ctx, GList* L, const GList* parent);
+int list_masks(orac_gpu_ctx* ctx, GList* L);
+// k_pair.cu
+int pair_launch(orac_gpu_ctx* ctx, const PairArgs& a, int maxg);
+int prep_launch(orac_gpu_ctx* ctx, const double* xyz, const double* grp);
+int finalize_launch(orac_gpu_ctx* ctx, const double* mol, double* fout_accum);
+// k_pme.cu
+int pme_setup(orac_gpu_ctx* ctx, int n1, int n2, int n3, int order);
+// d_eout[16]: energy sum (eer = 0.5 * [0]), virial sums v11 v22 v33 v12 v13
+// v23 (x0.5 gives ORAC's vir), then the 9 molecular-correction terms
+// row-major.  d_sxyz/d_mol may be null (no molecular correction).
+int pme_run(orac_gpu_ctx* ctx, int natom, const double* d_cart /*3N*/,
+            const double* d_q, const double* recip, double volume,
+            double alpha, double* d_f /*3N accumulated*/, double* d_eout,
+            const double* d_sxyz, const double* d_mol);
+// k_small.cu: kind 0 fnb14, 1 fnbgrp, 2 ferrf; d_e[4]
+int small_launch(orac_gpu_ctx* ctx, int kind, const double* d_xyz,
+                 const int* d_pairs, const int* d_ptype, int npairs,
+                 const double* d_t12, const double* d_t6, double fudge,
+                 double lj_fudge, int coul_mode, int forces, double* d_f,
+                 double* d_e, const int* d_ss);
+int self_launch(orac_gpu_ctx* ctx, const int* d_ss, double* d_e);
+// api.cu
+int shell_run(orac_gpu_ctx* ctx, char rshell, const double* d_xyz,
+              const double* d_grp, const double* d_mol, double* d_f,
+              double* d_e, double* d_stress);

@@ -1,0 +1,396 @@
+// Real-space r-RESPA shell kernel: the B200 counterpart of ORAC's `force`
+// (src/force.f:1-917).
+//
+// One warp owns one i-group (a charge group, <= ORAC_MAXG atoms, staged in
+// shared memory); its 32 lanes walk the group's neighbour-list row, one
+// partner group per lane.  Per partner the lane
+//   1. forms the group-centre minimum image in FP64 scaled coordinates and
+//      classifies the pair into ORAC's bands (non-switched [rinn0, rout),
+//      switched S on [rout, rout0), 1-S on [rinn, rinn0)), src/force.f:265-333;
+//   2. writes the next inner shell's list entry (order preserved with a warp
+//      ballot), src/force.f:279-286;
+//   3. evaluates every atom pair of the two groups in FP32 -- LJ
+//      ecc12/r^12 - ecc6/r^6 and q q erfc_AS(alpha r)/r with the A&S 7.1.26
+//      polynomial ORAC uses -- skipping excluded pairs through the list
+//      entry's mask, src/force.f:396-731;
+//   4. for switched pairs adds the S'(R) V_ij term distributed by mass
+//      fraction, src/force.f:754-817.
+// i-atom forces stay in registers for the whole row and are warp-reduced
+// once; j-atom forces go to 64-bit fixed-point accumulators with atomics, so
+// the sum is independent of the order of the atomics.
+// The molecular virial is assembled without per-pair work: ORAC's
+// sum_pairs f (x) (Rm_i - Rm_j - img) equals sum_atoms F_a (x) Rm_a (done in
+// the finalize kernel) plus, for pairs that cross the box, G_ij (x) co.img
+// where G_ij is the pair's total force on the j group (done here).
+#include "common.cuh"
+
+namespace {
+
+constexpr int WPB = 4;  // warps per block
+constexpr float AS_A1 = 0.2548296f, AS_A2 = -0.28449674f, AS_A3 = 1.4214137f;
+constexpr float AS_A4 = -1.453152f, AS_A5 = 1.0614054f, AS_QP = 0.3275911f;
+constexpr int LJ_SMEM_MAX = 64 * 64;
+
+__device__ __forceinline__ void fix_add(unsigned long long* p, float v) {
+  long long q = __float2ll_rn(v * (float)ORAC_FSCALE);
+  if (q != 0) atomicAdd(p, (unsigned long long)q);
+}
+
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+__device__ __forceinline__ double warp_sumd(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+template <int MG>
+__global__ void __launch_bounds__(WPB * 32)
+    k_pair(const PairArgs A) {
+  extern __shared__ float2 s_lj[];
+  __shared__ float4 s_ai[WPB][MG];
+  __shared__ int s_ti[WPB][MG];
+  __shared__ float s_pm[WPB][MG];
+  __shared__ double s_red[WPB][ACC_N];
+
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nt2 = A.ntype * A.ntype;
+  const bool staged = nt2 <= LJ_SMEM_MAX;
+  if (staged)
+    for (int k = threadIdx.x; k < nt2; k += blockDim.x) s_lj[k] = A.lj[k];
+  __syncthreads();
+  const float2* lj = staged ? s_lj : A.lj;
+
+  double ec0 = 0, ec1 = 0, ec2 = 0, eq0 = 0, eq1 = 0, eq2 = 0;
+  float v00 = 0, v01 = 0, v02 = 0, v10 = 0, v11 = 0, v12 = 0, v20 = 0,
+        v21 = 0, v22 = 0;
+
+  for (int i = blockIdx.x * WPB + warp; i < A.ngrp; i += gridDim.x * WPB) {
+    const int2 mi = A.gmeta[i];
+    const int ifirst = mi.x, ni = mi.y & 0xff, typei = mi.y >> 8;
+    const double4 gi = A.gpos[i];
+    if (lane < ni) {
+      s_ai[warp][lane] = A.aoff[ifirst + lane];
+      s_ti[warp][lane] = A.atype[ifirst + lane];
+      s_pm[warp][lane] = A.apm[ifirst + lane];
+    }
+    __syncwarp();
+    float fi[MG][3];
+#pragma unroll
+    for (int a = 0; a < MG; a++) fi[a][0] = fi[a][1] = fi[a][2] = 0.f;
+
+    const int row = A.off[i], m = A.cnt[i];
+    int nout = 0;
+    for (int base = 0; base < m; base += 32) {
+      const int k = base + lane;
+      const bool valid = k < m;
+      int j = 0;
+      unsigned long long msk = 0ull;
+      double drj = 1e300, cx = 0, cy = 0, cz = 0, imx = 0, imy = 0, imz = 0;
+      if (valid) {
+        j = A.lj_[row + k];
+        msk = A.lmask[row + k];
+        const double4 gj = A.gpos[j];
+        double dx = gi.x - gj.x, dy = gi.y - gj.y, dz = gi.z - gj.z;
+        imx = 2.0 * round(0.5 * dx);
+        imy = 2.0 * round(0.5 * dy);
+        imz = 2.0 * round(0.5 * dz);
+        dx -= imx;
+        dy -= imy;
+        dz -= imz;
+        cx = A.c11 * dx + A.c12 * dy + A.c13 * dz;
+        cy = A.c22 * dy + A.c23 * dz;
+        cz = A.c33 * dz;
+        drj = cx * cx + cy * cy + cz * cz;
+      }
+      if (A.next_on) {
+        const bool keep = valid && drj < A.r2neigh;
+        const unsigned bal = __ballot_sync(0xffffffffu, keep);
+        if (keep) {
+          const int pos = nout + __popc(bal & ((1u << lane) - 1u));
+          A.j_out[row + pos] = j;
+          A.mask_out[row + pos] = msk;
+        }
+        nout += __popc(bal);
+      }
+      if (!A.forces_on || !valid) continue;
+      bool switched;
+      float sw = 1.f, dsw = 0.f;
+      if (drj >= A.r2inn0 && drj < A.r2out) {
+        switched = false;
+      } else if (drj >= A.r2out && drj < A.r2out0) {
+        const double rsp = sqrt(drj);
+        const double auxa = (A.arsout1 + 2.0 * rsp) / A.arsout2;
+        const double auxb = A.rout0 - rsp;
+        sw = (float)(auxa * auxb * auxb);
+        dsw = (float)((-2.0 * auxa * auxb + 2.0 * auxb * auxb / A.arsout2) / rsp);
+        switched = true;
+      } else if (drj >= A.r2inn && drj < A.r2inn0) {
+        const double rsp = sqrt(drj);
+        const double auxa = (A.arsinn1 + 2.0 * rsp) / A.arsinn2;
+        const double auxb = A.rinn0 - rsp;
+        sw = (float)(1.0 - auxa * auxb * auxb);
+        dsw = (float)((2.0 * auxa * auxb - 2.0 * auxb * auxb / A.arsinn2) / rsp);
+        switched = true;
+      } else {
+        continue;
+      }
+      const int2 mj = A.gmeta[j];
+      const int jfirst = mj.x, nj = mj.y & 0xff, typej = mj.y >> 8;
+      const float dcx = (float)cx, dcy = (float)cy, dcz = (float)cz;
+      float pconf = 0.f, pcoul = 0.f, vsum = 0.f;
+      float gx = 0.f, gy = 0.f, gz = 0.f;  // total force on the j group
+      for (int b = 0; b < nj; b++) {
+        const float4 ob = A.aoff[jfirst + b];
+        const int tb = A.atype[jfirst + b];
+        float fbx = 0.f, fby = 0.f, fbz = 0.f;
+#pragma unroll
+        for (int a = 0; a < MG; a++) {
+          if (a >= ni) break;
+          if ((msk >> (a * 8 + b)) & 1ull) continue;
+          const float4 ai = s_ai[warp][a];
+          const float2 L = lj[s_ti[warp][a] * A.ntype + tb];
+          const bool ljon = L.y != 0.f;
+          if (A.lskip && !ljon && A.ewald) continue;  // src/force.f:416-417
+          const float rx = dcx + ai.x - ob.x;
+          const float ry = dcy + ai.y - ob.y;
+          const float rz = dcz + ai.z - ob.z;
+          const float r2 = rx * rx + ry * ry + rz * rz;
+          const float rsqi = 1.0f / r2;
+          float qf = 0.f, conf = 0.f, coul = 0.f;
+          if (ljon) {
+            const float r6 = rsqi * rsqi * rsqi;
+            const float r12 = r6 * r6;
+            qf = (12.0f * L.x * r12 - 6.0f * L.y * r6) * rsqi;
+            conf = L.x * r12 - L.y * r6;
+          }
+          if (!A.lskip) {
+            const float rsp = sqrtf(r2);
+            const float ar = A.alphal * rsp;
+            const float qt = 1.0f / (1.0f + AS_QP * ar);
+            const float ex = expf(-ar * ar);
+            const float erfcst =
+                ((((AS_A5 * qt + AS_A4) * qt + AS_A3) * qt + AS_A2) * qt + AS_A1) *
+                qt * ex;
+            const float qq = ai.w * ob.w;
+            coul = qq * erfcst / rsp;
+            qf += qq * (erfcst + A.twrtpi * ar * ex) * rsqi / rsp;
+          } else if (!A.ewald) {
+            const float rsp = sqrtf(r2);
+            coul = ai.w * ob.w / rsp;
+            qf += coul * rsqi;
+          }
+          if (switched) {
+            vsum += conf + coul;
+            qf *= sw;
+          }
+          pconf += conf;
+          pcoul += coul;
+          const float fx = qf * rx, fy = qf * ry, fz = qf * rz;
+          fi[a][0] += fx;
+          fi[a][1] += fy;
+          fi[a][2] += fz;
+          fbx -= fx;
+          fby -= fy;
+          fbz -= fz;
+        }
+        gx += fbx;
+        gy += fby;
+        gz += fbz;
+        fix_add(A.ffix + jfirst + b, fbx);
+        fix_add(A.ffix + A.natom + jfirst + b, fby);
+        fix_add(A.ffix + 2 * A.natom + jfirst + b, fbz);
+      }
+      if (switched) {
+        pconf *= sw;
+        pcoul *= sw;
+        // S'(R) V term: X = -dS/dR / R * V * R_vec on i atoms by mass fraction
+        const float sx = -dsw * vsum * dcx, sy = -dsw * vsum * dcy,
+                    sz = -dsw * vsum * dcz;
+#pragma unroll
+        for (int a = 0; a < MG; a++) {
+          if (a >= ni) break;
+          const float pm = s_pm[warp][a];
+          fi[a][0] += pm * sx;
+          fi[a][1] += pm * sy;
+          fi[a][2] += pm * sz;
+        }
+        for (int b = 0; b < nj; b++) {
+          const float pm = A.apm[jfirst + b];
+          fix_add(A.ffix + jfirst + b, -pm * sx);
+          fix_add(A.ffix + A.natom + jfirst + b, -pm * sy);
+          fix_add(A.ffix + 2 * A.natom + jfirst + b, -pm * sz);
+        }
+        gx -= sx;
+        gy -= sy;
+        gz -= sz;
+      }
+      const int t = typei + typej - 2;  // 0 slt-slt, 1 slt-slv, 2 slv-slv
+      if (t == 0) {
+        ec0 += pconf;
+        eq0 += pcoul;
+      } else if (t == 1) {
+        ec1 += pconf;
+        eq1 += pcoul;
+      } else {
+        ec2 += pconf;
+        eq2 += pcoul;
+      }
+      if (imx != 0.0 || imy != 0.0 || imz != 0.0) {
+        // j sits at its image xpg_j + img: its virial arm gains co.img
+        const float ix = (float)(A.c11 * imx + A.c12 * imy + A.c13 * imz);
+        const float iy = (float)(A.c22 * imy + A.c23 * imz);
+        const float iz = (float)(A.c33 * imz);
+        v00 += gx * ix;
+        v01 += gx * iy;
+        v02 += gx * iz;
+        v10 += gy * ix;
+        v11 += gy * iy;
+        v12 += gy * iz;
+        v20 += gz * ix;
+        v21 += gz * iy;
+        v22 += gz * iz;
+      }
+    }
+    if (A.next_on && lane == 0) A.cnt_out[i] = nout;
+    if (A.forces_on) {
+#pragma unroll
+      for (int a = 0; a < MG; a++) {
+        if (a >= ni) break;
+        const float sx = warp_sum(fi[a][0]);
+        const float sy = warp_sum(fi[a][1]);
+        const float sz = warp_sum(fi[a][2]);
+        if (lane == 0) {
+          fix_add(A.ffix + ifirst + a, sx);
+          fix_add(A.ffix + A.natom + ifirst + a, sy);
+          fix_add(A.ffix + 2 * A.natom + ifirst + a, sz);
+        }
+      }
+    }
+    __syncwarp();
+  }
+  if (!A.forces_on) return;
+  // block reduction of energies and image virial
+  double vals[15] = {ec0, ec1, ec2, eq0, eq1, eq2, v00, v01, v02,
+                     v10, v11, v12, v20, v21, v22};
+#pragma unroll
+  for (int q = 0; q < 15; q++) {
+    const double s = warp_sumd(vals[q]);
+    if (lane == 0) s_red[warp][q] = s;
+  }
+  __syncthreads();
+  if (threadIdx.x < 15) {
+    double s = 0;
+    for (int w = 0; w < WPB; w++) s += s_red[w][threadIdx.x];
+    if (s != 0.0) atomicAdd(A.acc + threadIdx.x, s);  // slots 0..14 = ACC_CONF..ACC_VIMG+8
+  }
+}
+
+// group centres as double4 and atom offsets from their group centre
+__global__ void k_prep(int N, int G, const double* __restrict__ xyz,
+                       const double* __restrict__ grp,
+                       const int* __restrict__ agrp,
+                       const float* __restrict__ aq, double c11, double c12,
+                       double c13, double c22, double c23, double c33,
+                       double4* __restrict__ gpos, float4* __restrict__ aoff,
+                       unsigned long long* __restrict__ ffix) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < G) gpos[t] = make_double4(grp[t], grp[G + t], grp[2 * G + t], 0.0);
+  if (t < N) {
+    const int g = agrp[t];
+    const double dx = xyz[t] - grp[g];
+    const double dy = xyz[N + t] - grp[G + g];
+    const double dz = xyz[2 * N + t] - grp[2 * G + g];
+    aoff[t] = make_float4((float)(c11 * dx + c12 * dy + c13 * dz),
+                          (float)(c22 * dy + c23 * dz), (float)(c33 * dz),
+                          aq[t]);
+    ffix[t] = 0ull;
+    ffix[N + t] = 0ull;
+    ffix[2 * N + t] = 0ull;
+  }
+}
+
+// fixed point -> double forces (accumulated into fout) and the atom part of
+// the molecular virial: sum_a F_a (x) co.Rm_a
+__global__ void k_finalize(int N, const unsigned long long* __restrict__ ffix,
+                           const double* __restrict__ mol, int P,
+                           const int* __restrict__ amol, double c11, double c12,
+                           double c13, double c22, double c23, double c33,
+                           double* __restrict__ fout, double* __restrict__ acc) {
+  __shared__ double s_red[8][9];
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  double st[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  if (t < N) {
+    const double fx = (double)(long long)ffix[t] * ORAC_FSCALE_INV;
+    const double fy = (double)(long long)ffix[N + t] * ORAC_FSCALE_INV;
+    const double fz = (double)(long long)ffix[2 * N + t] * ORAC_FSCALE_INV;
+    fout[t] += fx;
+    fout[N + t] += fy;
+    fout[2 * N + t] += fz;
+    const int p = amol[t];
+    const double sx = mol[p], sy = mol[P + p], sz = mol[2 * P + p];
+    const double rx = c11 * sx + c12 * sy + c13 * sz;
+    const double ry = c22 * sy + c23 * sz;
+    const double rz = c33 * sz;
+    st[0] = fx * rx;
+    st[1] = fx * ry;
+    st[2] = fx * rz;
+    st[3] = fy * rx;
+    st[4] = fy * ry;
+    st[5] = fy * rz;
+    st[6] = fz * rx;
+    st[7] = fz * ry;
+    st[8] = fz * rz;
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int q = 0; q < 9; q++) {
+    const double s = warp_sumd(st[q]);
+    if (lane == 0) s_red[warp][q] = s;
+  }
+  __syncthreads();
+  if (threadIdx.x < 9) {
+    double s = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) s += s_red[w][threadIdx.x];
+    atomicAdd(acc + ACC_STR + threadIdx.x, s);
+  }
+}
+
+}  // namespace
+
+int pair_launch(orac_gpu_ctx* ctx, const PairArgs& a, int maxg) {
+  int nb = (a.ngrp + WPB - 1) / WPB;
+  if (nb < 1) nb = 1;
+  const size_t smem = (size_t)(a.ntype * a.ntype <= LJ_SMEM_MAX ? a.ntype * a.ntype : 0) * sizeof(float2);
+  if (maxg <= 4) {
+    k_pair<4><<<nb, WPB * 32, smem, ctx->stream>>>(a);
+  } else if (maxg <= 8) {
+    k_pair<8><<<nb, WPB * 32, smem, ctx->stream>>>(a);
+  } else {
+    return ctx_fail(ctx, ORAC_ERR_PARAM, "charge group of %d atoms exceeds %d", maxg, ORAC_MAXG);
+  }
+  CKL();
+  return ORAC_OK;
+}
+
+int prep_launch(orac_gpu_ctx* ctx, const double* xyz, const double* grp) {
+  const int n = ctx->N > ctx->G ? ctx->N : ctx->G;
+  const double* c = ctx->co;
+  k_prep<<<(n + 255) / 256, 256, 0, ctx->stream>>>(
+      ctx->N, ctx->G, xyz, grp, ctx->d_agrp, ctx->d_aq, c[0], c[3], c[6], c[4], c[7], c[8], ctx->d_gpos,
+      ctx->d_aoff, ctx->d_ffix);
+  CKL();
+  return ORAC_OK;
+}
+
+int finalize_launch(orac_gpu_ctx* ctx, const double* mol, double* fout) {
+  const double* c = ctx->co;
+  k_finalize<<<(ctx->N + 255) / 256, 256, 0, ctx->stream>>>(ctx->N, ctx->d_ffix, mol, ctx->P, ctx->d_amol, c[0],
+                                                            c[3], c[6], c[4], c[7], c[8], fout, ctx->d_acc);
+  CKL();
+  return ORAC_OK;
+}

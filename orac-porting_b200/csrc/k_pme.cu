@@ -1,0 +1,654 @@
+// Smooth particle-mesh Ewald on the GPU: the counterpart of ORAC's FFTW
+// build of do_pmesh_kspace (src/pme_fftw3.f90:56-130) with scalar_sum
+// (src/scalar_sum.f:2-135), replacing FFTW by a shared-memory FFT.
+//
+//   k_spread      fractional coordinates in FP64 (get_scaled_fractionals,
+//                 pme_fftw3.f90:132-163), cardinal B-splines in FP32
+//                 (fill_bspline :518-576), charge spreading with 64-bit
+//                 fixed-point atomics (fill_charge_grid :233-298) so the grid
+//                 does not depend on the order of the atomics
+//   k_fft<MODE>   Stockham mixed-radix (2,3,4,5,7) FFT of batches of grid lines
+//                 held in shared memory; MODE selects the axis and the
+//                 r2c / c2c / c2r form.  FFTW's conventions: r2c forward
+//                 exp(-i..) along the fastest axis n1 giving (n1/2+1,n2,n3),
+//                 c2r backward, unnormalised.
+//   ZCONV         the z pass runs forward FFT, the influence function of
+//                 scalar_sum (energy and virial with ORAC's fac12/13/23
+//                 masks, FP64 reductions) and the inverse FFT on the same
+//                 lines without leaving shared memory
+//   k_gather      forces (grad_sum :310-372) and the molecular virial
+//                 correction of fft_pme (src/fft_pme.f:65-106)
+#include <cmath>
+
+#include "common.cuh"
+
+namespace {
+
+constexpr int MAXR = 12;  // max radix stages
+struct FftPlan {
+  int n;
+  int nst;
+  int rad[MAXR];
+};
+
+int make_plan(int n, FftPlan* p) {
+  p->n = n;
+  p->nst = 0;
+  int m = n;
+  while (m % 4 == 0 && p->nst < MAXR) {
+    p->rad[p->nst++] = 4;
+    m /= 4;
+  }
+  const int rs[] = {2, 3, 5, 7};
+  for (int r : rs)
+    while (m % r == 0 && p->nst < MAXR) {
+      p->rad[p->nst++] = r;
+      m /= r;
+    }
+  return m == 1 ? 0 : -1;
+}
+
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+
+// W_n^k for sign -1 (forward) is tw[k]; sign +1 takes the conjugate.
+__device__ __forceinline__ float2 twid(const float2* tw, int n, int k, int sign) {
+  float2 w = tw[k % n];
+  if (sign > 0) w.y = -w.y;
+  return w;
+}
+
+// Stockham passes over `nl` lines of length n stored line-major in a; the
+// result ends in the returned buffer (a or b).
+__device__ float2* fft_smem(float2* a, float2* b, int nl, const FftPlan& P, const float2* tw, int sign) {
+  const int n = P.n;
+  int Ns = 1;
+  for (int s = 0; s < P.nst; s++) {
+    const int R = P.rad[s];
+    const int nb = n / R;
+    const int tot = nl * nb;
+    for (int t = threadIdx.x; t < tot; t += blockDim.x) {
+      const int l = t / nb, j = t - l * nb;
+      const float2* in = a + l * n;
+      float2* out = b + l * n;
+      const int k = j % Ns;
+      const int tstep = k * (n / (Ns * R));
+      float2 v[7];
+      for (int r = 0; r < R; r++) {
+        float2 x = in[j + r * nb];
+        if (r && tstep) x = cmul(x, twid(tw, n, tstep * r, sign));
+        v[r] = x;
+      }
+      const int idxD = (j / Ns) * Ns * R + k;
+      if (R == 2) {
+        out[idxD] = cadd(v[0], v[1]);
+        out[idxD + Ns] = csub(v[0], v[1]);
+      } else if (R == 4) {
+        const float2 s02 = cadd(v[0], v[2]), d02 = csub(v[0], v[2]);
+        const float2 s13 = cadd(v[1], v[3]), d13 = csub(v[1], v[3]);
+        // -i*sign(-1) d13 : forward multiplies by -i, inverse by +i
+        const float2 rot = sign < 0 ? make_float2(d13.y, -d13.x) : make_float2(-d13.y, d13.x);
+        out[idxD] = cadd(s02, s13);
+        out[idxD + Ns] = cadd(d02, rot);
+        out[idxD + 2 * Ns] = csub(s02, s13);
+        out[idxD + 3 * Ns] = csub(d02, rot);
+      } else {
+        for (int q = 0; q < R; q++) {
+          float2 acc = v[0];
+          for (int r = 1; r < R; r++) acc = cadd(acc, cmul(v[r], twid(tw, n, ((r * q) % R) * nb, sign)));
+          out[idxD + q * Ns] = acc;
+        }
+      }
+    }
+    __syncthreads();
+    float2* t = a;
+    a = b;
+    b = t;
+    Ns *= R;
+  }
+  return a;
+}
+
+__device__ __forceinline__ double warp_sumd(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Block reduction of NV doubles into out[] with atomics.
+template <int NV>
+__device__ void block_reduce_add(double* v, double* out) {
+  __shared__ double s[32][NV];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int q = 0; q < NV; q++) {
+    const double x = warp_sumd(v[q]);
+    if (lane == 0) s[w][q] = x;
+  }
+  __syncthreads();
+  if (threadIdx.x < NV) {
+    double x = 0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); k++) x += s[k][threadIdx.x];
+    if (x != 0.0) atomicAdd(out + threadIdx.x, x);
+  }
+}
+
+struct GridArgs {
+  int n1, n2, n3, h1;
+  const unsigned long long* qfix;
+  float2* cg;
+  float* rg;
+  const float2* tw;
+  FftPlan P;
+  int B;  // lines per block
+  // convolution
+  const float* bsp1;
+  const float* bsp2;
+  const float* bsp3;
+  double r11, r12, r13, r21, r22, r23, r31, r32, r33;  // recip(i,j)
+  float fac, pivol;  // pi^2/alpha^2, pi*volume
+  double rkcut2;
+  double* eout;  // [7] energy, v11 v22 v33 v12 v13 v23
+};
+
+enum { XF = 0, YF = 1, ZC = 2, YI = 3, XI = 4 };
+
+template <int MODE>
+__global__ void __launch_bounds__(256) k_fft(const GridArgs A) {
+  extern __shared__ float2 sm[];
+  const int n = A.P.n;
+  const int B = A.B;
+  float2* a = sm;
+  float2* b = sm + B * n;
+  // line geometry
+  int nlines, i0 = 0, j0 = 0, k0 = 0, nl;
+  if (MODE == XF || MODE == XI) {
+    nlines = A.n2 * A.n3;
+    const int L0 = blockIdx.x * B;
+    nl = min(B, nlines - L0);
+    j0 = L0;  // linear (j + n2 k) of first line
+  } else if (MODE == YF || MODE == YI) {
+    const int nib = (A.h1 + B - 1) / B;
+    k0 = blockIdx.x / nib;
+    i0 = (blockIdx.x % nib) * B;
+    nl = min(B, A.h1 - i0);
+  } else {
+    const int nib = (A.h1 + B - 1) / B;
+    j0 = blockIdx.x / nib;
+    i0 = (blockIdx.x % nib) * B;
+    nl = min(B, A.h1 - i0);
+  }
+  // ---- load
+  if (MODE == XF) {
+    const size_t g0 = (size_t)j0 * A.n1;
+    for (int e = threadIdx.x; e < nl * n; e += blockDim.x) {
+      const long long q = (long long)A.qfix[g0 + e];
+      a[e] = make_float2((float)((double)q * (1.0 / ORAC_QSCALE)), 0.f);
+    }
+  } else if (MODE == XI) {
+    // Hermitian extension of the half line (c2r)
+    const int h1 = A.h1;
+    for (int e = threadIdx.x; e < nl * n; e += blockDim.x) {
+      const int l = e / n, i = e - l * n;
+      const size_t row = (size_t)(j0 + l) * h1;
+      float2 v;
+      if (i < h1) {
+        v = A.cg[row + i];
+      } else {
+        v = A.cg[row + (n - i)];
+        v.y = -v.y;
+      }
+      a[e] = v;
+    }
+  } else if (MODE == YF || MODE == YI) {
+    for (int e = threadIdx.x; e < nl * n; e += blockDim.x) {
+      const int pos = e / nl, l = e - pos * nl;
+      a[l * n + pos] = A.cg[((size_t)k0 * A.n2 + pos) * A.h1 + i0 + l];
+    }
+  } else {
+    for (int e = threadIdx.x; e < nl * n; e += blockDim.x) {
+      const int pos = e / nl, l = e - pos * nl;
+      a[l * n + pos] = A.cg[((size_t)pos * A.n2 + j0) * A.h1 + i0 + l];
+    }
+  }
+  __syncthreads();
+  const int sign = (MODE == XF || MODE == YF) ? -1 : +1;
+  float2* res = fft_smem(a, b, nl, A.P, A.tw, MODE == ZC ? -1 : sign);
+  if (MODE == ZC) {
+    // influence function, src/scalar_sum.f:40-121 (element (1,1,1) untouched)
+    double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+    const int ndim1 = A.h1;
+    int nf1 = A.n1 / 2;
+    if (2 * nf1 < A.n1) nf1++;
+    int nf2 = A.n2 / 2;
+    if (2 * nf2 < A.n2) nf2++;
+    int nf3 = A.n3 / 2;
+    if (2 * nf3 < A.n3) nf3++;
+    for (int e = threadIdx.x; e < nl * n; e += blockDim.x) {
+      const int l = e / n, kk = e - l * n;
+      const int k1 = i0 + l + 1, k2 = j0 + 1, k3 = kk + 1;
+      if (k1 == 1 && k2 == 1 && k3 == 1) continue;
+      const int m1 = k1 > nf1 ? k1 - 1 - A.n1 : k1 - 1;
+      const int m2 = k2 > nf2 ? k2 - 1 - A.n2 : k2 - 1;
+      const int m3 = k3 > nf3 ? k3 - 1 - A.n3 : k3 - 1;
+      const double mh1 = A.r11 * m1 + A.r12 * m2 + A.r13 * m3;
+      const double mh2 = A.r21 * m1 + A.r22 * m2 + A.r23 * m3;
+      const double mh3 = A.r31 * m1 + A.r32 * m2 + A.r33 * m3;
+      const double msq = mh1 * mh1 + mh2 * mh2 + mh3 * mh3;
+      float2 q = res[e];
+      float eterm = 0.f;
+      if (msq <= A.rkcut2) {
+        const float fm = (float)msq;
+        const float denom = A.pivol * A.bsp1[k1 - 1] * A.bsp2[k2 - 1] * A.bsp3[k3 - 1] * fm;
+        eterm = expf(-A.fac * fm) / denom;
+        const double vterm = 2.0 * ((double)A.fac * msq + 1.0) / msq;
+        const double q2 = (double)q.x * q.x + (double)q.y * q.y;
+        double struc2;
+        double f12 = 1, f13 = 1, f23 = 1;
+        if (k1 == 1 || (k1 == ndim1 && (A.n1 % 2) == 0)) {
+          struc2 = (double)eterm * q2;
+        } else {
+          struc2 = 2.0 * (double)eterm * q2;
+          f12 = (mh1 * mh2 < 0.0 && k2 <= ndim1) ? 0.0 : 1.0;
+          f13 = (mh1 * mh3 < 0.0 && k3 <= ndim1) ? 0.0 : 1.0;
+          const bool neg = mh2 * mh3 < 0.0;
+          if (k2 <= ndim1 && k3 <= ndim1)
+            f23 = neg ? 0.0 : 1.0;
+          else if (k2 > ndim1 && k3 <= ndim1)
+            f23 = neg ? 1.0 : 0.0;
+          else if (k3 > ndim1 && k2 <= ndim1)
+            f23 = neg ? 1.0 : 0.0;
+          else
+            f23 = neg ? 0.0 : 1.0;
+        }
+        const double vvir = struc2 * vterm;
+        acc[0] += struc2;
+        acc[1] += struc2 * (vterm * mh1 * mh1 - 1.0);
+        acc[2] += struc2 * (vterm * mh2 * mh2 - 1.0);
+        acc[3] += struc2 * (vterm * mh3 * mh3 - 1.0);
+        acc[4] += vvir * mh1 * mh2 * f12;
+        acc[5] += vvir * mh1 * mh3 * f13;
+        acc[6] += vvir * mh2 * mh3 * f23;
+      }
+      res[e] = make_float2(q.x * eterm, q.y * eterm);
+    }
+    __syncthreads();
+    block_reduce_add<7>(acc, A.eout);
+    float2* other = (res == a) ? b : a;
+    res = fft_smem(res, other, nl, A.P, A.tw, +1);
+  }
+  // ---- store
+  if (MODE == XF) {
+    const int h1 = A.h1;
+    for (int e = threadIdx.x; e < nl * h1; e += blockDim.x) {
+      const int l = e / h1, i = e - l * h1;
+      A.cg[(size_t)(j0 + l) * h1 + i] = res[l * n + i];
+    }
+  } else if (MODE == XI) {
+    const size_t g0 = (size_t)j0 * A.n1;
+    for (int e = threadIdx.x; e < nl * n; e += blockDim.x) A.rg[g0 + e] = res[e].x;
+  } else if (MODE == YF || MODE == YI) {
+    for (int e = threadIdx.x; e < nl * n; e += blockDim.x) {
+      const int pos = e / nl, l = e - pos * nl;
+      A.cg[((size_t)k0 * A.n2 + pos) * A.h1 + i0 + l] = res[l * n + pos];
+    }
+  } else {
+    for (int e = threadIdx.x; e < nl * n; e += blockDim.x) {
+      const int pos = e / nl, l = e - pos * nl;
+      A.cg[((size_t)pos * A.n2 + j0) * A.h1 + i0 + l] = res[l * n + pos];
+    }
+  }
+}
+
+struct AtomArgs {
+  int natom, order, n1, n2, n3;
+  const double* xyz;  // [3N] Cartesian
+  const double* q;
+  double r11, r12, r13, r21, r22, r23, r31, r32, r33;
+  unsigned long long* qfix;
+  const float* rg;
+  double* f;  // [3N] accumulated
+  // molecular correction (optional)
+  const double* sxyz;  // [3N] scaled
+  const double* mol;   // [3P] scaled
+  const int* amol;
+  int P;
+  double c11, c12, c13, c22, c23, c33;
+  double* eout;  // [7+9]
+};
+
+// fill_bspline restated in FP32 (src/pme_fftw3.f90:518-576)
+__device__ __forceinline__ void bspline(float w, int order, float* c, float* d) {
+  c[order - 1] = 0.f;
+  c[1] = w;
+  c[0] = 1.f - w;
+  for (int k = 3; k <= order - 1; k++) {
+    const float div = 1.f / (k - 1);
+    c[k - 1] = div * w * c[k - 2];
+    for (int j = 1; j <= k - 2; j++) c[k - j - 1] = div * ((w + j) * c[k - j - 2] + (k - j - w) * c[k - j - 1]);
+    c[0] = div * (1.f - w) * c[0];
+  }
+  d[0] = -c[0];
+  for (int j = 2; j <= order; j++) d[j - 1] = c[j - 2] - c[j - 1];
+  {
+    const int k = order;
+    const float div = 1.f / (k - 1);
+    c[k - 1] = div * w * c[k - 2];
+    for (int j = 1; j <= k - 2; j++) c[k - j - 1] = div * ((w + j) * c[k - j - 2] + (k - j - w) * c[k - j - 1]);
+    c[0] = div * (1.f - w) * c[0];
+  }
+}
+
+constexpr int MAXORD = 12;
+
+__device__ __forceinline__ void frac_coord(const AtomArgs& A, int t, double* fr) {
+  const double x = A.xyz[t], y = A.xyz[A.natom + t], z = A.xyz[2 * A.natom + t];
+  double w = x * A.r11 + y * A.r21 + z * A.r31;
+  fr[0] = A.n1 * (w - round(w) + 0.5);
+  w = x * A.r12 + y * A.r22 + z * A.r32;
+  fr[1] = A.n2 * (w - round(w) + 0.5);
+  w = x * A.r13 + y * A.r23 + z * A.r33;
+  fr[2] = A.n3 * (w - round(w) + 0.5);
+}
+
+// w - anint(w) + 0.5 lies in [0, 1] for finite w, so fr lies in [0, n]
+__device__ __forceinline__ bool frac_ok(const AtomArgs& A, const double* fr) {
+  return fr[0] >= 0.0 && fr[0] <= A.n1 && fr[1] >= 0.0 && fr[1] <= A.n2 && fr[2] >= 0.0 && fr[2] <= A.n3;
+}
+
+__device__ __forceinline__ int gidx(int k0, int n) {
+  int k = k0 >= 0 ? k0 : k0 + n;
+  if (k >= n) k -= n;  // fractional coordinate exactly at n
+  return k;
+}
+
+// one thread per (atom, i3 plane)
+__global__ void k_spread(const AtomArgs A) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int p = A.order;
+  if (t >= A.natom * p) return;
+  const int at = t / p, i3 = t - at * p;
+  double fr[3];
+  frac_coord(A, at, fr);
+  if (!frac_ok(A, fr)) return;  // non-finite coordinates never index the grid
+  float th1[MAXORD], th2[MAXORD], th3[MAXORD], d[MAXORD];
+  bspline((float)(fr[0] - (int)fr[0]), p, th1, d);
+  bspline((float)(fr[1] - (int)fr[1]), p, th2, d);
+  bspline((float)(fr[2] - (int)fr[2]), p, th3, d);
+  const float qa = (float)A.q[at];
+  const int kk = gidx((int)fr[2] - p + 1 + i3, A.n3);
+  for (int i2 = 0; i2 < p; i2++) {
+    const int jj = gidx((int)fr[1] - p + 1 + i2, A.n2);
+    const float prod = th2[i2] * th3[i3] * qa;
+    unsigned long long* row = A.qfix + ((size_t)kk * A.n2 + jj) * A.n1;
+    for (int i1 = 0; i1 < p; i1++) {
+      const int ii = gidx((int)fr[0] - p + 1 + i1, A.n1);
+      const long long v = __double2ll_rn((double)(th1[i1] * prod) * ORAC_QSCALE);
+      if (v) atomicAdd(row + ii, (unsigned long long)v);
+    }
+  }
+}
+
+__global__ void k_gather(const AtomArgs A) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int p = A.order;
+  double st[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  double fr[3] = {0, 0, 0};
+  if (t < A.natom) frac_coord(A, t, fr);
+  if (t < A.natom && frac_ok(A, fr)) {
+    float th1[MAXORD], th2[MAXORD], th3[MAXORD], d1[MAXORD], d2[MAXORD], d3[MAXORD];
+    bspline((float)(fr[0] - (int)fr[0]), p, th1, d1);
+    bspline((float)(fr[1] - (int)fr[1]), p, th2, d2);
+    bspline((float)(fr[2] - (int)fr[2]), p, th3, d3);
+    float f1 = 0.f, f2 = 0.f, f3 = 0.f;
+    for (int i3 = 0; i3 < p; i3++) {
+      const int kk = gidx((int)fr[2] - p + 1 + i3, A.n3);
+      for (int i2 = 0; i2 < p; i2++) {
+        const int jj = gidx((int)fr[1] - p + 1 + i2, A.n2);
+        const float* row = A.rg + ((size_t)kk * A.n2 + jj) * A.n1;
+        float s1 = 0.f, s2 = 0.f, s3 = 0.f;
+        for (int i1 = 0; i1 < p; i1++) {
+          const float qv = row[gidx((int)fr[0] - p + 1 + i1, A.n1)];
+          s1 += d1[i1] * qv;
+          s2 += th1[i1] * qv;
+        }
+        s3 = s2;
+        f1 += s1 * th2[i2] * th3[i3];
+        f2 += s2 * d2[i2] * th3[i3];
+        f3 += s3 * th2[i2] * d3[i3];
+      }
+    }
+    const double qa = A.q[t];
+    const double g1 = -A.n1 * qa * (double)f1, g2 = -A.n2 * qa * (double)f2, g3 = -A.n3 * qa * (double)f3;
+    const double fx = A.r11 * g1 + A.r12 * g2 + A.r13 * g3;
+    const double fy = A.r21 * g1 + A.r22 * g2 + A.r23 * g3;
+    const double fz = A.r31 * g1 + A.r32 * g2 + A.r33 * g3;
+    A.f[t] += fx;
+    A.f[A.natom + t] += fy;
+    A.f[2 * A.natom + t] += fz;
+    if (A.sxyz) {
+      const int m = A.amol[t];
+      const double sx = A.sxyz[t] - A.mol[m], sy = A.sxyz[A.natom + t] - A.mol[A.P + m],
+                   sz = A.sxyz[2 * A.natom + t] - A.mol[2 * A.P + m];
+      const double gx = sx * A.c11 + sy * A.c12 + sz * A.c13;
+      const double gy = sy * A.c22 + sz * A.c23;
+      const double gz = sz * A.c33;
+      st[0] = -gx * fx;
+      st[1] = -gy * fx;
+      st[2] = -gz * fx;
+      st[3] = -gx * fy;
+      st[4] = -gy * fy;
+      st[5] = -gz * fy;
+      st[6] = -gx * fz;
+      st[7] = -gy * fz;
+      st[8] = -gz * fz;
+    }
+  }
+  if (A.sxyz) block_reduce_add<9>(st, A.eout + 7);
+}
+
+void host_bspline(double w, int order, double* c, double* d) {
+  c[order - 1] = 0.0;
+  c[1] = w;
+  c[0] = 1.0 - w;
+  for (int k = 3; k <= order - 1; k++) {
+    const double div = 1.0 / (k - 1);
+    c[k - 1] = div * w * c[k - 2];
+    for (int j = 1; j <= k - 2; j++) c[k - j - 1] = div * ((w + j) * c[k - j - 2] + (k - j - w) * c[k - j - 1]);
+    c[0] = div * (1 - w) * c[0];
+  }
+  d[0] = -c[0];
+  for (int j = 2; j <= order; j++) d[j - 1] = c[j - 2] - c[j - 1];
+  const int k = order;
+  const double div = 1.0 / (k - 1);
+  c[k - 1] = div * w * c[k - 2];
+  for (int j = 1; j <= k - 2; j++) c[k - j - 1] = div * ((w + j) * c[k - j - 2] + (k - j - w) * c[k - j - 1]);
+  c[0] = div * (1 - w) * c[0];
+}
+
+// load_bsp_moduli + DFTMOD (src/pme_fftw3.f90:165-230); twopi is 2 times a
+// default-real (single precision) literal of pi in the reference.
+void host_bsp_moduli(int nfft, int order, std::vector<float>& out) {
+  std::vector<double> arr(order + 2), darr(order + 2), bsp(nfft + order + 2, 0.0), mod(nfft);
+  host_bspline(0.0, order, arr.data(), darr.data());
+  for (int i = 2; i <= order + 1 && i <= nfft; i++) bsp[i - 1] = arr[i - 2];
+  const double twopi = 2.0 * (double)3.14159265358979323846f;
+  for (int k = 1; k <= nfft; k++) {
+    double s1 = 0, s2 = 0;
+    for (int j = 1; j <= nfft; j++) {
+      const double arg = twopi * (k - 1) * (j - 1) / nfft;
+      s1 += bsp[j - 1] * cos(arg);
+      s2 += bsp[j - 1] * sin(arg);
+    }
+    mod[k - 1] = s1 * s1 + s2 * s2;
+  }
+  for (int k = 1; k <= nfft; k++)
+    if (mod[k - 1] < 1.0e-7) {
+      const double lo = (k >= 2) ? mod[k - 2] : mod[nfft - 1];
+      const double hi = (k <= nfft - 1) ? mod[k] : mod[0];
+      mod[k - 1] = 0.5 * (lo + hi);
+    }
+  out.resize(nfft);
+  for (int k = 0; k < nfft; k++) out[k] = (float)mod[k];
+}
+
+int upload_tw(orac_gpu_ctx* ctx, float2** dst, int n) {
+  std::vector<float2> tw(n);
+  const double pi = 4.0 * atan(1.0);
+  for (int k = 0; k < n; k++) tw[k] = make_float2((float)cos(-2.0 * pi * k / n), (float)sin(-2.0 * pi * k / n));
+  if (dev_alloc(ctx, dst, n)) return ORAC_ERR_CUDA;
+  CK(cudaMemcpy(*dst, tw.data(), sizeof(float2) * n, cudaMemcpyHostToDevice));
+  return ORAC_OK;
+}
+
+int lines_per_block(int n) {
+  int B = 3072 / n;  // 2 buffers * B * n * 8 bytes <= 48 KB
+  if (B > 16) B = 16;
+  if (B < 1) B = 1;
+  return B;
+}
+
+}  // namespace
+
+int pme_setup(orac_gpu_ctx* ctx, int n1, int n2, int n3, int order) {
+  PmePlan& P = ctx->pme;
+  if (order > MAXORD) return ctx_fail(ctx, ORAC_ERR_PARAM, "PME order %d > %d", order, MAXORD);
+  FftPlan f;
+  if (make_plan(n1, &f) || make_plan(n2, &f) || make_plan(n3, &f))
+    return ctx_fail(ctx, ORAC_ERR_PARAM, "PME grid %dx%dx%d: sizes must factor into 2, 3, 5, 7", n1, n2, n3);
+  if (P.n1 == n1 && P.n2 == n2 && P.n3 == n3 && P.order == order && P.qfix) return ORAC_OK;
+  P.n1 = n1;
+  P.n2 = n2;
+  P.n3 = n3;
+  P.order = order;
+  P.h1 = n1 / 2 + 1;
+  if (upload_tw(ctx, &P.tw1, n1) || upload_tw(ctx, &P.tw2, n2) || upload_tw(ctx, &P.tw3, n3)) return ORAC_ERR_CUDA;
+  std::vector<float> b1, b2, b3;
+  host_bsp_moduli(n1, order, b1);
+  host_bsp_moduli(n2, order, b2);
+  host_bsp_moduli(n3, order, b3);
+  if (dev_alloc(ctx, &P.bsp1, n1) || dev_alloc(ctx, &P.bsp2, n2) || dev_alloc(ctx, &P.bsp3, n3)) return ORAC_ERR_CUDA;
+  CK(cudaMemcpy(P.bsp1, b1.data(), sizeof(float) * n1, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(P.bsp2, b2.data(), sizeof(float) * n2, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(P.bsp3, b3.data(), sizeof(float) * n3, cudaMemcpyHostToDevice));
+  const size_t ng = (size_t)n1 * n2 * n3;
+  if (dev_alloc(ctx, &P.qfix, ng) || dev_alloc(ctx, &P.rgrid, ng) || dev_alloc(ctx, &P.cgrid, (size_t)P.h1 * n2 * n3))
+    return ORAC_ERR_CUDA;
+  return ORAC_OK;
+}
+
+int pme_run(orac_gpu_ctx* ctx, int natom, const double* d_cart, const double* d_q, const double* recip,
+            double volume, double alpha, double* d_f, double* d_eout, const double* d_sxyz, const double* d_mol) {
+  PmePlan& P = ctx->pme;
+  if (!P.qfix) return ctx_fail(ctx, ORAC_ERR_STATE, "PME not set up");
+  const int n1 = P.n1, n2 = P.n2, n3 = P.n3, h1 = P.h1;
+  CK(cudaMemsetAsync(P.qfix, 0, sizeof(unsigned long long) * (size_t)n1 * n2 * n3, ctx->stream));
+  CK(cudaMemsetAsync(d_eout, 0, sizeof(double) * 16, ctx->stream));
+  AtomArgs A;
+  memset(&A, 0, sizeof(A));
+  A.natom = natom;
+  A.order = P.order;
+  A.n1 = n1;
+  A.n2 = n2;
+  A.n3 = n3;
+  A.xyz = d_cart;
+  A.q = d_q;
+  A.r11 = recip[0];
+  A.r21 = recip[1];
+  A.r31 = recip[2];
+  A.r12 = recip[3];
+  A.r22 = recip[4];
+  A.r32 = recip[5];
+  A.r13 = recip[6];
+  A.r23 = recip[7];
+  A.r33 = recip[8];
+  A.qfix = P.qfix;
+  A.rg = P.rgrid;
+  A.f = d_f;
+  A.sxyz = d_sxyz;
+  A.mol = d_mol;
+  A.amol = ctx->d_amol;
+  A.P = ctx->P;
+  A.c11 = ctx->co[0];
+  A.c12 = ctx->co[3];
+  A.c13 = ctx->co[6];
+  A.c22 = ctx->co[4];
+  A.c23 = ctx->co[7];
+  A.c33 = ctx->co[8];
+  A.eout = d_eout;
+  const int nsp = natom * P.order;
+  k_spread<<<(nsp + 255) / 256, 256, 0, ctx->stream>>>(A);
+  CKL();
+  GridArgs G;
+  memset(&G, 0, sizeof(G));
+  G.n1 = n1;
+  G.n2 = n2;
+  G.n3 = n3;
+  G.h1 = h1;
+  G.qfix = P.qfix;
+  G.cg = P.cgrid;
+  G.rg = P.rgrid;
+  G.bsp1 = P.bsp1;
+  G.bsp2 = P.bsp2;
+  G.bsp3 = P.bsp3;
+  G.r11 = recip[0];
+  G.r21 = recip[1];
+  G.r31 = recip[2];
+  G.r12 = recip[3];
+  G.r22 = recip[4];
+  G.r32 = recip[5];
+  G.r13 = recip[6];
+  G.r23 = recip[7];
+  G.r33 = recip[8];
+  const double pif = (double)3.14159265358979323846f;  // scalar_sum's single-precision pi
+  G.fac = (float)(pif * pif / (alpha * alpha));
+  G.pivol = (float)(pif * volume);
+  G.rkcut2 = 0.25 * ctx->rkcut * ctx->rkcut / (pif * pif);
+  G.eout = d_eout;
+  // x forward (r2c)
+  make_plan(n1, &G.P);
+  G.tw = P.tw1;
+  G.B = lines_per_block(n1);
+  int nb = (n2 * n3 + G.B - 1) / G.B;
+  size_t sm = 2 * (size_t)G.B * n1 * sizeof(float2);
+  k_fft<XF><<<nb, 256, sm, ctx->stream>>>(G);
+  CKL();
+  // y forward
+  make_plan(n2, &G.P);
+  G.tw = P.tw2;
+  G.B = lines_per_block(n2);
+  nb = n3 * ((h1 + G.B - 1) / G.B);
+  sm = 2 * (size_t)G.B * n2 * sizeof(float2);
+  k_fft<YF><<<nb, 256, sm, ctx->stream>>>(G);
+  CKL();
+  // z forward + influence function + z inverse
+  make_plan(n3, &G.P);
+  G.tw = P.tw3;
+  G.B = lines_per_block(n3);
+  nb = n2 * ((h1 + G.B - 1) / G.B);
+  sm = 2 * (size_t)G.B * n3 * sizeof(float2);
+  k_fft<ZC><<<nb, 256, sm, ctx->stream>>>(G);
+  CKL();
+  // y inverse
+  make_plan(n2, &G.P);
+  G.tw = P.tw2;
+  G.B = lines_per_block(n2);
+  nb = n3 * ((h1 + G.B - 1) / G.B);
+  sm = 2 * (size_t)G.B * n2 * sizeof(float2);
+  k_fft<YI><<<nb, 256, sm, ctx->stream>>>(G);
+  CKL();
+  // x inverse (c2r)
+  make_plan(n1, &G.P);
+  G.tw = P.tw1;
+  G.B = lines_per_block(n1);
+  nb = (n2 * n3 + G.B - 1) / G.B;
+  sm = 2 * (size_t)G.B * n1 * sizeof(float2);
+  k_fft<XI><<<nb, 256, sm, ctx->stream>>>(G);
+  CKL();
+  k_gather<<<(natom + 255) / 256, 256, 0, ctx->stream>>>(A);
+  CKL();
+  return ORAC_OK;
+}

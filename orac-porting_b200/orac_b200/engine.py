@@ -1,0 +1,211 @@
+"""Host-side mirror of ORAC's nonbonded force-path interface over
+liborac_gpu.so.
+
+`Engine` owns one GPU context for one System and exposes the reference's
+routine names with their argument meaning: mts_forces (per r-RESPA shell),
+lc_list, fft_pme, do_pmesh_kspace, fnb14, fnbgrp, ferrf, cself.  update_lists
+and refresh_m_list replay the driver's list-update sequence of
+src/mtsmd.f:2403-2470 and :3287-3295, including its temporary swaps of the
+shell radii (done here through orac_gpu_set_shells).  Every call goes through
+the C ABI with host arrays, exactly as a Fortran caller would.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import dataclasses
+
+import numpy as np
+
+from . import lib as L
+from .lib import check, colmajor, f64, i32
+
+
+class Engine:
+    def __init__(self, s, device=0):
+        self.s = s
+        self.lib = L.load()
+        ctx = C.c_void_p()
+        rc = self.lib.orac_gpu_create(device, C.byref(ctx))
+        if rc != L.ORAC_OK:
+            raise L.OracGpuError(f"orac_gpu_create: {L.ERRORS.get(rc, rc)}")
+        self.ctx = ctx
+        self._upload()
+
+    def close(self):
+        if self.ctx:
+            self.lib.orac_gpu_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ------------------------------------------------------------ setup
+    def _upload(self):
+        s = self.s
+        self._type_cm = i32(np.asarray(s.type_table).T.ravel())
+        check(self.ctx, self.lib.orac_gpu_set_topology(
+            self.ctx, s.ntap, s.ngrp, s.nprot, i32(s.grppt.ravel()), i32(s.atomp), i32(s.atomg), i32(s.ss_index),
+            f64(s.charge), i32(s.nbtype), s.ntype, self._type_cm, f64(s.ecc12), f64(s.ecc6), f64(s.mass),
+            f64(s.pmass), s.massinfty, i32(s.mapnl), len(s.mapnl)), "set_topology")
+        n1, n2, n3 = s.nfft
+        check(self.ctx, self.lib.orac_gpu_set_ewald(self.ctx, 1, s.alphal, s.order, n1, n2, n3, s.rkcut),
+              "set_ewald")
+        self.set_shells(s.shells)
+        if s.ncell is not None:
+            check(self.ctx, self.lib.orac_gpu_set_linked_cell(self.ctx, *s.ncell), "set_linked_cell")
+        else:
+            check(self.ctx, self.lib.orac_gpu_set_linked_cell(self.ctx, 0, 0, 0), "set_linked_cell")
+        self.set_box(s.co)
+        self._coords()
+
+    def set_shells(self, sh):
+        check(self.ctx, self.lib.orac_gpu_set_shells(self.ctx, sh.rcutm, sh.rtolm, sh.rneim, sh.rcutl, sh.rtoll,
+                                                     sh.rneil, sh.rcuth, sh.rtolh, sh.rneih), "set_shells")
+
+    def set_box(self, co):
+        self.s.co = np.asarray(co, dtype=np.float64)
+        check(self.ctx, self.lib.orac_gpu_set_box(self.ctx, colmajor(self.s.co), colmajor(np.linalg.inv(self.s.co))),
+              "set_box")
+
+    def _coords(self):
+        s = self.s
+        self.xp0, self.yp0, self.zp0 = f64(s.xp0), f64(s.yp0), f64(s.zp0)
+        xg, yg, zg = s.group_centres()
+        self.xpg, self.ypg, self.zpg = f64(xg), f64(yg), f64(zg)
+        xm, ym, zm = s.molecule_centres()
+        self.xpcm, self.ypcm, self.zpcm = f64(xm), f64(ym), f64(zm)
+
+    def set_coords(self, xp0, yp0, zp0):
+        self.s.xp0, self.s.yp0, self.s.zp0 = f64(xp0), f64(yp0), f64(zp0)
+        self._coords()
+
+    # ------------------------------------------------------------ lists
+    def lc_list(self, rcut):
+        n = C.c_int64()
+        check(self.ctx, self.lib.orac_gpu_lc_list(self.ctx, rcut, self.xpg, self.ypg, self.zpg, C.byref(n)),
+              "lc_list")
+        return int(n.value)
+
+    def mts_forces(self, rshell, nstep=0):
+        """One mts_forces call: returns (F (3,N), energies dict, stress (3,3))."""
+        s = self.s
+        fx = np.zeros(s.ntap)
+        fy = np.zeros(s.ntap)
+        fz = np.zeros(s.ntap)
+        st = np.zeros(9)
+        e = [C.c_double() for _ in range(8)]
+        check(self.ctx, self.lib.orac_gpu_mts_forces(
+            self.ctx, nstep, rshell.encode(), self.xp0, self.yp0, self.zp0, self.xpg, self.ypg, self.zpg, self.xpcm,
+            self.ypcm, self.zpcm, *[C.byref(x) for x in e], fx, fy, fz, st), f"mts_forces('{rshell}')")
+        names = ["ucns", "ucos", "virs", "virsp", "ucnp", "ucop", "ucnsp", "ucosp"]
+        en = {k: v.value for k, v in zip(names, e)}
+        return np.stack([fx, fy, fz]), en, st.reshape(3, 3, order="F")
+
+    @staticmethod
+    def ue6(en):
+        """Energies in the oracle's order: LJ slt, slv, mixed; Coulomb slt, slv, mixed."""
+        return np.array([en["ucnp"], en["ucns"], en["ucnsp"], en["ucop"], en["ucos"], en["ucosp"]])
+
+    def update_lists(self):
+        """H list by linked cells (or the 'u' all-pairs update), then the two
+        phony calls deriving the L and M lists (src/mtsmd.f:2403-2470)."""
+        sh = self.s.shells
+        if self.s.ncell is None:
+            self.mts_forces("u")
+        else:
+            self.lc_list(sh.rcuth + sh.rtolh + sh.rneih)
+        sh1 = dataclasses.replace(sh, rcuth=sh.rcutl, rtolh=0.0)
+        self.set_shells(sh1)
+        self.mts_forces("h")
+        sh2 = dataclasses.replace(sh1, rcutl=sh.rcutm, rtoll=0.0)
+        self.set_shells(sh2)
+        self.mts_forces("l")
+        self.set_shells(sh)
+
+    def shell(self, rshell):
+        return self.mts_forces(rshell)
+
+    def refresh_m_list(self):
+        sh = self.s.shells
+        self.set_shells(dataclasses.replace(sh, rcutl=sh.rcutm))
+        self.mts_forces("l")
+        self.set_shells(sh)
+
+    def list_pairs(self):
+        lp = (C.c_int64 * 3)()
+        n = C.c_int64()
+        check(self.ctx, self.lib.orac_gpu_stats(self.ctx, lp, C.byref(n)), "stats")
+        return {"h": lp[0], "l": lp[1], "m": lp[2]}, n.value
+
+    # -------------------------------------------------------------- PME
+    def fft_pme(self, pressure=True):
+        s = self.s
+        fx = np.zeros(s.ntap)
+        fy = np.zeros(s.ntap)
+        fz = np.zeros(s.ntap)
+        st = np.zeros(9)
+        eer = C.c_double()
+        check(self.ctx, self.lib.orac_gpu_fft_pme(self.ctx, self.xp0, self.yp0, self.zp0, self.xpcm, self.ypcm,
+                                                  self.zpcm, C.byref(eer), fx, fy, fz, st, int(pressure)), "fft_pme")
+        return np.stack([fx, fy, fz]), eer.value, st.reshape(3, 3, order="F")
+
+    def do_pmesh_kspace(self, x, y, z, charge, recip, volume, alpha, order, nfft):
+        n = len(x)
+        dx = np.zeros(n)
+        dy = np.zeros(n)
+        dz = np.zeros(n)
+        vir = np.zeros(9)
+        eer = C.c_double()
+        check(self.ctx, self.lib.orac_gpu_do_pmesh_kspace(self.ctx, n, f64(x), f64(y), f64(z), f64(charge),
+                                                          colmajor(recip), volume, alpha, order, nfft[0], nfft[1],
+                                                          nfft[2], C.byref(eer), dx, dy, dz, vir), "do_pmesh_kspace")
+        return np.stack([dx, dy, dz]), eer.value, vir.reshape(3, 3, order="F")
+
+    # ------------------------------------------------------ short lists
+    def _cart(self):
+        r = self.s.cartesian()
+        return f64(r[0]), f64(r[1]), f64(r[2])
+
+    def fnb14(self, cut=True):
+        s = self.s
+        x, y, z = self._cart()
+        fx = np.zeros(s.ntap)
+        fy = np.zeros(s.ntap)
+        fz = np.zeros(s.ntap)
+        ue = np.zeros(4)
+        check(self.ctx, self.lib.orac_gpu_fnb14(self.ctx, x, y, z, int(cut), i32(s.int14.ravel()), len(s.int14),
+                                                i32(s.type14), f64(s.ecc1412), f64(s.ecc146), len(s.ecc1412),
+                                                s.fudge, 1.0, fx, fy, fz, ue), "fnb14")
+        return np.stack([fx, fy, fz]), ue
+
+    def fnbgrp(self):
+        s = self.s
+        x, y, z = self._cart()
+        fx = np.zeros(s.ntap)
+        fy = np.zeros(s.ntap)
+        fz = np.zeros(s.ntap)
+        ue = np.zeros(4)
+        check(self.ctx, self.lib.orac_gpu_fnbgrp(self.ctx, x, y, z, i32(s.ingrp.ravel()), len(s.ingrp), fx, fy, fz,
+                                                 ue), "fnbgrp")
+        return np.stack([fx, fy, fz]), ue
+
+    def ferrf(self, pairs, fudge, iz=1):
+        s = self.s
+        x, y, z = self._cart()
+        fx = np.zeros(s.ntap)
+        fy = np.zeros(s.ntap)
+        fz = np.zeros(s.ntap)
+        fs = np.zeros(2)
+        p = i32(np.asarray(pairs).reshape(-1, 2).ravel())
+        check(self.ctx, self.lib.orac_gpu_ferrf(self.ctx, fudge, x, y, z, iz, p, len(p) // 2, fs, fx, fy, fz),
+              "ferrf")
+        return np.stack([fx, fy, fz]), fs
+
+    def cself(self):
+        a = C.c_double()
+        b = C.c_double()
+        check(self.ctx, self.lib.orac_gpu_cself(self.ctx, self.s.rkcut, C.byref(a), C.byref(b)), "cself")
+        return a.value, b.value

@@ -362,14 +362,15 @@ def config1_liquid():
 # ------------------------------------------------------------------ polymer
 
 
-def _grow_chain(n, rng, bond=1.53, angle=112.0, box=None, center=None, clash=2.4, others=None, max_tries=200):
+def _grow_chain(n, rng, bond=1.53, angle=112.0, box=None, center=None, clash=2.2, others=None, max_tries=100):
     """Self-avoiding chain growth with fixed bond length and angle and random
-    torsions."""
+    torsions; a step that finds no free position backtracks a few atoms."""
     th = math.radians(angle)
     pos = [np.zeros(3) if center is None else np.array(center, dtype=float)]
     d0 = rng.standard_normal(3)
     d0 /= np.linalg.norm(d0)
     pos.append(pos[0] + bond * d0)
+    stuck = 0
     while len(pos) < n:
         ok = False
         for _ in range(max_tries):
@@ -395,7 +396,11 @@ def _grow_chain(n, rng, bond=1.53, angle=112.0, box=None, center=None, clash=2.4
             ok = True
             break
         if not ok:
-            raise RuntimeError("chain growth failed")
+            stuck += 1
+            if stuck > 1000 or len(pos) < 8:
+                raise RuntimeError("chain growth failed")
+            del pos[-5:]
+            continue
         pos.append(p)
     return np.array(pos)
 
@@ -404,7 +409,7 @@ NTYPE_CHAIN = 64
 
 
 def polymer_in_water(nchain=1700, nwat=7000, box=62.0, seed_chain=5, seed_lj=6, seed_wat=7, nfft=(64, 64, 64),
-                     order=5, alphal=0.35, name="config2_polymer22700"):
+                     order=5, alphal=0.35, name="config2_polymer22700", group_size=3, ncell=None):
     """Bonded polymer chain in water (22,700 atoms in the default sizes).
 
     Chain: bond 1.53 A, angle 112 deg, random torsions, seeded self-avoiding
@@ -420,7 +425,7 @@ def polymer_in_water(nchain=1700, nwat=7000, box=62.0, seed_chain=5, seed_lj=6, 
     # wrap the chain as a whole molecule: keep it unwrapped (one molecule)
     rl = np.random.default_rng(seed_lj)
     q = rng.normal(0.0, 0.35, nchain)
-    cgroups = [(a, min(a + 2, nchain - 1)) for a in range(0, nchain, 3)]
+    cgroups = [(a, min(a + group_size - 1, nchain - 1)) for a in range(0, nchain, group_size)]
     for a, b in cgroups:
         q[a:b + 1] -= q[a:b + 1].mean()
     q -= q.mean()
@@ -491,7 +496,8 @@ def polymer_in_water(nchain=1700, nwat=7000, box=62.0, seed_chain=5, seed_lj=6, 
     solute[:nchain] = True
     co = np.diag([box / 2.0] * 3)
     s = _assemble(name, co, pos, mass, qa, lt, types, groups, molecules, bonds, solute, constraints=cons,
-                  seed_v=4, alphal=alphal, order=order, nfft=tuple(nfft), ncell=(int(box / 3.1),) * 3,
+                  seed_v=4, alphal=alphal, order=order, nfft=tuple(nfft),
+                  ncell=ncell if ncell is not None else (int(box / 3.1),) * 3,
                   fudge=0.8333, lj_fudge=0.5)
     # bonded terms of the chain: harmonic bond 1.53 A, harmonic angle 112 deg,
     # 3-fold cosine torsion
