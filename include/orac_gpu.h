@@ -177,7 +177,9 @@ int orac_gpu_cself(orac_gpu_ctx* ctx, double kcut, double* self_slt,
  * The same computations on device pointers (CUDA global memory, FP64 SoA),
  * for drivers that keep the state in HBM.  Forces are accumulated into the
  * device arrays fdev[0..3*ntap) laid out x|y|z; energies[8] and stress[9]
- * are device pointers that receive the shell's results (set). */
+ * are device pointers that receive the shell's results (set).  energies may
+ * be NULL: the shell then runs forces only and skips the FP64 pair-energy
+ * evaluation (forces are identical either way). */
 int orac_gpu_mts_forces_dev(orac_gpu_ctx* ctx, char rshell,
                             const double* xyz_scaled /* 3*ntap, x|y|z */,
                             const double* grp_scaled /* 3*ngrp */,

@@ -53,12 +53,12 @@ int upload3(orac_gpu_ctx* ctx, double* dst, int n, const double* a, const double
 __global__ void k_shell_out(const double* __restrict__ acc, int forces_on, double* __restrict__ e,
                             double* __restrict__ stress) {
   const int t = threadIdx.x;
-  if (t < 8) {
+  if (e && t < 8) {
     // ORAC argument order: ucns ucos virs virsp ucnp ucop ucnsp ucosp
     const int src[8] = {ACC_CONF + 2, ACC_COUL + 2, -1, -1, ACC_CONF + 0, ACC_COUL + 0, ACC_CONF + 1, ACC_COUL + 1};
     e[t] = (forces_on && src[t] >= 0) ? acc[src[t]] : 0.0;
   }
-  if (t < 9) {
+  if (stress && t < 9) {
     const int i = t / 3, j = t % 3;  // stress(i,j) column-major
     stress[i + 3 * j] = forces_on ? acc[ACC_STR + t] + acc[ACC_VIMG + t] : 0.0;
   }
@@ -104,7 +104,7 @@ int check_ready(orac_gpu_ctx* ctx) {
 
 // Shell evaluation on device-resident coordinates (used by both ABIs).
 int shell_run(orac_gpu_ctx* ctx, char rshell, const double* d_xyz, const double* d_grp, const double* d_mol,
-              double* d_f, double* d_e, double* d_stress) {
+              double* d_f, double* d_e, double* d_stress, int energy) {
   ShellSel s;
   if (int rc = select_shell(ctx, rshell, &s)) return rc;
   if (rshell == 'u') {
@@ -113,8 +113,8 @@ int shell_run(orac_gpu_ctx* ctx, char rshell, const double* d_xyz, const double*
     if (d_grp != ctx->d_grp)
       CK(cudaMemcpyAsync(ctx->d_grp, d_grp, sizeof(double) * 3 * ctx->G, cudaMemcpyDeviceToDevice, ctx->stream));
     if (int rc = list_build_allpairs(ctx, s.ri + s.rti + s.rni, &ctx->lists[0])) return rc;
-    CK(cudaMemsetAsync(d_e, 0, 8 * sizeof(double), ctx->stream));
-    CK(cudaMemsetAsync(d_stress, 0, 9 * sizeof(double), ctx->stream));
+    if (d_e) CK(cudaMemsetAsync(d_e, 0, 8 * sizeof(double), ctx->stream));
+    if (d_stress) CK(cudaMemsetAsync(d_stress, 0, 9 * sizeof(double), ctx->stream));
     return ORAC_OK;
   }
   GList& Lin = ctx->lists[s.in];
@@ -155,6 +155,10 @@ int shell_run(orac_gpu_ctx* ctx, char rshell, const double* d_xyz, const double*
   a.arsinn1 = rinn0 - 3.0 * rinn;
   a.arsinn2 = rtolinn * rtolinn * rtolinn;
   a.alphal = (float)ctx->alphal;
+  a.alphad = ctx->alphal;
+  a.energy = energy ? 1 : 0;
+  a.ljd = ctx->d_ljd;
+  a.qd = ctx->d_aqd;
   a.twrtpi = (float)(2.0 / std::sqrt(4.0 * std::atan(1.0)));
   a.forces_on = (s.iz == 1 && rinn0 < rout) ? 1 : 0;  // src/force.f:288,848
   a.next_on = (a.r2inn > 1.0e-5 && s.out >= 0) ? 1 : 0;  // src/force.f:279,337
@@ -218,7 +222,7 @@ int orac_gpu_destroy(orac_gpu_ctx* ctx) {
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   void* ptrs[] = {ctx->d_gmeta, ctx->d_atype, ctx->d_apm, ctx->d_aq, ctx->d_aqd, ctx->d_amol, ctx->d_agrp,
-                  ctx->d_gmol, ctx->d_amassinf, ctx->d_lj, ctx->d_exoff, ctx->d_exj, ctx->d_xyz, ctx->d_grp,
+                  ctx->d_gmol, ctx->d_amassinf, ctx->d_lj, ctx->d_ljd, ctx->d_exoff, ctx->d_exj, ctx->d_xyz, ctx->d_grp,
                   ctx->d_mol, ctx->d_gpos, ctx->d_aoff, ctx->d_ffix, ctx->d_acc, ctx->d_fout, ctx->d_red,
                   ctx->d_scan_tmp, ctx->d_total, ctx->d_flag, ctx->d_cell_of, ctx->d_cell_cnt, ctx->d_cell_start,
                   ctx->d_cell_grp, ctx->d_stencil, ctx->pme.tw1, ctx->pme.tw2, ctx->pme.tw3, ctx->pme.bsp1,
@@ -289,12 +293,17 @@ int orac_gpu_set_topology(orac_gpu_ctx* ctx, int ntap, int ngrp, int nprot, cons
   // LJ table (type(ma,ma) -> ecc index), flagged off when ecc6 <= 1e-12
   const int npair = ntype * (ntype + 1) / 2;
   std::vector<float2> lj((size_t)ntype * ntype);
+  std::vector<double2> ljd((size_t)ntype * ntype);
   for (int t1 = 0; t1 < ntype; t1++)
     for (int t2 = 0; t2 < ntype; t2++) {
       const int lij = type_table[t1 + (size_t)ntype * t2];
       if (lij < 1 || lij > npair) return ctx_fail(ctx, ORAC_ERR_PARAM, "type(%d,%d) = %d", t1 + 1, t2 + 1, lij);
       const double c12 = ecc12[lij - 1], c6 = ecc6[lij - 1];
-      lj[t1 * (size_t)ntype + t2] = (c6 > 1e-12) ? make_float2((float)c12, (float)c6) : make_float2(0.f, 0.f);
+      const bool on = c6 > 1e-12;  // src/force.f:416,431
+      lj[t1 * (size_t)ntype + t2] = on ? make_float2((float)c12, (float)c6) : make_float2(0.f, 0.f);
+      ljd[t1 * (size_t)ntype + t2] = on ? make_double2(c12, c6) : make_double2(0.0, 0.0);
+      if (on && (float)c6 == 0.f)
+        return ctx_fail(ctx, ORAC_ERR_PARAM, "ecc6(%d) = %g underflows single precision", lij, c6);
     }
   // exclusions: serial mapnl -> CSR with 0-based partners
   std::vector<int> exoff(N + 1), exj;
@@ -348,6 +357,7 @@ int orac_gpu_set_topology(orac_gpu_ctx* ctx, int ntap, int ngrp, int nprot, cons
   UP(ctx->d_aq, aq);
   UP(ctx->d_amassinf, minf);
   UP(ctx->d_lj, lj);
+  UP(ctx->d_ljd, ljd);
   UP(ctx->d_exoff, exoff);
   if (exj.empty()) exj.push_back(0);
   UP(ctx->d_exj, exj);
@@ -449,7 +459,8 @@ int orac_gpu_mts_forces(orac_gpu_ctx* ctx, int nstep, char rshell, const double*
   if (int rc = upload3(ctx, ctx->d_mol, ctx->P, xpcm, ypcm, zpcm)) return rc;
   CK(cudaMemsetAsync(ctx->d_fout, 0, sizeof(double) * 3 * (size_t)N, ctx->stream));
   double* d_out = ctx->d_red;  // [8] energies + [9] stress
-  if (int rc = shell_run(ctx, rshell, ctx->d_xyz, ctx->d_grp, ctx->d_mol, ctx->d_fout, d_out, d_out + 8)) return rc;
+  if (int rc = shell_run(ctx, rshell, ctx->d_xyz, ctx->d_grp, ctx->d_mol, ctx->d_fout, d_out, d_out + 8, 1))
+    return rc;
   if (int rc = ensure_stage(ctx, sizeof(double) * (3 * (size_t)N + 17))) return rc;
   CK(cudaMemcpyAsync(ctx->h_stage, ctx->d_fout, sizeof(double) * 3 * (size_t)N, cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaMemcpyAsync(ctx->h_stage + 3 * (size_t)N, d_out, sizeof(double) * 17, cudaMemcpyDeviceToHost, ctx->stream));
@@ -477,7 +488,7 @@ int orac_gpu_mts_forces_dev(orac_gpu_ctx* ctx, char rshell, const double* xyz_sc
                             const double* mol_scaled, double* fdev, double* energies, double* stress) {
   if (int rc = check_ready(ctx)) return rc;
   CK(cudaSetDevice(ctx->device));
-  return shell_run(ctx, rshell, xyz_scaled, grp_scaled, mol_scaled, fdev, energies, stress);
+  return shell_run(ctx, rshell, xyz_scaled, grp_scaled, mol_scaled, fdev, energies, stress, energies != nullptr);
 }
 
 int orac_gpu_sync(orac_gpu_ctx* ctx) {

@@ -66,7 +66,12 @@ struct PairArgs {
   double r2inn, r2inn0, r2out, r2out0, rinn0, rout0, r2neigh;
   double arsout1, arsout2, arsinn1, arsinn2;
   float alphal, twrtpi;
+  double alphad;
   int forces_on, next_on, lskip, ewald;
+  // energies: 0 = forces only, 1 = also FP64 pair energies
+  int energy;
+  const double2* ljd;  // [ntype*ntype] FP64 (ecc12, ecc6), 0 when ecc6 <= 1e-12
+  const double* qd;    // [N] FP64 charges
   // lists
   const int* off;
   const int* cnt;
@@ -144,6 +149,7 @@ struct orac_gpu_ctx {
   int* d_gmol = nullptr;
   unsigned char* d_amassinf = nullptr;
   float2* d_lj = nullptr;
+  double2* d_ljd = nullptr;
   int* d_exoff = nullptr;  // [N+1]
   int* d_exj = nullptr;    // 0-based partners j > i
 
@@ -251,4 +257,4 @@ int self_launch(orac_gpu_ctx* ctx, const int* d_ss, double* d_e);
 // api.cu
 int shell_run(orac_gpu_ctx* ctx, char rshell, const double* d_xyz,
               const double* d_grp, const double* d_mol, double* d_f,
-              double* d_e, double* d_stress);
+              double* d_e, double* d_stress, int energy);

@@ -48,13 +48,39 @@ __device__ __forceinline__ double warp_sumd(double v) {
   return v;
 }
 
-template <int MG>
+// Pair energies in FP64 from the FP64 centre distance, the stored atom
+// offsets, FP64 charges and FP64 LJ parameters: used only when energies are
+// requested (EN), so the FP32 force path is the same in both modes.
+__device__ __forceinline__ void pair_energy_fp64(const PairArgs& A, double rx, double ry, double rz, double2 L,
+                                                 bool ljon, double qq, double* conf, double* coul) {
+  const double r2 = rx * rx + ry * ry + rz * rz;
+  const double rsqi = 1.0 / r2;
+  *conf = 0.0;
+  *coul = 0.0;
+  if (ljon) {
+    const double r6 = rsqi * rsqi * rsqi;
+    *conf = L.x * r6 * r6 - L.y * r6;
+  }
+  if (!A.lskip) {
+    const double rsp = sqrt(r2);
+    const double ar = A.alphad * rsp;
+    const double qt = 1.0 / (1.0 + 0.3275911 * ar);
+    const double erfcst =
+        ((((1.0614054 * qt - 1.453152) * qt + 1.4214137) * qt - 0.28449674) * qt + 0.2548296) * qt * exp(-ar * ar);
+    *coul = qq * erfcst / rsp;
+  } else if (!A.ewald) {
+    *coul = qq / sqrt(r2);
+  }
+}
+
+template <int MG, bool EN>
 __global__ void __launch_bounds__(WPB * 32)
     k_pair(const PairArgs A) {
   extern __shared__ float2 s_lj[];
   __shared__ float4 s_ai[WPB][MG];
   __shared__ int s_ti[WPB][MG];
   __shared__ float s_pm[WPB][MG];
+  __shared__ double s_qd[WPB][MG];
   __shared__ double s_red[WPB][ACC_N];
 
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -77,6 +103,7 @@ __global__ void __launch_bounds__(WPB * 32)
       s_ai[warp][lane] = A.aoff[ifirst + lane];
       s_ti[warp][lane] = A.atype[ifirst + lane];
       s_pm[warp][lane] = A.apm[ifirst + lane];
+      if (EN) s_qd[warp][lane] = A.qd[ifirst + lane];
     }
     __syncwarp();
     float fi[MG][3];
@@ -120,20 +147,23 @@ __global__ void __launch_bounds__(WPB * 32)
       if (!A.forces_on || !valid) continue;
       bool switched;
       float sw = 1.f, dsw = 0.f;
+      double swd = 1.0;
       if (drj >= A.r2inn0 && drj < A.r2out) {
         switched = false;
       } else if (drj >= A.r2out && drj < A.r2out0) {
         const double rsp = sqrt(drj);
         const double auxa = (A.arsout1 + 2.0 * rsp) / A.arsout2;
         const double auxb = A.rout0 - rsp;
-        sw = (float)(auxa * auxb * auxb);
+        swd = auxa * auxb * auxb;
+        sw = (float)swd;
         dsw = (float)((-2.0 * auxa * auxb + 2.0 * auxb * auxb / A.arsout2) / rsp);
         switched = true;
       } else if (drj >= A.r2inn && drj < A.r2inn0) {
         const double rsp = sqrt(drj);
         const double auxa = (A.arsinn1 + 2.0 * rsp) / A.arsinn2;
         const double auxb = A.rinn0 - rsp;
-        sw = (float)(1.0 - auxa * auxb * auxb);
+        swd = 1.0 - auxa * auxb * auxb;
+        sw = (float)swd;
         dsw = (float)((2.0 * auxa * auxb - 2.0 * auxb * auxb / A.arsinn2) / rsp);
         switched = true;
       } else {
@@ -142,11 +172,13 @@ __global__ void __launch_bounds__(WPB * 32)
       const int2 mj = A.gmeta[j];
       const int jfirst = mj.x, nj = mj.y & 0xff, typej = mj.y >> 8;
       const float dcx = (float)cx, dcy = (float)cy, dcz = (float)cz;
-      float pconf = 0.f, pcoul = 0.f, vsum = 0.f;
+      double pconf = 0.0, pcoul = 0.0;
+      float vsum = 0.f;
       float gx = 0.f, gy = 0.f, gz = 0.f;  // total force on the j group
       for (int b = 0; b < nj; b++) {
         const float4 ob = A.aoff[jfirst + b];
         const int tb = A.atype[jfirst + b];
+        const double qbd = EN ? A.qd[jfirst + b] : 0.0;
         float fbx = 0.f, fby = 0.f, fbz = 0.f;
 #pragma unroll
         for (int a = 0; a < MG; a++) {
@@ -188,8 +220,14 @@ __global__ void __launch_bounds__(WPB * 32)
             vsum += conf + coul;
             qf *= sw;
           }
-          pconf += conf;
-          pcoul += coul;
+          if (EN) {
+            double cd, qd;
+            pair_energy_fp64(A, cx + ((double)ai.x - (double)ob.x), cy + ((double)ai.y - (double)ob.y),
+                             cz + ((double)ai.z - (double)ob.z), A.ljd[s_ti[warp][a] * A.ntype + tb], ljon,
+                             s_qd[warp][a] * qbd, &cd, &qd);
+            pconf += cd;
+            pcoul += qd;
+          }
           const float fx = qf * rx, fy = qf * ry, fz = qf * rz;
           fi[a][0] += fx;
           fi[a][1] += fy;
@@ -206,8 +244,8 @@ __global__ void __launch_bounds__(WPB * 32)
         fix_add(A.ffix + 2 * A.natom + jfirst + b, fbz);
       }
       if (switched) {
-        pconf *= sw;
-        pcoul *= sw;
+        pconf *= swd;
+        pcoul *= swd;
         // S'(R) V term: X = -dS/dR / R * V * R_vec on i atoms by mass fraction
         const float sx = -dsw * vsum * dcx, sy = -dsw * vsum * dcy,
                     sz = -dsw * vsum * dcz;
@@ -367,9 +405,15 @@ int pair_launch(orac_gpu_ctx* ctx, const PairArgs& a, int maxg) {
   if (nb < 1) nb = 1;
   const size_t smem = (size_t)(a.ntype * a.ntype <= LJ_SMEM_MAX ? a.ntype * a.ntype : 0) * sizeof(float2);
   if (maxg <= 4) {
-    k_pair<4><<<nb, WPB * 32, smem, ctx->stream>>>(a);
+    if (a.energy)
+      k_pair<4, true><<<nb, WPB * 32, smem, ctx->stream>>>(a);
+    else
+      k_pair<4, false><<<nb, WPB * 32, smem, ctx->stream>>>(a);
   } else if (maxg <= 8) {
-    k_pair<8><<<nb, WPB * 32, smem, ctx->stream>>>(a);
+    if (a.energy)
+      k_pair<8, true><<<nb, WPB * 32, smem, ctx->stream>>>(a);
+    else
+      k_pair<8, false><<<nb, WPB * 32, smem, ctx->stream>>>(a);
   } else {
     return ctx_fail(ctx, ORAC_ERR_PARAM, "charge group of %d atoms exceeds %d", maxg, ORAC_MAXG);
   }
