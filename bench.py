@@ -1,0 +1,351 @@
+#!/usr/bin/env python
+"""MD throughput (ns/day) of the B200 r-RESPA nonbonded force path.
+
+One step = one outer r-RESPA step (H = 4 fs: 1 H shell, 2 L shells + SPME,
+8 M shells, drift + SHAKE/RATTLE) of the 3,000-water 31 A box (9,000 atoms,
+alpha 0.35, SPME 32^3 order 4, shells 5.0/7.5/10.0 A, list update every
+6 steps), run by the device-resident driver of liborac_gpu.so with the
+state resident in HBM.  Prints one JSON line.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+--impl reference times the CPU restatement of ORAC's loop (the oracle, FP64,
+OpenMP over all host cores) on the same workload.  Under torchrun each rank
+runs an independent replica (the path does not shard within one system).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for p in (os.path.join(ROOT, "orac-porting_b200"), os.path.join(ROOT, "oracle")):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+import numpy as np  # noqa: E402
+
+from orac_b200 import systems  # noqa: E402
+
+FS_PER_DAY = 86400.0e15  # fs per day of wall time per 1 fs/s
+FP32_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # 74.4: no measured FP32 peak on this pool
+METRIC = "MD ns/day and p50/p99 segment latency, batched vs plain, at force err<=1e-5"
+
+WORKLOADS = {
+    "config1": dict(build=systems.config1_water, dt_h=4.0, lrespa=2, mrespa=4, nupdte=6, rshk="l",
+                    desc="3,000 rigid 3-site waters (9,000 atoms), 31.0 A cubic box, alpha 0.35, SPME 32^3 "
+                         "order 4, r-RESPA 0.5/2/4 fs with shells 5.0/7.5/10.0 A, list update every 6 H steps"),
+    "liquid": dict(build=systems.config1_liquid, dt_h=4.0, lrespa=2, mrespa=4, nupdte=6, rshk="l",
+                   desc="the same 3,000 waters at liquid density (44.7 A box, SPME 48^3)"),
+}
+
+
+def ns_per_day(steps, dt_h_fs, seconds):
+    return steps * dt_h_fs * 1e-6 * 86400.0 / seconds
+
+
+def dist_info():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def econst_of(s, engine=None):
+    """Self energy (cself) + the constant erf correction of rigid bonds
+    (ferrf with iz = 0, src/mtsmd.f:1641-1645)."""
+    if engine is not None:
+        a, b = engine.cself()
+        _, fs = engine.ferrf(s.constraints, 1.0, iz=0)
+    else:
+        import oracle
+
+        o = oracle.Oracle(s)
+        a, b = o.cself()
+        _, fs = o.ferrf(s.constraints, 1.0, iz=0)
+    return a + b + float(fs.sum())
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                       "-i", str(index), "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[0]))
+                mx.append(float(r[1]))
+                for k, nm in enumerate(names):
+                    if r[4 + k].strip().lower() == "active":
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                continue
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        return {}
+
+
+def ncu_traffic():
+    """DRAM bytes per launch of the real-space kernel from the committed ncu
+    summary (profiles/k_pair_config1.json), or None."""
+    try:
+        d = json.load(open(os.path.join(ROOT, "profiles", "k_pair_config1.json")))
+        return float(d["dram_bytes_per_launch"])
+    except Exception:
+        return None
+
+
+# ----------------------------------------------------------------------- CPU
+
+
+def cpu_run(wl, s, steps, warmup, budget_s=None):
+    """Oracle r-RESPA loop on all host cores; returns (seconds, steps, cores)."""
+    import oracle
+
+    cores = os.cpu_count() or 1
+    md = oracle.OracleMD(s, wl["dt_h"], wl["lrespa"], wl["mrespa"], wl["nupdte"], wl["rshk"], nthreads=cores,
+                         econst=0.0)
+    if warmup:
+        md.run(warmup)
+    done, t = 0, 0.0
+    while done < steps:
+        t0 = time.perf_counter()
+        md.run(1)
+        t += time.perf_counter() - t0
+        done += 1
+        if budget_s is not None and t >= budget_s and done >= 3:
+            break
+    md.close()
+    return t, done, cores
+
+
+# ----------------------------------------------------------------------- GPU
+
+
+def gpu_arm(args, wl, s, device):
+    import ctypes as C
+
+    import torch
+
+    from orac_b200.engine import Engine
+
+    torch.cuda.set_device(device)
+    eng = Engine(s.copy(), device=device)
+    L = eng.lib
+    ec = econst_of(s, eng)
+    eng.md_setup(wl["dt_h"], wl["lrespa"], wl["mrespa"], wl["nupdte"], wl["rshk"], econst=ec)
+    L.orac_gpu_prof_enable(eng.ctx, 1)
+    stream = torch.cuda.ExternalStream(L.orac_gpu_get_stream(eng.ctx), device=device)
+    # warm-up (also captures the step graphs)
+    for _ in range(args.warmup):
+        assert L.orac_gpu_md_run_async(eng.ctx, 1) == 0
+        assert L.orac_gpu_md_collect(eng.ctx) == 0
+    cnt = (C.c_int64 * 4)()
+    L.orac_gpu_counters(eng.ctx, cnt, 1)
+    L.orac_gpu_prof_read(eng.ctx, None, None, 1)
+    l0 = C.c_int64()
+    L.orac_gpu_stats(eng.ctx, None, C.byref(l0))
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{device}")  # > 126 MB L2
+    ws, rank, local = dist_info()
+    if ws > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(device) if rank == 0 else None
+    total_ms = 0.0
+    step_ms = []
+    for _ in range(args.steps):
+        flush.zero_()  # L2 flushed between timed steps
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        rc = L.orac_gpu_md_run_async(eng.ctx, 1)
+        e1.record(stream)
+        rc |= L.orac_gpu_md_collect(eng.ctx)
+        if rc:
+            raise RuntimeError(L.orac_gpu_last_error(eng.ctx).decode())
+        ms = e0.elapsed_time(e1)
+        step_ms.append(ms)
+        total_ms += ms
+    torch.cuda.synchronize()
+    if ws > 1:
+        import torch.distributed as dist
+
+        t = torch.tensor([total_ms], device=f"cuda:{device}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    clk = clocks.stop() if clocks else None
+    l1 = C.c_int64()
+    L.orac_gpu_stats(eng.ctx, None, C.byref(l1))
+    L.orac_gpu_counters(eng.ctx, cnt, 0)
+    pms = C.c_double()
+    pn = C.c_int64()
+    L.orac_gpu_prof_read(eng.ctx, C.byref(pms), C.byref(pn), 0)
+    res = dict(total_ms=total_ms, step_ms=step_ms, launches=int(l1.value - l0.value), scanned=cnt[0], kept=cnt[1],
+               pairs_ewald=cnt[2], pairs_lj=cnt[3], kpair_ms=pms.value, kpair_n=int(pn.value), clocks=clk)
+    # end-to-end through the public ABI with host buffers: every step copies
+    # the state in from pinned host memory and reads it back
+    n = s.ntap
+    host = [torch.empty(n, dtype=torch.float64).pin_memory() for _ in range(6)]
+    x, v = eng.md_state()
+    for k in range(3):
+        host[k].copy_(torch.from_numpy(x[k]))
+        host[3 + k].copy_(torch.from_numpy(v[k]))
+    ptrs = [h.data_ptr() for h in host]
+    views = [h.numpy() for h in host]
+    e2e_steps = max(3, min(args.steps, 20))
+    t_e2e = 0.0
+    for _ in range(e2e_steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        rc = L.orac_gpu_md_set_state(eng.ctx, *ptrs)
+        rc |= L.orac_gpu_md_run_async(eng.ctx, 1)
+        rc |= L.orac_gpu_md_get_state(eng.ctx, *views)
+        rc |= L.orac_gpu_md_collect(eng.ctx)
+        t_e2e += time.perf_counter() - t0
+        if rc:
+            raise RuntimeError(L.orac_gpu_last_error(eng.ctx).decode())
+    res["e2e_s"] = t_e2e
+    res["e2e_steps"] = e2e_steps
+    res["bytes_io"] = 6 * n * 8
+    res["G"], res["N"] = s.ngrp, s.ntap
+    eng.close()
+    return res
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=60)
+    ap.add_argument("--warmup", type=int, default=6)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="config1")
+    ap.add_argument("--cpu-budget", type=float, default=12.0, help="seconds of CPU-baseline sampling")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    wl = WORKLOADS[args.workload]
+    ws, rank, local = dist_info()
+    s = wl["build"]()
+    config = {"workload": f"{args.workload}: {wl['desc']}", "atoms": s.ntap, "groups": s.ngrp,
+              "step": "one outer r-RESPA step (4 fs)", "l2": "flushed (256 MB write) between timed steps",
+              "parallelism": f"replicas x{ws}" if ws > 1 else "single system, 1 GPU"}
+    base = {"metric": METRIC, "unit": "ns/day", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32+int64fixed+fp64",
+            "data": "synthetic (seeded lattice water, random-orientation, Maxwell-Boltzmann 300 K)",
+            "config": config}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        t, done, cores = cpu_run(wl, s, args.steps, args.warmup)
+        val = ns_per_day(done, wl["dt_h"], t)
+        out = dict(base, impl="reference", value=val, ms_per_step=1e3 * t / done,
+                   cpu_baseline={"value": val, "unit": "ns/day", "cores": cores, "kind": "port",
+                                 "sample": f"{done} H steps of the workload after {args.warmup} warm-up steps "
+                                           "(FP64 C restatement of ORAC's loop, OpenMP)"},
+                   e2e={"value": val, "unit": "ns/day", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0})
+        out["steps"] = done
+        print(json.dumps(out))
+        return 0
+
+    if ws > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    res = gpu_arm(args, wl, s, local)
+    if ws > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    secs = res["total_ms"] / 1e3
+    value = ws * ns_per_day(args.steps, wl["dt_h"], secs)
+    peaks = measured_peaks()
+    # dominant kernel: the real-space shell kernel (all shells)
+    n_l = max(1, res["kpair_n"])
+    kp_s = res["kpair_ms"] / 1e3
+    flops = 60.0 * res["pairs_ewald"] + 36.0 * res["pairs_lj"]
+    bytes_alg = 12.0 * (res["scanned"] + res["kept"]) + n_l * (40.0 * res["G"] + 48.0 * res["N"])
+    hbm_peak = peaks.get("hbm_gbs")
+    achieved_gbs = bytes_alg / kp_s / 1e9 if kp_s > 0 else 0.0
+    roofline = {"kernel": "k_pair (real-space r-RESPA shell kernel, all shells)", "bound": "hbm",
+                "achieved": achieved_gbs, "peak": hbm_peak if hbm_peak else 6650.0, "unit": "GB/s",
+                "frac": achieved_gbs / (hbm_peak if hbm_peak else 6650.0),
+                "peak_source": "measured" if hbm_peak else "fallback",
+                "traffic": ncu_traffic(), "bytes_per_launch": bytes_alg / n_l, "launches": res["kpair_n"],
+                "avg_launch_us": 1e6 * kp_s / n_l,
+                "fp32_view": {"achieved": flops / kp_s / 1e12 if kp_s > 0 else 0.0, "unit": "TFLOP/s",
+                              "peak": FP32_NOMINAL_TFLOPS, "peak_source": "nominal (no measured FP32 peak)",
+                              "frac": (flops / kp_s / 1e12) / FP32_NOMINAL_TFLOPS if kp_s > 0 else 0.0,
+                              "pair_evaluations": res["pairs_ewald"] + res["pairs_lj"],
+                              "flops_per_pair": "60 LJ+Ewald, 36 LJ-only"},
+                "share_of_step": res["kpair_ms"] / res["total_ms"] if res["total_ms"] else None}
+    cpu = None
+    if not args.no_cpu_baseline:
+        t, done, cores = cpu_run(wl, s, 200, 1, budget_s=args.cpu_budget)
+        cpu = {"value": ns_per_day(done, wl["dt_h"], t), "unit": "ns/day", "cores": cores, "kind": "port",
+               "sample": f"{done} H steps of the same workload on {cores} host threads (FP64 C restatement of "
+                         "ORAC's r-RESPA loop, OpenMP), after 1 warm-up step"}
+    e2e_val = ns_per_day(res["e2e_steps"], wl["dt_h"], res["e2e_s"])
+    st = sorted(res["step_ms"])
+    out = dict(base, value=value, ms_per_step=res["total_ms"] / args.steps,
+               step_ms_p50=st[len(st) // 2], step_ms_p99=st[min(len(st) - 1, int(0.99 * len(st)))],
+               roofline=roofline, cpu_baseline=cpu,
+               e2e={"value": e2e_val, "unit": "ns/day", "h2d_bytes_per_step": res["bytes_io"],
+                    "d2h_bytes_per_step": res["bytes_io"],
+                    "how": "orac_gpu_md_set_state (pinned host -> device), one step, orac_gpu_md_get_state "
+                           "(device -> pinned host), wall clock"},
+               gpu_launches=res["launches"], clocks=res["clocks"])
+    print(json.dumps(out))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -190,6 +190,63 @@ int orac_gpu_fft_pme_dev(orac_gpu_ctx* ctx, const double* xyz_scaled,
                          const double* mol_scaled, double* fdev,
                          double* eer_dev, double* stress_dev);
 
+/* r-RESPA molecular dynamics on the device ---------------------------------
+ * The NVE part of ORAC's step loop, mtsmd (src/mtsmd.f:2390-3540), with its
+ * kick correc (src/correc.f), drift verlet (src/verlet.f) and the SHAKE /
+ * RATTLE solvers (src/rattle_verlet.f, src/rattle_correc.f), driving the
+ * shells and SPME above.  x/y/z are Cartesian positions, vx/vy/vz velocities
+ * (A/fs); cnst(2,ncnst) are the rigid bonds with squared lengths dss;
+ * dt_h is the outer (H) time step in fs, lrespa/mrespa/n1respa/n0respa the
+ * substeps of the L, M, N1 and N0 levels, nupdte the list-update period in
+ * H steps, rshk the shell ('m','l','h') that carries the SPME term; econst is
+ * added to the reported total energy (self and constraint corrections). */
+int orac_gpu_md_setup(orac_gpu_ctx* ctx, const double* x, const double* y,
+                      const double* z, const double* vx, const double* vy,
+                      const double* vz, const int* cnst, const double* dss,
+                      int ncnst, double dt_h, int lrespa, int mrespa,
+                      int n1respa, int n0respa, int nupdte, char rshk,
+                      double econst);
+
+/* Advance nsteps H steps (steady-state steps run as one captured CUDA graph
+ * per step kind).  Every energy_every steps one record of 12 doubles goes to
+ * rec: step, kinetic, U_M LJ, U_M Coulomb, U_L LJ, U_L Coulomb, U_H LJ,
+ * U_H Coulomb, E_reciprocal, econst, total, status flag. */
+int orac_gpu_md_run(orac_gpu_ctx* ctx, int nsteps, int energy_every,
+                    double* rec);
+
+/* Queue nsteps steps on the context's stream and return at once (no energy
+ * records, no status check); orac_gpu_md_collect waits, checks the status
+ * (SHAKE convergence, list capacity) and gathers profiling events. */
+int orac_gpu_md_run_async(orac_gpu_ctx* ctx, int nsteps);
+int orac_gpu_md_collect(orac_gpu_ctx* ctx);
+
+int orac_gpu_md_get_state(orac_gpu_ctx* ctx, double* x, double* y, double* z,
+                          double* vx, double* vy, double* vz);
+
+/* Replace positions and velocities (host arrays; pinned memory avoids a
+ * staging copy).  The copies are queued on the context's stream. */
+int orac_gpu_md_set_state(orac_gpu_ctx* ctx, const double* x, const double* y,
+                          const double* z, const double* vx,
+                          const double* vy, const double* vz);
+
+/* 0 = launch every kernel of a step directly, 1 = replay captured graphs. */
+int orac_gpu_md_set_graphs(orac_gpu_ctx* ctx, int on);
+
+/* Measurement (no counterpart in the reference, which times with wall
+ * clocks in src/timer.f) ---------------------------------------------------
+ * The context's cudaStream_t, for callers that record their own events. */
+void* orac_gpu_get_stream(orac_gpu_ctx* ctx);
+/* Work counters of the real-space kernel since the last reset: list entries
+ * scanned, entries kept for the next shell, atom pairs evaluated with Ewald,
+ * atom pairs evaluated LJ-only. */
+int orac_gpu_counters(orac_gpu_ctx* ctx, int64_t* out4, int reset);
+/* With profiling on, every real-space kernel launch is bracketed by CUDA
+ * events (also inside captured graphs); prof_read returns the summed device
+ * time in ms and the number of launches timed. */
+int orac_gpu_prof_enable(orac_gpu_ctx* ctx, int on);
+int orac_gpu_prof_read(orac_gpu_ctx* ctx, double* ms_total, int64_t* nlaunch,
+                       int reset);
+
 /* Synchronise the context's stream. */
 int orac_gpu_sync(orac_gpu_ctx* ctx);
 

@@ -71,8 +71,7 @@ struct ShellSel {
 };
 
 // src/mts_forces.f:57-93
-int select_shell(orac_gpu_ctx* ctx, char rshell, ShellSel* s) {
-  const ShellRadii& r = ctx->sh;
+int select_shell(orac_gpu_ctx* ctx, const ShellRadii& r, char rshell, ShellSel* s) {
   switch (rshell) {
     case 'u':
       *s = {r.rcuth, r.rcuth, 0.0, r.rtolh, r.rneih, 0, -1, 0};
@@ -105,8 +104,13 @@ int check_ready(orac_gpu_ctx* ctx) {
 // Shell evaluation on device-resident coordinates (used by both ABIs).
 int shell_run(orac_gpu_ctx* ctx, char rshell, const double* d_xyz, const double* d_grp, const double* d_mol,
               double* d_f, double* d_e, double* d_stress, int energy) {
+  return shell_run_r(ctx, rshell, ctx->sh, d_xyz, d_grp, d_mol, d_f, d_e, d_stress, energy);
+}
+
+int shell_run_r(orac_gpu_ctx* ctx, char rshell, const ShellRadii& radii, const double* d_xyz, const double* d_grp,
+                const double* d_mol, double* d_f, double* d_e, double* d_stress, int energy) {
   ShellSel s;
-  if (int rc = select_shell(ctx, rshell, &s)) return rc;
+  if (int rc = select_shell(ctx, radii, rshell, &s)) return rc;
   if (rshell == 'u') {
     if (ctx->ncx > 0)
       return ctx_fail(ctx, ORAC_ERR_PARAM, "'u' update is for runs without LINKED_CELL; use orac_gpu_lc_list");
@@ -177,6 +181,7 @@ int shell_run(orac_gpu_ctx* ctx, char rshell, const double* d_xyz, const double*
   a.ffix = ctx->d_ffix;
   a.acc = ctx->d_acc;
   a.natom = ctx->N;
+  a.wcnt = ctx->d_wcnt;
   CK(cudaMemsetAsync(ctx->d_acc, 0, ACC_N * sizeof(double), ctx->stream));
   if (int rc = prep_launch(ctx, d_xyz, d_grp)) return rc;
   if (int rc = pair_launch(ctx, a, ctx->maxg)) return rc;
@@ -209,7 +214,8 @@ int orac_gpu_create(int device, orac_gpu_ctx** out) {
     return ORAC_ERR_CUDA;
   }
   if (dev_alloc(ctx, &ctx->d_acc, ACC_N) || dev_alloc(ctx, &ctx->d_red, 64) || dev_alloc(ctx, &ctx->d_total, 4) ||
-      dev_alloc(ctx, &ctx->d_flag, 4)) {
+      dev_alloc(ctx, &ctx->d_flag, 4) || dev_alloc(ctx, &ctx->d_wcnt, 4) ||
+      cudaMemset(ctx->d_wcnt, 0, 4 * sizeof(unsigned long long)) != cudaSuccess) {
     orac_gpu_destroy(ctx);
     return ORAC_ERR_CUDA;
   }
@@ -221,6 +227,7 @@ int orac_gpu_destroy(orac_gpu_ctx* ctx) {
   if (!ctx) return ORAC_OK;
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  md_destroy(ctx);
   void* ptrs[] = {ctx->d_gmeta, ctx->d_atype, ctx->d_apm, ctx->d_aq, ctx->d_aqd, ctx->d_amol, ctx->d_agrp,
                   ctx->d_gmol, ctx->d_amassinf, ctx->d_lj, ctx->d_ljd, ctx->d_exoff, ctx->d_exj, ctx->d_xyz, ctx->d_grp,
                   ctx->d_mol, ctx->d_gpos, ctx->d_aoff, ctx->d_ffix, ctx->d_acc, ctx->d_fout, ctx->d_red,
@@ -233,6 +240,8 @@ int orac_gpu_destroy(orac_gpu_ctx* ctx) {
                  ctx->api.t6,   ctx->api.ss,   ctx->api.e4,     ctx->api.q};
   for (void* p : aps)
     if (p) cudaFree(p);
+  if (ctx->d_wcnt) cudaFree(ctx->d_wcnt);
+  for (auto& e : ctx->prof_ev) cudaEventDestroy(e);
   for (int q = 0; q < 3; q++) {
     if (q == 0 && ctx->lists[q].off) cudaFree(ctx->lists[q].off);
     if (ctx->lists[q].cnt) cudaFree(ctx->lists[q].cnt);
@@ -494,6 +503,39 @@ int orac_gpu_mts_forces_dev(orac_gpu_ctx* ctx, char rshell, const double* xyz_sc
 int orac_gpu_sync(orac_gpu_ctx* ctx) {
   if (!ctx) return ORAC_ERR_PARAM;
   CK(cudaStreamSynchronize(ctx->stream));
+  return ORAC_OK;
+}
+
+void* orac_gpu_get_stream(orac_gpu_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+int orac_gpu_counters(orac_gpu_ctx* ctx, int64_t* out4, int reset) {
+  if (!ctx) return ORAC_ERR_PARAM;
+  unsigned long long h[4];
+  CK(cudaStreamSynchronize(ctx->stream));
+  CK(cudaMemcpy(h, ctx->d_wcnt, sizeof(h), cudaMemcpyDeviceToHost));
+  for (int k = 0; k < 4; k++) out4[k] = (int64_t)h[k];
+  if (reset) CK(cudaMemset(ctx->d_wcnt, 0, sizeof(h)));
+  return ORAC_OK;
+}
+
+int orac_gpu_prof_enable(orac_gpu_ctx* ctx, int on) {
+  if (!ctx) return ORAC_ERR_PARAM;
+  if (on && ctx->prof_ev.empty()) {
+    ctx->prof_ev.resize(2048);
+    for (auto& e : ctx->prof_ev) CK(cudaEventCreate(&e));
+  }
+  ctx->prof = on != 0;
+  return ORAC_OK;
+}
+
+int orac_gpu_prof_read(orac_gpu_ctx* ctx, double* ms_total, int64_t* nlaunch, int reset) {
+  if (!ctx) return ORAC_ERR_PARAM;
+  if (ms_total) *ms_total = ctx->prof_ms;
+  if (nlaunch) *nlaunch = ctx->prof_n;
+  if (reset) {
+    ctx->prof_ms = 0;
+    ctx->prof_n = 0;
+  }
   return ORAC_OK;
 }
 

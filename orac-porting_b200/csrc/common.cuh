@@ -84,6 +84,9 @@ struct PairArgs {
   unsigned long long* ffix;  // [3N] x|y|z fixed point
   double* acc;               // [ACC_N]
   int natom;
+  // work counters: list entries scanned, entries kept for the next shell,
+  // atom pairs evaluated with Ewald, atom pairs evaluated LJ-only
+  unsigned long long* wcnt;
 };
 
 struct PmePlan {
@@ -120,7 +123,10 @@ struct ApiScratch {
   size_t q_n = 0;
 };
 
+struct MdState;  // md.cu
+
 struct orac_gpu_ctx {
+  MdState* md = nullptr;
   int device = 0;
   cudaStream_t stream = nullptr;
   char err[1024] = {0};
@@ -197,7 +203,22 @@ struct orac_gpu_ctx {
 
   // PME
   PmePlan pme;
+
+  // measurement: work counters of the pair kernel and CUDA events around
+  // its launches (recorded into captured graphs as event nodes)
+  unsigned long long* d_wcnt = nullptr;  // [4]
+  bool prof = false;
+  std::vector<cudaEvent_t> prof_ev;  // pairs (start, end)
+  int prof_next = 0;
+  double prof_ms = 0;
+  int64_t prof_n = 0;
 };
+
+// record the start/end events of one profiled launch (no-op unless prof)
+int prof_begin(orac_gpu_ctx* ctx, int* slot);
+int prof_end(orac_gpu_ctx* ctx, int slot);
+// sum the elapsed time of slots [a, b) into prof_ms / prof_n (after a sync)
+int prof_collect(orac_gpu_ctx* ctx, int a, int b);
 
 // ---------------------------------------------------------------- errors
 int ctx_fail(orac_gpu_ctx* c, int code, const char* fmt, ...);
@@ -258,3 +279,19 @@ int self_launch(orac_gpu_ctx* ctx, const int* d_ss, double* d_e);
 int shell_run(orac_gpu_ctx* ctx, char rshell, const double* d_xyz,
               const double* d_grp, const double* d_mol, double* d_f,
               double* d_e, double* d_stress, int energy);
+// the same with explicit shell radii (the driver's list-update calls swap
+// radii, src/mtsmd.f:2436-2469)
+int shell_run_r(orac_gpu_ctx* ctx, char rshell, const ShellRadii& radii,
+                const double* d_xyz, const double* d_grp, const double* d_mol,
+                double* d_f, double* d_e, double* d_stress, int energy);
+// graph-capturable H-list rebuild: no host synchronisation, capacity must be
+// reserved beforehand; an overflow sets *d_flag bit 1 and leaves the list
+// invalid on the device
+int list_build_cells_async(orac_gpu_ctx* ctx, double rcut, GList* out,
+                           int* d_flag);
+int list_prepare_stencil(orac_gpu_ctx* ctx, double rcut);
+// md.cu
+void md_destroy(orac_gpu_ctx* ctx);
+// device part of fft_pme (api_pme.cu)
+int fft_pme_device(orac_gpu_ctx* ctx, const double* d_sxyz,
+                   const double* d_mol, double* d_f, double* d_eout);

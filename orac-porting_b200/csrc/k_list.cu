@@ -126,6 +126,8 @@ struct ListArgs {
   const int* exj;
   const unsigned char* massinf;
   int allpairs;
+  int64_t cap;  // fill pass: entries available (negative: unchecked)
+  int* flag;    // fill pass: bit 1 set on overflow
 };
 
 __device__ __forceinline__ bool pair_in(const ListArgs& A, double xi, double yi,
@@ -172,6 +174,10 @@ __global__ void __launch_bounds__(128) k_pairs(const ListArgs A) {
   const int lane = threadIdx.x & 31;
   const int i = blockIdx.x * 4 + (threadIdx.x >> 5);
   if (i >= A.G) return;
+  if (FILL && A.cap >= 0 && (int64_t)A.off[A.G] > A.cap) {  // ORAC: xerror on nnlpp overflow
+    if (i == 0 && lane == 0) atomicOr(A.flag, 2);
+    return;
+  }
   const double xi = A.grp[i], yi = A.grp[A.G + i], zi = A.grp[2 * A.G + i];
   int total = 0;
   const int base = FILL ? A.off[i] : 0;
@@ -344,6 +350,8 @@ ListArgs base_args(orac_gpu_ctx* ctx, double rcut, GList* out) {
   A.exoff = ctx->d_exoff;
   A.exj = ctx->d_exj;
   A.massinf = ctx->d_amassinf;
+  A.cap = -1;
+  A.flag = ctx->d_flag;
   return A;
 }
 
@@ -415,4 +423,49 @@ int list_build_allpairs(orac_gpu_ctx* ctx, double rcut, GList* out) {
   ListArgs A = base_args(ctx, rcut, out);
   A.allpairs = 1;
   return pairs_count_fill(ctx, A, out);
+}
+
+int list_prepare_stencil(orac_gpu_ctx* ctx, double rcut) {
+  if (int rc = build_stencil(ctx, rcut)) return rc;
+  const int ncell = ctx->ncx * ctx->ncy * ctx->ncz;
+  if (ncell > ctx->ncell_cap) {
+    if (dev_alloc(ctx, &ctx->d_cell_cnt, ncell + 1)) return ORAC_ERR_CUDA;
+    if (dev_alloc(ctx, &ctx->d_cell_start, ncell + 1)) return ORAC_ERR_CUDA;
+    ctx->ncell_cap = ncell;
+  }
+  return ORAC_OK;
+}
+
+int list_build_cells_async(orac_gpu_ctx* ctx, double rcut, GList* out, int* d_flag) {
+  if (!ctx->d_stencil || ctx->sten_rcut != rcut)
+    return ctx_fail(ctx, ORAC_ERR_STATE, "stencil for rcut %.3f not prepared", rcut);
+  const int ncell = ctx->ncx * ctx->ncy * ctx->ncz;
+  const int G = ctx->G;
+  CK(cudaMemsetAsync(ctx->d_cell_cnt, 0, sizeof(int) * (ncell + 1), ctx->stream));
+  k_cell_assign<<<(G + 255) / 256, 256, 0, ctx->stream>>>(G, ctx->d_grp, ctx->ncx, ctx->ncy, ctx->ncz,
+                                                         ctx->d_cell_of, ctx->d_cell_cnt);
+  CKL();
+  k_scan<<<1, 1024, 0, ctx->stream>>>(ncell, ctx->d_cell_cnt, ctx->d_cell_start, nullptr);
+  CKL();
+  CK(cudaMemsetAsync(ctx->d_cell_cnt, 0, sizeof(int) * (ncell + 1), ctx->stream));
+  k_cell_fill<<<(G + 255) / 256, 256, 0, ctx->stream>>>(G, ctx->d_cell_of, ctx->d_cell_start, ctx->d_cell_cnt,
+                                                       ctx->d_cell_grp);
+  CKL();
+  k_cell_order<<<(ncell + 255) / 256, 256, 0, ctx->stream>>>(ncell, ctx->d_cell_start, ctx->d_cell_grp);
+  CKL();
+  ListArgs A = base_args(ctx, rcut, out);
+  A.allpairs = 0;
+  A.cap = out->cap;
+  A.flag = d_flag;
+  const int nb = (G + 3) / 4;
+  k_pairs<false><<<nb, 128, 0, ctx->stream>>>(A);
+  CKL();
+  k_scan<<<1, 1024, 0, ctx->stream>>>(G, out->cnt, out->off, ctx->d_total);
+  CKL();
+  A.j = out->j;
+  A.mask = out->mask;
+  k_pairs<true><<<nb, 128, 0, ctx->stream>>>(A);
+  CKL();
+  out->valid = true;
+  return ORAC_OK;
 }

@@ -92,6 +92,7 @@ __global__ void __launch_bounds__(WPB * 32)
   const float2* lj = staged ? s_lj : A.lj;
 
   double ec0 = 0, ec1 = 0, ec2 = 0, eq0 = 0, eq1 = 0, eq2 = 0;
+  unsigned npairs = 0, nscan = 0, nkept = 0;
   float v00 = 0, v01 = 0, v02 = 0, v10 = 0, v11 = 0, v12 = 0, v20 = 0,
         v21 = 0, v22 = 0;
 
@@ -144,6 +145,7 @@ __global__ void __launch_bounds__(WPB * 32)
         }
         nout += __popc(bal);
       }
+      nscan += valid ? 1u : 0u;
       if (!A.forces_on || !valid) continue;
       bool switched;
       float sw = 1.f, dsw = 0.f;
@@ -188,6 +190,7 @@ __global__ void __launch_bounds__(WPB * 32)
           const float2 L = lj[s_ti[warp][a] * A.ntype + tb];
           const bool ljon = L.y != 0.f;
           if (A.lskip && !ljon && A.ewald) continue;  // src/force.f:416-417
+          npairs++;
           const float rx = dcx + ai.x - ob.x;
           const float ry = dcy + ai.y - ob.y;
           const float rz = dcz + ai.z - ob.z;
@@ -294,7 +297,10 @@ __global__ void __launch_bounds__(WPB * 32)
         v22 += gz * iz;
       }
     }
-    if (A.next_on && lane == 0) A.cnt_out[i] = nout;
+    if (A.next_on && lane == 0) {
+      A.cnt_out[i] = nout;
+      nkept += (unsigned)nout;
+    }
     if (A.forces_on) {
 #pragma unroll
       for (int a = 0; a < MG; a++) {
@@ -310,6 +316,21 @@ __global__ void __launch_bounds__(WPB * 32)
       }
     }
     __syncwarp();
+  }
+  {
+    // work counters, one atomic per warp
+    unsigned s0 = nscan, s1 = nkept, s2 = npairs;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+      s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+      s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+    }
+    if (lane == 0) {
+      if (s0) atomicAdd(A.wcnt + 0, (unsigned long long)s0);
+      if (s1) atomicAdd(A.wcnt + 1, (unsigned long long)s1);
+      if (s2) atomicAdd(A.wcnt + (A.lskip ? 3 : 2), (unsigned long long)s2);
+    }
   }
   if (!A.forces_on) return;
   // block reduction of energies and image virial
@@ -404,6 +425,10 @@ int pair_launch(orac_gpu_ctx* ctx, const PairArgs& a, int maxg) {
   int nb = (a.ngrp + WPB - 1) / WPB;
   if (nb < 1) nb = 1;
   const size_t smem = (size_t)(a.ntype * a.ntype <= LJ_SMEM_MAX ? a.ntype * a.ntype : 0) * sizeof(float2);
+  if (maxg > ORAC_MAXG)
+    return ctx_fail(ctx, ORAC_ERR_PARAM, "charge group of %d atoms exceeds %d", maxg, ORAC_MAXG);
+  int slot = -1;
+  if (int rc = prof_begin(ctx, &slot)) return rc;
   if (maxg <= 4) {
     if (a.energy)
       k_pair<4, true><<<nb, WPB * 32, smem, ctx->stream>>>(a);
@@ -414,10 +439,33 @@ int pair_launch(orac_gpu_ctx* ctx, const PairArgs& a, int maxg) {
       k_pair<8, true><<<nb, WPB * 32, smem, ctx->stream>>>(a);
     else
       k_pair<8, false><<<nb, WPB * 32, smem, ctx->stream>>>(a);
-  } else {
-    return ctx_fail(ctx, ORAC_ERR_PARAM, "charge group of %d atoms exceeds %d", maxg, ORAC_MAXG);
   }
   CKL();
+  return prof_end(ctx, slot);
+}
+
+int prof_begin(orac_gpu_ctx* ctx, int* slot) {
+  *slot = -1;
+  if (!ctx->prof) return ORAC_OK;
+  if (2 * (ctx->prof_next + 1) > (int)ctx->prof_ev.size()) return ORAC_OK;  // pool exhausted: not profiled
+  *slot = ctx->prof_next++;
+  CK(cudaEventRecord(ctx->prof_ev[2 * *slot], ctx->stream));
+  return ORAC_OK;
+}
+
+int prof_end(orac_gpu_ctx* ctx, int slot) {
+  if (slot < 0) return ORAC_OK;
+  CK(cudaEventRecord(ctx->prof_ev[2 * slot + 1], ctx->stream));
+  return ORAC_OK;
+}
+
+int prof_collect(orac_gpu_ctx* ctx, int a, int b) {
+  for (int s = a; s < b; s++) {
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, ctx->prof_ev[2 * s], ctx->prof_ev[2 * s + 1]));
+    ctx->prof_ms += ms;
+    ctx->prof_n++;
+  }
   return ORAC_OK;
 }
 

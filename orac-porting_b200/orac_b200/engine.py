@@ -204,6 +204,31 @@ class Engine:
               "ferrf")
         return np.stack([fx, fy, fz]), fs
 
+    # --------------------------------------------------------------- MD
+    def md_setup(self, dt_h, lrespa, mrespa, nupdte, rshk="l", n1respa=1, n0respa=1, econst=0.0, graphs=True):
+        """Device-resident r-RESPA run of this system (orac_gpu_md_setup)."""
+        s = self.s
+        r = s.cartesian()
+        self._cn = i32(s.constraints.ravel())
+        self._dss = f64(s.cdist ** 2)
+        check(self.ctx, self.lib.orac_gpu_md_setup(self.ctx, f64(r[0]), f64(r[1]), f64(r[2]), f64(s.vx), f64(s.vy),
+                                                   f64(s.vz), self._cn, self._dss, len(s.constraints), dt_h, lrespa,
+                                                   mrespa, n1respa, n0respa, nupdte, rshk.encode(), econst),
+              "md_setup")
+        check(self.ctx, self.lib.orac_gpu_md_set_graphs(self.ctx, int(graphs)), "md_set_graphs")
+
+    def md_run(self, nsteps, energy_every=0):
+        nrec = nsteps // energy_every if energy_every else 0
+        rec = np.zeros(max(1, nrec) * 12)
+        check(self.ctx, self.lib.orac_gpu_md_run(self.ctx, nsteps, energy_every, rec), "md_run")
+        return rec[:nrec * 12].reshape(-1, 12)
+
+    def md_state(self):
+        n = self.s.ntap
+        a = [np.zeros(n) for _ in range(6)]
+        check(self.ctx, self.lib.orac_gpu_md_get_state(self.ctx, *a), "md_get_state")
+        return np.stack(a[:3]), np.stack(a[3:])
+
     def cself(self):
         a = C.c_double()
         b = C.c_double()

@@ -33,7 +33,7 @@ class OracGpuError(RuntimeError):
 def declared_symbols(header=HEADER):
     """Names of every function declared in include/orac_gpu.h."""
     text = open(header).read()
-    return sorted(set(re.findall(r"^\s*(?:int|const char\*|void)\s+(orac_gpu_\w+)\s*\(", text, re.M)))
+    return sorted(set(re.findall(r"^\s*(?:int|const char\s*\*|void\s*\*?)\s*(orac_gpu_\w+)\s*\(", text, re.M)))
 
 
 def load():
@@ -66,6 +66,17 @@ def load():
         "orac_gpu_cself": (i, [_P, d, _DP, _DP]),
         "orac_gpu_mts_forces_dev": (i, [_P, ch, _P, _P, _P, _P, _P, _P]),
         "orac_gpu_fft_pme_dev": (i, [_P, _P, _P, _P, _P, _P]),
+        "orac_gpu_md_setup": (i, [_P, _D, _D, _D, _D, _D, _D, _I, _D, i, d, i, i, i, i, i, ch, d]),
+        "orac_gpu_md_run": (i, [_P, i, i, _D]),
+        "orac_gpu_md_get_state": (i, [_P, _D, _D, _D, _D, _D, _D]),
+        "orac_gpu_md_set_graphs": (i, [_P, i]),
+        "orac_gpu_md_set_state": (i, [_P, _P, _P, _P, _P, _P, _P]),
+        "orac_gpu_md_run_async": (i, [_P, i]),
+        "orac_gpu_md_collect": (i, [_P]),
+        "orac_gpu_get_stream": (_P, [_P]),
+        "orac_gpu_counters": (i, [_P, C.POINTER(i64), i]),
+        "orac_gpu_prof_enable": (i, [_P, i]),
+        "orac_gpu_prof_read": (i, [_P, C.POINTER(d), C.POINTER(i64), i]),
         "orac_gpu_sync": (i, [_P]),
         "orac_gpu_stats": (i, [_P, C.POINTER(i64), C.POINTER(i64)]),
     }

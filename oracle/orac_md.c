@@ -1,0 +1,414 @@
+/*
+ * ORACLE — test infrastructure only.
+ *
+ * FP64 CPU restatement of the NVE r-RESPA step loop of ORAC's mtsmd
+ * (src/mtsmd.f:2390-3540) over the restated force routines of
+ * orac_oracle.c: kicks as correc (src/correc.f), drift as verlet
+ * (src/verlet.f), SHAKE/RATTLE as the iterative branches of
+ * src/rattle_verlet.f and src/rattle_correc.f (tolerance 1e-8 A^2,
+ * 5000-iteration cap), the list update of src/mtsmd.f:2403-2470 and the
+ * phony M-list refresh of :3287-3295.  It serves as the checker of the GPU
+ * driver and as the timed CPU baseline (OpenMP over groups, as ORAC).
+ */
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#include "orac_oracle.h"
+
+typedef struct {
+  int ntap, ngrp, nprot, ma;
+  const int *ss, *nbtype, *type, *atomg, *atomp, *grppt, *mapnl;
+  const double *charge, *ecc12, *ecc6, *mass, *pmass;
+  double massinfty;
+  double co[9], oc[9], volume;
+  double alphal, rkcut;
+  int order, n1, n2, n3;
+  double sh[9]; /* rcutm rtolm rneim rcutl rtoll rneil rcuth rtolh rneih */
+  int ncx, ncy, ncz;
+  int ncnst;
+  int *cnst;
+  double* dss;
+  int nmolc;
+  int* cstart; /* constraints sorted by molecule */
+  double dth;
+  int lrespa, mrespa, nupdte;
+  char rshk;
+  int nthreads;
+  double econst;
+  /* state */
+  double *x, *v, *xo, *fh, *fl, *fm, *s, *g, *m;
+  int *lh, *ll, *lm;
+  long caph, capl, capm;
+  int *indxi, *indxj, *indxk, nind;
+  long step;
+  double e[3][6], eer, ekin;
+} orc_md;
+
+static void md_coords(orc_md* M) {
+  int N = M->ntap;
+  orc_change_frame(M->co, M->oc, -1, N, M->x, M->x + N, M->x + 2 * N, M->s, M->s + N, M->s + 2 * N);
+  orc_appbou(M->s, M->s + N, M->s + 2 * N, M->g, M->g + M->ngrp, M->g + 2 * M->ngrp, M->pmass, M->ngrp, M->grppt);
+  int P = M->nprot;
+  double* mt = (double*)calloc(P, sizeof(double));
+  for (int k = 0; k < 3 * P; k++) M->m[k] = 0.0;
+  for (int a = 0; a < N; a++) {
+    int p = M->atomp[a] - 1;
+    mt[p] += M->mass[a];
+    M->m[p] += M->mass[a] * M->s[a];
+    M->m[P + p] += M->mass[a] * M->s[N + a];
+    M->m[2 * P + p] += M->mass[a] * M->s[2 * N + a];
+  }
+  for (int p = 0; p < P; p++) {
+    M->m[p] /= mt[p];
+    M->m[P + p] /= mt[p];
+    M->m[2 * P + p] /= mt[p];
+  }
+  free(mt);
+}
+
+/* one call of force with explicit radii, like mts_forces (src/mts_forces.f) */
+static long md_force(orc_md* M, const int* in, int* out, long capout, double rneigh, double rinn, double rout,
+                     double rtolinn, double rtolout, double* f, double* ue) {
+  int N = M->ntap, G = M->ngrp;
+  double st[9] = {0};
+  double uel[6];
+  int lskip = orc_decide_force(rinn, M->alphal);
+  double* tmp = (double*)calloc(3 * (size_t)N, sizeof(double));
+  long n = orc_force(M->ss, M->s, M->s + N, M->s + 2 * N, M->g, M->g + G, M->g + 2 * G, M->charge, M->nbtype,
+                     M->type, M->ma, N, M->atomg, M->m, M->m + M->nprot, M->m + 2 * M->nprot, M->atomp, M->co,
+                     M->ecc12, M->ecc6, M->alphal, M->mapnl, G, M->grppt, uel, tmp, tmp + N, tmp + 2 * N, st, in,
+                     out, capout, rneigh, rinn, rout, rtolinn, rtolout, M->pmass, 1, M->mass, M->massinfty, lskip, 1,
+                     M->nthreads);
+  if (f)
+    for (long k = 0; k < 3 * (long)N; k++) f[k] += tmp[k];
+  if (ue) memcpy(ue, uel, sizeof(uel));
+  free(tmp);
+  return n;
+}
+
+static int md_lists(orc_md* M) {
+  int G = M->ngrp;
+  double* r = M->sh;
+  double rc = r[6] + r[7] + r[8];
+  for (;;) {
+    long n = orc_lc_list(M->ncx, M->ncy, M->ncz, M->nind, M->indxi, M->indxj, M->indxk, rc, M->co, M->g, M->g + G,
+                         M->g + 2 * G, G, M->lh, M->caph);
+    if (n >= 0) break;
+    M->caph *= 2;
+    M->lh = (int*)realloc(M->lh, sizeof(int) * M->caph);
+  }
+  /* phony 'h' with rcuth=rcutl, rtolh=0: ro=rcutl ri=rcutl rto=0 rti=rtoll rni=rneil */
+  if (M->capl < M->caph) {
+    M->capl = M->caph;
+    M->ll = (int*)realloc(M->ll, sizeof(int) * M->capl);
+  }
+  if (md_force(M, M->lh, M->ll, M->capl, r[5], r[3], r[3], r[4], 0.0, NULL, NULL) < 0) return -1;
+  /* phony 'l' with rcutl=rcutm, rtoll=0: ro=rcutm ri=rcutm rto=0 rti=rtolm rni=rneim */
+  if (M->capm < M->caph) {
+    M->capm = M->caph;
+    M->lm = (int*)realloc(M->lm, sizeof(int) * M->capm);
+  }
+  if (md_force(M, M->ll, M->lm, M->capm, r[2], r[0], r[0], r[1], 0.0, NULL, NULL) < 0) return -1;
+  return 0;
+}
+
+static void md_kick(orc_md* M, const double* f, double dt);
+static int md_shake(orc_md* M, double dt);
+static int md_rattle(orc_md* M);
+
+static void md_forces(orc_md* M, char sh, double* f) {
+  int N = M->ntap;
+  double* r = M->sh;
+  memset(f, 0, sizeof(double) * 3 * N);
+  if (sh == 'm') {
+    md_force(M, M->lm, NULL, 0, 0.0, 0.0, r[0], 0.0, r[1], f, M->e[0]);
+  } else if (sh == 'l') {
+    md_force(M, M->ll, M->lm, M->capm, r[2], r[0], r[3], r[1], r[4], f, M->e[1]);
+  } else {
+    md_force(M, M->lh, M->ll, M->capl, r[5], r[3], r[6], r[4], r[7], f, M->e[2]);
+  }
+  if (M->rshk == sh) {
+    double st[9] = {0};
+    orc_fft_pme(N, M->s, M->s + N, M->s + 2 * N, M->m, M->m + M->nprot, M->m + 2 * M->nprot, M->charge, M->co,
+                M->oc, M->volume, M->alphal, M->order, M->n1, M->n2, M->n3, &M->eer, f, f + N, f + 2 * N, st,
+                M->atomp, 0, M->rkcut, M->nthreads);
+  }
+}
+
+static void md_refresh_m(orc_md* M) {
+  double* r = M->sh;
+  /* phony 'l' with rcutl = rcutm: ro=rcutm rto=rtoll ri=rcutm rti=rtolm rni=rneim */
+  md_force(M, M->ll, M->lm, M->capm, r[2], r[0], r[0], r[1], r[4], NULL, NULL);
+}
+
+static void md_kick(orc_md* M, const double* f, double dt) {
+  int N = M->ntap;
+#pragma omp parallel for num_threads(M->nthreads) schedule(static)
+  for (int k = 0; k < 3 * N; k++) M->v[k] += f[k] * 0.5 * dt / M->mass[k % N];
+}
+
+static int md_shake(orc_md* M, double dt) {
+  int N = M->ntap, fail = 0;
+  double dti = dt != 0.0 ? 1.0 / dt : 0.0;
+#pragma omp parallel for num_threads(M->nthreads) schedule(static) reduction(| : fail)
+  for (int mo = 0; mo < M->nmolc; mo++) {
+    int it;
+    for (it = 0; it < 5000; it++) {
+      int moved = 0;
+      for (int k = M->cstart[mo]; k < M->cstart[mo + 1]; k++) {
+        int a = M->cnst[2 * k] - 1, b = M->cnst[2 * k + 1] - 1;
+        double dx = M->x[a] - M->x[b], dy = M->x[N + a] - M->x[N + b], dz = M->x[2 * N + a] - M->x[2 * N + b];
+        double dcnt = dx * dx + dy * dy + dz * dz - M->dss[k];
+        if (fabs(dcnt) >= 1.0e-8) {
+          moved = 1;
+          double rx = M->xo[a] - M->xo[b], ry = M->xo[N + a] - M->xo[N + b], rz = M->xo[2 * N + a] - M->xo[2 * N + b];
+          double ia = 1.0 / M->mass[a], ib = 1.0 / M->mass[b];
+          double gg = dcnt / ((dx * rx + dy * ry + dz * rz) * 2.0 * (ia + ib));
+          double ga = -gg * ia, gb = gg * ib;
+          M->x[a] += rx * ga;
+          M->x[b] += rx * gb;
+          M->x[N + a] += ry * ga;
+          M->x[N + b] += ry * gb;
+          M->x[2 * N + a] += rz * ga;
+          M->x[2 * N + b] += rz * gb;
+          M->v[a] += rx * ga * dti;
+          M->v[b] += rx * gb * dti;
+          M->v[N + a] += ry * ga * dti;
+          M->v[N + b] += ry * gb * dti;
+          M->v[2 * N + a] += rz * ga * dti;
+          M->v[2 * N + b] += rz * gb * dti;
+        }
+      }
+      if (!moved) break;
+    }
+    if (it == 5000) fail = 1;
+  }
+  return fail;
+}
+
+static int md_rattle(orc_md* M) {
+  int N = M->ntap, fail = 0;
+#pragma omp parallel for num_threads(M->nthreads) schedule(static) reduction(| : fail)
+  for (int mo = 0; mo < M->nmolc; mo++) {
+    int it;
+    for (it = 0; it < 5000; it++) {
+      int moved = 0;
+      for (int k = M->cstart[mo]; k < M->cstart[mo + 1]; k++) {
+        int a = M->cnst[2 * k] - 1, b = M->cnst[2 * k + 1] - 1;
+        double rx = M->x[a] - M->x[b], ry = M->x[N + a] - M->x[N + b], rz = M->x[2 * N + a] - M->x[2 * N + b];
+        double vx = M->v[a] - M->v[b], vy = M->v[N + a] - M->v[N + b], vz = M->v[2 * N + a] - M->v[2 * N + b];
+        double dpp = rx * vx + ry * vy + rz * vz;
+        if (fabs(dpp) > 1.0e-12) {
+          moved = 1;
+          double ia = 1.0 / M->mass[a], ib = 1.0 / M->mass[b];
+          double g = -dpp / (M->dss[k] * (ia + ib));
+          M->v[a] += g * ia * rx;
+          M->v[b] -= g * ib * rx;
+          M->v[N + a] += g * ia * ry;
+          M->v[N + b] -= g * ib * ry;
+          M->v[2 * N + a] += g * ia * rz;
+          M->v[2 * N + b] -= g * ib * rz;
+        }
+      }
+      if (!moved) break;
+    }
+    if (it == 5000) fail = 1;
+  }
+  return fail;
+}
+
+static int md_kick_r(orc_md* M, const double* f, double dt) {
+  md_kick(M, f, dt);
+  return md_rattle(M);
+}
+
+void* orc_md_create(int ntap, int ngrp, int nprot, int ma, const int* ss, const int* nbtype, const int* type,
+                    const int* atomg, const int* atomp, const int* grppt, const int* mapnl, const double* charge,
+                    const double* ecc12, const double* ecc6, const double* mass, const double* pmass,
+                    double massinfty, const double* co, const double* oc, double alphal, int order, int n1, int n2,
+                    int n3, double rkcut, const double* sh, int ncx, int ncy, int ncz, const int* cnst,
+                    const double* dss, int ncnst, double dth, int lrespa, int mrespa, int nupdte, char rshk,
+                    const double* x, const double* v, int nthreads, double econst) {
+  orc_md* M = (orc_md*)calloc(1, sizeof(orc_md));
+  M->ntap = ntap;
+  M->ngrp = ngrp;
+  M->nprot = nprot;
+  M->ma = ma;
+  M->ss = ss;
+  M->nbtype = nbtype;
+  M->type = type;
+  M->atomg = atomg;
+  M->atomp = atomp;
+  M->grppt = grppt;
+  M->mapnl = mapnl;
+  M->charge = charge;
+  M->ecc12 = ecc12;
+  M->ecc6 = ecc6;
+  M->mass = mass;
+  M->pmass = pmass;
+  M->massinfty = massinfty;
+  memcpy(M->co, co, sizeof(M->co));
+  memcpy(M->oc, oc, sizeof(M->oc));
+  M->volume = 8.0 * fabs(co[0] * co[4] * co[8]);
+  M->alphal = alphal;
+  M->order = order;
+  M->n1 = n1;
+  M->n2 = n2;
+  M->n3 = n3;
+  M->rkcut = rkcut;
+  memcpy(M->sh, sh, sizeof(M->sh));
+  M->ncx = ncx;
+  M->ncy = ncy;
+  M->ncz = ncz;
+  M->dth = dth;
+  M->lrespa = lrespa;
+  M->mrespa = mrespa;
+  M->nupdte = nupdte;
+  M->rshk = rshk;
+  M->nthreads = nthreads;
+  M->econst = econst;
+  int N = ntap;
+  M->x = (double*)malloc(sizeof(double) * 3 * N);
+  M->v = (double*)malloc(sizeof(double) * 3 * N);
+  M->xo = (double*)malloc(sizeof(double) * 3 * N);
+  M->fh = (double*)calloc(3 * (size_t)N, sizeof(double));
+  M->fl = (double*)calloc(3 * (size_t)N, sizeof(double));
+  M->fm = (double*)calloc(3 * (size_t)N, sizeof(double));
+  M->s = (double*)malloc(sizeof(double) * 3 * N);
+  M->g = (double*)malloc(sizeof(double) * 3 * ngrp);
+  M->m = (double*)malloc(sizeof(double) * 3 * nprot);
+  memcpy(M->x, x, sizeof(double) * 3 * N);
+  memcpy(M->v, v, sizeof(double) * 3 * N);
+  /* constraints grouped by molecule (stable) */
+  M->ncnst = ncnst;
+  M->cnst = (int*)malloc(sizeof(int) * 2 * (ncnst + 1));
+  M->dss = (double*)malloc(sizeof(double) * (ncnst + 1));
+  M->cstart = (int*)malloc(sizeof(int) * (nprot + 2));
+  int k2 = 0, nm = 0;
+  M->cstart[0] = 0;
+  int* order_k = (int*)malloc(sizeof(int) * (ncnst + 1));
+  int* cntp = (int*)calloc(nprot + 1, sizeof(int));
+  for (int k = 0; k < ncnst; k++) cntp[atomp[cnst[2 * k] - 1]]++;
+  int* startp = (int*)calloc(nprot + 2, sizeof(int));
+  for (int p = 1; p <= nprot; p++) startp[p + 1] = startp[p] + cntp[p];
+  for (int k = 0; k < ncnst; k++) order_k[startp[atomp[cnst[2 * k] - 1]]++] = k;
+  for (int p = 1, pos = 0; p <= nprot; p++) {
+    if (!cntp[p]) continue;
+    for (int q = 0; q < cntp[p]; q++, pos++) {
+      int k = order_k[pos];
+      M->cnst[2 * k2] = cnst[2 * k];
+      M->cnst[2 * k2 + 1] = cnst[2 * k + 1];
+      M->dss[k2] = dss[k];
+      k2++;
+    }
+    M->cstart[++nm] = k2;
+  }
+  M->nmolc = nm;
+  free(order_k);
+  free(cntp);
+  free(startp);
+  int indmax = (2 * ncx) * (2 * ncy) * (2 * ncz) + 1;
+  M->indxi = (int*)malloc(sizeof(int) * indmax);
+  M->indxj = (int*)malloc(sizeof(int) * indmax);
+  M->indxk = (int*)malloc(sizeof(int) * indmax);
+  M->nind = orc_lc_index(indmax, ncx, ncy, ncz, sh[6] + sh[7] + sh[8], co, M->indxi, M->indxj, M->indxk);
+  M->caph = M->capl = M->capm = 1 << 20;
+  M->lh = (int*)malloc(sizeof(int) * M->caph);
+  M->ll = (int*)malloc(sizeof(int) * M->capl);
+  M->lm = (int*)malloc(sizeof(int) * M->capm);
+  if (M->nind < 0) return NULL;
+  md_coords(M);
+  md_lists(M);
+  md_forces(M, 'm', M->fm);
+  md_forces(M, 'l', M->fl);
+  md_forces(M, 'h', M->fh);
+  md_refresh_m(M);
+  return M;
+}
+
+static double md_ekin(orc_md* M) {
+  int N = M->ntap;
+  double e = 0;
+  for (int a = 0; a < N; a++)
+    e += 0.5 * M->mass[a] * (M->v[a] * M->v[a] + M->v[N + a] * M->v[N + a] + M->v[2 * N + a] * M->v[2 * N + a]);
+  return e;
+}
+
+/* nsteps H steps; records as the GPU driver: 12 doubles every energy_every */
+int orc_md_run(void* h, int nsteps, int energy_every, double* rec) {
+  orc_md* M = (orc_md*)h;
+  int N = M->ntap, fail = 0, nrec = 0;
+  for (int k = 0; k < nsteps; k++) {
+    if (M->step % M->nupdte == 0 && M->step > 0)
+      if (md_lists(M)) return 3;
+    fail |= md_kick_r(M, M->fh, M->dth);
+    double tl = M->dth / M->lrespa, tm = tl / M->mrespa;
+    for (int il = 0; il < M->lrespa; il++) {
+      fail |= md_kick_r(M, M->fl, tl);
+      for (int im = 0; im < M->mrespa; im++) {
+        fail |= md_kick_r(M, M->fm, tm);
+        memcpy(M->xo, M->x, sizeof(double) * 3 * N);
+        for (int q = 0; q < 3 * N; q++) M->x[q] += tm * M->v[q];
+        fail |= md_shake(M, tm);
+        fail |= md_rattle(M);
+        md_coords(M);
+        md_forces(M, 'm', M->fm);
+        fail |= md_kick_r(M, M->fm, tm);
+      }
+      md_forces(M, 'l', M->fl);
+      fail |= md_kick_r(M, M->fl, tl);
+    }
+    md_forces(M, 'h', M->fh);
+    md_refresh_m(M);
+    fail |= md_kick_r(M, M->fh, M->dth);
+    M->step++;
+    if (energy_every > 0 && (k + 1) % energy_every == 0) {
+      double* r = rec + 12 * (size_t)nrec++;
+      r[0] = (double)M->step;
+      r[1] = md_ekin(M);
+      for (int s = 0; s < 3; s++) {
+        r[2 + 2 * s] = M->e[s][0] + M->e[s][1] + M->e[s][2];
+        r[3 + 2 * s] = M->e[s][3] + M->e[s][4] + M->e[s][5];
+      }
+      r[8] = M->eer;
+      r[9] = M->econst;
+      r[10] = r[1] + r[2] + r[3] + r[4] + r[5] + r[6] + r[7] + r[8] + r[9];
+      r[11] = fail;
+    }
+  }
+  return fail ? 1 : 0;
+}
+
+void orc_md_get_state(void* h, double* x, double* v) {
+  orc_md* M = (orc_md*)h;
+  memcpy(x, M->x, sizeof(double) * 3 * M->ntap);
+  memcpy(v, M->v, sizeof(double) * 3 * M->ntap);
+}
+
+void orc_md_destroy(void* h) {
+  orc_md* M = (orc_md*)h;
+  if (!M) return;
+  free(M->x);
+  free(M->v);
+  free(M->xo);
+  free(M->fh);
+  free(M->fl);
+  free(M->fm);
+  free(M->s);
+  free(M->g);
+  free(M->m);
+  free(M->cnst);
+  free(M->dss);
+  free(M->cstart);
+  free(M->indxi);
+  free(M->indxj);
+  free(M->indxk);
+  free(M->lh);
+  free(M->ll);
+  free(M->lm);
+  free(M);
+}

@@ -291,6 +291,69 @@ class Oracle:
         return np.stack([fx, fy, fz]), ue
 
 
+class OracleMD:
+    """CPU restatement of ORAC's NVE r-RESPA loop (orac_md.c)."""
+
+    def __init__(self, s, dt_h, lrespa, mrespa, nupdte, rshk="l", nthreads=None, econst=0.0):
+        L = lib()
+        self.L = L
+        self.s = s
+        vp = C.c_void_p
+        L.orc_md_create.restype = vp
+        L.orc_md_create.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, _I, _I, _I, _I, _I, _I, _I, _D, _D, _D, _D,
+                                    _D, C.c_double, _D, _D, C.c_double, C.c_int, C.c_int, C.c_int, C.c_int,
+                                    C.c_double, _D, C.c_int, C.c_int, C.c_int, _I, _D, C.c_int, C.c_double, C.c_int,
+                                    C.c_int, C.c_int, C.c_char, _D, _D, C.c_int, C.c_double]
+        L.orc_md_run.restype = C.c_int
+        L.orc_md_run.argtypes = [vp, C.c_int, C.c_int, _D]
+        L.orc_md_get_state.argtypes = [vp, _D, _D]
+        L.orc_md_destroy.argtypes = [vp]
+        sh = s.shells
+        self._keep = dict(
+            ss=_i(s.ss_index), nbt=_i(s.nbtype), tt=_i(np.asarray(s.type_table).T.ravel()), ag=_i(s.atomg),
+            ap=_i(s.atomp), gp=_i(s.grppt.ravel()), mp=_i(s.mapnl), q=_f(s.charge), e12=_f(s.ecc12), e6=_f(s.ecc6),
+            m=_f(s.mass), pm=_f(s.pmass), co=_colmajor(s.co), oc=_colmajor(s.oc),
+            sh=_f([sh.rcutm, sh.rtolm, sh.rneim, sh.rcutl, sh.rtoll, sh.rneil, sh.rcuth, sh.rtolh, sh.rneih]),
+            cn=_i(s.constraints.ravel()), dss=_f(s.cdist ** 2))
+        k = self._keep
+        x = _f(s.cartesian().ravel())
+        v = _f(np.concatenate([s.vx, s.vy, s.vz]))
+        n1, n2, n3 = s.nfft
+        self.h = L.orc_md_create(s.ntap, s.ngrp, s.nprot, s.ntype, k["ss"], k["nbt"], k["tt"], k["ag"], k["ap"],
+                                 k["gp"], k["mp"], k["q"], k["e12"], k["e6"], k["m"], k["pm"], s.massinfty, k["co"],
+                                 k["oc"], s.alphal, s.order, n1, n2, n3, s.rkcut, k["sh"], *s.ncell, k["cn"],
+                                 k["dss"], len(s.constraints), dt_h, lrespa, mrespa, nupdte, rshk.encode(), x, v,
+                                 nthreads or default_threads(), econst)
+        if not self.h:
+            raise RuntimeError("orc_md_create failed")
+
+    def run(self, nsteps, energy_every=0):
+        nrec = nsteps // energy_every if energy_every else 0
+        rec = np.zeros(max(1, nrec) * 12)
+        rc = self.L.orc_md_run(self.h, nsteps, energy_every, rec)
+        if rc:
+            raise RuntimeError(f"orc_md_run status {rc}")
+        return rec[:nrec * 12].reshape(-1, 12)
+
+    def state(self):
+        n = self.s.ntap
+        x = np.zeros(3 * n)
+        v = np.zeros(3 * n)
+        self.L.orc_md_get_state(self.h, x, v)
+        return x.reshape(3, n), v.reshape(3, n)
+
+    def close(self):
+        if self.h:
+            self.L.orc_md_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def rel_rms(F, Fref):
     """ORAC's check_force metric (src/pme_code.f:378-396)."""
     return float(np.sqrt(((F - Fref) ** 2).sum() / (Fref ** 2).sum()))
