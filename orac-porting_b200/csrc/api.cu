@@ -531,10 +531,11 @@ int orac_gpu_prof_enable(orac_gpu_ctx* ctx, int on) {
 int orac_gpu_prof_read(orac_gpu_ctx* ctx, double* ms_total, int64_t* nlaunch, int reset) {
   if (!ctx) return ORAC_ERR_PARAM;
   if (ms_total) *ms_total = ctx->prof_ms;
-  if (nlaunch) *nlaunch = ctx->prof_n;
+  if (nlaunch) *nlaunch = ctx->prof_bad ? -1 : ctx->prof_n;  // -1: some launches could not be timed
   if (reset) {
     ctx->prof_ms = 0;
     ctx->prof_n = 0;
+    ctx->prof_bad = false;
   }
   return ORAC_OK;
 }

@@ -208,6 +208,7 @@ struct orac_gpu_ctx {
   // its launches (recorded into captured graphs as event nodes)
   unsigned long long* d_wcnt = nullptr;  // [4]
   bool prof = false;
+  bool prof_bad = false;  // an event pair could not be timed
   std::vector<cudaEvent_t> prof_ev;  // pairs (start, end)
   int prof_next = 0;
   double prof_ms = 0;

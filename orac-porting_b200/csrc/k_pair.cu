@@ -444,25 +444,39 @@ int pair_launch(orac_gpu_ctx* ctx, const PairArgs& a, int maxg) {
   return prof_end(ctx, slot);
 }
 
+// Inside a stream capture an event must be recorded as an external event
+// node to be a real, timed record when the graph replays.
+static int prof_record(orac_gpu_ctx* ctx, cudaEvent_t ev) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  CK(cudaStreamIsCapturing(ctx->stream, &cs));
+  if (cs == cudaStreamCaptureStatusActive)
+    CK(cudaEventRecordWithFlags(ev, ctx->stream, cudaEventRecordExternal));
+  else
+    CK(cudaEventRecord(ev, ctx->stream));
+  return ORAC_OK;
+}
+
 int prof_begin(orac_gpu_ctx* ctx, int* slot) {
   *slot = -1;
   if (!ctx->prof) return ORAC_OK;
   if (2 * (ctx->prof_next + 1) > (int)ctx->prof_ev.size()) return ORAC_OK;  // pool exhausted: not profiled
   *slot = ctx->prof_next++;
-  CK(cudaEventRecord(ctx->prof_ev[2 * *slot], ctx->stream));
-  return ORAC_OK;
+  return prof_record(ctx, ctx->prof_ev[2 * *slot]);
 }
 
 int prof_end(orac_gpu_ctx* ctx, int slot) {
   if (slot < 0) return ORAC_OK;
-  CK(cudaEventRecord(ctx->prof_ev[2 * slot + 1], ctx->stream));
-  return ORAC_OK;
+  return prof_record(ctx, ctx->prof_ev[2 * slot + 1]);
 }
 
 int prof_collect(orac_gpu_ctx* ctx, int a, int b) {
   for (int s = a; s < b; s++) {
     float ms = 0.f;
-    CK(cudaEventElapsedTime(&ms, ctx->prof_ev[2 * s], ctx->prof_ev[2 * s + 1]));
+    if (cudaEventElapsedTime(&ms, ctx->prof_ev[2 * s], ctx->prof_ev[2 * s + 1]) != cudaSuccess) {
+      cudaGetLastError();  // not sticky: mark the measurement invalid, keep running
+      ctx->prof_bad = true;
+      continue;
+    }
     ctx->prof_ms += ms;
     ctx->prof_n++;
   }
