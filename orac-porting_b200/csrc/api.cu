@@ -104,11 +104,12 @@ int check_ready(orac_gpu_ctx* ctx) {
 // Shell evaluation on device-resident coordinates (used by both ABIs).
 int shell_run(orac_gpu_ctx* ctx, char rshell, const double* d_xyz, const double* d_grp, const double* d_mol,
               double* d_f, double* d_e, double* d_stress, int energy) {
-  return shell_run_r(ctx, rshell, ctx->sh, d_xyz, d_grp, d_mol, d_f, d_e, d_stress, energy);
+  return shell_run_r(ctx, rshell, ctx->sh, d_xyz, d_grp, d_mol, d_f, d_e, d_stress,
+                     SH_STRESS | (energy ? SH_ENERGY : 0));
 }
 
 int shell_run_r(orac_gpu_ctx* ctx, char rshell, const ShellRadii& radii, const double* d_xyz, const double* d_grp,
-                const double* d_mol, double* d_f, double* d_e, double* d_stress, int energy) {
+                const double* d_mol, double* d_f, double* d_e, double* d_stress, int flags) {
   ShellSel s;
   if (int rc = select_shell(ctx, radii, rshell, &s)) return rc;
   if (rshell == 'u') {
@@ -160,7 +161,6 @@ int shell_run_r(orac_gpu_ctx* ctx, char rshell, const ShellRadii& radii, const d
   a.arsinn2 = rtolinn * rtolinn * rtolinn;
   a.alphal = (float)ctx->alphal;
   a.alphad = ctx->alphal;
-  a.energy = energy ? 1 : 0;
   a.ljd = ctx->d_ljd;
   a.qd = ctx->d_aqd;
   a.twrtpi = (float)(2.0 / std::sqrt(4.0 * std::atan(1.0)));
@@ -182,13 +182,21 @@ int shell_run_r(orac_gpu_ctx* ctx, char rshell, const ShellRadii& radii, const d
   a.acc = ctx->d_acc;
   a.natom = ctx->N;
   a.wcnt = ctx->d_wcnt;
-  CK(cudaMemsetAsync(ctx->d_acc, 0, ACC_N * sizeof(double), ctx->stream));
-  if (int rc = prep_launch(ctx, d_xyz, d_grp)) return rc;
+  const bool want_e = (flags & SH_ENERGY) && d_e, want_s = (flags & SH_STRESS) && d_stress;
+  a.energy = want_e ? 1 : 0;
+  a.stress = want_s ? 1 : 0;
+  if (flags & SH_FIXED_OUT) a.ffix = reinterpret_cast<unsigned long long*>(d_f);
+  if (want_e || want_s) CK(cudaMemsetAsync(ctx->d_acc, 0, ACC_N * sizeof(double), ctx->stream));
+  if (!(flags & SH_PREPPED))
+    if (int rc = prep_launch(ctx, d_xyz, d_grp)) return rc;
   if (int rc = pair_launch(ctx, a, ctx->maxg)) return rc;
-  if (a.forces_on)
-    if (int rc = finalize_launch(ctx, d_mol, d_f)) return rc;
-  k_shell_out<<<1, 32, 0, ctx->stream>>>(ctx->d_acc, a.forces_on, d_e, d_stress);
-  CKL();
+  if (a.forces_on && !(flags & SH_FIXED_OUT))
+    if (int rc = finalize_launch(ctx, d_mol, d_f, want_s ? 1 : 0)) return rc;
+  if (want_e || want_s) {
+    k_shell_out<<<1, 32, 0, ctx->stream>>>(ctx->d_acc, a.forces_on, want_e ? d_e : nullptr,
+                                           want_s ? d_stress : nullptr);
+    CKL();
+  }
   if (a.next_on) ctx->lists[s.out].valid = true;
   return ORAC_OK;
 }

@@ -87,6 +87,17 @@ struct PairArgs {
   // work counters: list entries scanned, entries kept for the next shell,
   // atom pairs evaluated with Ewald, atom pairs evaluated LJ-only
   unsigned long long* wcnt;
+  // 0: skip the image term of the molecular virial and the block reduction
+  // (MD without pressure coupling needs neither)
+  int stress;
+};
+
+// flags of shell_run_r
+enum {
+  SH_ENERGY = 1,    // FP64 pair energies into the energy outputs
+  SH_STRESS = 2,    // molecular virial (finalize + image term)
+  SH_PREPPED = 4,   // gpos/aoff already written and the force accumulator zeroed
+  SH_FIXED_OUT = 8  // d_f is a fixed-point accumulator: skip finalize
 };
 
 struct PmePlan {
@@ -259,7 +270,8 @@ int list_masks(orac_gpu_ctx* ctx, GList* L);
 // k_pair.cu
 int pair_launch(orac_gpu_ctx* ctx, const PairArgs& a, int maxg);
 int prep_launch(orac_gpu_ctx* ctx, const double* xyz, const double* grp);
-int finalize_launch(orac_gpu_ctx* ctx, const double* mol, double* fout_accum);
+int finalize_launch(orac_gpu_ctx* ctx, const double* mol, double* fout_accum,
+                    int stress);
 // k_pme.cu
 int pme_setup(orac_gpu_ctx* ctx, int n1, int n2, int n3, int order);
 // d_eout[16]: energy sum (eer = 0.5 * [0]), virial sums v11 v22 v33 v12 v13
@@ -268,7 +280,8 @@ int pme_setup(orac_gpu_ctx* ctx, int n1, int n2, int n3, int order);
 int pme_run(orac_gpu_ctx* ctx, int natom, const double* d_cart /*3N*/,
             const double* d_q, const double* recip, double volume,
             double alpha, double* d_f /*3N accumulated*/, double* d_eout,
-            const double* d_sxyz, const double* d_mol);
+            const double* d_sxyz, const double* d_mol,
+            unsigned long long* d_ffix = nullptr /*3N fixed point instead of d_f*/);
 // k_small.cu: kind 0 fnb14, 1 fnbgrp, 2 ferrf; d_e[4]
 int small_launch(orac_gpu_ctx* ctx, int kind, const double* d_xyz,
                  const int* d_pairs, const int* d_ptype, int npairs,

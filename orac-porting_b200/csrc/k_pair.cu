@@ -281,7 +281,7 @@ __global__ void __launch_bounds__(WPB * 32)
         ec2 += pconf;
         eq2 += pcoul;
       }
-      if (imx != 0.0 || imy != 0.0 || imz != 0.0) {
+      if (A.stress && (imx != 0.0 || imy != 0.0 || imz != 0.0)) {
         // j sits at its image xpg_j + img: its virial arm gains co.img
         const float ix = (float)(A.c11 * imx + A.c12 * imy + A.c13 * imz);
         const float iy = (float)(A.c22 * imy + A.c23 * imz);
@@ -332,7 +332,7 @@ __global__ void __launch_bounds__(WPB * 32)
       if (s2) atomicAdd(A.wcnt + (A.lskip ? 3 : 2), (unsigned long long)s2);
     }
   }
-  if (!A.forces_on) return;
+  if (!A.forces_on || (!EN && !A.stress)) return;
   // block reduction of energies and image virial
   double vals[15] = {ec0, ec1, ec2, eq0, eq1, eq2, v00, v01, v02,
                      v10, v11, v12, v20, v21, v22};
@@ -382,6 +382,14 @@ __global__ void k_finalize(int N, const unsigned long long* __restrict__ ffix,
                            double* __restrict__ fout, double* __restrict__ acc) {
   __shared__ double s_red[8][9];
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (!mol) {  // forces only; the condition is uniform over the grid
+    if (t < N) {
+      fout[t] += (double)(long long)ffix[t] * ORAC_FSCALE_INV;
+      fout[N + t] += (double)(long long)ffix[N + t] * ORAC_FSCALE_INV;
+      fout[2 * N + t] += (double)(long long)ffix[2 * N + t] * ORAC_FSCALE_INV;
+    }
+    return;
+  }
   double st[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
   if (t < N) {
     const double fx = (double)(long long)ffix[t] * ORAC_FSCALE_INV;
@@ -493,10 +501,11 @@ int prep_launch(orac_gpu_ctx* ctx, const double* xyz, const double* grp) {
   return ORAC_OK;
 }
 
-int finalize_launch(orac_gpu_ctx* ctx, const double* mol, double* fout) {
+int finalize_launch(orac_gpu_ctx* ctx, const double* mol, double* fout, int stress) {
   const double* c = ctx->co;
-  k_finalize<<<(ctx->N + 255) / 256, 256, 0, ctx->stream>>>(ctx->N, ctx->d_ffix, mol, ctx->P, ctx->d_amol, c[0],
-                                                            c[3], c[6], c[4], c[7], c[8], fout, ctx->d_acc);
+  k_finalize<<<(ctx->N + 255) / 256, 256, 0, ctx->stream>>>(ctx->N, ctx->d_ffix, stress ? mol : nullptr, ctx->P,
+                                                            ctx->d_amol, c[0], c[3], c[6], c[4], c[7], c[8], fout,
+                                                            ctx->d_acc);
   CKL();
   return ORAC_OK;
 }

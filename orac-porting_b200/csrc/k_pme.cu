@@ -311,6 +311,7 @@ struct AtomArgs {
   unsigned long long* qfix;
   const float* rg;
   double* f;  // [3N] accumulated
+  unsigned long long* ffix;  // [3N] fixed-point alternative to f (or null)
   // molecular correction (optional)
   const double* sxyz;  // [3N] scaled
   const double* mol;   // [3P] scaled
@@ -426,9 +427,15 @@ __global__ void k_gather(const AtomArgs A) {
     const double fx = A.r11 * g1 + A.r12 * g2 + A.r13 * g3;
     const double fy = A.r21 * g1 + A.r22 * g2 + A.r23 * g3;
     const double fz = A.r31 * g1 + A.r32 * g2 + A.r33 * g3;
-    A.f[t] += fx;
-    A.f[A.natom + t] += fy;
-    A.f[2 * A.natom + t] += fz;
+    if (A.ffix) {  // fixed-point accumulator of the caller's RESPA level (one writer per atom)
+      A.ffix[t] += (unsigned long long)__double2ll_rn(fx * ORAC_FSCALE);
+      A.ffix[A.natom + t] += (unsigned long long)__double2ll_rn(fy * ORAC_FSCALE);
+      A.ffix[2 * A.natom + t] += (unsigned long long)__double2ll_rn(fz * ORAC_FSCALE);
+    } else {
+      A.f[t] += fx;
+      A.f[A.natom + t] += fy;
+      A.f[2 * A.natom + t] += fz;
+    }
     if (A.sxyz) {
       const int m = A.amol[t];
       const double sx = A.sxyz[t] - A.mol[m], sy = A.sxyz[A.natom + t] - A.mol[A.P + m],
@@ -541,7 +548,8 @@ int pme_setup(orac_gpu_ctx* ctx, int n1, int n2, int n3, int order) {
 }
 
 int pme_run(orac_gpu_ctx* ctx, int natom, const double* d_cart, const double* d_q, const double* recip,
-            double volume, double alpha, double* d_f, double* d_eout, const double* d_sxyz, const double* d_mol) {
+            double volume, double alpha, double* d_f, double* d_eout, const double* d_sxyz, const double* d_mol,
+            unsigned long long* d_ffix) {
   PmePlan& P = ctx->pme;
   if (!P.qfix) return ctx_fail(ctx, ORAC_ERR_STATE, "PME not set up");
   const int n1 = P.n1, n2 = P.n2, n3 = P.n3, h1 = P.h1;
@@ -568,6 +576,7 @@ int pme_run(orac_gpu_ctx* ctx, int natom, const double* d_cart, const double* d_
   A.qfix = P.qfix;
   A.rg = P.rgrid;
   A.f = d_f;
+  A.ffix = d_ffix;
   A.sxyz = d_sxyz;
   A.mol = d_mol;
   A.amol = ctx->d_amol;

@@ -3,17 +3,18 @@
 // correc (src/correc.f), verlet (src/verlet.f) and the SHAKE/RATTLE
 // constraint solvers (src/rattle_verlet.f, src/rattle_correc.f).
 //
-// State lives in HBM in FP64 (positions, velocities, per-level forces); the
-// nonbonded shells and SPME run through the same device entry points as the
-// single-call ABI.  One outer (H) step:
+// State lives in HBM: FP64 positions and velocities, and one int64
+// fixed-point force accumulator per RESPA level (H, L, M) that the shell
+// kernels and the SPME gather add into and the kicks read.  One outer (H)
+// step:
 //
 //   [every nupdte steps] linked-cell H list, phony 'h' (L list), phony 'l'
 //                        (M list)                       src/mtsmd.f:2403-2470
 //   H half kick + RATTLE                                        :2477-2484
 //   do lrespa:   L half kick + RATTLE
 //     do mrespa: M half kick + RATTLE
-//                drift (verlet) + SHAKE, coordinates -> scaled frame,
-//                group and molecule centres                :2660-2955
+//                drift (verlet) + SHAKE + RATTLE, scaled frame, group
+//                centres, pair-kernel inputs      (one fused kernel)
 //                M shell forces                                    :3030
 //                M half kick + RATTLE
 //     L shell forces (+ SPME when the reciprocal shell is L)   :3185-3201
@@ -22,41 +23,458 @@
 //   phony 'l' refresh of the M list                            :3287-3295
 //   H half kick + RATTLE
 //
-// Constraints: SHAKE with ORAC's tolerance 1e-8 A^2 on squared bond lengths
-// and a 5000-iteration cap (src/rattle_verlet.f:76,209) for every molecule;
-// ORAC solves molecules of <= 20 constraints by matrix inversion instead,
-// which converges to the same constrained positions.
+// Constraints.  Molecules with at most 3 constraints on at most 4 atoms (the
+// rigid waters) are solved by one thread with the molecule in registers, as
+// ORAC's matrix-inversion branch does for small molecules
+// (src/rattle_verlet.f:228-330): Newton iterations on the linearised
+// constraint system for SHAKE (converged to 1e-12 A^2, well inside ORAC's
+// 1e-8) and one exact linear solve for the RATTLE velocity step.  Larger
+// constrained molecules use the iterative branch (tolerance 1e-8 A^2, 5000
+// iterations, src/rattle_verlet.f:76,209).
 #include <cmath>
 
 #include "common.cuh"
 
 namespace {
 
-__global__ void k_kick(int n3, int N, double* __restrict__ v, const double* __restrict__ f,
-                       const double* __restrict__ invm, double hdt) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= n3) return;
-  v[t] += f[t] * hdt * invm[t % N];  // correc: v += f 0.5 dt / m
+constexpr int SMA = 4;  // atoms of a register-solved molecule
+constexpr int SMC = 3;  // constraints of a register-solved molecule
+
+__device__ __forceinline__ double dot3(const double* a, const double* b) {
+  return a[0] * b[0] + a[1] * b[1] + a[2] * b[2];
 }
 
-// verlet (src/verlet.f): x += dt v + 0.5 dt^2 f/m ; v += 0.5 dt f/m ; old x kept for SHAKE
-__global__ void k_verlet(int n3, int N, double* __restrict__ x, double* __restrict__ v,
-                         const double* __restrict__ f, const double* __restrict__ invm, double dt,
-                         double* __restrict__ xo) {
+// Gaussian elimination without pivoting for n <= 3 (the matrices are
+// J M^-1 J^T products: symmetric positive definite up to the small
+// difference between old and new bond vectors).  Returns false on a zero
+// pivot.
+__device__ __forceinline__ bool solve3(double A[SMC][SMC], double b[SMC], int n) {
+#pragma unroll
+  for (int k = 0; k < SMC; k++) {
+    if (k < n) {
+      if (A[k][k] == 0.0) return false;
+      const double inv = 1.0 / A[k][k];
+#pragma unroll
+      for (int i = k + 1; i < SMC; i++) {
+        if (i < n) {
+          const double f = A[i][k] * inv;
+#pragma unroll
+          for (int j = k; j < SMC; j++) A[i][j] -= f * A[k][j];
+          b[i] -= f * b[k];
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int k = SMC - 1; k >= 0; k--) {
+    if (k < n) {
+      double s = b[k];
+#pragma unroll
+      for (int j = k + 1; j < SMC; j++)
+        if (j < n) s -= A[k][j] * b[j];
+      b[k] = s / A[k][k];
+    }
+  }
+  return true;
+}
+
+struct MolArgs {
+  int N;
+  // small constrained molecules
+  int nsm;
+  const int4* sm;      // (first atom, natoms, first constraint, nconstraints)
+  const int2* smg;     // (first group, ngroups)
+  const int2* cloc;    // constraint atoms, local to the molecule
+  const double* dss;   // squared lengths
+  // atoms handled one by one (everything outside small molecules)
+  int nfree;
+  const int* free_atoms;
+  int nfreeg;
+  const int* free_groups;
+  // state
+  double* x;
+  double* xo;
+  double* v;
+  const double* invm;
+  const double* pm;
+  const float* q;
+  const int2* gmeta;
+  // scaled frame and pair-kernel inputs
+  double o11, o12, o13, o22, o23, o33;
+  double c11, c12, c13, c22, c23, c33;
+  int G;
+  double* grp;       // [3G] scaled group centres (for the list builder)
+  double4* gpos;     // [G]
+  float4* aoff;      // [N]
+  unsigned long long* fzero;  // [3N] accumulator zeroed for the coming shell (or null)
+  const unsigned long long* fkick;  // [3N] fixed-point forces of a kick
+  const double* fn;  // [3N] intramolecular forces for the drift (or null)
+  double dt;
+  double tol;
+  int* flag;
+};
+
+__device__ __forceinline__ double fixd(unsigned long long v) { return (double)(long long)v * ORAC_FSCALE_INV; }
+
+// RATTLE velocity projection of one small molecule held in registers
+__device__ __forceinline__ bool rattle_small(double x[SMA][3], double v[SMA][3], const double im[SMA], const int2* c,
+                                             int nc) {
+  double r[SMC][3], M[SMC][SMC], rhs[SMC];
+  int ca[SMC], cb[SMC];
+#pragma unroll
+  for (int k = 0; k < SMC; k++) {
+    if (k < nc) {
+      ca[k] = c[k].x;
+      cb[k] = c[k].y;
+    } else {
+      ca[k] = cb[k] = 0;
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < SMC; k++) {
+    if (k < nc) {
+      double va[3], vb[3];
+#pragma unroll
+      for (int d = 0; d < 3; d++) {
+        double xa = 0, xb = 0;
+#pragma unroll
+        for (int a = 0; a < SMA; a++) {
+          if (a == ca[k]) {
+            xa = x[a][d];
+            va[d] = v[a][d];
+          }
+          if (a == cb[k]) {
+            xb = x[a][d];
+            vb[d] = v[a][d];
+          }
+        }
+        r[k][d] = xa - xb;
+      }
+      rhs[k] = -(r[k][0] * (va[0] - vb[0]) + r[k][1] * (va[1] - vb[1]) + r[k][2] * (va[2] - vb[2]));
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < SMC; k++)
+#pragma unroll
+    for (int l = 0; l < SMC; l++) {
+      if (k < nc && l < nc) {
+        double ia = 0, ib = 0;
+#pragma unroll
+        for (int a = 0; a < SMA; a++) {
+          if (a == ca[k]) ia = im[a];
+          if (a == cb[k]) ib = im[a];
+        }
+        const double cc = (ca[k] == ca[l] ? ia : 0.0) - (ca[k] == cb[l] ? ia : 0.0) - (cb[k] == ca[l] ? ib : 0.0) +
+                          (cb[k] == cb[l] ? ib : 0.0);
+        M[k][l] = cc * dot3(r[k], r[l]);
+      } else {
+        M[k][l] = 0.0;
+      }
+    }
+  if (!solve3(M, rhs, nc)) return false;
+#pragma unroll
+  for (int l = 0; l < SMC; l++) {
+    if (l < nc) {
+#pragma unroll
+      for (int a = 0; a < SMA; a++) {
+        const double s = (a == ca[l]) ? 1.0 : ((a == cb[l]) ? -1.0 : 0.0);
+        if (s != 0.0) {
+          v[a][0] += s * rhs[l] * r[l][0] * im[a];
+          v[a][1] += s * rhs[l] * r[l][1] * im[a];
+          v[a][2] += s * rhs[l] * r[l][2] * im[a];
+        }
+      }
+    }
+  }
+  return true;
+}
+
+// SHAKE of one small molecule: Newton iterations on g_k = |d_k|^2 - L_k^2
+// with displacements along the old bond vectors r0_l, positions and
+// velocities corrected in place.
+__device__ __forceinline__ bool shake_small(double x[SMA][3], const double xo[SMA][3], double v[SMA][3],
+                                            const double im[SMA], const int2* c, const double* L2, int nc, double dt,
+                                            double tol) {
+  int ca[SMC], cb[SMC];
+  double r0[SMC][3], lam[SMC];
+#pragma unroll
+  for (int k = 0; k < SMC; k++) {
+    lam[k] = 0.0;
+    if (k < nc) {
+      ca[k] = c[k].x;
+      cb[k] = c[k].y;
+#pragma unroll
+      for (int d = 0; d < 3; d++) {
+        double xa = 0, xb = 0;
+#pragma unroll
+        for (int a = 0; a < SMA; a++) {
+          if (a == ca[k]) xa = xo[a][d];
+          if (a == cb[k]) xb = xo[a][d];
+        }
+        r0[k][d] = xa - xb;
+      }
+    } else {
+      ca[k] = cb[k] = 0;
+      r0[k][0] = r0[k][1] = r0[k][2] = 0.0;
+    }
+  }
+  bool ok = false;
+  for (int it = 0; it < 50; it++) {
+    double dk[SMC][3], g[SMC];
+    double gmax = 0.0;
+#pragma unroll
+    for (int k = 0; k < SMC; k++) {
+      if (k < nc) {
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+          double xa = 0, xb = 0;
+#pragma unroll
+          for (int a = 0; a < SMA; a++) {
+            if (a == ca[k]) xa = x[a][d];
+            if (a == cb[k]) xb = x[a][d];
+          }
+          dk[k][d] = xa - xb;
+        }
+        g[k] = -(dot3(dk[k], dk[k]) - L2[k]);
+        gmax = fmax(gmax, fabs(g[k]));
+      } else {
+        g[k] = 0.0;
+      }
+    }
+    if (gmax < tol) {
+      ok = true;
+      break;
+    }
+    double J[SMC][SMC];
+#pragma unroll
+    for (int k = 0; k < SMC; k++)
+#pragma unroll
+      for (int l = 0; l < SMC; l++) {
+        if (k < nc && l < nc) {
+          double ia = 0, ib = 0;
+#pragma unroll
+          for (int a = 0; a < SMA; a++) {
+            if (a == ca[k]) ia = im[a];
+            if (a == cb[k]) ib = im[a];
+          }
+          const double cc = (ca[k] == ca[l] ? ia : 0.0) - (ca[k] == cb[l] ? ia : 0.0) -
+                            (cb[k] == ca[l] ? ib : 0.0) + (cb[k] == cb[l] ? ib : 0.0);
+          J[k][l] = 2.0 * cc * dot3(dk[k], r0[l]);
+        } else {
+          J[k][l] = 0.0;
+        }
+      }
+    if (!solve3(J, g, nc)) return false;
+#pragma unroll
+    for (int l = 0; l < SMC; l++) {
+      if (l < nc) {
+        lam[l] += g[l];
+#pragma unroll
+        for (int a = 0; a < SMA; a++) {
+          const double s = (a == ca[l]) ? 1.0 : ((a == cb[l]) ? -1.0 : 0.0);
+          if (s != 0.0) {
+            x[a][0] += s * g[l] * r0[l][0] * im[a];
+            x[a][1] += s * g[l] * r0[l][1] * im[a];
+            x[a][2] += s * g[l] * r0[l][2] * im[a];
+          }
+        }
+      }
+    }
+  }
+  if (dt != 0.0) {
+    const double dti = 1.0 / dt;
+#pragma unroll
+    for (int l = 0; l < SMC; l++) {
+      if (l < nc) {
+#pragma unroll
+        for (int a = 0; a < SMA; a++) {
+          const double s = (a == ca[l]) ? 1.0 : ((a == cb[l]) ? -1.0 : 0.0);
+          if (s != 0.0) {
+            v[a][0] += s * lam[l] * r0[l][0] * im[a] * dti;
+            v[a][1] += s * lam[l] * r0[l][1] * im[a] * dti;
+            v[a][2] += s * lam[l] * r0[l][2] * im[a] * dti;
+          }
+        }
+      }
+    }
+  }
+  return ok;
+}
+
+// correc (v += f dt/2m) from a fixed-point level accumulator, then RATTLE.
+// Threads [0, nsm) take one small molecule each, the rest one free atom.
+__global__ void k_kick(const MolArgs A) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= n3) return;
-  const double im = invm[t % N];
-  xo[t] = x[t];
-  x[t] += dt * v[t] + f[t] * 0.5 * dt * dt * im;
-  v[t] += f[t] * 0.5 * dt * im;
+  const int N = A.N;
+  const double hdt = 0.5 * A.dt;
+  if (t < A.nsm) {
+    const int4 m = A.sm[t];
+    double x[SMA][3], v[SMA][3], im[SMA];
+#pragma unroll
+    for (int a = 0; a < SMA; a++) {
+      if (a < m.y) {
+        const int g = m.x + a;
+        im[a] = A.invm[g];
+        x[a][0] = A.x[g];
+        x[a][1] = A.x[N + g];
+        x[a][2] = A.x[2 * N + g];
+        v[a][0] = A.v[g] + fixd(A.fkick[g]) * hdt * im[a];
+        v[a][1] = A.v[N + g] + fixd(A.fkick[N + g]) * hdt * im[a];
+        v[a][2] = A.v[2 * N + g] + fixd(A.fkick[2 * N + g]) * hdt * im[a];
+      } else {
+        im[a] = 0;
+        x[a][0] = x[a][1] = x[a][2] = 0;
+        v[a][0] = v[a][1] = v[a][2] = 0;
+      }
+    }
+    if (!rattle_small(x, v, im, A.cloc + m.z, m.w)) atomicOr(A.flag, 1);
+#pragma unroll
+    for (int a = 0; a < SMA; a++) {
+      if (a < m.y) {
+        const int g = m.x + a;
+        A.v[g] = v[a][0];
+        A.v[N + g] = v[a][1];
+        A.v[2 * N + g] = v[a][2];
+      }
+    }
+  } else if (t < A.nsm + A.nfree) {
+    const int g = A.free_atoms[t - A.nsm];
+    const double im = A.invm[g];
+    A.v[g] += fixd(A.fkick[g]) * hdt * im;
+    A.v[N + g] += fixd(A.fkick[N + g]) * hdt * im;
+    A.v[2 * N + g] += fixd(A.fkick[2 * N + g]) * hdt * im;
+  }
+}
+
+// verlet drift (src/verlet.f) + SHAKE + RATTLE of small molecules, then
+// the scaled frame, group centres (appbou) and the pair-kernel inputs of
+// their groups; free atoms drift here and get their groups in k_free_groups.
+__global__ void k_drift(const MolArgs A) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int N = A.N;
+  const double dt = A.dt;
+  if (t < A.nsm) {
+    const int4 m = A.sm[t];
+    double x[SMA][3], xo[SMA][3], v[SMA][3], im[SMA];
+#pragma unroll
+    for (int a = 0; a < SMA; a++) {
+      if (a < m.y) {
+        const int g = m.x + a;
+        im[a] = A.invm[g];
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+          const double f = A.fn ? A.fn[d * N + g] : 0.0;
+          xo[a][d] = A.x[d * N + g];
+          v[a][d] = A.v[d * N + g];
+          x[a][d] = xo[a][d] + dt * v[a][d] + f * 0.5 * dt * dt * im[a];
+          v[a][d] += f * 0.5 * dt * im[a];
+        }
+      } else {
+        im[a] = 0;
+#pragma unroll
+        for (int d = 0; d < 3; d++) x[a][d] = xo[a][d] = v[a][d] = 0.0;
+      }
+    }
+    if (m.w > 0) {
+      if (!shake_small(x, xo, v, im, A.cloc + m.z, A.dss + m.z, m.w, dt, A.tol)) atomicOr(A.flag, 1);
+      if (!rattle_small(x, v, im, A.cloc + m.z, m.w)) atomicOr(A.flag, 1);
+    }
+    double s[SMA][3];
+#pragma unroll
+    for (int a = 0; a < SMA; a++) {
+      if (a < m.y) {
+        const int g = m.x + a;
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+          A.x[d * N + g] = x[a][d];
+          A.xo[d * N + g] = xo[a][d];
+          A.v[d * N + g] = v[a][d];
+          if (A.fzero) A.fzero[d * N + g] = 0ull;
+        }
+        s[a][0] = A.o11 * x[a][0] + A.o12 * x[a][1] + A.o13 * x[a][2];
+        s[a][1] = A.o22 * x[a][1] + A.o23 * x[a][2];
+        s[a][2] = A.o33 * x[a][2];
+      }
+    }
+    const int2 gg = A.smg[t];
+    for (int gi = gg.x; gi < gg.x + gg.y; gi++) {
+      const int2 mg = A.gmeta[gi];
+      double c[3] = {0, 0, 0};
+#pragma unroll
+      for (int a = 0; a < SMA; a++) {
+        const int ga = m.x + a;
+        if (a < m.y && ga >= mg.x && ga < mg.x + (mg.y & 0xff)) {
+          const double w = A.pm[ga];
+          c[0] += w * s[a][0];
+          c[1] += w * s[a][1];
+          c[2] += w * s[a][2];
+        }
+      }
+      A.grp[gi] = c[0];
+      A.grp[A.G + gi] = c[1];
+      A.grp[2 * A.G + gi] = c[2];
+      A.gpos[gi] = make_double4(c[0], c[1], c[2], 0.0);
+#pragma unroll
+      for (int a = 0; a < SMA; a++) {
+        const int ga = m.x + a;
+        if (a < m.y && ga >= mg.x && ga < mg.x + (mg.y & 0xff)) {
+          const double dx = s[a][0] - c[0], dy = s[a][1] - c[1], dz = s[a][2] - c[2];
+          A.aoff[ga] = make_float4((float)(A.c11 * dx + A.c12 * dy + A.c13 * dz), (float)(A.c22 * dy + A.c23 * dz),
+                                   (float)(A.c33 * dz), A.q[ga]);
+        }
+      }
+    }
+  } else if (t < A.nsm + A.nfree) {
+    const int g = A.free_atoms[t - A.nsm];
+    const double im = A.invm[g];
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      const double f = A.fn ? A.fn[d * N + g] : 0.0;
+      const double xo = A.x[d * N + g];
+      A.xo[d * N + g] = xo;
+      A.x[d * N + g] = xo + dt * A.v[d * N + g] + f * 0.5 * dt * dt * im;
+      A.v[d * N + g] += f * 0.5 * dt * im;
+      if (A.fzero) A.fzero[d * N + g] = 0ull;
+    }
+  }
+}
+
+// group centres and pair-kernel inputs of groups outside small molecules
+__global__ void k_free_groups(const MolArgs A) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= A.nfreeg) return;
+  const int gi = A.free_groups[t];
+  const int N = A.N;
+  const int2 mg = A.gmeta[gi];
+  const int a0 = mg.x, n = mg.y & 0xff;
+  double c[3] = {0, 0, 0};
+  for (int a = a0; a < a0 + n; a++) {
+    const double x = A.x[a], y = A.x[N + a], z = A.x[2 * N + a];
+    const double w = A.pm[a];
+    c[0] += w * (A.o11 * x + A.o12 * y + A.o13 * z);
+    c[1] += w * (A.o22 * y + A.o23 * z);
+    c[2] += w * (A.o33 * z);
+  }
+  A.grp[gi] = c[0];
+  A.grp[A.G + gi] = c[1];
+  A.grp[2 * A.G + gi] = c[2];
+  A.gpos[gi] = make_double4(c[0], c[1], c[2], 0.0);
+  for (int a = a0; a < a0 + n; a++) {
+    const double x = A.x[a], y = A.x[N + a], z = A.x[2 * N + a];
+    const double dx = (A.o11 * x + A.o12 * y + A.o13 * z) - c[0];
+    const double dy = (A.o22 * y + A.o23 * z) - c[1];
+    const double dz = (A.o33 * z) - c[2];
+    A.aoff[a] = make_float4((float)(A.c11 * dx + A.c12 * dy + A.c13 * dz), (float)(A.c22 * dy + A.c23 * dz),
+                            (float)(A.c33 * dz), A.q[a]);
+  }
 }
 
 struct ConsArgs {
-  int nmol;             // molecules with constraints
-  const int* cstart;    // [nmol+1] into constraint arrays
-  const int2* cab;      // constraint atoms (0-based)
-  const double* dss;    // squared lengths
-  const double* invm;   // [N]
+  int nmol;           // large constrained molecules
+  const int* cstart;  // [nmol+1]
+  const int2* cab;    // constraint atoms (global)
+  const double* dss;
+  const double* invm;
   int N;
   double* x;
   const double* xo;
@@ -64,11 +482,11 @@ struct ConsArgs {
   double dt;
   double tol;
   int maxit;
-  int* flag;  // bit 0: constraint iteration did not converge
+  int* flag;
 };
 
-// SHAKE (src/rattle_verlet.f, iterative branch): one thread per molecule
-__global__ void k_shake(const ConsArgs A) {
+// iterative SHAKE (src/rattle_verlet.f SHAKE branch) for large molecules
+__global__ void k_shake_big(const ConsArgs A) {
   const int m = blockIdx.x * blockDim.x + threadIdx.x;
   if (m >= A.nmol) return;
   const int c0 = A.cstart[m], c1 = A.cstart[m + 1];
@@ -84,8 +502,7 @@ __global__ void k_shake(const ConsArgs A) {
         moved = true;
         const double rx = A.xo[a] - A.xo[b], ry = A.xo[N + a] - A.xo[N + b], rz = A.xo[2 * N + a] - A.xo[2 * N + b];
         const double ia = A.invm[a], ib = A.invm[b];
-        const double dps = dx * rx + dy * ry + dz * rz;
-        const double gg = dcnt / (dps * 2.0 * (ia + ib));
+        const double gg = dcnt / ((dx * rx + dy * ry + dz * rz) * 2.0 * (ia + ib));
         const double ga = -gg * ia, gb = gg * ib;
         A.x[a] += rx * ga;
         A.x[b] += rx * gb;
@@ -103,12 +520,11 @@ __global__ void k_shake(const ConsArgs A) {
     }
     if (!moved) return;
   }
-  atomicOr(A.flag, 1);  // ORAC: "While SHAKEing: the iteration procedure did not converge"
+  atomicOr(A.flag, 1);
 }
 
-// RATTLE velocity step (src/rattle_correc.f): remove the velocity component
-// along every constraint, one thread per molecule
-__global__ void k_rattle(const ConsArgs A) {
+// iterative RATTLE velocity step (src/rattle_correc.f) for large molecules
+__global__ void k_rattle_big(const ConsArgs A) {
   const int m = blockIdx.x * blockDim.x + threadIdx.x;
   if (m >= A.nmol) return;
   const int c0 = A.cstart[m], c1 = A.cstart[m + 1];
@@ -137,67 +553,11 @@ __global__ void k_rattle(const ConsArgs A) {
   atomicOr(A.flag, 1);
 }
 
-// Cartesian -> scaled frame (change_frame way=-1, src/change_frame.f)
-__global__ void k_scaled(int N, const double* __restrict__ x, double o11, double o12, double o13, double o22,
-                         double o23, double o33, double* __restrict__ s) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= N) return;
-  const double a = x[t], b = x[N + t], c = x[2 * N + t];
-  s[t] = o11 * a + o12 * b + o13 * c;
-  s[N + t] = o22 * b + o23 * c;
-  s[2 * N + t] = o33 * c;
-}
-
-// appbou (src/appbou.f:57-69) on scaled coordinates
-__global__ void k_gcom(int G, int N, const int2* __restrict__ gmeta, const double* __restrict__ pm,
-                       const double* __restrict__ s, double* __restrict__ grp) {
-  const int g = blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= G) return;
-  const int2 mg = gmeta[g];
-  const int a0 = mg.x, n = mg.y & 0xff;
-  double sx = 0, sy = 0, sz = 0;
-  for (int a = a0; a < a0 + n; a++) {
-    sx += pm[a] * s[a];
-    sy += pm[a] * s[N + a];
-    sz += pm[a] * s[2 * N + a];
-  }
-  grp[g] = sx;
-  grp[G + g] = sy;
-  grp[2 * G + g] = sz;
-}
-
-// molecule centres of mass (scaled), one warp per molecule
-__global__ void k_mcom(int P, int N, const int* __restrict__ mstart, const double* __restrict__ mass,
-                       const double* __restrict__ s, double* __restrict__ mol) {
-  const int lane = threadIdx.x & 31;
-  const int m = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  if (m >= P) return;
-  double sx = 0, sy = 0, sz = 0, mt = 0;
-  for (int a = mstart[m] + lane; a < mstart[m + 1]; a += 32) {
-    const double w = mass[a];
-    sx += w * s[a];
-    sy += w * s[N + a];
-    sz += w * s[2 * N + a];
-    mt += w;
-  }
-  for (int o = 16; o > 0; o >>= 1) {
-    sx += __shfl_xor_sync(0xffffffffu, sx, o);
-    sy += __shfl_xor_sync(0xffffffffu, sy, o);
-    sz += __shfl_xor_sync(0xffffffffu, sz, o);
-    mt += __shfl_xor_sync(0xffffffffu, mt, o);
-  }
-  if (lane == 0) {
-    mol[m] = sx / mt;
-    mol[P + m] = sy / mt;
-    mol[2 * P + m] = sz / mt;
-  }
-}
-
-__global__ void k_ekin(int N, const double* __restrict__ v, const double* __restrict__ mass, double* __restrict__ out) {
+__global__ void k_ekin(int N, const double* __restrict__ v, const double* __restrict__ invm, double* __restrict__ out) {
   __shared__ double s[8];
   double e = 0;
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < N; t += gridDim.x * blockDim.x)
-    e += 0.5 * mass[t] * (v[t] * v[t] + v[N + t] * v[N + t] + v[2 * N + t] * v[2 * N + t]);
+    e += 0.5 / invm[t] * (v[t] * v[t] + v[N + t] * v[N + t] + v[2 * N + t] * v[2 * N + t]);
   for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(0xffffffffu, e, o);
   if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = e;
   __syncthreads();
@@ -215,32 +575,37 @@ __global__ void k_ekin(int N, const double* __restrict__ v, const double* __rest
 struct MdState {
   bool ready = false;
   int N = 0;
-  double* x = nullptr;   // [3N] Cartesian
+  double* x = nullptr;  // [3N] Cartesian
   double* v = nullptr;
   double* xo = nullptr;
-  double* fh = nullptr;
-  double* fl = nullptr;
-  double* fm = nullptr;
-  double* fn = nullptr;  // intramolecular (N0/N1) forces, zero without bonded terms
-  double* invm3 = nullptr;
-  double* mass = nullptr;
-  double* pmass = nullptr;
-  int* mstart = nullptr;
-  // constraints
-  int nmolc = 0, ncons = 0;
-  int* cstart = nullptr;
-  int2* cab = nullptr;
-  double* dss = nullptr;
+  unsigned long long* ffix[3] = {nullptr, nullptr, nullptr};  // H, L, M accumulators
+  double* fn = nullptr;   // intramolecular (N0/N1) forces; null without bonded terms
+  double* invm = nullptr;
+  double* pm = nullptr;
+  // small constrained molecules
+  int nsm = 0;
+  int4* sm = nullptr;
+  int2* smg = nullptr;
+  int2* cloc = nullptr;
+  double* cdss = nullptr;
+  // free atoms and groups
+  int nfree = 0, nfreeg = 0;
+  int* free_atoms = nullptr;
+  int* free_groups = nullptr;
+  // large constrained molecules
+  int nbig = 0;
+  int* bstart = nullptr;
+  int2* bcab = nullptr;
+  double* bdss = nullptr;
   // energies: [0..7] M, [8..15] L, [16..23] H (ORAC order), [24..39] SPME eout, [40] ekin
   double* e = nullptr;
-  double* stress = nullptr;  // [3*9] scratch
   int* flag = nullptr;
   // schedule
   double dth = 0;
   int lrespa = 1, mrespa = 1, n1respa = 1, n0respa = 1, nupdte = 1;
   char rshk = 'l';
   long long step = 0;
-  double econst = 0;  // self energy + constant corrections (host)
+  double econst = 0;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t gexec = nullptr;
   cudaGraph_t graph_u = nullptr;  // step with list update
@@ -263,33 +628,67 @@ void md_destroy(orac_gpu_ctx* ctx) {
   if (S->graph) cudaGraphDestroy(S->graph);
   if (S->gexec_u) cudaGraphExecDestroy(S->gexec_u);
   if (S->graph_u) cudaGraphDestroy(S->graph_u);
-  void* ptrs[] = {S->x,    S->v,      S->xo,     S->fh,     S->fl,     S->fm,    S->fn,  S->invm3, S->mass,
-                  S->pmass, S->mstart, S->cstart, S->cab, S->dss, S->e, S->stress, S->flag};
+  void* ptrs[] = {S->x,         S->v,        S->xo,          S->ffix[0],   S->ffix[1], S->ffix[2], S->fn,
+                  S->invm,      S->pm,       S->sm,          S->smg,       S->cloc,    S->cdss,    S->free_atoms,
+                  S->free_groups, S->bstart, S->bcab,        S->bdss,      S->e,       S->flag};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   delete S;
   ctx->md = nullptr;
 }
 
-static int md_coords(orac_gpu_ctx* ctx, MdState& S) {
-  const int N = ctx->N, G = ctx->G, P = ctx->P;
+static MolArgs mol_args(orac_gpu_ctx* ctx, MdState& S, double dt) {
+  MolArgs A;
+  memset(&A, 0, sizeof(A));
+  A.N = ctx->N;
+  A.nsm = S.nsm;
+  A.sm = S.sm;
+  A.smg = S.smg;
+  A.cloc = S.cloc;
+  A.dss = S.cdss;
+  A.nfree = S.nfree;
+  A.free_atoms = S.free_atoms;
+  A.nfreeg = S.nfreeg;
+  A.free_groups = S.free_groups;
+  A.x = S.x;
+  A.xo = S.xo;
+  A.v = S.v;
+  A.invm = S.invm;
+  A.pm = S.pm;
+  A.q = ctx->d_aq;
+  A.gmeta = ctx->d_gmeta;
   const double* o = ctx->oc;
-  k_scaled<<<(N + 255) / 256, 256, 0, ctx->stream>>>(N, S.x, o[0], o[3], o[6], o[4], o[7], o[8], ctx->d_xyz);
-  CKL();
-  k_gcom<<<(G + 255) / 256, 256, 0, ctx->stream>>>(G, N, ctx->d_gmeta, S.pmass, ctx->d_xyz, ctx->d_grp);
-  CKL();
-  k_mcom<<<(P + 7) / 8, 256, 0, ctx->stream>>>(P, N, S.mstart, S.mass, ctx->d_xyz, ctx->d_mol);
-  CKL();
-  return ORAC_OK;
+  const double* c = ctx->co;
+  A.o11 = o[0];
+  A.o12 = o[3];
+  A.o13 = o[6];
+  A.o22 = o[4];
+  A.o23 = o[7];
+  A.o33 = o[8];
+  A.c11 = c[0];
+  A.c12 = c[3];
+  A.c13 = c[6];
+  A.c22 = c[4];
+  A.c23 = c[7];
+  A.c33 = c[8];
+  A.G = ctx->G;
+  A.grp = ctx->d_grp;
+  A.gpos = ctx->d_gpos;
+  A.aoff = ctx->d_aoff;
+  A.fn = S.fn;
+  A.dt = dt;
+  A.tol = 1e-12;
+  A.flag = S.flag;
+  return A;
 }
 
-static ConsArgs cons_args(orac_gpu_ctx* ctx, MdState& S, double dt, double tol) {
+static ConsArgs big_args(orac_gpu_ctx* ctx, MdState& S, double dt, double tol) {
   ConsArgs A;
-  A.nmol = S.nmolc;
-  A.cstart = S.cstart;
-  A.cab = S.cab;
-  A.dss = S.dss;
-  A.invm = S.invm3;
+  A.nmol = S.nbig;
+  A.cstart = S.bstart;
+  A.cab = S.bcab;
+  A.dss = S.bdss;
+  A.invm = S.invm;
   A.N = ctx->N;
   A.x = S.x;
   A.xo = S.xo;
@@ -301,24 +700,61 @@ static ConsArgs cons_args(orac_gpu_ctx* ctx, MdState& S, double dt, double tol) 
   return A;
 }
 
-static int md_kick(orac_gpu_ctx* ctx, MdState& S, const double* f, double dt) {
-  const int n3 = 3 * ctx->N;
-  k_kick<<<(n3 + 255) / 256, 256, 0, ctx->stream>>>(n3, ctx->N, S.v, f, S.invm3, 0.5 * dt);
+static int md_kick(orac_gpu_ctx* ctx, MdState& S, int lvl, double dt) {
+  MolArgs A = mol_args(ctx, S, dt);
+  A.fkick = S.ffix[lvl];
+  const int n = S.nsm + S.nfree;
+  k_kick<<<(n + 127) / 128, 128, 0, ctx->stream>>>(A);
   CKL();
-  if (S.nmolc) {
-    k_rattle<<<(S.nmolc + 127) / 128, 128, 0, ctx->stream>>>(cons_args(ctx, S, dt, 1e-12));
+  if (S.nbig) {
+    k_rattle_big<<<(S.nbig + 127) / 128, 128, 0, ctx->stream>>>(big_args(ctx, S, dt, 1e-12));
     CKL();
   }
   return ORAC_OK;
 }
 
-static int md_forces_shell(orac_gpu_ctx* ctx, MdState& S, char sh, double* f, double* e, bool energy) {
-  CK(cudaMemsetAsync(f, 0, sizeof(double) * 3 * ctx->N, ctx->stream));
-  if (int rc = shell_run(ctx, sh, ctx->d_xyz, ctx->d_grp, ctx->d_mol, f, energy ? e : nullptr, S.stress, energy ? 1 : 0))
-    return rc;
-  if (ctx->clewld && S.rshk == sh)
-    if (int rc = fft_pme_device(ctx, ctx->d_xyz, ctx->d_mol, f, S.e + 24)) return rc;
+// drift + constraints + scaled frame + pair-kernel inputs; zeroes `fzero`
+static int md_drift(orac_gpu_ctx* ctx, MdState& S, double dt, unsigned long long* fzero) {
+  MolArgs A = mol_args(ctx, S, dt);
+  A.fzero = fzero;
+  const int n = S.nsm + S.nfree;
+  k_drift<<<(n + 127) / 128, 128, 0, ctx->stream>>>(A);
+  CKL();
+  if (S.nbig) {
+    k_shake_big<<<(S.nbig + 127) / 128, 128, 0, ctx->stream>>>(big_args(ctx, S, dt, 1e-8));
+    CKL();
+    k_rattle_big<<<(S.nbig + 127) / 128, 128, 0, ctx->stream>>>(big_args(ctx, S, dt, 1e-12));
+    CKL();
+  }
+  if (S.nfreeg) {
+    k_free_groups<<<(S.nfreeg + 127) / 128, 128, 0, ctx->stream>>>(A);
+    CKL();
+  }
   return ORAC_OK;
+}
+
+// one shell's forces into the level accumulator (already zeroed or zeroed here)
+static int md_forces_shell(orac_gpu_ctx* ctx, MdState& S, char sh, int lvl, bool zero, double* e, bool energy) {
+  unsigned long long* f = S.ffix[lvl];
+  if (zero) CK(cudaMemsetAsync(f, 0, sizeof(unsigned long long) * 3 * ctx->N, ctx->stream));
+  const int flags = SH_PREPPED | SH_FIXED_OUT | (energy ? SH_ENERGY : 0);
+  if (int rc = shell_run_r(ctx, sh, ctx->sh, ctx->d_xyz, ctx->d_grp, ctx->d_mol, reinterpret_cast<double*>(f),
+                           energy ? e : nullptr, nullptr, flags))
+    return rc;
+  if (ctx->clewld && S.rshk == sh) {
+    double recip[9];
+    for (int i = 0; i < 3; i++)
+      for (int j = 0; j < 3; j++) recip[i + 3 * j] = 0.5 * ctx->oc[j + 3 * i];  // src/fft_pme.f:47-51
+    if (int rc = pme_run(ctx, ctx->N, S.x, ctx->d_aqd, recip, ctx->volume, ctx->alphal, nullptr, S.e + 24, nullptr,
+                         nullptr, f))
+      return rc;
+  }
+  return ORAC_OK;
+}
+
+static int md_phony(orac_gpu_ctx* ctx, const ShellRadii& r, char sh) {
+  return shell_run_r(ctx, sh, r, ctx->d_xyz, ctx->d_grp, ctx->d_mol, nullptr, nullptr, nullptr,
+                     SH_PREPPED | SH_FIXED_OUT);
 }
 
 static int md_list_update(orac_gpu_ctx* ctx, MdState& S) {
@@ -327,57 +763,52 @@ static int md_list_update(orac_gpu_ctx* ctx, MdState& S) {
   ShellRadii r1 = r;
   r1.rcuth = r.rcutl;
   r1.rtolh = 0.0;
-  if (int rc = shell_run_r(ctx, 'h', r1, ctx->d_xyz, ctx->d_grp, ctx->d_mol, S.fn, nullptr, S.stress, 0)) return rc;
+  if (int rc = md_phony(ctx, r1, 'h')) return rc;
   ShellRadii r2 = r1;
   r2.rcutl = r.rcutm;
   r2.rtoll = 0.0;
-  return shell_run_r(ctx, 'l', r2, ctx->d_xyz, ctx->d_grp, ctx->d_mol, S.fn, nullptr, S.stress, 0);
+  return md_phony(ctx, r2, 'l');
 }
+
+enum { LH = 0, LL = 1, LM = 2 };
 
 // one outer step; energies of the last evaluations when `energy`
 static int md_step(orac_gpu_ctx* ctx, MdState& S, bool update, bool energy) {
-  const int n3 = 3 * ctx->N;
   if (update)
     if (int rc = md_list_update(ctx, S)) return rc;
-  if (int rc = md_kick(ctx, S, S.fh, S.dth)) return rc;
+  if (int rc = md_kick(ctx, S, LH, S.dth)) return rc;
   const double tl = S.dth / S.lrespa;
   const double tm = tl / S.mrespa;
   for (int il = 0; il < S.lrespa; il++) {
-    if (int rc = md_kick(ctx, S, S.fl, tl)) return rc;
+    if (int rc = md_kick(ctx, S, LL, tl)) return rc;
     for (int im = 0; im < S.mrespa; im++) {
-      if (int rc = md_kick(ctx, S, S.fm, tm)) return rc;
+      if (int rc = md_kick(ctx, S, LM, tm)) return rc;
       // intramolecular levels: with no N0/N1 forces the n1respa*n0respa
       // verlet steps compose into one drift of tm
-      k_verlet<<<(n3 + 255) / 256, 256, 0, ctx->stream>>>(n3, ctx->N, S.x, S.v, S.fn, S.invm3, tm, S.xo);
-      CKL();
-      if (S.nmolc) {
-        k_shake<<<(S.nmolc + 127) / 128, 128, 0, ctx->stream>>>(cons_args(ctx, S, tm, 1e-8));
-        CKL();
-        k_rattle<<<(S.nmolc + 127) / 128, 128, 0, ctx->stream>>>(cons_args(ctx, S, tm, 1e-12));
-        CKL();
-      }
-      if (int rc = md_coords(ctx, S)) return rc;
+      if (int rc = md_drift(ctx, S, tm, S.ffix[LM])) return rc;
       const bool last = energy && il == S.lrespa - 1 && im == S.mrespa - 1;
-      if (int rc = md_forces_shell(ctx, S, 'm', S.fm, S.e, last)) return rc;
-      if (int rc = md_kick(ctx, S, S.fm, tm)) return rc;
+      if (int rc = md_forces_shell(ctx, S, 'm', LM, false, S.e, last)) return rc;
+      if (int rc = md_kick(ctx, S, LM, tm)) return rc;
     }
-    if (int rc = md_forces_shell(ctx, S, 'l', S.fl, S.e + 8, energy && il == S.lrespa - 1)) return rc;
-    if (int rc = md_kick(ctx, S, S.fl, tl)) return rc;
+    if (int rc = md_forces_shell(ctx, S, 'l', LL, true, S.e + 8, energy && il == S.lrespa - 1)) return rc;
+    if (int rc = md_kick(ctx, S, LL, tl)) return rc;
   }
-  if (int rc = md_forces_shell(ctx, S, 'h', S.fh, S.e + 16, energy)) return rc;
+  if (int rc = md_forces_shell(ctx, S, 'h', LH, true, S.e + 16, energy)) return rc;
   {
     ShellRadii r = ctx->sh;
     r.rcutl = r.rcutm;
-    if (int rc = shell_run_r(ctx, 'l', r, ctx->d_xyz, ctx->d_grp, ctx->d_mol, S.fn, nullptr, S.stress, 0)) return rc;
+    if (int rc = md_phony(ctx, r, 'l')) return rc;
   }
-  if (int rc = md_kick(ctx, S, S.fh, S.dth)) return rc;
+  if (int rc = md_kick(ctx, S, LH, S.dth)) return rc;
   if (energy) {
     CK(cudaMemsetAsync(S.e + 40, 0, sizeof(double), ctx->stream));
-    k_ekin<<<64, 256, 0, ctx->stream>>>(ctx->N, S.v, S.mass, S.e + 40);
+    k_ekin<<<64, 256, 0, ctx->stream>>>(ctx->N, S.v, S.invm, S.e + 40);
     CKL();
   }
   return ORAC_OK;
 }
+
+static int md_run_impl(orac_gpu_ctx* ctx, int nsteps, int energy_every, double* rec, bool async);
 
 extern "C" {
 
@@ -391,44 +822,44 @@ int orac_gpu_md_setup(orac_gpu_ctx* ctx, const double* x, const double* y, const
   if (dt_h <= 0 || lrespa < 1 || mrespa < 1 || n1respa < 1 || n0respa < 1 || nupdte < 1)
     return ctx_fail(ctx, ORAC_ERR_PARAM, "bad r-RESPA schedule");
   CK(cudaSetDevice(ctx->device));
+  md_destroy(ctx);
   MdState& S = *md_of(ctx);
-  const int N = ctx->N, P = ctx->P;
+  const int N = ctx->N, P = ctx->P, G = ctx->G;
   S.N = N;
   if (dev_alloc(ctx, &S.x, 3 * (size_t)N) || dev_alloc(ctx, &S.v, 3 * (size_t)N) ||
-      dev_alloc(ctx, &S.xo, 3 * (size_t)N) || dev_alloc(ctx, &S.fh, 3 * (size_t)N) ||
-      dev_alloc(ctx, &S.fl, 3 * (size_t)N) || dev_alloc(ctx, &S.fm, 3 * (size_t)N) ||
-      dev_alloc(ctx, &S.fn, 3 * (size_t)N) || dev_alloc(ctx, &S.invm3, N) || dev_alloc(ctx, &S.mass, N) ||
-      dev_alloc(ctx, &S.pmass, N) || dev_alloc(ctx, &S.mstart, P + 1) || dev_alloc(ctx, &S.e, 48) ||
-      dev_alloc(ctx, &S.stress, 32) || dev_alloc(ctx, &S.flag, 4))
+      dev_alloc(ctx, &S.xo, 3 * (size_t)N) || dev_alloc(ctx, &S.ffix[0], 3 * (size_t)N) ||
+      dev_alloc(ctx, &S.ffix[1], 3 * (size_t)N) || dev_alloc(ctx, &S.ffix[2], 3 * (size_t)N) ||
+      dev_alloc(ctx, &S.invm, N) || dev_alloc(ctx, &S.pm, N) || dev_alloc(ctx, &S.e, 48) ||
+      dev_alloc(ctx, &S.flag, 4))
     return ORAC_ERR_CUDA;
-  std::vector<double> h(3 * (size_t)N);
-  memcpy(h.data(), x, sizeof(double) * N);
-  memcpy(h.data() + N, y, sizeof(double) * N);
-  memcpy(h.data() + 2 * (size_t)N, z, sizeof(double) * N);
-  CK(cudaMemcpy(S.x, h.data(), sizeof(double) * 3 * N, cudaMemcpyHostToDevice));
-  memcpy(h.data(), vx, sizeof(double) * N);
-  memcpy(h.data() + N, vy, sizeof(double) * N);
-  memcpy(h.data() + 2 * (size_t)N, vz, sizeof(double) * N);
-  CK(cudaMemcpy(S.v, h.data(), sizeof(double) * 3 * N, cudaMemcpyHostToDevice));
+  const double* src[2][3] = {{x, y, z}, {vx, vy, vz}};
+  double* dst[2] = {S.x, S.v};
+  for (int k = 0; k < 2; k++)
+    for (int d = 0; d < 3; d++)
+      CK(cudaMemcpy(dst[k] + (size_t)d * N, src[k][d], sizeof(double) * N, cudaMemcpyHostToDevice));
   std::vector<double> im(N), pm(N);
   for (int a = 0; a < N; a++) im[a] = 1.0 / ctx->h_mass[a];
-  CK(cudaMemcpy(S.invm3, im.data(), sizeof(double) * N, cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(S.mass, ctx->h_mass.data(), sizeof(double) * N, cudaMemcpyHostToDevice));
-  // mass fractions of atoms in their groups (ORAC pmass) and molecule ranges
-  for (int g = 0; g < ctx->G; g++) {
+  for (int g = 0; g < G; g++) {
     double mt = 0;
     for (int a = ctx->h_gfirst[g]; a < ctx->h_gfirst[g] + ctx->h_gn[g]; a++) mt += ctx->h_mass[a];
     for (int a = ctx->h_gfirst[g]; a < ctx->h_gfirst[g] + ctx->h_gn[g]; a++) pm[a] = ctx->h_mass[a] / mt;
   }
-  CK(cudaMemcpy(S.pmass, pm.data(), sizeof(double) * N, cudaMemcpyHostToDevice));
-  std::vector<int> ms(P + 1, 0);
-  for (int a = 0; a < N; a++) ms[ctx->h_amol[a] + 1] = a + 1;
-  for (int p = 1; p <= P; p++)
-    if (ms[p] < ms[p - 1]) ms[p] = ms[p - 1];
-  for (int a = 1; a < N; a++)
-    if (ctx->h_amol[a] < ctx->h_amol[a - 1]) return ctx_fail(ctx, ORAC_ERR_PARAM, "molecules must be contiguous");
-  CK(cudaMemcpy(S.mstart, ms.data(), sizeof(int) * (P + 1), cudaMemcpyHostToDevice));
-  // constraints grouped by molecule
+  CK(cudaMemcpy(S.invm, im.data(), sizeof(double) * N, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(S.pm, pm.data(), sizeof(double) * N, cudaMemcpyHostToDevice));
+  // molecule atom ranges (contiguous) and group ranges
+  std::vector<int> ma0(P, -1), mna(P, 0), mg0(P, -1), mng(P, 0);
+  for (int a = 0; a < N; a++) {
+    const int p = ctx->h_amol[a];
+    if (a > 0 && ctx->h_amol[a] < ctx->h_amol[a - 1])
+      return ctx_fail(ctx, ORAC_ERR_PARAM, "molecules must be contiguous");
+    if (ma0[p] < 0) ma0[p] = a;
+    mna[p]++;
+  }
+  for (int g = 0; g < G; g++) {
+    const int p = ctx->h_gmol[g];
+    if (mg0[p] < 0) mg0[p] = g;
+    mng[p]++;
+  }
   std::vector<std::vector<int>> bym(P);
   for (int k = 0; k < ncnst; k++) {
     const int a = cnst[2 * k] - 1, b = cnst[2 * k + 1] - 1;
@@ -436,26 +867,54 @@ int orac_gpu_md_setup(orac_gpu_ctx* ctx, const double* x, const double* y, const
       return ctx_fail(ctx, ORAC_ERR_PARAM, "constraint %d", k + 1);
     bym[ctx->h_amol[a]].push_back(k);
   }
-  std::vector<int> cs = {0};
-  std::vector<int2> cab;
-  std::vector<double> cd;
+  std::vector<int4> sm;
+  std::vector<int2> smg, cloc, bcab;
+  std::vector<double> cd, bd;
+  std::vector<int> bst = {0}, fa, fg;
+  std::vector<char> small(P, 0);
   for (int p = 0; p < P; p++) {
-    if (bym[p].empty()) continue;
-    for (int k : bym[p]) {
-      cab.push_back(make_int2(cnst[2 * k] - 1, cnst[2 * k + 1] - 1));
-      cd.push_back(dss[k]);
+    const int nc = (int)bym[p].size();
+    if (nc > 0 && nc <= SMC && mna[p] <= SMA) {
+      small[p] = 1;
+      sm.push_back(make_int4(ma0[p], mna[p], (int)cloc.size(), nc));
+      smg.push_back(make_int2(mg0[p], mng[p]));
+      for (int k : bym[p]) {
+        cloc.push_back(make_int2(cnst[2 * k] - 1 - ma0[p], cnst[2 * k + 1] - 1 - ma0[p]));
+        cd.push_back(dss[k]);
+      }
+    } else if (nc > 0) {
+      for (int k : bym[p]) {
+        bcab.push_back(make_int2(cnst[2 * k] - 1, cnst[2 * k + 1] - 1));
+        bd.push_back(dss[k]);
+      }
+      bst.push_back((int)bcab.size());
     }
-    cs.push_back((int)cab.size());
   }
-  S.nmolc = (int)cs.size() - 1;
-  S.ncons = (int)cab.size();
-  if (S.nmolc) {
-    if (dev_alloc(ctx, &S.cstart, cs.size()) || dev_alloc(ctx, &S.cab, cab.size()) || dev_alloc(ctx, &S.dss, cd.size()))
-      return ORAC_ERR_CUDA;
-    CK(cudaMemcpy(S.cstart, cs.data(), sizeof(int) * cs.size(), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(S.cab, cab.data(), sizeof(int2) * cab.size(), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(S.dss, cd.data(), sizeof(double) * cd.size(), cudaMemcpyHostToDevice));
+  for (int a = 0; a < N; a++)
+    if (!small[ctx->h_amol[a]]) fa.push_back(a);
+  for (int g = 0; g < G; g++)
+    if (!small[ctx->h_gmol[g]]) fg.push_back(g);
+  S.nsm = (int)sm.size();
+  S.nfree = (int)fa.size();
+  S.nfreeg = (int)fg.size();
+  S.nbig = (int)bst.size() - 1;
+#define UPV(dst, vec)                                                                                        \
+  if (!vec.empty()) {                                                                                        \
+    if (dev_alloc(ctx, &dst, vec.size())) return ORAC_ERR_CUDA;                                            \
+    CK(cudaMemcpy(dst, vec.data(), sizeof(vec[0]) * vec.size(), cudaMemcpyHostToDevice));                  \
   }
+  UPV(S.sm, sm);
+  UPV(S.smg, smg);
+  UPV(S.cloc, cloc);
+  UPV(S.cdss, cd);
+  UPV(S.free_atoms, fa);
+  UPV(S.free_groups, fg);
+  if (S.nbig) {
+    UPV(S.bstart, bst);
+    UPV(S.bcab, bcab);
+    UPV(S.bdss, bd);
+  }
+#undef UPV
   S.dth = dt_h;
   S.lrespa = lrespa;
   S.mrespa = mrespa;
@@ -466,25 +925,19 @@ int orac_gpu_md_setup(orac_gpu_ctx* ctx, const double* x, const double* y, const
   S.econst = econst;
   S.step = 0;
   CK(cudaMemset(S.flag, 0, sizeof(int)));
-  CK(cudaMemset(S.fn, 0, sizeof(double) * 3 * N));
-  if (S.gexec) cudaGraphExecDestroy(S.gexec);
-  if (S.graph) cudaGraphDestroy(S.graph);
-  if (S.gexec_u) cudaGraphExecDestroy(S.gexec_u);
-  if (S.graph_u) cudaGraphDestroy(S.graph_u);
-  S.gexec = S.gexec_u = nullptr;
-  S.graph = S.graph_u = nullptr;
-  // first list build with host synchronisation (sizes the list capacity with
-  // headroom for the run), then the first forces (src/mtsmd.f:1986-2152)
-  if (int rc = md_coords(ctx, S)) return rc;
+  // positions -> scaled frame, group centres, pair-kernel inputs (a drift of
+  // zero length); then the first list build with host synchronisation (it
+  // sizes the list capacity with 30% headroom for in-graph rebuilds) and the
+  // first forces (src/mtsmd.f:1986-2152)
+  if (int rc = md_drift(ctx, S, 0.0, nullptr)) return rc;
   const ShellRadii r = ctx->sh;
-  if (int rc = list_prepare_stencil(ctx, r.rcuth + r.rtolh + r.rneih)) return rc;
-  if (int rc = list_build_cells(ctx, r.rcuth + r.rtolh + r.rneih, &ctx->lists[0])) return rc;
+  const double rc_h = r.rcuth + r.rtolh + r.rneih;
+  if (int rc = list_prepare_stencil(ctx, rc_h)) return rc;
+  if (int rc = list_build_cells(ctx, rc_h, &ctx->lists[0])) return rc;
   {
-    // reserve 30% headroom so in-graph rebuilds do not overflow
     GList& H = ctx->lists[0];
     const int64_t want = H.npairs + H.npairs * 3 / 10 + 4096;
     if (H.cap < want) {
-      std::vector<int> cnt(ctx->G);
       if (dev_alloc(ctx, &H.j, want) || dev_alloc(ctx, &H.mask, want)) return ORAC_ERR_CUDA;
       H.cap = want;
       for (int q = 1; q < 3; q++) {
@@ -492,25 +945,31 @@ int orac_gpu_md_setup(orac_gpu_ctx* ctx, const double* x, const double* y, const
         if (dev_alloc(ctx, &L.j, want) || dev_alloc(ctx, &L.mask, want)) return ORAC_ERR_CUDA;
         L.cap = want;
       }
-      if (int rc = list_build_cells(ctx, r.rcuth + r.rtolh + r.rneih, &ctx->lists[0])) return rc;
+      if (int rc = list_build_cells(ctx, rc_h, &ctx->lists[0])) return rc;
     }
   }
-  if (int rc = md_list_update(ctx, S)) return rc;
-  if (int rc = md_forces_shell(ctx, S, 'm', S.fm, S.e, true)) return rc;
-  if (int rc = md_forces_shell(ctx, S, 'l', S.fl, S.e + 8, true)) return rc;
-  if (int rc = md_forces_shell(ctx, S, 'h', S.fh, S.e + 16, true)) return rc;
+  {
+    ShellRadii r1 = r;
+    r1.rcuth = r.rcutl;
+    r1.rtolh = 0.0;
+    if (int rc = md_phony(ctx, r1, 'h')) return rc;
+    ShellRadii r2 = r1;
+    r2.rcutl = r.rcutm;
+    r2.rtoll = 0.0;
+    if (int rc = md_phony(ctx, r2, 'l')) return rc;
+  }
+  if (int rc = md_forces_shell(ctx, S, 'm', LM, true, S.e, true)) return rc;
+  if (int rc = md_forces_shell(ctx, S, 'l', LL, true, S.e + 8, true)) return rc;
+  if (int rc = md_forces_shell(ctx, S, 'h', LH, true, S.e + 16, true)) return rc;
   {
     ShellRadii rr = ctx->sh;
     rr.rcutl = rr.rcutm;
-    if (int rc = shell_run_r(ctx, 'l', rr, ctx->d_xyz, ctx->d_grp, ctx->d_mol, S.fn, nullptr, S.stress, 0)) return rc;
-    CK(cudaMemsetAsync(S.fn, 0, sizeof(double) * 3 * N, ctx->stream));
+    if (int rc = md_phony(ctx, rr, 'l')) return rc;
   }
   CK(cudaStreamSynchronize(ctx->stream));
   S.ready = true;
   return ORAC_OK;
 }
-
-static int md_run_impl(orac_gpu_ctx* ctx, int nsteps, int energy_every, double* rec, bool async);
 
 // Run nsteps outer steps.  Every `energy_every` steps (0: never) one record
 // of NE = 12 doubles is written to rec (host): step, ekin, U_M (LJ, Coul),
@@ -534,10 +993,42 @@ int orac_gpu_md_collect(orac_gpu_ctx* ctx) {
   S.last_kind = -1;
   int flag = 0;
   CK(cudaMemcpy(&flag, S.flag, sizeof(int), cudaMemcpyDeviceToHost));
-  if (flag & 1) return ctx_fail(ctx, ORAC_ERR_CAPACITY, "SHAKE/RATTLE did not converge in 5000 iterations");
+  if (flag & 1) return ctx_fail(ctx, ORAC_ERR_CAPACITY, "SHAKE/RATTLE did not converge");
   if (flag & 2) return ctx_fail(ctx, ORAC_ERR_CAPACITY, "neighbour list capacity exceeded during the run");
   return ORAC_OK;
 }
+
+int orac_gpu_md_get_state(orac_gpu_ctx* ctx, double* x, double* y, double* z, double* vx, double* vy, double* vz) {
+  if (!ctx) return ORAC_ERR_PARAM;
+  MdState& S = *md_of(ctx);
+  if (!S.ready) return ctx_fail(ctx, ORAC_ERR_STATE, "md_setup not called");
+  const size_t n = (size_t)ctx->N * sizeof(double);
+  double* dst[6] = {x, y, z, vx, vy, vz};
+  const double* src[6] = {S.x, S.x + ctx->N, S.x + 2 * (size_t)ctx->N, S.v, S.v + ctx->N, S.v + 2 * (size_t)ctx->N};
+  for (int k = 0; k < 6; k++) CK(cudaMemcpyAsync(dst[k], src[k], n, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return ORAC_OK;
+}
+
+int orac_gpu_md_set_state(orac_gpu_ctx* ctx, const double* x, const double* y, const double* z, const double* vx,
+                          const double* vy, const double* vz) {
+  if (!ctx) return ORAC_ERR_PARAM;
+  MdState& S = *md_of(ctx);
+  if (!S.ready) return ctx_fail(ctx, ORAC_ERR_STATE, "md_setup not called");
+  const size_t n = (size_t)ctx->N * sizeof(double);
+  const double* src[6] = {x, y, z, vx, vy, vz};
+  double* dst[6] = {S.x, S.x + ctx->N, S.x + 2 * (size_t)ctx->N, S.v, S.v + ctx->N, S.v + 2 * (size_t)ctx->N};
+  for (int k = 0; k < 6; k++) CK(cudaMemcpyAsync(dst[k], src[k], n, cudaMemcpyHostToDevice, ctx->stream));
+  return ORAC_OK;
+}
+
+int orac_gpu_md_set_graphs(orac_gpu_ctx* ctx, int on) {
+  if (!ctx) return ORAC_ERR_PARAM;
+  md_of(ctx)->use_graph = on != 0;
+  return ORAC_OK;
+}
+
+}  // extern "C"
 
 static int md_run_impl(orac_gpu_ctx* ctx, int nsteps, int energy_every, double* rec, bool async) {
   if (!ctx) return ORAC_ERR_PARAM;
@@ -596,8 +1087,8 @@ static int md_run_impl(orac_gpu_ctx* ctx, int nsteps, int energy_every, double* 
       double* r = rec + 12 * (size_t)nrec++;
       r[0] = (double)S.step;
       r[1] = e[40];
-      r[2] = e[4] + e[0] + e[6];   // M: ucnp + ucns + ucnsp
-      r[3] = e[5] + e[1] + e[7];   // M: ucop + ucos + ucosp
+      r[2] = e[4] + e[0] + e[6];  // M: ucnp + ucns + ucnsp
+      r[3] = e[5] + e[1] + e[7];  // M: ucop + ucos + ucosp
       r[4] = e[12] + e[8] + e[14];
       r[5] = e[13] + e[9] + e[15];
       r[6] = e[20] + e[16] + e[22];
@@ -612,39 +1103,7 @@ static int md_run_impl(orac_gpu_ctx* ctx, int nsteps, int energy_every, double* 
   int flag = 0;
   CK(cudaMemcpyAsync(&flag, S.flag, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
-  if (flag & 1) return ctx_fail(ctx, ORAC_ERR_CAPACITY, "SHAKE/RATTLE did not converge in 5000 iterations");
+  if (flag & 1) return ctx_fail(ctx, ORAC_ERR_CAPACITY, "SHAKE/RATTLE did not converge");
   if (flag & 2) return ctx_fail(ctx, ORAC_ERR_CAPACITY, "neighbour list capacity exceeded during the run");
   return ORAC_OK;
 }
-
-int orac_gpu_md_get_state(orac_gpu_ctx* ctx, double* x, double* y, double* z, double* vx, double* vy, double* vz) {
-  if (!ctx) return ORAC_ERR_PARAM;
-  MdState& S = *md_of(ctx);
-  if (!S.ready) return ctx_fail(ctx, ORAC_ERR_STATE, "md_setup not called");
-  const size_t n = (size_t)ctx->N * sizeof(double);
-  double* dst[6] = {x, y, z, vx, vy, vz};
-  const double* src[6] = {S.x, S.x + ctx->N, S.x + 2 * (size_t)ctx->N, S.v, S.v + ctx->N, S.v + 2 * (size_t)ctx->N};
-  for (int k = 0; k < 6; k++) CK(cudaMemcpyAsync(dst[k], src[k], n, cudaMemcpyDeviceToHost, ctx->stream));
-  CK(cudaStreamSynchronize(ctx->stream));
-  return ORAC_OK;
-}
-
-int orac_gpu_md_set_state(orac_gpu_ctx* ctx, const double* x, const double* y, const double* z, const double* vx,
-                          const double* vy, const double* vz) {
-  if (!ctx) return ORAC_ERR_PARAM;
-  MdState& S = *md_of(ctx);
-  if (!S.ready) return ctx_fail(ctx, ORAC_ERR_STATE, "md_setup not called");
-  const size_t n = (size_t)ctx->N * sizeof(double);
-  const double* src[6] = {x, y, z, vx, vy, vz};
-  double* dst[6] = {S.x, S.x + ctx->N, S.x + 2 * (size_t)ctx->N, S.v, S.v + ctx->N, S.v + 2 * (size_t)ctx->N};
-  for (int k = 0; k < 6; k++) CK(cudaMemcpyAsync(dst[k], src[k], n, cudaMemcpyHostToDevice, ctx->stream));
-  return ORAC_OK;
-}
-
-int orac_gpu_md_set_graphs(orac_gpu_ctx* ctx, int on) {
-  if (!ctx) return ORAC_ERR_PARAM;
-  md_of(ctx)->use_graph = on != 0;
-  return ORAC_OK;
-}
-
-}  // extern "C"

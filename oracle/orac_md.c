@@ -151,12 +151,104 @@ static void md_kick(orc_md* M, const double* f, double dt) {
   for (int k = 0; k < 3 * N; k++) M->v[k] += f[k] * 0.5 * dt / M->mass[k % N];
 }
 
+/* Matrix-inversion constraint solve of one small molecule (<= 3 constraints),
+ * as ORAC's MIM branch (src/rattle_verlet.f:228-330): Newton iterations for
+ * the positions (shake = 1) or one exact solve for the velocities
+ * (shake = 0).  Constraint k joins atoms ca[k], cb[k] (global indices). */
+static int solve_small(int n, double A[3][3], double* b) {
+  for (int k = 0; k < n; k++) {
+    if (A[k][k] == 0.0) return 0;
+    for (int i = k + 1; i < n; i++) {
+      double f = A[i][k] / A[k][k];
+      for (int j = k; j < n; j++) A[i][j] -= f * A[k][j];
+      b[i] -= f * b[k];
+    }
+  }
+  for (int k = n - 1; k >= 0; k--) {
+    double s = b[k];
+    for (int j = k + 1; j < n; j++) s -= A[k][j] * b[j];
+    b[k] = s / A[k][k];
+  }
+  return 1;
+}
+
+static double cfac(orc_md* M, int ak, int bk, int al, int bl) {
+  double ia = 1.0 / M->mass[ak], ib = 1.0 / M->mass[bk];
+  return (ak == al ? ia : 0.0) - (ak == bl ? ia : 0.0) - (bk == al ? ib : 0.0) + (bk == bl ? ib : 0.0);
+}
+
+static int mim_molecule(orc_md* M, int c0, int nc, double dt, int shake) {
+  int N = M->ntap;
+  int ca[3], cb[3];
+  double r0[3][3], lam[3] = {0, 0, 0};
+  for (int k = 0; k < nc; k++) {
+    ca[k] = M->cnst[2 * (c0 + k)] - 1;
+    cb[k] = M->cnst[2 * (c0 + k) + 1] - 1;
+    const double* ref = shake ? M->xo : M->x;
+    for (int d = 0; d < 3; d++) r0[k][d] = ref[d * N + ca[k]] - ref[d * N + cb[k]];
+  }
+  if (!shake) { /* exact RATTLE velocity projection */
+    double A[3][3], rhs[3];
+    for (int k = 0; k < nc; k++) {
+      double vab = 0;
+      for (int d = 0; d < 3; d++) vab += r0[k][d] * (M->v[d * N + ca[k]] - M->v[d * N + cb[k]]);
+      rhs[k] = -vab;
+      for (int l = 0; l < nc; l++)
+        A[k][l] = cfac(M, ca[k], cb[k], ca[l], cb[l]) *
+                  (r0[k][0] * r0[l][0] + r0[k][1] * r0[l][1] + r0[k][2] * r0[l][2]);
+    }
+    if (!solve_small(nc, A, rhs)) return 0;
+    for (int l = 0; l < nc; l++)
+      for (int d = 0; d < 3; d++) {
+        M->v[d * N + ca[l]] += rhs[l] * r0[l][d] / M->mass[ca[l]];
+        M->v[d * N + cb[l]] -= rhs[l] * r0[l][d] / M->mass[cb[l]];
+      }
+    return 1;
+  }
+  int ok = 0;
+  for (int it = 0; it < 50; it++) {
+    double dk[3][3], g[3], gmax = 0, J[3][3];
+    for (int k = 0; k < nc; k++) {
+      for (int d = 0; d < 3; d++) dk[k][d] = M->x[d * N + ca[k]] - M->x[d * N + cb[k]];
+      g[k] = -(dk[k][0] * dk[k][0] + dk[k][1] * dk[k][1] + dk[k][2] * dk[k][2] - M->dss[c0 + k]);
+      if (fabs(g[k]) > gmax) gmax = fabs(g[k]);
+    }
+    if (gmax < 1e-12) {
+      ok = 1;
+      break;
+    }
+    for (int k = 0; k < nc; k++)
+      for (int l = 0; l < nc; l++)
+        J[k][l] = 2.0 * cfac(M, ca[k], cb[k], ca[l], cb[l]) *
+                  (dk[k][0] * r0[l][0] + dk[k][1] * r0[l][1] + dk[k][2] * r0[l][2]);
+    if (!solve_small(nc, J, g)) return 0;
+    for (int l = 0; l < nc; l++) {
+      lam[l] += g[l];
+      for (int d = 0; d < 3; d++) {
+        M->x[d * N + ca[l]] += g[l] * r0[l][d] / M->mass[ca[l]];
+        M->x[d * N + cb[l]] -= g[l] * r0[l][d] / M->mass[cb[l]];
+      }
+    }
+  }
+  if (dt != 0.0)
+    for (int l = 0; l < nc; l++)
+      for (int d = 0; d < 3; d++) {
+        M->v[d * N + ca[l]] += lam[l] * r0[l][d] / M->mass[ca[l]] / dt;
+        M->v[d * N + cb[l]] -= lam[l] * r0[l][d] / M->mass[cb[l]] / dt;
+      }
+  return ok;
+}
+
 static int md_shake(orc_md* M, double dt) {
   int N = M->ntap, fail = 0;
   double dti = dt != 0.0 ? 1.0 / dt : 0.0;
 #pragma omp parallel for num_threads(M->nthreads) schedule(static) reduction(| : fail)
   for (int mo = 0; mo < M->nmolc; mo++) {
     int it;
+    if (M->cstart[mo + 1] - M->cstart[mo] <= 3) {
+      if (!mim_molecule(M, M->cstart[mo], M->cstart[mo + 1] - M->cstart[mo], dt, 1)) fail = 1;
+      continue;
+    }
     for (it = 0; it < 5000; it++) {
       int moved = 0;
       for (int k = M->cstart[mo]; k < M->cstart[mo + 1]; k++) {
@@ -195,6 +287,10 @@ static int md_rattle(orc_md* M) {
 #pragma omp parallel for num_threads(M->nthreads) schedule(static) reduction(| : fail)
   for (int mo = 0; mo < M->nmolc; mo++) {
     int it;
+    if (M->cstart[mo + 1] - M->cstart[mo] <= 3) {
+      if (!mim_molecule(M, M->cstart[mo], M->cstart[mo + 1] - M->cstart[mo], 0.0, 0)) fail = 1;
+      continue;
+    }
     for (it = 0; it < 5000; it++) {
       int moved = 0;
       for (int k = M->cstart[mo]; k < M->cstart[mo + 1]; k++) {
