@@ -276,7 +276,51 @@ def gpu_arm(args, wl, s, device):
     res["bytes_io"] = 6 * n * 8
     res["G"], res["N"] = s.ngrp, s.ntap
     eng.close()
+    if args.batch > 1:
+        res["batched"] = batch_arm(args, wl, s, device, flush)
     return res
+
+
+def batch_arm(args, wl, s, device, flush):
+    """B replicas of the workload (different Maxwell-Boltzmann velocities)
+    advanced by one graph launch per step (orac_gpu_batch_run)."""
+    import torch
+
+    from orac_b200.engine import Batch, Engine
+
+    engines = []
+    for r in range(args.batch):
+        t = s.copy()
+        rng = np.random.default_rng(1000 + r)
+        scale = np.sqrt(1.0 / t.mass)
+        v = rng.standard_normal((3, t.ntap)) * scale * np.sqrt(np.mean(t.mass * (t.vx ** 2 + t.vy ** 2 + t.vz ** 2)))
+        v -= (v * t.mass).sum(axis=1, keepdims=True) / t.mass.sum()
+        t.vx, t.vy, t.vz = v[0].copy(), v[1].copy(), v[2].copy()
+        e = Engine(t, device=device)
+        e.md_setup(wl["dt_h"], wl["lrespa"], wl["mrespa"], wl["nupdte"], wl["rshk"])
+        engines.append(e)
+    b = Batch(engines)
+    stream = torch.cuda.ExternalStream(b.stream(), device=device)
+    b.run(args.warmup)
+    total_ms, step_ms = 0.0, []
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        b.run(1, sync=False)
+        e1.record(stream)
+        b.sync()
+        ms = e0.elapsed_time(e1)
+        step_ms.append(ms)
+        total_ms += ms
+    b.close()
+    for e in engines:
+        e.close()
+    st = sorted(step_ms)
+    return {"systems": args.batch, "total_ms": total_ms, "step_ms_p50": st[len(st) // 2],
+            "step_ms_p99": st[min(len(st) - 1, int(0.99 * len(st)))]}
 
 
 def main():
@@ -292,6 +336,7 @@ def main():
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="liquid")
     ap.add_argument("--cpu-budget", type=float, default=12.0, help="seconds of CPU-baseline sampling")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--batch", type=int, default=32, help="replicas advanced together (0/1: skip the batched leg)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     wl = WORKLOADS[args.workload]
@@ -372,6 +417,14 @@ def main():
                     "how": "orac_gpu_md_set_state (pinned host -> device), one step, orac_gpu_md_get_state "
                            "(device -> pinned host), wall clock"},
                gpu_launches=res["launches"], clocks=res["clocks"])
+    if "batched" in res:
+        bt = res["batched"]
+        bval = ns_per_day(args.steps, wl["dt_h"], bt["total_ms"] / 1e3) * bt["systems"]
+        out["batched"] = {"systems": bt["systems"], "value": bval, "unit": "ns/day (aggregate)",
+                          "ms_per_step": bt["total_ms"] / args.steps, "step_ms_p50": bt["step_ms_p50"],
+                          "step_ms_p99": bt["step_ms_p99"], "speedup_vs_plain": bval / value,
+                          "how": "one graph launch per H step advances every replica (orac_gpu_batch_run); "
+                                 "replicas differ in their Maxwell-Boltzmann velocities"}
     print(json.dumps(out))
     return 0
 

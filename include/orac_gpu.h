@@ -232,6 +232,22 @@ int orac_gpu_md_set_state(orac_gpu_ctx* ctx, const double* x, const double* y,
 /* 0 = launch every kernel of a step directly, 1 = replay captured graphs. */
 int orac_gpu_md_set_graphs(orac_gpu_ctx* ctx, int on);
 
+/* Batched systems ----------------------------------------------------------
+ * Many independent systems (replicas, HREM states, alchemical windows), one
+ * context each, advanced together: the batch splices every context's step
+ * graph into one parent graph, so one launch moves all systems one H step
+ * and their kernels run concurrently.  Replaces running ORAC replicas as
+ * separate MPI ranks (src/rem.f90, src/orac_mpi.f90).  The contexts must be
+ * set up with orac_gpu_md_setup, share one device, one list-update period
+ * and one step index, and must not be driven on their own while batched. */
+typedef struct orac_gpu_batch orac_gpu_batch;
+int orac_gpu_batch_create(orac_gpu_ctx** ctxs, int n, orac_gpu_batch** out);
+int orac_gpu_batch_run(orac_gpu_batch* b, int nsteps);
+int orac_gpu_batch_sync(orac_gpu_batch* b);
+int orac_gpu_batch_destroy(orac_gpu_batch* b);
+const char* orac_gpu_batch_last_error(const orac_gpu_batch* b);
+void* orac_gpu_batch_stream(orac_gpu_batch* b);
+
 /* Measurement (no counterpart in the reference, which times with wall
  * clocks in src/timer.f) ---------------------------------------------------
  * The context's cudaStream_t, for callers that record their own events. */

@@ -74,7 +74,7 @@ __device__ __forceinline__ void pair_energy_fp64(const PairArgs& A, double rx, d
 }
 
 template <int MG, bool EN>
-__global__ void __launch_bounds__(WPB * 32)
+__global__ void __launch_bounds__(WPB * 32, (MG <= 4 && !EN) ? 5 : 1)
     k_pair(const PairArgs A) {
   extern __shared__ float2 s_lj[];
   __shared__ float4 s_ai[WPB][MG];

@@ -25,6 +25,7 @@
 namespace {
 
 constexpr int MAXR = 12;  // max radix stages
+constexpr int FFT_THREADS = 128;
 struct FftPlan {
   int n;
   int nst;
@@ -157,7 +158,7 @@ struct GridArgs {
 enum { XF = 0, YF = 1, ZC = 2, YI = 3, XI = 4 };
 
 template <int MODE>
-__global__ void __launch_bounds__(256) k_fft(const GridArgs A) {
+__global__ void __launch_bounds__(FFT_THREADS) k_fft(const GridArgs A) {
   extern __shared__ float2 sm[];
   const int n = A.P.n;
   const int B = A.B;
@@ -512,8 +513,10 @@ int upload_tw(orac_gpu_ctx* ctx, float2** dst, int n) {
 }
 
 int lines_per_block(int n) {
+  // few lines per block: the grids here are small (32^3-96^3), so many
+  // small blocks spread a pass over all SMs
   int B = 3072 / n;  // 2 buffers * B * n * 8 bytes <= 48 KB
-  if (B > 16) B = 16;
+  if (B > 4) B = 4;
   if (B < 1) B = 1;
   return B;
 }
@@ -623,7 +626,7 @@ int pme_run(orac_gpu_ctx* ctx, int natom, const double* d_cart, const double* d_
   G.B = lines_per_block(n1);
   int nb = (n2 * n3 + G.B - 1) / G.B;
   size_t sm = 2 * (size_t)G.B * n1 * sizeof(float2);
-  k_fft<XF><<<nb, 256, sm, ctx->stream>>>(G);
+  k_fft<XF><<<nb, FFT_THREADS, sm, ctx->stream>>>(G);
   CKL();
   // y forward
   make_plan(n2, &G.P);
@@ -631,7 +634,7 @@ int pme_run(orac_gpu_ctx* ctx, int natom, const double* d_cart, const double* d_
   G.B = lines_per_block(n2);
   nb = n3 * ((h1 + G.B - 1) / G.B);
   sm = 2 * (size_t)G.B * n2 * sizeof(float2);
-  k_fft<YF><<<nb, 256, sm, ctx->stream>>>(G);
+  k_fft<YF><<<nb, FFT_THREADS, sm, ctx->stream>>>(G);
   CKL();
   // z forward + influence function + z inverse
   make_plan(n3, &G.P);
@@ -639,7 +642,7 @@ int pme_run(orac_gpu_ctx* ctx, int natom, const double* d_cart, const double* d_
   G.B = lines_per_block(n3);
   nb = n2 * ((h1 + G.B - 1) / G.B);
   sm = 2 * (size_t)G.B * n3 * sizeof(float2);
-  k_fft<ZC><<<nb, 256, sm, ctx->stream>>>(G);
+  k_fft<ZC><<<nb, FFT_THREADS, sm, ctx->stream>>>(G);
   CKL();
   // y inverse
   make_plan(n2, &G.P);
@@ -647,7 +650,7 @@ int pme_run(orac_gpu_ctx* ctx, int natom, const double* d_cart, const double* d_
   G.B = lines_per_block(n2);
   nb = n3 * ((h1 + G.B - 1) / G.B);
   sm = 2 * (size_t)G.B * n2 * sizeof(float2);
-  k_fft<YI><<<nb, 256, sm, ctx->stream>>>(G);
+  k_fft<YI><<<nb, FFT_THREADS, sm, ctx->stream>>>(G);
   CKL();
   // x inverse (c2r)
   make_plan(n1, &G.P);
@@ -655,9 +658,9 @@ int pme_run(orac_gpu_ctx* ctx, int natom, const double* d_cart, const double* d_
   G.B = lines_per_block(n1);
   nb = (n2 * n3 + G.B - 1) / G.B;
   sm = 2 * (size_t)G.B * n1 * sizeof(float2);
-  k_fft<XI><<<nb, 256, sm, ctx->stream>>>(G);
+  k_fft<XI><<<nb, FFT_THREADS, sm, ctx->stream>>>(G);
   CKL();
-  k_gather<<<(natom + 255) / 256, 256, 0, ctx->stream>>>(A);
+  k_gather<<<(natom + 63) / 64, 64, 0, ctx->stream>>>(A);
   CKL();
   return ORAC_OK;
 }

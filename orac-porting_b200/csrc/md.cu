@@ -704,7 +704,7 @@ static int md_kick(orac_gpu_ctx* ctx, MdState& S, int lvl, double dt) {
   MolArgs A = mol_args(ctx, S, dt);
   A.fkick = S.ffix[lvl];
   const int n = S.nsm + S.nfree;
-  k_kick<<<(n + 127) / 128, 128, 0, ctx->stream>>>(A);
+  k_kick<<<(n + 31) / 32, 32, 0, ctx->stream>>>(A);
   CKL();
   if (S.nbig) {
     k_rattle_big<<<(S.nbig + 127) / 128, 128, 0, ctx->stream>>>(big_args(ctx, S, dt, 1e-12));
@@ -718,7 +718,7 @@ static int md_drift(orac_gpu_ctx* ctx, MdState& S, double dt, unsigned long long
   MolArgs A = mol_args(ctx, S, dt);
   A.fzero = fzero;
   const int n = S.nsm + S.nfree;
-  k_drift<<<(n + 127) / 128, 128, 0, ctx->stream>>>(A);
+  k_drift<<<(n + 31) / 32, 32, 0, ctx->stream>>>(A);
   CKL();
   if (S.nbig) {
     k_shake_big<<<(S.nbig + 127) / 128, 128, 0, ctx->stream>>>(big_args(ctx, S, dt, 1e-8));
@@ -727,7 +727,7 @@ static int md_drift(orac_gpu_ctx* ctx, MdState& S, double dt, unsigned long long
     CKL();
   }
   if (S.nfreeg) {
-    k_free_groups<<<(S.nfreeg + 127) / 128, 128, 0, ctx->stream>>>(A);
+    k_free_groups<<<(S.nfreeg + 31) / 32, 32, 0, ctx->stream>>>(A);
     CKL();
   }
   return ORAC_OK;
@@ -1030,6 +1030,58 @@ int orac_gpu_md_set_graphs(orac_gpu_ctx* ctx, int on) {
 
 }  // extern "C"
 
+// capture (once) the step graph of one kind: 0 plain step, 1 step with list update
+static int md_capture(orac_gpu_ctx* ctx, MdState& S, int kind) {
+  cudaGraphExec_t* ge = kind ? &S.gexec_u : &S.gexec;
+  cudaGraph_t* gg = kind ? &S.graph_u : &S.graph;
+  if (*ge) return ORAC_OK;
+  const int64_t l0 = ctx->launches;
+  S.pslot[kind][0] = ctx->prof_next;
+  CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+  const int rc = md_step(ctx, S, kind == 1, false);
+  cudaGraph_t g = nullptr;
+  const cudaError_t ce = cudaStreamEndCapture(ctx->stream, &g);
+  if (rc) {
+    if (g) cudaGraphDestroy(g);
+    return rc;
+  }
+  CK(ce);
+  *gg = g;
+  CK(cudaGraphInstantiate(ge, g, 0));
+  S.pslot[kind][1] = ctx->prof_next;
+  S.kpg[kind] = ctx->launches - l0;
+  ctx->launches = l0;
+  return ORAC_OK;
+}
+
+// ---- hooks of the batch driver (batch.cu)
+int md_step_graph(orac_gpu_ctx* ctx, int kind, cudaGraph_t* out) {
+  MdState& S = *md_of(ctx);
+  if (!S.ready) return ctx_fail(ctx, ORAC_ERR_STATE, "md_setup not called");
+  if (int rc = md_capture(ctx, S, kind)) return rc;
+  *out = kind ? S.graph_u : S.graph;
+  return ORAC_OK;
+}
+
+int md_advance(orac_gpu_ctx* ctx, int nsteps) {
+  MdState& S = *md_of(ctx);
+  S.step += nsteps;
+  ctx->launches += S.kpg[0] * nsteps;
+  return ORAC_OK;
+}
+
+long long md_step_index(orac_gpu_ctx* ctx) { return ctx->md ? ctx->md->step : -1; }
+int md_nupdte(orac_gpu_ctx* ctx) { return ctx->md && ctx->md->ready ? ctx->md->nupdte : -1; }
+
+int md_check_flags(orac_gpu_ctx* ctx) {
+  MdState& S = *md_of(ctx);
+  int flag = 0;
+  CK(cudaMemcpy(&flag, S.flag, sizeof(int), cudaMemcpyDeviceToHost));
+  if (flag & 1) return ctx_fail(ctx, ORAC_ERR_CAPACITY, "SHAKE/RATTLE did not converge");
+  if (flag & 2) return ctx_fail(ctx, ORAC_ERR_CAPACITY, "neighbour list capacity exceeded during the run");
+  return ORAC_OK;
+}
+
 static int md_run_impl(orac_gpu_ctx* ctx, int nsteps, int energy_every, double* rec, bool async) {
   if (!ctx) return ORAC_ERR_PARAM;
   MdState& S = *md_of(ctx);
@@ -1042,25 +1094,7 @@ static int md_run_impl(orac_gpu_ctx* ctx, int nsteps, int energy_every, double* 
     if (S.use_graph && !energy) {
       const int kind = update ? 1 : 0;
       cudaGraphExec_t* ge = update ? &S.gexec_u : &S.gexec;
-      cudaGraph_t* gg = update ? &S.graph_u : &S.graph;
-      if (!*ge) {
-        const int64_t l0 = ctx->launches;
-        S.pslot[kind][0] = ctx->prof_next;
-        CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
-        const int rc = md_step(ctx, S, update, false);
-        cudaGraph_t g = nullptr;
-        const cudaError_t ce = cudaStreamEndCapture(ctx->stream, &g);
-        if (rc) {
-          if (g) cudaGraphDestroy(g);
-          return rc;
-        }
-        CK(ce);
-        *gg = g;
-        CK(cudaGraphInstantiate(ge, g, 0));
-        S.pslot[kind][1] = ctx->prof_next;
-        S.kpg[kind] = ctx->launches - l0;
-        ctx->launches = l0;
-      }
+      if (int rc = md_capture(ctx, S, kind)) return rc;
       CK(cudaGraphLaunch(*ge, ctx->stream));
       ctx->launches += S.kpg[kind];
       S.last_kind = kind;

@@ -234,3 +234,44 @@ class Engine:
         b = C.c_double()
         check(self.ctx, self.lib.orac_gpu_cself(self.ctx, self.s.rkcut, C.byref(a), C.byref(b)), "cself")
         return a.value, b.value
+
+
+class Batch:
+    """Many Engines advanced together by one graph launch per H step
+    (orac_gpu_batch_*).  Every engine must have run md_setup."""
+
+    def __init__(self, engines):
+        self.engines = list(engines)
+        self.lib = L.load()
+        arr = (C.c_void_p * len(self.engines))(*[e.ctx.value for e in self.engines])
+        h = C.c_void_p()
+        rc = self.lib.orac_gpu_batch_create(arr, len(self.engines), C.byref(h))
+        if rc != L.ORAC_OK:
+            raise L.OracGpuError(f"orac_gpu_batch_create: {L.ERRORS.get(rc, rc)}")
+        self.h = h
+
+    def _check(self, rc, what):
+        if rc != L.ORAC_OK:
+            raise L.OracGpuError(f"{what}: {L.ERRORS.get(rc, rc)} {self.lib.orac_gpu_batch_last_error(self.h).decode()}")
+
+    def run(self, nsteps, sync=True):
+        self._check(self.lib.orac_gpu_batch_run(self.h, nsteps), "batch_run")
+        if sync:
+            self.sync()
+
+    def sync(self):
+        self._check(self.lib.orac_gpu_batch_sync(self.h), "batch_sync")
+
+    def stream(self):
+        return self.lib.orac_gpu_batch_stream(self.h)
+
+    def close(self):
+        if self.h:
+            self.lib.orac_gpu_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -74,6 +74,12 @@ def load():
         "orac_gpu_md_run_async": (i, [_P, i]),
         "orac_gpu_md_collect": (i, [_P]),
         "orac_gpu_get_stream": (_P, [_P]),
+        "orac_gpu_batch_create": (i, [C.POINTER(_P), i, C.POINTER(_P)]),
+        "orac_gpu_batch_run": (i, [_P, i]),
+        "orac_gpu_batch_sync": (i, [_P]),
+        "orac_gpu_batch_destroy": (i, [_P]),
+        "orac_gpu_batch_last_error": (C.c_char_p, [_P]),
+        "orac_gpu_batch_stream": (_P, [_P]),
         "orac_gpu_counters": (i, [_P, C.POINTER(i64), i]),
         "orac_gpu_prof_enable": (i, [_P, i]),
         "orac_gpu_prof_read": (i, [_P, C.POINTER(d), C.POINTER(i64), i]),
