@@ -277,7 +277,10 @@ def gpu_arm(args, wl, s, device):
     res["G"], res["N"] = s.ngrp, s.ntap
     eng.close()
     if args.batch > 1:
-        res["batched"] = batch_arm(args, wl, s, device, flush)
+        try:
+            res["batched"] = batch_arm(args, wl, s, device, flush)
+        except Exception as exc:  # reported in the JSON line; the plain leg stands on its own
+            res["batched_error"] = f"{type(exc).__name__}: {exc}"
     return res
 
 
@@ -425,6 +428,8 @@ def main():
                           "step_ms_p99": bt["step_ms_p99"], "speedup_vs_plain": bval / value,
                           "how": "one graph launch per H step advances every replica (orac_gpu_batch_run); "
                                  "replicas differ in their Maxwell-Boltzmann velocities"}
+    elif "batched_error" in res:
+        out["batched"] = {"error": res["batched_error"]}
     print(json.dumps(out))
     return 0
 
