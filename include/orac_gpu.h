@@ -190,6 +190,41 @@ int orac_gpu_fft_pme_dev(orac_gpu_ctx* ctx, const double* xyz_scaled,
                          const double* mol_scaled, double* fdev,
                          double* eer_dev, double* stress_dev);
 
+/* orac_gpu_pme_kspace_static — has no counterpart in the reference.
+ *
+ * The SPME reciprocal sum of orac_gpu_do_pmesh_kspace for callers that cannot
+ * allocate device memory: a host program that owns the HBM budget and passes
+ * libraries only buffers it carved out itself, a serving loop that cannot
+ * take the device-wide synchronisation cudaMalloc/cudaFree bring, a plugin
+ * whose host forbids allocation.  It needs no context (creating one
+ * allocates), calls no cudaMalloc, cudaFree or allocating library routine,
+ * and keeps its scratch in one fixed device array of 5 MiB + 16 KiB that
+ * every GPU loading the library holds until the process exits.
+ *
+ * Limit: each of nfft1..3 at most 256 and n1*n2*n3 at most 262144 (64^3);
+ * larger grids return ORAC_ERR_CAPACITY with the reason in err.  Each axis
+ * must also be at least order (2..12) and factor into 2, 3, 5, 7.
+ *
+ * Runs on the current device, on `stream` (a cudaStream_t; NULL = the legacy
+ * default stream), asynchronously.  Device pointers: xyz[3*numatoms] Cartesian
+ * x|y|z, charge[numatoms] (ORAC's internal charges), force[3*numatoms] x|y|z
+ * which is ACCUMULATED into, energy[10] which receives eer then the 3x3
+ * column-major virial.  recip (= 0.5 oc^T) is a host array of 9; rkcut <= 0
+ * means no reciprocal-space cut.  err (may be NULL) receives a message of at
+ * most err_len bytes on failure.
+ *
+ * The first call on a device looks up the scratch array's device address
+ * (cudaGetSymbolAddress, with that device current); make that first call
+ * before any stream capture.  Every call on a device shares the one array:
+ * calls that overlap on the GPU (other streams, other host threads) race and
+ * give wrong results — serialise them. */
+int orac_gpu_pme_kspace_static(void* stream, int numatoms, const double* xyz,
+                               const double* charge, const double* recip,
+                               double volume, double ewald_coeff, double rkcut,
+                               int order, int nfft1, int nfft2, int nfft3,
+                               double* force, double* energy, char* err,
+                               int err_len);
+
 /* r-RESPA molecular dynamics on the device ---------------------------------
  * The NVE part of ORAC's step loop, mtsmd (src/mtsmd.f:2390-3540), with its
  * kick correc (src/correc.f), drift verlet (src/verlet.f) and the SHAKE /

@@ -19,6 +19,9 @@
 //   k_gather      forces (grad_sum :310-372) and the molecular virial
 //                 correction of fft_pme (src/fft_pme.f:65-106)
 #include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <mutex>
 
 #include "common.cuh"
 
@@ -662,5 +665,275 @@ int pme_run(orac_gpu_ctx* ctx, int natom, const double* d_cart, const double* d_
   CKL();
   k_gather<<<(natom + 63) / 64, 64, 0, ctx->stream>>>(A);
   CKL();
+  return ORAC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// orac_gpu_pme_kspace_static: the SPME reciprocal sum of do_pmesh_kspace with
+// no allocation at all.
+//
+// Some callers cannot allocate device memory: a host program that owns the
+// whole HBM budget and hands libraries only buffers it carved out itself, a
+// latency-bound serving loop that cannot take the device-wide
+// synchronisation cudaMalloc / cudaFree imply, or a plugin whose host forbids
+// allocation.  Such callers cannot create a context either (that allocates),
+// so this entry point takes everything as arguments, reads and writes only
+// the caller's device buffers, and keeps its working set -- charge grid,
+// complex and real grids, twiddles, B-spline moduli, energy/virial sums -- in
+// the fixed array below.  Every GPU that loads the library holds that array
+// (ORAC_STATIC_PME_BYTES) until the process exits.
+//
+// Host code must never hand orac_static_pme_scratch itself to a kernel: on
+// the host that name is a stand-in, not a device address.  The device address
+// is looked up with cudaGetSymbolAddress once per device, with that device
+// current, on the first call made on it.
+#define ORAC_STATIC_PME_BYTES (5u * 1024u * 1024u + 16u * 1024u)
+static __device__ __align__(256) unsigned char orac_static_pme_scratch[ORAC_STATIC_PME_BYTES];
+
+namespace {
+
+constexpr int STATIC_MAX_AXIS = 256;             // points per grid axis
+constexpr long long STATIC_MAX_POINTS = 262144;  // n1*n2*n3 (64^3)
+constexpr int STATIC_MAX_DEVICES = 64;
+
+std::mutex g_static_mu;
+unsigned char* g_static_base[STATIC_MAX_DEVICES];  // device address of the array, per device
+
+struct SplineAt0 {
+  double c[MAXORD + 2];
+};
+
+// Twiddles and |DFT(B-spline)|^2 moduli of the three axes (one block per
+// axis), the same FP64 sums as upload_tw and host_bsp_moduli: only the order
+// non-zero spline values enter the DFT, products and sums are kept unfused,
+// and the small-modulus patch runs serially in index order like
+// DFTMOD's loop (src/pme_fftw3.f90:202-230).
+__global__ void k_static_tables(int n1, int n2, int n3, int order, SplineAt0 arr, float2* tw, float* bsp) {
+  __shared__ double mod[STATIC_MAX_AXIS];
+  const int axis = blockIdx.x;
+  const int n = axis == 0 ? n1 : (axis == 1 ? n2 : n3);
+  float2* t = tw + axis * STATIC_MAX_AXIS;
+  float* b = bsp + axis * STATIC_MAX_AXIS;
+  const double pi = 3.14159265358979323846;
+  const double twopi = 2.0 * (double)3.14159265358979323846f;  // single-precision pi, as DFTMOD
+  for (int k = threadIdx.x; k < n; k += blockDim.x) {
+    t[k] = make_float2((float)cos(-2.0 * pi * k / n), (float)sin(-2.0 * pi * k / n));
+    double s1 = 0.0, s2 = 0.0;
+    for (int j = 1; j <= order && j < n; j++) {
+      const double arg = twopi * k * j / n;
+      s1 = __dadd_rn(s1, __dmul_rn(arr.c[j - 1], cos(arg)));
+      s2 = __dadd_rn(s2, __dmul_rn(arr.c[j - 1], sin(arg)));
+    }
+    mod[k] = __dadd_rn(__dmul_rn(s1, s1), __dmul_rn(s2, s2));
+  }
+  __syncthreads();
+  if (threadIdx.x == 0)
+    for (int k = 0; k < n; k++)
+      if (mod[k] < 1.0e-7) mod[k] = 0.5 * ((k >= 1 ? mod[k - 1] : mod[n - 1]) + (k <= n - 2 ? mod[k + 1] : mod[0]));
+  __syncthreads();
+  for (int k = threadIdx.x; k < n; k += blockDim.x) b[k] = (float)mod[k];
+}
+
+// eer and the 3x3 column-major virial from the grid sums, as
+// orac_gpu_do_pmesh_kspace finishes them on the host
+__global__ void k_static_finish(const double* __restrict__ e, double* __restrict__ out) {
+  if (threadIdx.x != 0) return;
+  out[0] = 0.5 * e[0];
+  out[1] = 0.5 * e[1];
+  out[2] = 0.5 * e[4];
+  out[3] = 0.5 * e[5];
+  out[4] = 0.5 * e[4];
+  out[5] = 0.5 * e[2];
+  out[6] = 0.5 * e[6];
+  out[7] = 0.5 * e[5];
+  out[8] = 0.5 * e[6];
+  out[9] = 0.5 * e[3];
+}
+
+int static_fail(char* err, int err_len, int code, const char* fmt, ...) {
+  if (err && err_len > 0) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(err, (size_t)err_len, fmt, ap);
+    va_end(ap);
+  }
+  return code;
+}
+
+// device address of the scratch array on device dev (which is current)
+int static_scratch(int dev, unsigned char** out, char* err, int err_len) {
+  std::lock_guard<std::mutex> lock(g_static_mu);
+  if (!g_static_base[dev]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, orac_static_pme_scratch);
+    if (e != cudaSuccess || !p)
+      return static_fail(err, err_len, ORAC_ERR_CUDA, "cudaGetSymbolAddress of the SPME scratch on device %d: %s",
+                         dev, cudaGetErrorString(e));
+    g_static_base[dev] = (unsigned char*)p;
+  }
+  *out = g_static_base[dev];
+  return ORAC_OK;
+}
+
+size_t up256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+}  // namespace
+
+extern "C" int orac_gpu_pme_kspace_static(void* stream, int numatoms, const double* d_xyz, const double* d_charge,
+                                          const double* recip, double volume, double ewald_coeff, double rkcut,
+                                          int order, int nfft1, int nfft2, int nfft3, double* d_force,
+                                          double* d_energy, char* err, int err_len) {
+  if (err && err_len > 0) err[0] = '\0';
+  if (numatoms <= 0) return static_fail(err, err_len, ORAC_ERR_PARAM, "numatoms = %d", numatoms);
+  if (!d_xyz || !d_charge || !recip || !d_force || !d_energy)
+    return static_fail(err, err_len, ORAC_ERR_PARAM, "null coordinate, charge, recip, force or energy pointer");
+  if (order < 2 || order > MAXORD)
+    return static_fail(err, err_len, ORAC_ERR_PARAM, "PME order %d outside 2..%d", order, MAXORD);
+  if (!(volume > 0.0) || !(ewald_coeff > 0.0))
+    return static_fail(err, err_len, ORAC_ERR_PARAM, "volume %g and ewald_coeff %g must be positive", volume,
+                       ewald_coeff);
+  const int dims[3] = {nfft1, nfft2, nfft3};
+  FftPlan plan;
+  for (int a = 0; a < 3; a++) {
+    if (dims[a] > STATIC_MAX_AXIS)
+      return static_fail(err, err_len, ORAC_ERR_CAPACITY,
+                         "grid axis %d has %d points: the fixed scratch of orac_gpu_pme_kspace_static takes at most "
+                         "%d per axis and %lld in all (64^3)",
+                         a + 1, dims[a], STATIC_MAX_AXIS, STATIC_MAX_POINTS);
+    if (dims[a] < order)
+      return static_fail(err, err_len, ORAC_ERR_PARAM, "grid axis %d has %d points, fewer than the order %d", a + 1,
+                         dims[a], order);
+    if (make_plan(dims[a], &plan))
+      return static_fail(err, err_len, ORAC_ERR_PARAM, "grid axis %d = %d does not factor into 2, 3, 5, 7", a + 1,
+                         dims[a]);
+  }
+  const long long ng = (long long)nfft1 * nfft2 * nfft3;
+  if (ng > STATIC_MAX_POINTS)
+    return static_fail(err, err_len, ORAC_ERR_CAPACITY,
+                       "grid %dx%dx%d has %lld points: the fixed scratch of orac_gpu_pme_kspace_static holds at "
+                       "most %lld (64^3)",
+                       nfft1, nfft2, nfft3, ng, STATIC_MAX_POINTS);
+  const int h1 = nfft1 / 2 + 1;
+  // scratch layout: sums | twiddles | moduli | charge grid | real grid | complex grid
+  const size_t o_tw = 256;
+  const size_t o_bsp = up256(o_tw + sizeof(float2) * 3 * STATIC_MAX_AXIS);
+  const size_t o_q = up256(o_bsp + sizeof(float) * 3 * STATIC_MAX_AXIS);
+  const size_t o_rg = up256(o_q + sizeof(unsigned long long) * (size_t)ng);
+  const size_t o_cg = up256(o_rg + sizeof(float) * (size_t)ng);
+  const size_t end = o_cg + sizeof(float2) * (size_t)h1 * nfft2 * nfft3;
+  if (end > ORAC_STATIC_PME_BYTES)
+    return static_fail(err, err_len, ORAC_ERR_CAPACITY, "grid %dx%dx%d needs %zu scratch bytes of %u", nfft1, nfft2,
+                       nfft3, end, ORAC_STATIC_PME_BYTES);
+
+  int dev = 0;
+  cudaError_t ce = cudaGetDevice(&dev);
+  if (ce != cudaSuccess)
+    return static_fail(err, err_len, ORAC_ERR_NODEVICE, "cudaGetDevice: %s", cudaGetErrorString(ce));
+  if (dev < 0 || dev >= STATIC_MAX_DEVICES)
+    return static_fail(err, err_len, ORAC_ERR_PARAM, "device %d beyond the %d this entry point tracks", dev,
+                       STATIC_MAX_DEVICES);
+  unsigned char* base = nullptr;
+  if (int rc = static_scratch(dev, &base, err, err_len)) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  double* eout = (double*)base;
+  float2* tw = (float2*)(base + o_tw);
+  float* bsp = (float*)(base + o_bsp);
+  unsigned long long* qfix = (unsigned long long*)(base + o_q);
+  float* rgrid = (float*)(base + o_rg);
+  float2* cgrid = (float2*)(base + o_cg);
+
+  // what must start at zero: the fixed-point charge grid and the energy sums
+  ce = cudaMemsetAsync(qfix, 0, sizeof(unsigned long long) * (size_t)ng, st);
+  if (ce == cudaSuccess) ce = cudaMemsetAsync(eout, 0, sizeof(double) * 16, st);
+  if (ce != cudaSuccess) return static_fail(err, err_len, ORAC_ERR_CUDA, "cudaMemsetAsync: %s", cudaGetErrorString(ce));
+
+  SplineAt0 arr;
+  double darr[MAXORD + 2];
+  for (int k = 0; k < MAXORD + 2; k++) arr.c[k] = darr[k] = 0.0;
+  host_bspline(0.0, order, arr.c, darr);
+  k_static_tables<<<3, 128, 0, st>>>(nfft1, nfft2, nfft3, order, arr, tw, bsp);
+
+  AtomArgs A;
+  memset(&A, 0, sizeof(A));
+  A.natom = numatoms;
+  A.order = order;
+  A.n1 = nfft1;
+  A.n2 = nfft2;
+  A.n3 = nfft3;
+  A.xyz = d_xyz;
+  A.q = d_charge;
+  A.r11 = recip[0];
+  A.r21 = recip[1];
+  A.r31 = recip[2];
+  A.r12 = recip[3];
+  A.r22 = recip[4];
+  A.r32 = recip[5];
+  A.r13 = recip[6];
+  A.r23 = recip[7];
+  A.r33 = recip[8];
+  A.qfix = qfix;
+  A.rg = rgrid;
+  A.f = d_force;
+  A.eout = eout;
+  const int nsp = numatoms * order;
+  k_spread<<<(nsp + 255) / 256, 256, 0, st>>>(A);
+
+  GridArgs G;
+  memset(&G, 0, sizeof(G));
+  G.n1 = nfft1;
+  G.n2 = nfft2;
+  G.n3 = nfft3;
+  G.h1 = h1;
+  G.qfix = qfix;
+  G.cg = cgrid;
+  G.rg = rgrid;
+  G.bsp1 = bsp;
+  G.bsp2 = bsp + STATIC_MAX_AXIS;
+  G.bsp3 = bsp + 2 * STATIC_MAX_AXIS;
+  G.r11 = recip[0];
+  G.r21 = recip[1];
+  G.r31 = recip[2];
+  G.r12 = recip[3];
+  G.r22 = recip[4];
+  G.r32 = recip[5];
+  G.r13 = recip[6];
+  G.r23 = recip[7];
+  G.r33 = recip[8];
+  const double pif = (double)3.14159265358979323846f;  // scalar_sum's single-precision pi
+  const double rk = rkcut > 0.0 ? rkcut : 1e9;
+  G.fac = (float)(pif * pif / (ewald_coeff * ewald_coeff));
+  G.pivol = (float)(pif * volume);
+  G.rkcut2 = 0.25 * rk * rk / (pif * pif);
+  G.eout = eout;
+  const float2* tws[3] = {tw, tw + STATIC_MAX_AXIS, tw + 2 * STATIC_MAX_AXIS};
+  // x forward (r2c)
+  make_plan(nfft1, &G.P);
+  G.tw = tws[0];
+  G.B = lines_per_block(nfft1);
+  k_fft<XF><<<(nfft2 * nfft3 + G.B - 1) / G.B, FFT_THREADS, 2 * (size_t)G.B * nfft1 * sizeof(float2), st>>>(G);
+  // y forward
+  make_plan(nfft2, &G.P);
+  G.tw = tws[1];
+  G.B = lines_per_block(nfft2);
+  k_fft<YF><<<nfft3 * ((h1 + G.B - 1) / G.B), FFT_THREADS, 2 * (size_t)G.B * nfft2 * sizeof(float2), st>>>(G);
+  // z forward + influence function + z inverse
+  make_plan(nfft3, &G.P);
+  G.tw = tws[2];
+  G.B = lines_per_block(nfft3);
+  k_fft<ZC><<<nfft2 * ((h1 + G.B - 1) / G.B), FFT_THREADS, 2 * (size_t)G.B * nfft3 * sizeof(float2), st>>>(G);
+  // y inverse
+  make_plan(nfft2, &G.P);
+  G.tw = tws[1];
+  G.B = lines_per_block(nfft2);
+  k_fft<YI><<<nfft3 * ((h1 + G.B - 1) / G.B), FFT_THREADS, 2 * (size_t)G.B * nfft2 * sizeof(float2), st>>>(G);
+  // x inverse (c2r)
+  make_plan(nfft1, &G.P);
+  G.tw = tws[0];
+  G.B = lines_per_block(nfft1);
+  k_fft<XI><<<(nfft2 * nfft3 + G.B - 1) / G.B, FFT_THREADS, 2 * (size_t)G.B * nfft1 * sizeof(float2), st>>>(G);
+  k_gather<<<(numatoms + 63) / 64, 64, 0, st>>>(A);
+  k_static_finish<<<1, 32, 0, st>>>(eout, d_energy);
+  ce = cudaGetLastError();
+  if (ce != cudaSuccess) return static_fail(err, err_len, ORAC_ERR_CUDA, "SPME launch: %s", cudaGetErrorString(ce));
   return ORAC_OK;
 }
