@@ -93,6 +93,16 @@ class System:
     tors_k: np.ndarray | None = None
     tors_n: np.ndarray | None = None
     tors_d: np.ndarray | None = None
+    lj_params: np.ndarray | None = None  # (ntype, 2): Rmin/2 (A), eps (kcal/mol) per LJ type
+    # alchemy (soft-core force_alchemy): 1 normal, 2 added, -2 removed per atom
+    ss_alchemy: np.ndarray | None = None
+    # REM segment (force_rem): 1 for atoms of the scaled segment
+    rematom: np.ndarray | None = None
+
+    def alchemy_params(self):
+        """Per-atom rmin, epsm of the soft-core kernel (src/mtsmd.f:1298-1303)."""
+        p = self.lj_params[self.nbtype - 1]
+        return units.alchemy_rmin_epsm(p[:, 0], p[:, 1])
 
     @property
     def oc(self):
@@ -255,6 +265,7 @@ def _assemble(name, co, pos_cart, mass, q_e, ltype, lj_types, groups, molecules,
     v -= ptot[:, None]
     ss = np.where(solute_mask, 1, 2).astype(np.int32)
     sysm = System(
+        lj_params=np.array(lj_types, dtype=np.float64).reshape(-1, 2),
         name=name, ntap=n, ngrp=len(groups), nprot=len(molecules), co=co,
         xp0=s[0].copy(), yp0=s[1].copy(), zp0=s[2].copy(), mass=np.asarray(mass, dtype=np.float64),
         charge=np.array([units.charge_internal(q) for q in q_e]), nbtype=np.asarray(ltype, dtype=np.int32),

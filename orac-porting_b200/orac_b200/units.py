@@ -43,6 +43,20 @@ def amber_pair(rmin_half_i, eps_i, rmin_half_j, eps_j):
     return tmpi * tmpj * tmpj, tmpi * tmpj
 
 
+def alchemy_rmin_epsm(rmin_half, eps_kcal):
+    """Per-atom soft-core parameters, src/mtsmd.f:1298-1303:
+    rmin = pnbd1 / 2**(1./6.) with the exponent a default-real (single
+    precision) quotient, epsm = |pnbd2 * (1000 * 4.184 / efact)| with a
+    single-precision 4.184, and rmin = 0.1 where epsm is zero."""
+    import numpy as np
+
+    sixth = float(np.float32(1.0) / np.float32(6.0))
+    rmin = np.asarray(rmin_half, dtype=np.float64) / 2.0 ** sixth
+    epsm = np.abs(np.asarray(eps_kcal, dtype=np.float64) * (1000.0 * _F4184 / EFACT))
+    rmin = np.where(epsm == 0.0, 0.1, rmin)
+    return rmin, epsm
+
+
 def kinetic_temperature(ekin_internal, ndf):
     """Temperature in K from kinetic energy in internal units and degrees of freedom."""
     return 2.0 * ekin_internal * UNITE / (ndf * BOLTZ)

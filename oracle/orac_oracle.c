@@ -249,6 +249,9 @@ typedef struct {
   double *xmap1, *ymap1, *zmap1, *xmap2, *ymap2, *zmap2, *cmap2, *swrs, *dswrs;
   double *xmap3, *ymap3, *zmap3;
   int* nlist_out; /* next-shell candidates of the current group */
+  double* drs;    /* alchemy: squared centre distance of each mapped group */
+  double seg_ene; /* REM: energy of the selected pairs */
+  double uconf0[3], ucoul0[3]; /* alchemy: energies at lambda0 */
 } force_ws;
 
 typedef struct {
@@ -270,7 +273,16 @@ typedef struct {
   int lskip_ewald, ewald, iz;
   double r2inn, r2out, rinn, rinn0, r2inn0, rout0, r2out0, r2neigh;
   double arsout1, arsout2, arsinn1, arsinn2, twrtpi;
+  const orc_variant* V; /* NULL: standard force */
 } force_args;
+
+/* seg_select, src/rem.f90:631-645 (0-based atoms) */
+static inline int seg_select(const orc_variant* V, int a, int b) {
+  const int ra = V->rematom[a] != 0, rb = V->rematom[b] != 0;
+  if (V->rem_kind == 0) return ra || rb;
+  if (V->rem_kind == 1) return ra && rb;
+  return ra != rb;
+}
 
 /* Pair loop body shared by the four loops of src/force.f:396-731.  sw < 0
  * marks the non-switched band (qforce unscaled, energies to ucoula/uconfa);
@@ -291,16 +303,20 @@ static inline void pair_eval(const force_args* A, force_ws* W, int i1, int j,
   double rsqi = 1.0 / rsq;
   double qforce = 0.0;
   double wsc = (sw < 0) ? 1.0 : sw;
+  /* force_rem: selected pairs scale their force and S'V share */
+  const int sel = A->V && A->V->mode == 1 && seg_select(A->V, i1, j);
+  const double rf = sel ? A->V->rem_factor : 1.0;
+  double conf = 0.0, coul = 0.0;
   if (e6 > 1e-12) {
     double r6 = rsqi * rsqi * rsqi;
     double r12 = r6 * r6;
     double ssvir = 12.0 * e12 * r12 - 6.0 * e6 * r6;
     qforce = ssvir * rsqi * wsc;
-    double conf = e12 * r12 - e6 * r6;
+    conf = e12 * r12 - e6 * r6;
     if (sw < 0) {
       *uconfa += conf;
     } else {
-      *cmap += conf;
+      *cmap += sel ? conf * rf : conf;
       W->uconf[typeij - 1] += sw * conf;
     }
   }
@@ -314,23 +330,29 @@ static inline void pair_eval(const force_args* A, force_ws* W, int i1, int j,
         ((((AS_A5 * qt + AS_A4) * qt + AS_A3) * qt + AS_A2) * qt + AS_A1) *
         qt * expcst;
     double furpar = chrgei * A->charge[j];
+    coul = furpar * erfcst / rsp;
     if (sw < 0) {
       *ucoula += furpar * erfcst / rsp;
     } else {
       W->ucoul[typeij - 1] += sw * furpar * erfcst / rsp;
-      *cmap += furpar * erfcst / rsp;
+      *cmap += sel ? coul * rf : furpar * erfcst / rsp;
     }
     qforce += furpar * (erfcst + A->twrtpi * alphar * expcst) * rspqi * wsc;
   } else if (!A->ewald) {
     double rsp = sqrt(rsq);
     double ssvir = chrgei * A->charge[j] / rsp;
+    coul = ssvir;
     if (sw < 0) {
       W->ucoul[typeij - 1] += ssvir;
     } else {
-      *cmap += ssvir;
+      *cmap += sel ? ssvir * rf : ssvir;
       W->ucoul[typeij - 1] += ssvir * sw;
     }
     qforce += ssvir * rsqi * wsc;
+  }
+  if (sel) { /* src/force_REM.f:491-495,634-678 */
+    W->seg_ene += (sw < 0) ? conf + coul : sw * conf + sw * coul;
+    qforce *= rf;
   }
   W->fx[i1] += qforce * xc;
   W->fy[i1] += qforce * yc;
@@ -532,6 +554,252 @@ static int force_group(const force_args* A, force_ws* W, int i, const int* lst,
   return map;
 }
 
+/* Soft-core pair of force_alchemy, src/force_alchemy.f:441-531.  j1 is the
+ * map slot of the partner group. */
+static inline void alch_pair(const force_args* A, force_ws* W, int i1, int j,
+                             int j1, double xpi, double ypi, double zpi,
+                             double xpcmp1, double ypcmp1, double zpcmp1,
+                             double chrgei, int typeij) {
+  const orc_variant* V = A->V;
+  const double* co = A->co;
+  double sigma = V->opls ? 2.0 * sqrt(V->rmin[j] * V->rmin[i1])
+                         : V->rmin[j] + V->rmin[i1];
+  double epsmin = 4.0 * sqrt(V->epsm[i1] * V->epsm[j]);
+  if (epsmin < 1.0e-12 && A->lskip_ewald && A->ewald) return;
+  const int t = V->ss_alchemy[i1] + V->ss_alchemy[j] + 4;
+  const double sw = W->swrs[j1];
+  int p2 = A->atomp[j] - 1;
+  double xxcm = xpcmp1 - A->xpcm[p2] - W->xmap1[j1];
+  double yycm = ypcmp1 - A->ypcm[p2] - W->ymap1[j1];
+  double zzcm = zpcmp1 - A->zpcm[p2] - W->zmap1[j1];
+  double xg = xpi - A->xp0[j] - W->xmap1[j1];
+  double yg = ypi - A->yp0[j] - W->ymap1[j1];
+  double zg = zpi - A->zp0[j] - W->zmap1[j1];
+  double xc = co[0] * xg + co[3] * yg + co[6] * zg;
+  double yc = co[4] * yg + co[7] * zg;
+  double zc = co[8] * zg;
+  double rsq = xc * xc + yc * yc + zc * zc;
+  double auxa = 1.0 / sqrt(rsq);
+  double fq = V->factq[0][t], fq0 = V->factq0[0][t];
+  double auxaa = 1.0 / sqrt(V->qsoft * (fq * fq) + rsq); /* soft core */
+  double auxa0 = 1.0 / sqrt(V->qsoft * (fq0 * fq0) + rsq);
+  double auxbb = auxaa * auxaa * auxaa;
+  double qforce;
+  if (epsmin > 1.0e-12) {
+    double r6 = rsq * rsq * rsq / pow(sigma, 6.0);
+    double gp = V->ljsoft * V->fact[0][t] + r6;
+    double gp1 = 1.0 / gp;
+    double gp2 = gp1 * gp1;
+    double gp0 = V->ljsoft * V->fact0[0][t] + r6;
+    double gp10 = 1.0 / gp0;
+    double gp20 = gp10 * gp10;
+    double gr = 6.0 * r6 * auxa;
+    double ssvir = V->fact[1][t] * epsmin * (2.0 * gp1 * gp2 - gp2);
+    double ssvirr = gr * ssvir;
+    double auxc = epsmin * (gp2 - gp1);
+    double auxc0 = epsmin * (gp20 - gp10);
+    double ucon = V->fact[1][t] * auxc;
+    double ucon0 = V->fact0[1][t] * auxc0;
+    qforce = ssvirr * sw * auxa;
+    W->cmap2[j1] += ucon;
+    W->uconf[typeij - 1] += sw * ucon;
+    W->uconf0[typeij - 1] += sw * ucon0;
+  } else {
+    qforce = 0.0;
+  }
+  if (!A->lskip_ewald) {
+    double alphar = A->alphal / auxa;
+    double qt = 1.0 / (1.0 + AS_QP * alphar);
+    double expcst = exp(-alphar * alphar);
+    double erfcst =
+        ((((AS_A5 * qt + AS_A4) * qt + AS_A3) * qt + AS_A2) * qt + AS_A1) *
+        qt * expcst;
+    double furpar = V->factq[1][t] * chrgei * A->charge[j];
+    double furpar0 = V->factq0[1][t] * chrgei * A->charge[j];
+    W->ucoul[typeij - 1] += sw * furpar * erfcst * auxaa;
+    W->ucoul0[typeij - 1] += sw * furpar0 * erfcst * auxa0;
+    W->cmap2[j1] += furpar * erfcst * auxaa;
+    qforce += furpar * erfcst * auxbb * sw +
+              furpar * A->twrtpi * alphar * expcst * auxa * auxa * auxaa * sw;
+  } else if (!A->ewald) {
+    double auxc = chrgei * A->charge[j] * auxaa;
+    double ssvir = V->factq[1][t] * auxc;
+    double ssvir0 = V->factq0[1][t] * chrgei * A->charge[j] * auxa0;
+    W->cmap2[j1] += ssvir;
+    W->ucoul[typeij - 1] += ssvir * sw;
+    W->ucoul0[typeij - 1] += ssvir0 * sw;
+    qforce += ssvir * sw * auxaa * auxaa;
+  }
+  W->fx[i1] += qforce * xc;
+  W->fy[i1] += qforce * yc;
+  W->fz[i1] += qforce * zc;
+  W->fx[j] -= qforce * xc;
+  W->fy[j] -= qforce * yc;
+  W->fz[j] -= qforce * zc;
+  W->st[0] += qforce * xc * xxcm;
+  W->st[1] += qforce * xc * yycm;
+  W->st[2] += qforce * xc * zzcm;
+  W->st[3] += qforce * yc * xxcm;
+  W->st[4] += qforce * yc * yycm;
+  W->st[5] += qforce * yc * zzcm;
+  W->st[6] += qforce * zc * xxcm;
+  W->st[7] += qforce * zc * yycm;
+  W->st[8] += qforce * zc * zzcm;
+}
+
+/* One group of force_alchemy's outer loop, src/force_alchemy.f:261-650:
+ * every partner in [rinn, rout0) is mapped once, with S = 1 on the
+ * non-switched band, and exclusions and fixed-mass pairs are always checked
+ * (there is no per-group fast path). */
+static int force_group_alch(const force_args* A, force_ws* W, int i,
+                            const int* lst, int m, int mbeg) {
+  const double* co = A->co;
+  double xpgi = A->xpg[i], ypgi = A->ypg[i], zpgi = A->zpg[i];
+  int map = 0, mp = 0;
+  int typei = A->ss_index[A->grppt[2 * i] - 1];
+  const double rout = sqrt(A->r2out);
+  for (int jj = mbeg; jj < m; jj++) {
+    int j = lst[jj] - 1;
+    double xgg = xpgi - A->xpg[j], ygg = ypgi - A->ypg[j], zgg = zpgi - A->zpg[j];
+    double xm = 2.0 * round(0.5 * xgg), ym = 2.0 * round(0.5 * ygg),
+           zm = 2.0 * round(0.5 * zgg);
+    xgg -= xm;
+    ygg -= ym;
+    zgg -= zm;
+    double xc = co[0] * xgg + co[3] * ygg + co[6] * zgg;
+    double yc = co[4] * ygg + co[7] * zgg;
+    double zc = co[8] * zgg;
+    double drj = xc * xc + yc * yc + zc * zc;
+    if (A->r2inn > 1.0e-5 && drj < A->r2neigh) W->nlist_out[map++] = j + 1;
+    if (A->rinn0 > rout) continue;
+    if (drj >= A->r2inn && drj < A->r2out0) {
+      W->xmap1[mp] = xm;
+      W->ymap1[mp] = ym;
+      W->zmap1[mp] = zm;
+      W->xmap2[mp] = xc;
+      W->ymap2[mp] = yc;
+      W->zmap2[mp] = zc;
+      W->drs[mp] = drj;
+      W->index1[mp] = j;
+      mp++;
+    }
+  }
+  int mapb = mp;
+  for (int jj = 0; jj < mapb; jj++) {
+    double d = W->drs[jj];
+    if (d < A->r2out && d >= A->r2inn0) {
+      W->swrs[jj] = 1.0;
+      W->dswrs[jj] = 0.0;
+    } else if (d >= A->r2out) {
+      double rsp = sqrt(d);
+      double auxa = (A->arsout1 + 2.0 * rsp) / A->arsout2;
+      double auxb = A->rout0 - rsp;
+      W->swrs[jj] = auxa * auxb * auxb;
+      W->dswrs[jj] = (-2.0 * auxa * auxb + 2.0 * auxb * auxb / A->arsout2) / rsp;
+    } else {
+      double rsp = sqrt(d);
+      double auxa = (A->arsinn1 + 2.0 * rsp) / A->arsinn2;
+      double auxb = A->rinn0 - rsp;
+      W->swrs[jj] = 1.0 - auxa * auxb * auxb;
+      W->dswrs[jj] = (2.0 * auxa * auxb - 2.0 * auxb * auxb / A->arsinn2) / rsp;
+    }
+    W->cmap2[jj] = 0.0;
+  }
+  if (mapb == 0) return map;
+  int g0 = A->grppt[2 * i] - 1, g1 = A->grppt[2 * i + 1] - 1;
+  for (int i1 = g0; i1 <= g1; i1++) {
+    const int* rec = A->mapnl + A->mapoff[i1];
+    int la = rec[0];
+    for (int q = 1; q <= la; q++) W->maplg[rec[q] - 1] = 0;
+    int p1 = A->atomp[i1] - 1;
+    for (int jj = 0; jj < mapb; jj++) {
+      int jg = W->index1[jj];
+      int typej = A->ss_index[A->grppt[2 * jg] - 1];
+      for (int j = A->grppt[2 * jg] - 1; j <= A->grppt[2 * jg + 1] - 1; j++) {
+        if (!(W->maplg[j] &&
+              (A->mass[j] < A->massinfty || A->mass[i1] < A->massinfty)))
+          continue;
+        alch_pair(A, W, i1, j, jj, A->xp0[i1], A->yp0[i1], A->zp0[i1],
+                  A->xpcm[p1], A->ypcm[p1], A->zpcm[p1], A->charge[i1],
+                  typei + typej - 1);
+      }
+    }
+    for (int q = 1; q <= la; q++) W->maplg[rec[q] - 1] = 1;
+  }
+  /* S'*V term, src/force_alchemy.f:552-622 (same as force) */
+  for (int jj = 0; jj < mapb; jj++) {
+    W->xmap3[jj] = -W->dswrs[jj] * W->cmap2[jj] * W->xmap2[jj];
+    W->ymap3[jj] = -W->dswrs[jj] * W->cmap2[jj] * W->ymap2[jj];
+    W->zmap3[jj] = -W->dswrs[jj] * W->cmap2[jj] * W->zmap2[jj];
+  }
+  for (int i1 = g0; i1 <= g1; i1++) {
+    double massi = A->gmass[i1];
+    int p1 = A->atomp[i1] - 1;
+    double xp1 = A->xpcm[p1], yp1 = A->ypcm[p1], zp1 = A->zpcm[p1];
+    for (int jj = 0; jj < mapb; jj++) {
+      W->fx[i1] += massi * W->xmap3[jj];
+      W->fy[i1] += massi * W->ymap3[jj];
+      W->fz[i1] += massi * W->zmap3[jj];
+      W->st[0] += massi * W->xmap3[jj] * xp1;
+      W->st[1] += massi * W->xmap3[jj] * yp1;
+      W->st[2] += massi * W->xmap3[jj] * zp1;
+      W->st[3] += massi * W->ymap3[jj] * xp1;
+      W->st[4] += massi * W->ymap3[jj] * yp1;
+      W->st[5] += massi * W->ymap3[jj] * zp1;
+      W->st[6] += massi * W->zmap3[jj] * xp1;
+      W->st[7] += massi * W->zmap3[jj] * yp1;
+      W->st[8] += massi * W->zmap3[jj] * zp1;
+    }
+  }
+  for (int jj = 0; jj < mapb; jj++) {
+    int j = W->index1[jj];
+    double xxcm = W->xmap1[jj], yycm = W->ymap1[jj], zzcm = W->zmap1[jj];
+    for (int j1 = A->grppt[2 * j] - 1; j1 <= A->grppt[2 * j + 1] - 1; j1++) {
+      double massj = A->gmass[j1];
+      W->fx[j1] -= massj * W->xmap3[jj];
+      W->fy[j1] -= massj * W->ymap3[jj];
+      W->fz[j1] -= massj * W->zmap3[jj];
+      int p2 = A->atomp[j1] - 1;
+      double xq = -(A->xpcm[p2] + xxcm) * massj;
+      double yq = -(A->ypcm[p2] + yycm) * massj;
+      double zq = -(A->zpcm[p2] + zzcm) * massj;
+      W->st[0] += W->xmap3[jj] * xq;
+      W->st[1] += W->xmap3[jj] * yq;
+      W->st[2] += W->xmap3[jj] * zq;
+      W->st[3] += W->ymap3[jj] * xq;
+      W->st[4] += W->ymap3[jj] * yq;
+      W->st[5] += W->ymap3[jj] * zq;
+      W->st[6] += W->zmap3[jj] * xq;
+      W->st[7] += W->zmap3[jj] * yq;
+      W->st[8] += W->zmap3[jj] * zq;
+    }
+  }
+  return map;
+}
+
+void orc_alch_set(double fact[2][9], double ladd, double lrm, int intramol,
+                  int ljintra, int qq) {
+  for (int k = 0; k < 2; k++)
+    for (int t = 0; t < 9; t++) fact[k][t] = 0.0;
+  const double la = fabs(ladd), lr = fabs(lrm);
+#define F(t, a, b) (fact[0][(t) + 4] = (a), fact[1][(t) + 4] = (b))
+  F(2, 0.0, 1.0);       /* normal-normal */
+  F(3, la, 1.0 - la);   /* normal-added */
+  F(-1, lr, 1.0 - lr);  /* normal-removed */
+  if (intramol && qq) {
+    F(4, la * la, 1.0 - la * la);
+    F(-4, lr * lr, 1.0 - lr * lr);
+  } else if (intramol && !ljintra) {
+    F(4, la, 1.0 - la);
+    F(-4, lr, 1.0 - lr);
+  } else {
+    F(4, 0.0, 1.0);
+    F(-4, 0.0, 1.0);
+  }
+  F(0, 0.0, 0.0); /* removed-added */
+#undef F
+}
+
 long orc_force(const int* ss_index, const double* xp0, const double* yp0,
                const double* zp0, const double* xpg, const double* ypg,
                const double* zpg, const double* charge, const int* nbtype,
@@ -545,8 +813,32 @@ long orc_force(const int* ss_index, const double* xp0, const double* yp0,
                double rtolinn, double rtolout, const double* gmass, int iz,
                const double* mass, double massinfty, int lskip_ewald,
                int ewald, int nthreads) {
+  return orc_force_ex(ss_index, xp0, yp0, zp0, xpg, ypg, zpg, charge, nbtype,
+                      type, ma, nato, atomg, xpcm, ypcm, zpcm, atomp, co,
+                      ecc12, ecc6, alphal, mapnl, ngrp, grppt, ue, fpx, fpy,
+                      fpz, stress, nnlpp, nnlpp1, cap1, rneigh, rinn, rout,
+                      rtolinn, rtolout, gmass, iz, mass, massinfty,
+                      lskip_ewald, ewald, nthreads, NULL, NULL);
+}
+
+long orc_force_ex(const int* ss_index, const double* xp0, const double* yp0,
+                  const double* zp0, const double* xpg, const double* ypg,
+                  const double* zpg, const double* charge, const int* nbtype,
+                  const int* type, int ma, int nato, const int* atomg,
+                  const double* xpcm, const double* ypcm, const double* zpcm,
+                  const int* atomp, const double* co, const double* ecc12,
+                  const double* ecc6, double alphal, const int* mapnl,
+                  int ngrp, const int* grppt, double* ue, double* fpx,
+                  double* fpy, double* fpz, double* stress, const int* nnlpp,
+                  int* nnlpp1, long cap1, double rneigh, double rinn,
+                  double rout, double rtolinn, double rtolout,
+                  const double* gmass, int iz, const double* mass,
+                  double massinfty, int lskip_ewald, int ewald, int nthreads,
+                  const orc_variant* V, double* extra) {
   force_args A;
   memset(&A, 0, sizeof(A));
+  A.V = (V && V->mode != 0) ? V : NULL;
+  const int alch = A.V && A.V->mode == 2;
   A.ss_index = ss_index;
   A.xp0 = xp0;
   A.yp0 = yp0;
@@ -621,6 +913,9 @@ long orc_force(const int* ss_index, const double* xp0, const double* yp0,
   int** nextlst = (int**)calloc(ngrp, sizeof(int*));
 
   double tot_conf[3] = {0, 0, 0}, tot_coul[3] = {0, 0, 0}, tot_st[9] = {0};
+  double tot_seg = 0.0, tot_conf0[3] = {0, 0, 0}, tot_coul0[3] = {0, 0, 0};
+  if (extra)
+    for (int k = 0; k < 4; k++) extra[k] = 0.0;
   double* gfx = (double*)calloc(nato, sizeof(double));
   double* gfy = (double*)calloc(nato, sizeof(double));
   double* gfz = (double*)calloc(nato, sizeof(double));
@@ -643,6 +938,7 @@ long orc_force(const int* ss_index, const double* xp0, const double* yp0,
     W.index0 = (int*)malloc(sizeof(int) * cap);
     W.index1 = (int*)malloc(sizeof(int) * cap);
     W.nlist_out = (int*)malloc(sizeof(int) * cap);
+    W.drs = (double*)malloc(sizeof(double) * cap);
     double** dp[] = {&W.xmap0, &W.ymap0, &W.zmap0, &W.xmap1, &W.ymap1,
                      &W.zmap1, &W.xmap2, &W.ymap2, &W.zmap2, &W.cmap2,
                      &W.swrs,  &W.dswrs, &W.xmap3, &W.ymap3, &W.zmap3};
@@ -657,7 +953,8 @@ long orc_force(const int* ss_index, const double* xp0, const double* yp0,
       const int* lst = nnlpp + loff[i] + 1;
       int m = nnlpp[loff[i]];
       int mbeg = (iz == 0) ? i + 1 : 0;
-      int map = force_group(&A, &W, i, lst, m, mbeg);
+      int map = alch ? force_group_alch(&A, &W, i, lst, m, mbeg)
+                     : force_group(&A, &W, i, lst, m, mbeg);
       if (want_next) {
         nextcnt[i] = map;
         nextlst[i] = (int*)malloc(sizeof(int) * (map > 0 ? map : 1));
@@ -678,6 +975,11 @@ long orc_force(const int* ss_index, const double* xp0, const double* yp0,
         tot_coul[k] += W.ucoul[k];
       }
       for (int k = 0; k < 9; k++) tot_st[k] += W.st[k];
+      tot_seg += W.seg_ene;
+      for (int k = 0; k < 3; k++) {
+        tot_conf0[k] += W.uconf0[k];
+        tot_coul0[k] += W.ucoul0[k];
+      }
     }
     free(W.fx);
     free(W.fy);
@@ -687,6 +989,7 @@ long orc_force(const int* ss_index, const double* xp0, const double* yp0,
     free(W.index0);
     free(W.index1);
     free(W.nlist_out);
+    free(W.drs);
     for (unsigned k = 0; k < sizeof(dp) / sizeof(dp[0]); k++) free(*dp[k]);
   }
   long ncount1 = 0;
@@ -717,6 +1020,19 @@ long orc_force(const int* ss_index, const double* xp0, const double* yp0,
     ue[3] = tot_coul[0];
     ue[4] = tot_coul[2];
     ue[5] = tot_coul[1];
+    if (extra) {
+      extra[0] = tot_seg;
+      /* src/force_alchemy.f:683-688 */
+      double dwrk = 0.0;
+      for (int k = 0; k < 3; k++) {
+        double auxa = tot_coul[k] - tot_coul0[k];
+        double auxb = tot_conf[k] - tot_conf0[k];
+        dwrk = dwrk + auxa + auxb;
+      }
+      extra[1] = alch ? dwrk : 0.0;
+      extra[2] = tot_conf0[0] + tot_conf0[1] + tot_conf0[2];
+      extra[3] = tot_coul0[0] + tot_coul0[1] + tot_coul0[2];
+    }
     /* st(i,j) row-major in tot_st[3*i+j]; stress(i,j) += sum_k st(i,k) co(j,k) */
     for (int a = 0; a < 3; a++)
       for (int b = 0; b < 3; b++)

@@ -77,6 +77,60 @@ long orc_force(const int* ss_index, const double* xp0, const double* yp0,
                const double* mass, double massinfty, int lskip_ewald,
                int ewald, int nthreads);
 
+/* Variants of the shell kernel selected by mts_forces (src/mts_forces.f:118-153).
+ *  mode 1  force_rem (src/force_REM.f): pairs with seg_select(kind, rematom,
+ *          i, j) (src/rem.f90:631-645) have their force, and their share of
+ *          the S'V switching term, multiplied by rem_factor(3); the energies
+ *          stay unscaled and seg_ene collects the selected pairs' LJ +
+ *          Coulomb energy (switched pairs weighted by S).  In shells that skip
+ *          Ewald (lskip_ewald with Ewald on) the reference adds a Coulomb term
+ *          left undefined; it is taken as 0 here.
+ *  mode 2  force_alchemy (src/force_alchemy.f): GROMOS-like soft core with
+ *          per-atom rmin/epsm, pair class t = ss_alchemy(i) + ss_alchemy(j)
+ *          in -4..4 and factor tables alch_fact(1:2, t) from alch_set
+ *          (src/force_alchemy_shifted.f:732-790), for the current (fact,
+ *          factq) and previous (fact0, factq0) lambdas.  Every pair in
+ *          [rinn, rout0) goes through the switched loop; the work
+ *          dwrk = U(lambda) - U(lambda0) (src/force_alchemy.f:683-688).
+ * Tables are indexed [k][t + 4], k = 0 for alch_fact(1, t) (soft-core
+ * shift), k = 1 for alch_fact(2, t) (scale). */
+typedef struct {
+  int mode;
+  const unsigned char* rematom; /* [nato], 1 = atom of the REM segment */
+  int rem_kind;                 /* 0 either, 1 both, 2 exactly one */
+  double rem_factor;            /* rem_factor(3) */
+  const int* ss_alchemy;        /* [nato]: 1 normal, 2 added, -2 removed */
+  const double* rmin;           /* [nato] */
+  const double* epsm;           /* [nato] */
+  double qsoft, ljsoft;
+  int opls;                     /* sigma = 2 sqrt(rmin_i rmin_j) if set */
+  double fact[2][9], factq[2][9], fact0[2][9], factq0[2][9];
+} orc_variant;
+
+/* force with a variant (NULL or mode 0: force).  extra[4] (may be NULL)
+ * receives seg_ene (mode 1), dwrk (mode 2), and the lambda0 LJ and Coulomb
+ * energy totals (mode 2). */
+long orc_force_ex(const int* ss_index, const double* xp0, const double* yp0,
+                  const double* zp0, const double* xpg, const double* ypg,
+                  const double* zpg, const double* charge, const int* nbtype,
+                  const int* type, int ma, int nato, const int* atomg,
+                  const double* xpcm, const double* ypcm, const double* zpcm,
+                  const int* atomp, const double* co, const double* ecc12,
+                  const double* ecc6, double alphal, const int* mapnl,
+                  int ngrp, const int* grppt, double* ue, double* fpx,
+                  double* fpy, double* fpz, double* stress, const int* nnlpp,
+                  int* nnlpp1, long cap1, double rneigh, double rinn,
+                  double rout, double rtolinn, double rtolout,
+                  const double* gmass, int iz, const double* mass,
+                  double massinfty, int lskip_ewald, int ewald, int nthreads,
+                  const orc_variant* V, double* extra);
+
+/* alch_set, src/force_alchemy_shifted.f:732-790: fact[k][t+4] for one
+ * (ladd, lrm) pair; qq selects the Coulomb form of the alchemical-alchemical
+ * entries. */
+void orc_alch_set(double fact[2][9], double ladd, double lrm, int intramol,
+                  int ljintra, int qq);
+
 /* PME (FFTW build): load_bsp_moduli + DFTMOD, src/pme_fftw3.f90:165-230 */
 void orc_load_bsp_moduli(double* bsp_mod1, double* bsp_mod2, double* bsp_mod3,
                          int nfft1, int nfft2, int nfft3, int order);

@@ -49,6 +49,9 @@ def lib():
                                 _D, _D, C.c_double, _I, C.c_int, _I, _D, _D, _D, _D, _D, _I, _I, C.c_long,
                                 C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, _D, C.c_int, _D,
                                 C.c_double, C.c_int, C.c_int, C.c_int]
+        L.orc_force_ex.restype = C.c_long
+        L.orc_force_ex.argtypes = L.orc_force.argtypes + [C.POINTER(Variant), _D]
+        L.orc_alch_set.argtypes = [C.POINTER(C.c_double * 18), C.c_double, C.c_double, C.c_int, C.c_int, C.c_int]
         L.orc_load_bsp_moduli.argtypes = [_D, _D, _D, C.c_int, C.c_int, C.c_int, C.c_int]
         L.orc_fill_bspline.argtypes = [C.c_double, C.c_int, _D, _D]
         L.orc_fft1d.argtypes = [C.c_int, _D, C.c_int]
@@ -67,6 +70,23 @@ def lib():
         L.orc_fnbgrp.argtypes = [_I, _D, _D, _D, _D, _I, _D, _D, C.c_int, C.c_double, _I, C.c_int, _D, _D, _D, _D]
         _lib = L
     return _lib
+
+
+class Variant(C.Structure):
+    """orc_variant (orac_oracle.h): REM segment or soft-core alchemy."""
+
+    _fields_ = [("mode", C.c_int), ("rematom", C.c_void_p), ("rem_kind", C.c_int), ("rem_factor", C.c_double),
+                ("ss_alchemy", C.c_void_p), ("rmin", C.c_void_p), ("epsm", C.c_void_p), ("qsoft", C.c_double),
+                ("ljsoft", C.c_double), ("opls", C.c_int), ("fact", C.c_double * 18), ("factq", C.c_double * 18),
+                ("fact0", C.c_double * 18), ("factq0", C.c_double * 18)]
+
+
+def alch_set(ladd, lrm, intramol=False, ljintra=False, qq=False):
+    """alch_set (src/force_alchemy_shifted.f:732-790) as a (2, 9) table
+    [k, t + 4]."""
+    t = (C.c_double * 18)()
+    lib().orc_alch_set(C.byref(t), ladd, lrm, int(intramol), int(ljintra), int(qq))
+    return np.array(t[:]).reshape(2, 9)
 
 
 def _f(a):
@@ -94,7 +114,53 @@ class Oracle:
         self.ewald = ewald
         self.L = lib()
         self.lists = {}
+        self.variant = None
+        self.last_extra = np.zeros(4)
         self._prep()
+
+    # -------------------------------------------------------- variants
+    def set_rem(self, rematom, kind=0, factor=1.0):
+        """force_rem (src/force_REM.f) for every later shell call."""
+        self._rem = np.ascontiguousarray(rematom, dtype=np.uint8)
+        v = Variant()
+        v.mode = 1
+        v.rematom = self._rem.ctypes.data
+        v.rem_kind = int(kind)
+        v.rem_factor = float(factor)
+        self.variant = v
+
+    def set_alchemy(self, ss_alchemy, qsoft=0.5, ljsoft=0.5, opls=False):
+        """force_alchemy (src/force_alchemy.f) with ORAC's per-atom soft-core
+        parameters (src/mtsmd.f:1298-1303); lambdas start at 0 (all on)."""
+        rmin, epsm = self.s.alchemy_params()
+        self._alch = (_i(ss_alchemy), _f(rmin), _f(epsm))
+        v = Variant()
+        v.mode = 2
+        v.ss_alchemy = self._alch[0].ctypes.data
+        v.rmin = self._alch[1].ctypes.data
+        v.epsm = self._alch[2].ctypes.data
+        v.qsoft = float(qsoft)
+        v.ljsoft = float(ljsoft)
+        v.opls = int(opls)
+        self.variant = v
+        self.set_lambda(0.0, 0.0, 0.0, 0.0)
+
+    def set_lambda(self, ladd, lrm, laddq, lrmq, ladd0=None, lrm0=None, laddq0=None, lrmq0=None, intramol=False,
+                   ljintra=False):
+        """Current and previous lambdas (cpropar ladd..lrmq0); the previous
+        ones default to the current (zero work)."""
+        v = self.variant
+        ladd0 = ladd if ladd0 is None else ladd0
+        lrm0 = lrm if lrm0 is None else lrm0
+        laddq0 = laddq if laddq0 is None else laddq0
+        lrmq0 = lrmq if lrmq0 is None else lrmq0
+        v.fact[:] = alch_set(ladd, lrm, intramol, ljintra, False).ravel()
+        v.factq[:] = alch_set(laddq, lrmq, intramol, ljintra, True).ravel()
+        v.fact0[:] = alch_set(ladd0, lrm0, intramol, ljintra, False).ravel()
+        v.factq0[:] = alch_set(laddq0, lrmq0, intramol, ljintra, True).ravel()
+
+    def clear_variant(self):
+        self.variant = None
 
     def _prep(self):
         s = self.s
@@ -154,12 +220,15 @@ class Oracle:
         if iz == 0:  # one shared list read from i+1: up to ngrp(ngrp-1)/2 pairs
             cap1 = s.ngrp * (s.ngrp + 1) // 2 + s.ngrp + 16
         nxt = np.zeros(cap1, np.int32)
-        n1 = self.L.orc_force(_i(s.ss_index), self.xp0, self.yp0, self.zp0, self.xpg, self.ypg, self.zpg,
-                              _f(s.charge), _i(s.nbtype), self.type_cm, s.ntype, s.ntap, _i(s.atomg), self.xpcm,
-                              self.ypcm, self.zpcm, _i(s.atomp), self.co, _f(s.ecc12), _f(s.ecc6), s.alphal,
-                              _i(s.mapnl), s.ngrp, self.grppt, ue, fx, fy, fz, st, nnlpp, nxt, cap1, rneigh, rinn,
-                              rout, rtolinn, rtolout, _f(s.pmass), iz, _f(s.mass), s.massinfty, int(lskip),
-                              int(self.ewald), self.nthreads)
+        extra = np.zeros(4)
+        n1 = self.L.orc_force_ex(_i(s.ss_index), self.xp0, self.yp0, self.zp0, self.xpg, self.ypg, self.zpg,
+                                 _f(s.charge), _i(s.nbtype), self.type_cm, s.ntype, s.ntap, _i(s.atomg), self.xpcm,
+                                 self.ypcm, self.zpcm, _i(s.atomp), self.co, _f(s.ecc12), _f(s.ecc6), s.alphal,
+                                 _i(s.mapnl), s.ngrp, self.grppt, ue, fx, fy, fz, st, nnlpp, nxt, cap1, rneigh, rinn,
+                                 rout, rtolinn, rtolout, _f(s.pmass), iz, _f(s.mass), s.massinfty, int(lskip),
+                                 int(self.ewald), self.nthreads,
+                                 C.byref(self.variant) if self.variant is not None else None, extra)
+        self.last_extra = extra
         if n1 < 0:
             raise RuntimeError("next list overflow")
         nxt = nxt[:n1].copy() if rinn > 1e-5 else None

@@ -28,7 +28,7 @@ def small_box(nw=64, box=16.5, seed=0):
     s = systems.water_box(nwat=nw, box=box, lattice=4, jitter=0.25, seeds=(seed + 1, seed + 2, seed + 3, seed + 4),
                           nfft=(16, 16, 16))
     s.ncell = None
-    s.shells = systems.Shells(rcutm=3.0, rtolm=0.4, rneim=0.4, rcutl=5.0, rtoll=0.4, rneil=0.4, rcuth=7.0,
+    s.shells = systems.Shells(rcutm=4.0, rtolm=0.4, rneim=0.4, rcutl=5.5, rtoll=0.4, rneil=0.4, rcuth=7.0,
                               rtolh=0.5, rneih=0.5)
     s.name = "water64"
     return s
