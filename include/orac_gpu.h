@@ -173,6 +173,47 @@ int orac_gpu_ferrf(orac_gpu_ctx* ctx, double fudge, const double* x0,
 int orac_gpu_cself(orac_gpu_ctx* ctx, double kcut, double* self_slt,
                    double* self_slv);
 
+/* Shell-kernel variants ----------------------------------------------------
+ * mts_forces dispatches to force_rem, force_alchemy or force
+ * (src/mts_forces.f:118-153) on the module flags rem_segment and alchemy;
+ * here the context carries the flag and every later shell evaluation
+ * (orac_gpu_mts_forces, _mts_forces_dev and the MD driver) uses it.
+ *
+ * orac_gpu_set_rem: force_rem (src/force_REM.f).  rematom[ntap] (Fortran
+ * LOGICAL as int, module rem) marks the REM segment; pairs passing
+ * seg_select(kind, ...) (src/rem.f90:631-645; kind 0 either atom, 1 both,
+ * 2 exactly one) have their force and S'V share scaled by rem_factor(3);
+ * energies stay unscaled and seg_ene (rem_hnb/lnb/mnb_energy) collects the
+ * selected pairs.  rematom = NULL returns to the standard kernel. */
+int orac_gpu_set_rem(orac_gpu_ctx* ctx, const int* rematom, int kind,
+                     double rem_factor);
+
+/* orac_gpu_set_alchemy: force_alchemy (src/force_alchemy.f), soft-core
+ * GROMOS-like form.  ss_alchemy[ntap] (cpropar): 1 normal, 2 added, -2
+ * removed (src/initialize_lambda.f:35,49); rmin, epsm per atom in internal
+ * units as src/mtsmd.f:1298-1303 computes them; qsoft, ljsoft of SOFT-CORE;
+ * opls selects the geometric sigma (ffield_type "opls").  Lambdas start at 0.
+ * ss_alchemy = NULL returns to the standard kernel. */
+int orac_gpu_set_alchemy(orac_gpu_ctx* ctx, const int* ss_alchemy,
+                         const double* rmin, const double* epsm, double qsoft,
+                         double ljsoft, int opls);
+
+/* orac_gpu_set_lambda: cpropar's ladd, lrm, laddq, lrmq and their previous
+ * values ladd0..lrmq0 (lam[8] in that order), with intramol / ljintra of
+ * alch_set (src/force_alchemy_shifted.f:732-790).  The PME charges become
+ * (1 - |lambdaq_i|) q_i (src/mts_furier_alchemy.f:75-88).  dlam[4] (may be
+ * NULL) gives d(ladd, lrm, laddq, lrmq)/dlambda of a control lambda: energy
+ * evaluations then also return dU/dlambda. */
+int orac_gpu_set_lambda(orac_gpu_ctx* ctx, const double* lam, int intramol,
+                        int ljintra, const double* dlam);
+
+/* Outputs of the last energy-evaluating shell call and fft_pme under a
+ * variant (module globals in ORAC): out[0] seg_ene (REM), out[1] dwrk =
+ * U(lambda) - U(lambda0) of the shell (src/force_alchemy.f:683-688), out[2]
+ * and out[3] the LJ and Coulomb energy at lambda0, out[4] dU/dlambda of the
+ * shell, out[5] the PME work eer - eer0 (src/do_pmesh_alchemy.f90:78). */
+int orac_gpu_variant_energies(orac_gpu_ctx* ctx, double* out);
+
 /* Device-resident entry points -------------------------------------------
  * The same computations on device pointers (CUDA global memory, FP64 SoA),
  * for drivers that keep the state in HBM.  Forces are accumulated into the

@@ -182,6 +182,7 @@ int shell_run_r(orac_gpu_ctx* ctx, char rshell, const ShellRadii& radii, const d
   a.acc = ctx->d_acc;
   a.natom = ctx->N;
   a.wcnt = ctx->d_wcnt;
+  variant_fill(ctx, &a);
   const bool want_e = (flags & SH_ENERGY) && d_e, want_s = (flags & SH_STRESS) && d_stress;
   a.energy = want_e ? 1 : 0;
   a.stress = want_s ? 1 : 0;
@@ -197,6 +198,8 @@ int shell_run_r(orac_gpu_ctx* ctx, char rshell, const ShellRadii& radii, const d
                                            want_s ? d_stress : nullptr);
     CKL();
   }
+  if (want_e && ctx->variant != VAR_STD)
+    if (int rc = variant_out_launch(ctx, a.forces_on)) return rc;
   if (a.next_on) ctx->lists[s.out].valid = true;
   return ORAC_OK;
 }
@@ -249,6 +252,7 @@ int orac_gpu_destroy(orac_gpu_ctx* ctx) {
   for (void* p : aps)
     if (p) cudaFree(p);
   if (ctx->d_wcnt) cudaFree(ctx->d_wcnt);
+  variant_free(ctx);
   for (auto& e : ctx->prof_ev) cudaEventDestroy(e);
   for (int q = 0; q < 3; q++) {
     if (q == 0 && ctx->lists[q].off) cudaFree(ctx->lists[q].off);

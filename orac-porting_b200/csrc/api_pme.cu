@@ -69,7 +69,7 @@ int fft_pme_device(orac_gpu_ctx* ctx, const double* d_sxyz, const double* d_mol,
   CKL();
   double recip[9];
   recip_of(ctx->oc, recip);
-  return pme_run(ctx, N, S.cart, ctx->d_aqd, recip, ctx->volume, ctx->alphal, d_f, d_eout, d_sxyz, d_mol);
+  return pme_run(ctx, N, S.cart, ctx->pme_q(), recip, ctx->volume, ctx->alphal, d_f, d_eout, d_sxyz, d_mol);
 }
 
 extern "C" {
@@ -101,6 +101,21 @@ int orac_gpu_fft_pme(orac_gpu_ctx* ctx, const double* xp, const double* yp, cons
   }
   const double* e = f + 3 * (size_t)N;
   *eer = 0.5 * e[0];
+  ctx->pme_dwrk = 0.0;
+  if (ctx->variant == VAR_ALCH && ctx->q0_differs) {
+    // do_pmesh_alchemy (src/do_pmesh_alchemy.f90:66-87): a second grid of the
+    // lambda0 charges gives eer0; the forces come from the lambda grid only
+    double recip[9];
+    recip_of(ctx->oc, recip);
+    CK(cudaMemsetAsync(ctx->d_fout, 0, sizeof(double) * 3 * (size_t)N, ctx->stream));
+    if (int rc = pme_run(ctx, N, S.cart, ctx->d_q0, recip, ctx->volume, ctx->alphal, ctx->d_fout, S.eout, nullptr,
+                         nullptr))  // both already copied out above
+      return rc;
+    double e0 = 0.0;
+    CK(cudaMemcpyAsync(&e0, S.eout, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->pme_dwrk = *eer - 0.5 * e0;
+  }
   if (pressure) {
     // vir (symmetric, x0.5), src/scalar_sum.f:125-133; stressc(a,b) += -vir(a,b) + stc(a,b)
     const double vir[9] = {0.5 * e[1], 0.5 * e[4], 0.5 * e[5], 0.5 * e[4], 0.5 * e[2],

@@ -1,0 +1,240 @@
+// Variants of the shell kernel: the REM segment scaling of force_rem
+// (src/force_REM.f, seg_select src/rem.f90:631-645) and the soft-core
+// alchemy of force_alchemy (src/force_alchemy.f with alch_set,
+// src/force_alchemy_shifted.f:732-790), selected as mts_forces does
+// (src/mts_forces.f:118-153).
+#include <cmath>
+
+#include "common.cuh"
+
+namespace {
+
+// alch_set: [0][t+4] soft-core shift, [1][t+4] scale
+void alch_set(double f[2][9], double ladd, double lrm, int intramol, int ljintra, int qq) {
+  for (int k = 0; k < 2; k++)
+    for (int t = 0; t < 9; t++) f[k][t] = 0.0;
+  const double la = std::fabs(ladd), lr = std::fabs(lrm);
+  auto put = [&](int t, double a, double b) {
+    f[0][t + 4] = a;
+    f[1][t + 4] = b;
+  };
+  put(2, 0.0, 1.0);
+  put(3, la, 1.0 - la);
+  put(-1, lr, 1.0 - lr);
+  if (intramol && qq) {
+    put(4, la * la, 1.0 - la * la);
+    put(-4, lr * lr, 1.0 - lr * lr);
+  } else if (intramol && !ljintra) {
+    put(4, la, 1.0 - la);
+    put(-4, lr, 1.0 - lr);
+  } else {
+    put(4, 0.0, 1.0);
+    put(-4, 0.0, 1.0);
+  }
+  put(0, 0.0, 0.0);
+}
+
+// derivative of alch_set's tables with respect to a control lambda that
+// moves ladd and lrm at rates dla and dlr (d|l|/dl taken as +1 at l = 0)
+void alch_set_d(double d[2][9], double ladd, double lrm, double dla, double dlr, int intramol, int ljintra, int qq) {
+  for (int k = 0; k < 2; k++)
+    for (int t = 0; t < 9; t++) d[k][t] = 0.0;
+  const double sa = ladd < 0 ? -1.0 : 1.0, sr = lrm < 0 ? -1.0 : 1.0;
+  const double la = std::fabs(ladd), lr = std::fabs(lrm);
+  auto put = [&](int t, double a, double b) {
+    d[0][t + 4] = a;
+    d[1][t + 4] = b;
+  };
+  put(3, sa * dla, -sa * dla);
+  put(-1, sr * dlr, -sr * dlr);
+  if (intramol && qq) {
+    put(4, 2.0 * la * sa * dla, -2.0 * la * sa * dla);
+    put(-4, 2.0 * lr * sr * dlr, -2.0 * lr * sr * dlr);
+  } else if (intramol && !ljintra) {
+    put(4, sa * dla, -sa * dla);
+    put(-4, sr * dlr, -sr * dlr);
+  }
+}
+
+// chrgec of mts_furier_alchemy (src/mts_furier_alchemy.f:75-88)
+double scaled_charge(double q, double lq) {
+  const double a = std::fabs(lq);
+  if (a == 1.0) return 0.0;
+  if (a == 0.0) return q;
+  return (1.0 - a) * q;
+}
+
+__global__ void k_variant_out(const double* __restrict__ acc, int variant, int forces_on, double* __restrict__ x) {
+  if (threadIdx.x != 0) return;
+  for (int k = 0; k < 5; k++) x[k] = 0.0;
+  if (!forces_on) return;
+  if (variant == VAR_REM) x[0] = acc[ACC_X];
+  if (variant == VAR_ALCH) {
+    double u = 0.0;
+    for (int k = 0; k < 6; k++) u += acc[ACC_CONF + k];
+    x[1] = u - acc[ACC_X] - acc[ACC_X + 1];
+    x[2] = acc[ACC_X];
+    x[3] = acc[ACC_X + 1];
+    x[4] = acc[ACC_X + 2];
+  }
+}
+
+int build_vflag(orac_gpu_ctx* ctx) {
+  const int N = ctx->N;
+  ctx->h_vflag.assign(N, 0);
+  for (int a = 0; a < N; a++) {
+    unsigned char f = 0;
+    if (ctx->h_mass[a] >= ctx->massinfty) f |= VF_MINF;
+    if (!ctx->h_rem.empty() && ctx->h_rem[a]) f |= VF_REM;
+    const int ss = ctx->h_ssal.empty() ? 1 : ctx->h_ssal[a];
+    f |= (unsigned char)((ss + 4) << VF_SSHIFT);
+    ctx->h_vflag[a] = f;
+  }
+  if (!ctx->d_vflag && dev_alloc(ctx, &ctx->d_vflag, N)) return ORAC_ERR_CUDA;
+  CK(cudaMemcpy(ctx->d_vflag, ctx->h_vflag.data(), N, cudaMemcpyHostToDevice));
+  return ORAC_OK;
+}
+
+int upload_alch_charges(orac_gpu_ctx* ctx) {
+  const int N = ctx->N;
+  std::vector<double> qc(N), q0(N);
+  for (int a = 0; a < N; a++) {
+    const int ss = ctx->h_ssal[a];
+    // lambdaq of added atoms is laddq, of removed atoms -lrmq (src/mtsmd.f:747,755)
+    const double lq = ss == 2 ? ctx->lam[2] : (ss == -2 ? -ctx->lam[3] : 0.0);
+    const double lq0 = ss == 2 ? ctx->lam[6] : (ss == -2 ? -ctx->lam[7] : 0.0);
+    qc[a] = scaled_charge(ctx->h_charge[a], lq);
+    q0[a] = scaled_charge(ctx->h_charge[a], lq0);
+  }
+  if (!ctx->d_qc && (dev_alloc(ctx, &ctx->d_qc, N) || dev_alloc(ctx, &ctx->d_q0, N))) return ORAC_ERR_CUDA;
+  CK(cudaMemcpy(ctx->d_qc, qc.data(), sizeof(double) * N, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(ctx->d_q0, q0.data(), sizeof(double) * N, cudaMemcpyHostToDevice));
+  ctx->q0_differs = qc != q0;
+  return ORAC_OK;
+}
+
+}  // namespace
+
+void variant_fill(const orac_gpu_ctx* ctx, PairArgs* a) {
+  a->variant = ctx->variant;
+  if (ctx->variant == VAR_STD) return;
+  a->vflag = ctx->d_vflag;
+  a->rem_kind = ctx->rem_kind;
+  a->rem_factor = (float)ctx->rem_factor;
+  if (ctx->variant == VAR_ALCH) {
+    a->soft = ctx->d_soft;
+    a->softd = ctx->d_softd;
+    a->at = ctx->at;
+    a->qsoft = (float)ctx->at.qsoft;
+    a->ljsoft = (float)ctx->at.ljsoft;
+    for (int k = 0; k < 2; k++)
+      for (int t = 0; t < 9; t++) {
+        a->af[k][t] = (float)ctx->at.f[k][t];
+        a->afq[k][t] = (float)ctx->at.fq[k][t];
+      }
+  }
+}
+
+int variant_out_launch(orac_gpu_ctx* ctx, int forces_on) {
+  if (!ctx->d_xtra && dev_alloc(ctx, &ctx->d_xtra, 8)) return ORAC_ERR_CUDA;
+  k_variant_out<<<1, 32, 0, ctx->stream>>>(ctx->d_acc, ctx->variant, forces_on, ctx->d_xtra);
+  CKL();
+  return ORAC_OK;
+}
+
+void variant_free(orac_gpu_ctx* ctx) {
+  void* p[] = {ctx->d_vflag, ctx->d_soft, ctx->d_softd, ctx->d_qc, ctx->d_q0, ctx->d_xtra};
+  for (void* q : p)
+    if (q) cudaFree(q);
+}
+
+extern "C" {
+
+int orac_gpu_set_rem(orac_gpu_ctx* ctx, const int* rematom, int kind, double rem_factor) {
+  if (!ctx || !ctx->have_topo) return ctx ? ctx_fail(ctx, ORAC_ERR_STATE, "topology not set") : ORAC_ERR_PARAM;
+  CK(cudaSetDevice(ctx->device));
+  if (!rematom) {
+    if (ctx->variant == VAR_REM) ctx->variant = VAR_STD;
+    ctx->h_rem.clear();
+    return ORAC_OK;
+  }
+  if (kind < 0 || kind > 2) return ctx_fail(ctx, ORAC_ERR_PARAM, "REM segment kind %d (0, 1 or 2)", kind);
+  if (!(rem_factor >= 0.0)) return ctx_fail(ctx, ORAC_ERR_PARAM, "rem_factor %g", rem_factor);
+  ctx->h_rem.assign(ctx->N, 0);
+  for (int a = 0; a < ctx->N; a++) ctx->h_rem[a] = rematom[a] ? 1 : 0;
+  ctx->rem_kind = kind;
+  ctx->rem_factor = rem_factor;
+  if (int rc = build_vflag(ctx)) return rc;
+  ctx->variant = VAR_REM;
+  return ORAC_OK;
+}
+
+int orac_gpu_set_alchemy(orac_gpu_ctx* ctx, const int* ss_alchemy, const double* rmin, const double* epsm,
+                         double qsoft, double ljsoft, int opls) {
+  if (!ctx || !ctx->have_topo) return ctx ? ctx_fail(ctx, ORAC_ERR_STATE, "topology not set") : ORAC_ERR_PARAM;
+  CK(cudaSetDevice(ctx->device));
+  if (!ss_alchemy) {
+    if (ctx->variant == VAR_ALCH) ctx->variant = VAR_STD;
+    ctx->h_ssal.clear();
+    return ORAC_OK;
+  }
+  if (!rmin || !epsm) return ctx_fail(ctx, ORAC_ERR_PARAM, "rmin and epsm are required");
+  const int N = ctx->N;
+  std::vector<float2> sf(N);
+  std::vector<double2> sd(N);
+  for (int a = 0; a < N; a++) {
+    const int s = ss_alchemy[a];
+    if (s != 1 && s != 2 && s != -2)
+      return ctx_fail(ctx, ORAC_ERR_PARAM, "ss_alchemy(%d) = %d (1 normal, 2 added, -2 removed)", a + 1, s);
+    if (!(rmin[a] >= 0.0) || !(epsm[a] >= 0.0))
+      return ctx_fail(ctx, ORAC_ERR_PARAM, "rmin/epsm of atom %d", a + 1);
+    sf[a] = make_float2((float)rmin[a], (float)(2.0 * std::sqrt(epsm[a])));
+    sd[a] = make_double2(rmin[a], epsm[a]);
+  }
+  ctx->h_ssal.assign(ss_alchemy, ss_alchemy + N);
+  if (!ctx->d_soft && (dev_alloc(ctx, &ctx->d_soft, N) || dev_alloc(ctx, &ctx->d_softd, N))) return ORAC_ERR_CUDA;
+  CK(cudaMemcpy(ctx->d_soft, sf.data(), sizeof(float2) * N, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(ctx->d_softd, sd.data(), sizeof(double2) * N, cudaMemcpyHostToDevice));
+  ctx->at.qsoft = qsoft;
+  ctx->at.ljsoft = ljsoft;
+  ctx->at.opls = opls ? 1 : 0;
+  if (int rc = build_vflag(ctx)) return rc;
+  ctx->variant = VAR_ALCH;
+  const double zero[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  return orac_gpu_set_lambda(ctx, zero, 0, 0, nullptr);
+}
+
+int orac_gpu_set_lambda(orac_gpu_ctx* ctx, const double* lam, int intramol, int ljintra, const double* dlam) {
+  if (!ctx) return ORAC_ERR_PARAM;
+  if (ctx->h_ssal.empty()) return ctx_fail(ctx, ORAC_ERR_STATE, "orac_gpu_set_alchemy first");
+  if (!lam) return ctx_fail(ctx, ORAC_ERR_PARAM, "lam is required");
+  for (int k = 0; k < 8; k++)
+    if (!(std::fabs(lam[k]) <= 1.0)) return ctx_fail(ctx, ORAC_ERR_PARAM, "lambda %d = %g outside [-1, 1]", k, lam[k]);
+  CK(cudaSetDevice(ctx->device));
+  for (int k = 0; k < 8; k++) ctx->lam[k] = lam[k];
+  const double d0[4] = {0, 0, 0, 0};
+  const double* d = dlam ? dlam : d0;
+  AlchTables& T = ctx->at;
+  alch_set(T.f, lam[0], lam[1], intramol, ljintra, 0);
+  alch_set(T.fq, lam[2], lam[3], intramol, ljintra, 1);
+  alch_set(T.f0, lam[4], lam[5], intramol, ljintra, 0);
+  alch_set(T.fq0, lam[6], lam[7], intramol, ljintra, 1);
+  alch_set_d(T.df, lam[0], lam[1], d[0], d[1], intramol, ljintra, 0);
+  alch_set_d(T.dfq, lam[2], lam[3], d[2], d[3], intramol, ljintra, 1);
+  return upload_alch_charges(ctx);
+}
+
+int orac_gpu_variant_energies(orac_gpu_ctx* ctx, double* out) {
+  if (!ctx || !out) return ORAC_ERR_PARAM;
+  CK(cudaSetDevice(ctx->device));
+  double x[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  if (ctx->d_xtra) {
+    CK(cudaMemcpyAsync(x, ctx->d_xtra, sizeof(double) * 5, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+  }
+  for (int k = 0; k < 5; k++) out[k] = x[k];
+  out[5] = ctx->pme_dwrk;
+  return ORAC_OK;
+}
+
+}  // extern "C"

@@ -29,7 +29,25 @@ enum {
   ACC_COUL = 3,   // [3] Coulomb by type pair
   ACC_VIMG = 6,   // [9] image term of the molecular virial, row-major
   ACC_STR = 15,   // [9] sum_a F_a (x) co.Rm_a, row-major
-  ACC_N = 24
+  ACC_X = 24,     // [3] variant sums: REM seg_ene | alchemy U0(LJ), U0(Coul), dU/dlambda
+  ACC_N = 27
+};
+
+// Shell-kernel variants, the dispatch of src/mts_forces.f:118-153.
+enum { VAR_STD = 0, VAR_REM = 1, VAR_ALCH = 2 };
+
+// Per-atom variant flags (d_vflag): bit 0 REM segment atom, bit 1 mass at or
+// above massinfty, bits 4..7 ss_alchemy + 4.
+enum { VF_REM = 1, VF_MINF = 2, VF_SSHIFT = 4 };
+
+// alch_fact tables of force_alchemy (src/force_alchemy.f:194-200): [k][t+4]
+// with k = 0 the soft-core shift, k = 1 the scale, t = ss_i + ss_j.
+struct AlchTables {
+  double f[2][9], fq[2][9];    // current lambdas (LJ, Coulomb)
+  double f0[2][9], fq0[2][9];  // previous lambdas
+  double df[2][9], dfq[2][9];  // derivatives with respect to the control lambda
+  double qsoft, ljsoft;        // SOFT-CORE parameters
+  int opls;                    // sigma = 2 sqrt(rmin_i rmin_j) instead of rmin_i + rmin_j
 };
 
 // A group-pair list in CSR form with fixed row capacities: row i occupies
@@ -90,6 +108,17 @@ struct PairArgs {
   // 0: skip the image term of the molecular virial and the block reduction
   // (MD without pressure coupling needs neither)
   int stress;
+  // variant (VAR_*); REM: seg_select kind and rem_factor(3)
+  int variant;
+  const unsigned char* vflag;  // [N]
+  int rem_kind;
+  float rem_factor;
+  // alchemy: per-atom (rmin, 2 sqrt(epsm)) in FP32, (rmin, epsm) in FP64
+  const float2* soft;
+  const double2* softd;
+  float qsoft, ljsoft;
+  float af[2][9], afq[2][9];  // FP32 copies of the current tables
+  AlchTables at;
 };
 
 // flags of shell_run_r
@@ -212,6 +241,25 @@ struct orac_gpu_ctx {
   double sten_rcut = -1, sten_co[9] = {0};
   int sten_nc[3] = {0, 0, 0};
 
+  // shell-kernel variant (orac_gpu_set_rem / orac_gpu_set_alchemy)
+  int variant = VAR_STD;
+  unsigned char* d_vflag = nullptr;  // [N]
+  std::vector<unsigned char> h_vflag;
+  int rem_kind = 0;
+  double rem_factor = 1.0;
+  float2* d_soft = nullptr;    // [N]
+  double2* d_softd = nullptr;  // [N]
+  AlchTables at{};
+  std::vector<int> h_ssal;            // ss_alchemy
+  double lam[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // ladd lrm laddq lrmq and the lambda0 set
+  double* d_qc = nullptr;  // [N] PME charges at lambda: (1 - |lambdaq_i|) q_i
+  double* d_q0 = nullptr;  // [N] PME charges at lambda0
+  std::vector<unsigned char> h_rem;   // REM segment atoms
+  bool q0_differs = false;            // lambda0 charges differ from lambda charges
+  double pme_dwrk = 0.0;              // eer(lambda) - eer(lambda0) of the last fft_pme
+  double* d_xtra = nullptr;  // [8] variant outputs of the last shell evaluation
+  const double* pme_q() const { return variant == VAR_ALCH && d_qc ? d_qc : d_aqd; }
+
   // PME
   PmePlan pme;
 
@@ -231,6 +279,11 @@ int prof_begin(orac_gpu_ctx* ctx, int* slot);
 int prof_end(orac_gpu_ctx* ctx, int slot);
 // sum the elapsed time of slots [a, b) into prof_ms / prof_n (after a sync)
 int prof_collect(orac_gpu_ctx* ctx, int a, int b);
+
+// shell-kernel variants (api_variant.cu)
+void variant_fill(const orac_gpu_ctx* ctx, PairArgs* a);
+int variant_out_launch(orac_gpu_ctx* ctx, int forces_on);
+void variant_free(orac_gpu_ctx* ctx);
 
 // ---------------------------------------------------------------- errors
 int ctx_fail(orac_gpu_ctx* c, int code, const char* fmt, ...);

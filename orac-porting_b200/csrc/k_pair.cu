@@ -73,7 +73,94 @@ __device__ __forceinline__ void pair_energy_fp64(const PairArgs& A, double rx, d
   }
 }
 
-template <int MG, bool EN>
+// seg_select, src/rem.f90:631-645: 0 either atom in the segment, 1 both,
+// 2 exactly one
+__device__ __forceinline__ bool seg_sel(int kind, int fa, int fb) {
+  const bool ra = (fa & VF_REM) != 0, rb = (fb & VF_REM) != 0;
+  return kind == 0 ? (ra || rb) : (kind == 1 ? (ra && rb) : (ra != rb));
+}
+
+// Soft-core pair of force_alchemy (src/force_alchemy.f:441-531) in FP32:
+// qf is the force over r, conf/coul the scaled energies that enter the S'V
+// sum.  t indexes the tables (ss_i + ss_j + 4).
+__device__ __forceinline__ void alch_pair_f32(const PairArgs& A, float r2, int t, float rmi, float rmj, float eps4,
+                                              float qq, float* qf, float* conf, float* coul) {
+  const float auxa = rsqrtf(r2);
+  const float fq1 = A.afq[0][t];
+  const float auxaa = rsqrtf(A.qsoft * fq1 * fq1 + r2);
+  float f = 0.f, uc = 0.f, uq = 0.f;
+  if (eps4 > 1e-12f) {
+    const float sig = A.at.opls ? 2.f * sqrtf(rmi * rmj) : rmi + rmj;
+    const float s2 = sig * sig;
+    const float r6 = r2 * r2 * r2 / (s2 * s2 * s2);
+    const float gp1 = 1.f / (A.ljsoft * A.af[0][t] + r6);
+    const float gp2 = gp1 * gp1;
+    const float sc = A.af[1][t] * eps4;
+    f = sc * (2.f * gp1 * gp2 - gp2) * 6.f * r6 * auxa * auxa;
+    uc = sc * (gp2 - gp1);
+  }
+  if (!A.lskip) {
+    const float rsp = r2 * auxa;
+    const float ar = A.alphal * rsp;
+    const float qt = 1.0f / (1.0f + AS_QP * ar);
+    const float ex = expf(-ar * ar);
+    const float erfcst = ((((AS_A5 * qt + AS_A4) * qt + AS_A3) * qt + AS_A2) * qt + AS_A1) * qt * ex;
+    const float furpar = A.afq[1][t] * qq;
+    uq = furpar * erfcst * auxaa;
+    f += uq * auxaa * auxaa + furpar * A.twrtpi * ar * ex * auxa * auxa * auxaa;
+  } else if (!A.ewald) {
+    uq = A.afq[1][t] * qq * auxaa;
+    f += uq * auxaa * auxaa;
+  }
+  *qf = f;
+  *conf = uc;
+  *coul = uq;
+}
+
+// The same pair in FP64 for the energy outputs: LJ and Coulomb at lambda,
+// their sum at lambda0, and dU/dlambda of the control lambda (chain rule
+// through the alch_fact tables).
+__device__ __forceinline__ void alch_energy_fp64(const PairArgs& A, double rx, double ry, double rz, double2 si,
+                                                 double2 sj, double qq, int t, double* cd, double* qd,
+                                                 double* c0, double* q0, double* du) {
+  const AlchTables& T = A.at;
+  const double rsq = rx * rx + ry * ry + rz * rz;
+  const double auxa = 1.0 / sqrt(rsq);
+  const double fq = T.fq[0][t], fq0 = T.fq0[0][t];
+  const double auxaa = 1.0 / sqrt(T.qsoft * (fq * fq) + rsq);
+  const double auxa0 = 1.0 / sqrt(T.qsoft * (fq0 * fq0) + rsq);
+  const double epsmin = 4.0 * sqrt(si.y * sj.y);
+  *cd = *qd = *c0 = *q0 = *du = 0.0;
+  if (epsmin > 1.0e-12) {
+    const double sigma = T.opls ? 2.0 * sqrt(si.x * sj.x) : si.x + sj.x;
+    const double s2 = sigma * sigma;
+    const double r6 = rsq * rsq * rsq / (s2 * s2 * s2);
+    const double gp1 = 1.0 / (T.ljsoft * T.f[0][t] + r6);
+    const double gp2 = gp1 * gp1;
+    const double gp10 = 1.0 / (T.ljsoft * T.f0[0][t] + r6);
+    const double gp20 = gp10 * gp10;
+    const double auxc = epsmin * (gp2 - gp1);
+    *cd = T.f[1][t] * auxc;
+    *c0 = T.f0[1][t] * epsmin * (gp20 - gp10);
+    *du = T.df[1][t] * auxc + T.f[1][t] * epsmin * (gp2 - 2.0 * gp1 * gp2) * T.ljsoft * T.df[0][t];
+  }
+  double g = 0.0;  // charge-pair kernel without its scale and soft core
+  if (!A.lskip) {
+    const double ar = A.alphad / auxa;
+    const double qt = 1.0 / (1.0 + 0.3275911 * ar);
+    g = qq * ((((1.0614054 * qt - 1.453152) * qt + 1.4214137) * qt - 0.28449674) * qt + 0.2548296) * qt *
+        exp(-ar * ar);
+  } else if (!A.ewald) {
+    g = qq;
+  }
+  if (g != 0.0) {
+    *qd = T.fq[1][t] * g * auxaa;
+    *q0 = T.fq0[1][t] * g * auxa0;
+    *du += T.dfq[1][t] * g * auxaa - T.fq[1][t] * g * T.qsoft * fq * T.dfq[0][t] * auxaa * auxaa * auxaa;
+  }
+}
+
+template <int MG, bool EN, int VAR>
 __global__ void __launch_bounds__(WPB * 32, (MG <= 4 && !EN) ? 5 : 1)
     k_pair(const PairArgs A) {
   extern __shared__ float2 s_lj[];
@@ -81,6 +168,8 @@ __global__ void __launch_bounds__(WPB * 32, (MG <= 4 && !EN) ? 5 : 1)
   __shared__ int s_ti[WPB][MG];
   __shared__ float s_pm[WPB][MG];
   __shared__ double s_qd[WPB][MG];
+  __shared__ int s_fi[WPB][MG];
+  __shared__ float2 s_sf[WPB][MG];
   __shared__ double s_red[WPB][ACC_N];
 
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -92,6 +181,7 @@ __global__ void __launch_bounds__(WPB * 32, (MG <= 4 && !EN) ? 5 : 1)
   const float2* lj = staged ? s_lj : A.lj;
 
   double ec0 = 0, ec1 = 0, ec2 = 0, eq0 = 0, eq1 = 0, eq2 = 0;
+  double ex0 = 0, ex1 = 0, ex2 = 0;  // variant sums (ACC_X)
   unsigned npairs = 0, nscan = 0, nkept = 0;
   float v00 = 0, v01 = 0, v02 = 0, v10 = 0, v11 = 0, v12 = 0, v20 = 0,
         v21 = 0, v22 = 0;
@@ -105,6 +195,8 @@ __global__ void __launch_bounds__(WPB * 32, (MG <= 4 && !EN) ? 5 : 1)
       s_ti[warp][lane] = A.atype[ifirst + lane];
       s_pm[warp][lane] = A.apm[ifirst + lane];
       if (EN) s_qd[warp][lane] = A.qd[ifirst + lane];
+      if (VAR != VAR_STD) s_fi[warp][lane] = A.vflag[ifirst + lane];
+      if (VAR == VAR_ALCH) s_sf[warp][lane] = A.soft[ifirst + lane];
     }
     __syncwarp();
     float fi[MG][3];
@@ -174,60 +266,97 @@ __global__ void __launch_bounds__(WPB * 32, (MG <= 4 && !EN) ? 5 : 1)
       const int2 mj = A.gmeta[j];
       const int jfirst = mj.x, nj = mj.y & 0xff, typej = mj.y >> 8;
       const float dcx = (float)cx, dcy = (float)cy, dcz = (float)cz;
-      double pconf = 0.0, pcoul = 0.0;
+      double pconf = 0.0, pcoul = 0.0, px0 = 0.0, px1 = 0.0, px2 = 0.0;
       float vsum = 0.f;
       float gx = 0.f, gy = 0.f, gz = 0.f;  // total force on the j group
       for (int b = 0; b < nj; b++) {
         const float4 ob = A.aoff[jfirst + b];
         const int tb = A.atype[jfirst + b];
         const double qbd = EN ? A.qd[jfirst + b] : 0.0;
+        const int fjb = (VAR != VAR_STD) ? (int)A.vflag[jfirst + b] : 0;
+        const float2 sfb = (VAR == VAR_ALCH) ? A.soft[jfirst + b] : make_float2(0.f, 0.f);
         float fbx = 0.f, fby = 0.f, fbz = 0.f;
 #pragma unroll
         for (int a = 0; a < MG; a++) {
           if (a >= ni) break;
           if ((msk >> (a * 8 + b)) & 1ull) continue;
           const float4 ai = s_ai[warp][a];
-          const float2 L = lj[s_ti[warp][a] * A.ntype + tb];
-          const bool ljon = L.y != 0.f;
-          if (A.lskip && !ljon && A.ewald) continue;  // src/force.f:416-417
-          npairs++;
-          const float rx = dcx + ai.x - ob.x;
-          const float ry = dcy + ai.y - ob.y;
-          const float rz = dcz + ai.z - ob.z;
-          const float r2 = rx * rx + ry * ry + rz * rz;
-          const float rsqi = 1.0f / r2;
           float qf = 0.f, conf = 0.f, coul = 0.f;
-          if (ljon) {
-            const float r6 = rsqi * rsqi * rsqi;
-            const float r12 = r6 * r6;
-            qf = (12.0f * L.x * r12 - 6.0f * L.y * r6) * rsqi;
-            conf = L.x * r12 - L.y * r6;
+          float rx, ry, rz;
+          bool ljon = false;
+          int tal = 0;
+          if constexpr (VAR == VAR_ALCH) {
+            // src/force_alchemy.f:412-451: exclusions and fixed-mass pairs
+            // are always skipped; no LJ and no Coulomb skips the pair
+            const int fia = s_fi[warp][a];
+            if (fia & fjb & VF_MINF) continue;
+            const float2 sa = s_sf[warp][a];
+            const float eps4 = sa.y * sfb.y;
+            if (eps4 < 1e-12f && A.lskip && A.ewald) continue;
+            npairs++;
+            tal = (fia >> VF_SSHIFT) + (fjb >> VF_SSHIFT) - 4;
+            rx = dcx + ai.x - ob.x;
+            ry = dcy + ai.y - ob.y;
+            rz = dcz + ai.z - ob.z;
+            alch_pair_f32(A, rx * rx + ry * ry + rz * rz, tal, sa.x, sfb.x, eps4, ai.w * ob.w, &qf, &conf, &coul);
+          } else {
+            const float2 L = lj[s_ti[warp][a] * A.ntype + tb];
+            ljon = L.y != 0.f;
+            if (A.lskip && !ljon && A.ewald) continue;  // src/force.f:416-417
+            npairs++;
+            rx = dcx + ai.x - ob.x;
+            ry = dcy + ai.y - ob.y;
+            rz = dcz + ai.z - ob.z;
+            const float r2 = rx * rx + ry * ry + rz * rz;
+            const float rsqi = 1.0f / r2;
+            if (ljon) {
+              const float r6 = rsqi * rsqi * rsqi;
+              const float r12 = r6 * r6;
+              qf = (12.0f * L.x * r12 - 6.0f * L.y * r6) * rsqi;
+              conf = L.x * r12 - L.y * r6;
+            }
+            if (!A.lskip) {
+              const float rsp = sqrtf(r2);
+              const float ar = A.alphal * rsp;
+              const float qt = 1.0f / (1.0f + AS_QP * ar);
+              const float ex = expf(-ar * ar);
+              const float erfcst =
+                  ((((AS_A5 * qt + AS_A4) * qt + AS_A3) * qt + AS_A2) * qt + AS_A1) *
+                  qt * ex;
+              const float qq = ai.w * ob.w;
+              coul = qq * erfcst / rsp;
+              qf += qq * (erfcst + A.twrtpi * ar * ex) * rsqi / rsp;
+            } else if (!A.ewald) {
+              const float rsp = sqrtf(r2);
+              coul = ai.w * ob.w / rsp;
+              qf += coul * rsqi;
+            }
           }
-          if (!A.lskip) {
-            const float rsp = sqrtf(r2);
-            const float ar = A.alphal * rsp;
-            const float qt = 1.0f / (1.0f + AS_QP * ar);
-            const float ex = expf(-ar * ar);
-            const float erfcst =
-                ((((AS_A5 * qt + AS_A4) * qt + AS_A3) * qt + AS_A2) * qt + AS_A1) *
-                qt * ex;
-            const float qq = ai.w * ob.w;
-            coul = qq * erfcst / rsp;
-            qf += qq * (erfcst + A.twrtpi * ar * ex) * rsqi / rsp;
-          } else if (!A.ewald) {
-            const float rsp = sqrtf(r2);
-            coul = ai.w * ob.w / rsp;
-            qf += coul * rsqi;
-          }
+          // force_rem (src/force_REM.f:491-495,634-678): selected pairs scale
+          // their force and their share of the S'V sum
+          const bool sel = (VAR == VAR_REM) && seg_sel(A.rem_kind, s_fi[warp][a], fjb);
           if (switched) {
-            vsum += conf + coul;
+            vsum += sel ? (conf + coul) * A.rem_factor : conf + coul;
             qf *= sw;
           }
+          if (sel) qf *= A.rem_factor;
           if (EN) {
+            const double erx = cx + ((double)ai.x - (double)ob.x);
+            const double ery = cy + ((double)ai.y - (double)ob.y);
+            const double erz = cz + ((double)ai.z - (double)ob.z);
             double cd, qd;
-            pair_energy_fp64(A, cx + ((double)ai.x - (double)ob.x), cy + ((double)ai.y - (double)ob.y),
-                             cz + ((double)ai.z - (double)ob.z), A.ljd[s_ti[warp][a] * A.ntype + tb], ljon,
-                             s_qd[warp][a] * qbd, &cd, &qd);
+            if constexpr (VAR == VAR_ALCH) {
+              double c0, q0, du;
+              alch_energy_fp64(A, erx, ery, erz, A.softd[ifirst + a], A.softd[jfirst + b], s_qd[warp][a] * qbd, tal,
+                               &cd, &qd, &c0, &q0, &du);
+              px0 += c0;
+              px1 += q0;
+              px2 += du;
+            } else {
+              pair_energy_fp64(A, erx, ery, erz, A.ljd[s_ti[warp][a] * A.ntype + tb], ljon, s_qd[warp][a] * qbd, &cd,
+                               &qd);
+              if (sel) px0 += cd + qd;  // seg_ene
+            }
             pconf += cd;
             pcoul += qd;
           }
@@ -249,6 +378,9 @@ __global__ void __launch_bounds__(WPB * 32, (MG <= 4 && !EN) ? 5 : 1)
       if (switched) {
         pconf *= swd;
         pcoul *= swd;
+        px0 *= swd;
+        px1 *= swd;
+        px2 *= swd;
         // S'(R) V term: X = -dS/dR / R * V * R_vec on i atoms by mass fraction
         const float sx = -dsw * vsum * dcx, sy = -dsw * vsum * dcy,
                     sz = -dsw * vsum * dcz;
@@ -281,6 +413,9 @@ __global__ void __launch_bounds__(WPB * 32, (MG <= 4 && !EN) ? 5 : 1)
         ec2 += pconf;
         eq2 += pcoul;
       }
+      ex0 += px0;
+      ex1 += px1;
+      ex2 += px2;
       if (A.stress && (imx != 0.0 || imy != 0.0 || imz != 0.0)) {
         // j sits at its image xpg_j + img: its virial arm gains co.img
         const float ix = (float)(A.c11 * imx + A.c12 * imy + A.c13 * imz);
@@ -334,18 +469,21 @@ __global__ void __launch_bounds__(WPB * 32, (MG <= 4 && !EN) ? 5 : 1)
   }
   if (!A.forces_on || (!EN && !A.stress)) return;
   // block reduction of energies and image virial
-  double vals[15] = {ec0, ec1, ec2, eq0, eq1, eq2, v00, v01, v02,
-                     v10, v11, v12, v20, v21, v22};
+  constexpr int NV = (VAR != VAR_STD && EN) ? 18 : 15;
+  double vals[18] = {ec0, ec1, ec2, eq0, eq1, eq2, v00, v01, v02,
+                     v10, v11, v12, v20, v21, v22, ex0, ex1, ex2};
 #pragma unroll
-  for (int q = 0; q < 15; q++) {
+  for (int q = 0; q < NV; q++) {
     const double s = warp_sumd(vals[q]);
     if (lane == 0) s_red[warp][q] = s;
   }
   __syncthreads();
-  if (threadIdx.x < 15) {
+  if (threadIdx.x < NV) {
     double s = 0;
     for (int w = 0; w < WPB; w++) s += s_red[w][threadIdx.x];
-    if (s != 0.0) atomicAdd(A.acc + threadIdx.x, s);  // slots 0..14 = ACC_CONF..ACC_VIMG+8
+    // slots 0..14 = ACC_CONF..ACC_VIMG+8, then ACC_X..ACC_X+2
+    const int slot = threadIdx.x < 15 ? (int)threadIdx.x : ACC_X + (int)threadIdx.x - 15;
+    if (s != 0.0) atomicAdd(A.acc + slot, s);
   }
 }
 
@@ -435,18 +573,28 @@ int pair_launch(orac_gpu_ctx* ctx, const PairArgs& a, int maxg) {
   const size_t smem = (size_t)(a.ntype * a.ntype <= LJ_SMEM_MAX ? a.ntype * a.ntype : 0) * sizeof(float2);
   if (maxg > ORAC_MAXG)
     return ctx_fail(ctx, ORAC_ERR_PARAM, "charge group of %d atoms exceeds %d", maxg, ORAC_MAXG);
+  if (a.variant < VAR_STD || a.variant > VAR_ALCH) return ctx_fail(ctx, ORAC_ERR_PARAM, "variant %d", a.variant);
   int slot = -1;
   if (int rc = prof_begin(ctx, &slot)) return rc;
-  if (maxg <= 4) {
-    if (a.energy)
-      k_pair<4, true><<<nb, WPB * 32, smem, ctx->stream>>>(a);
-    else
-      k_pair<4, false><<<nb, WPB * 32, smem, ctx->stream>>>(a);
-  } else if (maxg <= 8) {
-    if (a.energy)
-      k_pair<8, true><<<nb, WPB * 32, smem, ctx->stream>>>(a);
-    else
-      k_pair<8, false><<<nb, WPB * 32, smem, ctx->stream>>>(a);
+  const bool small = maxg <= 4;
+  switch (a.variant * 4 + (small ? 0 : 2) + (a.energy ? 1 : 0)) {
+#define ORAC_KP(code, MG, EN, VAR) \
+  case code:                       \
+    k_pair<MG, EN, VAR><<<nb, WPB * 32, smem, ctx->stream>>>(a); \
+    break;
+    ORAC_KP(0, 4, false, VAR_STD)
+    ORAC_KP(1, 4, true, VAR_STD)
+    ORAC_KP(2, 8, false, VAR_STD)
+    ORAC_KP(3, 8, true, VAR_STD)
+    ORAC_KP(4, 4, false, VAR_REM)
+    ORAC_KP(5, 4, true, VAR_REM)
+    ORAC_KP(6, 8, false, VAR_REM)
+    ORAC_KP(7, 8, true, VAR_REM)
+    ORAC_KP(8, 4, false, VAR_ALCH)
+    ORAC_KP(9, 4, true, VAR_ALCH)
+    ORAC_KP(10, 8, false, VAR_ALCH)
+    ORAC_KP(11, 8, true, VAR_ALCH)
+#undef ORAC_KP
   }
   CKL();
   return prof_end(ctx, slot);

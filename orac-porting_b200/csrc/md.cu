@@ -745,7 +745,7 @@ static int md_forces_shell(orac_gpu_ctx* ctx, MdState& S, char sh, int lvl, bool
     double recip[9];
     for (int i = 0; i < 3; i++)
       for (int j = 0; j < 3; j++) recip[i + 3 * j] = 0.5 * ctx->oc[j + 3 * i];  // src/fft_pme.f:47-51
-    if (int rc = pme_run(ctx, ctx->N, S.x, ctx->d_aqd, recip, ctx->volume, ctx->alphal, nullptr, S.e + 24, nullptr,
+    if (int rc = pme_run(ctx, ctx->N, S.x, ctx->pme_q(), recip, ctx->volume, ctx->alphal, nullptr, S.e + 24, nullptr,
                          nullptr, f))
       return rc;
   }

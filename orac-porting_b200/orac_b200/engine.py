@@ -109,6 +109,38 @@ class Engine:
         """Energies in the oracle's order: LJ slt, slv, mixed; Coulomb slt, slv, mixed."""
         return np.array([en["ucnp"], en["ucns"], en["ucnsp"], en["ucop"], en["ucos"], en["ucosp"]])
 
+    # ------------------------------------------------------ variants
+    def set_rem(self, rematom, kind=0, factor=1.0):
+        """force_rem for every later shell (orac_gpu_set_rem); None: standard."""
+        arr = None if rematom is None else i32(np.asarray(rematom) != 0)
+        check(self.ctx, self.lib.orac_gpu_set_rem(self.ctx, arr, int(kind), float(factor)), "set_rem")
+
+    def set_alchemy(self, ss_alchemy, qsoft=0.5, ljsoft=0.5, opls=False):
+        """force_alchemy with ORAC's per-atom soft-core parameters; None: standard."""
+        if ss_alchemy is None:
+            check(self.ctx, self.lib.orac_gpu_set_alchemy(self.ctx, None, None, None, 0.0, 0.0, 0), "set_alchemy")
+            return
+        rmin, epsm = self.s.alchemy_params()
+        check(self.ctx, self.lib.orac_gpu_set_alchemy(self.ctx, i32(ss_alchemy), f64(rmin), f64(epsm), qsoft, ljsoft,
+                                                      int(opls)), "set_alchemy")
+
+    def set_lambda(self, ladd, lrm, laddq, lrmq, ladd0=None, lrm0=None, laddq0=None, lrmq0=None, intramol=False,
+                   ljintra=False, dlam=None):
+        """cpropar lambdas (previous ones default to the current); dlam =
+        d(ladd, lrm, laddq, lrmq)/dlambda for the dU/dlambda output."""
+        lam = [ladd, lrm, laddq, lrmq, ladd if ladd0 is None else ladd0, lrm if lrm0 is None else lrm0,
+               laddq if laddq0 is None else laddq0, lrmq if lrmq0 is None else lrmq0]
+        d = None if dlam is None else f64(dlam)
+        check(self.ctx, self.lib.orac_gpu_set_lambda(self.ctx, f64(lam), int(intramol), int(ljintra),
+                                                     None if d is None else d.ctypes.data), "set_lambda")
+
+    def variant_energies(self):
+        """(seg_ene, dwrk, U0 LJ, U0 Coulomb, dU/dlambda, PME work) of the last
+        energy evaluation (orac_gpu_variant_energies)."""
+        out = np.zeros(6)
+        check(self.ctx, self.lib.orac_gpu_variant_energies(self.ctx, out), "variant_energies")
+        return out
+
     def update_lists(self):
         """H list by linked cells (or the 'u' all-pairs update), then the two
         phony calls deriving the L and M lists (src/mtsmd.f:2403-2470)."""

@@ -66,6 +66,10 @@ def load():
         "orac_gpu_cself": (i, [_P, d, _DP, _DP]),
         "orac_gpu_mts_forces_dev": (i, [_P, ch, _P, _P, _P, _P, _P, _P]),
         "orac_gpu_fft_pme_dev": (i, [_P, _P, _P, _P, _P, _P]),
+        "orac_gpu_set_rem": (i, [_P, _I, i, d]),
+        "orac_gpu_set_alchemy": (i, [_P, _I, _D, _D, d, d, i]),
+        "orac_gpu_set_lambda": (i, [_P, _D, i, i, _P]),
+        "orac_gpu_variant_energies": (i, [_P, _D]),
         "orac_gpu_pme_kspace_static": (i, [_P, i, _P, _P, _D, d, d, d, i, i, i, i, _P, _P, C.c_char_p, i]),
         "orac_gpu_md_setup": (i, [_P, _D, _D, _D, _D, _D, _D, _I, _D, i, d, i, i, i, i, i, ch, d]),
         "orac_gpu_md_run": (i, [_P, i, i, _D]),

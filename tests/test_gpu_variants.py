@@ -1,0 +1,162 @@
+"""GPU parity of the shell-kernel variants against the FP64 oracle:
+force_rem (REM segment scaling) and force_alchemy (soft-core alchemy), plus
+the alchemical PME charges and work of do_pmesh_alchemy.
+
+Tolerances are those of the standard parity tests: forces relative RMS
+<= 1e-5, energies relative <= 1e-6 of the value or of the sum of the term
+magnitudes when the value cancels, stress <= 1e-5 of its norm.  dU/dlambda
+from the GPU's analytic chain rule is compared with a central difference of
+the oracle's U(lambda) (step 1e-4, truncation error ~1e-8 relative) at
+relative 1e-5.
+"""
+import functools
+
+import numpy as np
+import pytest
+
+import oracle
+from orac_b200 import systems
+
+pytestmark = pytest.mark.gpu
+
+FORCE_RMS = 1e-5
+ENERGY_REL = 1e-6
+STRESS_REL = 1e-5
+LAM = dict(ladd=0.3, lrm=0.6, laddq=0.4, lrmq=0.7)
+LAM0 = dict(ladd0=0.2, lrm0=0.5, laddq0=0.35, lrmq0=0.65)
+
+
+def small_box():
+    s = systems.water_box(nwat=64, box=16.5, lattice=4, jitter=0.25, seeds=(1, 2, 3, 4), nfft=(16, 16, 16))
+    s.ncell = None
+    s.shells = systems.Shells(rcutm=4.0, rtolm=0.4, rneim=0.4, rcutl=5.5, rtoll=0.4, rneil=0.4, rcuth=7.0,
+                              rtolh=0.5, rneih=0.5)
+    return s
+
+
+@functools.lru_cache(maxsize=None)
+def system(name):
+    if name == "water64":
+        s = small_box()
+        ss = np.ones(s.ntap, np.int32)
+        ss[0:9] = -2
+        ss[9:15] = 2
+        rem = np.zeros(s.ntap, np.uint8)
+        rem[0:12] = 1
+    elif name == "config1":
+        s = systems.config1_water()
+        ss = np.ones(s.ntap, np.int32)
+        ss[0:30] = -2
+        rem = np.zeros(s.ntap, np.uint8)
+        rem[0:60] = 1
+    elif name == "polymer_small":
+        s = systems.polymer_in_water(nchain=240, nwat=900, box=32.0, nfft=(36, 36, 36), order=5, group_size=5,
+                                     name="polymer_small")
+        ss = np.ones(s.ntap, np.int32)
+        ss[20:30] = -2  # a stretch of the chain: intramolecular exclusions matter
+        rem = (s.ss_index == 1).astype(np.uint8)  # solute tempering
+    else:
+        raise KeyError(name)
+    s.ss_alchemy = ss
+    s.rematom = rem
+    return s
+
+
+def rel_rms(F, Fref):
+    return float(np.sqrt(((F - Fref) ** 2).sum() / (Fref ** 2).sum()))
+
+
+def close(g, r, scale, what):
+    tol = ENERGY_REL * max(abs(r), scale, 1e-300)
+    assert abs(g - r) <= tol, f"{what}: gpu {g!r} oracle {r!r} diff {g - r:.3e} tol {tol:.3e}"
+
+
+def pair(name, variant, **kw):
+    from orac_b200.engine import Engine
+
+    s = system(name)
+    o = oracle.Oracle(s.copy())
+    g = Engine(s.copy())
+    if variant == "rem":
+        o.set_rem(s.rematom, kw["kind"], kw["factor"])
+        g.set_rem(s.rematom, kw["kind"], kw["factor"])
+    else:
+        o.set_alchemy(s.ss_alchemy, 0.5, 0.5)
+        g.set_alchemy(s.ss_alchemy, 0.5, 0.5)
+        lam = dict(kw.get("lam", LAM))
+        lam.update(kw.get("lam0", {}))
+        o.set_lambda(**lam)
+        g.set_lambda(**lam, dlam=kw.get("dlam"))
+    o.update_lists()
+    g.update_lists()
+    return o, g
+
+
+def compare_shell(o, g, shell):
+    Fr, uer, str_ = o.shell(shell)
+    Fg, en, stg = g.shell(shell)
+    ueg = g.ue6(en)
+    assert rel_rms(Fg, Fr) <= FORCE_RMS, f"{shell}: force rel RMS {rel_rms(Fg, Fr):.3e}"
+    scale = np.abs(uer).sum()
+    for k in range(6):
+        close(ueg[k], uer[k], 0.0, f"{shell} energy {k}")
+    assert np.linalg.norm(stg - str_) <= STRESS_REL * max(np.linalg.norm(str_), 1e-300)
+    return o.last_extra.copy(), g.variant_energies(), scale
+
+
+@pytest.mark.parametrize("shell", ["m", "l", "h"])
+@pytest.mark.parametrize("kind", [0, 1, 2])
+@pytest.mark.parametrize("name", ["water64", "config1", "polymer_small"])
+def test_rem_shell_parity(name, kind, shell):
+    o, g = pair(name, "rem", kind=kind, factor=0.4)
+    xr, xg, scale = compare_shell(o, g, shell)
+    close(xg[0], xr[0], scale, f"{shell} seg_ene")
+
+
+@pytest.mark.parametrize("shell", ["m", "l", "h"])
+@pytest.mark.parametrize("name", ["water64", "config1", "polymer_small"])
+def test_alchemy_shell_parity(name, shell):
+    o, g = pair(name, "alch", lam0=LAM0)
+    xr, xg, scale = compare_shell(o, g, shell)
+    close(xg[1], xr[1], scale, f"{shell} dwrk")
+    close(xg[2], xr[2], scale, f"{shell} U0 LJ")
+    close(xg[3], xr[3], scale, f"{shell} U0 Coulomb")
+
+
+@pytest.mark.parametrize("shell", ["m", "l", "h"])
+@pytest.mark.parametrize("name", ["water64", "polymer_small"])
+def test_alchemy_dudl_matches_oracle_central_difference(name, shell):
+    lam = 0.4
+    h = 1e-4
+    o, g = pair(name, "alch", lam=dict(ladd=0.0, lrm=lam, laddq=0.0, lrmq=lam), dlam=[0.0, 1.0, 0.0, 1.0])
+    g.shell(shell)
+    dudl = g.variant_energies()[4]
+    u = []
+    for sgn in (1, -1):
+        l2 = lam + sgn * h
+        o.set_lambda(ladd=0.0, lrm=l2, laddq=0.0, lrmq=l2)
+        o.update_lists()
+        _, ue, _ = o.shell(shell)
+        u.append(ue.sum())
+    fd = (u[0] - u[1]) / (2 * h)
+    assert abs(dudl - fd) <= 1e-5 * max(abs(fd), 1e-12), (dudl, fd)
+    assert dudl != 0.0
+
+
+@pytest.mark.parametrize("name", ["water64", "polymer_small"])
+def test_alchemy_pme_charges_and_work(name):
+    o, g = pair(name, "alch", lam0=LAM0)
+    s = system(name)
+    lq = np.where(s.ss_alchemy == 2, LAM["laddq"], np.where(s.ss_alchemy == -2, -LAM["lrmq"], 0.0))
+    lq0 = np.where(s.ss_alchemy == 2, LAM0["laddq0"], np.where(s.ss_alchemy == -2, -LAM0["lrmq0"], 0.0))
+    t = s.copy()
+    t.charge = (1.0 - np.abs(lq)) * s.charge
+    Fr, er, sr = oracle.Oracle(t).fft_pme()
+    t0 = s.copy()
+    t0.charge = (1.0 - np.abs(lq0)) * s.charge
+    _, er0, _ = oracle.Oracle(t0).fft_pme()
+    Fg, eg, sg = g.fft_pme()
+    assert rel_rms(Fg, Fr) <= FORCE_RMS
+    close(eg, er, 0.0, "eer")
+    assert np.linalg.norm(sg - sr) <= STRESS_REL * np.linalg.norm(sr)
+    close(g.variant_energies()[5], er - er0, abs(er), "PME work")
