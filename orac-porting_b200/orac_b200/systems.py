@@ -89,10 +89,16 @@ class System:
     bends: np.ndarray | None = None  # (na, 3)
     bend_k: np.ndarray | None = None
     bend_t0: np.ndarray | None = None
+    bend_ub_r0: np.ndarray | None = None  # Urey-Bradley 1-3 spring (fpbend potc, potd)
+    bend_ub_k: np.ndarray | None = None
     tors: np.ndarray | None = None  # (nt, 4)
-    tors_k: np.ndarray | None = None
-    tors_n: np.ndarray | None = None
-    tors_d: np.ndarray | None = None
+    tors_k: np.ndarray | None = None  # fptors potb (V)
+    tors_n: np.ndarray | None = None  # fptors pota: +-n, the sign selecting phase 0 or pi
+    # improper torsions (fitors): atoms, pota, potb, potc (potc > 0: harmonic)
+    itors: np.ndarray | None = None
+    itors_a: np.ndarray | None = None
+    itors_b: np.ndarray | None = None
+    itors_c: np.ndarray | None = None
     lj_params: np.ndarray | None = None  # (ntype, 2): Rmin/2 (A), eps (kcal/mol) per LJ type
     # alchemy (soft-core force_alchemy): 1 normal, 2 added, -2 removed per atom
     ss_alchemy: np.ndarray | None = None
@@ -519,8 +525,7 @@ def polymer_in_water(nchain=1700, nwat=7000, box=62.0, seed_chain=5, seed_lj=6, 
     s.bend_t0 = np.full(len(s.bends), math.radians(112.0))
     s.tors = np.array([(i + 1, i + 2, i + 3, i + 4) for i in range(nchain - 3)], dtype=np.int32)
     s.tors_k = np.full(len(s.tors), 1.4 * 4184.0 / units.EFACT)
-    s.tors_n = np.full(len(s.tors), 3, dtype=np.int32)
-    s.tors_d = np.zeros(len(s.tors))
+    s.tors_n = np.full(len(s.tors), -3.0)  # U = V cos(3 phi) - V: trans minimum
     return s
 
 

@@ -131,6 +131,31 @@ long orc_force_ex(const int* ss_index, const double* xp0, const double* yp0,
 void orc_alch_set(double fact[2][9], double ladd, double lrm, int intramol,
                   int ljintra, int qq);
 
+/* Bonded intramolecular forces (orac_bonded.c), Cartesian coordinates,
+ * forces accumulated, ue[2] set (solute, solvent):
+ * fpbond (src/fpbond.f): U = kb (r - r0)^2 over lbnd(2, nb);
+ * fpbend (src/fpbend.f): pot[7 i + 0..6] = pota..potg of bend i (theta0, k,
+ *   Urey-Bradley r0 and k, coupling); fptors (src/fptors.f): pota = +-n,
+ *   potb = V, U = sig (|V| - V cos n phi); fitors (src/fitors.f): potc > 0
+ *   harmonic in phi, else the cosine form.  fptors/fitors return the number
+ *   of degenerate or unsupported terms skipped. */
+void orc_fpbond(const int* ss_index, const int* lbnd, int nb, const double* x,
+                const double* y, const double* z, const double* r0,
+                const double* kb, double* ue, double* fx, double* fy,
+                double* fz);
+void orc_fpbend(const int* ss_index, const int* lbndg, int nbend,
+                const double* x, const double* y, const double* z,
+                const double* pot, double* ue, double* fx, double* fy,
+                double* fz);
+int orc_fptors(const int* ss_index, const int* ltor, int nt, const double* x,
+               const double* y, const double* z, const double* pota,
+               const double* potb, double* ue, double* fx, double* fy,
+               double* fz);
+int orc_fitors(const int* ss_index, const int* litr, int nt, const double* x,
+               const double* y, const double* z, const double* pota,
+               const double* potb, const double* potc, double* ue, double* fx,
+               double* fy, double* fz);
+
 /* PME (FFTW build): load_bsp_moduli + DFTMOD, src/pme_fftw3.f90:165-230 */
 void orc_load_bsp_moduli(double* bsp_mod1, double* bsp_mod2, double* bsp_mod3,
                          int nfft1, int nfft2, int nfft3, int order);

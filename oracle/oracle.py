@@ -52,6 +52,12 @@ def lib():
         L.orc_force_ex.restype = C.c_long
         L.orc_force_ex.argtypes = L.orc_force.argtypes + [C.POINTER(Variant), _D]
         L.orc_alch_set.argtypes = [C.POINTER(C.c_double * 18), C.c_double, C.c_double, C.c_int, C.c_int, C.c_int]
+        L.orc_fpbond.argtypes = [_I, _I, C.c_int, _D, _D, _D, _D, _D, _D, _D, _D, _D]
+        L.orc_fpbend.argtypes = [_I, _I, C.c_int, _D, _D, _D, _D, _D, _D, _D, _D]
+        L.orc_fptors.restype = C.c_int
+        L.orc_fptors.argtypes = [_I, _I, C.c_int, _D, _D, _D, _D, _D, _D, _D, _D, _D]
+        L.orc_fitors.restype = C.c_int
+        L.orc_fitors.argtypes = [_I, _I, C.c_int, _D, _D, _D, _D, _D, _D, _D, _D, _D, _D]
         L.orc_load_bsp_moduli.argtypes = [_D, _D, _D, C.c_int, C.c_int, C.c_int, C.c_int]
         L.orc_fill_bspline.argtypes = [C.c_double, C.c_int, _D, _D]
         L.orc_fft1d.argtypes = [C.c_int, _D, C.c_int]
@@ -87,6 +93,19 @@ def alch_set(ladd, lrm, intramol=False, ljintra=False, qq=False):
     t = (C.c_double * 18)()
     lib().orc_alch_set(C.byref(t), ladd, lrm, int(intramol), int(ljintra), int(qq))
     return np.array(t[:]).reshape(2, 9)
+
+
+def bend_pot(s):
+    """fpbend's pota..potg per bend (theta0, k, no Urey-Bradley, no coupling
+    unless the System carries bend_ub_r0 / bend_ub_k)."""
+    n = len(s.bends)
+    p = np.zeros((n, 7))
+    p[:, 0] = s.bend_t0
+    p[:, 1] = s.bend_k
+    if getattr(s, "bend_ub_k", None) is not None:
+        p[:, 2] = s.bend_ub_r0
+        p[:, 3] = s.bend_ub_k
+    return p
 
 
 def _f(a):
@@ -161,6 +180,45 @@ class Oracle:
 
     def clear_variant(self):
         self.variant = None
+
+    # ---------------------------------------------------------- bonded
+    def intra_n0(self):
+        """The bonded terms of mts_intra_n0 (src/mts_intra_n0.f:73-100):
+        fpbond + fpbend + fitors.  Returns (F (3,N), {name: (slt, slv)})."""
+        s = self.s
+        r = self.cartesian()
+        x, y, z = _f(r[0]), _f(r[1]), _f(r[2])
+        fx, fy, fz = np.zeros(s.ntap), np.zeros(s.ntap), np.zeros(s.ntap)
+        e = {}
+        ss = _i(s.ss_index)
+        ue = np.zeros(2)
+        if s.bond_k is not None and len(s.bonds):
+            self.L.orc_fpbond(ss, _i(s.bonds.ravel()), len(s.bonds), x, y, z, _f(s.bond_r0), _f(s.bond_k), ue, fx,
+                              fy, fz)
+        e["bond"] = tuple(ue)
+        ue = np.zeros(2)
+        if s.bends is not None and len(s.bends):
+            self.L.orc_fpbend(ss, _i(s.bends.ravel()), len(s.bends), x, y, z, _f(bend_pot(s).ravel()), ue, fx, fy, fz)
+        e["bend"] = tuple(ue)
+        ue = np.zeros(2)
+        self.last_skipped = 0
+        if s.itors is not None and len(s.itors):
+            self.last_skipped = self.L.orc_fitors(ss, _i(s.itors.ravel()), len(s.itors), x, y, z, _f(s.itors_a),
+                                                  _f(s.itors_b), _f(s.itors_c), ue, fx, fy, fz)
+        e["itors"] = tuple(ue)
+        return np.stack([fx, fy, fz]), e
+
+    def intra_torsions(self):
+        """fptors (src/fptors.f), the torsion part of mts_intra_n1."""
+        s = self.s
+        r = self.cartesian()
+        fx, fy, fz = np.zeros(s.ntap), np.zeros(s.ntap), np.zeros(s.ntap)
+        ue = np.zeros(2)
+        self.last_skipped = 0
+        if s.tors is not None and len(s.tors):
+            self.last_skipped = self.L.orc_fptors(_i(s.ss_index), _i(s.tors.ravel()), len(s.tors), _f(r[0]),
+                                                  _f(r[1]), _f(r[2]), _f(s.tors_n), _f(s.tors_k), ue, fx, fy, fz)
+        return np.stack([fx, fy, fz]), tuple(ue)
 
     def _prep(self):
         s = self.s
