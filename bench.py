@@ -60,18 +60,15 @@ def dist_info():
 
 
 def econst_of(s, engine=None):
-    """Self energy (cself) + the constant erf correction of rigid bonds
-    (ferrf with iz = 0, src/mtsmd.f:1641-1645)."""
+    """Self energy (cself): the constant of the energy records (the erf
+    corrections of the constraints are part of the records themselves)."""
     if engine is not None:
         a, b = engine.cself()
-        _, fs = engine.ferrf(s.constraints, 1.0, iz=0)
     else:
         import oracle
 
-        o = oracle.Oracle(s)
-        a, b = o.cself()
-        _, fs = o.ferrf(s.constraints, 1.0, iz=0)
-    return a + b + float(fs.sum())
+        a, b = oracle.Oracle(s).cself()
+    return a + b
 
 
 class ClockSampler:

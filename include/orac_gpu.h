@@ -173,6 +173,49 @@ int orac_gpu_ferrf(orac_gpu_ctx* ctx, double fudge, const double* x0,
 int orac_gpu_cself(orac_gpu_ctx* ctx, double kcut, double* self_slt,
                    double* self_slv);
 
+/* Intramolecular terms -------------------------------------------------------
+ * orac_gpu_set_bonded: the bonded terms of mts_intra_n0 / mts_intra_n1 as
+ * ORAC's module arrays hold them, 1-based atoms: stretching lbnd(2, nb) with
+ * r0, kb (fpbond, src/fpbond.f: U = kb (r - r0)^2); bending lbndg(3, nbend)
+ * with bendpot(7, nbend) = pota..potg (fpbend, src/fpbend.f: theta0, k,
+ * Urey-Bradley r0 and k, coupling terms); proper torsions ltor(4, nt) with
+ * tpota = +-n, tpotb = V (fptors, src/fptors.f: U = sig (|V| - V cos n phi),
+ * n = 1..8); improper torsions litr(4, nit) with ipota, ipotb, ipotc (fitors,
+ * src/fitors.f: ipotc > 0 harmonic in phi, else the cosine form).  The bond
+ * list is also the bond list of the erf corrections. */
+int orac_gpu_set_bonded(orac_gpu_ctx* ctx, int nb, const int* lbnd,
+                        const double* r0, const double* kb, int nbend,
+                        const int* lbndg, const double* bendpot, int nt,
+                        const int* ltor, const double* tpota,
+                        const double* tpotb, int nit, const int* litr,
+                        const double* ipota, const double* ipotb,
+                        const double* ipotc);
+
+/* orac_gpu_set_intra_pairs: the pair lists of mts_intra_n1 and mts_furier:
+ * 1-4 pairs int14(2, n14) with type14 into the (already lj_fudge-scaled)
+ * tables ecc1412/ecc146 and the Coulomb fudge (fnb14), the non-excluded
+ * intra-group pairs ingrp(2, ningrp) (fnbgrp, with the topology's LJ
+ * tables) and the 1-3 pairs int13(2, n13) of the erf corrections. */
+int orac_gpu_set_intra_pairs(orac_gpu_ctx* ctx, int n14, const int* int14,
+                             const int* type14, const double* ecc1412,
+                             const double* ecc146, int ntab14, double fudge,
+                             double lj_fudge, int ningrp, const int* ingrp,
+                             int n13, const int* int13);
+
+/* mts_intra_n0 (src/mts_intra_n0.f:73-100): fpbond + fpbend + fitors on
+ * Cartesian coordinates; forces accumulated; energies[6] = ubond, uslvbon,
+ * ubend, uslvben, uitors, uslvitor (set). */
+int orac_gpu_mts_intra_n0(orac_gpu_ctx* ctx, const double* x, const double* y,
+                          const double* z, double* fpx, double* fpy,
+                          double* fpz, double* energies);
+
+/* mts_intra_n1 (src/mts_intra_n1.f:76-118): fptors + fnb14 + fnbgrp;
+ * forces accumulated; energies[10] = uptors, uslvtor, then the 1-4 and the
+ * intra-group terms each as LJ slt, LJ slv, Coulomb slt, Coulomb slv. */
+int orac_gpu_mts_intra_n1(orac_gpu_ctx* ctx, const double* x, const double* y,
+                          const double* z, double* fpx, double* fpy,
+                          double* fpz, double* energies);
+
 /* Shell-kernel variants ----------------------------------------------------
  * mts_forces dispatches to force_rem, force_alchemy or force
  * (src/mts_forces.f:118-153) on the module flags rem_segment and alchemy;

@@ -253,6 +253,7 @@ int orac_gpu_destroy(orac_gpu_ctx* ctx) {
     if (p) cudaFree(p);
   if (ctx->d_wcnt) cudaFree(ctx->d_wcnt);
   variant_free(ctx);
+  bonded_free(ctx);
   for (auto& e : ctx->prof_ev) cudaEventDestroy(e);
   for (int q = 0; q < 3; q++) {
     if (q == 0 && ctx->lists[q].off) cudaFree(ctx->lists[q].off);

@@ -23,6 +23,9 @@
 // Fixed-point scale of the PME charge grid: 2^40 per internal charge unit.
 #define ORAC_QSCALE 1099511627776.0
 
+// doubles per energy record of orac_gpu_md_run
+#define ORAC_MD_REC 16
+
 // Accumulator slots (double) of one force evaluation.
 enum {
   ACC_CONF = 0,   // [3] LJ by type pair: slt-slt, slt-slv, slv-slv
@@ -119,6 +122,40 @@ struct PairArgs {
   float qsoft, ljsoft;
   float af[2][9], afq[2][9];  // FP32 copies of the current tables
   AlchTables at;
+};
+
+// Bonded intramolecular terms (orac_gpu_set_bonded / _set_intra_pairs), the
+// N0 (bonds, bends, impropers) and N1 (torsions, 1-4, intra-group) terms of
+// mts_intra_n0 / mts_intra_n1 and the pair lists of the erf corrections.
+enum { BK_BOND = 1, BK_BEND = 2, BK_TORS = 4, BK_ITORS = 8 };
+struct BondedDev {
+  int nb = 0, nbend = 0, nt = 0, nit = 0;
+  int2* bij = nullptr;     // 0-based atoms
+  double2* bpar = nullptr;  // (r0, k)
+  int4* aijk = nullptr;
+  double* apot = nullptr;   // [7 nbend] pota..potg
+  int4* tijkl = nullptr;
+  double2* tpar = nullptr;  // (+-n, V)
+  int4* iijkl = nullptr;
+  double4* ipar = nullptr;  // (pota, potb, potc, 0)
+  int* ss = nullptr;        // ss_index per atom
+  // 1-based pair lists: 1-4 (with type14 and the scaled tables), intra-group,
+  // 1-3 and bonds (for ferrf), constraints (ferrf, energy only)
+  int n14 = 0, ningrp = 0, n13 = 0, ncn = 0, ntab14 = 0;
+  int* p14 = nullptr;
+  int* t14 = nullptr;
+  double* e1412 = nullptr;
+  double* e146 = nullptr;
+  double fudge = 1.0, lj_fudge = 1.0;
+  int* pgrp = nullptr;
+  int* p13 = nullptr;
+  int* pbond = nullptr;
+  int* pcn = nullptr;
+  int* nbt = nullptr;       // nbtype (1-based) for fnbgrp
+  double* e12 = nullptr;    // LJ tables for fnbgrp
+  double* e6 = nullptr;
+  bool have_pairs = false;
+  double* xs = nullptr;  // [6N + 16] staging of the host entry points
 };
 
 // flags of shell_run_r
@@ -250,6 +287,7 @@ struct orac_gpu_ctx {
   float2* d_soft = nullptr;    // [N]
   double2* d_softd = nullptr;  // [N]
   AlchTables at{};
+  BondedDev bd;
   std::vector<int> h_ssal;            // ss_alchemy
   double lam[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // ladd lrm laddq lrmq and the lambda0 set
   double* d_qc = nullptr;  // [N] PME charges at lambda: (1 - |lambdaq_i|) q_i
@@ -342,6 +380,18 @@ int small_launch(orac_gpu_ctx* ctx, int kind, const double* d_xyz,
                  double lj_fudge, int coul_mode, int forces, double* d_f,
                  double* d_e, const int* d_ss);
 int self_launch(orac_gpu_ctx* ctx, const int* d_ss, double* d_e);
+// the same with explicit charges (null: the topology's) and an optional
+// fixed-point force output (the MD driver's level accumulators)
+int small_launch_x(orac_gpu_ctx* ctx, int kind, const double* d_xyz, const int* d_pairs, const int* d_ptype,
+                   int npairs, const double* d_t12, const double* d_t6, double fudge, double lj_fudge,
+                   int coul_mode, int forces, double* d_f, double* d_e, const int* d_ss, const double* d_q,
+                   unsigned long long* d_ffix);
+// k_bonded.cu: mask of BK_* kinds; forces into d_f (FP64 atomics) or d_ffix
+// (fixed point); d_e[8] (bond, bend, tors, itors) x (slt, slv) or null
+int bonded_launch(orac_gpu_ctx* ctx, int mask, const double* d_x, double* d_f, unsigned long long* d_ffix,
+                  double* d_e);
+void bonded_free(orac_gpu_ctx* ctx);
+int bonded_set_constraints(orac_gpu_ctx* ctx, const int* cnst, int ncnst);
 // api.cu
 int shell_run(orac_gpu_ctx* ctx, char rshell, const double* d_xyz,
               const double* d_grp, const double* d_mol, double* d_f,

@@ -35,6 +35,7 @@ struct SmallArgs {
   int forces;
   double* f;  // [3N]
   double* e;  // [4]
+  unsigned long long* ffix;  // [3N] fixed-point output instead of f (or null)
 };
 
 __global__ void k_small(const SmallArgs A) {
@@ -91,7 +92,17 @@ __global__ void k_small(const SmallArgs A) {
         qforce += sv * rsqi;
       }
     }
-    if (A.forces) {
+    if (A.forces && A.ffix) {
+      const double fv[3] = {qforce * xa, qforce * ya, qforce * za};
+#pragma unroll
+      for (int d = 0; d < 3; d++) {
+        const long long q = __double2ll_rn(fv[d] * ORAC_FSCALE);
+        if (q) {
+          atomicAdd(A.ffix + d * A.natom + i1, (unsigned long long)q);
+          atomicAdd(A.ffix + d * A.natom + i2, (unsigned long long)(-q));
+        }
+      }
+    } else if (A.forces) {
       atomicAdd(A.f + i1, qforce * xa);
       atomicAdd(A.f + A.natom + i1, qforce * ya);
       atomicAdd(A.f + 2 * A.natom + i1, qforce * za);
@@ -108,7 +119,7 @@ __global__ void k_small(const SmallArgs A) {
     if (lane == 0) s[w][q] = x;
   }
   __syncthreads();
-  if (threadIdx.x < 4) {
+  if (A.e && threadIdx.x < 4) {
     double x = 0;
     for (int k = 0; k < (int)(blockDim.x >> 5); k++) x += s[k][threadIdx.x];
     if (x != 0.0) atomicAdd(A.e + threadIdx.x, x);
@@ -138,6 +149,14 @@ __global__ void k_self(int n, const double* q, const int* ss, double* e) {
 int small_launch(orac_gpu_ctx* ctx, int kind, const double* d_xyz, const int* d_pairs, const int* d_ptype, int npairs,
                  const double* d_t12, const double* d_t6, double fudge, double lj_fudge, int coul_mode, int forces,
                  double* d_f, double* d_e, const int* d_ss) {
+  return small_launch_x(ctx, kind, d_xyz, d_pairs, d_ptype, npairs, d_t12, d_t6, fudge, lj_fudge, coul_mode, forces,
+                        d_f, d_e, d_ss, nullptr, nullptr);
+}
+
+int small_launch_x(orac_gpu_ctx* ctx, int kind, const double* d_xyz, const int* d_pairs, const int* d_ptype,
+                   int npairs, const double* d_t12, const double* d_t6, double fudge, double lj_fudge,
+                   int coul_mode, int forces, double* d_f, double* d_e, const int* d_ss, const double* d_q,
+                   unsigned long long* d_ffix) {
   SmallArgs A;
   memset(&A, 0, sizeof(A));
   A.kind = kind;
@@ -148,8 +167,9 @@ int small_launch(orac_gpu_ctx* ctx, int kind, const double* d_xyz, const int* d_
   A.ptype = d_ptype;
   A.tab12 = d_t12;
   A.tab6 = d_t6;
-  A.q = ctx->d_aqd;
+  A.q = d_q ? d_q : ctx->d_aqd;
   A.ss = d_ss;
+  A.ffix = d_ffix;
   A.alpha = ctx->alphal;
   A.fudge = fudge;
   A.lj_fudge = lj_fudge;

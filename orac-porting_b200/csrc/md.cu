@@ -39,6 +39,7 @@ namespace {
 
 constexpr int SMA = 4;  // atoms of a register-solved molecule
 constexpr int SMC = 3;  // constraints of a register-solved molecule
+constexpr int NLV = 5;  // r-RESPA force levels: H, L, M, N1, N0
 
 __device__ __forceinline__ double dot3(const double* a, const double* b) {
   return a[0] * b[0] + a[1] * b[1] + a[2] * b[2];
@@ -106,9 +107,17 @@ struct MolArgs {
   double* grp;       // [3G] scaled group centres (for the list builder)
   double4* gpos;     // [G]
   float4* aoff;      // [N]
-  unsigned long long* fzero;  // [3N] accumulator zeroed for the coming shell (or null)
-  const unsigned long long* fkick;  // [3N] fixed-point forces of a kick
-  const double* fn;  // [3N] intramolecular forces for the drift (or null)
+  // kick: v += sum_l ck[l] f_l / m over the level accumulators, then RATTLE
+  // (several correc + rattle_correc calls of one instant merged: RATTLE is a
+  // linear projection, so one projection of the summed kick is the same)
+  const unsigned long long* fk[NLV];
+  double ck[NLV];
+  int kick;
+  // the N0 force of the verlet step (src/verlet.f: half kick without
+  // RATTLE, then the drift), or null
+  const unsigned long long* fv;
+  // accumulators zeroed for the evaluations that follow this drift
+  unsigned long long* fz[NLV];
   double dt;
   double tol;
   int* flag;
@@ -301,12 +310,19 @@ __device__ __forceinline__ bool shake_small(double x[SMA][3], const double xo[SM
   return ok;
 }
 
-// correc (v += f dt/2m) from a fixed-point level accumulator, then RATTLE.
+__device__ __forceinline__ double kick_dv(const MolArgs& A, int i) {
+  double dv = 0.0;
+#pragma unroll
+  for (int l = 0; l < NLV; l++)
+    if (A.ck[l] != 0.0) dv += A.ck[l] * fixd(A.fk[l][i]);
+  return dv;
+}
+
+// correc (v += f dt/2m) from the fixed-point level accumulators, then RATTLE.
 // Threads [0, nsm) take one small molecule each, the rest one free atom.
 __global__ void k_kick(const MolArgs A) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int N = A.N;
-  const double hdt = 0.5 * A.dt;
   if (t < A.nsm) {
     const int4 m = A.sm[t];
     double x[SMA][3], v[SMA][3], im[SMA];
@@ -318,9 +334,9 @@ __global__ void k_kick(const MolArgs A) {
         x[a][0] = A.x[g];
         x[a][1] = A.x[N + g];
         x[a][2] = A.x[2 * N + g];
-        v[a][0] = A.v[g] + fixd(A.fkick[g]) * hdt * im[a];
-        v[a][1] = A.v[N + g] + fixd(A.fkick[N + g]) * hdt * im[a];
-        v[a][2] = A.v[2 * N + g] + fixd(A.fkick[2 * N + g]) * hdt * im[a];
+        v[a][0] = A.v[g] + kick_dv(A, g) * im[a];
+        v[a][1] = A.v[N + g] + kick_dv(A, N + g) * im[a];
+        v[a][2] = A.v[2 * N + g] + kick_dv(A, 2 * N + g) * im[a];
       } else {
         im[a] = 0;
         x[a][0] = x[a][1] = x[a][2] = 0;
@@ -340,9 +356,9 @@ __global__ void k_kick(const MolArgs A) {
   } else if (t < A.nsm + A.nfree) {
     const int g = A.free_atoms[t - A.nsm];
     const double im = A.invm[g];
-    A.v[g] += fixd(A.fkick[g]) * hdt * im;
-    A.v[N + g] += fixd(A.fkick[N + g]) * hdt * im;
-    A.v[2 * N + g] += fixd(A.fkick[2 * N + g]) * hdt * im;
+    A.v[g] += kick_dv(A, g) * im;
+    A.v[N + g] += kick_dv(A, N + g) * im;
+    A.v[2 * N + g] += kick_dv(A, 2 * N + g) * im;
   }
 }
 
@@ -363,16 +379,28 @@ __global__ void k_drift(const MolArgs A) {
         im[a] = A.invm[g];
 #pragma unroll
         for (int d = 0; d < 3; d++) {
-          const double f = A.fn ? A.fn[d * N + g] : 0.0;
           xo[a][d] = A.x[d * N + g];
           v[a][d] = A.v[d * N + g];
-          x[a][d] = xo[a][d] + dt * v[a][d] + f * 0.5 * dt * dt * im[a];
-          v[a][d] += f * 0.5 * dt * im[a];
+          if (A.kick) v[a][d] += kick_dv(A, d * N + g) * im[a];
         }
       } else {
         im[a] = 0;
 #pragma unroll
         for (int d = 0; d < 3; d++) x[a][d] = xo[a][d] = v[a][d] = 0.0;
+      }
+    }
+    if (A.kick && m.w > 0)
+      if (!rattle_small(xo, v, im, A.cloc + m.z, m.w)) atomicOr(A.flag, 1);
+#pragma unroll
+    for (int a = 0; a < SMA; a++) {
+      if (a < m.y) {
+        const int g = m.x + a;
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+          const double f = A.fv ? fixd(A.fv[d * N + g]) : 0.0;
+          x[a][d] = xo[a][d] + dt * v[a][d] + f * 0.5 * dt * dt * im[a];
+          v[a][d] += f * 0.5 * dt * im[a];
+        }
       }
     }
     if (m.w > 0) {
@@ -389,7 +417,9 @@ __global__ void k_drift(const MolArgs A) {
           A.x[d * N + g] = x[a][d];
           A.xo[d * N + g] = xo[a][d];
           A.v[d * N + g] = v[a][d];
-          if (A.fzero) A.fzero[d * N + g] = 0ull;
+#pragma unroll
+          for (int l = 0; l < NLV; l++)
+            if (A.fz[l]) A.fz[l][d * N + g] = 0ull;
         }
         s[a][0] = A.o11 * x[a][0] + A.o12 * x[a][1] + A.o13 * x[a][2];
         s[a][1] = A.o22 * x[a][1] + A.o23 * x[a][2];
@@ -429,12 +459,17 @@ __global__ void k_drift(const MolArgs A) {
     const double im = A.invm[g];
 #pragma unroll
     for (int d = 0; d < 3; d++) {
-      const double f = A.fn ? A.fn[d * N + g] : 0.0;
-      const double xo = A.x[d * N + g];
-      A.xo[d * N + g] = xo;
-      A.x[d * N + g] = xo + dt * A.v[d * N + g] + f * 0.5 * dt * dt * im;
-      A.v[d * N + g] += f * 0.5 * dt * im;
-      if (A.fzero) A.fzero[d * N + g] = 0ull;
+      const int i = d * N + g;
+      const double f = A.fv ? fixd(A.fv[i]) : 0.0;
+      double v = A.v[i];
+      if (A.kick) v += kick_dv(A, i) * im;
+      const double xo = A.x[i];
+      A.xo[i] = xo;
+      A.x[i] = xo + dt * v + f * 0.5 * dt * dt * im;
+      A.v[i] = v + f * 0.5 * dt * im;
+#pragma unroll
+      for (int l = 0; l < NLV; l++)
+        if (A.fz[l]) A.fz[l][i] = 0ull;
     }
   }
 }
@@ -578,8 +613,9 @@ struct MdState {
   double* x = nullptr;  // [3N] Cartesian
   double* v = nullptr;
   double* xo = nullptr;
-  unsigned long long* ffix[3] = {nullptr, nullptr, nullptr};  // H, L, M accumulators
-  double* fn = nullptr;   // intramolecular (N0/N1) forces; null without bonded terms
+  // level accumulators H, L, M, N1, N0 (N1/N0 only with intramolecular terms)
+  unsigned long long* ffix[NLV] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  bool has_n0 = false, has_n1 = false;
   double* invm = nullptr;
   double* pm = nullptr;
   // small constrained molecules
@@ -597,7 +633,9 @@ struct MdState {
   int* bstart = nullptr;
   int2* bcab = nullptr;
   double* bdss = nullptr;
-  // energies: [0..7] M, [8..15] L, [16..23] H (ORAC order), [24..39] SPME eout, [40] ekin
+  // energies: [0..7] M, [8..15] L, [16..23] H (ORAC order), [24..39] SPME
+  // eout, [40] ekin, [E_BOND..+8) bonded, [E_14..+4) 1-4, [E_GRP..+4)
+  // intra-group, [E_ERF..+16) erf corrections (bonds, constraints, 1-3, 1-4)
   double* e = nullptr;
   int* flag = nullptr;
   // schedule
@@ -628,7 +666,8 @@ void md_destroy(orac_gpu_ctx* ctx) {
   if (S->graph) cudaGraphDestroy(S->graph);
   if (S->gexec_u) cudaGraphExecDestroy(S->gexec_u);
   if (S->graph_u) cudaGraphDestroy(S->graph_u);
-  void* ptrs[] = {S->x,         S->v,        S->xo,          S->ffix[0],   S->ffix[1], S->ffix[2], S->fn,
+  void* ptrs[] = {S->x,         S->v,        S->xo,          S->ffix[0],   S->ffix[1], S->ffix[2], S->ffix[3],
+                  S->ffix[4],
                   S->invm,      S->pm,       S->sm,          S->smg,       S->cloc,    S->cdss,    S->free_atoms,
                   S->free_groups, S->bstart, S->bcab,        S->bdss,      S->e,       S->flag};
   for (void* p : ptrs)
@@ -675,7 +714,6 @@ static MolArgs mol_args(orac_gpu_ctx* ctx, MdState& S, double dt) {
   A.grp = ctx->d_grp;
   A.gpos = ctx->d_gpos;
   A.aoff = ctx->d_aoff;
-  A.fn = S.fn;
   A.dt = dt;
   A.tol = 1e-12;
   A.flag = S.flag;
@@ -700,23 +738,46 @@ static ConsArgs big_args(orac_gpu_ctx* ctx, MdState& S, double dt, double tol) {
   return A;
 }
 
-static int md_kick(orac_gpu_ctx* ctx, MdState& S, int lvl, double dt) {
-  MolArgs A = mol_args(ctx, S, dt);
-  A.fkick = S.ffix[lvl];
+enum { LH = 0, LL = 1, LM = 2, LN1 = 3, LN0 = 4 };
+enum { E_BOND = 41, E_14 = 49, E_GRP = 53, E_ERF = 57, E_N = 80 };
+
+// kick of the level accumulators with velocity factors c[l] (0: skip) + RATTLE
+static void kick_fill(MolArgs& A, MdState& S, const double* c) {
+  A.kick = 0;
+  for (int l = 0; l < NLV; l++) {
+    A.fk[l] = S.ffix[l];
+    A.ck[l] = (c && S.ffix[l]) ? c[l] : 0.0;
+    if (A.ck[l] != 0.0) A.kick = 1;
+  }
+}
+
+static int md_kick(orac_gpu_ctx* ctx, MdState& S, const double* c) {
+  MolArgs A = mol_args(ctx, S, 0.0);
+  kick_fill(A, S, c);
+  if (!A.kick) return ORAC_OK;
   const int n = S.nsm + S.nfree;
   k_kick<<<(n + 31) / 32, 32, 0, ctx->stream>>>(A);
   CKL();
   if (S.nbig) {
-    k_rattle_big<<<(S.nbig + 127) / 128, 128, 0, ctx->stream>>>(big_args(ctx, S, dt, 1e-12));
+    k_rattle_big<<<(S.nbig + 127) / 128, 128, 0, ctx->stream>>>(big_args(ctx, S, 0.0, 1e-12));
     CKL();
   }
   return ORAC_OK;
 }
 
-// drift + constraints + scaled frame + pair-kernel inputs; zeroes `fzero`
-static int md_drift(orac_gpu_ctx* ctx, MdState& S, double dt, unsigned long long* fzero) {
+// [kick c + RATTLE] + verlet drift of dt (with the N0 half kick when
+// present) + SHAKE + RATTLE, scaled frame and pair-kernel inputs; zeroes the
+// accumulators of the levels in `zmask` (bit l) after reading them
+static int md_drift(orac_gpu_ctx* ctx, MdState& S, double dt, const double* c, int zmask) {
+  if (S.nbig && c) {
+    // the RATTLE of large molecules is a separate kernel: kick first
+    if (int rc = md_kick(ctx, S, c)) return rc;
+    c = nullptr;
+  }
   MolArgs A = mol_args(ctx, S, dt);
-  A.fzero = fzero;
+  kick_fill(A, S, c);
+  A.fv = S.has_n0 ? S.ffix[LN0] : nullptr;
+  for (int l = 0; l < NLV; l++) A.fz[l] = ((zmask >> l) & 1) ? S.ffix[l] : nullptr;
   const int n = S.nsm + S.nfree;
   k_drift<<<(n + 31) / 32, 32, 0, ctx->stream>>>(A);
   CKL();
@@ -733,7 +794,34 @@ static int md_drift(orac_gpu_ctx* ctx, MdState& S, double dt, unsigned long long
   return ORAC_OK;
 }
 
-// one shell's forces into the level accumulator (already zeroed or zeroed here)
+// erf corrections of the excluded pairs at the reciprocal level
+// (mts_furier, src/mts_furier.f:85-141): bonds and 1-3 pairs with forces,
+// 1-4 pairs with fudgec = 1 - fudge (src/mtsmd.f:474), constraints energy
+// only (their forces would be removed by the constraints)
+static int md_ferrf(orac_gpu_ctx* ctx, MdState& S, unsigned long long* f, bool energy) {
+  const BondedDev& B = ctx->bd;
+  const double* q = ctx->pme_q();
+  if (B.nb > 0)
+    if (int rc = small_launch_x(ctx, 2, S.x, B.pbond, nullptr, B.nb, nullptr, nullptr, 1.0, 1.0, 1, 1, nullptr,
+                                energy ? S.e + E_ERF : nullptr, B.ss, q, f))
+      return rc;
+  if (energy && B.ncn > 0)
+    if (int rc = small_launch_x(ctx, 2, S.x, B.pcn, nullptr, B.ncn, nullptr, nullptr, 1.0, 1.0, 1, 0, nullptr,
+                                S.e + E_ERF + 4, B.ss, q, nullptr))
+      return rc;
+  if (B.n13 > 0)
+    if (int rc = small_launch_x(ctx, 2, S.x, B.p13, nullptr, B.n13, nullptr, nullptr, 1.0, 1.0, 1, 1, nullptr,
+                                energy ? S.e + E_ERF + 8 : nullptr, B.ss, q, f))
+      return rc;
+  if (B.n14 > 0)
+    if (int rc = small_launch_x(ctx, 2, S.x, B.p14, nullptr, B.n14, nullptr, nullptr, 1.0 - B.fudge, 1.0, 1, 1,
+                                nullptr, energy ? S.e + E_ERF + 12 : nullptr, B.ss, q, f))
+      return rc;
+  return ORAC_OK;
+}
+
+// one shell's forces into its level accumulator (zeroed by the preceding
+// drift, or here when `zero`)
 static int md_forces_shell(orac_gpu_ctx* ctx, MdState& S, char sh, int lvl, bool zero, double* e, bool energy) {
   unsigned long long* f = S.ffix[lvl];
   if (zero) CK(cudaMemsetAsync(f, 0, sizeof(unsigned long long) * 3 * ctx->N, ctx->stream));
@@ -748,6 +836,27 @@ static int md_forces_shell(orac_gpu_ctx* ctx, MdState& S, char sh, int lvl, bool
     if (int rc = pme_run(ctx, ctx->N, S.x, ctx->pme_q(), recip, ctx->volume, ctx->alphal, nullptr, S.e + 24, nullptr,
                          nullptr, f))
       return rc;
+    if (int rc = md_ferrf(ctx, S, f, energy)) return rc;
+  }
+  return ORAC_OK;
+}
+
+// mts_intra_n0 / mts_intra_n1 into their level accumulators
+static int md_forces_intra(orac_gpu_ctx* ctx, MdState& S, int lvl, bool energy) {
+  const BondedDev& B = ctx->bd;
+  if (lvl == LN0)
+    return bonded_launch(ctx, BK_BOND | BK_BEND | BK_ITORS, S.x, nullptr, S.ffix[LN0], energy ? S.e + E_BOND : nullptr);
+  if (int rc = bonded_launch(ctx, BK_TORS, S.x, nullptr, S.ffix[LN1], energy ? S.e + E_BOND : nullptr)) return rc;
+  if (B.have_pairs) {
+    const int coul = ctx->clewld ? 1 : 0;
+    if (B.n14 > 0)
+      if (int rc = small_launch_x(ctx, 0, S.x, B.p14, B.t14, B.n14, B.e1412, B.e146, B.fudge, B.lj_fudge, coul, 1,
+                                  nullptr, energy ? S.e + E_14 : nullptr, B.ss, nullptr, S.ffix[LN1]))
+        return rc;
+    if (B.ningrp > 0)
+      if (int rc = small_launch_x(ctx, 1, S.x, B.pgrp, B.nbt, B.ningrp, B.e12, B.e6, 1.0, 1.0, coul, 1, nullptr,
+                                  energy ? S.e + E_GRP : nullptr, B.ss, nullptr, S.ffix[LN1]))
+        return rc;
   }
   return ORAC_OK;
 }
@@ -770,36 +879,64 @@ static int md_list_update(orac_gpu_ctx* ctx, MdState& S) {
   return md_phony(ctx, r2, 'l');
 }
 
-enum { LH = 0, LL = 1, LM = 2 };
-
-// one outer step; energies of the last evaluations when `energy`
+// One outer step as a sequence of K = lrespa mrespa n1respa n0respa drifts
+// of tn0.  Level l (periods pN0 = 1, pN1 = n0respa, pM = pN1 n1respa, pL =
+// pM mrespa, pH = K drifts) ends its inner step after drift k when
+// (k+1) % p == 0: its forces are evaluated there, and its end half kick
+// and the next step's start half kick (correc + rattle_correc twice at the
+// same instant) are applied together before the next drift.  The start half
+// kicks of the outer step go before the first drift; all end half kicks come
+// after the last force evaluation.  The N0 start half kick is verlet's,
+// without RATTLE (src/verlet.f), as in ORAC's n0 loop
+// (src/mtsmd.f:2641-2930).
 static int md_step(orac_gpu_ctx* ctx, MdState& S, bool update, bool energy) {
   if (update)
     if (int rc = md_list_update(ctx, S)) return rc;
-  if (int rc = md_kick(ctx, S, LH, S.dth)) return rc;
-  const double tl = S.dth / S.lrespa;
-  const double tm = tl / S.mrespa;
-  for (int il = 0; il < S.lrespa; il++) {
-    if (int rc = md_kick(ctx, S, LL, tl)) return rc;
-    for (int im = 0; im < S.mrespa; im++) {
-      if (int rc = md_kick(ctx, S, LM, tm)) return rc;
-      // intramolecular levels: with no N0/N1 forces the n1respa*n0respa
-      // verlet steps compose into one drift of tm
-      if (int rc = md_drift(ctx, S, tm, S.ffix[LM])) return rc;
-      const bool last = energy && il == S.lrespa - 1 && im == S.mrespa - 1;
-      if (int rc = md_forces_shell(ctx, S, 'm', LM, false, S.e, last)) return rc;
-      if (int rc = md_kick(ctx, S, LM, tm)) return rc;
+  if (energy) CK(cudaMemsetAsync(S.e + E_BOND, 0, sizeof(double) * (E_N - E_BOND), ctx->stream));
+  const int n0 = S.n0respa, n1 = S.n1respa;
+  const int per[NLV] = {S.lrespa * S.mrespa * n1 * n0, S.mrespa * n1 * n0, n1 * n0, n0, 1};
+  const int K = per[LH];
+  double dt[NLV];
+  dt[LH] = S.dth;
+  dt[LL] = dt[LH] / S.lrespa;
+  dt[LM] = dt[LL] / S.mrespa;
+  dt[LN1] = dt[LM] / n1;
+  dt[LN0] = dt[LN1] / n0;
+  for (int k = 0; k < K; k++) {
+    double c[NLV] = {0, 0, 0, 0, 0};
+    if (k == 0) {
+      for (int l = 0; l < LN0; l++) c[l] = 0.5 * dt[l];
+    } else {
+      c[LN0] = 0.5 * dt[LN0];  // end half kick of the last N0 step (the start one is verlet's)
+      for (int l = LL; l < LN0; l++)
+        if (k % per[l] == 0) c[l] = dt[l];
     }
-    if (int rc = md_forces_shell(ctx, S, 'l', LL, true, S.e + 8, energy && il == S.lrespa - 1)) return rc;
-    if (int rc = md_kick(ctx, S, LL, tl)) return rc;
+    int zmask = 0;
+    for (int l = 0; l < NLV; l++)
+      if ((k + 1) % per[l] == 0) zmask |= 1 << l;
+    if (int rc = md_drift(ctx, S, dt[LN0], c, zmask)) return rc;
+    const bool last = k == K - 1;
+    const bool e_now = energy && last;
+    if (S.has_n0)
+      if (int rc = md_forces_intra(ctx, S, LN0, e_now)) return rc;
+    if (S.has_n1 && (k + 1) % per[LN1] == 0)
+      if (int rc = md_forces_intra(ctx, S, LN1, e_now)) return rc;
+    if ((k + 1) % per[LM] == 0)
+      if (int rc = md_forces_shell(ctx, S, 'm', LM, false, S.e, e_now)) return rc;
+    if ((k + 1) % per[LL] == 0)
+      if (int rc = md_forces_shell(ctx, S, 'l', LL, false, S.e + 8, e_now)) return rc;
   }
-  if (int rc = md_forces_shell(ctx, S, 'h', LH, true, S.e + 16, energy)) return rc;
+  if (int rc = md_forces_shell(ctx, S, 'h', LH, false, S.e + 16, energy)) return rc;
   {
     ShellRadii r = ctx->sh;
     r.rcutl = r.rcutm;
     if (int rc = md_phony(ctx, r, 'l')) return rc;
   }
-  if (int rc = md_kick(ctx, S, LH, S.dth)) return rc;
+  {
+    double c[NLV];
+    for (int l = 0; l < NLV; l++) c[l] = 0.5 * dt[l];
+    if (int rc = md_kick(ctx, S, c)) return rc;
+  }
   if (energy) {
     CK(cudaMemsetAsync(S.e + 40, 0, sizeof(double), ctx->stream));
     k_ekin<<<64, 256, 0, ctx->stream>>>(ctx->N, S.v, S.invm, S.e + 40);
@@ -829,9 +966,20 @@ int orac_gpu_md_setup(orac_gpu_ctx* ctx, const double* x, const double* y, const
   if (dev_alloc(ctx, &S.x, 3 * (size_t)N) || dev_alloc(ctx, &S.v, 3 * (size_t)N) ||
       dev_alloc(ctx, &S.xo, 3 * (size_t)N) || dev_alloc(ctx, &S.ffix[0], 3 * (size_t)N) ||
       dev_alloc(ctx, &S.ffix[1], 3 * (size_t)N) || dev_alloc(ctx, &S.ffix[2], 3 * (size_t)N) ||
-      dev_alloc(ctx, &S.invm, N) || dev_alloc(ctx, &S.pm, N) || dev_alloc(ctx, &S.e, 48) ||
+      dev_alloc(ctx, &S.invm, N) || dev_alloc(ctx, &S.pm, N) || dev_alloc(ctx, &S.e, 96) ||
       dev_alloc(ctx, &S.flag, 4))
     return ORAC_ERR_CUDA;
+  {
+    // intramolecular levels (mts_intra_n0 / mts_intra_n1) when the topology has terms for them
+    const BondedDev& B = ctx->bd;
+    S.has_n0 = B.nb + B.nbend + B.nit > 0;
+    S.has_n1 = B.nt > 0 || (B.have_pairs && B.n14 + B.ningrp > 0);
+    if ((S.has_n1 && dev_alloc(ctx, &S.ffix[LN1], 3 * (size_t)N)) ||
+        (S.has_n0 && dev_alloc(ctx, &S.ffix[LN0], 3 * (size_t)N)))
+      return ORAC_ERR_CUDA;
+    CK(cudaMemset(S.e, 0, sizeof(double) * 96));
+  }
+  if (int rc = bonded_set_constraints(ctx, cnst, ncnst)) return rc;
   const double* src[2][3] = {{x, y, z}, {vx, vy, vz}};
   double* dst[2] = {S.x, S.v};
   for (int k = 0; k < 2; k++)
@@ -929,7 +1077,7 @@ int orac_gpu_md_setup(orac_gpu_ctx* ctx, const double* x, const double* y, const
   // zero length); then the first list build with host synchronisation (it
   // sizes the list capacity with 30% headroom for in-graph rebuilds) and the
   // first forces (src/mtsmd.f:1986-2152)
-  if (int rc = md_drift(ctx, S, 0.0, nullptr)) return rc;
+  if (int rc = md_drift(ctx, S, 0.0, nullptr, 0)) return rc;
   const ShellRadii r = ctx->sh;
   const double rc_h = r.rcuth + r.rtolh + r.rneih;
   if (int rc = list_prepare_stencil(ctx, rc_h)) return rc;
@@ -961,6 +1109,11 @@ int orac_gpu_md_setup(orac_gpu_ctx* ctx, const double* x, const double* y, const
   if (int rc = md_forces_shell(ctx, S, 'm', LM, true, S.e, true)) return rc;
   if (int rc = md_forces_shell(ctx, S, 'l', LL, true, S.e + 8, true)) return rc;
   if (int rc = md_forces_shell(ctx, S, 'h', LH, true, S.e + 16, true)) return rc;
+  for (int l = LN1; l <= LN0; l++) {
+    if (!S.ffix[l]) continue;
+    CK(cudaMemsetAsync(S.ffix[l], 0, sizeof(unsigned long long) * 3 * (size_t)N, ctx->stream));
+    if (int rc = md_forces_intra(ctx, S, l, false)) return rc;
+  }
   {
     ShellRadii rr = ctx->sh;
     rr.rcutl = rr.rcutm;
@@ -972,8 +1125,10 @@ int orac_gpu_md_setup(orac_gpu_ctx* ctx, const double* x, const double* y, const
 }
 
 // Run nsteps outer steps.  Every `energy_every` steps (0: never) one record
-// of NE = 12 doubles is written to rec (host): step, ekin, U_M (LJ, Coul),
-// U_L (LJ, Coul), U_H (LJ, Coul), E_rec, econst, total, flag.
+// of ORAC_MD_REC = 16 doubles is written to rec (host): step, ekin, U_M (LJ,
+// Coul), U_L (LJ, Coul), U_H (LJ, Coul), E_rec, econst, total, flag,
+// bonded (bonds, bends, torsions, impropers), 1-4 + intra-group, erf
+// corrections, 0.
 int orac_gpu_md_run(orac_gpu_ctx* ctx, int nsteps, int energy_every, double* rec) {
   return md_run_impl(ctx, nsteps, energy_every, rec, false);
 }
@@ -1113,12 +1268,12 @@ static int md_run_impl(orac_gpu_ctx* ctx, int nsteps, int energy_every, double* 
     }
     S.step++;
     if (energy) {
-      double e[48];
+      double e[96];
       int flag = 0;
-      CK(cudaMemcpyAsync(e, S.e, sizeof(double) * 48, cudaMemcpyDeviceToHost, ctx->stream));
+      CK(cudaMemcpyAsync(e, S.e, sizeof(double) * 96, cudaMemcpyDeviceToHost, ctx->stream));
       CK(cudaMemcpyAsync(&flag, S.flag, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
       CK(cudaStreamSynchronize(ctx->stream));
-      double* r = rec + 12 * (size_t)nrec++;
+      double* r = rec + ORAC_MD_REC * (size_t)nrec++;
       r[0] = (double)S.step;
       r[1] = e[40];
       r[2] = e[4] + e[0] + e[6];  // M: ucnp + ucns + ucnsp
@@ -1129,7 +1284,11 @@ static int md_run_impl(orac_gpu_ctx* ctx, int nsteps, int energy_every, double* 
       r[7] = e[21] + e[17] + e[23];
       r[8] = 0.5 * e[24];
       r[9] = S.econst;
-      r[10] = r[1] + r[2] + r[3] + r[4] + r[5] + r[6] + r[7] + r[8] + r[9];
+      r[12] = r[13] = r[14] = r[15] = 0.0;
+      for (int q = E_BOND; q < E_14; q++) r[12] += e[q];
+      for (int q = E_14; q < E_ERF; q++) r[13] += e[q];
+      for (int q = E_ERF; q < E_N; q++) r[14] += e[q];
+      r[10] = r[1] + r[2] + r[3] + r[4] + r[5] + r[6] + r[7] + r[8] + r[9] + r[12] + r[13] + r[14];
       r[11] = (double)flag;
     }
   }

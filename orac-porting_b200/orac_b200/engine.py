@@ -60,6 +60,38 @@ class Engine:
             check(self.ctx, self.lib.orac_gpu_set_linked_cell(self.ctx, 0, 0, 0), "set_linked_cell")
         self.set_box(s.co)
         self._coords()
+        if s.has_intra():
+            self._upload_intra()
+
+    def _upload_intra(self):
+        """Bonded terms and intramolecular pair lists (orac_gpu_set_bonded,
+        orac_gpu_set_intra_pairs)."""
+        s = self.s
+        a = s.intra_lists()
+        self._intra = a
+        check(self.ctx, self.lib.orac_gpu_set_bonded(
+            self.ctx, len(a["lbnd"]) // 2, a["lbnd"], a["r0"], a["kb"], len(a["lbndg"]) // 3, a["lbndg"],
+            a["bendpot"], len(a["ltor"]) // 4, a["ltor"], a["tpota"], a["tpotb"], len(a["litr"]) // 4, a["litr"],
+            a["ipota"], a["ipotb"], a["ipotc"]), "set_bonded")
+        check(self.ctx, self.lib.orac_gpu_set_intra_pairs(
+            self.ctx, len(a["int14"]) // 2, a["int14"], a["type14"], a["ecc1412"], a["ecc146"], len(a["ecc1412"]),
+            s.fudge, 1.0, len(a["ingrp"]) // 2, a["ingrp"], len(a["int13"]) // 2, a["int13"]), "set_intra_pairs")
+
+    def intra_n0(self):
+        """mts_intra_n0: (F (3,N), energies[6])."""
+        r = self.s.cartesian()
+        F = [np.zeros(self.s.ntap) for _ in range(3)]
+        e = np.zeros(6)
+        check(self.ctx, self.lib.orac_gpu_mts_intra_n0(self.ctx, f64(r[0]), f64(r[1]), f64(r[2]), *F, e), "intra_n0")
+        return np.stack(F), e
+
+    def intra_n1(self):
+        """mts_intra_n1: (F (3,N), energies[10])."""
+        r = self.s.cartesian()
+        F = [np.zeros(self.s.ntap) for _ in range(3)]
+        e = np.zeros(10)
+        check(self.ctx, self.lib.orac_gpu_mts_intra_n1(self.ctx, f64(r[0]), f64(r[1]), f64(r[2]), *F, e), "intra_n1")
+        return np.stack(F), e
 
     def set_shells(self, sh):
         check(self.ctx, self.lib.orac_gpu_set_shells(self.ctx, sh.rcutm, sh.rtolm, sh.rneim, sh.rcutl, sh.rtoll,
@@ -249,11 +281,17 @@ class Engine:
               "md_setup")
         check(self.ctx, self.lib.orac_gpu_md_set_graphs(self.ctx, int(graphs)), "md_set_graphs")
 
+    MD_REC = 16  # doubles per energy record (ORAC_MD_REC)
+
     def md_run(self, nsteps, energy_every=0):
+        """nsteps outer steps; every energy_every steps a record of MD_REC
+        doubles: step, kinetic, (LJ, Coulomb) of M, L, H, SPME, constant,
+        total, flags, bonded, 1-4 + intra-group, erf corrections, 0."""
+        R = self.MD_REC
         nrec = nsteps // energy_every if energy_every else 0
-        rec = np.zeros(max(1, nrec) * 12)
+        rec = np.zeros(max(1, nrec) * R)
         check(self.ctx, self.lib.orac_gpu_md_run(self.ctx, nsteps, energy_every, rec), "md_run")
-        return rec[:nrec * 12].reshape(-1, 12)
+        return rec[:nrec * R].reshape(-1, R)
 
     def md_state(self):
         n = self.s.ntap

@@ -66,6 +66,10 @@ def load():
         "orac_gpu_cself": (i, [_P, d, _DP, _DP]),
         "orac_gpu_mts_forces_dev": (i, [_P, ch, _P, _P, _P, _P, _P, _P]),
         "orac_gpu_fft_pme_dev": (i, [_P, _P, _P, _P, _P, _P]),
+        "orac_gpu_set_bonded": (i, [_P, i, _I, _D, _D, i, _I, _D, i, _I, _D, _D, i, _I, _D, _D, _D]),
+        "orac_gpu_set_intra_pairs": (i, [_P, i, _I, _I, _D, _D, i, d, d, i, _I, i, _I]),
+        "orac_gpu_mts_intra_n0": (i, [_P, _D, _D, _D, _D, _D, _D, _D]),
+        "orac_gpu_mts_intra_n1": (i, [_P, _D, _D, _D, _D, _D, _D, _D]),
         "orac_gpu_set_rem": (i, [_P, _I, i, d]),
         "orac_gpu_set_alchemy": (i, [_P, _I, _D, _D, d, d, i]),
         "orac_gpu_set_lambda": (i, [_P, _D, i, i, _P]),

@@ -105,6 +105,55 @@ class System:
     # REM segment (force_rem): 1 for atoms of the scaled segment
     rematom: np.ndarray | None = None
 
+    def bend_pot(self):
+        """fpbend's pota..potg per bend: theta0, k, Urey-Bradley r0 and k,
+        no stretch-stretch coupling."""
+        n = 0 if self.bends is None else len(self.bends)
+        p = np.zeros((n, 7))
+        if n:
+            p[:, 0] = self.bend_t0
+            p[:, 1] = self.bend_k
+            if self.bend_ub_k is not None:
+                p[:, 2] = self.bend_ub_r0
+                p[:, 3] = self.bend_ub_k
+        return p
+
+    def intra_lists(self):
+        """Flat 1-based lists and parameter arrays of the intramolecular
+        terms: bonds (lbnd, r0, kb), bends (lbndg, bendpot), torsions (ltor,
+        tpota, tpotb), impropers (litr, ipota..ipotc), 1-4 pairs (int14,
+        type14, ecc1412, ecc146), intra-group pairs (ingrp), 1-3 pairs
+        (int13)."""
+        def ints(a, w):
+            return np.ascontiguousarray(np.zeros((0, w)) if a is None else np.asarray(a).reshape(-1, w),
+                                        dtype=np.int32).ravel()
+
+        def dbl(a, n):
+            return np.ascontiguousarray(np.zeros(n) if a is None else a, dtype=np.float64)
+
+        has_b = self.bond_k is not None
+        out = dict(lbnd=ints(self.bonds if has_b else None, 2))
+        nb = len(out["lbnd"]) // 2
+        out["r0"], out["kb"] = dbl(self.bond_r0 if has_b else None, nb), dbl(self.bond_k if has_b else None, nb)
+        out["lbndg"] = ints(self.bends, 3)
+        out["bendpot"] = dbl(self.bend_pot().ravel(), 0)
+        out["ltor"] = ints(self.tors, 4)
+        nt = len(out["ltor"]) // 4
+        out["tpota"], out["tpotb"] = dbl(self.tors_n, nt), dbl(self.tors_k, nt)
+        out["litr"] = ints(self.itors, 4)
+        ni = len(out["litr"]) // 4
+        out["ipota"], out["ipotb"], out["ipotc"] = dbl(self.itors_a, ni), dbl(self.itors_b, ni), dbl(self.itors_c, ni)
+        out["int14"] = ints(self.int14, 2)
+        out["type14"] = np.ascontiguousarray(self.type14 if len(self.int14) else np.zeros(0), dtype=np.int32)
+        out["ecc1412"], out["ecc146"] = dbl(self.ecc1412, 0), dbl(self.ecc146, 0)
+        out["ingrp"] = ints(self.ingrp, 2)
+        out["int13"] = ints(self.bend13, 2)
+        return out
+
+    def has_intra(self):
+        a = self.intra_lists()
+        return any(len(a[k]) for k in ("lbnd", "lbndg", "ltor", "litr", "int14", "ingrp", "int13"))
+
     def alchemy_params(self):
         """Per-atom rmin, epsm of the soft-core kernel (src/mtsmd.f:1298-1303)."""
         p = self.lj_params[self.nbtype - 1]

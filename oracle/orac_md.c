@@ -46,7 +46,17 @@ typedef struct {
   int *indxi, *indxj, *indxk, nind;
   long step;
   double e[3][6], eer, ekin;
+  /* intramolecular N0/N1 terms and the reciprocal corrections of mts_furier */
+  int nb, nbend, nt, nit, n14, ningrp, n13;
+  int *lbnd, *lbndg, *ltor, *litr, *int14, *type14, *ingrp, *int13;
+  double *r0, *kb, *bendpot, *tpota, *tpotb, *ipota, *ipotb, *ipotc, *ecc1412, *ecc146;
+  double fudge;
+  int n1respa, n0respa, has_n0, has_n1;
+  double *fn0, *fn1;
+  double e_bonded, e_tors, e_14grp, e_ferrf;
 } orc_md;
+
+#define ORC_MD_REC 16
 
 static void md_coords(orc_md* M) {
   int N = M->ntap;
@@ -120,6 +130,86 @@ static void md_kick(orc_md* M, const double* f, double dt);
 static int md_shake(orc_md* M, double dt);
 static int md_rattle(orc_md* M);
 
+/* The erf corrections of mts_furier (src/mts_furier.f:85-141) for the
+ * excluded pairs: bonds and bends with forces, the 1-4 pairs with
+ * fudgec = 1 - fudge (src/mtsmd.f:474), constraints energy only. */
+static void md_ferrf(orc_md* M, double* f) {
+  int N = M->ntap;
+  double fs[2], dummy_e = 0.0;
+  double* scratch = (double*)calloc(3 * (size_t)N, sizeof(double));
+  M->e_ferrf = 0.0;
+  if (M->nb > 0) {
+    orc_ferrf(M->ss, M->alphal, M->charge, 1.0, M->x, M->x + N, M->x + 2 * N, 1, M->lbnd, M->nb, fs, f, f + N,
+              f + 2 * N);
+    M->e_ferrf += fs[0] + fs[1];
+  }
+  if (M->ncnst > 0) {
+    orc_ferrf(M->ss, M->alphal, M->charge, 1.0, M->x, M->x + N, M->x + 2 * N, 0, M->cnst, M->ncnst, fs, scratch,
+              scratch + N, scratch + 2 * N);
+    M->e_ferrf += fs[0] + fs[1];
+  }
+  if (M->n13 > 0) {
+    orc_ferrf(M->ss, M->alphal, M->charge, 1.0, M->x, M->x + N, M->x + 2 * N, 1, M->int13, M->n13, fs, f, f + N,
+              f + 2 * N);
+    M->e_ferrf += fs[0] + fs[1];
+  }
+  if (M->n14 > 0) {
+    orc_ferrf(M->ss, M->alphal, M->charge, 1.0 - M->fudge, M->x, M->x + N, M->x + 2 * N, 1, M->int14, M->n14, fs,
+              f, f + N, f + 2 * N);
+    M->e_ferrf += fs[0] + fs[1];
+  }
+  (void)dummy_e;
+  free(scratch);
+}
+
+/* mts_intra_n0: fpbond + fpbend + fitors (src/mts_intra_n0.f:73-100) */
+static void md_intra_n0(orc_md* M) {
+  int N = M->ntap;
+  double ue[2];
+  memset(M->fn0, 0, sizeof(double) * 3 * N);
+  M->e_bonded = 0.0;
+  double *fx = M->fn0, *fy = M->fn0 + N, *fz = M->fn0 + 2 * N;
+  const double *x = M->x, *y = M->x + N, *z = M->x + 2 * N;
+  if (M->nb > 0) {
+    orc_fpbond(M->ss, M->lbnd, M->nb, x, y, z, M->r0, M->kb, ue, fx, fy, fz);
+    M->e_bonded += ue[0] + ue[1];
+  }
+  if (M->nbend > 0) {
+    orc_fpbend(M->ss, M->lbndg, M->nbend, x, y, z, M->bendpot, ue, fx, fy, fz);
+    M->e_bonded += ue[0] + ue[1];
+  }
+  if (M->nit > 0) {
+    orc_fitors(M->ss, M->litr, M->nit, x, y, z, M->ipota, M->ipotb, M->ipotc, ue, fx, fy, fz);
+    M->e_bonded += ue[0] + ue[1];
+  }
+}
+
+/* mts_intra_n1: fptors + fnb14 + fnbgrp (src/mts_intra_n1.f:76-118); the
+ * torsion energy is added to the bonded total of the last N0 call */
+static void md_intra_n1(orc_md* M) {
+  int N = M->ntap;
+  double ue[4];
+  memset(M->fn1, 0, sizeof(double) * 3 * N);
+  M->e_14grp = 0.0;
+  double *fx = M->fn1, *fy = M->fn1 + N, *fz = M->fn1 + 2 * N;
+  const double *x = M->x, *y = M->x + N, *z = M->x + 2 * N;
+  M->e_tors = 0.0;
+  if (M->nt > 0) {
+    orc_fptors(M->ss, M->ltor, M->nt, x, y, z, M->tpota, M->tpotb, ue, fx, fy, fz);
+    M->e_tors = ue[0] + ue[1];
+  }
+  if (M->n14 > 0) {
+    orc_fnb14(M->ss, x, y, z, M->charge, N, M->ecc1412, M->ecc146, 1, 1, M->alphal, M->int14, M->n14, M->type14,
+              M->fudge, 1.0, fx, fy, fz, ue);
+    M->e_14grp += ue[0] + ue[1] + ue[2] + ue[3];
+  }
+  if (M->ningrp > 0) {
+    orc_fnbgrp(M->ss, x, y, z, M->charge, M->nbtype, M->ecc12, M->ecc6, 1, M->alphal, M->ingrp, M->ningrp, fx, fy,
+               fz, ue);
+    M->e_14grp += ue[0] + ue[1] + ue[2] + ue[3];
+  }
+}
+
 static void md_forces(orc_md* M, char sh, double* f) {
   int N = M->ntap;
   double* r = M->sh;
@@ -136,6 +226,7 @@ static void md_forces(orc_md* M, char sh, double* f) {
     orc_fft_pme(N, M->s, M->s + N, M->s + 2 * N, M->m, M->m + M->nprot, M->m + 2 * M->nprot, M->charge, M->co,
                 M->oc, M->volume, M->alphal, M->order, M->n1, M->n2, M->n3, &M->eer, f, f + N, f + 2 * N, st,
                 M->atomp, 0, M->rkcut, M->nthreads);
+    md_ferrf(M, f);
   }
 }
 
@@ -330,6 +421,8 @@ void* orc_md_create(int ntap, int ngrp, int nprot, int ma, const int* ss, const 
                     const double* dss, int ncnst, double dth, int lrespa, int mrespa, int nupdte, char rshk,
                     const double* x, const double* v, int nthreads, double econst) {
   orc_md* M = (orc_md*)calloc(1, sizeof(orc_md));
+  M->n1respa = 1;
+  M->n0respa = 1;
   M->ntap = ntap;
   M->ngrp = ngrp;
   M->nprot = nprot;
@@ -426,6 +519,66 @@ void* orc_md_create(int ntap, int ngrp, int nprot, int ma, const int* ss, const 
   return M;
 }
 
+static int* dup_i(const int* a, size_t n) {
+  int* p = (int*)malloc(sizeof(int) * (n ? n : 1));
+  if (n) memcpy(p, a, sizeof(int) * n);
+  return p;
+}
+static double* dup_d(const double* a, size_t n) {
+  double* p = (double*)malloc(sizeof(double) * (n ? n : 1));
+  if (n) memcpy(p, a, sizeof(double) * n);
+  return p;
+}
+
+/* Intramolecular terms and the N1/N0 sub-steps (mts_intra_n0/n1, the
+ * n1respa/n0respa loops of src/mtsmd.f:2641-2930); recomputes the forces of
+ * the starting configuration. */
+void orc_md_set_intra(void* h, int nb, const int* lbnd, const double* r0, const double* kb, int nbend,
+                      const int* lbndg, const double* bendpot, int nt, const int* ltor, const double* tpota,
+                      const double* tpotb, int nit, const int* litr, const double* ipota, const double* ipotb,
+                      const double* ipotc, int n14, const int* int14, const int* type14, const double* ecc1412,
+                      const double* ecc146, int ntab14, double fudge, int ningrp, const int* ingrp, int n13,
+                      const int* int13, int n1respa, int n0respa) {
+  orc_md* M = (orc_md*)h;
+  int N = M->ntap;
+  M->nb = nb;
+  M->lbnd = dup_i(lbnd, 2 * (size_t)nb);
+  M->r0 = dup_d(r0, nb);
+  M->kb = dup_d(kb, nb);
+  M->nbend = nbend;
+  M->lbndg = dup_i(lbndg, 3 * (size_t)nbend);
+  M->bendpot = dup_d(bendpot, 7 * (size_t)nbend);
+  M->nt = nt;
+  M->ltor = dup_i(ltor, 4 * (size_t)nt);
+  M->tpota = dup_d(tpota, nt);
+  M->tpotb = dup_d(tpotb, nt);
+  M->nit = nit;
+  M->litr = dup_i(litr, 4 * (size_t)nit);
+  M->ipota = dup_d(ipota, nit);
+  M->ipotb = dup_d(ipotb, nit);
+  M->ipotc = dup_d(ipotc, nit);
+  M->n14 = n14;
+  M->int14 = dup_i(int14, 2 * (size_t)n14);
+  M->type14 = dup_i(type14, n14);
+  M->ecc1412 = dup_d(ecc1412, ntab14);
+  M->ecc146 = dup_d(ecc146, ntab14);
+  M->fudge = fudge;
+  M->ningrp = ningrp;
+  M->ingrp = dup_i(ingrp, 2 * (size_t)ningrp);
+  M->n13 = n13;
+  M->int13 = dup_i(int13, 2 * (size_t)n13);
+  M->n1respa = n1respa > 0 ? n1respa : 1;
+  M->n0respa = n0respa > 0 ? n0respa : 1;
+  M->has_n0 = (nb + nbend + nit) > 0;
+  M->has_n1 = (nt + n14 + ningrp) > 0;
+  M->fn0 = (double*)calloc(3 * (size_t)N, sizeof(double));
+  M->fn1 = (double*)calloc(3 * (size_t)N, sizeof(double));
+  if (M->has_n0) md_intra_n0(M);
+  if (M->has_n1) md_intra_n1(M);
+  double* fr = M->rshk == 'h' ? M->fh : (M->rshk == 'l' ? M->fl : M->fm);
+  md_forces(M, M->rshk, fr);
+}
+
 static double md_ekin(orc_md* M) {
   int N = M->ntap;
   double e = 0;
@@ -447,11 +600,32 @@ int orc_md_run(void* h, int nsteps, int energy_every, double* rec) {
       fail |= md_kick_r(M, M->fl, tl);
       for (int im = 0; im < M->mrespa; im++) {
         fail |= md_kick_r(M, M->fm, tm);
-        memcpy(M->xo, M->x, sizeof(double) * 3 * N);
-        for (int q = 0; q < 3 * N; q++) M->x[q] += tm * M->v[q];
-        fail |= md_shake(M, tm);
-        fail |= md_rattle(M);
-        md_coords(M);
+        const double tn1 = tm / M->n1respa, tn0 = tn1 / M->n0respa;
+        for (int i1 = 0; i1 < M->n1respa; i1++) {
+          if (M->has_n1) fail |= md_kick_r(M, M->fn1, tn1);
+          for (int i0 = 0; i0 < M->n0respa; i0++) {
+            /* verlet (src/verlet.f): the N0 half kick without RATTLE, then
+             * the drift; rattle_verlet corrects both */
+            memcpy(M->xo, M->x, sizeof(double) * 3 * N);
+            const double ts2 = tn0 * tn0;
+            for (int q = 0; q < 3 * N; q++) {
+              const double fq = M->has_n0 ? M->fn0[q] : 0.0;
+              M->x[q] = M->x[q] + tn0 * M->v[q] + fq * 0.5 * ts2 / M->mass[q % N];
+              M->v[q] = M->v[q] + fq * 0.5 * tn0 / M->mass[q % N];
+            }
+            fail |= md_shake(M, tn0);
+            fail |= md_rattle(M);
+            md_coords(M);
+            if (M->has_n0) {
+              md_intra_n0(M);
+              fail |= md_kick_r(M, M->fn0, tn0);
+            }
+          }
+          if (M->has_n1) {
+            md_intra_n1(M);
+            fail |= md_kick_r(M, M->fn1, tn1);
+          }
+        }
         md_forces(M, 'm', M->fm);
         fail |= md_kick_r(M, M->fm, tm);
       }
@@ -463,7 +637,7 @@ int orc_md_run(void* h, int nsteps, int energy_every, double* rec) {
     fail |= md_kick_r(M, M->fh, M->dth);
     M->step++;
     if (energy_every > 0 && (k + 1) % energy_every == 0) {
-      double* r = rec + 12 * (size_t)nrec++;
+      double* r = rec + ORC_MD_REC * (size_t)nrec++;
       r[0] = (double)M->step;
       r[1] = md_ekin(M);
       for (int s = 0; s < 3; s++) {
@@ -472,7 +646,11 @@ int orc_md_run(void* h, int nsteps, int energy_every, double* rec) {
       }
       r[8] = M->eer;
       r[9] = M->econst;
-      r[10] = r[1] + r[2] + r[3] + r[4] + r[5] + r[6] + r[7] + r[8] + r[9];
+      r[12] = M->e_bonded + M->e_tors;
+      r[13] = M->e_14grp;
+      r[14] = M->e_ferrf;
+      r[15] = 0.0;
+      r[10] = r[1] + r[2] + r[3] + r[4] + r[5] + r[6] + r[7] + r[8] + r[9] + r[12] + r[13] + r[14];
       r[11] = fail;
     }
   }
@@ -506,5 +684,8 @@ void orc_md_destroy(void* h) {
   free(M->lh);
   free(M->ll);
   free(M->lm);
+  void* extra[] = {M->lbnd, M->r0, M->kb, M->lbndg, M->bendpot, M->ltor, M->tpota, M->tpotb, M->litr, M->ipota,
+                   M->ipotb, M->ipotc, M->int14, M->type14, M->ecc1412, M->ecc146, M->ingrp, M->int13, M->fn0, M->fn1};
+  for (unsigned k = 0; k < sizeof(extra) / sizeof(extra[0]); k++) free(extra[k]);
   free(M);
 }

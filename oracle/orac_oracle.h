@@ -222,6 +222,21 @@ void orc_fnbgrp(const int* ss_index, const double* xp0, const double* yp0,
                 double alphal, const int* ingrp, int ingrpp, double* fpx,
                 double* fpy, double* fpz, double* ue);
 
+/* Oracle MD (orac_md.c): records of ORC_MD_REC = 16 doubles per energy
+ * sample: step, kinetic, (LJ, Coulomb) of the M, L, H shells, SPME eer,
+ * the caller's constant, total, failure flags, bonded (bonds, bends,
+ * torsions, impropers), 1-4 + intra-group nonbonded, erf corrections. */
+void orc_md_set_intra(void* h, int nb, const int* lbnd, const double* r0,
+                      const double* kb, int nbend, const int* lbndg,
+                      const double* bendpot, int nt, const int* ltor,
+                      const double* tpota, const double* tpotb, int nit,
+                      const int* litr, const double* ipota,
+                      const double* ipotb, const double* ipotc, int n14,
+                      const int* int14, const int* type14,
+                      const double* ecc1412, const double* ecc146, int ntab14,
+                      double fudge, int ningrp, const int* ingrp, int n13,
+                      const int* int13, int n1respa, int n0respa);
+
 #ifdef __cplusplus
 }
 #endif

@@ -95,21 +95,13 @@ def alch_set(ladd, lrm, intramol=False, ljintra=False, qq=False):
     return np.array(t[:]).reshape(2, 9)
 
 
-def bend_pot(s):
-    """fpbend's pota..potg per bend (theta0, k, no Urey-Bradley, no coupling
-    unless the System carries bend_ub_r0 / bend_ub_k)."""
-    n = len(s.bends)
-    p = np.zeros((n, 7))
-    p[:, 0] = s.bend_t0
-    p[:, 1] = s.bend_k
-    if getattr(s, "bend_ub_k", None) is not None:
-        p[:, 2] = s.bend_ub_r0
-        p[:, 3] = s.bend_ub_k
-    return p
-
-
 def _f(a):
     return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def intra_lists(s):
+    """Flat lists of the intramolecular terms (System.intra_lists)."""
+    return {k: (_i(v) if v.dtype.kind == "i" else _f(v)) for k, v in s.intra_lists().items()}
 
 
 def _i(a):
@@ -198,7 +190,7 @@ class Oracle:
         e["bond"] = tuple(ue)
         ue = np.zeros(2)
         if s.bends is not None and len(s.bends):
-            self.L.orc_fpbend(ss, _i(s.bends.ravel()), len(s.bends), x, y, z, _f(bend_pot(s).ravel()), ue, fx, fy, fz)
+            self.L.orc_fpbend(ss, _i(s.bends.ravel()), len(s.bends), x, y, z, _f(s.bend_pot().ravel()), ue, fx, fy, fz)
         e["bend"] = tuple(ue)
         ue = np.zeros(2)
         self.last_skipped = 0
@@ -421,7 +413,9 @@ class Oracle:
 class OracleMD:
     """CPU restatement of ORAC's NVE r-RESPA loop (orac_md.c)."""
 
-    def __init__(self, s, dt_h, lrespa, mrespa, nupdte, rshk="l", nthreads=None, econst=0.0):
+    REC = 16  # doubles per energy record (orac_oracle.h)
+
+    def __init__(self, s, dt_h, lrespa, mrespa, nupdte, rshk="l", nthreads=None, econst=0.0, n1respa=1, n0respa=1):
         L = lib()
         self.L = L
         self.s = s
@@ -453,14 +447,28 @@ class OracleMD:
                                  nthreads or default_threads(), econst)
         if not self.h:
             raise RuntimeError("orc_md_create failed")
+        a = intra_lists(s)
+        if n1respa != 1 or n0respa != 1 or any(len(a[k]) for k in ("lbnd", "lbndg", "ltor", "litr", "int14", "ingrp",
+                                                                     "int13")):
+            L.orc_md_set_intra.argtypes = [vp, C.c_int, _I, _D, _D, C.c_int, _I, _D, C.c_int, _I, _D, _D, C.c_int,
+                                           _I, _D, _D, _D, C.c_int, _I, _I, _D, _D, C.c_int, C.c_double, C.c_int,
+                                           _I, C.c_int, _I, C.c_int, C.c_int]
+            self._keep["intra"] = a
+            L.orc_md_set_intra(self.h, len(a["lbnd"]) // 2, a["lbnd"], a["r0"], a["kb"], len(a["lbndg"]) // 3,
+                               a["lbndg"], a["bendpot"], len(a["ltor"]) // 4, a["ltor"], a["tpota"], a["tpotb"],
+                               len(a["litr"]) // 4, a["litr"], a["ipota"], a["ipotb"], a["ipotc"],
+                               len(a["int14"]) // 2, a["int14"], a["type14"], a["ecc1412"], a["ecc146"],
+                               len(a["ecc1412"]), s.fudge, len(a["ingrp"]) // 2, a["ingrp"], len(a["int13"]) // 2,
+                               a["int13"], n1respa, n0respa)
 
     def run(self, nsteps, energy_every=0):
+        R = self.REC
         nrec = nsteps // energy_every if energy_every else 0
-        rec = np.zeros(max(1, nrec) * 12)
+        rec = np.zeros(max(1, nrec) * R)
         rc = self.L.orc_md_run(self.h, nsteps, energy_every, rec)
         if rc:
             raise RuntimeError(f"orc_md_run status {rc}")
-        return rec[:nrec * 12].reshape(-1, 12)
+        return rec[:nrec * R].reshape(-1, R)
 
     def state(self):
         n = self.s.ntap
