@@ -31,7 +31,7 @@ for p in (os.path.join(ROOT, "orac-porting_b200"), os.path.join(ROOT, "oracle"))
 
 import numpy as np  # noqa: E402
 
-from orac_b200 import systems  # noqa: E402
+from orac_b200 import systems, units  # noqa: E402
 
 FS_PER_DAY = 86400.0e15  # fs per day of wall time per 1 fs/s
 FP32_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # 74.4: no measured FP32 peak on this pool
@@ -281,46 +281,87 @@ def gpu_arm(args, wl, s, device):
     return res
 
 
-def batch_arm(args, wl, s, device, flush):
-    """B replicas of the workload (different Maxwell-Boltzmann velocities)
-    advanced by one graph launch per step (orac_gpu_batch_run)."""
+def _timed_steps(run_one, stream, flush, steps):
+    """CUDA-event time of each of `steps` calls of run_one on `stream`, L2
+    flushed before each."""
     import torch
 
-    from orac_b200.engine import Batch, Engine
-
-    engines = []
-    for r in range(args.batch):
-        t = s.copy()
-        rng = np.random.default_rng(1000 + r)
-        scale = np.sqrt(1.0 / t.mass)
-        v = rng.standard_normal((3, t.ntap)) * scale * np.sqrt(np.mean(t.mass * (t.vx ** 2 + t.vy ** 2 + t.vz ** 2)))
-        v -= (v * t.mass).sum(axis=1, keepdims=True) / t.mass.sum()
-        t.vx, t.vy, t.vz = v[0].copy(), v[1].copy(), v[2].copy()
-        e = Engine(t, device=device)
-        e.md_setup(wl["dt_h"], wl["lrespa"], wl["mrespa"], wl["nupdte"], wl["rshk"])
-        engines.append(e)
-    b = Batch(engines)
-    stream = torch.cuda.ExternalStream(b.stream(), device=device)
-    b.run(args.warmup)
-    total_ms, step_ms = 0.0, []
-    for _ in range(args.steps):
+    out = []
+    for _ in range(steps):
         flush.zero_()
         torch.cuda.synchronize()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        b.run(1, sync=False)
+        run_one()
         e1.record(stream)
-        b.sync()
-        ms = e0.elapsed_time(e1)
-        step_ms.append(ms)
-        total_ms += ms
+        torch.cuda.synchronize()
+        out.append(e0.elapsed_time(e1))
+    return out
+
+
+def window_engine(base, k, nwin, device, wl):
+    """Lambda window k: the ligand removed at lambda = k / (nwin - 1) (lrm =
+    lrmq = lambda, soft core 0.5 0.5), dU/dlambda of that control lambda."""
+    from orac_b200.engine import Engine
+
+    lam = k / (nwin - 1)
+    e = Engine(base.copy(), device=device)
+    e.set_alchemy(base.ss_alchemy, 0.5, 0.5)
+    e.set_lambda(0.0, lam, 0.0, lam, dlam=[0.0, 1.0, 0.0, 1.0])
+    e.md_setup(wl["dt_h"], wl["lrespa"], wl["mrespa"], wl["nupdte"], wl["rshk"], econst=0.0)
+    return e, lam
+
+
+def batch_arm(args, wl, s, device, flush):
+    """The alchemical lambda-window batch: `args.batch` windows of the
+    40-atom ligand in the liquid water box (lambda_k = k / (B - 1) on the
+    ligand's LJ and charges) advanced by one graph launch per outer step
+    (orac_gpu_batch_run); the plain reference is one window alone on the
+    same driver.  Every window ends with an energy step that yields its
+    dU/dlambda."""
+    import torch
+
+    from orac_b200.engine import Batch
+
+    base = systems.ligand_in_water()
+    nwin = args.batch
+    # one window alone (plain)
+    e1, _ = window_engine(base, nwin // 2, nwin, device, wl)
+    L = e1.lib
+    st1 = torch.cuda.ExternalStream(L.orac_gpu_get_stream(e1.ctx), device=device)
+    for _ in range(args.warmup):
+        L.orac_gpu_md_run_async(e1.ctx, 1)
+        L.orac_gpu_md_collect(e1.ctx)
+
+    def one_plain():
+        L.orac_gpu_md_run_async(e1.ctx, 1)
+
+    plain_ms = _timed_steps(one_plain, st1, flush, args.steps)
+    if L.orac_gpu_md_collect(e1.ctx):
+        raise RuntimeError(L.orac_gpu_last_error(e1.ctx).decode())
+    e1.close()
+    # the batch
+    engines, lams = [], []
+    for k in range(nwin):
+        e, lam = window_engine(base, k, nwin, device, wl)
+        engines.append(e)
+        lams.append(lam)
+    b = Batch(engines)
+    stream = torch.cuda.ExternalStream(b.stream(), device=device)
+    b.run(args.warmup)
+    step_ms = _timed_steps(lambda: b.run(1, sync=False), stream, flush, args.steps)
+    b.sync()
     b.close()
+    dudl = []
     for e in engines:
+        rec = e.md_run(1, energy_every=1)
+        dudl.append(float(rec[0, 15]))
         e.close()
     st = sorted(step_ms)
-    return {"systems": args.batch, "total_ms": total_ms, "step_ms_p50": st[len(st) // 2],
-            "step_ms_p99": st[min(len(st) - 1, int(0.99 * len(st)))]}
+    return {"systems": nwin, "atoms_per_window": base.ntap, "total_ms": sum(step_ms),
+            "step_ms_p50": st[len(st) // 2], "step_ms_p99": st[min(len(st) - 1, int(0.99 * len(st)))],
+            "plain_total_ms": sum(plain_ms), "lambdas": lams, "dudl": dudl}
 
 
 def main():
@@ -336,7 +377,7 @@ def main():
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="liquid")
     ap.add_argument("--cpu-budget", type=float, default=12.0, help="seconds of CPU-baseline sampling")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--batch", type=int, default=32, help="replicas advanced together (0/1: skip the batched leg)")
+    ap.add_argument("--batch", type=int, default=64, help="alchemical lambda windows advanced together (0/1: skip)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     wl = WORKLOADS[args.workload]
@@ -420,11 +461,21 @@ def main():
     if "batched" in res:
         bt = res["batched"]
         bval = ns_per_day(args.steps, wl["dt_h"], bt["total_ms"] / 1e3) * bt["systems"]
-        out["batched"] = {"systems": bt["systems"], "value": bval, "unit": "ns/day (aggregate)",
-                          "ms_per_step": bt["total_ms"] / args.steps, "step_ms_p50": bt["step_ms_p50"],
-                          "step_ms_p99": bt["step_ms_p99"], "speedup_vs_plain": bval / value,
-                          "how": "one graph launch per H step advances every replica (orac_gpu_batch_run); "
-                                 "replicas differ in their Maxwell-Boltzmann velocities"}
+        pval = ns_per_day(args.steps, wl["dt_h"], bt["plain_total_ms"] / 1e3)
+        d = np.array(bt["dudl"])
+        out["batched"] = {
+            "workload": f"{bt['systems']} alchemical lambda windows (lambda_k = k/{bt['systems'] - 1}) of a 40-atom "
+                        f"flexible ligand in the liquid water box ({bt['atoms_per_window']} atoms per window), "
+                        "soft-core force_alchemy, SPME of the scaled charges, bonded N0/N1 levels",
+            "systems": bt["systems"], "value": bval, "unit": "ns/day (aggregate over windows)",
+            "ms_per_step": bt["total_ms"] / args.steps, "step_ms_p50": bt["step_ms_p50"],
+            "step_ms_p99": bt["step_ms_p99"], "plain_window_value": pval,
+            "speedup_vs_plain": bval / pval,
+            "dudl_kjmol": {"first": float(d[0]) * units.KJMOL, "mid": float(d[len(d) // 2]) * units.KJMOL,
+                           "last": float(d[-1]) * units.KJMOL,
+                           "trapezoid_dG": float(np.trapezoid(d, bt["lambdas"])) * units.KJMOL},
+            "how": "one graph launch per H step advances every window (orac_gpu_batch_run); plain = one window "
+                   "alone through the same driver; dU/dlambda from an energy step at the end of each window"}
     elif "batched_error" in res:
         out["batched"] = {"error": res["batched_error"]}
     print(json.dumps(out))

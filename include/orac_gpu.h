@@ -254,7 +254,11 @@ int orac_gpu_set_lambda(orac_gpu_ctx* ctx, const double* lam, int intramol,
  * variant (module globals in ORAC): out[0] seg_ene (REM), out[1] dwrk =
  * U(lambda) - U(lambda0) of the shell (src/force_alchemy.f:683-688), out[2]
  * and out[3] the LJ and Coulomb energy at lambda0, out[4] dU/dlambda of the
- * shell, out[5] the PME work eer - eer0 (src/do_pmesh_alchemy.f90:78). */
+ * shell, out[5] the PME work eer - eer0 (src/do_pmesh_alchemy.f90:78),
+ * out[6] dE_rec/dlambda of the last fft_pme (sum of the reciprocal
+ * potential at each atom times its dq/dlambda), out[7] d(self energy)/dlambda
+ * (cself_alchemy, src/cself_alchemy.f).  out has 8 doubles.  In MD, record
+ * column 15 carries the total dU/dlambda of the window. */
 int orac_gpu_variant_energies(orac_gpu_ctx* ctx, double* out);
 
 /* Device-resident entry points -------------------------------------------

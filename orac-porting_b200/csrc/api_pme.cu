@@ -69,7 +69,9 @@ int fft_pme_device(orac_gpu_ctx* ctx, const double* d_sxyz, const double* d_mol,
   CKL();
   double recip[9];
   recip_of(ctx->oc, recip);
-  return pme_run(ctx, N, S.cart, ctx->pme_q(), recip, ctx->volume, ctx->alphal, d_f, d_eout, d_sxyz, d_mol);
+  const bool dq = ctx->variant == VAR_ALCH && ctx->d_dq && ctx->d_xtra;
+  return pme_run(ctx, N, S.cart, ctx->pme_q(), recip, ctx->volume, ctx->alphal, d_f, d_eout, d_sxyz, d_mol, nullptr,
+                 dq ? ctx->d_dq : nullptr, dq ? ctx->d_xtra + 5 : nullptr);
 }
 
 extern "C" {
@@ -88,6 +90,10 @@ int orac_gpu_fft_pme(orac_gpu_ctx* ctx, const double* xp, const double* yp, cons
   if (int rc = up_doubles(ctx, ctx->d_mol, m3, 3, P)) return rc;
   if (!S.eout && dev_alloc(ctx, &S.eout, 16)) return ORAC_ERR_CUDA;
   CK(cudaMemsetAsync(ctx->d_fout, 0, sizeof(double) * 3 * (size_t)N, ctx->stream));
+  if (ctx->variant == VAR_ALCH && ctx->d_dq) {
+    if (!ctx->d_xtra && dev_alloc(ctx, &ctx->d_xtra, 8)) return ORAC_ERR_CUDA;
+    CK(cudaMemsetAsync(ctx->d_xtra + 5, 0, sizeof(double), ctx->stream));
+  }
   if (int rc = fft_pme_device(ctx, ctx->d_xyz, ctx->d_mol, ctx->d_fout, S.eout)) return rc;
   if (int rc = ensure_host(ctx, sizeof(double) * (3 * (size_t)N + 16))) return rc;
   CK(cudaMemcpyAsync(ctx->h_stage, ctx->d_fout, sizeof(double) * 3 * (size_t)N, cudaMemcpyDeviceToHost, ctx->stream));

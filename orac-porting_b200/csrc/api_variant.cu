@@ -66,7 +66,7 @@ double scaled_charge(double q, double lq) {
 
 __global__ void k_variant_out(const double* __restrict__ acc, int variant, int forces_on, double* __restrict__ x) {
   if (threadIdx.x != 0) return;
-  for (int k = 0; k < 5; k++) x[k] = 0.0;
+  for (int k = 0; k < 5; k++) x[k] = 0.0;  // x[5] is the PME's
   if (!forces_on) return;
   if (variant == VAR_REM) x[0] = acc[ACC_X];
   if (variant == VAR_ALCH) {
@@ -95,9 +95,10 @@ int build_vflag(orac_gpu_ctx* ctx) {
   return ORAC_OK;
 }
 
-int upload_alch_charges(orac_gpu_ctx* ctx) {
+int upload_alch_charges(orac_gpu_ctx* ctx, const double* dlam) {
   const int N = ctx->N;
-  std::vector<double> qc(N), q0(N);
+  std::vector<double> qc(N), q0(N), dq(N, 0.0);
+  double sq = 0.0;
   for (int a = 0; a < N; a++) {
     const int ss = ctx->h_ssal[a];
     // lambdaq of added atoms is laddq, of removed atoms -lrmq (src/mtsmd.f:747,755)
@@ -105,11 +106,32 @@ int upload_alch_charges(orac_gpu_ctx* ctx) {
     const double lq0 = ss == 2 ? ctx->lam[6] : (ss == -2 ? -ctx->lam[7] : 0.0);
     qc[a] = scaled_charge(ctx->h_charge[a], lq);
     q0[a] = scaled_charge(ctx->h_charge[a], lq0);
+    if (dlam) {
+      // d/dlambda of (1 - |lambdaq|) q with lambdaq = laddq or -lrmq
+      if (ss == 2) dq[a] = -(ctx->lam[2] < 0 ? -1.0 : 1.0) * ctx->h_charge[a] * dlam[2];
+      if (ss == -2) dq[a] = -(ctx->lam[3] < 0 ? -1.0 : 1.0) * ctx->h_charge[a] * dlam[3];
+    }
+    if (ctx->h_ss[a] == 1) sq += 2.0 * qc[a] * dq[a];
+  }
+  // cself_alchemy (src/cself_alchemy.f): -alpha/sqrt(pi) sum_slt qc^2 (1 - erfc(kcut/2 alpha))
+  {
+    const double ar = ctx->rkcut / (2.0 * ctx->alphal);
+    const double qt = 1.0 / (1.0 + 0.3275911 * ar);
+    const double erfcst =
+        ((((1.0614054 * qt - 1.453152) * qt + 1.4214137) * qt - 0.28449674) * qt + 0.2548296) * qt * std::exp(-ar * ar);
+    ctx->self_dudl = -sq * ctx->alphal / std::sqrt(4.0 * std::atan(1.0)) * (1.0 - erfcst);
   }
   if (!ctx->d_qc && (dev_alloc(ctx, &ctx->d_qc, N) || dev_alloc(ctx, &ctx->d_q0, N))) return ORAC_ERR_CUDA;
   CK(cudaMemcpy(ctx->d_qc, qc.data(), sizeof(double) * N, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(ctx->d_q0, q0.data(), sizeof(double) * N, cudaMemcpyHostToDevice));
   ctx->q0_differs = qc != q0;
+  if (dlam) {
+    if (!ctx->d_dq && dev_alloc(ctx, &ctx->d_dq, N)) return ORAC_ERR_CUDA;
+    CK(cudaMemcpy(ctx->d_dq, dq.data(), sizeof(double) * N, cudaMemcpyHostToDevice));
+  } else if (ctx->d_dq) {
+    cudaFree(ctx->d_dq);
+    ctx->d_dq = nullptr;
+  }
   return ORAC_OK;
 }
 
@@ -143,7 +165,7 @@ int variant_out_launch(orac_gpu_ctx* ctx, int forces_on) {
 }
 
 void variant_free(orac_gpu_ctx* ctx) {
-  void* p[] = {ctx->d_vflag, ctx->d_soft, ctx->d_softd, ctx->d_qc, ctx->d_q0, ctx->d_xtra};
+  void* p[] = {ctx->d_vflag, ctx->d_soft, ctx->d_softd, ctx->d_qc, ctx->d_q0, ctx->d_xtra, ctx->d_dq};
   for (void* q : p)
     if (q) cudaFree(q);
 }
@@ -221,7 +243,7 @@ int orac_gpu_set_lambda(orac_gpu_ctx* ctx, const double* lam, int intramol, int 
   alch_set(T.fq0, lam[6], lam[7], intramol, ljintra, 1);
   alch_set_d(T.df, lam[0], lam[1], d[0], d[1], intramol, ljintra, 0);
   alch_set_d(T.dfq, lam[2], lam[3], d[2], d[3], intramol, ljintra, 1);
-  return upload_alch_charges(ctx);
+  return upload_alch_charges(ctx, dlam);
 }
 
 int orac_gpu_variant_energies(orac_gpu_ctx* ctx, double* out) {
@@ -229,11 +251,13 @@ int orac_gpu_variant_energies(orac_gpu_ctx* ctx, double* out) {
   CK(cudaSetDevice(ctx->device));
   double x[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   if (ctx->d_xtra) {
-    CK(cudaMemcpyAsync(x, ctx->d_xtra, sizeof(double) * 5, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(x, ctx->d_xtra, sizeof(double) * 6, cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
   }
   for (int k = 0; k < 5; k++) out[k] = x[k];
   out[5] = ctx->pme_dwrk;
+  out[6] = x[5];  // PME dU/dlambda of the last fft_pme
+  out[7] = ctx->self_dudl;
   return ORAC_OK;
 }
 

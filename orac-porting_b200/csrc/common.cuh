@@ -292,6 +292,8 @@ struct orac_gpu_ctx {
   double lam[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // ladd lrm laddq lrmq and the lambda0 set
   double* d_qc = nullptr;  // [N] PME charges at lambda: (1 - |lambdaq_i|) q_i
   double* d_q0 = nullptr;  // [N] PME charges at lambda0
+  double* d_dq = nullptr;  // [N] d(PME charge)/d(control lambda), or null
+  double self_dudl = 0.0;  // d(self energy)/d(control lambda) (cself_alchemy)
   std::vector<unsigned char> h_rem;   // REM segment atoms
   bool q0_differs = false;            // lambda0 charges differ from lambda charges
   double pme_dwrk = 0.0;              // eer(lambda) - eer(lambda0) of the last fft_pme
@@ -372,7 +374,8 @@ int pme_run(orac_gpu_ctx* ctx, int natom, const double* d_cart /*3N*/,
             const double* d_q, const double* recip, double volume,
             double alpha, double* d_f /*3N accumulated*/, double* d_eout,
             const double* d_sxyz, const double* d_mol,
-            unsigned long long* d_ffix = nullptr /*3N fixed point instead of d_f*/);
+            unsigned long long* d_ffix = nullptr /*3N fixed point instead of d_f*/,
+            const double* d_dq = nullptr, double* d_edq = nullptr /*sum phi_i dq_i, accumulated*/);
 // k_small.cu: kind 0 fnb14, 1 fnbgrp, 2 ferrf; d_e[4]
 int small_launch(orac_gpu_ctx* ctx, int kind, const double* d_xyz,
                  const int* d_pairs, const int* d_ptype, int npairs,
@@ -385,7 +388,7 @@ int self_launch(orac_gpu_ctx* ctx, const int* d_ss, double* d_e);
 int small_launch_x(orac_gpu_ctx* ctx, int kind, const double* d_xyz, const int* d_pairs, const int* d_ptype,
                    int npairs, const double* d_t12, const double* d_t6, double fudge, double lj_fudge,
                    int coul_mode, int forces, double* d_f, double* d_e, const int* d_ss, const double* d_q,
-                   unsigned long long* d_ffix);
+                   unsigned long long* d_ffix, const double* d_dq = nullptr, double* d_edq = nullptr);
 // k_bonded.cu: mask of BK_* kinds; forces into d_f (FP64 atomics) or d_ffix
 // (fixed point); d_e[8] (bond, bend, tors, itors) x (slt, slv) or null
 int bonded_launch(orac_gpu_ctx* ctx, int mask, const double* d_x, double* d_f, unsigned long long* d_ffix,

@@ -323,6 +323,10 @@ struct AtomArgs {
   int P;
   double c11, c12, c13, c22, c23, c33;
   double* eout;  // [7+9]
+  // dE/dlambda of alchemical charges: sum_i phi_i dq_i/dlambda, with phi_i the
+  // reciprocal potential at atom i (dE/dq_i), into *edq (both null: off)
+  const double* dq;
+  double* edq;
 };
 
 // fill_bspline restated in FP32 (src/pme_fftw3.f90:518-576)
@@ -401,6 +405,7 @@ __global__ void k_gather(const AtomArgs A) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int p = A.order;
   double st[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  double dphi = 0.0;
   double fr[3] = {0, 0, 0};
   if (t < A.natom) frac_coord(A, t, fr);
   if (t < A.natom && frac_ok(A, fr)) {
@@ -408,7 +413,7 @@ __global__ void k_gather(const AtomArgs A) {
     bspline((float)(fr[0] - (int)fr[0]), p, th1, d1);
     bspline((float)(fr[1] - (int)fr[1]), p, th2, d2);
     bspline((float)(fr[2] - (int)fr[2]), p, th3, d3);
-    float f1 = 0.f, f2 = 0.f, f3 = 0.f;
+    float f1 = 0.f, f2 = 0.f, f3 = 0.f, phi = 0.f;
     for (int i3 = 0; i3 < p; i3++) {
       const int kk = gidx((int)fr[2] - p + 1 + i3, A.n3);
       for (int i2 = 0; i2 < p; i2++) {
@@ -421,6 +426,7 @@ __global__ void k_gather(const AtomArgs A) {
           s2 += th1[i1] * qv;
         }
         s3 = s2;
+        phi += s2 * th2[i2] * th3[i3];
         f1 += s1 * th2[i2] * th3[i3];
         f2 += s2 * d2[i2] * th3[i3];
         f3 += s3 * th2[i2] * d3[i3];
@@ -457,8 +463,10 @@ __global__ void k_gather(const AtomArgs A) {
       st[7] = -gy * fz;
       st[8] = -gz * fz;
     }
+    if (A.dq) dphi = (double)phi * A.dq[t];
   }
   if (A.sxyz) block_reduce_add<9>(st, A.eout + 7);
+  if (A.dq) block_reduce_add<1>(&dphi, A.edq);
 }
 
 void host_bspline(double w, int order, double* c, double* d) {
@@ -555,7 +563,7 @@ int pme_setup(orac_gpu_ctx* ctx, int n1, int n2, int n3, int order) {
 
 int pme_run(orac_gpu_ctx* ctx, int natom, const double* d_cart, const double* d_q, const double* recip,
             double volume, double alpha, double* d_f, double* d_eout, const double* d_sxyz, const double* d_mol,
-            unsigned long long* d_ffix) {
+            unsigned long long* d_ffix, const double* d_dq, double* d_edq) {
   PmePlan& P = ctx->pme;
   if (!P.qfix) return ctx_fail(ctx, ORAC_ERR_STATE, "PME not set up");
   const int n1 = P.n1, n2 = P.n2, n3 = P.n3, h1 = P.h1;
@@ -594,6 +602,8 @@ int pme_run(orac_gpu_ctx* ctx, int natom, const double* d_cart, const double* d_
   A.c23 = ctx->co[7];
   A.c33 = ctx->co[8];
   A.eout = d_eout;
+  A.dq = d_edq ? d_dq : nullptr;
+  A.edq = d_edq;
   const int nsp = natom * P.order;
   k_spread<<<(nsp + 255) / 256, 256, 0, ctx->stream>>>(A);
   CKL();

@@ -36,11 +36,15 @@ struct SmallArgs {
   double* f;  // [3N]
   double* e;  // [4]
   unsigned long long* ffix;  // [3N] fixed-point output instead of f (or null)
+  // ferrf: d/dlambda of the correction for charges q(lambda) with dq/dlambda
+  const double* dq;
+  double* edq;
 };
 
 __global__ void k_small(const SmallArgs A) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   double e[4] = {0, 0, 0, 0};
+  double dedl = 0.0;
   if (t < A.n) {
     const int i1 = A.pairs[2 * t] - 1, i2 = A.pairs[2 * t + 1] - 1;
     const int type = A.ss[i1] - 1;
@@ -61,6 +65,8 @@ __global__ void k_small(const SmallArgs A) {
       const double erfst = 1.0 - erfcst;
       e[type] -= furpar * erfst / rsp;
       qforce = -furpar * (erfst - A.twrtpi * alphar * expcst) / (rsp * rsq);
+      if (A.dq)
+        dedl = -(A.forces ? A.fudge : 1.0) * (A.dq[i1] * A.q[i2] + A.q[i1] * A.dq[i2]) * erfst / rsp;
     } else {
       int lij;
       if (A.kind == 0) {
@@ -124,6 +130,10 @@ __global__ void k_small(const SmallArgs A) {
     for (int k = 0; k < (int)(blockDim.x >> 5); k++) x += s[k][threadIdx.x];
     if (x != 0.0) atomicAdd(A.e + threadIdx.x, x);
   }
+  if (A.edq) {
+    const double x = warp_sumd(dedl);
+    if (lane == 0 && x != 0.0) atomicAdd(A.edq, x);
+  }
 }
 
 __global__ void k_self(int n, const double* q, const int* ss, double* e) {
@@ -156,7 +166,7 @@ int small_launch(orac_gpu_ctx* ctx, int kind, const double* d_xyz, const int* d_
 int small_launch_x(orac_gpu_ctx* ctx, int kind, const double* d_xyz, const int* d_pairs, const int* d_ptype,
                    int npairs, const double* d_t12, const double* d_t6, double fudge, double lj_fudge,
                    int coul_mode, int forces, double* d_f, double* d_e, const int* d_ss, const double* d_q,
-                   unsigned long long* d_ffix) {
+                   unsigned long long* d_ffix, const double* d_dq, double* d_edq) {
   SmallArgs A;
   memset(&A, 0, sizeof(A));
   A.kind = kind;
@@ -170,6 +180,8 @@ int small_launch_x(orac_gpu_ctx* ctx, int kind, const double* d_xyz, const int* 
   A.q = d_q ? d_q : ctx->d_aqd;
   A.ss = d_ss;
   A.ffix = d_ffix;
+  A.dq = (kind == 2 && d_edq) ? d_dq : nullptr;
+  A.edq = A.dq ? d_edq : nullptr;
   A.alpha = ctx->alphal;
   A.fudge = fudge;
   A.lj_fudge = lj_fudge;

@@ -739,7 +739,7 @@ static ConsArgs big_args(orac_gpu_ctx* ctx, MdState& S, double dt, double tol) {
 }
 
 enum { LH = 0, LL = 1, LM = 2, LN1 = 3, LN0 = 4 };
-enum { E_BOND = 41, E_14 = 49, E_GRP = 53, E_ERF = 57, E_N = 80 };
+enum { E_BOND = 41, E_14 = 49, E_GRP = 53, E_ERF = 57, E_DUDL = 73, E_N = 80 };
 
 // kick of the level accumulators with velocity factors c[l] (0: skip) + RATTLE
 static void kick_fill(MolArgs& A, MdState& S, const double* c) {
@@ -801,21 +801,24 @@ static int md_drift(orac_gpu_ctx* ctx, MdState& S, double dt, const double* c, i
 static int md_ferrf(orac_gpu_ctx* ctx, MdState& S, unsigned long long* f, bool energy) {
   const BondedDev& B = ctx->bd;
   const double* q = ctx->pme_q();
+  // d/dlambda of the corrections of alchemical charges (ferrf_alchemy)
+  const double* dq = (energy && ctx->variant == VAR_ALCH) ? ctx->d_dq : nullptr;
+  double* edq = dq ? S.e + E_DUDL + 4 : nullptr;
   if (B.nb > 0)
     if (int rc = small_launch_x(ctx, 2, S.x, B.pbond, nullptr, B.nb, nullptr, nullptr, 1.0, 1.0, 1, 1, nullptr,
-                                energy ? S.e + E_ERF : nullptr, B.ss, q, f))
+                                energy ? S.e + E_ERF : nullptr, B.ss, q, f, dq, edq))
       return rc;
   if (energy && B.ncn > 0)
     if (int rc = small_launch_x(ctx, 2, S.x, B.pcn, nullptr, B.ncn, nullptr, nullptr, 1.0, 1.0, 1, 0, nullptr,
-                                S.e + E_ERF + 4, B.ss, q, nullptr))
+                                S.e + E_ERF + 4, B.ss, q, nullptr, dq, edq))
       return rc;
   if (B.n13 > 0)
     if (int rc = small_launch_x(ctx, 2, S.x, B.p13, nullptr, B.n13, nullptr, nullptr, 1.0, 1.0, 1, 1, nullptr,
-                                energy ? S.e + E_ERF + 8 : nullptr, B.ss, q, f))
+                                energy ? S.e + E_ERF + 8 : nullptr, B.ss, q, f, dq, edq))
       return rc;
   if (B.n14 > 0)
     if (int rc = small_launch_x(ctx, 2, S.x, B.p14, nullptr, B.n14, nullptr, nullptr, 1.0 - B.fudge, 1.0, 1, 1,
-                                nullptr, energy ? S.e + E_ERF + 12 : nullptr, B.ss, q, f))
+                                nullptr, energy ? S.e + E_ERF + 12 : nullptr, B.ss, q, f, dq, edq))
       return rc;
   return ORAC_OK;
 }
@@ -829,12 +832,15 @@ static int md_forces_shell(orac_gpu_ctx* ctx, MdState& S, char sh, int lvl, bool
   if (int rc = shell_run_r(ctx, sh, ctx->sh, ctx->d_xyz, ctx->d_grp, ctx->d_mol, reinterpret_cast<double*>(f),
                            energy ? e : nullptr, nullptr, flags))
     return rc;
+  const bool dudl = energy && ctx->variant == VAR_ALCH && ctx->d_dq;
+  if (dudl)  // the shell's dU/dlambda (k_variant_out)
+    CK(cudaMemcpyAsync(S.e + E_DUDL + lvl, ctx->d_xtra + 4, sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
   if (ctx->clewld && S.rshk == sh) {
     double recip[9];
     for (int i = 0; i < 3; i++)
       for (int j = 0; j < 3; j++) recip[i + 3 * j] = 0.5 * ctx->oc[j + 3 * i];  // src/fft_pme.f:47-51
     if (int rc = pme_run(ctx, ctx->N, S.x, ctx->pme_q(), recip, ctx->volume, ctx->alphal, nullptr, S.e + 24, nullptr,
-                         nullptr, f))
+                         nullptr, f, dudl ? ctx->d_dq : nullptr, dudl ? S.e + E_DUDL + 3 : nullptr))
       return rc;
     if (int rc = md_ferrf(ctx, S, f, energy)) return rc;
   }
@@ -1287,7 +1293,12 @@ static int md_run_impl(orac_gpu_ctx* ctx, int nsteps, int energy_every, double* 
       r[12] = r[13] = r[14] = r[15] = 0.0;
       for (int q = E_BOND; q < E_14; q++) r[12] += e[q];
       for (int q = E_14; q < E_ERF; q++) r[13] += e[q];
-      for (int q = E_ERF; q < E_N; q++) r[14] += e[q];
+      for (int q = E_ERF; q < E_DUDL; q++) r[14] += e[q];
+      // dU/dlambda of the alchemical windows: shells, PME, erf corrections, self term
+      if (ctx->variant == VAR_ALCH && ctx->d_dq) {
+        for (int q = E_DUDL; q < E_DUDL + 5; q++) r[15] += e[q];
+        r[15] += ctx->self_dudl;
+      }
       r[10] = r[1] + r[2] + r[3] + r[4] + r[5] + r[6] + r[7] + r[8] + r[9] + r[12] + r[13] + r[14];
       r[11] = (double)flag;
     }

@@ -167,9 +167,10 @@ class Engine:
                                                      None if d is None else d.ctypes.data), "set_lambda")
 
     def variant_energies(self):
-        """(seg_ene, dwrk, U0 LJ, U0 Coulomb, dU/dlambda, PME work) of the last
-        energy evaluation (orac_gpu_variant_energies)."""
-        out = np.zeros(6)
+        """(seg_ene, dwrk, U0 LJ, U0 Coulomb, dU/dlambda, PME work, PME
+        dU/dlambda, self dU/dlambda) of the last energy evaluations
+        (orac_gpu_variant_energies)."""
+        out = np.zeros(8)
         check(self.ctx, self.lib.orac_gpu_variant_energies(self.ctx, out), "variant_energies")
         return out
 

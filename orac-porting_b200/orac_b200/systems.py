@@ -578,6 +578,83 @@ def polymer_in_water(nchain=1700, nwat=7000, box=62.0, seed_chain=5, seed_lj=6, 
     return s
 
 
+def ligand_in_water(nlig=40, seed=8, box=44.7, nwat=3000, nfft=(48, 48, 48), group_size=3, remove_within=2.4,
+                    name="ligand40_liquid"):
+    """A flexible 40-atom ligand (a chain fragment built like the polymer:
+    bond 1.53 A, angle 112 deg, random torsions, charges N(0, 0.35)
+    neutralised per group and per molecule, LJ types drawn from the chain
+    types) at the centre of the liquid-density water box, with every water
+    whose oxygen lies within 2.4 A of a ligand atom removed.  The ligand
+    atoms are the alchemical ("removed", ss_alchemy = -2) species of the
+    lambda windows; its bonded terms are those of polymer_in_water."""
+    w = water_box(nwat=nwat, box=box, nfft=nfft, name="tmp")
+    rng = np.random.default_rng(seed)
+    lig = _grow_chain(nlig, rng)
+    lig -= lig.mean(axis=0)
+    wc = w.cartesian()
+    keep = []
+    for k in range(nwat):
+        o = wc[:, 3 * k]
+        d = lig - o
+        d -= box * np.round(d / box)
+        if (np.einsum("ij,ij->i", d, d) >= remove_within ** 2).all():
+            keep.append(k)
+    nw = len(keep)
+    q = rng.normal(0.0, 0.35, nlig)
+    lgroups = [(a, min(a + group_size - 1, nlig - 1)) for a in range(0, nlig, group_size)]
+    for a, b in lgroups:
+        q[a:b + 1] -= q[a:b + 1].mean()
+    q -= q.mean()
+    rl = np.random.default_rng(6)
+    sig = rl.uniform(2.0, 3.8, NTYPE_CHAIN)
+    eps = rl.uniform(0.02, 0.2, NTYPE_CHAIN)
+    chain_types = [(s_ * 2.0 ** (1.0 / 6.0) / 2.0, e_) for s_, e_ in zip(sig, eps)]
+    lt_lig = rng.integers(1, NTYPE_CHAIN + 1, nlig)
+    n = nlig + 3 * nw
+    pos = np.zeros((3, n))
+    pos[:, :nlig] = lig.T
+    for i, k in enumerate(keep):
+        pos[:, nlig + 3 * i:nlig + 3 * i + 3] = wc[:, 3 * k:3 * k + 3]
+    mass = np.concatenate([np.full(nlig, 12.011), np.tile([M_O, M_H, M_H], nw)])
+    qa = np.concatenate([q, np.tile([Q_O, Q_H, Q_H], nw)])
+    lt = np.concatenate([lt_lig, np.tile([NTYPE_CHAIN + 1, NTYPE_CHAIN + 2, NTYPE_CHAIN + 2], nw)]).astype(np.int32)
+    groups = lgroups + [(nlig + 3 * i, nlig + 3 * i + 2) for i in range(nw)]
+    molecules = [(0, nlig - 1)] + [(nlig + 3 * i, nlig + 3 * i + 2) for i in range(nw)]
+    bonds = [(i, i + 1) for i in range(nlig - 1)]
+    cons = []
+    for i in range(nw):
+        o = nlig + 3 * i
+        for b in ((o, o + 1), (o, o + 2), (o + 1, o + 2)):
+            bonds.append(b)
+            cons.append(b)
+    solute = np.zeros(n, dtype=bool)
+    solute[:nlig] = True
+    co = np.diag([box / 2.0] * 3)
+    s = _assemble(name, co, pos, mass, qa, lt, chain_types + water_lj_types(), groups, molecules, bonds, solute,
+                  constraints=cons, seed_v=4, alphal=0.35, order=4, nfft=tuple(nfft),
+                  ncell=(max(3, int(box / 3.1)),) * 3, fudge=0.8333, lj_fudge=0.5)
+    s.bond_k = np.full(len(s.bonds), 300.0 * 4184.0 / units.EFACT)
+    s.bond_r0 = np.full(len(s.bonds), 1.53)
+    s.bends = np.array([(i + 1, i + 2, i + 3) for i in range(nlig - 2)], dtype=np.int32)
+    s.bend_k = np.full(len(s.bends), 60.0 * 4184.0 / units.EFACT)
+    s.bend_t0 = np.full(len(s.bends), math.radians(112.0))
+    s.tors = np.array([(i + 1, i + 2, i + 3, i + 4) for i in range(nlig - 3)], dtype=np.int32)
+    s.tors_k = np.full(len(s.tors), 1.4 * 4184.0 / units.EFACT)
+    s.tors_n = np.full(len(s.tors), -3.0)
+    ss = np.ones(n, dtype=np.int32)
+    ss[:nlig] = -2
+    s.ss_alchemy = ss
+    return s
+
+
+def config3_window(k, nwin=64):
+    """Lambda window k of the 64-window alchemical batch: the ligand system
+    with lrm = lrmq = k / (nwin - 1) (soft core 0.5 0.5)."""
+    s = ligand_in_water()
+    s.name = f"ligand40_window{k}"
+    return s, k / (nwin - 1)
+
+
 def config2_polymer():
     return polymer_in_water()
 

@@ -160,3 +160,62 @@ def test_alchemy_pme_charges_and_work(name):
     close(eg, er, 0.0, "eer")
     assert np.linalg.norm(sg - sr) <= STRESS_REL * np.linalg.norm(sr)
     close(g.variant_energies()[5], er - er0, abs(er), "PME work")
+
+
+def test_alchemy_pme_dudl_matches_oracle_central_difference():
+    from orac_b200.engine import Engine
+
+    s = system("polymer_small")
+    lam, h = 0.4, 1e-4
+    g = Engine(s.copy())
+    g.set_alchemy(s.ss_alchemy)
+    g.set_lambda(0.0, lam, 0.0, lam, dlam=[0.0, 1.0, 0.0, 1.0])
+    g.fft_pme()
+    dudl = g.variant_energies()[6]
+    e = []
+    for sgn in (1, -1):
+        t = s.copy()
+        lq = np.where(s.ss_alchemy == -2, lam + sgn * h, 0.0)
+        t.charge = (1.0 - lq) * s.charge
+        e.append(oracle.Oracle(t).fft_pme()[1])
+    fd = (e[0] - e[1]) / (2 * h)
+    assert abs(dudl - fd) <= 1e-5 * abs(fd), (dudl, fd)
+
+
+def test_md_window_dudl_is_derivative_of_potential():
+    """Record column 15 of an alchemical MD window (shells, SPME, erf
+    corrections, self term) against the central difference of the oracle's
+    potential energy at the same configuration (a 1e-9 fs step leaves the
+    atoms in place)."""
+    from orac_b200.engine import Engine
+
+    s = systems.ligand_in_water()
+    lam, h = 0.3, 1e-4
+    g = Engine(s.copy())
+    g.set_alchemy(s.ss_alchemy)
+    g.set_lambda(0.0, lam, 0.0, lam, dlam=[0.0, 1.0, 0.0, 1.0])
+    g.md_setup(1e-9, 2, 4, 6, "l")
+    rec = g.md_run(1, energy_every=1)
+    dudl = rec[0, 15]
+    a = s.intra_lists()
+    u = []
+    for sgn in (1, -1):
+        lr = lam + sgn * h
+        o = oracle.Oracle(s.copy())
+        o.set_alchemy(s.ss_alchemy)
+        o.set_lambda(0.0, lr, 0.0, lr)
+        o.update_lists()
+        esh = sum(o.shell(sh)[1].sum() for sh in "mlh")
+        t = s.copy()
+        t.charge = np.where(s.ss_alchemy == -2, 1.0 - lr, 1.0) * s.charge
+        ot = oracle.Oracle(t)
+        epme = ot.fft_pme()[1]
+        eerf = 0.0
+        for pairs, fudge, iz in ((a["lbnd"], 1.0, 1), (t.constraints.ravel(), 1.0, 0), (a["int13"], 1.0, 1),
+                                 (a["int14"], 1.0 - s.fudge, 1)):
+            if len(pairs):
+                eerf += ot.ferrf(np.asarray(pairs).reshape(-1, 2), fudge, iz=iz)[1].sum()
+        eself = ot.cself()[0]
+        u.append(esh + epme + eerf + eself)
+    fd = (u[0] - u[1]) / (2 * h)
+    assert abs(dudl - fd) <= 1e-5 * abs(fd), (dudl, fd)
