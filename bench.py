@@ -25,6 +25,8 @@ import tempfile
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
+# batched systems are parallel graph branches: let the device run 32 at a time
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 for p in (os.path.join(ROOT, "orac-porting_b200"), os.path.join(ROOT, "oracle")):
     if p not in sys.path:
         sys.path.insert(0, p)

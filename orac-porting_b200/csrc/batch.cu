@@ -31,6 +31,34 @@ static int bfail(orac_gpu_batch* b, int code, const char* msg) {
   return code;
 }
 
+// parent graph of one step kind: every context's step graph as an
+// independent child node
+static int build_kind(orac_gpu_batch* b, int kind) {
+  if (b->exec[kind]) return ORAC_OK;
+  cudaGraph_t parent;
+  if (cudaGraphCreate(&parent, 0) != cudaSuccess) return bfail(b, ORAC_ERR_CUDA, "cudaGraphCreate");
+  for (auto* c : b->ctx) {
+    cudaGraph_t child = nullptr;
+    if (int rc = md_step_graph(c, kind, &child)) {
+      cudaGraphDestroy(parent);
+      return bfail(b, rc, orac_gpu_last_error(c));
+    }
+    cudaGraphNode_t node;
+    if (cudaGraphAddChildGraphNode(&node, parent, nullptr, 0, child) != cudaSuccess) {
+      cudaGraphDestroy(parent);
+      return bfail(b, ORAC_ERR_CUDA, "cudaGraphAddChildGraphNode");
+    }
+  }
+  if (cudaGraphInstantiate(&b->exec[kind], parent, 0) != cudaSuccess) {
+    cudaGraphDestroy(parent);
+    return bfail(b, ORAC_ERR_CUDA, "cudaGraphInstantiate");
+  }
+  b->graph[kind] = parent;
+  // the systems' own streams must not run work concurrently with the batch
+  for (auto* c : b->ctx) cudaStreamSynchronize(c->stream);
+  return ORAC_OK;
+}
+
 extern "C" {
 
 int orac_gpu_batch_create(orac_gpu_ctx** ctxs, int n, orac_gpu_batch** out) {
@@ -50,6 +78,13 @@ int orac_gpu_batch_create(orac_gpu_ctx** ctxs, int n, orac_gpu_batch** out) {
     return ORAC_ERR_CUDA;
   }
   *out = b;
+  // instantiate both step kinds now when every system is set up, so that no
+  // step of a run pays for it
+  bool ready = true;
+  for (auto* c : b->ctx) ready = ready && md_nupdte(c) > 0;
+  if (ready)
+    for (int kind = 0; kind < 2; kind++)
+      if (int rc = build_kind(b, kind)) return rc;
   return ORAC_OK;
 }
 
@@ -82,29 +117,7 @@ int orac_gpu_batch_run(orac_gpu_batch* b, int nsteps) {
   for (int s = 0; s < nsteps; s++) {
     const long long step = md_step_index(b->ctx[0]);
     const int kind = (step % nup == 0 && step > 0) ? 1 : 0;
-    if (!b->exec[kind]) {
-      cudaGraph_t parent;
-      if (cudaGraphCreate(&parent, 0) != cudaSuccess) return bfail(b, ORAC_ERR_CUDA, "cudaGraphCreate");
-      for (auto* c : b->ctx) {
-        cudaGraph_t child = nullptr;
-        if (int rc = md_step_graph(c, kind, &child)) {
-          cudaGraphDestroy(parent);
-          return bfail(b, rc, orac_gpu_last_error(c));
-        }
-        cudaGraphNode_t node;
-        if (cudaGraphAddChildGraphNode(&node, parent, nullptr, 0, child) != cudaSuccess) {
-          cudaGraphDestroy(parent);
-          return bfail(b, ORAC_ERR_CUDA, "cudaGraphAddChildGraphNode");
-        }
-      }
-      if (cudaGraphInstantiate(&b->exec[kind], parent, 0) != cudaSuccess) {
-        cudaGraphDestroy(parent);
-        return bfail(b, ORAC_ERR_CUDA, "cudaGraphInstantiate");
-      }
-      b->graph[kind] = parent;
-      // the systems' own streams must not run work concurrently with the batch
-      for (auto* c : b->ctx) cudaStreamSynchronize(c->stream);
-    }
+    if (int rc = build_kind(b, kind)) return rc;
     if (cudaGraphLaunch(b->exec[kind], b->stream) != cudaSuccess) return bfail(b, ORAC_ERR_CUDA, "cudaGraphLaunch");
     for (auto* c : b->ctx) md_advance(c, 1);
   }

@@ -160,8 +160,12 @@ __device__ __forceinline__ void alch_energy_fp64(const PairArgs& A, double rx, d
   }
 }
 
+#ifndef ORAC_KPAIR_MINB
+#define ORAC_KPAIR_MINB 6  // resident blocks per SM requested of the forces-only kernel
+#endif
+
 template <int MG, bool EN, int VAR>
-__global__ void __launch_bounds__(WPB * 32, (MG <= 4 && !EN) ? 5 : 1)
+__global__ void __launch_bounds__(WPB * 32, (MG <= 4 && !EN) ? ORAC_KPAIR_MINB : 1)
     k_pair(const PairArgs A) {
   extern __shared__ float2 s_lj[];
   __shared__ float4 s_ai[WPB][MG];

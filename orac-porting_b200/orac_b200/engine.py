@@ -318,7 +318,10 @@ class Batch:
         h = C.c_void_p()
         rc = self.lib.orac_gpu_batch_create(arr, len(self.engines), C.byref(h))
         if rc != L.ORAC_OK:
-            raise L.OracGpuError(f"orac_gpu_batch_create: {L.ERRORS.get(rc, rc)}")
+            msg = self.lib.orac_gpu_batch_last_error(h).decode() if h.value else ""
+            if h.value:
+                self.lib.orac_gpu_batch_destroy(h)
+            raise L.OracGpuError(f"orac_gpu_batch_create: {L.ERRORS.get(rc, rc)} {msg}")
         self.h = h
 
     def _check(self, rc, what):
