@@ -214,11 +214,13 @@ __global__ void __launch_bounds__(WPB * 32, (MG <= 4 && !EN) ? ORAC_KPAIR_MINB :
       const bool valid = k < m;
       int j = 0;
       unsigned long long msk = 0ull;
+      int2 mj = make_int2(0, 0);
       double drj = 1e300, cx = 0, cy = 0, cz = 0, imx = 0, imy = 0, imz = 0;
       if (valid) {
         j = A.lj_[row + k];
         msk = A.lmask[row + k];
         const double4 gj = A.gpos[j];
+        mj = A.gmeta[j];  // issued with the centre load: the atoms' loads need it
         double dx = gi.x - gj.x, dy = gi.y - gj.y, dz = gi.z - gj.z;
         imx = 2.0 * round(0.5 * dx);
         imy = 2.0 * round(0.5 * dy);
@@ -249,25 +251,42 @@ __global__ void __launch_bounds__(WPB * 32, (MG <= 4 && !EN) ? ORAC_KPAIR_MINB :
       if (drj >= A.r2inn0 && drj < A.r2out) {
         switched = false;
       } else if (drj >= A.r2out && drj < A.r2out0) {
-        const double rsp = sqrt(drj);
-        const double auxa = (A.arsout1 + 2.0 * rsp) / A.arsout2;
-        const double auxb = A.rout0 - rsp;
-        swd = auxa * auxb * auxb;
-        sw = (float)swd;
-        dsw = (float)((-2.0 * auxa * auxb + 2.0 * auxb * auxb / A.arsout2) / rsp);
+        // S(R) of src/force.f:311-317: FP64 where it enters the energies,
+        // FP32 (relative error 1e-7, as the pair forces) for forces only
+        if (EN) {
+          const double rsp = sqrt(drj);
+          const double auxa = (A.arsout1 + 2.0 * rsp) / A.arsout2;
+          const double auxb = A.rout0 - rsp;
+          swd = auxa * auxb * auxb;
+          sw = (float)swd;
+          dsw = (float)((-2.0 * auxa * auxb + 2.0 * auxb * auxb / A.arsout2) / rsp);
+        } else {
+          const float rsp = sqrtf((float)drj);
+          const float auxa = ((float)A.arsout1 + 2.0f * rsp) * A.iarsout2;
+          const float auxb = (float)A.rout0 - rsp;
+          sw = auxa * auxb * auxb;
+          dsw = (-2.0f * auxa * auxb + 2.0f * auxb * auxb * A.iarsout2) / rsp;
+        }
         switched = true;
       } else if (drj >= A.r2inn && drj < A.r2inn0) {
-        const double rsp = sqrt(drj);
-        const double auxa = (A.arsinn1 + 2.0 * rsp) / A.arsinn2;
-        const double auxb = A.rinn0 - rsp;
-        swd = 1.0 - auxa * auxb * auxb;
-        sw = (float)swd;
-        dsw = (float)((2.0 * auxa * auxb - 2.0 * auxb * auxb / A.arsinn2) / rsp);
+        if (EN) {
+          const double rsp = sqrt(drj);
+          const double auxa = (A.arsinn1 + 2.0 * rsp) / A.arsinn2;
+          const double auxb = A.rinn0 - rsp;
+          swd = 1.0 - auxa * auxb * auxb;
+          sw = (float)swd;
+          dsw = (float)((2.0 * auxa * auxb - 2.0 * auxb * auxb / A.arsinn2) / rsp);
+        } else {
+          const float rsp = sqrtf((float)drj);
+          const float auxa = ((float)A.arsinn1 + 2.0f * rsp) * A.iarsinn2;
+          const float auxb = (float)A.rinn0 - rsp;
+          sw = 1.0f - auxa * auxb * auxb;
+          dsw = (2.0f * auxa * auxb - 2.0f * auxb * auxb * A.iarsinn2) / rsp;
+        }
         switched = true;
       } else {
         continue;
       }
-      const int2 mj = A.gmeta[j];
       const int jfirst = mj.x, nj = mj.y & 0xff, typej = mj.y >> 8;
       const float dcx = (float)cx, dcy = (float)cy, dcz = (float)cz;
       double pconf = 0.0, pcoul = 0.0, px0 = 0.0, px1 = 0.0, px2 = 0.0;

@@ -310,6 +310,116 @@ __device__ __forceinline__ bool shake_small(double x[SMA][3], const double xo[SM
   return ok;
 }
 
+// Rigid three-atom molecules (the waters) with constraints (0,1), (0,2),
+// (1,2) in this order: the same Newton SHAKE and exact RATTLE as above with
+// the constraint topology fixed at compile time and the 3x3 systems solved
+// in closed form (adjugate over determinant).  MOL3 in the molecule record
+// marks them.
+constexpr int MOL3 = 256;
+
+__device__ __forceinline__ bool solve3x3(const double J[3][3], const double g[3], double out[3]) {
+  const double c00 = J[1][1] * J[2][2] - J[1][2] * J[2][1];
+  const double c01 = J[1][2] * J[2][0] - J[1][0] * J[2][2];
+  const double c02 = J[1][0] * J[2][1] - J[1][1] * J[2][0];
+  const double det = J[0][0] * c00 + J[0][1] * c01 + J[0][2] * c02;
+  if (det == 0.0 || !isfinite(det)) return false;
+  const double id = 1.0 / det;
+  const double c10 = J[0][2] * J[2][1] - J[0][1] * J[2][2];
+  const double c11 = J[0][0] * J[2][2] - J[0][2] * J[2][0];
+  const double c12 = J[0][1] * J[2][0] - J[0][0] * J[2][1];
+  const double c20 = J[0][1] * J[1][2] - J[0][2] * J[1][1];
+  const double c21 = J[0][2] * J[1][0] - J[0][0] * J[1][2];
+  const double c22 = J[0][0] * J[1][1] - J[0][1] * J[1][0];
+  out[0] = (c00 * g[0] + c10 * g[1] + c20 * g[2]) * id;
+  out[1] = (c01 * g[0] + c11 * g[1] + c21 * g[2]) * id;
+  out[2] = (c02 * g[0] + c12 * g[1] + c22 * g[2]) * id;
+  return true;
+}
+
+// coupling of constraints k = (a,b), l = (c,d) through the shared atoms:
+// delta(a,c) im_a - delta(a,d) im_a - delta(b,c) im_b + delta(b,d) im_b
+__device__ __forceinline__ void coupling3(const double im[SMA], double cc[3][3]) {
+  cc[0][0] = im[0] + im[1];
+  cc[0][1] = im[0];
+  cc[0][2] = -im[1];
+  cc[1][0] = im[0];
+  cc[1][1] = im[0] + im[2];
+  cc[1][2] = im[2];
+  cc[2][0] = -im[1];
+  cc[2][1] = im[2];
+  cc[2][2] = im[1] + im[2];
+}
+
+__device__ __forceinline__ void bonds3(const double x[SMA][3], double r[3][3]) {
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    r[0][d] = x[0][d] - x[1][d];
+    r[1][d] = x[0][d] - x[2][d];
+    r[2][d] = x[1][d] - x[2][d];
+  }
+}
+
+// add lambda_l * r_l * im to atom a and subtract it from atom b of each constraint
+__device__ __forceinline__ void apply3(double y[SMA][3], const double lam[3], const double r[3][3], const double im[SMA],
+                                       double scale) {
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    const double u0 = lam[0] * r[0][d] * scale, u1 = lam[1] * r[1][d] * scale, u2 = lam[2] * r[2][d] * scale;
+    y[0][d] += (u0 + u1) * im[0];
+    y[1][d] += (u2 - u0) * im[1];
+    y[2][d] -= (u1 + u2) * im[2];
+  }
+}
+
+__device__ __forceinline__ bool rattle3(const double x[SMA][3], double v[SMA][3], const double im[SMA]) {
+  double r[3][3], cc[3][3], M[3][3], rhs[3], lam[3];
+  bonds3(x, r);
+  coupling3(im, cc);
+  const int ca[3] = {0, 0, 1}, cb[3] = {1, 2, 2};
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    rhs[k] = -(r[k][0] * (v[ca[k]][0] - v[cb[k]][0]) + r[k][1] * (v[ca[k]][1] - v[cb[k]][1]) +
+               r[k][2] * (v[ca[k]][2] - v[cb[k]][2]));
+#pragma unroll
+    for (int l = 0; l < 3; l++) M[k][l] = cc[k][l] * dot3(r[k], r[l]);
+  }
+  if (!solve3x3(M, rhs, lam)) return false;
+  apply3(v, lam, r, im, 1.0);
+  return true;
+}
+
+__device__ __forceinline__ bool shake3(double x[SMA][3], const double xo[SMA][3], double v[SMA][3],
+                                       const double im[SMA], const double* L2, double dt, double tol) {
+  double r0[3][3], cc[3][3], lam[3] = {0.0, 0.0, 0.0};
+  bonds3(xo, r0);
+  coupling3(im, cc);
+  bool ok = false;
+  for (int it = 0; it < 50; it++) {
+    double dk[3][3], g[3], J[3][3], dl[3];
+    bonds3(x, dk);
+    double gmax = 0.0;
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      g[k] = -(dot3(dk[k], dk[k]) - L2[k]);
+      gmax = fmax(gmax, fabs(g[k]));
+    }
+    if (gmax < tol) {
+      ok = true;
+      break;
+    }
+#pragma unroll
+    for (int k = 0; k < 3; k++)
+#pragma unroll
+      for (int l = 0; l < 3; l++) J[k][l] = 2.0 * cc[k][l] * dot3(dk[k], r0[l]);
+    if (!solve3x3(J, g, dl)) return false;
+#pragma unroll
+    for (int l = 0; l < 3; l++) lam[l] += dl[l];
+    apply3(x, dl, r0, im, 1.0);
+  }
+  if (dt != 0.0) apply3(v, lam, r0, im, 1.0 / dt);
+  return ok;
+}
+
 __device__ __forceinline__ double kick_dv(const MolArgs& A, int i) {
   double dv = 0.0;
 #pragma unroll
@@ -343,7 +453,8 @@ __global__ void k_kick(const MolArgs A) {
         v[a][0] = v[a][1] = v[a][2] = 0;
       }
     }
-    if (!rattle_small(x, v, im, A.cloc + m.z, m.w)) atomicOr(A.flag, 1);
+    const bool ok = (m.w & MOL3) ? rattle3(x, v, im) : rattle_small(x, v, im, A.cloc + m.z, m.w & 0xff);
+    if (!ok) atomicOr(A.flag, 1);
 #pragma unroll
     for (int a = 0; a < SMA; a++) {
       if (a < m.y) {
@@ -389,8 +500,10 @@ __global__ void k_drift(const MolArgs A) {
         for (int d = 0; d < 3; d++) x[a][d] = xo[a][d] = v[a][d] = 0.0;
       }
     }
-    if (A.kick && m.w > 0)
-      if (!rattle_small(xo, v, im, A.cloc + m.z, m.w)) atomicOr(A.flag, 1);
+    const int nc = m.w & 0xff;
+    const bool mol3 = (m.w & MOL3) != 0;
+    if (A.kick && nc > 0)
+      if (!(mol3 ? rattle3(xo, v, im) : rattle_small(xo, v, im, A.cloc + m.z, nc))) atomicOr(A.flag, 1);
 #pragma unroll
     for (int a = 0; a < SMA; a++) {
       if (a < m.y) {
@@ -403,9 +516,12 @@ __global__ void k_drift(const MolArgs A) {
         }
       }
     }
-    if (m.w > 0) {
-      if (!shake_small(x, xo, v, im, A.cloc + m.z, A.dss + m.z, m.w, dt, A.tol)) atomicOr(A.flag, 1);
-      if (!rattle_small(x, v, im, A.cloc + m.z, m.w)) atomicOr(A.flag, 1);
+    if (mol3) {
+      if (!shake3(x, xo, v, im, A.dss + m.z, dt, A.tol)) atomicOr(A.flag, 1);
+      if (!rattle3(x, v, im)) atomicOr(A.flag, 1);
+    } else if (nc > 0) {
+      if (!shake_small(x, xo, v, im, A.cloc + m.z, A.dss + m.z, nc, dt, A.tol)) atomicOr(A.flag, 1);
+      if (!rattle_small(x, v, im, A.cloc + m.z, nc)) atomicOr(A.flag, 1);
     }
     double s[SMA][3];
 #pragma unroll
@@ -1030,11 +1146,29 @@ int orac_gpu_md_setup(orac_gpu_ctx* ctx, const double* x, const double* y, const
     const int nc = (int)bym[p].size();
     if (nc > 0 && nc <= SMC && mna[p] <= SMA) {
       small[p] = 1;
-      sm.push_back(make_int4(ma0[p], mna[p], (int)cloc.size(), nc));
+      // a rigid triangle (3 atoms, pairs 01, 02, 12) gets the closed-form solver
+      int slot[3] = {-1, -1, -1};
+      if (nc == 3 && mna[p] == 3)
+        for (int k : bym[p]) {
+          int a = cnst[2 * k] - 1 - ma0[p], b = cnst[2 * k + 1] - 1 - ma0[p];
+          if (a > b) std::swap(a, b);
+          const int s = (a == 0 && b == 1) ? 0 : (a == 0 && b == 2) ? 1 : (a == 1 && b == 2) ? 2 : -1;
+          if (s >= 0) slot[s] = k;
+        }
+      const bool tri = slot[0] >= 0 && slot[1] >= 0 && slot[2] >= 0;
+      sm.push_back(make_int4(ma0[p], mna[p], (int)cloc.size(), nc | (tri ? MOL3 : 0)));
       smg.push_back(make_int2(mg0[p], mng[p]));
-      for (int k : bym[p]) {
-        cloc.push_back(make_int2(cnst[2 * k] - 1 - ma0[p], cnst[2 * k + 1] - 1 - ma0[p]));
-        cd.push_back(dss[k]);
+      if (tri) {
+        const int2 pr[3] = {make_int2(0, 1), make_int2(0, 2), make_int2(1, 2)};
+        for (int q = 0; q < 3; q++) {
+          cloc.push_back(pr[q]);
+          cd.push_back(dss[slot[q]]);
+        }
+      } else {
+        for (int k : bym[p]) {
+          cloc.push_back(make_int2(cnst[2 * k] - 1 - ma0[p], cnst[2 * k + 1] - 1 - ma0[p]));
+          cd.push_back(dss[k]);
+        }
       }
     } else if (nc > 0) {
       for (int k : bym[p]) {
