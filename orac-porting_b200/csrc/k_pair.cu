@@ -92,8 +92,8 @@ __device__ __forceinline__ void alch_pair_f32(const PairArgs& A, float r2, int t
   if (eps4 > 1e-12f) {
     const float sig = A.at.opls ? 2.f * sqrtf(rmi * rmj) : rmi + rmj;
     const float s2 = sig * sig;
-    const float r6 = r2 * r2 * r2 / (s2 * s2 * s2);
-    const float gp1 = 1.f / (A.ljsoft * A.af[0][t] + r6);
+    const float r6 = __fdividef(r2 * r2 * r2, s2 * s2 * s2);
+    const float gp1 = __fdividef(1.f, A.ljsoft * A.af[0][t] + r6);
     const float gp2 = gp1 * gp1;
     const float sc = A.af[1][t] * eps4;
     f = sc * (2.f * gp1 * gp2 - gp2) * 6.f * r6 * auxa * auxa;
@@ -102,8 +102,8 @@ __device__ __forceinline__ void alch_pair_f32(const PairArgs& A, float r2, int t
   if (!A.lskip) {
     const float rsp = r2 * auxa;
     const float ar = A.alphal * rsp;
-    const float qt = 1.0f / (1.0f + AS_QP * ar);
-    const float ex = expf(-ar * ar);
+    const float qt = __fdividef(1.0f, 1.0f + AS_QP * ar);
+    const float ex = __expf(-ar * ar);
     const float erfcst = ((((AS_A5 * qt + AS_A4) * qt + AS_A3) * qt + AS_A2) * qt + AS_A1) * qt * ex;
     const float furpar = A.afq[1][t] * qq;
     uq = furpar * erfcst * auxaa;
@@ -331,7 +331,11 @@ __global__ void __launch_bounds__(WPB * 32, (MG <= 4 && !EN) ? ORAC_KPAIR_MINB :
             ry = dcy + ai.y - ob.y;
             rz = dcz + ai.z - ob.z;
             const float r2 = rx * rx + ry * ry + rz * rz;
-            const float rsqi = 1.0f / r2;
+            // 1/r from the hardware reciprocal square root, exp from ex2 and
+            // an approximate reciprocal: a few ulp, far below the pair's FP32
+            // rounding budget, and a fraction of the IEEE sequences' cost
+            const float rinv = rsqrtf(r2);
+            const float rsqi = rinv * rinv;
             if (ljon) {
               const float r6 = rsqi * rsqi * rsqi;
               const float r12 = r6 * r6;
@@ -339,19 +343,18 @@ __global__ void __launch_bounds__(WPB * 32, (MG <= 4 && !EN) ? ORAC_KPAIR_MINB :
               conf = L.x * r12 - L.y * r6;
             }
             if (!A.lskip) {
-              const float rsp = sqrtf(r2);
+              const float rsp = r2 * rinv;
               const float ar = A.alphal * rsp;
-              const float qt = 1.0f / (1.0f + AS_QP * ar);
-              const float ex = expf(-ar * ar);
+              const float qt = __fdividef(1.0f, 1.0f + AS_QP * ar);
+              const float ex = __expf(-ar * ar);
               const float erfcst =
                   ((((AS_A5 * qt + AS_A4) * qt + AS_A3) * qt + AS_A2) * qt + AS_A1) *
                   qt * ex;
               const float qq = ai.w * ob.w;
-              coul = qq * erfcst / rsp;
-              qf += qq * (erfcst + A.twrtpi * ar * ex) * rsqi / rsp;
+              coul = qq * erfcst * rinv;
+              qf += qq * (erfcst + A.twrtpi * ar * ex) * rsqi * rinv;
             } else if (!A.ewald) {
-              const float rsp = sqrtf(r2);
-              coul = ai.w * ob.w / rsp;
+              coul = ai.w * ob.w * rinv;
               qf += coul * rsqi;
             }
           }

@@ -148,6 +148,9 @@ struct GridArgs {
   const float2* tw;
   FftPlan P;
   int B;  // lines per block
+  // the y axis of the per-plane kernels
+  const float2* tw2;
+  FftPlan P2;
   // convolution
   const float* bsp1;
   const float* bsp2;
@@ -307,6 +310,68 @@ __global__ void __launch_bounds__(FFT_THREADS) k_fft(const GridArgs A) {
   }
 }
 
+// The x and y passes of one z-plane in one block, the plane staying in
+// shared memory: forward = real x rows -> r2c along x (FFTW's half spectrum
+// h1 = n1/2+1) -> c2c along y; inverse = c2c along y -> Hermitian extension
+// -> c2r along x.  Replaces two launches of k_fft each way when the plane
+// (2 n1 n2 complex values) fits in shared memory.
+constexpr int PLANE_THREADS = 256;
+
+template <bool FWD>
+__global__ void __launch_bounds__(PLANE_THREADS) k_fft_plane(const GridArgs A) {
+  extern __shared__ float2 sm[];
+  const int n1 = A.n1, n2 = A.n2, h1 = A.h1;
+  const int k = blockIdx.x;
+  const int S = n1 * n2;
+  float2* a = sm;
+  float2* b = sm + S;
+  const size_t g0 = (size_t)k * n2 * n1;
+  if (FWD) {
+    for (int e = threadIdx.x; e < S; e += blockDim.x) {
+      const long long q = (long long)A.qfix[g0 + e];
+      a[e] = make_float2((float)((double)q * (1.0 / ORAC_QSCALE)), 0.f);
+    }
+    __syncthreads();
+    float2* r = fft_smem(a, b, n2, A.P, A.tw, -1);
+    float2* o = (r == a) ? b : a;
+    for (int e = threadIdx.x; e < h1 * n2; e += blockDim.x) {
+      const int i = e / n2, j = e - i * n2;
+      o[e] = r[j * n1 + i];
+    }
+    __syncthreads();
+    float2* y = fft_smem(o, r, h1, A.P2, A.tw2, -1);
+    for (int e = threadIdx.x; e < h1 * n2; e += blockDim.x) {
+      const int j = e / h1, i = e - j * h1;
+      A.cg[((size_t)k * n2 + j) * h1 + i] = y[i * n2 + j];
+    }
+  } else {
+    for (int e = threadIdx.x; e < h1 * n2; e += blockDim.x) {
+      const int j = e / h1, i = e - j * h1;
+      a[i * n2 + j] = A.cg[((size_t)k * n2 + j) * h1 + i];
+    }
+    __syncthreads();
+    float2* y = fft_smem(a, b, h1, A.P2, A.tw2, +1);
+    float2* o = (y == a) ? b : a;
+    for (int e = threadIdx.x; e < S; e += blockDim.x) {
+      const int j = e / n1, i = e - j * n1;
+      float2 v;
+      if (i < h1) {
+        v = y[i * n2 + j];
+      } else {
+        v = y[(n1 - i) * n2 + j];
+        v.y = -v.y;
+      }
+      o[e] = v;
+    }
+    __syncthreads();
+    float2* r = fft_smem(o, y, n2, A.P, A.tw, +1);
+    for (int e = threadIdx.x; e < S; e += blockDim.x) A.rg[g0 + e] = r[e].x;
+  }
+}
+
+size_t plane_smem(int n1, int n2) { return 2 * (size_t)n1 * n2 * sizeof(float2); }
+constexpr size_t PLANE_SMEM_MAX = 200 * 1024;
+
 struct AtomArgs {
   int natom, order, n1, n2, n3;
   const double* xyz;  // [3N] Cartesian
@@ -401,20 +466,26 @@ __global__ void k_spread(const AtomArgs A) {
   }
 }
 
+// Four lanes per atom, lane s taking the B-spline planes i3 = s, s+4, s+8
+// of the p^3 grid points; the partial sums meet by shuffles.
+constexpr int GATHER_LANES = 4;
+
 __global__ void k_gather(const AtomArgs A) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+  const int t = gt / GATHER_LANES, sub = gt % GATHER_LANES;
   const int p = A.order;
   double st[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
   double dphi = 0.0;
   double fr[3] = {0, 0, 0};
   if (t < A.natom) frac_coord(A, t, fr);
-  if (t < A.natom && frac_ok(A, fr)) {
+  const bool active = t < A.natom && frac_ok(A, fr);
+  float f1 = 0.f, f2 = 0.f, f3 = 0.f, phi = 0.f;
+  if (active) {
     float th1[MAXORD], th2[MAXORD], th3[MAXORD], d1[MAXORD], d2[MAXORD], d3[MAXORD];
     bspline((float)(fr[0] - (int)fr[0]), p, th1, d1);
     bspline((float)(fr[1] - (int)fr[1]), p, th2, d2);
     bspline((float)(fr[2] - (int)fr[2]), p, th3, d3);
-    float f1 = 0.f, f2 = 0.f, f3 = 0.f, phi = 0.f;
-    for (int i3 = 0; i3 < p; i3++) {
+    for (int i3 = sub; i3 < p; i3 += GATHER_LANES) {
       const int kk = gidx((int)fr[2] - p + 1 + i3, A.n3);
       for (int i2 = 0; i2 < p; i2++) {
         const int jj = gidx((int)fr[1] - p + 1 + i2, A.n2);
@@ -432,6 +503,15 @@ __global__ void k_gather(const AtomArgs A) {
         f3 += s3 * th2[i2] * d3[i3];
       }
     }
+  }
+#pragma unroll
+  for (int o = 1; o < GATHER_LANES; o <<= 1) {
+    f1 += __shfl_xor_sync(0xffffffffu, f1, o);
+    f2 += __shfl_xor_sync(0xffffffffu, f2, o);
+    f3 += __shfl_xor_sync(0xffffffffu, f3, o);
+    phi += __shfl_xor_sync(0xffffffffu, phi, o);
+  }
+  if (active && sub == 0) {
     const double qa = A.q[t];
     const double g1 = -A.n1 * qa * (double)f1, g2 = -A.n2 * qa * (double)f2, g3 = -A.n3 * qa * (double)f3;
     const double fx = A.r11 * g1 + A.r12 * g2 + A.r13 * g3;
@@ -541,6 +621,10 @@ int pme_setup(orac_gpu_ctx* ctx, int n1, int n2, int n3, int order) {
   if (make_plan(n1, &f) || make_plan(n2, &f) || make_plan(n3, &f))
     return ctx_fail(ctx, ORAC_ERR_PARAM, "PME grid %dx%dx%d: sizes must factor into 2, 3, 5, 7", n1, n2, n3);
   if (P.n1 == n1 && P.n2 == n2 && P.n3 == n3 && P.order == order && P.qfix) return ORAC_OK;
+  if (plane_smem(n1, n2) <= PLANE_SMEM_MAX) {
+    CK(cudaFuncSetAttribute(k_fft_plane<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PLANE_SMEM_MAX));
+    CK(cudaFuncSetAttribute(k_fft_plane<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PLANE_SMEM_MAX));
+  }
   P.n1 = n1;
   P.n2 = n2;
   P.n3 = n3;
@@ -633,22 +717,35 @@ int pme_run(orac_gpu_ctx* ctx, int natom, const double* d_cart, const double* d_
   G.pivol = (float)(pif * volume);
   G.rkcut2 = 0.25 * ctx->rkcut * ctx->rkcut / (pif * pif);
   G.eout = d_eout;
-  // x forward (r2c)
-  make_plan(n1, &G.P);
-  G.tw = P.tw1;
-  G.B = lines_per_block(n1);
-  int nb = (n2 * n3 + G.B - 1) / G.B;
-  size_t sm = 2 * (size_t)G.B * n1 * sizeof(float2);
-  k_fft<XF><<<nb, FFT_THREADS, sm, ctx->stream>>>(G);
-  CKL();
-  // y forward
-  make_plan(n2, &G.P);
-  G.tw = P.tw2;
-  G.B = lines_per_block(n2);
-  nb = n3 * ((h1 + G.B - 1) / G.B);
-  sm = 2 * (size_t)G.B * n2 * sizeof(float2);
-  k_fft<YF><<<nb, FFT_THREADS, sm, ctx->stream>>>(G);
-  CKL();
+  const bool planes = plane_smem(n1, n2) <= PLANE_SMEM_MAX;
+  int nb;
+  size_t sm;
+  if (planes) {
+    // x and y forward, one block per z-plane
+    make_plan(n1, &G.P);
+    make_plan(n2, &G.P2);
+    G.tw = P.tw1;
+    G.tw2 = P.tw2;
+    k_fft_plane<true><<<n3, PLANE_THREADS, plane_smem(n1, n2), ctx->stream>>>(G);
+    CKL();
+  } else {
+    // x forward (r2c)
+    make_plan(n1, &G.P);
+    G.tw = P.tw1;
+    G.B = lines_per_block(n1);
+    nb = (n2 * n3 + G.B - 1) / G.B;
+    sm = 2 * (size_t)G.B * n1 * sizeof(float2);
+    k_fft<XF><<<nb, FFT_THREADS, sm, ctx->stream>>>(G);
+    CKL();
+    // y forward
+    make_plan(n2, &G.P);
+    G.tw = P.tw2;
+    G.B = lines_per_block(n2);
+    nb = n3 * ((h1 + G.B - 1) / G.B);
+    sm = 2 * (size_t)G.B * n2 * sizeof(float2);
+    k_fft<YF><<<nb, FFT_THREADS, sm, ctx->stream>>>(G);
+    CKL();
+  }
   // z forward + influence function + z inverse
   make_plan(n3, &G.P);
   G.tw = P.tw3;
@@ -657,23 +754,33 @@ int pme_run(orac_gpu_ctx* ctx, int natom, const double* d_cart, const double* d_
   sm = 2 * (size_t)G.B * n3 * sizeof(float2);
   k_fft<ZC><<<nb, FFT_THREADS, sm, ctx->stream>>>(G);
   CKL();
-  // y inverse
-  make_plan(n2, &G.P);
-  G.tw = P.tw2;
-  G.B = lines_per_block(n2);
-  nb = n3 * ((h1 + G.B - 1) / G.B);
-  sm = 2 * (size_t)G.B * n2 * sizeof(float2);
-  k_fft<YI><<<nb, FFT_THREADS, sm, ctx->stream>>>(G);
-  CKL();
-  // x inverse (c2r)
-  make_plan(n1, &G.P);
-  G.tw = P.tw1;
-  G.B = lines_per_block(n1);
-  nb = (n2 * n3 + G.B - 1) / G.B;
-  sm = 2 * (size_t)G.B * n1 * sizeof(float2);
-  k_fft<XI><<<nb, FFT_THREADS, sm, ctx->stream>>>(G);
-  CKL();
-  k_gather<<<(natom + 63) / 64, 64, 0, ctx->stream>>>(A);
+  if (planes) {
+    // y and x inverse, one block per z-plane
+    make_plan(n1, &G.P);
+    make_plan(n2, &G.P2);
+    G.tw = P.tw1;
+    G.tw2 = P.tw2;
+    k_fft_plane<false><<<n3, PLANE_THREADS, plane_smem(n1, n2), ctx->stream>>>(G);
+    CKL();
+  } else {
+    // y inverse
+    make_plan(n2, &G.P);
+    G.tw = P.tw2;
+    G.B = lines_per_block(n2);
+    nb = n3 * ((h1 + G.B - 1) / G.B);
+    sm = 2 * (size_t)G.B * n2 * sizeof(float2);
+    k_fft<YI><<<nb, FFT_THREADS, sm, ctx->stream>>>(G);
+    CKL();
+    // x inverse (c2r)
+    make_plan(n1, &G.P);
+    G.tw = P.tw1;
+    G.B = lines_per_block(n1);
+    nb = (n2 * n3 + G.B - 1) / G.B;
+    sm = 2 * (size_t)G.B * n1 * sizeof(float2);
+    k_fft<XI><<<nb, FFT_THREADS, sm, ctx->stream>>>(G);
+    CKL();
+  }
+  k_gather<<<(GATHER_LANES * natom + 127) / 128, 128, 0, ctx->stream>>>(A);
   CKL();
   return ORAC_OK;
 }
@@ -941,7 +1048,7 @@ extern "C" int orac_gpu_pme_kspace_static(void* stream, int numatoms, const doub
   G.tw = tws[0];
   G.B = lines_per_block(nfft1);
   k_fft<XI><<<(nfft2 * nfft3 + G.B - 1) / G.B, FFT_THREADS, 2 * (size_t)G.B * nfft1 * sizeof(float2), st>>>(G);
-  k_gather<<<(numatoms + 63) / 64, 64, 0, st>>>(A);
+  k_gather<<<(GATHER_LANES * numatoms + 127) / 128, 128, 0, st>>>(A);
   k_static_finish<<<1, 32, 0, st>>>(eout, d_energy);
   ce = cudaGetLastError();
   if (ce != cudaSuccess) return static_fail(err, err_len, ORAC_ERR_CUDA, "SPME launch: %s", cudaGetErrorString(ce));
