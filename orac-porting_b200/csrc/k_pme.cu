@@ -148,9 +148,6 @@ struct GridArgs {
   const float2* tw;
   FftPlan P;
   int B;  // lines per block
-  // the y axis of the per-plane kernels
-  const float2* tw2;
-  FftPlan P2;
   // convolution
   const float* bsp1;
   const float* bsp2;
@@ -170,6 +167,9 @@ __global__ void __launch_bounds__(FFT_THREADS) k_fft(const GridArgs A) {
   const int B = A.B;
   float2* a = sm;
   float2* b = sm + B * n;
+  // the line's twiddles, staged after the two line buffers
+  float2* tws = sm + 2 * B * n;
+  for (int e = threadIdx.x; e < n; e += blockDim.x) tws[e] = A.tw[e];
   // line geometry
   int nlines, i0 = 0, j0 = 0, k0 = 0, nl;
   if (MODE == XF || MODE == XI) {
@@ -223,7 +223,7 @@ __global__ void __launch_bounds__(FFT_THREADS) k_fft(const GridArgs A) {
   }
   __syncthreads();
   const int sign = (MODE == XF || MODE == YF) ? -1 : +1;
-  float2* res = fft_smem(a, b, nl, A.P, A.tw, MODE == ZC ? -1 : sign);
+  float2* res = fft_smem(a, b, nl, A.P, tws, MODE == ZC ? -1 : sign);
   if (MODE == ZC) {
     // influence function, src/scalar_sum.f:40-121 (element (1,1,1) untouched)
     double acc[7] = {0, 0, 0, 0, 0, 0, 0};
@@ -285,7 +285,7 @@ __global__ void __launch_bounds__(FFT_THREADS) k_fft(const GridArgs A) {
     __syncthreads();
     block_reduce_add<7>(acc, A.eout);
     float2* other = (res == a) ? b : a;
-    res = fft_smem(res, other, nl, A.P, A.tw, +1);
+    res = fft_smem(res, other, nl, A.P, tws, +1);
   }
   // ---- store
   if (MODE == XF) {
@@ -309,68 +309,6 @@ __global__ void __launch_bounds__(FFT_THREADS) k_fft(const GridArgs A) {
     }
   }
 }
-
-// The x and y passes of one z-plane in one block, the plane staying in
-// shared memory: forward = real x rows -> r2c along x (FFTW's half spectrum
-// h1 = n1/2+1) -> c2c along y; inverse = c2c along y -> Hermitian extension
-// -> c2r along x.  Replaces two launches of k_fft each way when the plane
-// (2 n1 n2 complex values) fits in shared memory.
-constexpr int PLANE_THREADS = 256;
-
-template <bool FWD>
-__global__ void __launch_bounds__(PLANE_THREADS) k_fft_plane(const GridArgs A) {
-  extern __shared__ float2 sm[];
-  const int n1 = A.n1, n2 = A.n2, h1 = A.h1;
-  const int k = blockIdx.x;
-  const int S = n1 * n2;
-  float2* a = sm;
-  float2* b = sm + S;
-  const size_t g0 = (size_t)k * n2 * n1;
-  if (FWD) {
-    for (int e = threadIdx.x; e < S; e += blockDim.x) {
-      const long long q = (long long)A.qfix[g0 + e];
-      a[e] = make_float2((float)((double)q * (1.0 / ORAC_QSCALE)), 0.f);
-    }
-    __syncthreads();
-    float2* r = fft_smem(a, b, n2, A.P, A.tw, -1);
-    float2* o = (r == a) ? b : a;
-    for (int e = threadIdx.x; e < h1 * n2; e += blockDim.x) {
-      const int i = e / n2, j = e - i * n2;
-      o[e] = r[j * n1 + i];
-    }
-    __syncthreads();
-    float2* y = fft_smem(o, r, h1, A.P2, A.tw2, -1);
-    for (int e = threadIdx.x; e < h1 * n2; e += blockDim.x) {
-      const int j = e / h1, i = e - j * h1;
-      A.cg[((size_t)k * n2 + j) * h1 + i] = y[i * n2 + j];
-    }
-  } else {
-    for (int e = threadIdx.x; e < h1 * n2; e += blockDim.x) {
-      const int j = e / h1, i = e - j * h1;
-      a[i * n2 + j] = A.cg[((size_t)k * n2 + j) * h1 + i];
-    }
-    __syncthreads();
-    float2* y = fft_smem(a, b, h1, A.P2, A.tw2, +1);
-    float2* o = (y == a) ? b : a;
-    for (int e = threadIdx.x; e < S; e += blockDim.x) {
-      const int j = e / n1, i = e - j * n1;
-      float2 v;
-      if (i < h1) {
-        v = y[i * n2 + j];
-      } else {
-        v = y[(n1 - i) * n2 + j];
-        v.y = -v.y;
-      }
-      o[e] = v;
-    }
-    __syncthreads();
-    float2* r = fft_smem(o, y, n2, A.P, A.tw, +1);
-    for (int e = threadIdx.x; e < S; e += blockDim.x) A.rg[g0 + e] = r[e].x;
-  }
-}
-
-size_t plane_smem(int n1, int n2) { return 2 * (size_t)n1 * n2 * sizeof(float2); }
-constexpr size_t PLANE_SMEM_MAX = 200 * 1024;
 
 struct AtomArgs {
   int natom, order, n1, n2, n3;
@@ -621,10 +559,6 @@ int pme_setup(orac_gpu_ctx* ctx, int n1, int n2, int n3, int order) {
   if (make_plan(n1, &f) || make_plan(n2, &f) || make_plan(n3, &f))
     return ctx_fail(ctx, ORAC_ERR_PARAM, "PME grid %dx%dx%d: sizes must factor into 2, 3, 5, 7", n1, n2, n3);
   if (P.n1 == n1 && P.n2 == n2 && P.n3 == n3 && P.order == order && P.qfix) return ORAC_OK;
-  if (plane_smem(n1, n2) <= PLANE_SMEM_MAX) {
-    CK(cudaFuncSetAttribute(k_fft_plane<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PLANE_SMEM_MAX));
-    CK(cudaFuncSetAttribute(k_fft_plane<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PLANE_SMEM_MAX));
-  }
   P.n1 = n1;
   P.n2 = n2;
   P.n3 = n3;
@@ -717,24 +651,15 @@ int pme_run(orac_gpu_ctx* ctx, int natom, const double* d_cart, const double* d_
   G.pivol = (float)(pif * volume);
   G.rkcut2 = 0.25 * ctx->rkcut * ctx->rkcut / (pif * pif);
   G.eout = d_eout;
-  const bool planes = plane_smem(n1, n2) <= PLANE_SMEM_MAX;
   int nb;
   size_t sm;
-  if (planes) {
-    // x and y forward, one block per z-plane
-    make_plan(n1, &G.P);
-    make_plan(n2, &G.P2);
-    G.tw = P.tw1;
-    G.tw2 = P.tw2;
-    k_fft_plane<true><<<n3, PLANE_THREADS, plane_smem(n1, n2), ctx->stream>>>(G);
-    CKL();
-  } else {
+  {
     // x forward (r2c)
     make_plan(n1, &G.P);
     G.tw = P.tw1;
     G.B = lines_per_block(n1);
     nb = (n2 * n3 + G.B - 1) / G.B;
-    sm = 2 * (size_t)G.B * n1 * sizeof(float2);
+    sm = (2 * (size_t)G.B + 1) * n1 * sizeof(float2);
     k_fft<XF><<<nb, FFT_THREADS, sm, ctx->stream>>>(G);
     CKL();
     // y forward
@@ -742,7 +667,7 @@ int pme_run(orac_gpu_ctx* ctx, int natom, const double* d_cart, const double* d_
     G.tw = P.tw2;
     G.B = lines_per_block(n2);
     nb = n3 * ((h1 + G.B - 1) / G.B);
-    sm = 2 * (size_t)G.B * n2 * sizeof(float2);
+    sm = (2 * (size_t)G.B + 1) * n2 * sizeof(float2);
     k_fft<YF><<<nb, FFT_THREADS, sm, ctx->stream>>>(G);
     CKL();
   }
@@ -751,24 +676,16 @@ int pme_run(orac_gpu_ctx* ctx, int natom, const double* d_cart, const double* d_
   G.tw = P.tw3;
   G.B = lines_per_block(n3);
   nb = n2 * ((h1 + G.B - 1) / G.B);
-  sm = 2 * (size_t)G.B * n3 * sizeof(float2);
+  sm = (2 * (size_t)G.B + 1) * n3 * sizeof(float2);
   k_fft<ZC><<<nb, FFT_THREADS, sm, ctx->stream>>>(G);
   CKL();
-  if (planes) {
-    // y and x inverse, one block per z-plane
-    make_plan(n1, &G.P);
-    make_plan(n2, &G.P2);
-    G.tw = P.tw1;
-    G.tw2 = P.tw2;
-    k_fft_plane<false><<<n3, PLANE_THREADS, plane_smem(n1, n2), ctx->stream>>>(G);
-    CKL();
-  } else {
+  {
     // y inverse
     make_plan(n2, &G.P);
     G.tw = P.tw2;
     G.B = lines_per_block(n2);
     nb = n3 * ((h1 + G.B - 1) / G.B);
-    sm = 2 * (size_t)G.B * n2 * sizeof(float2);
+    sm = (2 * (size_t)G.B + 1) * n2 * sizeof(float2);
     k_fft<YI><<<nb, FFT_THREADS, sm, ctx->stream>>>(G);
     CKL();
     // x inverse (c2r)
@@ -776,7 +693,7 @@ int pme_run(orac_gpu_ctx* ctx, int natom, const double* d_cart, const double* d_
     G.tw = P.tw1;
     G.B = lines_per_block(n1);
     nb = (n2 * n3 + G.B - 1) / G.B;
-    sm = 2 * (size_t)G.B * n1 * sizeof(float2);
+    sm = (2 * (size_t)G.B + 1) * n1 * sizeof(float2);
     k_fft<XI><<<nb, FFT_THREADS, sm, ctx->stream>>>(G);
     CKL();
   }
@@ -1027,27 +944,27 @@ extern "C" int orac_gpu_pme_kspace_static(void* stream, int numatoms, const doub
   make_plan(nfft1, &G.P);
   G.tw = tws[0];
   G.B = lines_per_block(nfft1);
-  k_fft<XF><<<(nfft2 * nfft3 + G.B - 1) / G.B, FFT_THREADS, 2 * (size_t)G.B * nfft1 * sizeof(float2), st>>>(G);
+  k_fft<XF><<<(nfft2 * nfft3 + G.B - 1) / G.B, FFT_THREADS, (2 * (size_t)G.B + 1) * nfft1 * sizeof(float2), st>>>(G);
   // y forward
   make_plan(nfft2, &G.P);
   G.tw = tws[1];
   G.B = lines_per_block(nfft2);
-  k_fft<YF><<<nfft3 * ((h1 + G.B - 1) / G.B), FFT_THREADS, 2 * (size_t)G.B * nfft2 * sizeof(float2), st>>>(G);
+  k_fft<YF><<<nfft3 * ((h1 + G.B - 1) / G.B), FFT_THREADS, (2 * (size_t)G.B + 1) * nfft2 * sizeof(float2), st>>>(G);
   // z forward + influence function + z inverse
   make_plan(nfft3, &G.P);
   G.tw = tws[2];
   G.B = lines_per_block(nfft3);
-  k_fft<ZC><<<nfft2 * ((h1 + G.B - 1) / G.B), FFT_THREADS, 2 * (size_t)G.B * nfft3 * sizeof(float2), st>>>(G);
+  k_fft<ZC><<<nfft2 * ((h1 + G.B - 1) / G.B), FFT_THREADS, (2 * (size_t)G.B + 1) * nfft3 * sizeof(float2), st>>>(G);
   // y inverse
   make_plan(nfft2, &G.P);
   G.tw = tws[1];
   G.B = lines_per_block(nfft2);
-  k_fft<YI><<<nfft3 * ((h1 + G.B - 1) / G.B), FFT_THREADS, 2 * (size_t)G.B * nfft2 * sizeof(float2), st>>>(G);
+  k_fft<YI><<<nfft3 * ((h1 + G.B - 1) / G.B), FFT_THREADS, (2 * (size_t)G.B + 1) * nfft2 * sizeof(float2), st>>>(G);
   // x inverse (c2r)
   make_plan(nfft1, &G.P);
   G.tw = tws[0];
   G.B = lines_per_block(nfft1);
-  k_fft<XI><<<(nfft2 * nfft3 + G.B - 1) / G.B, FFT_THREADS, 2 * (size_t)G.B * nfft1 * sizeof(float2), st>>>(G);
+  k_fft<XI><<<(nfft2 * nfft3 + G.B - 1) / G.B, FFT_THREADS, (2 * (size_t)G.B + 1) * nfft1 * sizeof(float2), st>>>(G);
   k_gather<<<(GATHER_LANES * numatoms + 127) / 128, 128, 0, st>>>(A);
   k_static_finish<<<1, 32, 0, st>>>(eout, d_energy);
   ce = cudaGetLastError();
