@@ -112,6 +112,9 @@ struct PairArgs {
   // 0: skip the image term of the molecular virial and the block reduction
   // (MD without pressure coupling needs neither)
   int stress;
+  // lanes that own one i group: 32, or 16 (two groups per warp) for lists
+  // with short rows; 16 applies to groups of at most 4 atoms
+  int lpg;
   // variant (VAR_*); REM: seg_select kind and rem_factor(3)
   int variant;
   const unsigned char* vflag;  // [N]

@@ -36,9 +36,11 @@ __device__ __forceinline__ void fix_add(unsigned long long* p, float v) {
   if (q != 0) atomicAdd(p, (unsigned long long)q);
 }
 
-__device__ __forceinline__ float warp_sum(float v) {
+// sum over the aligned runs of W lanes of a warp
+template <int W>
+__device__ __forceinline__ float seg_sum(float v) {
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  for (int o = W / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   return v;
 }
 
@@ -164,19 +166,24 @@ __device__ __forceinline__ void alch_energy_fp64(const PairArgs& A, double rx, d
 #define ORAC_KPAIR_MINB 6  // resident blocks per SM requested of the forces-only kernel
 #endif
 
-template <int MG, bool EN, int VAR>
+// LPG lanes own one i-group: 32 (a warp) for the long rows of the L and H
+// lists, 16 (a half warp, two groups per warp) for the short rows of the M
+// list, where a full warp would leave most lanes idle.
+template <int MG, bool EN, int VAR, int LPG>
 __global__ void __launch_bounds__(WPB * 32, (MG <= 4 && !EN) ? ORAC_KPAIR_MINB : 1)
     k_pair(const PairArgs A) {
+  constexpr int SEG = 32 / LPG;  // groups per warp
   extern __shared__ float2 s_lj[];
-  __shared__ float4 s_ai[WPB][MG];
-  __shared__ int s_ti[WPB][MG];
-  __shared__ float s_pm[WPB][MG];
-  __shared__ double s_qd[WPB][MG];
-  __shared__ int s_fi[WPB][MG];
-  __shared__ float2 s_sf[WPB][MG];
+  __shared__ float4 s_ai[WPB * SEG][MG];
+  __shared__ int s_ti[WPB * SEG][MG];
+  __shared__ float s_pm[WPB * SEG][MG];
+  __shared__ double s_qd[WPB * SEG][MG];
+  __shared__ int s_fi[WPB * SEG][MG];
+  __shared__ float2 s_sf[WPB * SEG][MG];
   __shared__ double s_red[WPB][ACC_N];
 
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int sub = lane / LPG, sl = lane % LPG, slot = warp * SEG + sub;
   const int nt2 = A.ntype * A.ntype;
   const bool staged = nt2 <= LJ_SMEM_MAX;
   if (staged)
@@ -190,27 +197,33 @@ __global__ void __launch_bounds__(WPB * 32, (MG <= 4 && !EN) ? ORAC_KPAIR_MINB :
   float v00 = 0, v01 = 0, v02 = 0, v10 = 0, v11 = 0, v12 = 0, v20 = 0,
         v21 = 0, v22 = 0;
 
-  for (int i = blockIdx.x * WPB + warp; i < A.ngrp; i += gridDim.x * WPB) {
-    const int2 mi = A.gmeta[i];
+  // every lane of a warp runs the same trip counts, so the warp-wide
+  // ballots and shuffles stay convergent
+  for (int pw = blockIdx.x * WPB + warp; pw * SEG < A.ngrp; pw += gridDim.x * WPB) {
+    const int i = pw * SEG + sub;
+    const bool gvalid = i < A.ngrp;
+    const int2 mi = gvalid ? A.gmeta[i] : make_int2(0, 0);
     const int ifirst = mi.x, ni = mi.y & 0xff, typei = mi.y >> 8;
-    const double4 gi = A.gpos[i];
-    if (lane < ni) {
-      s_ai[warp][lane] = A.aoff[ifirst + lane];
-      s_ti[warp][lane] = A.atype[ifirst + lane];
-      s_pm[warp][lane] = A.apm[ifirst + lane];
-      if (EN) s_qd[warp][lane] = A.qd[ifirst + lane];
-      if (VAR != VAR_STD) s_fi[warp][lane] = A.vflag[ifirst + lane];
-      if (VAR == VAR_ALCH) s_sf[warp][lane] = A.soft[ifirst + lane];
+    const double4 gi = gvalid ? A.gpos[i] : make_double4(0, 0, 0, 0);
+    if (sl < ni) {
+      s_ai[slot][sl] = A.aoff[ifirst + sl];
+      s_ti[slot][sl] = A.atype[ifirst + sl];
+      s_pm[slot][sl] = A.apm[ifirst + sl];
+      if (EN) s_qd[slot][sl] = A.qd[ifirst + sl];
+      if (VAR != VAR_STD) s_fi[slot][sl] = A.vflag[ifirst + sl];
+      if (VAR == VAR_ALCH) s_sf[slot][sl] = A.soft[ifirst + sl];
     }
     __syncwarp();
     float fi[MG][3];
 #pragma unroll
     for (int a = 0; a < MG; a++) fi[a][0] = fi[a][1] = fi[a][2] = 0.f;
 
-    const int row = A.off[i], m = A.cnt[i];
+    const int row = gvalid ? A.off[i] : 0, m = gvalid ? A.cnt[i] : 0;
+    int mmax = m;
+    if (SEG == 2) mmax = max(mmax, __shfl_xor_sync(0xffffffffu, m, 16));
     int nout = 0;
-    for (int base = 0; base < m; base += 32) {
-      const int k = base + lane;
+    for (int base = 0; base < mmax; base += LPG) {
+      const int k = base + sl;
       const bool valid = k < m;
       int j = 0;
       unsigned long long msk = 0ull;
@@ -235,9 +248,10 @@ __global__ void __launch_bounds__(WPB * 32, (MG <= 4 && !EN) ? ORAC_KPAIR_MINB :
       }
       if (A.next_on) {
         const bool keep = valid && drj < A.r2neigh;
-        const unsigned bal = __ballot_sync(0xffffffffu, keep);
+        const unsigned ball = __ballot_sync(0xffffffffu, keep);
+        const unsigned bal = SEG == 2 ? (ball >> (sub * 16)) & 0xffffu : ball;
         if (keep) {
-          const int pos = nout + __popc(bal & ((1u << lane) - 1u));
+          const int pos = nout + __popc(bal & ((1u << sl) - 1u));
           A.j_out[row + pos] = j;
           A.mask_out[row + pos] = msk;
         }
@@ -303,7 +317,7 @@ __global__ void __launch_bounds__(WPB * 32, (MG <= 4 && !EN) ? ORAC_KPAIR_MINB :
         for (int a = 0; a < MG; a++) {
           if (a >= ni) break;
           if ((msk >> (a * 8 + b)) & 1ull) continue;
-          const float4 ai = s_ai[warp][a];
+          const float4 ai = s_ai[slot][a];
           float qf = 0.f, conf = 0.f, coul = 0.f;
           float rx, ry, rz;
           bool ljon = false;
@@ -311,9 +325,9 @@ __global__ void __launch_bounds__(WPB * 32, (MG <= 4 && !EN) ? ORAC_KPAIR_MINB :
           if constexpr (VAR == VAR_ALCH) {
             // src/force_alchemy.f:412-451: exclusions and fixed-mass pairs
             // are always skipped; no LJ and no Coulomb skips the pair
-            const int fia = s_fi[warp][a];
+            const int fia = s_fi[slot][a];
             if (fia & fjb & VF_MINF) continue;
-            const float2 sa = s_sf[warp][a];
+            const float2 sa = s_sf[slot][a];
             const float eps4 = sa.y * sfb.y;
             if (eps4 < 1e-12f && A.lskip && A.ewald) continue;
             npairs++;
@@ -323,7 +337,7 @@ __global__ void __launch_bounds__(WPB * 32, (MG <= 4 && !EN) ? ORAC_KPAIR_MINB :
             rz = dcz + ai.z - ob.z;
             alch_pair_f32(A, rx * rx + ry * ry + rz * rz, tal, sa.x, sfb.x, eps4, ai.w * ob.w, &qf, &conf, &coul);
           } else {
-            const float2 L = lj[s_ti[warp][a] * A.ntype + tb];
+            const float2 L = lj[s_ti[slot][a] * A.ntype + tb];
             ljon = L.y != 0.f;
             if (A.lskip && !ljon && A.ewald) continue;  // src/force.f:416-417
             npairs++;
@@ -360,7 +374,7 @@ __global__ void __launch_bounds__(WPB * 32, (MG <= 4 && !EN) ? ORAC_KPAIR_MINB :
           }
           // force_rem (src/force_REM.f:491-495,634-678): selected pairs scale
           // their force and their share of the S'V sum
-          const bool sel = (VAR == VAR_REM) && seg_sel(A.rem_kind, s_fi[warp][a], fjb);
+          const bool sel = (VAR == VAR_REM) && seg_sel(A.rem_kind, s_fi[slot][a], fjb);
           if (switched) {
             vsum += sel ? (conf + coul) * A.rem_factor : conf + coul;
             qf *= sw;
@@ -373,13 +387,13 @@ __global__ void __launch_bounds__(WPB * 32, (MG <= 4 && !EN) ? ORAC_KPAIR_MINB :
             double cd, qd;
             if constexpr (VAR == VAR_ALCH) {
               double c0, q0, du;
-              alch_energy_fp64(A, erx, ery, erz, A.softd[ifirst + a], A.softd[jfirst + b], s_qd[warp][a] * qbd, tal,
+              alch_energy_fp64(A, erx, ery, erz, A.softd[ifirst + a], A.softd[jfirst + b], s_qd[slot][a] * qbd, tal,
                                &cd, &qd, &c0, &q0, &du);
               px0 += c0;
               px1 += q0;
               px2 += du;
             } else {
-              pair_energy_fp64(A, erx, ery, erz, A.ljd[s_ti[warp][a] * A.ntype + tb], ljon, s_qd[warp][a] * qbd, &cd,
+              pair_energy_fp64(A, erx, ery, erz, A.ljd[s_ti[slot][a] * A.ntype + tb], ljon, s_qd[slot][a] * qbd, &cd,
                                &qd);
               if (sel) px0 += cd + qd;  // seg_ene
             }
@@ -413,7 +427,7 @@ __global__ void __launch_bounds__(WPB * 32, (MG <= 4 && !EN) ? ORAC_KPAIR_MINB :
 #pragma unroll
         for (int a = 0; a < MG; a++) {
           if (a >= ni) break;
-          const float pm = s_pm[warp][a];
+          const float pm = s_pm[slot][a];
           fi[a][0] += pm * sx;
           fi[a][1] += pm * sy;
           fi[a][2] += pm * sz;
@@ -458,18 +472,22 @@ __global__ void __launch_bounds__(WPB * 32, (MG <= 4 && !EN) ? ORAC_KPAIR_MINB :
         v22 += gz * iz;
       }
     }
-    if (A.next_on && lane == 0) {
+    if (A.next_on && sl == 0 && gvalid) {
       A.cnt_out[i] = nout;
       nkept += (unsigned)nout;
     }
     if (A.forces_on) {
+      // the segments of a warp may hold groups of different sizes: the
+      // shuffles run to the larger one
+      int nimax = ni;
+      if (SEG == 2) nimax = max(nimax, __shfl_xor_sync(0xffffffffu, ni, 16));
 #pragma unroll
       for (int a = 0; a < MG; a++) {
-        if (a >= ni) break;
-        const float sx = warp_sum(fi[a][0]);
-        const float sy = warp_sum(fi[a][1]);
-        const float sz = warp_sum(fi[a][2]);
-        if (lane == 0) {
+        if (a >= nimax) break;
+        const float sx = seg_sum<LPG>(fi[a][0]);
+        const float sy = seg_sum<LPG>(fi[a][1]);
+        const float sz = seg_sum<LPG>(fi[a][2]);
+        if (sl == 0 && a < ni) {
           fix_add(A.ffix + ifirst + a, sx);
           fix_add(A.ffix + A.natom + ifirst + a, sy);
           fix_add(A.ffix + 2 * A.natom + ifirst + a, sz);
@@ -508,8 +526,8 @@ __global__ void __launch_bounds__(WPB * 32, (MG <= 4 && !EN) ? ORAC_KPAIR_MINB :
     double s = 0;
     for (int w = 0; w < WPB; w++) s += s_red[w][threadIdx.x];
     // slots 0..14 = ACC_CONF..ACC_VIMG+8, then ACC_X..ACC_X+2
-    const int slot = threadIdx.x < 15 ? (int)threadIdx.x : ACC_X + (int)threadIdx.x - 15;
-    if (s != 0.0) atomicAdd(A.acc + slot, s);
+    const int acc_slot = threadIdx.x < 15 ? (int)threadIdx.x : ACC_X + (int)threadIdx.x - 15;
+    if (s != 0.0) atomicAdd(A.acc + acc_slot, s);
   }
 }
 
@@ -594,32 +612,40 @@ __global__ void k_finalize(int N, const unsigned long long* __restrict__ ffix,
 }  // namespace
 
 int pair_launch(orac_gpu_ctx* ctx, const PairArgs& a, int maxg) {
-  int nb = (a.ngrp + WPB - 1) / WPB;
-  if (nb < 1) nb = 1;
   const size_t smem = (size_t)(a.ntype * a.ntype <= LJ_SMEM_MAX ? a.ntype * a.ntype : 0) * sizeof(float2);
   if (maxg > ORAC_MAXG)
     return ctx_fail(ctx, ORAC_ERR_PARAM, "charge group of %d atoms exceeds %d", maxg, ORAC_MAXG);
   if (a.variant < VAR_STD || a.variant > VAR_ALCH) return ctx_fail(ctx, ORAC_ERR_PARAM, "variant %d", a.variant);
+  const bool small = maxg <= 4;
+  const bool half = small && a.lpg == 16;
+  const int gpb = WPB * (half ? 2 : 1);  // groups per block
+  int nb = (a.ngrp + gpb - 1) / gpb;
+  if (nb < 1) nb = 1;
   int slot = -1;
   if (int rc = prof_begin(ctx, &slot)) return rc;
-  const bool small = maxg <= 4;
-  switch (a.variant * 4 + (small ? 0 : 2) + (a.energy ? 1 : 0)) {
-#define ORAC_KP(code, MG, EN, VAR) \
-  case code:                       \
-    k_pair<MG, EN, VAR><<<nb, WPB * 32, smem, ctx->stream>>>(a); \
+  switch (a.variant * 4 + (small ? 0 : 2) + (a.energy ? 1 : 0) + (half ? 12 : 0)) {
+#define ORAC_KP(code, MG, EN, VAR, LPG) \
+  case code:                            \
+    k_pair<MG, EN, VAR, LPG><<<nb, WPB * 32, smem, ctx->stream>>>(a); \
     break;
-    ORAC_KP(0, 4, false, VAR_STD)
-    ORAC_KP(1, 4, true, VAR_STD)
-    ORAC_KP(2, 8, false, VAR_STD)
-    ORAC_KP(3, 8, true, VAR_STD)
-    ORAC_KP(4, 4, false, VAR_REM)
-    ORAC_KP(5, 4, true, VAR_REM)
-    ORAC_KP(6, 8, false, VAR_REM)
-    ORAC_KP(7, 8, true, VAR_REM)
-    ORAC_KP(8, 4, false, VAR_ALCH)
-    ORAC_KP(9, 4, true, VAR_ALCH)
-    ORAC_KP(10, 8, false, VAR_ALCH)
-    ORAC_KP(11, 8, true, VAR_ALCH)
+    ORAC_KP(0, 4, false, VAR_STD, 32)
+    ORAC_KP(1, 4, true, VAR_STD, 32)
+    ORAC_KP(2, 8, false, VAR_STD, 32)
+    ORAC_KP(3, 8, true, VAR_STD, 32)
+    ORAC_KP(4, 4, false, VAR_REM, 32)
+    ORAC_KP(5, 4, true, VAR_REM, 32)
+    ORAC_KP(6, 8, false, VAR_REM, 32)
+    ORAC_KP(7, 8, true, VAR_REM, 32)
+    ORAC_KP(8, 4, false, VAR_ALCH, 32)
+    ORAC_KP(9, 4, true, VAR_ALCH, 32)
+    ORAC_KP(10, 8, false, VAR_ALCH, 32)
+    ORAC_KP(11, 8, true, VAR_ALCH, 32)
+    ORAC_KP(12, 4, false, VAR_STD, 16)
+    ORAC_KP(13, 4, true, VAR_STD, 16)
+    ORAC_KP(16, 4, false, VAR_REM, 16)
+    ORAC_KP(17, 4, true, VAR_REM, 16)
+    ORAC_KP(20, 4, false, VAR_ALCH, 16)
+    ORAC_KP(21, 4, true, VAR_ALCH, 16)
 #undef ORAC_KP
   }
   CKL();
