@@ -280,6 +280,16 @@ def gpu_arm(args, wl, s, device):
             res["batched"] = batch_arm(args, wl, s, device, flush)
         except Exception as exc:  # reported in the JSON line; the plain leg stands on its own
             res["batched_error"] = f"{type(exc).__name__}: {exc}"
+    if ws == 1 and args.uneven > 1:
+        try:
+            res["uneven"] = uneven_arm(args, wl, device, flush)
+        except Exception as exc:
+            res["uneven"] = {"error": f"{type(exc).__name__}: {exc}"}
+    if ws == 1 and args.serve > 0:
+        try:
+            res["served"] = serve_arm(args, wl, device)
+        except Exception as exc:
+            res["served"] = {"error": f"{type(exc).__name__}: {exc}"}
     return res
 
 
@@ -366,6 +376,151 @@ def batch_arm(args, wl, s, device, flush):
             "plain_total_ms": sum(plain_ms), "lambdas": lams, "dudl": dudl}
 
 
+def build_pool(specs):
+    """Host-side systems of `specs` (systems.build_spec), built in a spawn
+    process pool (no CUDA state is inherited)."""
+    import multiprocessing as mp
+    from concurrent.futures import ProcessPoolExecutor
+
+    workers = max(1, min(32, (os.cpu_count() or 1), len(specs)))
+    with ProcessPoolExecutor(max_workers=workers, mp_context=mp.get_context("spawn")) as ex:
+        return list(ex.map(systems.build_spec, specs, chunksize=1))
+
+
+def uneven_engine(s, spec, device, wl):
+    from orac_b200.engine import Engine
+
+    e = Engine(s, device=device)
+    e.set_rem(s.rematom, 0, spec["rem_factor"])  # seg_select kind 0: pairs touching the solute
+    e.md_setup(wl["dt_h"], wl["lrespa"], wl["mrespa"], wl["nupdte"], wl["rshk"], econst=0.0)
+    return e
+
+
+def uneven_arm(args, wl, device, flush):
+    """The uneven HREM batch: args.uneven solvated-chain systems with atom
+    counts log-uniform in [3k, 60k] and per-replica solute scaling
+    U[0.3, 1.0] (rem_factor on pairs touching the solute), advanced by one
+    graph launch per outer step; plain = each system alone on the same
+    driver, one after the other."""
+    import torch
+
+    from orac_b200.engine import Batch
+
+    specs = systems.uneven_specs(args.uneven)
+    t0 = time.perf_counter()
+    syst = build_pool(specs)
+    t_build = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    engines = [uneven_engine(s, sp, device, wl) for s, sp in zip(syst, specs)]
+    t_setup = time.perf_counter() - t0
+    footprint = sum(e.footprint() for e in engines)
+    kp = max(2, min(args.steps, 5))
+    plain_ms = []
+    for e in engines:
+        L = e.lib
+        st = torch.cuda.ExternalStream(L.orac_gpu_get_stream(e.ctx), device=device)
+        for _ in range(args.warmup):
+            L.orac_gpu_md_run_async(e.ctx, 1)
+        if L.orac_gpu_md_collect(e.ctx):
+            raise RuntimeError(L.orac_gpu_last_error(e.ctx).decode())
+        ms = _timed_steps(lambda: L.orac_gpu_md_run_async(e.ctx, 1), st, flush, kp)
+        if L.orac_gpu_md_collect(e.ctx):
+            raise RuntimeError(L.orac_gpu_last_error(e.ctx).decode())
+        plain_ms.append(sum(ms) / len(ms))
+    b = Batch(engines)
+    stream = torch.cuda.ExternalStream(b.stream(), device=device)
+    b.run(args.warmup)
+    nb = max(3, min(args.steps, 20))
+    step_ms = _timed_steps(lambda: b.run(1, sync=False), stream, flush, nb)
+    b.sync()
+    b.close()
+    status = [e.collect() for e in engines]
+    for e in engines:
+        e.close()
+    n = len(engines)
+    st = sorted(step_ms)
+    bval = ns_per_day(nb * n, wl["dt_h"], sum(step_ms) / 1e3)
+    pval = ns_per_day(n, wl["dt_h"], sum(plain_ms) / 1e3)
+    nat = [s.ntap for s in syst]
+    return {"workload": f"{n} solvated-chain systems, atoms log-uniform in [3k, 60k] ({min(nat)}..{max(nat)}, "
+                        f"{sum(nat)} in all), solute 5-10% as 100-atom chains, water at 0.100 atoms/A^3, SPME grid "
+                        "about 1 A (32..96), per-replica solute scaling U[0.3, 1.0] as rem_factor (kind 0), "
+                        "reciprocal space unscaled, same r-RESPA schedule as the plain workload",
+            "systems": n, "value": bval, "unit": "ns/day (aggregate over systems)",
+            "ms_per_step": sum(step_ms) / nb, "step_ms_p50": st[len(st) // 2],
+            "step_ms_p99": st[min(len(st) - 1, int(0.99 * len(st)))],
+            "plain_value": pval, "plain_ms_per_step_sum": sum(plain_ms), "speedup_vs_plain": bval / pval,
+            "device_bytes": footprint, "status_ok": all(x == 0 for x in status),
+            "host_build_s": t_build, "setup_s": t_setup,
+            "how": f"one graph launch per H step advances all {n} systems (orac_gpu_batch_run), {nb} timed steps; "
+                   f"plain = each system alone, {kp} timed steps each, summed (one at a time)"}
+
+
+def serve_arm(args, wl, device):
+    """The serving loop: Poisson arrivals (20/s, seed 11) over args.serve
+    seconds of 500-step segment requests for a population of
+    args.serve_systems solvated-chain systems (atoms log-uniform in
+    [2k, 100k]), state resident on the device, admission by a 150 GB
+    budget, at most 32 segments in flight.  Plain = the same requests one
+    at a time, first come first served, each taking 500 x its system's
+    measured single-system step time."""
+    from orac_b200 import serve
+
+    nsteps = 500
+    specs = systems.uneven_specs(args.serve_systems, seed=12, lo=2000, hi=100000, seed_scale=13)
+    for sp in specs:
+        sp["name"] = sp["name"].replace("uneven", "served")
+    syst = build_pool(specs)
+    pop = {k: s for k, s in enumerate(syst)}
+    # single-system step time of each system (plain path, engine alone)
+    t_step = {}
+    for k, (s, sp) in enumerate(zip(syst, specs)):
+        e = uneven_engine(s.copy(), sp, device, wl)
+        L = e.lib
+        for _ in range(3):
+            L.orac_gpu_md_run_async(e.ctx, 1)
+        e.collect()
+        t0 = time.perf_counter()
+        L.orac_gpu_md_run_async(e.ctx, 10)
+        if e.collect():
+            raise RuntimeError(L.orac_gpu_last_error(e.ctx).decode())
+        t_step[k] = (time.perf_counter() - t0) / 10
+        e.close()
+    arrivals = serve.poisson_arrivals(20.0, args.serve, len(specs), seed=11)
+    srv = serve.Server(device=device, budget_bytes=150e9, max_active=32, chunk=4)
+    svc = serve.Service(srv, pop, lambda s: uneven_engine(s, specs[int(s.name[len("served"):])], device, wl),
+                        nsteps=nsteps)
+    res = svc.run(arrivals, timeout=900.0)
+    stats = srv.stats()
+    svc.close()
+    srv.close()
+    lat = np.array(sorted(r["latency"] for r in res))
+    span = max(r["t_end"] for r in res) - min(r["t_arrival"] for r in res)
+    sim_ns = len(res) * nsteps * wl["dt_h"] * 1e-6
+    plat, pend = serve.fifo_one_at_a_time(arrivals, [nsteps * t_step[sid] for _, sid in arrivals])
+    pspan = pend - arrivals[0][0]
+    plat = np.sort(plat)
+    nat = [s.ntap for s in syst]
+
+    def pct(a, q):
+        return float(a[min(len(a) - 1, int(q * len(a)))])
+
+    return {"workload": f"Poisson arrivals 20/s for {args.serve:g} s ({len(arrivals)} requests) of {nsteps}-step "
+                        f"segments, systems drawn from {len(specs)} solvated-chain systems of {min(nat)}..{max(nat)} "
+                        "atoms (log-uniform in [2k, 100k], HREM solute scaling), state resident on the device, "
+                        "admission by a 150 GB budget, at most 32 segments in flight",
+            "requests": len(res), "value": sim_ns / span * 86400.0, "unit": "ns/day (aggregate)",
+            "latency_s_p50": pct(lat, 0.5), "latency_s_p99": pct(lat, 0.99),
+            "plain_value": sim_ns / pspan * 86400.0, "plain_latency_s_p50": pct(plat, 0.5),
+            "plain_latency_s_p99": pct(plat, 0.99),
+            "speedup_vs_plain": (sim_ns / span) / (sim_ns / pspan),
+            "status_ok": all(r["status"] == 0 for r in res), "builds": svc.builds, "evictions": svc.evictions,
+            "peak_reserved_gb": stats["peak_reserved"] / 1e9,
+            "how": "native executor (orac_gpu_server_*): per-system streams, 4 step graphs per chunk, pump thread; "
+                   "latency = segment end - arrival (host monotonic clock); plain = first-come-first-served single "
+                   "server with each request taking 500 x the system's measured single-system step time"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -380,6 +535,9 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=12.0, help="seconds of CPU-baseline sampling")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batch", type=int, default=64, help="alchemical lambda windows advanced together (0/1: skip)")
+    ap.add_argument("--uneven", type=int, default=128, help="systems of the uneven HREM batch (0/1: skip)")
+    ap.add_argument("--serve", type=float, default=3.0, help="seconds of Poisson arrivals of the serving leg (0: skip)")
+    ap.add_argument("--serve-systems", type=int, default=16, help="systems the serving requests draw from")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     wl = WORKLOADS[args.workload]
@@ -480,6 +638,9 @@ def main():
                    "alone through the same driver; dU/dlambda from an energy step at the end of each window"}
     elif "batched_error" in res:
         out["batched"] = {"error": res["batched_error"]}
+    for key in ("uneven", "served"):
+        if key in res:
+            out[key] = res[key]
     print(json.dumps(out))
     return 0
 

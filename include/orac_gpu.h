@@ -371,6 +371,39 @@ int orac_gpu_batch_destroy(orac_gpu_batch* b);
 const char* orac_gpu_batch_last_error(const orac_gpu_batch* b);
 void* orac_gpu_batch_stream(orac_gpu_batch* b);
 
+/* Serving (no counterpart in the reference, which runs one system per
+ * process, src/mtsmd.f) --------------------------------------------------
+ * Executor of a request loop that keeps many systems resident on one GPU:
+ * a device-memory budget (reserve / unreserve of footprints), at most
+ * max_active segments in flight (the rest wait first come first served),
+ * and a pump thread that launches each running segment's steps on its own
+ * context stream `chunk` step graphs at a time (at most two chunks queued
+ * per stream), so segments submitted while others run start at once and
+ * their kernels overlap.  A context passed to submit (set up with
+ * orac_gpu_md_setup) belongs to the server until poll reports its segment
+ * finished; then orac_gpu_md_collect gives the run's status.  Times are
+ * seconds on the host's monotonic clock (orac_gpu_server_now). */
+typedef struct orac_gpu_server orac_gpu_server;
+double orac_gpu_server_now(void);
+int orac_gpu_server_create(int device, int64_t budget_bytes, int max_active,
+                           int chunk, orac_gpu_server** out);
+/* Waits for every submitted segment, stops the pump, frees the server. */
+int orac_gpu_server_destroy(orac_gpu_server* s);
+const char* orac_gpu_server_last_error(const orac_gpu_server* s);
+/* granted = 1 and the bytes held when they fit in the budget, else 0. */
+int orac_gpu_server_reserve(orac_gpu_server* s, int64_t bytes, int* granted);
+int orac_gpu_server_unreserve(orac_gpu_server* s, int64_t bytes);
+/* Queue a segment of nsteps H steps; t_arrival <= 0 stamps the call time. */
+int orac_gpu_server_submit(orac_gpu_server* s, orac_gpu_ctx* ctx, int nsteps,
+                           int64_t tag, double t_arrival, int64_t* ticket);
+/* Up to max finished segments: ticket, tag, (arrival, start, end) times,
+ * launch status; n = how many were returned. */
+int orac_gpu_server_poll(orac_gpu_server* s, int max, int64_t* tickets,
+                         int64_t* tags, double* times3, int* status, int* n);
+/* pending, running, finished not yet polled, submitted, finished,
+ * reserved bytes, peak reserved bytes, steps launched */
+int orac_gpu_server_stats(orac_gpu_server* s, int64_t* out8);
+
 /* Measurement (no counterpart in the reference, which times with wall
  * clocks in src/timer.f) ---------------------------------------------------
  * The context's cudaStream_t, for callers that record their own events. */
@@ -385,6 +418,11 @@ int orac_gpu_counters(orac_gpu_ctx* ctx, int64_t* out4, int reset);
 int orac_gpu_prof_enable(orac_gpu_ctx* ctx, int on);
 int orac_gpu_prof_read(orac_gpu_ctx* ctx, double* ms_total, int64_t* nlaunch,
                        int reset);
+
+/* Bytes of device memory the context holds (every device allocation it
+ * made and has not freed): the footprint a memory-budgeted scheduler
+ * admits by. */
+int orac_gpu_footprint(orac_gpu_ctx* ctx, int64_t* bytes);
 
 /* Synchronise the context's stream. */
 int orac_gpu_sync(orac_gpu_ctx* ctx);

@@ -260,24 +260,30 @@ int orac_gpu_destroy(orac_gpu_ctx* ctx) {
                   ctx->d_cell_grp, ctx->d_stencil, ctx->pme.tw1, ctx->pme.tw2, ctx->pme.tw3, ctx->pme.bsp1,
                   ctx->pme.bsp2, ctx->pme.bsp3, ctx->pme.qfix, ctx->pme.cgrid, ctx->pme.rgrid, ctx->pme.theta};
   for (void* p : ptrs)
-    if (p) cudaFree(p);
+    if (p) dev_free(ctx, p);
   void* aps[] = {ctx->api.cart, ctx->api.eout, ctx->api.ipairs, ctx->api.itype, ctx->api.t12,
                  ctx->api.t6,   ctx->api.ss,   ctx->api.e4,     ctx->api.q};
   for (void* p : aps)
-    if (p) cudaFree(p);
-  if (ctx->d_wcnt) cudaFree(ctx->d_wcnt);
+    if (p) dev_free(ctx, p);
+  if (ctx->d_wcnt) dev_free(ctx, ctx->d_wcnt);
   variant_free(ctx);
   bonded_free(ctx);
   for (auto& e : ctx->prof_ev) cudaEventDestroy(e);
   for (int q = 0; q < 3; q++) {
-    if (q == 0 && ctx->lists[q].off) cudaFree(ctx->lists[q].off);
-    if (ctx->lists[q].cnt) cudaFree(ctx->lists[q].cnt);
-    if (ctx->lists[q].j) cudaFree(ctx->lists[q].j);
-    if (ctx->lists[q].mask) cudaFree(ctx->lists[q].mask);
+    if (q == 0 && ctx->lists[q].off) dev_free(ctx, ctx->lists[q].off);
+    if (ctx->lists[q].cnt) dev_free(ctx, ctx->lists[q].cnt);
+    if (ctx->lists[q].j) dev_free(ctx, ctx->lists[q].j);
+    if (ctx->lists[q].mask) dev_free(ctx, ctx->lists[q].mask);
   }
   if (ctx->h_stage) cudaFreeHost(ctx->h_stage);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
+  return ORAC_OK;
+}
+
+int orac_gpu_footprint(orac_gpu_ctx* ctx, int64_t* bytes) {
+  if (!ctx || !bytes) return ORAC_ERR_PARAM;
+  *bytes = (int64_t)ctx->dmem_bytes;
   return ORAC_OK;
 }
 

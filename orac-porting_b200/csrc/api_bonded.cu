@@ -10,7 +10,7 @@ namespace {
 
 template <typename T>
 int upload(orac_gpu_ctx* ctx, T** dst, const std::vector<T>& v) {
-  if (*dst) cudaFree(*dst);
+  if (*dst) dev_free(ctx, *dst);
   *dst = nullptr;
   if (v.empty()) return ORAC_OK;
   if (dev_alloc(ctx, dst, v.size())) return ORAC_ERR_CUDA;
@@ -85,7 +85,7 @@ void bonded_free(orac_gpu_ctx* ctx) {
   void* p[] = {B.bij, B.bpar, B.aijk, B.apot, B.tijkl, B.tpar, B.iijkl, B.ipar, B.ss, B.p14, B.t14,
                B.e1412, B.e146, B.pgrp, B.p13, B.pbond, B.pcn, B.nbt, B.e12, B.e6, B.xs};
   for (void* q : p)
-    if (q) cudaFree(q);
+    if (q) dev_free(ctx, q);
   ctx->bd = BondedDev();
 }
 

@@ -129,7 +129,7 @@ int upload_alch_charges(orac_gpu_ctx* ctx, const double* dlam) {
     if (!ctx->d_dq && dev_alloc(ctx, &ctx->d_dq, N)) return ORAC_ERR_CUDA;
     CK(cudaMemcpy(ctx->d_dq, dq.data(), sizeof(double) * N, cudaMemcpyHostToDevice));
   } else if (ctx->d_dq) {
-    cudaFree(ctx->d_dq);
+    dev_free(ctx, ctx->d_dq);
     ctx->d_dq = nullptr;
   }
   return ORAC_OK;
@@ -167,7 +167,7 @@ int variant_out_launch(orac_gpu_ctx* ctx, int forces_on) {
 void variant_free(orac_gpu_ctx* ctx) {
   void* p[] = {ctx->d_vflag, ctx->d_soft, ctx->d_softd, ctx->d_qc, ctx->d_q0, ctx->d_xtra, ctx->d_dq};
   for (void* q : p)
-    if (q) cudaFree(q);
+    if (q) dev_free(ctx, q);
 }
 
 extern "C" {

@@ -7,6 +7,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <unordered_map>
 #include <vector>
 
 #include "orac_gpu.h"
@@ -208,6 +209,8 @@ struct MdState;  // md.cu
 
 struct orac_gpu_ctx {
   MdState* md = nullptr;
+  std::unordered_map<void*, size_t> dmem;  // live device allocations
+  size_t dmem_bytes = 0;
   int device = 0;
   cudaStream_t stream = nullptr;
   char err[1024] = {0};
@@ -349,12 +352,27 @@ int ctx_fail(orac_gpu_ctx* c, int code, const char* fmt, ...);
                       __LINE__, cudaGetErrorString(e_));                    \
   } while (0)
 
+// Device allocations of a context go through dev_alloc / dev_free, which
+// keep the context's footprint (bytes held on the device) for admission by
+// memory budget.
+static inline void dev_free(orac_gpu_ctx* ctx, void* p) {
+  if (!p) return;
+  auto it = ctx->dmem.find(p);
+  if (it != ctx->dmem.end()) {
+    ctx->dmem_bytes -= it->second;
+    ctx->dmem.erase(it);
+  }
+  cudaFree(p);
+}
+
 template <typename T>
 static inline int dev_alloc(orac_gpu_ctx* ctx, T** p, size_t n) {
-  if (*p) cudaFree(*p);
+  dev_free(ctx, (void*)*p);
   *p = nullptr;
   if (n == 0) n = 1;
   CK(cudaMalloc((void**)p, n * sizeof(T)));
+  ctx->dmem[(void*)*p] = n * sizeof(T);
+  ctx->dmem_bytes += n * sizeof(T);
   return ORAC_OK;
 }
 

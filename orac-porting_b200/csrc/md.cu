@@ -787,7 +787,7 @@ void md_destroy(orac_gpu_ctx* ctx) {
                   S->invm,      S->pm,       S->sm,          S->smg,       S->cloc,    S->cdss,    S->free_atoms,
                   S->free_groups, S->bstart, S->bcab,        S->bdss,      S->e,       S->flag};
   for (void* p : ptrs)
-    if (p) cudaFree(p);
+    if (p) dev_free(ctx, p);
   delete S;
   ctx->md = nullptr;
 }

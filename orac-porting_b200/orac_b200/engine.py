@@ -300,6 +300,17 @@ class Engine:
         check(self.ctx, self.lib.orac_gpu_md_get_state(self.ctx, *a), "md_get_state")
         return np.stack(a[:3]), np.stack(a[3:])
 
+    def footprint(self):
+        """Bytes of device memory the context holds (orac_gpu_footprint)."""
+        b = C.c_int64(0)
+        check(self.ctx, self.lib.orac_gpu_footprint(self.ctx, C.byref(b)), "footprint")
+        return b.value
+
+    def collect(self):
+        """Wait for queued steps and return the run's status code
+        (orac_gpu_md_collect: SHAKE convergence, list capacity)."""
+        return self.lib.orac_gpu_md_collect(self.ctx)
+
     def cself(self):
         a = C.c_double()
         b = C.c_double()

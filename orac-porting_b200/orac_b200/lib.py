@@ -33,7 +33,7 @@ class OracGpuError(RuntimeError):
 def declared_symbols(header=HEADER):
     """Names of every function declared in include/orac_gpu.h."""
     text = open(header).read()
-    return sorted(set(re.findall(r"^\s*(?:int|const char\s*\*|void\s*\*?)\s*(orac_gpu_\w+)\s*\(", text, re.M)))
+    return sorted(set(re.findall(r"^\s*(?:int|double|const char\s*\*|void\s*\*?)\s*(orac_gpu_\w+)\s*\(", text, re.M)))
 
 
 def load():
@@ -94,6 +94,16 @@ def load():
         "orac_gpu_prof_read": (i, [_P, C.POINTER(d), C.POINTER(i64), i]),
         "orac_gpu_sync": (i, [_P]),
         "orac_gpu_stats": (i, [_P, C.POINTER(i64), C.POINTER(i64)]),
+        "orac_gpu_footprint": (i, [_P, C.POINTER(i64)]),
+        "orac_gpu_server_now": (d, []),
+        "orac_gpu_server_create": (i, [i, i64, i, i, C.POINTER(_P)]),
+        "orac_gpu_server_destroy": (i, [_P]),
+        "orac_gpu_server_last_error": (C.c_char_p, [_P]),
+        "orac_gpu_server_reserve": (i, [_P, i64, C.POINTER(i)]),
+        "orac_gpu_server_unreserve": (i, [_P, i64]),
+        "orac_gpu_server_submit": (i, [_P, _P, i, i64, d, C.POINTER(i64)]),
+        "orac_gpu_server_poll": (i, [_P, i, _P, _P, _P, _P, C.POINTER(i)]),
+        "orac_gpu_server_stats": (i, [_P, C.POINTER(i64)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name, None)

@@ -659,6 +659,167 @@ def config2_polymer():
     return polymer_in_water()
 
 
+# ------------------------------------------------- uneven solvated systems
+
+
+def _smooth(n):
+    for f in (2, 3, 5, 7):
+        while n % f == 0:
+            n //= f
+    return n == 1
+
+
+def pme_grid_for(box, spacing=1.0, lo=32, hi=96):
+    """SPME grid points per axis for a cubic box: ceil(L / spacing) rounded up
+    to the next size that factors into 2, 3, 5 and 7, clamped to [lo, hi]."""
+    n = max(lo, int(math.ceil(box / spacing - 1e-9)))
+    while not _smooth(n):
+        n += 1
+    return min(n, hi)
+
+
+def _rotations(rng, n):
+    q = rng.standard_normal((n, 4))
+    q /= np.linalg.norm(q, axis=1)[:, None]
+    a, b, c, d = q.T
+    return np.stack([
+        np.stack([a * a + b * b - c * c - d * d, 2 * (b * c - a * d), 2 * (b * d + a * c)], axis=1),
+        np.stack([2 * (b * c + a * d), a * a - b * b + c * c - d * d, 2 * (c * d - a * b)], axis=1),
+        np.stack([2 * (b * d - a * c), 2 * (c * d + a * b), a * a - b * b - c * c + d * d], axis=1),
+    ], axis=1)
+
+
+def _chain_lj_types():
+    rl = np.random.default_rng(6)
+    sig = rl.uniform(2.0, 3.8, NTYPE_CHAIN)
+    eps = rl.uniform(0.02, 0.2, NTYPE_CHAIN)
+    return [(s_ * 2.0 ** (1.0 / 6.0) / 2.0, e_) for s_, e_ in zip(sig, eps)]
+
+
+def solvated_chains(natoms, seed, solute_frac=0.075, chain_len=100, density=0.100, group_size=3, name=None,
+                    clash=2.2, remove_within=2.4, jitter=0.3):
+    """A solute of bonded chains (built like the polymer: bond 1.53 A, angle
+    112 deg, random torsions, charges N(0, 0.35) neutralised per group and
+    per chain, LJ types of the polymer) in water, about `natoms` atoms in a
+    cubic box sized for `density` atoms/A^3, SPME grid of about 1 A spacing
+    (pme_grid_for).  The solute is round(solute_frac * natoms) atoms in
+    chains of chain_len atoms (the last one takes the remainder), placed at
+    random centres with no atom within `clash` A of an earlier chain; waters
+    sit on a jittered cubic lattice, sites within `remove_within` A of a
+    solute atom removed, the rest drawn at random.  Solute atoms are
+    ss_index 1 (the rematom segment of the HREM replicas)."""
+    from scipy.spatial import cKDTree
+
+    rng = np.random.default_rng(seed)
+    box = (natoms / density) ** (1.0 / 3.0)
+    nsol = max(8, int(round(solute_frac * natoms)))
+    lens = [chain_len] * (nsol // chain_len)
+    rem = nsol - sum(lens)
+    if rem >= 8 or not lens:
+        lens.append(max(rem, 8))
+    else:
+        lens[-1] += rem
+    nsol = sum(lens)
+    chains = []
+    placed = np.zeros((0, 3))
+    for n_c in lens:
+        for _ in range(200):
+            c = _grow_chain(n_c, rng, center=rng.uniform(-box / 2, box / 2, 3), clash=clash)
+            if len(placed):
+                t = cKDTree(np.mod(placed + box / 2, box), boxsize=box)
+                if any(t.query_ball_point(np.mod(c + box / 2, box), clash, return_length=True)):
+                    continue
+            break
+        else:
+            raise RuntimeError("chain placement failed")
+        chains.append(c)
+        placed = np.concatenate([placed, c])
+    nwat = (natoms - nsol) // 3
+    tsol = cKDTree(np.mod(placed + box / 2, box), boxsize=box)
+    nl = int(math.ceil((nwat * 1.05) ** (1.0 / 3.0)))
+    while True:
+        a = box / nl
+        g = (np.stack(np.meshgrid(*(np.arange(nl),) * 3, indexing="ij"), -1).reshape(-1, 3) + 0.5) * a
+        g = g + rng.uniform(-jitter, jitter, g.shape)
+        free = tsol.query_ball_point(np.mod(g, box), remove_within, return_length=True) == 0
+        if free.sum() >= nwat:
+            break
+        nl += 1
+    sites = g[free]
+    sites = sites[np.sort(rng.permutation(len(sites))[:nwat])] - box / 2
+    R = _rotations(rng, nwat)
+    tmpl = _water_template()
+    wpos = sites[:, None, :] + np.einsum("wij,kj->wki", R, tmpl)  # [nwat, 3, 3]
+    n = nsol + 3 * nwat
+    pos = np.zeros((3, n))
+    pos[:, :nsol] = np.concatenate(chains).T
+    pos[:, nsol:] = wpos.reshape(-1, 3).T
+    q = np.zeros(nsol)
+    groups, molecules, bonds, bends, tors = [], [], [], [], []
+    a0 = 0
+    for n_c in lens:
+        qc = rng.normal(0.0, 0.35, n_c)
+        for a in range(0, n_c, group_size):
+            b = min(a + group_size, n_c)
+            qc[a:b] -= qc[a:b].mean()
+            groups.append((a0 + a, a0 + b - 1))
+        qc -= qc.mean()
+        q[a0:a0 + n_c] = qc
+        molecules.append((a0, a0 + n_c - 1))
+        bonds += [(a0 + i, a0 + i + 1) for i in range(n_c - 1)]
+        bends += [(a0 + i + 1, a0 + i + 2, a0 + i + 3) for i in range(n_c - 2)]
+        tors += [(a0 + i + 1, a0 + i + 2, a0 + i + 3, a0 + i + 4) for i in range(n_c - 3)]
+        a0 += n_c
+    lt_sol = rng.integers(1, NTYPE_CHAIN + 1, nsol)
+    mass = np.concatenate([np.full(nsol, 12.011), np.tile([M_O, M_H, M_H], nwat)])
+    qa = np.concatenate([q, np.tile([Q_O, Q_H, Q_H], nwat)])
+    lt = np.concatenate([lt_sol, np.tile([NTYPE_CHAIN + 1, NTYPE_CHAIN + 2, NTYPE_CHAIN + 2], nwat)]).astype(np.int32)
+    wg = [(nsol + 3 * i, nsol + 3 * i + 2) for i in range(nwat)]
+    groups += wg
+    molecules += wg
+    cons = []
+    for i in range(nwat):
+        o = nsol + 3 * i
+        cons += [(o, o + 1), (o, o + 2), (o + 1, o + 2)]
+    bonds += cons
+    solute = np.zeros(n, dtype=bool)
+    solute[:nsol] = True
+    ng = pme_grid_for(box)
+    sysm = _assemble(name or f"chains{nsol}_water{nwat}", np.diag([box / 2.0] * 3), pos, mass, qa, lt,
+                     _chain_lj_types() + water_lj_types(), groups, molecules, bonds, solute, constraints=cons,
+                     seed_v=seed + 1, alphal=0.35, order=4, nfft=(ng, ng, ng),
+                     ncell=(max(3, int(box / 3.1)),) * 3, fudge=0.8333, lj_fudge=0.5)
+    sysm.bond_k = np.full(len(sysm.bonds), 300.0 * 4184.0 / units.EFACT)
+    sysm.bond_r0 = np.full(len(sysm.bonds), 1.53)
+    sysm.bends = np.array(bends, dtype=np.int32).reshape(-1, 3) + 0
+    sysm.bend_k = np.full(len(sysm.bends), 60.0 * 4184.0 / units.EFACT)
+    sysm.bend_t0 = np.full(len(sysm.bends), math.radians(112.0))
+    sysm.tors = np.array(tors, dtype=np.int32).reshape(-1, 4) + 0
+    sysm.tors_k = np.full(len(sysm.tors), 1.4 * 4184.0 / units.EFACT)
+    sysm.tors_n = np.full(len(sysm.tors), -3.0)
+    sysm.rematom = solute.astype(np.uint8)
+    return sysm
+
+
+def uneven_specs(n=128, seed=9, lo=3000, hi=60000, seed_scale=10):
+    """The uneven HREM batch: n systems with atom counts log-uniform in
+    [lo, hi] and solute fractions U[0.05, 0.10] (seed), each with a solute
+    scaling factor U[0.3, 1.0] (seed_scale) applied as rem_factor to the
+    pairs touching the solute (seg_select kind 0)."""
+    r = np.random.default_rng(seed)
+    nat = np.exp(r.uniform(math.log(lo), math.log(hi), n)).round().astype(int)
+    frac = r.uniform(0.05, 0.10, n)
+    scale = np.random.default_rng(seed_scale).uniform(0.3, 1.0, n)
+    return [dict(natoms=int(nat[k]), solute_frac=float(frac[k]), rem_factor=float(scale[k]), seed=1000 + k,
+                 name=f"uneven{k}") for k in range(n)]
+
+
+def build_spec(spec):
+    """System of one uneven_specs entry (module-level so a process pool can
+    map it)."""
+    return solvated_chains(spec["natoms"], spec["seed"], spec["solute_frac"], name=spec["name"])
+
+
 # -------------------------------------------------------------- small cases
 
 
