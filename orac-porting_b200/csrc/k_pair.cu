@@ -265,37 +265,33 @@ __global__ void __launch_bounds__(WPB * 32, (MG <= 4 && !EN) ? ORAC_KPAIR_MINB :
       if (drj >= A.r2inn0 && drj < A.r2out) {
         switched = false;
       } else if (drj >= A.r2out && drj < A.r2out0) {
-        // S(R) of src/force.f:311-317: FP64 where it enters the energies,
-        // FP32 (relative error 1e-7, as the pair forces) for forces only
+        // S(R) of src/force.f:311-317: FP32 (relative error 1e-7, as the
+        // pair forces) for the forces, the same with or without energies,
+        // so an energy step leaves the trajectory bitwise unchanged; FP64
+        // where it enters the energies
+        const float rsp = sqrtf((float)drj);
+        const float auxa = ((float)A.arsout1 + 2.0f * rsp) * A.iarsout2;
+        const float auxb = (float)A.rout0 - rsp;
+        sw = auxa * auxb * auxb;
+        dsw = (-2.0f * auxa * auxb + 2.0f * auxb * auxb * A.iarsout2) / rsp;
         if (EN) {
-          const double rsp = sqrt(drj);
-          const double auxa = (A.arsout1 + 2.0 * rsp) / A.arsout2;
-          const double auxb = A.rout0 - rsp;
-          swd = auxa * auxb * auxb;
-          sw = (float)swd;
-          dsw = (float)((-2.0 * auxa * auxb + 2.0 * auxb * auxb / A.arsout2) / rsp);
-        } else {
-          const float rsp = sqrtf((float)drj);
-          const float auxa = ((float)A.arsout1 + 2.0f * rsp) * A.iarsout2;
-          const float auxb = (float)A.rout0 - rsp;
-          sw = auxa * auxb * auxb;
-          dsw = (-2.0f * auxa * auxb + 2.0f * auxb * auxb * A.iarsout2) / rsp;
+          const double rspd = sqrt(drj);
+          const double auxad = (A.arsout1 + 2.0 * rspd) / A.arsout2;
+          const double auxbd = A.rout0 - rspd;
+          swd = auxad * auxbd * auxbd;
         }
         switched = true;
       } else if (drj >= A.r2inn && drj < A.r2inn0) {
+        const float rsp = sqrtf((float)drj);
+        const float auxa = ((float)A.arsinn1 + 2.0f * rsp) * A.iarsinn2;
+        const float auxb = (float)A.rinn0 - rsp;
+        sw = 1.0f - auxa * auxb * auxb;
+        dsw = (2.0f * auxa * auxb - 2.0f * auxb * auxb * A.iarsinn2) / rsp;
         if (EN) {
-          const double rsp = sqrt(drj);
-          const double auxa = (A.arsinn1 + 2.0 * rsp) / A.arsinn2;
-          const double auxb = A.rinn0 - rsp;
-          swd = 1.0 - auxa * auxb * auxb;
-          sw = (float)swd;
-          dsw = (float)((2.0 * auxa * auxb - 2.0 * auxb * auxb / A.arsinn2) / rsp);
-        } else {
-          const float rsp = sqrtf((float)drj);
-          const float auxa = ((float)A.arsinn1 + 2.0f * rsp) * A.iarsinn2;
-          const float auxb = (float)A.rinn0 - rsp;
-          sw = 1.0f - auxa * auxb * auxb;
-          dsw = (2.0f * auxa * auxb - 2.0f * auxb * auxb * A.iarsinn2) / rsp;
+          const double rspd = sqrt(drj);
+          const double auxad = (A.arsinn1 + 2.0 * rspd) / A.arsinn2;
+          const double auxbd = A.rinn0 - rspd;
+          swd = 1.0 - auxad * auxbd * auxbd;
         }
         switched = true;
       } else {

@@ -273,7 +273,7 @@ class Engine:
     def md_setup(self, dt_h, lrespa, mrespa, nupdte, rshk="l", n1respa=1, n0respa=1, econst=0.0, graphs=True):
         """Device-resident r-RESPA run of this system (orac_gpu_md_setup)."""
         s = self.s
-        r = s.cartesian()
+        r = s.xyz_restart if s.xyz_restart is not None else s.cartesian()
         self._cn = i32(s.constraints.ravel())
         self._dss = f64(s.cdist ** 2)
         check(self.ctx, self.lib.orac_gpu_md_setup(self.ctx, f64(r[0]), f64(r[1]), f64(r[2]), f64(s.vx), f64(s.vy),

@@ -174,6 +174,7 @@ class Service:
         s = self.systems[sid]
         sc = np.linalg.inv(np.asarray(s.co)) @ x
         s.xp0, s.yp0, s.zp0 = sc[0].copy(), sc[1].copy(), sc[2].copy()
+        s.xyz_restart = np.ascontiguousarray(x)
         s.vx, s.vy, s.vz = v[0].copy(), v[1].copy(), v[2].copy()
         r.engine.close()
         self.ex.unreserve(r.nbytes)

@@ -104,6 +104,10 @@ class System:
     ss_alchemy: np.ndarray | None = None
     # REM segment (force_rem): 1 for atoms of the scaled segment
     rematom: np.ndarray | None = None
+    # Cartesian positions (3, N) saved when a resident system leaves the
+    # device; the next md_setup starts from them exactly (xp0..zp0 hold the
+    # same positions scaled, rounded)
+    xyz_restart: np.ndarray | None = None
 
     def bend_pot(self):
         """fpbend's pota..potg per bend: theta0, k, Urey-Bradley r0 and k,
@@ -678,6 +682,19 @@ def pme_grid_for(box, spacing=1.0, lo=32, hi=96):
     return min(n, hi)
 
 
+def linked_cells_for(box, shells, cell=3.1):
+    """Cells per axis of a cubic box for the outer list radius (rcuth +
+    rtolh + rneih): about `cell` A wide, and fine enough that the stencil
+    reaches no cell twice (the check of src/lc_index.f:106-122: the widest
+    offset floor(r / w) + 1 must stay below (n + 1) / 2)."""
+    r = shells.rcuth + shells.rtolh + shells.rneih
+    n0 = max(3, int(box / cell))
+    for n in range(n0, 4 * n0 + 8):
+        if int(r / (box / n)) + 1 < (n + 1) // 2:
+            return n
+    raise ValueError(f"box {box:.2f} A too small for linked cells at list radius {r:.2f} A")
+
+
 def _rotations(rng, n):
     q = rng.standard_normal((n, 4))
     q /= np.linalg.norm(q, axis=1)[:, None]
@@ -697,7 +714,7 @@ def _chain_lj_types():
 
 
 def solvated_chains(natoms, seed, solute_frac=0.075, chain_len=100, density=0.100, group_size=3, name=None,
-                    clash=2.2, remove_within=2.4, jitter=0.3):
+                    clash=2.2, remove_within=2.4, jitter=0.3, min_spacing=2.95):
     """A solute of bonded chains (built like the polymer: bond 1.53 A, angle
     112 deg, random torsions, charges N(0, 0.35) neutralised per group and
     per chain, LJ types of the polymer) in water, about `natoms` atoms in a
@@ -720,31 +737,38 @@ def solvated_chains(natoms, seed, solute_frac=0.075, chain_len=100, density=0.10
     else:
         lens[-1] += rem
     nsol = sum(lens)
-    chains = []
-    placed = np.zeros((0, 3))
-    for n_c in lens:
-        for _ in range(200):
-            c = _grow_chain(n_c, rng, center=rng.uniform(-box / 2, box / 2, 3), clash=clash)
-            if len(placed):
-                t = cKDTree(np.mod(placed + box / 2, box), boxsize=box)
-                if any(t.query_ball_point(np.mod(c + box / 2, box), clash, return_length=True)):
-                    continue
-            break
-        else:
-            raise RuntimeError("chain placement failed")
-        chains.append(c)
-        placed = np.concatenate([placed, c])
     nwat = (natoms - nsol) // 3
-    tsol = cKDTree(np.mod(placed + box / 2, box), boxsize=box)
-    nl = int(math.ceil((nwat * 1.05) ** (1.0 / 3.0)))
+    # The water lattice is no denser than the liquid box's (spacing >=
+    # min_spacing).  Where the volume the solute leaves cannot hold the
+    # waters at that spacing, the box grows by 1% (density a little below
+    # `density`) and the chains are placed again: a chain placed in a
+    # smaller box can sit closer to another's periodic image in a larger one.
     while True:
+        state = rng.bit_generator.state
+        chains = []
+        placed = np.zeros((0, 3))
+        for n_c in lens:
+            for _ in range(200):
+                c = _grow_chain(n_c, rng, center=rng.uniform(-box / 2, box / 2, 3), clash=clash, box=box)
+                if len(placed):
+                    t = cKDTree(np.mod(placed + box / 2, box), boxsize=box)
+                    if any(t.query_ball_point(np.mod(c + box / 2, box), clash, return_length=True)):
+                        continue
+                break
+            else:
+                raise RuntimeError("chain placement failed")
+            chains.append(c)
+            placed = np.concatenate([placed, c])
+        tsol = cKDTree(np.mod(placed + box / 2, box), boxsize=box)
+        nl = int(box / min_spacing)
         a = box / nl
         g = (np.stack(np.meshgrid(*(np.arange(nl),) * 3, indexing="ij"), -1).reshape(-1, 3) + 0.5) * a
         g = g + rng.uniform(-jitter, jitter, g.shape)
         free = tsol.query_ball_point(np.mod(g, box), remove_within, return_length=True) == 0
         if free.sum() >= nwat:
             break
-        nl += 1
+        box *= 1.01
+        rng.bit_generator.state = state
     sites = g[free]
     sites = sites[np.sort(rng.permutation(len(sites))[:nwat])] - box / 2
     R = _rotations(rng, nwat)
@@ -785,10 +809,11 @@ def solvated_chains(natoms, seed, solute_frac=0.075, chain_len=100, density=0.10
     solute = np.zeros(n, dtype=bool)
     solute[:nsol] = True
     ng = pme_grid_for(box)
+    nc = linked_cells_for(box, Shells())
     sysm = _assemble(name or f"chains{nsol}_water{nwat}", np.diag([box / 2.0] * 3), pos, mass, qa, lt,
                      _chain_lj_types() + water_lj_types(), groups, molecules, bonds, solute, constraints=cons,
-                     seed_v=seed + 1, alphal=0.35, order=4, nfft=(ng, ng, ng),
-                     ncell=(max(3, int(box / 3.1)),) * 3, fudge=0.8333, lj_fudge=0.5)
+                     seed_v=seed + 1, alphal=0.35, order=4, nfft=(ng, ng, ng), ncell=(nc, nc, nc),
+                     fudge=0.8333, lj_fudge=0.5)
     sysm.bond_k = np.full(len(sysm.bonds), 300.0 * 4184.0 / units.EFACT)
     sysm.bond_r0 = np.full(len(sysm.bonds), 1.53)
     sysm.bends = np.array(bends, dtype=np.int32).reshape(-1, 3) + 0
