@@ -126,9 +126,9 @@ def measured_peaks():
 
 def ncu_traffic():
     """DRAM bytes per launch of the real-space kernel from the committed ncu
-    summary (profiles/k_pair_config1.json), or None."""
+    summary (profiles/k_pair_liquid.json), or None."""
     try:
-        d = json.load(open(os.path.join(ROOT, "profiles", "k_pair_config1.json")))
+        d = json.load(open(os.path.join(ROOT, "profiles", "k_pair_liquid.json")))
         return float(d["dram_bytes_per_launch"])
     except Exception:
         return None

@@ -331,9 +331,11 @@ int orac_gpu_md_setup(orac_gpu_ctx* ctx, const double* x, const double* y,
                       double econst);
 
 /* Advance nsteps H steps (steady-state steps run as one captured CUDA graph
- * per step kind).  Every energy_every steps one record of 12 doubles goes to
+ * per step kind).  Every energy_every steps one record of 16 doubles goes to
  * rec: step, kinetic, U_M LJ, U_M Coulomb, U_L LJ, U_L Coulomb, U_H LJ,
- * U_H Coulomb, E_reciprocal, econst, total, status flag. */
+ * U_H Coulomb, E_reciprocal, econst, total, status flag, bonded (bonds,
+ * bends, torsions, impropers), 1-4 + intra-group pairs, erf corrections,
+ * dU/dlambda (alchemical contexts with dlam set, else 0). */
 int orac_gpu_md_run(orac_gpu_ctx* ctx, int nsteps, int energy_every,
                     double* rec);
 
