@@ -313,7 +313,7 @@ int orac_gpu_set_topology(orac_gpu_ctx* ctx, int ntap, int ngrp, int nprot, cons
     maxg = n > maxg ? n : maxg;
     const int ss = ss_index[a0];
     if (ss != 1 && ss != 2) return ctx_fail(ctx, ORAC_ERR_PARAM, "ss_index of atom %d is %d", a0 + 1, ss);
-    gmeta[g] = make_int2(a0, n | (ss << 8));
+    gmeta[g] = make_int2(a0, n | (ss << 8));  // LJ-atom mask added below
     gmol[g] = atomp[a0] - 1;
     for (int a = a0; a <= a1; a++) {
       if (atomg[a] != g + 1) return ctx_fail(ctx, ORAC_ERR_PARAM, "atomg(%d) != %d", a + 1, g + 1);
@@ -347,6 +347,22 @@ int orac_gpu_set_topology(orac_gpu_ctx* ctx, int ntap, int ngrp, int nprot, cons
       if (on && (float)c6 == 0.f)
         return ctx_fail(ctx, ORAC_ERR_PARAM, "ecc6(%d) = %g underflows single precision", lij, c6);
     }
+  // atoms whose type has no LJ partner at all: under lskip_ewald every pair
+  // of theirs is skipped (src/force.f:416-417), and the pair kernel skips
+  // them without a table lookup; bit a of gmeta.y >> 16 marks atom a of the
+  // group as having LJ
+  {
+    std::vector<unsigned char> tlj(ntype, 0);
+    for (int t1 = 0; t1 < ntype; t1++)
+      for (int t2 = 0; t2 < ntype; t2++)
+        if (lj[t1 * (size_t)ntype + t2].y != 0.f) tlj[t1] = 1;
+    for (int g = 0; g < G; g++) {
+      int m = 0;
+      for (int a = 0; a < (gmeta[g].y & 0xff); a++)
+        if (tlj[nbtype[gmeta[g].x + a] - 1]) m |= 1 << a;
+      gmeta[g].y |= m << 16;
+    }
+  }
   // exclusions: serial mapnl -> CSR with 0-based partners
   std::vector<int> exoff(N + 1), exj;
   {

@@ -163,16 +163,24 @@ __device__ __forceinline__ void alch_energy_fp64(const PairArgs& A, double rx, d
 }
 
 #ifndef ORAC_KPAIR_MINB
-#define ORAC_KPAIR_MINB 6  // resident blocks per SM requested of the forces-only kernel
+#define ORAC_KPAIR_MINB 6  // resident blocks per SM requested of the half-warp forces-only kernel
+#endif
+#ifndef ORAC_KPAIR_MINB32
+#define ORAC_KPAIR_MINB32 6  // the same for the warp-per-group (compacting) forces-only kernel
 #endif
 
 // LPG lanes own one i-group: 32 (a warp) for the long rows of the L and H
 // lists, 16 (a half warp, two groups per warp) for the short rows of the M
 // list, where a full warp would leave most lanes idle.
 template <int MG, bool EN, int VAR, int LPG>
-__global__ void __launch_bounds__(WPB * 32, (MG <= 4 && !EN) ? ORAC_KPAIR_MINB : 1)
+__global__ void __launch_bounds__(WPB * 32, (MG <= 4 && !EN) ? (LPG == 16 ? ORAC_KPAIR_MINB : ORAC_KPAIR_MINB32) : 1)
     k_pair(const PairArgs A) {
   constexpr int SEG = 32 / LPG;  // groups per warp
+  // long rows (a warp per group): in-band entries are compacted through a
+  // shared queue so the pair work runs on every lane; the short rows of the
+  // half-warp kernel are mostly in band and run where they are
+  constexpr bool COMPACT = LPG == 32;
+  __shared__ int s_q[COMPACT ? WPB : 1][64];
   extern __shared__ float2 s_lj[];
   __shared__ float4 s_ai[WPB * SEG][MG];
   __shared__ int s_ti[WPB * SEG][MG];
@@ -186,6 +194,8 @@ __global__ void __launch_bounds__(WPB * 32, (MG <= 4 && !EN) ? ORAC_KPAIR_MINB :
   const int sub = lane / LPG, sl = lane % LPG, slot = warp * SEG + sub;
   const int nt2 = A.ntype * A.ntype;
   const bool staged = nt2 <= LJ_SMEM_MAX;
+  __shared__ double s_vimg[WPB][9];
+  if (threadIdx.x < WPB * 9) s_vimg[threadIdx.x / 9][threadIdx.x % 9] = 0.0;
   if (staged)
     for (int k = threadIdx.x; k < nt2; k += blockDim.x) s_lj[k] = A.lj[k];
   __syncthreads();
@@ -194,8 +204,20 @@ __global__ void __launch_bounds__(WPB * 32, (MG <= 4 && !EN) ? ORAC_KPAIR_MINB :
   double ec0 = 0, ec1 = 0, ec2 = 0, eq0 = 0, eq1 = 0, eq2 = 0;
   double ex0 = 0, ex1 = 0, ex2 = 0;  // variant sums (ACC_X)
   unsigned npairs = 0, nscan = 0, nkept = 0;
-  float v00 = 0, v01 = 0, v02 = 0, v10 = 0, v11 = 0, v12 = 0, v20 = 0,
-        v21 = 0, v22 = 0;
+  // image term of the molecular virial: each pass's per-lane FP32 terms are
+  // summed over the warp in FP64 into this warp's accumulator (stress only;
+  // the terms cancel heavily, so no FP32 sums across lanes)
+  float vimg[9];
+#pragma unroll
+  for (int q = 0; q < 9; q++) vimg[q] = 0.f;
+  auto flush_vimg = [&]() {  // every lane of the warp calls it
+#pragma unroll
+    for (int q = 0; q < 9; q++) {
+      const double t = warp_sumd((double)vimg[q]);
+      if (lane == 0) s_vimg[warp][q] += t;
+      vimg[q] = 0.f;
+    }
+  };
 
   // every lane of a warp runs the same trip counts, so the warp-wide
   // ballots and shuffles stay convergent
@@ -203,7 +225,7 @@ __global__ void __launch_bounds__(WPB * 32, (MG <= 4 && !EN) ? ORAC_KPAIR_MINB :
     const int i = pw * SEG + sub;
     const bool gvalid = i < A.ngrp;
     const int2 mi = gvalid ? A.gmeta[i] : make_int2(0, 0);
-    const int ifirst = mi.x, ni = mi.y & 0xff, typei = mi.y >> 8;
+    const int ifirst = mi.x, ni = mi.y & 0xff, typei = (mi.y >> 8) & 0xff, ljmi = mi.y >> 16;
     const double4 gi = gvalid ? A.gpos[i] : make_double4(0, 0, 0, 0);
     if (sl < ni) {
       s_ai[slot][sl] = A.aoff[ifirst + sl];
@@ -221,88 +243,82 @@ __global__ void __launch_bounds__(WPB * 32, (MG <= 4 && !EN) ? ORAC_KPAIR_MINB :
     const int row = gvalid ? A.off[i] : 0, m = gvalid ? A.cnt[i] : 0;
     int mmax = m;
     if (SEG == 2) mmax = max(mmax, __shfl_xor_sync(0xffffffffu, m, 16));
-    int nout = 0;
-    for (int base = 0; base < mmax; base += LPG) {
-      const int k = base + sl;
-      const bool valid = k < m;
-      int j = 0;
-      unsigned long long msk = 0ull;
-      int2 mj = make_int2(0, 0);
-      double drj = 1e300, cx = 0, cy = 0, cz = 0, imx = 0, imy = 0, imz = 0;
-      if (valid) {
-        j = A.lj_[row + k];
-        msk = A.lmask[row + k];
-        const double4 gj = A.gpos[j];
-        mj = A.gmeta[j];  // issued with the centre load: the atoms' loads need it
-        double dx = gi.x - gj.x, dy = gi.y - gj.y, dz = gi.z - gj.z;
-        imx = 2.0 * round(0.5 * dx);
-        imy = 2.0 * round(0.5 * dy);
-        imz = 2.0 * round(0.5 * dz);
-        dx -= imx;
-        dy -= imy;
-        dz -= imz;
-        cx = A.c11 * dx + A.c12 * dy + A.c13 * dz;
-        cy = A.c22 * dy + A.c23 * dz;
-        cz = A.c33 * dz;
-        drj = cx * cx + cy * cy + cz * cz;
-      }
-      if (A.next_on) {
-        const bool keep = valid && drj < A.r2neigh;
-        const unsigned ball = __ballot_sync(0xffffffffu, keep);
-        const unsigned bal = SEG == 2 ? (ball >> (sub * 16)) & 0xffffu : ball;
-        if (keep) {
-          const int pos = nout + __popc(bal & ((1u << sl) - 1u));
-          A.j_out[row + pos] = j;
-          A.mask_out[row + pos] = msk;
-        }
-        nout += __popc(bal);
-      }
-      nscan += valid ? 1u : 0u;
-      if (!A.forces_on || !valid) continue;
-      bool switched;
-      float sw = 1.f, dsw = 0.f;
-      double swd = 1.0;
+    // Geometry of list entry k of this row: FP64 minimum image of the group
+    // centres (src/force.f:265-277) and the band of src/force.f:290-333
+    // (non-switched, or switched with S and S'); false when outside.
+    auto geometry = [&](int k, int& j, unsigned long long& msk, int2& mj, double& drj, double& cx, double& cy,
+                        double& cz, double& imx, double& imy, double& imz) {
+      j = A.lj_[row + k];
+      msk = A.lmask[row + k];
+      const double4 gj = A.gpos[j];
+      mj = A.gmeta[j];  // issued with the centre load: the atoms' loads need it
+      double dx = gi.x - gj.x, dy = gi.y - gj.y, dz = gi.z - gj.z;
+      imx = 2.0 * round(0.5 * dx);
+      imy = 2.0 * round(0.5 * dy);
+      imz = 2.0 * round(0.5 * dz);
+      dx -= imx;
+      dy -= imy;
+      dz -= imz;
+      cx = A.c11 * dx + A.c12 * dy + A.c13 * dz;
+      cy = A.c22 * dy + A.c23 * dz;
+      cz = A.c33 * dz;
+      drj = cx * cx + cy * cy + cz * cz;
+    };
+    auto band = [&](double drj, bool& switched, float& sw, float& dsw, double& swd) -> bool {
+      sw = 1.f;
+      dsw = 0.f;
+      swd = 1.0;
       if (drj >= A.r2inn0 && drj < A.r2out) {
         switched = false;
       } else if (drj >= A.r2out && drj < A.r2out0) {
-        // S(R) of src/force.f:311-317: FP32 (relative error 1e-7, as the
-        // pair forces) for the forces, the same with or without energies,
-        // so an energy step leaves the trajectory bitwise unchanged; FP64
-        // where it enters the energies
-        const float rsp = sqrtf((float)drj);
+        // S(R) of src/force.f:311-317 for the forces: FP32 arithmetic on the
+        // FP64 distance to the band edge (rout0 - R cancels to a few tenths
+        // of an A, which FP32 R would leave with 1e-5 relative error), the
+        // same expression with or without energies; FP64 where S enters the
+        // energies
+        const double rspd = sqrt(drj);
+        const float rsp = (float)rspd;
         const float auxa = ((float)A.arsout1 + 2.0f * rsp) * A.iarsout2;
-        const float auxb = (float)A.rout0 - rsp;
+        const float auxb = (float)(A.rout0 - rspd);
         sw = auxa * auxb * auxb;
         dsw = (-2.0f * auxa * auxb + 2.0f * auxb * auxb * A.iarsout2) / rsp;
         if (EN) {
-          const double rspd = sqrt(drj);
           const double auxad = (A.arsout1 + 2.0 * rspd) / A.arsout2;
           const double auxbd = A.rout0 - rspd;
           swd = auxad * auxbd * auxbd;
         }
         switched = true;
       } else if (drj >= A.r2inn && drj < A.r2inn0) {
-        const float rsp = sqrtf((float)drj);
+        const double rspd = sqrt(drj);
+        const float rsp = (float)rspd;
         const float auxa = ((float)A.arsinn1 + 2.0f * rsp) * A.iarsinn2;
-        const float auxb = (float)A.rinn0 - rsp;
+        const float auxb = (float)(A.rinn0 - rspd);
         sw = 1.0f - auxa * auxb * auxb;
         dsw = (2.0f * auxa * auxb - 2.0f * auxb * auxb * A.iarsinn2) / rsp;
         if (EN) {
-          const double rspd = sqrt(drj);
           const double auxad = (A.arsinn1 + 2.0 * rspd) / A.arsinn2;
           const double auxbd = A.rinn0 - rspd;
           swd = 1.0 - auxad * auxbd * auxbd;
         }
         switched = true;
       } else {
-        continue;
+        return false;
       }
-      const int jfirst = mj.x, nj = mj.y & 0xff, typej = mj.y >> 8;
+      return true;
+    };
+    // The pair work of one in-band entry: atom pairs, S'V term, energies
+    // and the image virial, into this lane's accumulators.
+    auto work = [&](int j, unsigned long long msk, int2 mj, double cx, double cy, double cz, double imx, double imy,
+                    double imz, bool switched, float sw, float dsw, double swd) {
+      const int jfirst = mj.x, nj = mj.y & 0xff, typej = (mj.y >> 8) & 0xff, ljmj = mj.y >> 16;
       const float dcx = (float)cx, dcy = (float)cy, dcz = (float)cz;
       double pconf = 0.0, pcoul = 0.0, px0 = 0.0, px1 = 0.0, px2 = 0.0;
       float vsum = 0.f;
       float gx = 0.f, gy = 0.f, gz = 0.f;  // total force on the j group
+      // under lskip_ewald an atom without LJ has no pair to evaluate
+      const bool ljonly = VAR != VAR_ALCH && A.lskip && A.ewald;
       for (int b = 0; b < nj; b++) {
+        if (ljonly && !((ljmj >> b) & 1)) continue;
         const float4 ob = A.aoff[jfirst + b];
         const int tb = A.atype[jfirst + b];
         const double qbd = EN ? A.qd[jfirst + b] : 0.0;
@@ -313,6 +329,7 @@ __global__ void __launch_bounds__(WPB * 32, (MG <= 4 && !EN) ? ORAC_KPAIR_MINB :
         for (int a = 0; a < MG; a++) {
           if (a >= ni) break;
           if ((msk >> (a * 8 + b)) & 1ull) continue;
+          if (ljonly && !((ljmi >> a) & 1)) continue;
           const float4 ai = s_ai[slot][a];
           float qf = 0.f, conf = 0.f, coul = 0.f;
           float rx, ry, rz;
@@ -457,16 +474,81 @@ __global__ void __launch_bounds__(WPB * 32, (MG <= 4 && !EN) ? ORAC_KPAIR_MINB :
         const float ix = (float)(A.c11 * imx + A.c12 * imy + A.c13 * imz);
         const float iy = (float)(A.c22 * imy + A.c23 * imz);
         const float iz = (float)(A.c33 * imz);
-        v00 += gx * ix;
-        v01 += gx * iy;
-        v02 += gx * iz;
-        v10 += gy * ix;
-        v11 += gy * iy;
-        v12 += gy * iz;
-        v20 += gz * ix;
-        v21 += gz * iy;
-        v22 += gz * iz;
+        vimg[0] += gx * ix;
+        vimg[1] += gx * iy;
+        vimg[2] += gx * iz;
+        vimg[3] += gy * ix;
+        vimg[4] += gy * iy;
+        vimg[5] += gy * iz;
+        vimg[6] += gz * ix;
+        vimg[7] += gz * iy;
+        vimg[8] += gz * iz;
       }
+    };
+    int nout = 0;
+    int qn = 0;  // in-band entries queued for the full-warp pass (COMPACT)
+    for (int base = 0; base < mmax; base += LPG) {
+      const int k = base + sl;
+      const bool valid = k < m;
+      int j = 0;
+      unsigned long long msk = 0ull;
+      int2 mj = make_int2(0, 0);
+      double drj = 1e300, cx = 0, cy = 0, cz = 0, imx = 0, imy = 0, imz = 0;
+      if (valid) geometry(k, j, msk, mj, drj, cx, cy, cz, imx, imy, imz);
+      if (A.next_on) {
+        const bool keep = valid && drj < A.r2neigh;
+        const unsigned ball = __ballot_sync(0xffffffffu, keep);
+        const unsigned bal = SEG == 2 ? (ball >> (sub * 16)) & 0xffffu : ball;
+        if (keep) {
+          const int pos = nout + __popc(bal & ((1u << sl) - 1u));
+          A.j_out[row + pos] = j;
+          A.mask_out[row + pos] = msk;
+        }
+        nout += __popc(bal);
+      }
+      nscan += valid ? 1u : 0u;
+      if (!A.forces_on) continue;
+      bool switched;
+      float sw, dsw;
+      double swd;
+      const bool inb = valid && band(drj, switched, sw, dsw, swd);
+      if constexpr (!COMPACT) {
+        if (inb) work(j, msk, mj, cx, cy, cz, imx, imy, imz, switched, sw, dsw, swd);
+        if (A.stress) flush_vimg();
+      } else {
+        // queue the in-band entries; a full queue runs on every lane
+        const unsigned bq = __ballot_sync(0xffffffffu, inb);
+        if (inb) s_q[warp][qn + __popc(bq & ((1u << lane) - 1u))] = k;
+        qn += __popc(bq);
+        __syncwarp();
+        if (qn >= 32) {
+          const int kq = s_q[warp][lane];
+          geometry(kq, j, msk, mj, drj, cx, cy, cz, imx, imy, imz);
+          band(drj, switched, sw, dsw, swd);
+          work(j, msk, mj, cx, cy, cz, imx, imy, imz, switched, sw, dsw, swd);
+          if (A.stress) flush_vimg();
+          __syncwarp();
+          if (lane < qn - 32) s_q[warp][lane] = s_q[warp][32 + lane];
+          qn -= 32;
+          __syncwarp();
+        }
+      }
+    }
+    if constexpr (COMPACT) {
+      if (A.forces_on && lane < qn) {
+        int j, kq = s_q[warp][lane];
+        unsigned long long msk;
+        int2 mj;
+        double drj, cx, cy, cz, imx, imy, imz;
+        bool switched;
+        float sw, dsw;
+        double swd;
+        geometry(kq, j, msk, mj, drj, cx, cy, cz, imx, imy, imz);
+        band(drj, switched, sw, dsw, swd);
+        work(j, msk, mj, cx, cy, cz, imx, imy, imz, switched, sw, dsw, swd);
+      }
+      __syncwarp();
+      if (A.stress) flush_vimg();
     }
     if (A.next_on && sl == 0 && gvalid) {
       A.cnt_out[i] = nout;
@@ -510,10 +592,13 @@ __global__ void __launch_bounds__(WPB * 32, (MG <= 4 && !EN) ? ORAC_KPAIR_MINB :
   if (!A.forces_on || (!EN && !A.stress)) return;
   // block reduction of energies and image virial
   constexpr int NV = (VAR != VAR_STD && EN) ? 18 : 15;
-  double vals[18] = {ec0, ec1, ec2, eq0, eq1, eq2, v00, v01, v02,
-                     v10, v11, v12, v20, v21, v22, ex0, ex1, ex2};
+  double vals[18] = {ec0, ec1, ec2, eq0, eq1, eq2, 0, 0, 0, 0, 0, 0, 0, 0, 0, ex0, ex1, ex2};
 #pragma unroll
   for (int q = 0; q < NV; q++) {
+    if (q >= 6 && q < 15) {
+      if (lane == 0) s_red[warp][q] = s_vimg[warp][q - 6];
+      continue;
+    }
     const double s = warp_sumd(vals[q]);
     if (lane == 0) s_red[warp][q] = s;
   }

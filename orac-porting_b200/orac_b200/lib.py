@@ -12,7 +12,8 @@ import re
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "liborac_gpu.so")
+# ORAC_GPU_LIB selects another in-tree build of the library (tuning sweeps)
+LIB_PATH = os.environ.get("ORAC_GPU_LIB") or os.path.join(HERE, "liborac_gpu.so")
 HEADER = os.path.join(os.path.dirname(os.path.dirname(HERE)), "include", "orac_gpu.h")
 
 ORAC_OK = 0
