@@ -455,10 +455,11 @@ __global__ void k_gather(const AtomArgs A) {
     const double fx = A.r11 * g1 + A.r12 * g2 + A.r13 * g3;
     const double fy = A.r21 * g1 + A.r22 * g2 + A.r23 * g3;
     const double fz = A.r31 * g1 + A.r32 * g2 + A.r33 * g3;
-    if (A.ffix) {  // fixed-point accumulator of the caller's RESPA level (one writer per atom)
-      A.ffix[t] += (unsigned long long)__double2ll_rn(fx * ORAC_FSCALE);
-      A.ffix[A.natom + t] += (unsigned long long)__double2ll_rn(fy * ORAC_FSCALE);
-      A.ffix[2 * A.natom + t] += (unsigned long long)__double2ll_rn(fz * ORAC_FSCALE);
+    if (A.ffix) {  // fixed-point accumulator of the caller's RESPA level, which
+                   // the shell pair kernel may be adding into at the same time
+      atomicAdd(A.ffix + t, (unsigned long long)__double2ll_rn(fx * ORAC_FSCALE));
+      atomicAdd(A.ffix + A.natom + t, (unsigned long long)__double2ll_rn(fy * ORAC_FSCALE));
+      atomicAdd(A.ffix + 2 * A.natom + t, (unsigned long long)__double2ll_rn(fz * ORAC_FSCALE));
     } else {
       A.f[t] += fx;
       A.f[A.natom + t] += fy;

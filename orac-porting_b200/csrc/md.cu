@@ -768,6 +768,12 @@ struct MdState {
   int pslot[2][2] = {{0, 0}, {0, 0}};  // profiling event slots of each graph
   int64_t kpg[2] = {0, 0};             // kernels per captured graph
   int last_kind = -1;                  // graph of the last queued step
+  // second stream of the step: work that depends only on the drifted
+  // positions and adds into its own level accumulators (intramolecular
+  // levels, SPME with its erf corrections) runs there beside the shell pair
+  // kernels; fork and join by events (captured as graph edges)
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
 };
 
 static MdState* md_of(orac_gpu_ctx* ctx) {
@@ -782,6 +788,9 @@ void md_destroy(orac_gpu_ctx* ctx) {
   if (S->graph) cudaGraphDestroy(S->graph);
   if (S->gexec_u) cudaGraphExecDestroy(S->gexec_u);
   if (S->graph_u) cudaGraphDestroy(S->graph_u);
+  if (S->ev_fork) cudaEventDestroy(S->ev_fork);
+  if (S->ev_join) cudaEventDestroy(S->ev_join);
+  if (S->side) cudaStreamDestroy(S->side);
   void* ptrs[] = {S->x,         S->v,        S->xo,          S->ffix[0],   S->ffix[1], S->ffix[2], S->ffix[3],
                   S->ffix[4],
                   S->invm,      S->pm,       S->sm,          S->smg,       S->cloc,    S->cdss,    S->free_atoms,
@@ -939,9 +948,9 @@ static int md_ferrf(orac_gpu_ctx* ctx, MdState& S, unsigned long long* f, bool e
   return ORAC_OK;
 }
 
-// one shell's forces into its level accumulator (zeroed by the preceding
-// drift, or here when `zero`)
-static int md_forces_shell(orac_gpu_ctx* ctx, MdState& S, char sh, int lvl, bool zero, double* e, bool energy) {
+// one shell's pair forces into its level accumulator (zeroed by the
+// preceding drift, or here when `zero`)
+static int md_shell_pair(orac_gpu_ctx* ctx, MdState& S, char sh, int lvl, bool zero, double* e, bool energy) {
   unsigned long long* f = S.ffix[lvl];
   if (zero) CK(cudaMemsetAsync(f, 0, sizeof(unsigned long long) * 3 * ctx->N, ctx->stream));
   const int flags = SH_PREPPED | SH_FIXED_OUT | (energy ? SH_ENERGY : 0);
@@ -951,17 +960,55 @@ static int md_forces_shell(orac_gpu_ctx* ctx, MdState& S, char sh, int lvl, bool
   const bool dudl = energy && ctx->variant == VAR_ALCH && ctx->d_dq;
   if (dudl)  // the shell's dU/dlambda (k_variant_out)
     CK(cudaMemcpyAsync(S.e + E_DUDL + lvl, ctx->d_xtra + 4, sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
-  if (ctx->clewld && S.rshk == sh) {
-    double recip[9];
-    for (int i = 0; i < 3; i++)
-      for (int j = 0; j < 3; j++) recip[i + 3 * j] = 0.5 * ctx->oc[j + 3 * i];  // src/fft_pme.f:47-51
-    if (int rc = pme_run(ctx, ctx->N, S.x, ctx->pme_q(), recip, ctx->volume, ctx->alphal, nullptr, S.e + 24, nullptr,
-                         nullptr, f, dudl ? ctx->d_dq : nullptr, dudl ? S.e + E_DUDL + 3 : nullptr))
-      return rc;
-    if (int rc = md_ferrf(ctx, S, f, energy)) return rc;
-  }
   return ORAC_OK;
 }
+
+// SPME and the erf corrections of the shell that carries the reciprocal
+// term (mts_furier, src/mts_furier.f:71-133), into the same accumulator
+static bool md_has_recip(const orac_gpu_ctx* ctx, const MdState& S, char sh) { return ctx->clewld && S.rshk == sh; }
+
+static int md_shell_recip(orac_gpu_ctx* ctx, MdState& S, char sh, int lvl, bool energy) {
+  if (!md_has_recip(ctx, S, sh)) return ORAC_OK;
+  unsigned long long* f = S.ffix[lvl];
+  const bool dudl = energy && ctx->variant == VAR_ALCH && ctx->d_dq;
+  double recip[9];
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) recip[i + 3 * j] = 0.5 * ctx->oc[j + 3 * i];  // src/fft_pme.f:47-51
+  if (int rc = pme_run(ctx, ctx->N, S.x, ctx->pme_q(), recip, ctx->volume, ctx->alphal, nullptr, S.e + 24, nullptr,
+                       nullptr, f, dudl ? ctx->d_dq : nullptr, dudl ? S.e + E_DUDL + 3 : nullptr))
+    return rc;
+  return md_ferrf(ctx, S, f, energy);
+}
+
+static int md_forces_shell(orac_gpu_ctx* ctx, MdState& S, char sh, int lvl, bool zero, double* e, bool energy) {
+  if (int rc = md_shell_pair(ctx, S, sh, lvl, zero, e, energy)) return rc;
+  return md_shell_recip(ctx, S, sh, lvl, energy);
+}
+
+// Fork and join of the step's second stream; launches between them go to
+// the side stream while the shell pair kernels run on the context's own.
+struct SideStream {
+  orac_gpu_ctx* ctx;
+  MdState& S;
+  int fork() {
+    CK(cudaEventRecord(S.ev_fork, ctx->stream));
+    CK(cudaStreamWaitEvent(S.side, S.ev_fork, 0));
+    return ORAC_OK;
+  }
+  int join() {
+    CK(cudaEventRecord(S.ev_join, S.side));
+    CK(cudaStreamWaitEvent(ctx->stream, S.ev_join, 0));
+    return ORAC_OK;
+  }
+  template <typename F>
+  int run(F&& fn) {  // every launcher uses ctx->stream: point it at the side stream meanwhile
+    cudaStream_t own = ctx->stream;
+    ctx->stream = S.side;
+    const int rc = fn();
+    ctx->stream = own;
+    return rc;
+  }
+};
 
 // mts_intra_n0 / mts_intra_n1 into their level accumulators
 static int md_forces_intra(orac_gpu_ctx* ctx, MdState& S, int lvl, bool energy) {
@@ -1018,6 +1065,7 @@ static int md_step(orac_gpu_ctx* ctx, MdState& S, bool update, bool energy) {
   const int n0 = S.n0respa, n1 = S.n1respa;
   const int per[NLV] = {S.lrespa * S.mrespa * n1 * n0, S.mrespa * n1 * n0, n1 * n0, n0, 1};
   const int K = per[LH];
+  SideStream sd{ctx, S};
   double dt[NLV];
   dt[LH] = S.dth;
   dt[LL] = dt[LH] / S.lrespa;
@@ -1039,20 +1087,47 @@ static int md_step(orac_gpu_ctx* ctx, MdState& S, bool update, bool energy) {
     if (int rc = md_drift(ctx, S, dt[LN0], c, zmask)) return rc;
     const bool last = k == K - 1;
     const bool e_now = energy && last;
-    if (S.has_n0)
-      if (int rc = md_forces_intra(ctx, S, LN0, e_now)) return rc;
-    if (S.has_n1 && (k + 1) % per[LN1] == 0)
-      if (int rc = md_forces_intra(ctx, S, LN1, e_now)) return rc;
-    if ((k + 1) % per[LM] == 0)
-      if (int rc = md_forces_shell(ctx, S, 'm', LM, false, S.e, e_now)) return rc;
-    if ((k + 1) % per[LL] == 0)
-      if (int rc = md_forces_shell(ctx, S, 'l', LL, false, S.e + 8, e_now)) return rc;
+    const bool due_n1 = S.has_n1 && (k + 1) % per[LN1] == 0;
+    const bool due_m = (k + 1) % per[LM] == 0, due_l = (k + 1) % per[LL] == 0;
+    // intramolecular levels and SPME beside the shell pair kernels: each
+    // adds into its own level accumulator (SPME into the pair kernel's, by
+    // exact fixed-point atomics), and all are joined before the next drift
+    const bool side = S.has_n0 || due_n1 || (due_m && md_has_recip(ctx, S, 'm')) ||
+                      (due_l && md_has_recip(ctx, S, 'l'));
+    if (side) {
+      if (int rc = sd.fork()) return rc;
+      if (int rc = sd.run([&]() -> int {
+            if (S.has_n0)
+              if (int r2 = md_forces_intra(ctx, S, LN0, e_now)) return r2;
+            if (due_n1)
+              if (int r2 = md_forces_intra(ctx, S, LN1, e_now)) return r2;
+            if (due_m)
+              if (int r2 = md_shell_recip(ctx, S, 'm', LM, e_now)) return r2;
+            if (due_l)
+              if (int r2 = md_shell_recip(ctx, S, 'l', LL, e_now)) return r2;
+            return ORAC_OK;
+          }))
+        return rc;
+    }
+    if (due_m)
+      if (int rc = md_shell_pair(ctx, S, 'm', LM, false, S.e, e_now)) return rc;
+    if (due_l)
+      if (int rc = md_shell_pair(ctx, S, 'l', LL, false, S.e + 8, e_now)) return rc;
+    if (side)
+      if (int rc = sd.join()) return rc;
   }
-  if (int rc = md_forces_shell(ctx, S, 'h', LH, false, S.e + 16, energy)) return rc;
   {
+    const bool side = md_has_recip(ctx, S, 'h');
+    if (side) {
+      if (int rc = sd.fork()) return rc;
+      if (int rc = sd.run([&]() -> int { return md_shell_recip(ctx, S, 'h', LH, energy); })) return rc;
+    }
+    if (int rc = md_shell_pair(ctx, S, 'h', LH, false, S.e + 16, energy)) return rc;
     ShellRadii r = ctx->sh;
     r.rcutl = r.rcutm;
     if (int rc = md_phony(ctx, r, 'l')) return rc;
+    if (side)
+      if (int rc = sd.join()) return rc;
   }
   {
     double c[NLV];
@@ -1085,6 +1160,9 @@ int orac_gpu_md_setup(orac_gpu_ctx* ctx, const double* x, const double* y, const
   MdState& S = *md_of(ctx);
   const int N = ctx->N, P = ctx->P, G = ctx->G;
   S.N = N;
+  CK(cudaStreamCreateWithFlags(&S.side, cudaStreamNonBlocking));
+  CK(cudaEventCreateWithFlags(&S.ev_fork, cudaEventDisableTiming));
+  CK(cudaEventCreateWithFlags(&S.ev_join, cudaEventDisableTiming));
   if (dev_alloc(ctx, &S.x, 3 * (size_t)N) || dev_alloc(ctx, &S.v, 3 * (size_t)N) ||
       dev_alloc(ctx, &S.xo, 3 * (size_t)N) || dev_alloc(ctx, &S.ffix[0], 3 * (size_t)N) ||
       dev_alloc(ctx, &S.ffix[1], 3 * (size_t)N) || dev_alloc(ctx, &S.ffix[2], 3 * (size_t)N) ||
