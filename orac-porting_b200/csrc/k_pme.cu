@@ -29,10 +29,22 @@ namespace {
 
 constexpr int MAXR = 12;  // max radix stages
 constexpr int FFT_THREADS = 128;
+
+// Division by a constant of the plan: q = umulhi(t, m) with m = 2^32/d + 1
+// is floor(t / d) whenever t * d < 2^32 (here t < 2^20, d <= 4096).  That m
+// does not fit 32 bits for d = 1, which is marked by m = 0.
+inline unsigned magic_of(unsigned d) { return d == 1 ? 0u : (unsigned)((1ull << 32) / d + 1ull); }
+__device__ __forceinline__ int qdiv(int t, unsigned m) { return m ? (int)__umulhi((unsigned)t, m) : t; }
+
 struct FftPlan {
   int n;
   int nst;
   int rad[MAXR];
+  // per stage: butterflies per line, span of the finished sub-transforms,
+  // twiddle stride, and the division constants of the first two
+  int nb[MAXR], ns[MAXR], tsc[MAXR];
+  unsigned mnb[MAXR], mns[MAXR];
+  unsigned mn;  // division by n
 };
 
 int make_plan(int n, FftPlan* p) {
@@ -49,7 +61,19 @@ int make_plan(int n, FftPlan* p) {
       p->rad[p->nst++] = r;
       m /= r;
     }
-  return m == 1 ? 0 : -1;
+  if (m != 1 || n > 4096) return -1;
+  int ns = 1;
+  for (int s = 0; s < p->nst; s++) {
+    const int R = p->rad[s];
+    p->nb[s] = n / R;
+    p->ns[s] = ns;
+    p->tsc[s] = n / (ns * R);
+    p->mnb[s] = magic_of((unsigned)p->nb[s]);
+    p->mns[s] = magic_of((unsigned)ns);
+    ns *= R;
+  }
+  p->mn = magic_of((unsigned)n);
+  return 0;
 }
 
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
@@ -58,60 +82,80 @@ __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
 __device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
 
-// W_n^k for sign -1 (forward) is tw[k]; sign +1 takes the conjugate.
-__device__ __forceinline__ float2 twid(const float2* tw, int n, int k, int sign) {
-  float2 w = tw[k % n];
+// W_n^k for sign -1 (forward) is tw[k] (0 <= k < n); sign +1 takes the
+// conjugate.
+__device__ __forceinline__ float2 twid(const float2* tw, int k, int sign) {
+  float2 w = tw[k];
   if (sign > 0) w.y = -w.y;
   return w;
+}
+
+// One Stockham pass of radix R over nl lines of length n (line-major, a ->
+// b): butterfly t = (line l, index j < n/R) reads a[l][j + r n/R], applies
+// the twiddles W_n^(k r tsc) with k = j mod Ns, and writes the R-point DFT
+// to b[l][(j/Ns) Ns R + k + q Ns].
+template <int R>
+__device__ __forceinline__ void fft_pass(const float2* __restrict__ in, float2* __restrict__ out, int nl, int n,
+                                         const FftPlan& P, int s, const float2* tw, int sign) {
+  const int nb = P.nb[s], Ns = P.ns[s], tsc = P.tsc[s];
+  const unsigned mnb = P.mnb[s], mns = P.mns[s];
+  float2 wr[R];  // W_R^m = W_n^(m nb)
+#pragma unroll
+  for (int m = 0; m < R; m++) wr[m] = twid(tw, m * nb, sign);
+  const int tot = nl * nb;
+  for (int t = threadIdx.x; t < tot; t += blockDim.x) {
+    const int l = qdiv(t, mnb), j = t - l * nb;
+    const int jq = qdiv(j, mns), k = j - jq * Ns;
+    const int tstep = k * tsc;
+    const float2* src = in + l * n + j;
+    float2 v[R];
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+      float2 x = src[r * nb];
+      if (r && tstep) x = cmul(x, twid(tw, tstep * r, sign));
+      v[r] = x;
+    }
+    float2* dst = out + l * n + jq * Ns * R + k;
+    if (R == 2) {
+      dst[0] = cadd(v[0], v[1]);
+      dst[Ns] = csub(v[0], v[1]);
+    } else if (R == 4) {
+      const float2 s02 = cadd(v[0], v[2]), d02 = csub(v[0], v[2]);
+      const float2 s13 = cadd(v[1], v[3]), d13 = csub(v[1], v[3]);
+      // -i*sign(-1) d13 : forward multiplies by -i, inverse by +i
+      const float2 rot = sign < 0 ? make_float2(d13.y, -d13.x) : make_float2(-d13.y, d13.x);
+      dst[0] = cadd(s02, s13);
+      dst[Ns] = cadd(d02, rot);
+      dst[2 * Ns] = csub(s02, s13);
+      dst[3 * Ns] = csub(d02, rot);
+    } else {
+#pragma unroll
+      for (int q = 0; q < R; q++) {
+        float2 acc = v[0];
+#pragma unroll
+        for (int r = 1; r < R; r++) acc = cadd(acc, cmul(v[r], wr[(r * q) % R]));
+        dst[q * Ns] = acc;
+      }
+    }
+  }
 }
 
 // Stockham passes over `nl` lines of length n stored line-major in a; the
 // result ends in the returned buffer (a or b).
 __device__ float2* fft_smem(float2* a, float2* b, int nl, const FftPlan& P, const float2* tw, int sign) {
   const int n = P.n;
-  int Ns = 1;
   for (int s = 0; s < P.nst; s++) {
-    const int R = P.rad[s];
-    const int nb = n / R;
-    const int tot = nl * nb;
-    for (int t = threadIdx.x; t < tot; t += blockDim.x) {
-      const int l = t / nb, j = t - l * nb;
-      const float2* in = a + l * n;
-      float2* out = b + l * n;
-      const int k = j % Ns;
-      const int tstep = k * (n / (Ns * R));
-      float2 v[7];
-      for (int r = 0; r < R; r++) {
-        float2 x = in[j + r * nb];
-        if (r && tstep) x = cmul(x, twid(tw, n, tstep * r, sign));
-        v[r] = x;
-      }
-      const int idxD = (j / Ns) * Ns * R + k;
-      if (R == 2) {
-        out[idxD] = cadd(v[0], v[1]);
-        out[idxD + Ns] = csub(v[0], v[1]);
-      } else if (R == 4) {
-        const float2 s02 = cadd(v[0], v[2]), d02 = csub(v[0], v[2]);
-        const float2 s13 = cadd(v[1], v[3]), d13 = csub(v[1], v[3]);
-        // -i*sign(-1) d13 : forward multiplies by -i, inverse by +i
-        const float2 rot = sign < 0 ? make_float2(d13.y, -d13.x) : make_float2(-d13.y, d13.x);
-        out[idxD] = cadd(s02, s13);
-        out[idxD + Ns] = cadd(d02, rot);
-        out[idxD + 2 * Ns] = csub(s02, s13);
-        out[idxD + 3 * Ns] = csub(d02, rot);
-      } else {
-        for (int q = 0; q < R; q++) {
-          float2 acc = v[0];
-          for (int r = 1; r < R; r++) acc = cadd(acc, cmul(v[r], twid(tw, n, ((r * q) % R) * nb, sign)));
-          out[idxD + q * Ns] = acc;
-        }
-      }
+    switch (P.rad[s]) {
+      case 4: fft_pass<4>(a, b, nl, n, P, s, tw, sign); break;
+      case 2: fft_pass<2>(a, b, nl, n, P, s, tw, sign); break;
+      case 3: fft_pass<3>(a, b, nl, n, P, s, tw, sign); break;
+      case 5: fft_pass<5>(a, b, nl, n, P, s, tw, sign); break;
+      default: fft_pass<7>(a, b, nl, n, P, s, tw, sign); break;
     }
     __syncthreads();
     float2* t = a;
     a = b;
     b = t;
-    Ns *= R;
   }
   return a;
 }
@@ -188,6 +232,7 @@ __global__ void __launch_bounds__(FFT_THREADS) k_fft(const GridArgs A) {
     i0 = (blockIdx.x % nib) * B;
     nl = min(B, A.h1 - i0);
   }
+  const unsigned mnl = nl == 1 ? 0u : (unsigned)((1ull << 32) / (unsigned)nl + 1ull);  // division by nl
   // ---- load
   if (MODE == XF) {
     const size_t g0 = (size_t)j0 * A.n1;
@@ -199,7 +244,7 @@ __global__ void __launch_bounds__(FFT_THREADS) k_fft(const GridArgs A) {
     // Hermitian extension of the half line (c2r)
     const int h1 = A.h1;
     for (int e = threadIdx.x; e < nl * n; e += blockDim.x) {
-      const int l = e / n, i = e - l * n;
+      const int l = qdiv(e, A.P.mn), i = e - l * n;
       const size_t row = (size_t)(j0 + l) * h1;
       float2 v;
       if (i < h1) {
@@ -212,12 +257,12 @@ __global__ void __launch_bounds__(FFT_THREADS) k_fft(const GridArgs A) {
     }
   } else if (MODE == YF || MODE == YI) {
     for (int e = threadIdx.x; e < nl * n; e += blockDim.x) {
-      const int pos = e / nl, l = e - pos * nl;
+      const int pos = qdiv(e, mnl), l = e - pos * nl;
       a[l * n + pos] = A.cg[((size_t)k0 * A.n2 + pos) * A.h1 + i0 + l];
     }
   } else {
     for (int e = threadIdx.x; e < nl * n; e += blockDim.x) {
-      const int pos = e / nl, l = e - pos * nl;
+      const int pos = qdiv(e, mnl), l = e - pos * nl;
       a[l * n + pos] = A.cg[((size_t)pos * A.n2 + j0) * A.h1 + i0 + l];
     }
   }
@@ -235,7 +280,7 @@ __global__ void __launch_bounds__(FFT_THREADS) k_fft(const GridArgs A) {
     int nf3 = A.n3 / 2;
     if (2 * nf3 < A.n3) nf3++;
     for (int e = threadIdx.x; e < nl * n; e += blockDim.x) {
-      const int l = e / n, kk = e - l * n;
+      const int l = qdiv(e, A.P.mn), kk = e - l * n;
       const int k1 = i0 + l + 1, k2 = j0 + 1, k3 = kk + 1;
       if (k1 == 1 && k2 == 1 && k3 == 1) continue;
       const int m1 = k1 > nf1 ? k1 - 1 - A.n1 : k1 - 1;
@@ -299,12 +344,12 @@ __global__ void __launch_bounds__(FFT_THREADS) k_fft(const GridArgs A) {
     for (int e = threadIdx.x; e < nl * n; e += blockDim.x) A.rg[g0 + e] = res[e].x;
   } else if (MODE == YF || MODE == YI) {
     for (int e = threadIdx.x; e < nl * n; e += blockDim.x) {
-      const int pos = e / nl, l = e - pos * nl;
+      const int pos = qdiv(e, mnl), l = e - pos * nl;
       A.cg[((size_t)k0 * A.n2 + pos) * A.h1 + i0 + l] = res[l * n + pos];
     }
   } else {
     for (int e = threadIdx.x; e < nl * n; e += blockDim.x) {
-      const int pos = e / nl, l = e - pos * nl;
+      const int pos = qdiv(e, mnl), l = e - pos * nl;
       A.cg[((size_t)pos * A.n2 + j0) * A.h1 + i0 + l] = res[l * n + pos];
     }
   }
