@@ -697,36 +697,38 @@ int pair_launch(orac_gpu_ctx* ctx, const PairArgs& a, int maxg) {
   if (maxg > ORAC_MAXG)
     return ctx_fail(ctx, ORAC_ERR_PARAM, "charge group of %d atoms exceeds %d", maxg, ORAC_MAXG);
   if (a.variant < VAR_STD || a.variant > VAR_ALCH) return ctx_fail(ctx, ORAC_ERR_PARAM, "variant %d", a.variant);
-  const bool small = maxg <= 4;
-  const bool half = small && a.lpg == 16;
+  // atoms-per-group bound of the instantiation: 3 (waters, and chains cut
+  // in threes), 4, or 8; half-warp groups only for the two small bounds
+  const int mgk = maxg <= 3 ? 0 : (maxg <= 4 ? 1 : 2);
+  const bool half = mgk < 2 && a.lpg == 16;
   const int gpb = WPB * (half ? 2 : 1);  // groups per block
   int nb = (a.ngrp + gpb - 1) / gpb;
   if (nb < 1) nb = 1;
   int slot = -1;
   if (int rc = prof_begin(ctx, &slot)) return rc;
-  switch (a.variant * 4 + (small ? 0 : 2) + (a.energy ? 1 : 0) + (half ? 12 : 0)) {
-#define ORAC_KP(code, MG, EN, VAR, LPG) \
-  case code:                            \
-    k_pair<MG, EN, VAR, LPG><<<nb, WPB * 32, smem, ctx->stream>>>(a); \
+  switch (((mgk * 3 + a.variant) * 2 + (a.energy ? 1 : 0)) * 2 + (half ? 1 : 0)) {
+#define ORAC_KP(MGK, MG, VAR, EN, LPG)                                             \
+  case ((MGK * 3 + VAR) * 2 + (EN ? 1 : 0)) * 2 + (LPG == 16 ? 1 : 0):             \
+    k_pair<MG, EN, VAR, LPG><<<nb, WPB * 32, smem, ctx->stream>>>(a);              \
     break;
-    ORAC_KP(0, 4, false, VAR_STD, 32)
-    ORAC_KP(1, 4, true, VAR_STD, 32)
-    ORAC_KP(2, 8, false, VAR_STD, 32)
-    ORAC_KP(3, 8, true, VAR_STD, 32)
-    ORAC_KP(4, 4, false, VAR_REM, 32)
-    ORAC_KP(5, 4, true, VAR_REM, 32)
-    ORAC_KP(6, 8, false, VAR_REM, 32)
-    ORAC_KP(7, 8, true, VAR_REM, 32)
-    ORAC_KP(8, 4, false, VAR_ALCH, 32)
-    ORAC_KP(9, 4, true, VAR_ALCH, 32)
-    ORAC_KP(10, 8, false, VAR_ALCH, 32)
-    ORAC_KP(11, 8, true, VAR_ALCH, 32)
-    ORAC_KP(12, 4, false, VAR_STD, 16)
-    ORAC_KP(13, 4, true, VAR_STD, 16)
-    ORAC_KP(16, 4, false, VAR_REM, 16)
-    ORAC_KP(17, 4, true, VAR_REM, 16)
-    ORAC_KP(20, 4, false, VAR_ALCH, 16)
-    ORAC_KP(21, 4, true, VAR_ALCH, 16)
+#define ORAC_KP_V(MGK, MG, VAR)                                                    \
+  ORAC_KP(MGK, MG, VAR, false, 32)                                                 \
+  ORAC_KP(MGK, MG, VAR, true, 32)                                                  \
+  ORAC_KP(MGK, MG, VAR, false, 16)                                                 \
+  ORAC_KP(MGK, MG, VAR, true, 16)
+    ORAC_KP_V(0, 3, VAR_STD)
+    ORAC_KP_V(0, 3, VAR_REM)
+    ORAC_KP_V(0, 3, VAR_ALCH)
+    ORAC_KP_V(1, 4, VAR_STD)
+    ORAC_KP_V(1, 4, VAR_REM)
+    ORAC_KP_V(1, 4, VAR_ALCH)
+    ORAC_KP(2, 8, VAR_STD, false, 32)
+    ORAC_KP(2, 8, VAR_STD, true, 32)
+    ORAC_KP(2, 8, VAR_REM, false, 32)
+    ORAC_KP(2, 8, VAR_REM, true, 32)
+    ORAC_KP(2, 8, VAR_ALCH, false, 32)
+    ORAC_KP(2, 8, VAR_ALCH, true, 32)
+#undef ORAC_KP_V
 #undef ORAC_KP
   }
   CKL();
