@@ -395,6 +395,8 @@ int orac_gpu_set_topology(orac_gpu_ctx* ctx, int ntap, int ngrp, int nprot, cons
   }
   ctx->h_amol = amol;
   ctx->h_gmol = gmol;
+  ctx->h_intra_b.clear();  // bonded terms of an earlier topology no longer apply
+  ctx->h_intra_p.clear();
   ctx->h_charge.assign(chrge, chrge + N);
   ctx->h_mass.assign(mass, mass + N);
   ctx->h_ss.assign(ss_index, ss_index + N);

@@ -110,6 +110,16 @@ int orac_gpu_set_bonded(orac_gpu_ctx* ctx, int nb, const int* lbnd, const double
   if (int rc = check_atoms(ctx, ltor, nt, 4, "ltor")) return rc;
   if (int rc = check_atoms(ctx, litr, nit, 4, "litr")) return rc;
   BondedDev& B = ctx->bd;
+  // intramolecular-level membership of the atoms (k_drift skips the N0/N1
+  // accumulators of small molecules with none)
+  ctx->h_intra_b.assign(ctx->N, 0);
+  auto mark = [&](const int* l, int n, int w, unsigned char bit) {
+    for (int k = 0; k < n * w; k++) ctx->h_intra_b[l[k] - 1] |= bit;
+  };
+  mark(lbnd, nb, 2, 1);
+  mark(lbndg, nbend, 3, 1);
+  mark(litr, nit, 4, 1);
+  mark(ltor, nt, 4, 2);
   std::vector<int2> bij(nb);
   std::vector<double2> bpar(nb);
   for (int k = 0; k < nb; k++) {
@@ -154,6 +164,9 @@ int orac_gpu_set_intra_pairs(orac_gpu_ctx* ctx, int n14, const int* int14, const
   for (int k = 0; k < n14; k++)
     if (type14[k] < 1 || type14[k] > ntab14) return ctx_fail(ctx, ORAC_ERR_PARAM, "type14 %d", type14[k]);
   BondedDev& B = ctx->bd;
+  ctx->h_intra_p.assign(ctx->N, 0);
+  for (int k = 0; k < 2 * n14; k++) ctx->h_intra_p[int14[k] - 1] |= 2;
+  for (int k = 0; k < 2 * ningrp; k++) ctx->h_intra_p[ingrp[k] - 1] |= 2;
   std::vector<int> t14(type14, type14 + n14);
   std::vector<double> e12(ecc1412, ecc1412 + ntab14), e6(ecc146, ecc146 + ntab14);
   std::vector<double> l12(ctx->h_ecc12), l6(ctx->h_ecc6);

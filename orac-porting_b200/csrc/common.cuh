@@ -223,6 +223,10 @@ struct orac_gpu_ctx {
 
   // host copies needed by the drivers
   std::vector<int> h_gfirst, h_gn, h_amol, h_gmol;
+  // atoms in a term of the intramolecular levels, bit 0 N0, bit 1 N1:
+  // h_intra_b from set_bonded (bonds, bends, impropers at N0; torsions at
+  // N1), h_intra_p from set_intra_pairs (1-4 and intra-group pairs at N1)
+  std::vector<unsigned char> h_intra_b, h_intra_p;
   std::vector<double> h_charge, h_mass;
   std::vector<int> h_ss, h_nbtype;
   std::vector<double> h_ecc12, h_ecc6;

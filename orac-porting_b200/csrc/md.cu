@@ -40,6 +40,7 @@ namespace {
 constexpr int SMA = 4;  // atoms of a register-solved molecule
 constexpr int SMC = 3;  // constraints of a register-solved molecule
 constexpr int NLV = 5;  // r-RESPA force levels: H, L, M, N1, N0
+enum { LH = 0, LL = 1, LM = 2, LN1 = 3, LN0 = 4 };
 
 __device__ __forceinline__ double dot3(const double* a, const double* b) {
   return a[0] * b[0] + a[1] * b[1] + a[2] * b[2];
@@ -92,6 +93,14 @@ struct MolArgs {
   const int* free_atoms;
   int nfreeg;
   const int* free_groups;
+  // the drift's split of the free atoms: groups of unconstrained molecules
+  // (one thread drifts the group's atoms and sets its centre) and atoms of
+  // large constrained molecules (one thread each; their groups follow the
+  // iterative SHAKE in k_free_groups)
+  int ndg;
+  const int* drift_groups;
+  int nda;
+  const int* drift_atoms;
   // state
   double* x;
   double* xo;
@@ -316,6 +325,8 @@ __device__ __forceinline__ bool shake_small(double x[SMA][3], const double xo[SM
 // in closed form (adjugate over determinant).  MOL3 in the molecule record
 // marks them.
 constexpr int MOL3 = 256;
+// a small molecule none of whose atoms has an intramolecular-level term
+constexpr int NOINTRA = 512;
 
 __device__ __forceinline__ bool solve3x3(const double J[3][3], const double g[3], double out[3]) {
   const double c00 = J[1][1] * J[2][2] - J[1][2] * J[2][1];
@@ -420,12 +431,63 @@ __device__ __forceinline__ bool shake3(double x[SMA][3], const double xo[SMA][3]
   return ok;
 }
 
-__device__ __forceinline__ double kick_dv(const MolArgs& A, int i) {
+// levels 0..nlev-1 (molecules without intramolecular terms have nothing at
+// the N1 and N0 levels: nlev = 3)
+__device__ __forceinline__ double kick_dv(const MolArgs& A, int i, int nlev = NLV) {
   double dv = 0.0;
 #pragma unroll
   for (int l = 0; l < NLV; l++)
-    if (A.ck[l] != 0.0) dv += A.ck[l] * fixd(A.fk[l][i]);
+    if (l < nlev && A.ck[l] != 0.0) dv += A.ck[l] * fixd(A.fk[l][i]);
   return dv;
+}
+
+// free atom i (SoA component index d*N + g): kick, verlet half kick of the N0
+// force and drift, zeroing of the level accumulators that restart here
+__device__ __forceinline__ void drift_atom(const MolArgs& A, int g, double dt) {
+  const int N = A.N;
+  const double im = A.invm[g];
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    const int i = d * N + g;
+    const double f = A.fv ? fixd(A.fv[i]) : 0.0;
+    double v = A.v[i];
+    if (A.kick) v += kick_dv(A, i) * im;
+    const double xo = A.x[i];
+    A.xo[i] = xo;
+    A.x[i] = xo + dt * v + f * 0.5 * dt * dt * im;
+    A.v[i] = v + f * 0.5 * dt * im;
+#pragma unroll
+    for (int l = 0; l < NLV; l++)
+      if (A.fz[l]) A.fz[l][i] = 0ull;
+  }
+}
+
+// scaled centre of group gi from its atoms' positions and the pair-kernel
+// inputs of its atoms (appbou, src/appbou.f:57-69)
+__device__ __forceinline__ void group_centre(const MolArgs& A, int gi) {
+  const int N = A.N;
+  const int2 mg = A.gmeta[gi];
+  const int a0 = mg.x, n = mg.y & 0xff;
+  double c[3] = {0, 0, 0};
+  for (int a = a0; a < a0 + n; a++) {
+    const double x = A.x[a], y = A.x[N + a], z = A.x[2 * N + a];
+    const double w = A.pm[a];
+    c[0] += w * (A.o11 * x + A.o12 * y + A.o13 * z);
+    c[1] += w * (A.o22 * y + A.o23 * z);
+    c[2] += w * (A.o33 * z);
+  }
+  A.grp[gi] = c[0];
+  A.grp[A.G + gi] = c[1];
+  A.grp[2 * A.G + gi] = c[2];
+  A.gpos[gi] = make_double4(c[0], c[1], c[2], 0.0);
+  for (int a = a0; a < a0 + n; a++) {
+    const double x = A.x[a], y = A.x[N + a], z = A.x[2 * N + a];
+    const double dx = (A.o11 * x + A.o12 * y + A.o13 * z) - c[0];
+    const double dy = (A.o22 * y + A.o23 * z) - c[1];
+    const double dz = (A.o33 * z) - c[2];
+    A.aoff[a] = make_float4((float)(A.c11 * dx + A.c12 * dy + A.c13 * dz), (float)(A.c22 * dy + A.c23 * dz),
+                            (float)(A.c33 * dz), A.q[a]);
+  }
 }
 
 // correc (v += f dt/2m) from the fixed-point level accumulators, then RATTLE.
@@ -444,9 +506,10 @@ __global__ void k_kick(const MolArgs A) {
         x[a][0] = A.x[g];
         x[a][1] = A.x[N + g];
         x[a][2] = A.x[2 * N + g];
-        v[a][0] = A.v[g] + kick_dv(A, g) * im[a];
-        v[a][1] = A.v[N + g] + kick_dv(A, N + g) * im[a];
-        v[a][2] = A.v[2 * N + g] + kick_dv(A, 2 * N + g) * im[a];
+        const int nlev = (m.w & NOINTRA) ? LN1 : NLV;
+        v[a][0] = A.v[g] + kick_dv(A, g, nlev) * im[a];
+        v[a][1] = A.v[N + g] + kick_dv(A, N + g, nlev) * im[a];
+        v[a][2] = A.v[2 * N + g] + kick_dv(A, 2 * N + g, nlev) * im[a];
       } else {
         im[a] = 0;
         x[a][0] = x[a][1] = x[a][2] = 0;
@@ -483,6 +546,7 @@ __global__ void k_drift(const MolArgs A) {
   if (t < A.nsm) {
     const int4 m = A.sm[t];
     double x[SMA][3], xo[SMA][3], v[SMA][3], im[SMA];
+    const int nlev = (m.w & NOINTRA) ? LN1 : NLV;
 #pragma unroll
     for (int a = 0; a < SMA; a++) {
       if (a < m.y) {
@@ -492,7 +556,7 @@ __global__ void k_drift(const MolArgs A) {
         for (int d = 0; d < 3; d++) {
           xo[a][d] = A.x[d * N + g];
           v[a][d] = A.v[d * N + g];
-          if (A.kick) v[a][d] += kick_dv(A, d * N + g) * im[a];
+          if (A.kick) v[a][d] += kick_dv(A, d * N + g, nlev) * im[a];
         }
       } else {
         im[a] = 0;
@@ -510,7 +574,7 @@ __global__ void k_drift(const MolArgs A) {
         const int g = m.x + a;
 #pragma unroll
         for (int d = 0; d < 3; d++) {
-          const double f = A.fv ? fixd(A.fv[d * N + g]) : 0.0;
+          const double f = (A.fv && nlev == NLV) ? fixd(A.fv[d * N + g]) : 0.0;
           x[a][d] = xo[a][d] + dt * v[a][d] + f * 0.5 * dt * dt * im[a];
           v[a][d] += f * 0.5 * dt * im[a];
         }
@@ -535,7 +599,7 @@ __global__ void k_drift(const MolArgs A) {
           A.v[d * N + g] = v[a][d];
 #pragma unroll
           for (int l = 0; l < NLV; l++)
-            if (A.fz[l]) A.fz[l][d * N + g] = 0ull;
+            if (l < nlev && A.fz[l]) A.fz[l][d * N + g] = 0ull;
         }
         s[a][0] = A.o11 * x[a][0] + A.o12 * x[a][1] + A.o13 * x[a][2];
         s[a][1] = A.o22 * x[a][1] + A.o23 * x[a][2];
@@ -570,54 +634,23 @@ __global__ void k_drift(const MolArgs A) {
         }
       }
     }
-  } else if (t < A.nsm + A.nfree) {
-    const int g = A.free_atoms[t - A.nsm];
-    const double im = A.invm[g];
-#pragma unroll
-    for (int d = 0; d < 3; d++) {
-      const int i = d * N + g;
-      const double f = A.fv ? fixd(A.fv[i]) : 0.0;
-      double v = A.v[i];
-      if (A.kick) v += kick_dv(A, i) * im;
-      const double xo = A.x[i];
-      A.xo[i] = xo;
-      A.x[i] = xo + dt * v + f * 0.5 * dt * dt * im;
-      A.v[i] = v + f * 0.5 * dt * im;
-#pragma unroll
-      for (int l = 0; l < NLV; l++)
-        if (A.fz[l]) A.fz[l][i] = 0ull;
-    }
+  } else if (t < A.nsm + A.ndg) {
+    // a group of an unconstrained molecule: its atoms, then its centre
+    const int gi = A.drift_groups[t - A.nsm];
+    const int2 mg = A.gmeta[gi];
+    for (int a = mg.x; a < mg.x + (mg.y & 0xff); a++) drift_atom(A, a, dt);
+    group_centre(A, gi);
+  } else if (t < A.nsm + A.ndg + A.nda) {
+    drift_atom(A, A.drift_atoms[t - A.nsm - A.ndg], dt);
   }
 }
 
-// group centres and pair-kernel inputs of groups outside small molecules
+// group centres and pair-kernel inputs of the groups of large constrained
+// molecules, after their iterative SHAKE
 __global__ void k_free_groups(const MolArgs A) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= A.nfreeg) return;
-  const int gi = A.free_groups[t];
-  const int N = A.N;
-  const int2 mg = A.gmeta[gi];
-  const int a0 = mg.x, n = mg.y & 0xff;
-  double c[3] = {0, 0, 0};
-  for (int a = a0; a < a0 + n; a++) {
-    const double x = A.x[a], y = A.x[N + a], z = A.x[2 * N + a];
-    const double w = A.pm[a];
-    c[0] += w * (A.o11 * x + A.o12 * y + A.o13 * z);
-    c[1] += w * (A.o22 * y + A.o23 * z);
-    c[2] += w * (A.o33 * z);
-  }
-  A.grp[gi] = c[0];
-  A.grp[A.G + gi] = c[1];
-  A.grp[2 * A.G + gi] = c[2];
-  A.gpos[gi] = make_double4(c[0], c[1], c[2], 0.0);
-  for (int a = a0; a < a0 + n; a++) {
-    const double x = A.x[a], y = A.x[N + a], z = A.x[2 * N + a];
-    const double dx = (A.o11 * x + A.o12 * y + A.o13 * z) - c[0];
-    const double dy = (A.o22 * y + A.o23 * z) - c[1];
-    const double dz = (A.o33 * z) - c[2];
-    A.aoff[a] = make_float4((float)(A.c11 * dx + A.c12 * dy + A.c13 * dz), (float)(A.c22 * dy + A.c23 * dz),
-                            (float)(A.c33 * dz), A.q[a]);
-  }
+  group_centre(A, A.free_groups[t]);
 }
 
 struct ConsArgs {
@@ -740,10 +773,14 @@ struct MdState {
   int2* smg = nullptr;
   int2* cloc = nullptr;
   double* cdss = nullptr;
-  // free atoms and groups
-  int nfree = 0, nfreeg = 0;
+  // free atoms and groups: all atoms outside small molecules (k_kick), the
+  // drift's groups of unconstrained molecules and atoms of large constrained
+  // ones, and the groups of the latter (k_free_groups)
+  int nfree = 0, nfreeg = 0, ndg = 0, nda = 0;
   int* free_atoms = nullptr;
   int* free_groups = nullptr;
+  int* drift_groups = nullptr;
+  int* drift_atoms = nullptr;
   // large constrained molecules
   int nbig = 0;
   int* bstart = nullptr;
@@ -794,7 +831,8 @@ void md_destroy(orac_gpu_ctx* ctx) {
   void* ptrs[] = {S->x,         S->v,        S->xo,          S->ffix[0],   S->ffix[1], S->ffix[2], S->ffix[3],
                   S->ffix[4],
                   S->invm,      S->pm,       S->sm,          S->smg,       S->cloc,    S->cdss,    S->free_atoms,
-                  S->free_groups, S->bstart, S->bcab,        S->bdss,      S->e,       S->flag};
+                  S->free_groups, S->bstart, S->bcab,        S->bdss,      S->e,       S->flag,
+                  S->drift_groups, S->drift_atoms};
   for (void* p : ptrs)
     if (p) dev_free(ctx, p);
   delete S;
@@ -814,6 +852,10 @@ static MolArgs mol_args(orac_gpu_ctx* ctx, MdState& S, double dt) {
   A.free_atoms = S.free_atoms;
   A.nfreeg = S.nfreeg;
   A.free_groups = S.free_groups;
+  A.ndg = S.ndg;
+  A.drift_groups = S.drift_groups;
+  A.nda = S.nda;
+  A.drift_atoms = S.drift_atoms;
   A.x = S.x;
   A.xo = S.xo;
   A.v = S.v;
@@ -863,7 +905,6 @@ static ConsArgs big_args(orac_gpu_ctx* ctx, MdState& S, double dt, double tol) {
   return A;
 }
 
-enum { LH = 0, LL = 1, LM = 2, LN1 = 3, LN0 = 4 };
 enum { E_BOND = 41, E_14 = 49, E_GRP = 53, E_ERF = 57, E_DUDL = 73, E_N = 80 };
 
 // kick of the level accumulators with velocity factors c[l] (0: skip) + RATTLE
@@ -903,7 +944,7 @@ static int md_drift(orac_gpu_ctx* ctx, MdState& S, double dt, const double* c, i
   kick_fill(A, S, c);
   A.fv = S.has_n0 ? S.ffix[LN0] : nullptr;
   for (int l = 0; l < NLV; l++) A.fz[l] = ((zmask >> l) & 1) ? S.ffix[l] : nullptr;
-  const int n = S.nsm + S.nfree;
+  const int n = S.nsm + S.ndg + S.nda;
   k_drift<<<(n + 31) / 32, 32, 0, ctx->stream>>>(A);
   CKL();
   if (S.nbig) {
@@ -1256,13 +1297,31 @@ int orac_gpu_md_setup(orac_gpu_ctx* ctx, const double* x, const double* y, const
       bst.push_back((int)bcab.size());
     }
   }
+  // molecules outside the small ones: unconstrained (drifted by group) or
+  // large constrained (drifted by atom, centred after their SHAKE)
+  std::vector<int> dg, da;
   for (int a = 0; a < N; a++)
-    if (!small[ctx->h_amol[a]]) fa.push_back(a);
+    if (!small[ctx->h_amol[a]]) {
+      fa.push_back(a);
+      if (!bym[ctx->h_amol[a]].empty()) da.push_back(a);
+    }
   for (int g = 0; g < G; g++)
-    if (!small[ctx->h_gmol[g]]) fg.push_back(g);
+    if (!small[ctx->h_gmol[g]]) (bym[ctx->h_gmol[g]].empty() ? dg : fg).push_back(g);
+  // small molecules without intramolecular-level terms skip the N1 and N0
+  // accumulators, which stay zero for their atoms
+  {
+    const bool hb = (int)ctx->h_intra_b.size() == N, hp = (int)ctx->h_intra_p.size() == N;
+    for (auto& m : sm) {
+      bool any = false;
+      for (int a = m.x; a < m.x + m.y; a++) any = any || (hb && ctx->h_intra_b[a]) || (hp && ctx->h_intra_p[a]);
+      if (!any) m.w |= NOINTRA;
+    }
+  }
   S.nsm = (int)sm.size();
   S.nfree = (int)fa.size();
   S.nfreeg = (int)fg.size();
+  S.ndg = (int)dg.size();
+  S.nda = (int)da.size();
   S.nbig = (int)bst.size() - 1;
 #define UPV(dst, vec)                                                                                        \
   if (!vec.empty()) {                                                                                        \
@@ -1275,6 +1334,8 @@ int orac_gpu_md_setup(orac_gpu_ctx* ctx, const double* x, const double* y, const
   UPV(S.cdss, cd);
   UPV(S.free_atoms, fa);
   UPV(S.free_groups, fg);
+  UPV(S.drift_groups, dg);
+  UPV(S.drift_atoms, da);
   if (S.nbig) {
     UPV(S.bstart, bst);
     UPV(S.bcab, bcab);
