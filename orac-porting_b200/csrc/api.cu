@@ -197,6 +197,7 @@ int shell_run_r(orac_gpu_ctx* ctx, char rshell, const ShellRadii& radii, const d
   variant_fill(ctx, &a);
   // the innermost shell's rows hold about a dozen groups: half a warp each
   a.lpg = rshell == 'm' ? kpair_lpg_inner() : 32;
+  a.occ_hi = ctx->shared_device ? 1 : 0;
   const bool want_e = (flags & SH_ENERGY) && d_e, want_s = (flags & SH_STRESS) && d_stress;
   a.energy = want_e ? 1 : 0;
   a.stress = want_s ? 1 : 0;

@@ -78,6 +78,9 @@ int orac_gpu_batch_create(orac_gpu_ctx** ctxs, int n, orac_gpu_batch** out) {
     return ORAC_ERR_CUDA;
   }
   *out = b;
+  // many systems share the device: their pair kernels take the
+  // higher-occupancy build (the step graphs are captured again for it)
+  for (auto* c : b->ctx) c->shared_device = n > 1;
   // instantiate both step kinds now when every system is set up, so that no
   // step of a run pays for it
   bool ready = true;
@@ -99,6 +102,7 @@ int orac_gpu_batch_destroy(orac_gpu_batch* b) {
     if (b->graph[k]) cudaGraphDestroy(b->graph[k]);
   }
   if (b->stream) cudaStreamDestroy(b->stream);
+  for (auto* c : b->ctx) c->shared_device = false;
   delete b;
   return ORAC_OK;
 }

@@ -116,6 +116,9 @@ struct PairArgs {
   // lanes that own one i group: 32, or 16 (two groups per warp) for lists
   // with short rows; 16 applies to groups of at most 4 atoms
   int lpg;
+  // the context runs beside others (batch, server): the forces-only kernel
+  // takes its higher-occupancy build (fewer registers, more warps per SM)
+  int occ_hi;
   // variant (VAR_*); REM: seg_select kind and rem_factor(3)
   int variant;
   const unsigned char* vflag;  // [N]
@@ -209,6 +212,7 @@ struct MdState;  // md.cu
 
 struct orac_gpu_ctx {
   MdState* md = nullptr;
+  bool shared_device = false;  // advanced beside other contexts (batch, server)
   std::unordered_map<void*, size_t> dmem;  // live device allocations
   size_t dmem_bytes = 0;
   int device = 0;

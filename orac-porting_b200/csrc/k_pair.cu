@@ -168,12 +168,20 @@ __device__ __forceinline__ void alch_energy_fp64(const PairArgs& A, double rx, d
 #ifndef ORAC_KPAIR_MINB32
 #define ORAC_KPAIR_MINB32 6  // the same for the warp-per-group (compacting) forces-only kernel
 #endif
+#ifndef ORAC_KPAIR_MINB_HI
+#define ORAC_KPAIR_MINB_HI 8  // both, for contexts that share the device with others
+#endif
 
 // LPG lanes own one i-group: 32 (a warp) for the long rows of the L and H
 // lists, 16 (a half warp, two groups per warp) for the short rows of the M
 // list, where a full warp would leave most lanes idle.
-template <int MG, bool EN, int VAR, int LPG>
-__global__ void __launch_bounds__(WPB * 32, (MG <= 4 && !EN) ? (LPG == 16 ? ORAC_KPAIR_MINB : ORAC_KPAIR_MINB32) : 1)
+// HI: the build for contexts sharing the device, where throughput over many
+// concurrent kernels matters more than one launch's latency.
+template <int MG, bool EN, int VAR, int LPG, bool HI>
+__global__ void __launch_bounds__(WPB * 32, (MG <= 4 && !EN)
+                                                ? (HI ? ORAC_KPAIR_MINB_HI
+                                                      : (LPG == 16 ? ORAC_KPAIR_MINB : ORAC_KPAIR_MINB32))
+                                                : 1)
     k_pair(const PairArgs A) {
   constexpr int SEG = 32 / LPG;  // groups per warp
   // long rows (a warp per group): in-band entries are compacted through a
@@ -706,28 +714,31 @@ int pair_launch(orac_gpu_ctx* ctx, const PairArgs& a, int maxg) {
   if (nb < 1) nb = 1;
   int slot = -1;
   if (int rc = prof_begin(ctx, &slot)) return rc;
-  switch (((mgk * 3 + a.variant) * 2 + (a.energy ? 1 : 0)) * 2 + (half ? 1 : 0)) {
-#define ORAC_KP(MGK, MG, VAR, EN, LPG)                                             \
-  case ((MGK * 3 + VAR) * 2 + (EN ? 1 : 0)) * 2 + (LPG == 16 ? 1 : 0):             \
-    k_pair<MG, EN, VAR, LPG><<<nb, WPB * 32, smem, ctx->stream>>>(a);              \
+  const bool hi = a.occ_hi && !a.energy && mgk < 2;
+  switch ((((mgk * 3 + a.variant) * 2 + (a.energy ? 1 : 0)) * 2 + (half ? 1 : 0)) * 2 + (hi ? 1 : 0)) {
+#define ORAC_KP(MGK, MG, VAR, EN, LPG, HI)                                                     \
+  case (((MGK * 3 + VAR) * 2 + (EN ? 1 : 0)) * 2 + (LPG == 16 ? 1 : 0)) * 2 + (HI ? 1 : 0):     \
+    k_pair<MG, EN, VAR, LPG, HI><<<nb, WPB * 32, smem, ctx->stream>>>(a);                      \
     break;
-#define ORAC_KP_V(MGK, MG, VAR)                                                    \
-  ORAC_KP(MGK, MG, VAR, false, 32)                                                 \
-  ORAC_KP(MGK, MG, VAR, true, 32)                                                  \
-  ORAC_KP(MGK, MG, VAR, false, 16)                                                 \
-  ORAC_KP(MGK, MG, VAR, true, 16)
+#define ORAC_KP_V(MGK, MG, VAR)                                                                \
+  ORAC_KP(MGK, MG, VAR, false, 32, false)                                                      \
+  ORAC_KP(MGK, MG, VAR, false, 32, true)                                                       \
+  ORAC_KP(MGK, MG, VAR, true, 32, false)                                                       \
+  ORAC_KP(MGK, MG, VAR, false, 16, false)                                                      \
+  ORAC_KP(MGK, MG, VAR, false, 16, true)                                                       \
+  ORAC_KP(MGK, MG, VAR, true, 16, false)
     ORAC_KP_V(0, 3, VAR_STD)
     ORAC_KP_V(0, 3, VAR_REM)
     ORAC_KP_V(0, 3, VAR_ALCH)
     ORAC_KP_V(1, 4, VAR_STD)
     ORAC_KP_V(1, 4, VAR_REM)
     ORAC_KP_V(1, 4, VAR_ALCH)
-    ORAC_KP(2, 8, VAR_STD, false, 32)
-    ORAC_KP(2, 8, VAR_STD, true, 32)
-    ORAC_KP(2, 8, VAR_REM, false, 32)
-    ORAC_KP(2, 8, VAR_REM, true, 32)
-    ORAC_KP(2, 8, VAR_ALCH, false, 32)
-    ORAC_KP(2, 8, VAR_ALCH, true, 32)
+    ORAC_KP(2, 8, VAR_STD, false, 32, false)
+    ORAC_KP(2, 8, VAR_STD, true, 32, false)
+    ORAC_KP(2, 8, VAR_REM, false, 32, false)
+    ORAC_KP(2, 8, VAR_REM, true, 32, false)
+    ORAC_KP(2, 8, VAR_ALCH, false, 32, false)
+    ORAC_KP(2, 8, VAR_ALCH, true, 32, false)
 #undef ORAC_KP_V
 #undef ORAC_KP
   }

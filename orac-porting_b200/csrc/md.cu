@@ -801,6 +801,7 @@ struct MdState {
   cudaGraphExec_t gexec = nullptr;
   cudaGraph_t graph_u = nullptr;  // step with list update
   cudaGraphExec_t gexec_u = nullptr;
+  bool graphs_shared = false;  // ctx->shared_device when the graphs were captured
   bool use_graph = true;
   int pslot[2][2] = {{0, 0}, {0, 0}};  // profiling event slots of each graph
   int64_t kpg[2] = {0, 0};             // kernels per captured graph
@@ -1466,6 +1467,16 @@ int orac_gpu_md_set_graphs(orac_gpu_ctx* ctx, int on) {
 
 // capture (once) the step graph of one kind: 0 plain step, 1 step with list update
 static int md_capture(orac_gpu_ctx* ctx, MdState& S, int kind) {
+  if ((S.gexec || S.gexec_u) && S.graphs_shared != ctx->shared_device) {
+    // captured for the other device-sharing mode: capture again
+    if (S.gexec) cudaGraphExecDestroy(S.gexec);
+    if (S.graph) cudaGraphDestroy(S.graph);
+    if (S.gexec_u) cudaGraphExecDestroy(S.gexec_u);
+    if (S.graph_u) cudaGraphDestroy(S.graph_u);
+    S.gexec = S.gexec_u = nullptr;
+    S.graph = S.graph_u = nullptr;
+  }
+  S.graphs_shared = ctx->shared_device;
   cudaGraphExec_t* ge = kind ? &S.gexec_u : &S.gexec;
   cudaGraph_t* gg = kind ? &S.graph_u : &S.graph;
   if (*ge) return ORAC_OK;

@@ -215,7 +215,8 @@ int orac_gpu_server_submit(orac_gpu_server* s, orac_gpu_ctx* ctx, int nsteps, in
   if (!s || !ctx || nsteps < 1 || !ticket) return ORAC_ERR_PARAM;
   if (ctx->device != s->device) return sfail(s, ORAC_ERR_PARAM, "context on another device");
   // capture both step graphs here, in the caller's thread, so the pump only
-  // launches
+  // launches; served contexts share the device with each other
+  ctx->shared_device = true;
   for (int kind = 0; kind < 2; kind++) {
     cudaGraph_t g = nullptr;
     if (int rc = md_step_graph(ctx, kind, &g)) return sfail(s, rc, orac_gpu_last_error(ctx));
