@@ -52,6 +52,7 @@ int upload3(orac_gpu_ctx* ctx, double* dst, int n, const double* a, const double
 
 __global__ void k_shell_out(const double* __restrict__ acc, int forces_on, double* __restrict__ e,
                             double* __restrict__ stress) {
+  pdl_enter();
   const int t = threadIdx.x;
   if (e && t < 8) {
     // ORAC argument order: ucns ucos virs virsp ucnp ucop ucnsp ucosp
@@ -209,7 +210,7 @@ int shell_run_r(orac_gpu_ctx* ctx, char rshell, const ShellRadii& radii, const d
   if (a.forces_on && !(flags & SH_FIXED_OUT))
     if (int rc = finalize_launch(ctx, d_mol, d_f, want_s ? 1 : 0)) return rc;
   if (want_e || want_s) {
-    k_shell_out<<<1, 32, 0, ctx->stream>>>(ctx->d_acc, a.forces_on, want_e ? d_e : nullptr,
+    orac_launch(k_shell_out, 1, 32, 0, ctx->stream, ctx->d_acc, a.forces_on, want_e ? d_e : nullptr,
                                            want_s ? d_stress : nullptr);
     CKL();
   }

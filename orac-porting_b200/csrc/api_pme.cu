@@ -8,6 +8,7 @@ namespace {
 
 __global__ void k_to_cart(int n, const double* __restrict__ s, double c11, double c12, double c13, double c22,
                           double c23, double c33, double* __restrict__ x) {
+  pdl_enter();
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
   const double a = s[t], b = s[n + t], c = s[2 * n + t];
@@ -65,7 +66,7 @@ int fft_pme_device(orac_gpu_ctx* ctx, const double* d_sxyz, const double* d_mol,
   const int N = ctx->N;
   if (grow(ctx, &S.cart, &S.cart_n, 3 * (size_t)N)) return ORAC_ERR_CUDA;
   const double* c = ctx->co;
-  k_to_cart<<<(N + 255) / 256, 256, 0, ctx->stream>>>(N, d_sxyz, c[0], c[3], c[6], c[4], c[7], c[8], S.cart);
+  orac_launch(k_to_cart, (N + 255) / 256, 256, 0, ctx->stream, N, d_sxyz, c[0], c[3], c[6], c[4], c[7], c[8], S.cart);
   CKL();
   double recip[9];
   recip_of(ctx->oc, recip);

@@ -65,6 +65,7 @@ double scaled_charge(double q, double lq) {
 }
 
 __global__ void k_variant_out(const double* __restrict__ acc, int variant, int forces_on, double* __restrict__ x) {
+  pdl_enter();
   if (threadIdx.x != 0) return;
   for (int k = 0; k < 5; k++) x[k] = 0.0;  // x[5] is the PME's
   if (!forces_on) return;
@@ -159,7 +160,7 @@ void variant_fill(const orac_gpu_ctx* ctx, PairArgs* a) {
 
 int variant_out_launch(orac_gpu_ctx* ctx, int forces_on) {
   if (!ctx->d_xtra && dev_alloc(ctx, &ctx->d_xtra, 8)) return ORAC_ERR_CUDA;
-  k_variant_out<<<1, 32, 0, ctx->stream>>>(ctx->d_acc, ctx->variant, forces_on, ctx->d_xtra);
+  orac_launch(k_variant_out, 1, 32, 0, ctx->stream, ctx->d_acc, ctx->variant, forces_on, ctx->d_xtra);
   CKL();
   return ORAC_OK;
 }

@@ -8,6 +8,7 @@
 #include <cstdio>
 #include <cstring>
 #include <unordered_map>
+#include <utility>
 #include <vector>
 
 #include "orac_gpu.h"
@@ -383,6 +384,33 @@ static inline int dev_alloc(orac_gpu_ctx* ctx, T** p, size_t n) {
   ctx->dmem_bytes += n * sizeof(T);
   return ORAC_OK;
 }
+
+// Kernel launches of the library go through orac_launch: programmatic
+// dependent launch, so a kernel's blocks are scheduled while its predecessor
+// in the stream still runs (in captured graphs too) and wait on the device
+// for the predecessor's completion and memory (pdl_enter, the first thing
+// every kernel of the library does).
+template <typename... KArgs, typename... Args>
+static inline cudaError_t orac_launch(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                                      cudaStream_t stream, Args&&... args) {
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = stream;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
+
+// Wait for the grids this one depends on (their memory operations complete
+// and visible).  The next grid is released when this one completes: blocks
+// released earlier would hold SM slots while they wait, which costs the
+// concurrent systems of a batch more than it saves.
+__device__ __forceinline__ void pdl_enter() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 
 // ------------------------------------------------------ internal drivers
 // k_list.cu

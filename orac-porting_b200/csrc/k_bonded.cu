@@ -153,6 +153,7 @@ __device__ __forceinline__ double warp_sumd(double v) {
 }
 
 __global__ void k_bonded(const BondedArgs A) {
+  pdl_enter();
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   double e[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   if ((A.mask & BK_BOND) && t < A.nb) {
@@ -351,7 +352,7 @@ int bonded_launch(orac_gpu_ctx* ctx, int mask, const double* d_x, double* d_f, u
   A.e = d_e;
   const int n = B.nb + B.nbend + B.nt + B.nit;
   if (n == 0) return ORAC_OK;
-  k_bonded<<<(n + 255) / 256, 256, 0, ctx->stream>>>(A);
+  orac_launch(k_bonded, (n + 255) / 256, 256, 0, ctx->stream, A);
   CKL();
   return ORAC_OK;
 }

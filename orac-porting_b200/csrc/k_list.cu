@@ -36,6 +36,7 @@ __device__ __forceinline__ int lc_cell(double x, double d, int nc) {
 __global__ void k_cell_assign(int G, const double* __restrict__ grp, int ncx,
                               int ncy, int ncz, int* __restrict__ cell_of,
                               int* __restrict__ cell_cnt) {
+  pdl_enter();
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= G) return;
   const int nx = lc_cell(grp[g], 2.0 / ncx, ncx);
@@ -50,6 +51,7 @@ __global__ void k_cell_assign(int G, const double* __restrict__ grp, int ncx,
 __global__ void __launch_bounds__(1024)
     k_scan(int n, const int* __restrict__ in, int* __restrict__ out,
            int64_t* __restrict__ total) {
+  pdl_enter();
   __shared__ long long s[1024];
   const int t = threadIdx.x;
   const int chunk = (n + 1023) / 1024;
@@ -80,6 +82,7 @@ __global__ void __launch_bounds__(1024)
 __global__ void k_cell_fill(int G, const int* __restrict__ cell_of,
                             const int* __restrict__ cell_start,
                             int* __restrict__ cursor, int* __restrict__ cell_grp) {
+  pdl_enter();
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= G) return;
   const int c = cell_of[g];
@@ -89,6 +92,7 @@ __global__ void k_cell_fill(int G, const int* __restrict__ cell_of,
 
 __global__ void k_cell_order(int ncell, const int* __restrict__ cell_start,
                              int* __restrict__ cell_grp) {
+  pdl_enter();
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= ncell) return;
   const int b = cell_start[c], e = cell_start[c + 1];
@@ -171,6 +175,7 @@ __device__ unsigned long long pair_mask(const ListArgs& A, int i, int l) {
 // hits), within a cell by group index.
 template <bool FILL>
 __global__ void __launch_bounds__(128) k_pairs(const ListArgs A) {
+  pdl_enter();
   const int lane = threadIdx.x & 31;
   const int i = blockIdx.x * 4 + (threadIdx.x >> 5);
   if (i >= A.G) return;
@@ -358,9 +363,9 @@ ListArgs base_args(orac_gpu_ctx* ctx, double rcut, GList* out) {
 // count -> scan -> (grow) -> fill
 int pairs_count_fill(orac_gpu_ctx* ctx, ListArgs A, GList* out) {
   const int nb = (ctx->G + 3) / 4;
-  k_pairs<false><<<nb, 128, 0, ctx->stream>>>(A);
+  orac_launch(k_pairs<false>, nb, 128, 0, ctx->stream, A);
   CKL();
-  k_scan<<<1, 1024, 0, ctx->stream>>>(ctx->G, out->cnt, out->off, ctx->d_total);
+  orac_launch(k_scan, 1, 1024, 0, ctx->stream, ctx->G, out->cnt, out->off, ctx->d_total);
   CKL();
   int64_t total = 0;
   CK(cudaMemcpyAsync(&total, ctx->d_total, sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream));
@@ -382,7 +387,7 @@ int pairs_count_fill(orac_gpu_ctx* ctx, ListArgs A, GList* out) {
   }
   A.j = out->j;
   A.mask = out->mask;
-  k_pairs<true><<<nb, 128, 0, ctx->stream>>>(A);
+  orac_launch(k_pairs<true>, nb, 128, 0, ctx->stream, A);
   CKL();
   out->npairs = total;
   out->valid = true;
@@ -403,16 +408,16 @@ int list_build_cells(orac_gpu_ctx* ctx, double rcut, GList* out) {
   }
   CK(cudaMemsetAsync(ctx->d_cell_cnt, 0, sizeof(int) * (ncell + 1), ctx->stream));
   const int G = ctx->G;
-  k_cell_assign<<<(G + 255) / 256, 256, 0, ctx->stream>>>(G, ctx->d_grp, ctx->ncx, ctx->ncy, ctx->ncz,
+  orac_launch(k_cell_assign, (G + 255) / 256, 256, 0, ctx->stream, G, ctx->d_grp, ctx->ncx, ctx->ncy, ctx->ncz,
                                                          ctx->d_cell_of, ctx->d_cell_cnt);
   CKL();
-  k_scan<<<1, 1024, 0, ctx->stream>>>(ncell, ctx->d_cell_cnt, ctx->d_cell_start, nullptr);
+  orac_launch(k_scan, 1, 1024, 0, ctx->stream, ncell, ctx->d_cell_cnt, ctx->d_cell_start, nullptr);
   CKL();
   CK(cudaMemsetAsync(ctx->d_cell_cnt, 0, sizeof(int) * (ncell + 1), ctx->stream));
-  k_cell_fill<<<(G + 255) / 256, 256, 0, ctx->stream>>>(G, ctx->d_cell_of, ctx->d_cell_start, ctx->d_cell_cnt,
+  orac_launch(k_cell_fill, (G + 255) / 256, 256, 0, ctx->stream, G, ctx->d_cell_of, ctx->d_cell_start, ctx->d_cell_cnt,
                                                        ctx->d_cell_grp);
   CKL();
-  k_cell_order<<<(ncell + 255) / 256, 256, 0, ctx->stream>>>(ncell, ctx->d_cell_start, ctx->d_cell_grp);
+  orac_launch(k_cell_order, (ncell + 255) / 256, 256, 0, ctx->stream, ncell, ctx->d_cell_start, ctx->d_cell_grp);
   CKL();
   ListArgs A = base_args(ctx, rcut, out);
   A.allpairs = 0;
@@ -442,29 +447,29 @@ int list_build_cells_async(orac_gpu_ctx* ctx, double rcut, GList* out, int* d_fl
   const int ncell = ctx->ncx * ctx->ncy * ctx->ncz;
   const int G = ctx->G;
   CK(cudaMemsetAsync(ctx->d_cell_cnt, 0, sizeof(int) * (ncell + 1), ctx->stream));
-  k_cell_assign<<<(G + 255) / 256, 256, 0, ctx->stream>>>(G, ctx->d_grp, ctx->ncx, ctx->ncy, ctx->ncz,
+  orac_launch(k_cell_assign, (G + 255) / 256, 256, 0, ctx->stream, G, ctx->d_grp, ctx->ncx, ctx->ncy, ctx->ncz,
                                                          ctx->d_cell_of, ctx->d_cell_cnt);
   CKL();
-  k_scan<<<1, 1024, 0, ctx->stream>>>(ncell, ctx->d_cell_cnt, ctx->d_cell_start, nullptr);
+  orac_launch(k_scan, 1, 1024, 0, ctx->stream, ncell, ctx->d_cell_cnt, ctx->d_cell_start, nullptr);
   CKL();
   CK(cudaMemsetAsync(ctx->d_cell_cnt, 0, sizeof(int) * (ncell + 1), ctx->stream));
-  k_cell_fill<<<(G + 255) / 256, 256, 0, ctx->stream>>>(G, ctx->d_cell_of, ctx->d_cell_start, ctx->d_cell_cnt,
+  orac_launch(k_cell_fill, (G + 255) / 256, 256, 0, ctx->stream, G, ctx->d_cell_of, ctx->d_cell_start, ctx->d_cell_cnt,
                                                        ctx->d_cell_grp);
   CKL();
-  k_cell_order<<<(ncell + 255) / 256, 256, 0, ctx->stream>>>(ncell, ctx->d_cell_start, ctx->d_cell_grp);
+  orac_launch(k_cell_order, (ncell + 255) / 256, 256, 0, ctx->stream, ncell, ctx->d_cell_start, ctx->d_cell_grp);
   CKL();
   ListArgs A = base_args(ctx, rcut, out);
   A.allpairs = 0;
   A.cap = out->cap;
   A.flag = d_flag;
   const int nb = (G + 3) / 4;
-  k_pairs<false><<<nb, 128, 0, ctx->stream>>>(A);
+  orac_launch(k_pairs<false>, nb, 128, 0, ctx->stream, A);
   CKL();
-  k_scan<<<1, 1024, 0, ctx->stream>>>(G, out->cnt, out->off, ctx->d_total);
+  orac_launch(k_scan, 1, 1024, 0, ctx->stream, G, out->cnt, out->off, ctx->d_total);
   CKL();
   A.j = out->j;
   A.mask = out->mask;
-  k_pairs<true><<<nb, 128, 0, ctx->stream>>>(A);
+  orac_launch(k_pairs<true>, nb, 128, 0, ctx->stream, A);
   CKL();
   out->valid = true;
   return ORAC_OK;

@@ -183,6 +183,7 @@ __global__ void __launch_bounds__(WPB * 32, (MG <= 4 && !EN)
                                                       : (LPG == 16 ? ORAC_KPAIR_MINB : ORAC_KPAIR_MINB32))
                                                 : 1)
     k_pair(const PairArgs A) {
+  pdl_enter();
   constexpr int SEG = 32 / LPG;  // groups per warp
   // long rows (a warp per group): in-band entries are compacted through a
   // shared queue so the pair work runs on every lane; the short rows of the
@@ -628,6 +629,7 @@ __global__ void k_prep(int N, int G, const double* __restrict__ xyz,
                        double c13, double c22, double c23, double c33,
                        double4* __restrict__ gpos, float4* __restrict__ aoff,
                        unsigned long long* __restrict__ ffix) {
+  pdl_enter();
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t < G) gpos[t] = make_double4(grp[t], grp[G + t], grp[2 * G + t], 0.0);
   if (t < N) {
@@ -651,6 +653,7 @@ __global__ void k_finalize(int N, const unsigned long long* __restrict__ ffix,
                            const int* __restrict__ amol, double c11, double c12,
                            double c13, double c22, double c23, double c33,
                            double* __restrict__ fout, double* __restrict__ acc) {
+  pdl_enter();
   __shared__ double s_red[8][9];
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (!mol) {  // forces only; the condition is uniform over the grid
@@ -718,7 +721,7 @@ int pair_launch(orac_gpu_ctx* ctx, const PairArgs& a, int maxg) {
   switch ((((mgk * 3 + a.variant) * 2 + (a.energy ? 1 : 0)) * 2 + (half ? 1 : 0)) * 2 + (hi ? 1 : 0)) {
 #define ORAC_KP(MGK, MG, VAR, EN, LPG, HI)                                                     \
   case (((MGK * 3 + VAR) * 2 + (EN ? 1 : 0)) * 2 + (LPG == 16 ? 1 : 0)) * 2 + (HI ? 1 : 0):     \
-    k_pair<MG, EN, VAR, LPG, HI><<<nb, WPB * 32, smem, ctx->stream>>>(a);                      \
+    orac_launch(k_pair<MG, EN, VAR, LPG, HI>, nb, WPB * 32, smem, ctx->stream, a);                      \
     break;
 #define ORAC_KP_V(MGK, MG, VAR)                                                                \
   ORAC_KP(MGK, MG, VAR, false, 32, false)                                                      \
@@ -788,7 +791,7 @@ int prof_collect(orac_gpu_ctx* ctx, int a, int b) {
 int prep_launch(orac_gpu_ctx* ctx, const double* xyz, const double* grp) {
   const int n = ctx->N > ctx->G ? ctx->N : ctx->G;
   const double* c = ctx->co;
-  k_prep<<<(n + 255) / 256, 256, 0, ctx->stream>>>(
+  orac_launch(k_prep, (n + 255) / 256, 256, 0, ctx->stream, 
       ctx->N, ctx->G, xyz, grp, ctx->d_agrp, ctx->d_aq, c[0], c[3], c[6], c[4], c[7], c[8], ctx->d_gpos,
       ctx->d_aoff, ctx->d_ffix);
   CKL();
@@ -797,7 +800,7 @@ int prep_launch(orac_gpu_ctx* ctx, const double* xyz, const double* grp) {
 
 int finalize_launch(orac_gpu_ctx* ctx, const double* mol, double* fout, int stress) {
   const double* c = ctx->co;
-  k_finalize<<<(ctx->N + 255) / 256, 256, 0, ctx->stream>>>(ctx->N, ctx->d_ffix, stress ? mol : nullptr, ctx->P,
+  orac_launch(k_finalize, (ctx->N + 255) / 256, 256, 0, ctx->stream, ctx->N, ctx->d_ffix, stress ? mol : nullptr, ctx->P,
                                                             ctx->d_amol, c[0], c[3], c[6], c[4], c[7], c[8], fout,
                                                             ctx->d_acc);
   CKL();

@@ -206,6 +206,7 @@ enum { XF = 0, YF = 1, ZC = 2, YI = 3, XI = 4 };
 
 template <int MODE>
 __global__ void __launch_bounds__(FFT_THREADS) k_fft(const GridArgs A) {
+  pdl_enter();
   extern __shared__ float2 sm[];
   const int n = A.P.n;
   const int B = A.B;
@@ -424,6 +425,7 @@ __device__ __forceinline__ int gidx(int k0, int n) {
 
 // one thread per (atom, i3 plane)
 __global__ void k_spread(const AtomArgs A) {
+  pdl_enter();
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int p = A.order;
   if (t >= A.natom * p) return;
@@ -454,6 +456,7 @@ __global__ void k_spread(const AtomArgs A) {
 constexpr int GATHER_LANES = 4;
 
 __global__ void k_gather(const AtomArgs A) {
+  pdl_enter();
   const int gt = blockIdx.x * blockDim.x + threadIdx.x;
   const int t = gt / GATHER_LANES, sub = gt % GATHER_LANES;
   const int p = A.order;
@@ -669,7 +672,7 @@ int pme_run(orac_gpu_ctx* ctx, int natom, const double* d_cart, const double* d_
   A.dq = d_edq ? d_dq : nullptr;
   A.edq = d_edq;
   const int nsp = natom * P.order;
-  k_spread<<<(nsp + 255) / 256, 256, 0, ctx->stream>>>(A);
+  orac_launch(k_spread, (nsp + 255) / 256, 256, 0, ctx->stream, A);
   CKL();
   GridArgs G;
   memset(&G, 0, sizeof(G));
@@ -706,7 +709,7 @@ int pme_run(orac_gpu_ctx* ctx, int natom, const double* d_cart, const double* d_
     G.B = lines_per_block(n1);
     nb = (n2 * n3 + G.B - 1) / G.B;
     sm = (2 * (size_t)G.B + 1) * n1 * sizeof(float2);
-    k_fft<XF><<<nb, FFT_THREADS, sm, ctx->stream>>>(G);
+    orac_launch(k_fft<XF>, nb, FFT_THREADS, sm, ctx->stream, G);
     CKL();
     // y forward
     make_plan(n2, &G.P);
@@ -714,7 +717,7 @@ int pme_run(orac_gpu_ctx* ctx, int natom, const double* d_cart, const double* d_
     G.B = lines_per_block(n2);
     nb = n3 * ((h1 + G.B - 1) / G.B);
     sm = (2 * (size_t)G.B + 1) * n2 * sizeof(float2);
-    k_fft<YF><<<nb, FFT_THREADS, sm, ctx->stream>>>(G);
+    orac_launch(k_fft<YF>, nb, FFT_THREADS, sm, ctx->stream, G);
     CKL();
   }
   // z forward + influence function + z inverse
@@ -723,7 +726,7 @@ int pme_run(orac_gpu_ctx* ctx, int natom, const double* d_cart, const double* d_
   G.B = lines_per_block(n3);
   nb = n2 * ((h1 + G.B - 1) / G.B);
   sm = (2 * (size_t)G.B + 1) * n3 * sizeof(float2);
-  k_fft<ZC><<<nb, FFT_THREADS, sm, ctx->stream>>>(G);
+  orac_launch(k_fft<ZC>, nb, FFT_THREADS, sm, ctx->stream, G);
   CKL();
   {
     // y inverse
@@ -732,7 +735,7 @@ int pme_run(orac_gpu_ctx* ctx, int natom, const double* d_cart, const double* d_
     G.B = lines_per_block(n2);
     nb = n3 * ((h1 + G.B - 1) / G.B);
     sm = (2 * (size_t)G.B + 1) * n2 * sizeof(float2);
-    k_fft<YI><<<nb, FFT_THREADS, sm, ctx->stream>>>(G);
+    orac_launch(k_fft<YI>, nb, FFT_THREADS, sm, ctx->stream, G);
     CKL();
     // x inverse (c2r)
     make_plan(n1, &G.P);
@@ -740,10 +743,10 @@ int pme_run(orac_gpu_ctx* ctx, int natom, const double* d_cart, const double* d_
     G.B = lines_per_block(n1);
     nb = (n2 * n3 + G.B - 1) / G.B;
     sm = (2 * (size_t)G.B + 1) * n1 * sizeof(float2);
-    k_fft<XI><<<nb, FFT_THREADS, sm, ctx->stream>>>(G);
+    orac_launch(k_fft<XI>, nb, FFT_THREADS, sm, ctx->stream, G);
     CKL();
   }
-  k_gather<<<(GATHER_LANES * natom + 127) / 128, 128, 0, ctx->stream>>>(A);
+  orac_launch(k_gather, (GATHER_LANES * natom + 127) / 128, 128, 0, ctx->stream, A);
   CKL();
   return ORAC_OK;
 }
@@ -789,6 +792,7 @@ struct SplineAt0 {
 // and the small-modulus patch runs serially in index order like
 // DFTMOD's loop (src/pme_fftw3.f90:202-230).
 __global__ void k_static_tables(int n1, int n2, int n3, int order, SplineAt0 arr, float2* tw, float* bsp) {
+  pdl_enter();
   __shared__ double mod[STATIC_MAX_AXIS];
   const int axis = blockIdx.x;
   const int n = axis == 0 ? n1 : (axis == 1 ? n2 : n3);
@@ -817,6 +821,7 @@ __global__ void k_static_tables(int n1, int n2, int n3, int order, SplineAt0 arr
 // eer and the 3x3 column-major virial from the grid sums, as
 // orac_gpu_do_pmesh_kspace finishes them on the host
 __global__ void k_static_finish(const double* __restrict__ e, double* __restrict__ out) {
+  pdl_enter();
   if (threadIdx.x != 0) return;
   out[0] = 0.5 * e[0];
   out[1] = 0.5 * e[1];
@@ -931,7 +936,7 @@ extern "C" int orac_gpu_pme_kspace_static(void* stream, int numatoms, const doub
   double darr[MAXORD + 2];
   for (int k = 0; k < MAXORD + 2; k++) arr.c[k] = darr[k] = 0.0;
   host_bspline(0.0, order, arr.c, darr);
-  k_static_tables<<<3, 128, 0, st>>>(nfft1, nfft2, nfft3, order, arr, tw, bsp);
+  orac_launch(k_static_tables, 3, 128, 0, st, nfft1, nfft2, nfft3, order, arr, tw, bsp);
 
   AtomArgs A;
   memset(&A, 0, sizeof(A));
@@ -956,7 +961,7 @@ extern "C" int orac_gpu_pme_kspace_static(void* stream, int numatoms, const doub
   A.f = d_force;
   A.eout = eout;
   const int nsp = numatoms * order;
-  k_spread<<<(nsp + 255) / 256, 256, 0, st>>>(A);
+  orac_launch(k_spread, (nsp + 255) / 256, 256, 0, st, A);
 
   GridArgs G;
   memset(&G, 0, sizeof(G));
@@ -990,29 +995,29 @@ extern "C" int orac_gpu_pme_kspace_static(void* stream, int numatoms, const doub
   make_plan(nfft1, &G.P);
   G.tw = tws[0];
   G.B = lines_per_block(nfft1);
-  k_fft<XF><<<(nfft2 * nfft3 + G.B - 1) / G.B, FFT_THREADS, (2 * (size_t)G.B + 1) * nfft1 * sizeof(float2), st>>>(G);
+  orac_launch(k_fft<XF>, (nfft2 * nfft3 + G.B - 1) / G.B, FFT_THREADS, (2 * (size_t)G.B + 1) * nfft1 * sizeof(float2), st, G);
   // y forward
   make_plan(nfft2, &G.P);
   G.tw = tws[1];
   G.B = lines_per_block(nfft2);
-  k_fft<YF><<<nfft3 * ((h1 + G.B - 1) / G.B), FFT_THREADS, (2 * (size_t)G.B + 1) * nfft2 * sizeof(float2), st>>>(G);
+  orac_launch(k_fft<YF>, nfft3 * ((h1 + G.B - 1) / G.B), FFT_THREADS, (2 * (size_t)G.B + 1) * nfft2 * sizeof(float2), st, G);
   // z forward + influence function + z inverse
   make_plan(nfft3, &G.P);
   G.tw = tws[2];
   G.B = lines_per_block(nfft3);
-  k_fft<ZC><<<nfft2 * ((h1 + G.B - 1) / G.B), FFT_THREADS, (2 * (size_t)G.B + 1) * nfft3 * sizeof(float2), st>>>(G);
+  orac_launch(k_fft<ZC>, nfft2 * ((h1 + G.B - 1) / G.B), FFT_THREADS, (2 * (size_t)G.B + 1) * nfft3 * sizeof(float2), st, G);
   // y inverse
   make_plan(nfft2, &G.P);
   G.tw = tws[1];
   G.B = lines_per_block(nfft2);
-  k_fft<YI><<<nfft3 * ((h1 + G.B - 1) / G.B), FFT_THREADS, (2 * (size_t)G.B + 1) * nfft2 * sizeof(float2), st>>>(G);
+  orac_launch(k_fft<YI>, nfft3 * ((h1 + G.B - 1) / G.B), FFT_THREADS, (2 * (size_t)G.B + 1) * nfft2 * sizeof(float2), st, G);
   // x inverse (c2r)
   make_plan(nfft1, &G.P);
   G.tw = tws[0];
   G.B = lines_per_block(nfft1);
-  k_fft<XI><<<(nfft2 * nfft3 + G.B - 1) / G.B, FFT_THREADS, (2 * (size_t)G.B + 1) * nfft1 * sizeof(float2), st>>>(G);
-  k_gather<<<(GATHER_LANES * numatoms + 127) / 128, 128, 0, st>>>(A);
-  k_static_finish<<<1, 32, 0, st>>>(eout, d_energy);
+  orac_launch(k_fft<XI>, (nfft2 * nfft3 + G.B - 1) / G.B, FFT_THREADS, (2 * (size_t)G.B + 1) * nfft1 * sizeof(float2), st, G);
+  orac_launch(k_gather, (GATHER_LANES * numatoms + 127) / 128, 128, 0, st, A);
+  orac_launch(k_static_finish, 1, 32, 0, st, eout, d_energy);
   ce = cudaGetLastError();
   if (ce != cudaSuccess) return static_fail(err, err_len, ORAC_ERR_CUDA, "SPME launch: %s", cudaGetErrorString(ce));
   return ORAC_OK;

@@ -42,6 +42,7 @@ struct SmallArgs {
 };
 
 __global__ void k_small(const SmallArgs A) {
+  pdl_enter();
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   double e[4] = {0, 0, 0, 0};
   double dedl = 0.0;
@@ -137,6 +138,7 @@ __global__ void k_small(const SmallArgs A) {
 }
 
 __global__ void k_self(int n, const double* q, const int* ss, double* e) {
+  pdl_enter();
   __shared__ double s[8][2];
   double v[2] = {0, 0};
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x)
@@ -191,14 +193,14 @@ int small_launch_x(orac_gpu_ctx* ctx, int kind, const double* d_xyz, const int* 
   A.f = d_f;
   A.e = d_e;
   if (npairs > 0) {
-    k_small<<<(npairs + 255) / 256, 256, 0, ctx->stream>>>(A);
+    orac_launch(k_small, (npairs + 255) / 256, 256, 0, ctx->stream, A);
     CKL();
   }
   return ORAC_OK;
 }
 
 int self_launch(orac_gpu_ctx* ctx, const int* d_ss, double* d_e) {
-  k_self<<<64, 256, 0, ctx->stream>>>(ctx->N, ctx->d_aqd, d_ss, d_e);
+  orac_launch(k_self, 64, 256, 0, ctx->stream, ctx->N, ctx->d_aqd, d_ss, d_e);
   CKL();
   return ORAC_OK;
 }

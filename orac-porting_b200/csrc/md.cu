@@ -431,6 +431,91 @@ __device__ __forceinline__ bool shake3(double x[SMA][3], const double xo[SMA][3]
   return ok;
 }
 
+// SETTLE (Miyamoto and Kollman, J. Comput. Chem. 13, 952 (1992)): the SHAKE
+// solution for a rigid isosceles triangle (atom 0 the apex, equal masses
+// and lengths to atoms 1 and 2) in closed form.  The constraint forces lie
+// along the old bonds, so in the frame whose z axis is the old plane's
+// normal the z coordinates keep their unconstrained values; they fix the
+// two tilts of the canonical triangle (phi about x, psi about y), and the
+// turn theta about z follows from the zero torque of forces along the old
+// bonds: sum_i m_i (x0_i dy_i - y0_i dx_i) = 0 with d = constrained -
+// unconstrained, i.e. alpha sin(theta) + beta cos(theta) = gamma.  x holds
+// the unconstrained positions on entry, the constrained ones on exit; v
+// gains the displacement / dt.  Returns false where no solution exists.
+__device__ __forceinline__ void cross3(const double* a, const double* b, double* c) {
+  c[0] = a[1] * b[2] - a[2] * b[1];
+  c[1] = a[2] * b[0] - a[0] * b[2];
+  c[2] = a[0] * b[1] - a[1] * b[0];
+}
+
+__device__ bool settle3(double x[SMA][3], const double xo[SMA][3], double v[SMA][3], const double im[SMA],
+                        const double* L2, double dt) {
+  const double mA = 1.0 / im[0], mB = 1.0 / im[1];
+  const double M = mA + 2.0 * mB, wA = mA / M, wB = mB / M;
+  const double rc = 0.5 * sqrt(L2[2]);
+  const double h2 = L2[0] - rc * rc;
+  if (!(h2 > 0.0)) return false;
+  const double h = sqrt(h2), ra = 2.0 * wB * h, rb = wA * h;  // apex and base from the centre of mass
+  double d[3], a1[3], b1[3], c1[3], b0[3], c0[3];
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    d[k] = wA * x[0][k] + wB * (x[1][k] + x[2][k]);
+    a1[k] = x[0][k] - d[k];
+    b1[k] = x[1][k] - d[k];
+    c1[k] = x[2][k] - d[k];
+    b0[k] = xo[1][k] - xo[0][k];
+    c0[k] = xo[2][k] - xo[0][k];
+  }
+  double ez[3], ex[3], ey[3];
+  cross3(b0, c0, ez);
+  cross3(a1, ez, ex);
+  cross3(ez, ex, ey);
+  const double nz = dot3(ez, ez), nx = dot3(ex, ex), ny = dot3(ey, ey);
+  if (!(nz > 0.0 && nx > 0.0 && ny > 0.0)) return false;
+  const double iz = 1.0 / sqrt(nz), ix = 1.0 / sqrt(nx), iy = 1.0 / sqrt(ny);
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    ez[k] *= iz;
+    ex[k] *= ix;
+    ey[k] *= iy;
+  }
+  const double b0x = dot3(ex, b0), b0y = dot3(ey, b0), c0x = dot3(ex, c0), c0y = dot3(ey, c0);
+  const double a1z = dot3(ez, a1);
+  const double b1x = dot3(ex, b1), b1y = dot3(ey, b1), b1z = dot3(ez, b1);
+  const double c1x = dot3(ex, c1), c1y = dot3(ey, c1), c1z = dot3(ez, c1);
+  const double sphi = a1z / ra;
+  if (!(fabs(sphi) < 1.0)) return false;
+  const double cphi = sqrt(1.0 - sphi * sphi);
+  const double spsi = (b1z - c1z) / (2.0 * rc * cphi);
+  if (!(fabs(spsi) < 1.0)) return false;
+  const double cpsi = sqrt(1.0 - spsi * spsi);
+  // the canonical triangle tilted by phi and psi
+  const double a2y = ra * cphi, a2z = ra * sphi;
+  const double b2x = -rc * cpsi, b2y = -rb * cphi - rc * spsi * sphi, b2z = -rb * sphi + rc * spsi * cphi;
+  const double c2x = rc * cpsi, c2y = -rb * cphi + rc * spsi * sphi, c2z = -rb * sphi - rc * spsi * cphi;
+  // the turn about z (the apex term vanishes: its old position is the origin)
+  const double alpha = b0x * b2x + b0y * b2y + c0x * c2x + c0y * c2y;
+  const double beta = b0x * b2y - b0y * b2x + c0x * c2y - c0y * c2x;
+  const double gamma = b0x * b1y - b0y * b1x + c0x * c1y - c0y * c1x;
+  const double ab2 = alpha * alpha + beta * beta, disc = ab2 - gamma * gamma;
+  if (!(disc >= 0.0 && ab2 > 0.0)) return false;
+  const double sth = (alpha * gamma - beta * sqrt(disc)) / ab2;
+  const double cth = sqrt(1.0 - sth * sth);
+  const double p[3][3] = {{-a2y * sth, a2y * cth, a2z},
+                          {b2x * cth - b2y * sth, b2x * sth + b2y * cth, b2z},
+                          {c2x * cth - c2y * sth, c2x * sth + c2y * cth, c2z}};
+  const double idt = dt != 0.0 ? 1.0 / dt : 0.0;
+#pragma unroll
+  for (int a = 0; a < 3; a++)
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      const double xn = d[k] + ex[k] * p[a][0] + ey[k] * p[a][1] + ez[k] * p[a][2];
+      v[a][k] += (xn - x[a][k]) * idt;
+      x[a][k] = xn;
+    }
+  return true;
+}
+
 // levels 0..nlev-1 (molecules without intramolecular terms have nothing at
 // the N1 and N0 levels: nlev = 3)
 __device__ __forceinline__ double kick_dv(const MolArgs& A, int i, int nlev = NLV) {
@@ -493,6 +578,7 @@ __device__ __forceinline__ void group_centre(const MolArgs& A, int gi) {
 // correc (v += f dt/2m) from the fixed-point level accumulators, then RATTLE.
 // Threads [0, nsm) take one small molecule each, the rest one free atom.
 __global__ void k_kick(const MolArgs A) {
+  pdl_enter();
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int N = A.N;
   if (t < A.nsm) {
@@ -540,6 +626,7 @@ __global__ void k_kick(const MolArgs A) {
 // the scaled frame, group centres (appbou) and the pair-kernel inputs of
 // their groups; free atoms drift here and get their groups in k_free_groups.
 __global__ void k_drift(const MolArgs A) {
+  pdl_enter();
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int N = A.N;
   const double dt = A.dt;
@@ -581,7 +668,10 @@ __global__ void k_drift(const MolArgs A) {
       }
     }
     if (mol3) {
-      if (!shake3(x, xo, v, im, A.dss + m.z, dt, A.tol)) atomicOr(A.flag, 1);
+      const double* L2 = A.dss + m.z;
+      // isosceles with equal masses at the base: SETTLE, else Newton steps
+      const bool iso = im[1] == im[2] && fabs(L2[0] - L2[1]) <= 1e-12 * L2[0];
+      if (!(iso ? settle3(x, xo, v, im, L2, dt) : shake3(x, xo, v, im, L2, dt, A.tol))) atomicOr(A.flag, 1);
       if (!rattle3(x, v, im)) atomicOr(A.flag, 1);
     } else if (nc > 0) {
       if (!shake_small(x, xo, v, im, A.cloc + m.z, A.dss + m.z, nc, dt, A.tol)) atomicOr(A.flag, 1);
@@ -648,6 +738,7 @@ __global__ void k_drift(const MolArgs A) {
 // group centres and pair-kernel inputs of the groups of large constrained
 // molecules, after their iterative SHAKE
 __global__ void k_free_groups(const MolArgs A) {
+  pdl_enter();
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= A.nfreeg) return;
   group_centre(A, A.free_groups[t]);
@@ -671,6 +762,7 @@ struct ConsArgs {
 
 // iterative SHAKE (src/rattle_verlet.f SHAKE branch) for large molecules
 __global__ void k_shake_big(const ConsArgs A) {
+  pdl_enter();
   const int m = blockIdx.x * blockDim.x + threadIdx.x;
   if (m >= A.nmol) return;
   const int c0 = A.cstart[m], c1 = A.cstart[m + 1];
@@ -709,6 +801,7 @@ __global__ void k_shake_big(const ConsArgs A) {
 
 // iterative RATTLE velocity step (src/rattle_correc.f) for large molecules
 __global__ void k_rattle_big(const ConsArgs A) {
+  pdl_enter();
   const int m = blockIdx.x * blockDim.x + threadIdx.x;
   if (m >= A.nmol) return;
   const int c0 = A.cstart[m], c1 = A.cstart[m + 1];
@@ -738,6 +831,7 @@ __global__ void k_rattle_big(const ConsArgs A) {
 }
 
 __global__ void k_ekin(int N, const double* __restrict__ v, const double* __restrict__ invm, double* __restrict__ out) {
+  pdl_enter();
   __shared__ double s[8];
   double e = 0;
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < N; t += gridDim.x * blockDim.x)
@@ -923,10 +1017,10 @@ static int md_kick(orac_gpu_ctx* ctx, MdState& S, const double* c) {
   kick_fill(A, S, c);
   if (!A.kick) return ORAC_OK;
   const int n = S.nsm + S.nfree;
-  k_kick<<<(n + 31) / 32, 32, 0, ctx->stream>>>(A);
+  orac_launch(k_kick, (n + 31) / 32, 32, 0, ctx->stream, A);
   CKL();
   if (S.nbig) {
-    k_rattle_big<<<(S.nbig + 127) / 128, 128, 0, ctx->stream>>>(big_args(ctx, S, 0.0, 1e-12));
+    orac_launch(k_rattle_big, (S.nbig + 127) / 128, 128, 0, ctx->stream, big_args(ctx, S, 0.0, 1e-12));
     CKL();
   }
   return ORAC_OK;
@@ -946,16 +1040,16 @@ static int md_drift(orac_gpu_ctx* ctx, MdState& S, double dt, const double* c, i
   A.fv = S.has_n0 ? S.ffix[LN0] : nullptr;
   for (int l = 0; l < NLV; l++) A.fz[l] = ((zmask >> l) & 1) ? S.ffix[l] : nullptr;
   const int n = S.nsm + S.ndg + S.nda;
-  k_drift<<<(n + 31) / 32, 32, 0, ctx->stream>>>(A);
+  orac_launch(k_drift, (n + 31) / 32, 32, 0, ctx->stream, A);
   CKL();
   if (S.nbig) {
-    k_shake_big<<<(S.nbig + 127) / 128, 128, 0, ctx->stream>>>(big_args(ctx, S, dt, 1e-8));
+    orac_launch(k_shake_big, (S.nbig + 127) / 128, 128, 0, ctx->stream, big_args(ctx, S, dt, 1e-8));
     CKL();
-    k_rattle_big<<<(S.nbig + 127) / 128, 128, 0, ctx->stream>>>(big_args(ctx, S, dt, 1e-12));
+    orac_launch(k_rattle_big, (S.nbig + 127) / 128, 128, 0, ctx->stream, big_args(ctx, S, dt, 1e-12));
     CKL();
   }
   if (S.nfreeg) {
-    k_free_groups<<<(S.nfreeg + 31) / 32, 32, 0, ctx->stream>>>(A);
+    orac_launch(k_free_groups, (S.nfreeg + 31) / 32, 32, 0, ctx->stream, A);
     CKL();
   }
   return ORAC_OK;
@@ -1178,7 +1272,7 @@ static int md_step(orac_gpu_ctx* ctx, MdState& S, bool update, bool energy) {
   }
   if (energy) {
     CK(cudaMemsetAsync(S.e + 40, 0, sizeof(double), ctx->stream));
-    k_ekin<<<64, 256, 0, ctx->stream>>>(ctx->N, S.v, S.invm, S.e + 40);
+    orac_launch(k_ekin, 64, 256, 0, ctx->stream, ctx->N, S.v, S.invm, S.e + 40);
     CKL();
   }
   return ORAC_OK;
