@@ -250,7 +250,9 @@ def gpu_arm(args, wl, s, device):
     # end-to-end through the public ABI with host buffers: every step copies
     # the state in from pinned host memory and reads it back
     n = s.ntap
-    host = [torch.empty(n, dtype=torch.float64).pin_memory() for _ in range(6)]
+    # one pinned buffer: x, y, z, vx, vy, vz back to back (two copies each way)
+    hbuf = torch.empty(6 * n, dtype=torch.float64).pin_memory()
+    host = [hbuf[k * n:(k + 1) * n] for k in range(6)]
     x, v = eng.md_state()
     for k in range(3):
         host[k].copy_(torch.from_numpy(x[k]))
@@ -616,7 +618,7 @@ def main():
                e2e={"value": e2e_val, "unit": "ns/day", "h2d_bytes_per_step": res["bytes_io"],
                     "d2h_bytes_per_step": res["bytes_io"],
                     "how": "orac_gpu_md_set_state (pinned host -> device), one step, orac_gpu_md_get_state "
-                           "(device -> pinned host), wall clock"},
+                           "(device -> pinned host, with the status flags), orac_gpu_md_collect, wall clock"},
                gpu_launches=res["launches"], clocks=res["clocks"])
     if "batched" in res:
         bt = res["batched"]

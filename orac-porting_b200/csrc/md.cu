@@ -906,6 +906,10 @@ struct MdState {
   // kernels; fork and join by events (captured as graph edges)
   cudaStream_t side = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  // status flags read back through pinned memory; flag_step is the step
+  // count at the last read-back that followed a synchronisation
+  int* h_flag = nullptr;
+  long long flag_step = -1;
 };
 
 static MdState* md_of(orac_gpu_ctx* ctx) {
@@ -920,6 +924,7 @@ void md_destroy(orac_gpu_ctx* ctx) {
   if (S->graph) cudaGraphDestroy(S->graph);
   if (S->gexec_u) cudaGraphExecDestroy(S->gexec_u);
   if (S->graph_u) cudaGraphDestroy(S->graph_u);
+  if (S->h_flag) cudaFreeHost(S->h_flag);
   if (S->ev_fork) cudaEventDestroy(S->ev_fork);
   if (S->ev_join) cudaEventDestroy(S->ev_join);
   if (S->side) cudaStreamDestroy(S->side);
@@ -1280,6 +1285,19 @@ static int md_step(orac_gpu_ctx* ctx, MdState& S, bool update, bool energy) {
 
 static int md_run_impl(orac_gpu_ctx* ctx, int nsteps, int energy_every, double* rec, bool async);
 
+// The six N-double arrays of a state transfer as few copies as possible:
+// arrays that follow each other in memory on both sides go as one copy.
+static int copy_runs(orac_gpu_ctx* ctx, double* const dst[6], const double* const src[6], cudaMemcpyKind kind) {
+  const size_t N = (size_t)ctx->N;
+  for (int k = 0; k < 6;) {
+    int e = k + 1;
+    while (e < 6 && dst[e] == dst[e - 1] + N && src[e] == src[e - 1] + N) e++;
+    CK(cudaMemcpyAsync(dst[k], src[k], (size_t)(e - k) * N * sizeof(double), kind, ctx->stream));
+    k = e;
+  }
+  return ORAC_OK;
+}
+
 extern "C" {
 
 int orac_gpu_md_setup(orac_gpu_ctx* ctx, const double* x, const double* y, const double* z, const double* vx,
@@ -1297,6 +1315,7 @@ int orac_gpu_md_setup(orac_gpu_ctx* ctx, const double* x, const double* y, const
   const int N = ctx->N, P = ctx->P, G = ctx->G;
   S.N = N;
   CK(cudaStreamCreateWithFlags(&S.side, cudaStreamNonBlocking));
+  CK(cudaMallocHost((void**)&S.h_flag, sizeof(int)));
   CK(cudaEventCreateWithFlags(&S.ev_fork, cudaEventDisableTiming));
   CK(cudaEventCreateWithFlags(&S.ev_join, cudaEventDisableTiming));
   if (dev_alloc(ctx, &S.x, 3 * (size_t)N) || dev_alloc(ctx, &S.v, 3 * (size_t)N) ||
@@ -1516,12 +1535,18 @@ int orac_gpu_md_run_async(orac_gpu_ctx* ctx, int nsteps) { return md_run_impl(ct
 int orac_gpu_md_collect(orac_gpu_ctx* ctx) {
   if (!ctx) return ORAC_ERR_PARAM;
   MdState& S = *md_of(ctx);
-  CK(cudaStreamSynchronize(ctx->stream));
+  if (!S.h_flag) return ctx_fail(ctx, ORAC_ERR_STATE, "md_setup not called");
+  if (S.flag_step != S.step) {
+    // steps were queued since the last read-back (md_get_state reads the
+    // flags with the state): wait for them and read the flags
+    CK(cudaMemcpyAsync(S.h_flag, S.flag, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    S.flag_step = S.step;
+  }
   if (ctx->prof && S.last_kind >= 0)
     if (int rc = prof_collect(ctx, S.pslot[S.last_kind][0], S.pslot[S.last_kind][1])) return rc;
   S.last_kind = -1;
-  int flag = 0;
-  CK(cudaMemcpy(&flag, S.flag, sizeof(int), cudaMemcpyDeviceToHost));
+  const int flag = *S.h_flag;
   if (flag & 1) return ctx_fail(ctx, ORAC_ERR_CAPACITY, "SHAKE/RATTLE did not converge");
   if (flag & 2) return ctx_fail(ctx, ORAC_ERR_CAPACITY, "neighbour list capacity exceeded during the run");
   return ORAC_OK;
@@ -1531,11 +1556,14 @@ int orac_gpu_md_get_state(orac_gpu_ctx* ctx, double* x, double* y, double* z, do
   if (!ctx) return ORAC_ERR_PARAM;
   MdState& S = *md_of(ctx);
   if (!S.ready) return ctx_fail(ctx, ORAC_ERR_STATE, "md_setup not called");
-  const size_t n = (size_t)ctx->N * sizeof(double);
   double* dst[6] = {x, y, z, vx, vy, vz};
   const double* src[6] = {S.x, S.x + ctx->N, S.x + 2 * (size_t)ctx->N, S.v, S.v + ctx->N, S.v + 2 * (size_t)ctx->N};
-  for (int k = 0; k < 6; k++) CK(cudaMemcpyAsync(dst[k], src[k], n, cudaMemcpyDeviceToHost, ctx->stream));
+  if (int rc = copy_runs(ctx, dst, src, cudaMemcpyDeviceToHost)) return rc;
+  // the status flags travel with the state: a following md_collect need not
+  // wait again
+  CK(cudaMemcpyAsync(S.h_flag, S.flag, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
+  S.flag_step = S.step;
   return ORAC_OK;
 }
 
@@ -1544,11 +1572,9 @@ int orac_gpu_md_set_state(orac_gpu_ctx* ctx, const double* x, const double* y, c
   if (!ctx) return ORAC_ERR_PARAM;
   MdState& S = *md_of(ctx);
   if (!S.ready) return ctx_fail(ctx, ORAC_ERR_STATE, "md_setup not called");
-  const size_t n = (size_t)ctx->N * sizeof(double);
   const double* src[6] = {x, y, z, vx, vy, vz};
   double* dst[6] = {S.x, S.x + ctx->N, S.x + 2 * (size_t)ctx->N, S.v, S.v + ctx->N, S.v + 2 * (size_t)ctx->N};
-  for (int k = 0; k < 6; k++) CK(cudaMemcpyAsync(dst[k], src[k], n, cudaMemcpyHostToDevice, ctx->stream));
-  return ORAC_OK;
+  return copy_runs(ctx, dst, src, cudaMemcpyHostToDevice);
 }
 
 int orac_gpu_md_set_graphs(orac_gpu_ctx* ctx, int on) {
