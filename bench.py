@@ -523,6 +523,30 @@ def serve_arm(args, wl, device):
                    "server with each request taking 500 x the system's measured single-system step time"}
 
 
+def profile_window_batch(nwin):
+    """One batched step of `nwin` lambda windows bracketed for a profiler
+    that starts collecting at cudaProfilerStart (the windows' set-up and
+    three warm-up steps stay outside)."""
+    import torch
+
+    from orac_b200.engine import Batch
+
+    wl = WORKLOADS["liquid"]
+    base = systems.ligand_in_water()
+    engines = [window_engine(base, k, nwin, 0, wl)[0] for k in range(nwin)]
+    b = Batch(engines)
+    b.run(3)
+    torch.cuda.synchronize()
+    torch.cuda.profiler.start()
+    b.run(1)
+    torch.cuda.synchronize()
+    torch.cuda.profiler.stop()
+    b.close()
+    for e in engines:
+        e.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -540,8 +564,13 @@ def main():
     ap.add_argument("--uneven", type=int, default=128, help="systems of the uneven HREM batch (0/1: skip)")
     ap.add_argument("--serve", type=float, default=3.0, help="seconds of Poisson arrivals of the serving leg (0: skip)")
     ap.add_argument("--serve-systems", type=int, default=16, help="systems the serving requests draw from")
+    ap.add_argument("--profile-window-batch", type=int, default=0, metavar="N",
+                    help="profiling aid, no JSON: N lambda windows batched, 3 steps, then one step bracketed by "
+                         "cudaProfilerStart/Stop (ncu --profile-from-start off --graph-profiling graph)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
+    if args.profile_window_batch > 0:
+        return profile_window_batch(args.profile_window_batch)
     wl = WORKLOADS[args.workload]
     ws, rank, local = dist_info()
     s = wl["build"]()
