@@ -172,6 +172,8 @@ int shell_run_r(orac_gpu_ctx* ctx, char rshell, const ShellRadii& radii, const d
   a.arsinn2 = rtolinn * rtolinn * rtolinn;
   a.iarsout2 = a.arsout2 > 0.0 ? (float)(1.0 / a.arsout2) : 0.0f;
   a.iarsinn2 = a.arsinn2 > 0.0 ? (float)(1.0 / a.arsinn2) : 0.0f;
+  a.diarsout2 = a.arsout2 > 0.0 ? 1.0 / a.arsout2 : 0.0;
+  a.diarsinn2 = a.arsinn2 > 0.0 ? 1.0 / a.arsinn2 : 0.0;
   a.alphal = (float)ctx->alphal;
   a.alphad = ctx->alphal;
   a.ljd = ctx->d_ljd;

@@ -89,6 +89,7 @@ struct PairArgs {
   double r2inn, r2inn0, r2out, r2out0, rinn0, rout0, r2neigh;
   double arsout1, arsout2, arsinn1, arsinn2;
   float iarsout2, iarsinn2;  // 1/arsout2, 1/arsinn2 (0 when the band is empty)
+  double diarsout2, diarsinn2;  // the same in FP64
   float alphal, twrtpi;
   double alphad;
   int forces_on, next_on, lskip, ewald;

@@ -281,13 +281,14 @@ __global__ void __launch_bounds__(WPB * 32, (MG <= 4 && !EN)
         switched = false;
       } else if (drj >= A.r2out && drj < A.r2out0) {
         // S(R) of src/force.f:311-317 for the forces: FP32 arithmetic on the
-        // FP64 distance to the band edge (rout0 - R cancels to a few tenths
-        // of an A, which FP32 R would leave with 1e-5 relative error), the
-        // same expression with or without energies; FP64 where S enters the
-        // energies
+        // two factors taken in FP64, the distance to the band edge (rout0 - R)
+        // and auxa (arsout1 + 2R, where -3 rout and 2R cancel to under a
+        // tenth of their size): FP32 R would leave both with 1e-5 relative
+        // error.  The same expression with or without energies; FP64 where S
+        // enters the energies
         const double rspd = sqrt(drj);
         const float rsp = (float)rspd;
-        const float auxa = ((float)A.arsout1 + 2.0f * rsp) * A.iarsout2;
+        const float auxa = (float)((A.arsout1 + 2.0 * rspd) * A.diarsout2);
         const float auxb = (float)(A.rout0 - rspd);
         sw = auxa * auxb * auxb;
         dsw = (-2.0f * auxa * auxb + 2.0f * auxb * auxb * A.iarsout2) / rsp;
@@ -300,7 +301,7 @@ __global__ void __launch_bounds__(WPB * 32, (MG <= 4 && !EN)
       } else if (drj >= A.r2inn && drj < A.r2inn0) {
         const double rspd = sqrt(drj);
         const float rsp = (float)rspd;
-        const float auxa = ((float)A.arsinn1 + 2.0f * rsp) * A.iarsinn2;
+        const float auxa = (float)((A.arsinn1 + 2.0 * rspd) * A.diarsinn2);
         const float auxb = (float)(A.rinn0 - rspd);
         sw = 1.0f - auxa * auxb * auxb;
         dsw = (2.0f * auxa * auxb - 2.0f * auxb * auxb * A.iarsinn2) / rsp;

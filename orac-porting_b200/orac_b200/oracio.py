@@ -1,0 +1,302 @@
+"""ORAC's topology-parameter and restart files.
+
+ORAC writes its assembled system (`WRITE_TPGPRM`, src/dumptp.f) and its MD
+state (`RESTART write`, src/dumprs.f) as Fortran list-directed ASCII; it
+reads them back with src/readtp.f and src/readrs.f.  This module reads
+both, converts the topology to ORAC's program units the way ORAC does
+after reading (src/covchg.f, src/covbd.f, src/covnb.f, src/setup_box.f
+:412-434), builds a `systems.System` from them, and writes restart files in
+the layout ORAC reads, so a real ORAC system can be run here and its state
+handed back.
+
+List-directed records: each Fortran READ statement starts at a new record
+(line), takes as many values as its list needs across lines, and skips the
+rest of its last line; a READ with an empty list still consumes one line.
+`_Records` follows these rules.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from . import units
+
+
+class _Records:
+    def __init__(self, path):
+        with open(path) as f:
+            self.lines = f.read().split("\n")
+        self.pos = 0
+
+    def read(self, n):
+        """The next n values of one READ statement (strings)."""
+        out = []
+        if n == 0:
+            self.pos += 1
+            return out
+        while len(out) < n:
+            if self.pos >= len(self.lines):
+                raise EOFError("end of file inside a record")
+            for tok in self.lines[self.pos].replace(",", " ").split():
+                if "*" in tok:  # r*c repeat count
+                    r, c = tok.split("*", 1)
+                    out.extend([c] * int(r))
+                else:
+                    out.append(tok)
+            self.pos += 1
+        return out[:n]  # the rest of the last record is skipped
+
+    def ints(self, n):
+        return np.array([int(t) for t in self.read(n)], dtype=np.int64)
+
+    def floats(self, n):
+        return np.array([float(t.replace("D", "E").replace("d", "e")) for t in self.read(n)], dtype=np.float64)
+
+
+def _logical(t):
+    return t.strip().upper().lstrip(".").startswith("T")
+
+
+def read_tpgprm(path, amphi=False):
+    """The topology-parameter file in src/readtp.f's order.  Arrays keep
+    ORAC's 1-based indices and the file's units (charges in e, energies in
+    kcal/mol, angles in degrees)."""
+    r = _Records(path)
+    h = r.read(23)
+    names = ("llacc", "lldon", "nbone", "ntap", "lbond", "lbend", "ltors", "litor", "lpnbd", "int14p", "int13p",
+             "nspw", "nunit", "lphyd", "ngrp", "nrigg", "nrigat", "nmapnl", "nmol", "nato_slv")
+    d = {k: int(v) for k, v in zip(names, h[:20])}
+    d["adihed"], d["slv_exist"], d["slt_exist"] = (_logical(t) for t in h[20:23])
+    N, G, nb, na, nt, ni, npot = d["ntap"], d["ngrp"], d["lbond"], d["lbend"], d["ltors"], d["litor"], d["lpnbd"]
+    sp = r.ints(2)
+    d["ss_point"] = r.ints(int(sp[0]) + int(sp[1]))
+    d["ss_index"] = r.ints(N)
+    r.ints(2 * d["llacc"] + 2 * d["lldon"])  # H-bond acceptors and donors
+    d["nbtype"] = r.ints(N)
+    d["nres1"] = r.ints(N)
+    d["nres2"] = r.ints(N)
+    d["mback"] = r.ints(N)
+    g = r.ints(2 * G)
+    d["grppt"] = np.stack([g[:G], g[G:]], axis=1)
+    b = r.ints(2 * nb)
+    d["lbnd"] = np.stack([b[:nb], b[nb:]], axis=1)
+    # connection table: per atom a count and that many neighbours, one READ
+    conn, buf = [], []
+    while len(conn) < N:
+        while not buf:
+            buf = r.lines[r.pos].split()
+            r.pos += 1
+        k = int(buf.pop(0))
+        while len(buf) < k:
+            buf += r.lines[r.pos].split()
+            r.pos += 1
+        conn.append([int(x) for x in buf[:k]])
+        buf = buf[k:]
+    if buf:
+        raise ValueError("connection table record longer than its counts")
+    d["concta"] = conn
+    d["lbndg"] = r.ints(3 * na).reshape(3, na).T
+    d["ltor"] = r.ints(4 * nt).reshape(4, nt).T
+    d["litr"] = r.ints(4 * ni).reshape(4, ni).T
+    n14, n13 = d["int14p"], d["int13p"]
+    v = r.read(2 * n14 + n14 + 2 * n13 + npot * npot)
+    o = 0
+    d["int14"] = np.array(v[o:o + 2 * n14], dtype=np.int64).reshape(n14, 2)
+    o += 2 * n14
+    d["type14"] = np.array(v[o:o + n14], dtype=np.int64)
+    o += n14
+    d["int13"] = np.array(v[o:o + 2 * n13], dtype=np.int64).reshape(n13, 2)
+    o += 2 * n13
+    d["nhtype"] = np.array(v[o:], dtype=np.int64).reshape(npot, npot)
+    v = r.floats(1 + 2 * N)
+    d["wmtp"], d["chrge"], d["mass"] = v[0], v[1:1 + N], v[1 + N:]
+    d["mapnl"] = r.ints(d["nmapnl"])
+    nbun, iz = r.ints(2)
+    d["nbun"], d["iz"] = int(nbun), int(iz)
+    ntc = 4 if amphi else 2
+    lp = d["lphyd"]
+    cnt = 2 * nb + 7 * na + ntc * nt + 3 * ni + 4 * npot + (2 * npot if amphi else 0) + 2 * lp
+    v = r.floats(cnt)
+    o = 0
+
+    def take(n, w):
+        nonlocal o
+        a = v[o:o + n * w].reshape(w, n).T.copy()  # ((p(i,j),i=1,n),j=1,w)
+        o += n * w
+        return a
+
+    d["potbo"] = take(nb, 2)
+    d["potbe"] = take(na, 7)
+    d["potto"] = take(nt, ntc)
+    d["potit"] = take(ni, 3)
+    d["pnbd"] = take(npot, 4)  # pnbd1..pnbd4 as columns
+    if amphi:
+        d["sjorg"], d["ejorg"] = take(npot, 1)[:, 0], take(npot, 1)[:, 0]
+    if iz == 1:
+        m = npot * (npot + 1) // 2
+        e = r.floats(2 * m)
+        d["ecc6_file"], d["ecc12_file"] = e[:m], e[m:]
+    return d
+
+
+def read_rst(path, ntap=None):
+    """An ORAC restart file (src/readrs.f:216-236): box co and oc, step and
+    temperature, sizes, Cartesian positions and velocities."""
+    r = _Records(path)
+    v = r.floats(18)
+    co = v[:9].reshape(3, 3)  # ((co(i,j),j=1,3),i=1,3): row by row
+    oc = v[9:].reshape(3, 3)
+    t = r.read(2)
+    nstep, temp = int(t[0]), float(t[1].replace("D", "E"))
+    n, ngrp, nprot = (int(x) for x in r.read(3))
+    if ntap is not None and n != ntap:
+        raise ValueError(f"restart holds {n} atoms, the topology {ntap}")
+    big = r.floats(6 * n + 3 * ngrp + 6 * nprot)
+    x = big[:3 * n].reshape(3, n)
+    vel = big[3 * n:6 * n].reshape(3, n)
+    return dict(co=co, oc=oc, nstep=nstep, temp=temp, ntap=n, ngrp=ngrp, nprot=nprot, xyz=x, v=vel)
+
+
+def write_rst(path, co, xyz, v, nstep=0, temp=0.0, grp=None, ngrp=0, mol=None, nprot=0):
+    """A restart file with the records ORAC reads (src/readrs.f:216-244):
+    box, step and temperature, sizes, positions, velocities (twice, as
+    src/dumprs.f writes vpx and vpx1), group and molecule centres (zero when
+    not given), no running averages, no thermostat or barostat state."""
+    co = np.asarray(co, dtype=np.float64)
+    oc = np.linalg.inv(co)
+    n = xyz.shape[1]
+    grp = np.zeros((3, ngrp)) if grp is None else np.asarray(grp)
+    mol = np.zeros((3, nprot)) if mol is None else np.asarray(mol)
+
+    def rec(vals):
+        return " ".join(repr(float(x)) if not isinstance(x, (int, np.integer)) else str(int(x)) for x in vals) + "\n"
+
+    with open(path, "w") as f:
+        f.write(rec(list(co.ravel()) + list(oc.ravel())))
+        f.write(f"{int(nstep)} {float(temp)!r}\n")
+        f.write(f"{n} {ngrp} {nprot}\n")
+        f.write(rec(np.concatenate([xyz.ravel(), v.ravel(), grp.ravel(), mol.ravel(), np.zeros(3 * nprot)])))
+        f.write(rec(v.ravel()))
+        f.write("0 0\n\n")
+        f.write("F F\n")
+        f.write("F\n")
+
+
+def _components(n, pairs):
+    """Connected components of the bond graph (0-based labels by first atom)."""
+    parent = np.arange(n)
+
+    def find(a):
+        while parent[a] != a:
+            parent[a] = parent[parent[a]]
+            a = parent[a]
+        return a
+
+    for a, b in pairs:
+        ra, rb = find(a), find(b)
+        if ra != rb:
+            parent[max(ra, rb)] = min(ra, rb)
+    roots = np.array([find(a) for a in range(n)])
+    _, lab = np.unique(roots, return_inverse=True)
+    return lab
+
+
+def system_from_orac(tp, rst, alphal, nfft, order, shells, ncell, fudge=0.83333, lj_fudge=0.5, name="orac"):
+    """A System from read_tpgprm / read_rst output with ORAC's conversions:
+    charges to program units (src/covchg.f), bonded parameters (src/covbd.f:
+    force constants from kcal/mol, angles of bends and harmonic impropers to
+    radians), LJ tables by the amber mixing rule from the per-type
+    parameters (src/covnb.f, iz = 0) with the 1-4 tables from their own
+    parameters or, where those vanish, lj_fudge times the regular ones.
+    Molecules are the connected components of the bond list; every bond is
+    flexible (constraints are an MD-input choice, not part of the file)."""
+    from . import systems
+
+    N, G = tp["ntap"], tp["ngrp"]
+    if tp["iz"] != 0:
+        raise NotImplementedError("topology without mixing rules (iz = 1)")
+    kconv = 4184.0 / units.EFACT
+    co = np.asarray(rst["co"], dtype=np.float64)
+    xyz = np.asarray(rst["xyz"], dtype=np.float64)
+    scaled = np.linalg.inv(co) @ xyz
+    grppt = tp["grppt"].astype(np.int32)
+    atomg = np.zeros(N, dtype=np.int32)
+    for g, (a, b) in enumerate(grppt):
+        atomg[a - 1:b] = g + 1
+    mol = _components(N, [(a - 1, b - 1) for a, b in tp["lbnd"]])
+    atomp = (mol + 1).astype(np.int32)
+    mass = tp["mass"].astype(np.float64)
+    gm = np.bincount(atomg - 1, weights=mass)
+    pmass = mass / gm[atomg - 1]
+    npot = tp["lpnbd"]
+    pn = tp["pnbd"]
+    fact = 1.0 / (2.0 ** (1.0 / 6.0))
+    e12 = np.zeros(npot * (npot + 1) // 2)
+    e6 = np.zeros_like(e12)
+    e1412 = np.zeros_like(e12)
+    e146 = np.zeros_like(e12)
+    tt = np.zeros((npot, npot), dtype=np.int32)
+    for i in range(npot):
+        for j in range(i, npot):
+            ij = (j + 1) * j // 2 + i  # 0-based of ORAC's j*(j-1)/2 + i
+            tt[i, j] = tt[j, i] = ij + 1
+            qe = math.sqrt(abs(pn[i, 1] * pn[j, 1])) * 4.0 * kconv
+            s6 = ((pn[i, 0] + pn[j, 0]) * fact) ** 6
+            e6[ij], e12[ij] = qe * s6, qe * s6 * s6
+            q4 = math.sqrt(abs(pn[i, 3] * pn[j, 3])) * 4.0 * kconv
+            s46 = ((pn[i, 2] + pn[j, 2]) * fact) ** 6
+            e146[ij], e1412[ij] = q4 * s46, q4 * s46 * s46
+            if abs(e1412[ij]) < 1e-12:
+                e146[ij], e1412[ij] = e6[ij] * lj_fudge, e12[ij] * lj_fudge
+    # non-excluded pairs inside a group (fnbgrp's list, built by ORAC at set-up)
+    mapnl = tp["mapnl"].astype(np.int32)
+    excl = [set() for _ in range(N)]
+    p = 0
+    for a in range(N):
+        k = int(mapnl[p])
+        excl[a].update(int(x) - 1 for x in mapnl[p + 1:p + 1 + k])
+        p += k + 1
+    ingrp = [(i + 1, j + 1) for a, b in grppt for i in range(a - 1, b) for j in range(i + 1, b) if j not in excl[i]]
+    be = tp["potbe"].copy()
+    it = tp["potit"].copy()
+    sysm = systems.System(
+        name=name, ntap=N, ngrp=G, nprot=int(atomp.max()), co=co,
+        xp0=scaled[0].copy(), yp0=scaled[1].copy(), zp0=scaled[2].copy(), mass=mass,
+        charge=np.array([units.charge_internal(q) for q in tp["chrge"]]), nbtype=tp["nbtype"].astype(np.int32),
+        ntype=npot, type_table=tt, ecc12=e12, ecc6=e6, grppt=grppt, atomg=atomg, atomp=atomp,
+        ss_index=tp["ss_index"].astype(np.int32), pmass=pmass, mapnl=mapnl,
+        int14=tp["int14"].astype(np.int32).reshape(-1, 2), type14=tp["type14"].astype(np.int32),
+        ecc1412=e1412, ecc146=e146, ingrp=np.array(ingrp, dtype=np.int32).reshape(-1, 2),
+        bonds=tp["lbnd"].astype(np.int32), bend13=tp["int13"].astype(np.int32).reshape(-1, 2),
+        constraints=np.zeros((0, 2), dtype=np.int32), cdist=np.zeros(0),
+        vx=rst["v"][0].copy(), vy=rst["v"][1].copy(), vz=rst["v"][2].copy(),
+        alphal=alphal, order=order, nfft=tuple(nfft), shells=shells, fudge=fudge, lj_fudge=lj_fudge,
+        ncell=tuple(ncell), lj_params=pn[:, :2].copy(),
+    )
+    # src/covbd.f: energies from kcal/mol, angles from degrees
+    sysm.bond_k = tp["potbo"][:, 0] * kconv
+    sysm.bond_r0 = tp["potbo"][:, 1].copy()
+    sysm.bends = tp["lbndg"].astype(np.int32)
+    sysm.bend_t0 = np.radians(be[:, 1])
+    sysm.bend_k = be[:, 0] * kconv
+    sysm.bend_ub_r0 = be[:, 3].copy()
+    sysm.bend_ub_k = be[:, 2] * kconv
+    sysm.tors = tp["ltor"].astype(np.int32)
+    sysm.tors_k = tp["potto"][:, 0] * kconv
+    sysm.tors_n = tp["potto"][:, 1].copy()
+    sysm.itors = tp["litr"].astype(np.int32)
+    sysm.itors_b = it[:, 0] * kconv
+    sysm.itors_a = np.where(it[:, 2] > 0.0, np.radians(it[:, 1]), it[:, 1])
+    sysm.itors_c = it[:, 2].copy()
+    return sysm
+
+
+def split_arrays(arrs):
+    """(topology, restart) dicts for system_from_orac from one mapping of
+    arrays holding read_tpgprm's and read_rst's fields (a saved fixture)."""
+    tp = {k: (int(arrs[k]) if np.ndim(arrs[k]) == 0 else np.asarray(arrs[k])) for k in arrs
+          if k not in ("co", "xyz", "v", "nstep")}
+    rst = dict(co=np.asarray(arrs["co"]), xyz=np.asarray(arrs["xyz"]), v=np.asarray(arrs["v"]),
+               nstep=int(arrs["nstep"]))
+    return tp, rst
