@@ -50,6 +50,27 @@ WORKLOADS = {
 }
 
 
+def f0_system():
+    """The reference's test1 system as ORAC assembled it (fixture F0:
+    solvated FKBP12 with its ligand, 14,900 atoms, from ORAC's own
+    topology-parameter and restart files), with test1's parameters: SPME
+    alpha 0.37 on 48^3 order 4, shells 5.1/7.8/10.0 A, 18^3 linked cells,
+    bonds to hydrogen rigid (STRETCHING HEAVY)."""
+    from orac_b200 import oracio
+
+    tp, rst = oracio.split_arrays(dict(np.load(os.path.join(ROOT, "tests", "golden", "f0_fkbp12.npz"))))
+    sh = systems.Shells(rcutm=5.1, rtolm=0.3, rneim=0.4, rcutl=7.8, rtoll=0.3, rneil=0.5, rcuth=10.0, rtolh=0.3,
+                        rneih=1.5)
+    return oracio.system_from_orac(tp, rst, alphal=0.37, nfft=(48, 48, 48), order=4, shells=sh, ncell=(18, 18, 18),
+                                   fudge=0.83333, lj_fudge=0.5, name="F0_fkbp12", rigid_hydrogen=True)
+
+
+# the reference's test1 schedule: 15 fs outer step, L 3 fs (SPME), M 1.5 fs,
+# intramolecular 0.75 / 0.375 fs, list update every 6 steps
+F0_WORKLOAD = dict(build=f0_system, dt_h=15.0, lrespa=5, mrespa=2, n1respa=2, n0respa=2, nupdte=6, rshk="l")
+TEST1_PUBLISHED_NS_DAY = 4.41  # test1/md.out:1061,1063: 58.799 s for 3,000 fs, 8 OpenMP threads, NPT
+
+
 def ns_per_day(steps, dt_h_fs, seconds):
     return steps * dt_h_fs * 1e-6 * 86400.0 / seconds
 
@@ -143,6 +164,7 @@ def cpu_run(wl, s, steps, warmup, budget_s=None):
 
     cores = os.cpu_count() or 1
     md = oracle.OracleMD(s, wl["dt_h"], wl["lrespa"], wl["mrespa"], wl["nupdte"], wl["rshk"], nthreads=cores,
+                         n1respa=wl.get("n1respa", 1), n0respa=wl.get("n0respa", 1),
                          econst=0.0)
     if warmup:
         md.run(warmup)
@@ -282,6 +304,11 @@ def gpu_arm(args, wl, s, device):
             res["batched"] = batch_arm(args, wl, s, device, flush)
         except Exception as exc:  # reported in the JSON line; the plain leg stands on its own
             res["batched_error"] = f"{type(exc).__name__}: {exc}"
+    if ws == 1 and args.f0:
+        try:
+            res["orac_test1"] = f0_arm(args, device, flush)
+        except Exception as exc:
+            res["orac_test1"] = {"error": f"{type(exc).__name__}: {exc}"}
     if ws == 1 and args.uneven > 1:
         try:
             res["uneven"] = uneven_arm(args, wl, device, flush)
@@ -523,6 +550,47 @@ def serve_arm(args, wl, device):
                    "server with each request taking 500 x the system's measured single-system step time"}
 
 
+def f0_arm(args, device, flush):
+    """The reference's own test system (F0, test1's schedule and
+    parameters, NVE here) through the device-resident driver; its CPU
+    restatement on the host cores beside it; ORAC's published rate for the
+    same system and schedule (test1) for reference."""
+    import torch
+
+    from orac_b200.engine import Engine
+
+    wl = F0_WORKLOAD
+    s = wl["build"]()
+    e = Engine(s.copy(), device=device)
+    e.md_setup(wl["dt_h"], wl["lrespa"], wl["mrespa"], wl["nupdte"], wl["rshk"], n1respa=wl["n1respa"],
+               n0respa=wl["n0respa"], econst=0.0)
+    L = e.lib
+    st = torch.cuda.ExternalStream(L.orac_gpu_get_stream(e.ctx), device=device)
+    for _ in range(args.warmup):
+        L.orac_gpu_md_run_async(e.ctx, 1)
+    if e.collect():
+        raise RuntimeError(L.orac_gpu_last_error(e.ctx).decode())
+    k = max(3, min(args.steps, 20))
+    ms = _timed_steps(lambda: L.orac_gpu_md_run_async(e.ctx, 1), st, flush, k)
+    if e.collect():
+        raise RuntimeError(L.orac_gpu_last_error(e.ctx).decode())
+    e.close()
+    val = ns_per_day(k, wl["dt_h"], sum(ms) / 1e3)
+    out = {"workload": f"ORAC test1 system as ORAC assembled it (solvated FKBP12 + ligand, {s.ntap} atoms, "
+                       f"{len(s.constraints)} bonds to hydrogen rigid, {len(s.bonds)} flexible), SPME alpha 0.37 48^3 "
+                       "order 4, shells 5.1/7.8/10.0 A, r-RESPA 15/3/1.5/0.75/0.375 fs, NVE",
+           "value": val, "unit": "ns/day", "ms_per_step": sum(ms) / k, "steps": k,
+           "orac_published": {"value": TEST1_PUBLISHED_NS_DAY, "unit": "ns/day",
+                              "how": "ORAC's own run of this system and schedule (test1/md.out:1061,1063), "
+                                     "8 OpenMP threads of an unrecorded CPU, NPT with Nose-Hoover"},
+           "speedup_vs_orac_published": val / TEST1_PUBLISHED_NS_DAY}
+    if not args.no_cpu_baseline:
+        t, done, cores = cpu_run(wl, s, 50, 1, budget_s=args.cpu_budget / 2)
+        out["cpu_restatement"] = {"value": ns_per_day(done, wl["dt_h"], t), "unit": "ns/day", "cores": cores,
+                                  "sample": f"{done} H steps"}
+    return out
+
+
 def profile_window_batch(nwin):
     """One batched step of `nwin` lambda windows bracketed for a profiler
     that starts collecting at cudaProfilerStart (the windows' set-up and
@@ -564,6 +632,7 @@ def main():
     ap.add_argument("--uneven", type=int, default=128, help="systems of the uneven HREM batch (0/1: skip)")
     ap.add_argument("--serve", type=float, default=3.0, help="seconds of Poisson arrivals of the serving leg (0: skip)")
     ap.add_argument("--serve-systems", type=int, default=16, help="systems the serving requests draw from")
+    ap.add_argument("--no-f0", dest="f0", action="store_false", help="skip the ORAC test1 system leg")
     ap.add_argument("--profile-window-batch", type=int, default=0, metavar="N",
                     help="profiling aid, no JSON: N lambda windows batched, 3 steps, then one step bracketed by "
                          "cudaProfilerStart/Stop (ncu --profile-from-start off --graph-profiling graph)")
@@ -669,7 +738,7 @@ def main():
                    "alone through the same driver; dU/dlambda from an energy step at the end of each window"}
     elif "batched_error" in res:
         out["batched"] = {"error": res["batched_error"]}
-    for key in ("uneven", "served"):
+    for key in ("orac_test1", "uneven", "served"):
         if key in res:
             out[key] = res[key]
     print(json.dumps(out))

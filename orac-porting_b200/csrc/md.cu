@@ -31,6 +31,7 @@
 // 1e-8) and one exact linear solve for the RATTLE velocity step.  Larger
 // constrained molecules use the iterative branch (tolerance 1e-8 A^2, 5000
 // iterations, src/rattle_verlet.f:76,209).
+#include <algorithm>
 #include <cmath>
 
 #include "common.cuh"
@@ -101,6 +102,7 @@ struct MolArgs {
   const int* drift_groups;
   int nda;
   const int* drift_atoms;
+  const int* sm_atoms;  // atoms of the constraint clusters
   // state
   double* x;
   double* xo;
@@ -131,6 +133,19 @@ struct MolArgs {
   double tol;
   int* flag;
 };
+
+// a constraint cluster of a large molecule (the atoms joined by one
+// connected set of constraints, at most SMA atoms and SMC constraints):
+// solved like a small molecule, its atoms listed in sm_atoms from m.x, no
+// groups of its own (the molecule's groups are centred after every atom
+// of the molecule has moved)
+constexpr int CLUSTER = 1024;
+
+// atom a of small molecule or constraint cluster m
+__device__ __forceinline__ int sm_atom(const MolArgs& A, const int4& m, int a) {
+  return (m.w & CLUSTER) ? A.sm_atoms[m.x + a] : m.x + a;
+}
+
 
 __device__ __forceinline__ double fixd(unsigned long long v) { return (double)(long long)v * ORAC_FSCALE_INV; }
 
@@ -587,7 +602,7 @@ __global__ void k_kick(const MolArgs A) {
 #pragma unroll
     for (int a = 0; a < SMA; a++) {
       if (a < m.y) {
-        const int g = m.x + a;
+        const int g = sm_atom(A, m, a);
         im[a] = A.invm[g];
         x[a][0] = A.x[g];
         x[a][1] = A.x[N + g];
@@ -607,7 +622,7 @@ __global__ void k_kick(const MolArgs A) {
 #pragma unroll
     for (int a = 0; a < SMA; a++) {
       if (a < m.y) {
-        const int g = m.x + a;
+        const int g = sm_atom(A, m, a);
         A.v[g] = v[a][0];
         A.v[N + g] = v[a][1];
         A.v[2 * N + g] = v[a][2];
@@ -637,7 +652,7 @@ __global__ void k_drift(const MolArgs A) {
 #pragma unroll
     for (int a = 0; a < SMA; a++) {
       if (a < m.y) {
-        const int g = m.x + a;
+        const int g = sm_atom(A, m, a);
         im[a] = A.invm[g];
 #pragma unroll
         for (int d = 0; d < 3; d++) {
@@ -658,7 +673,7 @@ __global__ void k_drift(const MolArgs A) {
 #pragma unroll
     for (int a = 0; a < SMA; a++) {
       if (a < m.y) {
-        const int g = m.x + a;
+        const int g = sm_atom(A, m, a);
 #pragma unroll
         for (int d = 0; d < 3; d++) {
           const double f = (A.fv && nlev == NLV) ? fixd(A.fv[d * N + g]) : 0.0;
@@ -681,7 +696,7 @@ __global__ void k_drift(const MolArgs A) {
 #pragma unroll
     for (int a = 0; a < SMA; a++) {
       if (a < m.y) {
-        const int g = m.x + a;
+        const int g = sm_atom(A, m, a);
 #pragma unroll
         for (int d = 0; d < 3; d++) {
           A.x[d * N + g] = x[a][d];
@@ -875,6 +890,7 @@ struct MdState {
   int* free_groups = nullptr;
   int* drift_groups = nullptr;
   int* drift_atoms = nullptr;
+  int* sm_atoms = nullptr;
   // large constrained molecules
   int nbig = 0;
   int* bstart = nullptr;
@@ -932,7 +948,7 @@ void md_destroy(orac_gpu_ctx* ctx) {
                   S->ffix[4],
                   S->invm,      S->pm,       S->sm,          S->smg,       S->cloc,    S->cdss,    S->free_atoms,
                   S->free_groups, S->bstart, S->bcab,        S->bdss,      S->e,       S->flag,
-                  S->drift_groups, S->drift_atoms};
+                  S->drift_groups, S->drift_atoms, S->sm_atoms};
   for (void* p : ptrs)
     if (p) dev_free(ctx, p);
   delete S;
@@ -956,6 +972,7 @@ static MolArgs mol_args(orac_gpu_ctx* ctx, MdState& S, double dt) {
   A.drift_groups = S.drift_groups;
   A.nda = S.nda;
   A.drift_atoms = S.drift_atoms;
+  A.sm_atoms = S.sm_atoms;
   A.x = S.x;
   A.xo = S.xo;
   A.v = S.v;
@@ -1374,7 +1391,8 @@ int orac_gpu_md_setup(orac_gpu_ctx* ctx, const double* x, const double* y, const
   std::vector<int2> smg, cloc, bcab;
   std::vector<double> cd, bd;
   std::vector<int> bst = {0}, fa, fg;
-  std::vector<char> small(P, 0);
+  std::vector<char> small(P, 0), in_cluster(N, 0);
+  std::vector<int> sm_atoms;
   for (int p = 0; p < P; p++) {
     const int nc = (int)bym[p].size();
     if (nc > 0 && nc <= SMC && mna[p] <= SMA) {
@@ -1404,18 +1422,77 @@ int orac_gpu_md_setup(orac_gpu_ctx* ctx, const double* x, const double* y, const
         }
       }
     } else if (nc > 0) {
+      // a large molecule: its constraints split into connected clusters
+      // (a heavy atom with its hydrogens, typically); those of at most SMA
+      // atoms and SMC constraints are solved like small molecules, the rest
+      // by the iterative SHAKE/RATTLE of large molecules, one unit each.
+      // Clusters share no atom, so this is the same constrained solution.
+      std::vector<int> par(mna[p]);
+      for (int q = 0; q < mna[p]; q++) par[q] = q;
+      auto find = [&](int q) {
+        while (par[q] != q) q = par[q] = par[par[q]];
+        return q;
+      };
       for (int k : bym[p]) {
-        bcab.push_back(make_int2(cnst[2 * k] - 1, cnst[2 * k + 1] - 1));
-        bd.push_back(dss[k]);
+        const int a = find(cnst[2 * k] - 1 - ma0[p]), b = find(cnst[2 * k + 1] - 1 - ma0[p]);
+        if (a != b) par[std::max(a, b)] = std::min(a, b);
       }
-      bst.push_back((int)bcab.size());
+      std::vector<std::vector<int>> comp_c(mna[p]);
+      for (int k : bym[p]) comp_c[find(cnst[2 * k] - 1 - ma0[p])].push_back(k);
+      for (int r = 0; r < mna[p]; r++) {
+        const std::vector<int>& ks = comp_c[r];
+        if (ks.empty()) continue;
+        std::vector<int> atoms;
+        for (int k : ks)
+          for (int e = 0; e < 2; e++) atoms.push_back(cnst[2 * k + e] - 1);
+        std::sort(atoms.begin(), atoms.end());
+        atoms.erase(std::unique(atoms.begin(), atoms.end()), atoms.end());
+        if ((int)atoms.size() <= SMA && (int)ks.size() <= SMC) {
+          auto loc = [&](int a) { return (int)(std::lower_bound(atoms.begin(), atoms.end(), a) - atoms.begin()); };
+          int slot[3] = {-1, -1, -1};
+          if (ks.size() == 3 && atoms.size() == 3)
+            for (int k : ks) {
+              int a = loc(cnst[2 * k] - 1), b = loc(cnst[2 * k + 1] - 1);
+              if (a > b) std::swap(a, b);
+              const int sl = (a == 0 && b == 1) ? 0 : (a == 0 && b == 2) ? 1 : (a == 1 && b == 2) ? 2 : -1;
+              if (sl >= 0) slot[sl] = k;
+            }
+          const bool tri = slot[0] >= 0 && slot[1] >= 0 && slot[2] >= 0;
+          sm.push_back(make_int4((int)sm_atoms.size(), (int)atoms.size(), (int)cloc.size(),
+                                 (int)ks.size() | CLUSTER | (tri ? MOL3 : 0)));
+          smg.push_back(make_int2(0, 0));
+          for (int a : atoms) {
+            sm_atoms.push_back(a);
+            in_cluster[a] = 1;
+          }
+          if (tri) {
+            const int2 pr[3] = {make_int2(0, 1), make_int2(0, 2), make_int2(1, 2)};
+            for (int q = 0; q < 3; q++) {
+              cloc.push_back(pr[q]);
+              cd.push_back(dss[slot[q]]);
+            }
+          } else {
+            for (int k : ks) {
+              cloc.push_back(make_int2(loc(cnst[2 * k] - 1), loc(cnst[2 * k + 1] - 1)));
+              cd.push_back(dss[k]);
+            }
+          }
+        } else {
+          for (int k : ks) {
+            bcab.push_back(make_int2(cnst[2 * k] - 1, cnst[2 * k + 1] - 1));
+            bd.push_back(dss[k]);
+          }
+          bst.push_back((int)bcab.size());
+        }
+      }
     }
   }
   // molecules outside the small ones: unconstrained (drifted by group) or
   // large constrained (drifted by atom, centred after their SHAKE)
   std::vector<int> dg, da;
+  // (atoms of constraint clusters move with their cluster)
   for (int a = 0; a < N; a++)
-    if (!small[ctx->h_amol[a]]) {
+    if (!small[ctx->h_amol[a]] && !in_cluster[a]) {
       fa.push_back(a);
       if (!bym[ctx->h_amol[a]].empty()) da.push_back(a);
     }
@@ -1427,7 +1504,10 @@ int orac_gpu_md_setup(orac_gpu_ctx* ctx, const double* x, const double* y, const
     const bool hb = (int)ctx->h_intra_b.size() == N, hp = (int)ctx->h_intra_p.size() == N;
     for (auto& m : sm) {
       bool any = false;
-      for (int a = m.x; a < m.x + m.y; a++) any = any || (hb && ctx->h_intra_b[a]) || (hp && ctx->h_intra_p[a]);
+      for (int q = 0; q < m.y; q++) {
+        const int a = (m.w & CLUSTER) ? sm_atoms[m.x + q] : m.x + q;
+        any = any || (hb && ctx->h_intra_b[a]) || (hp && ctx->h_intra_p[a]);
+      }
       if (!any) m.w |= NOINTRA;
     }
   }
@@ -1450,6 +1530,7 @@ int orac_gpu_md_setup(orac_gpu_ctx* ctx, const double* x, const double* y, const
   UPV(S.free_groups, fg);
   UPV(S.drift_groups, dg);
   UPV(S.drift_atoms, da);
+  UPV(S.sm_atoms, sm_atoms);
   if (S.nbig) {
     UPV(S.bstart, bst);
     UPV(S.bcab, bcab);

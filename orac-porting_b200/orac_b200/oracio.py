@@ -202,15 +202,20 @@ def _components(n, pairs):
     return lab
 
 
-def system_from_orac(tp, rst, alphal, nfft, order, shells, ncell, fudge=0.83333, lj_fudge=0.5, name="orac"):
+def system_from_orac(tp, rst, alphal, nfft, order, shells, ncell, fudge=0.83333, lj_fudge=0.5, name="orac",
+                     rigid_hydrogen=False):
     """A System from read_tpgprm / read_rst output with ORAC's conversions:
     charges to program units (src/covchg.f), bonded parameters (src/covbd.f:
     force constants from kcal/mol, angles of bends and harmonic impropers to
     radians), LJ tables by the amber mixing rule from the per-type
     parameters (src/covnb.f, iz = 0) with the 1-4 tables from their own
     parameters or, where those vanish, lj_fudge times the regular ones.
-    Molecules are the connected components of the bond list; every bond is
-    flexible (constraints are an MD-input choice, not part of the file)."""
+    Molecules are the connected components of the bond list.  Constraints
+    are an MD-input choice, not part of the file: every bond is flexible,
+    or with rigid_hydrogen every bond to a hydrogen (mass below 1.5 amu) is
+    a constraint at its force-field length (ORAC's `STRETCHING HEAVY` with
+    the bond lengths adjusted to the force field) and leaves the bond
+    list."""
     from . import systems
 
     N, G = tp["ntap"], tp["ngrp"]
@@ -258,6 +263,10 @@ def system_from_orac(tp, rst, alphal, nfft, order, shells, ncell, fudge=0.83333,
         excl[a].update(int(x) - 1 for x in mapnl[p + 1:p + 1 + k])
         p += k + 1
     ingrp = [(i + 1, j + 1) for a, b in grppt for i in range(a - 1, b) for j in range(i + 1, b) if j not in excl[i]]
+    lb = tp["lbnd"]
+    flex = np.ones(len(lb), dtype=bool)
+    if rigid_hydrogen:
+        flex = ~((mass[lb[:, 0] - 1] < 1.5) | (mass[lb[:, 1] - 1] < 1.5))
     be = tp["potbe"].copy()
     it = tp["potit"].copy()
     sysm = systems.System(
@@ -268,15 +277,15 @@ def system_from_orac(tp, rst, alphal, nfft, order, shells, ncell, fudge=0.83333,
         ss_index=tp["ss_index"].astype(np.int32), pmass=pmass, mapnl=mapnl,
         int14=tp["int14"].astype(np.int32).reshape(-1, 2), type14=tp["type14"].astype(np.int32),
         ecc1412=e1412, ecc146=e146, ingrp=np.array(ingrp, dtype=np.int32).reshape(-1, 2),
-        bonds=tp["lbnd"].astype(np.int32), bend13=tp["int13"].astype(np.int32).reshape(-1, 2),
-        constraints=np.zeros((0, 2), dtype=np.int32), cdist=np.zeros(0),
+        bonds=tp["lbnd"][flex].astype(np.int32), bend13=tp["int13"].astype(np.int32).reshape(-1, 2),
+        constraints=tp["lbnd"][~flex].astype(np.int32), cdist=tp["potbo"][~flex, 1].copy(),
         vx=rst["v"][0].copy(), vy=rst["v"][1].copy(), vz=rst["v"][2].copy(),
         alphal=alphal, order=order, nfft=tuple(nfft), shells=shells, fudge=fudge, lj_fudge=lj_fudge,
         ncell=tuple(ncell), lj_params=pn[:, :2].copy(),
     )
     # src/covbd.f: energies from kcal/mol, angles from degrees
-    sysm.bond_k = tp["potbo"][:, 0] * kconv
-    sysm.bond_r0 = tp["potbo"][:, 1].copy()
+    sysm.bond_k = tp["potbo"][flex, 0] * kconv
+    sysm.bond_r0 = tp["potbo"][flex, 1].copy()
     sysm.bends = tp["lbndg"].astype(np.int32)
     sysm.bend_t0 = np.radians(be[:, 1])
     sysm.bend_k = be[:, 0] * kconv

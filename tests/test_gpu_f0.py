@@ -9,15 +9,17 @@ tests/golden/make_f0.py, read by orac_b200.oracio).  The parameters are
 those of the reference's test1 input: SPME alpha 0.37 on 48^3 with order 4,
 shells 5.1/7.8/10.0 A with tolerances 0.3 A and neighbour margins
 0.4/0.5/1.5 A, 18^3 linked cells, 1-4 fudge 0.83333 (Coulomb) and 0.5
-(LJ), r-RESPA 15/3/1.5/0.75/0.375 fs.  Every bond is flexible here
-(constraints are an MD input choice, not part of the files).
+(LJ), r-RESPA 15/3/1.5/0.75/0.375 fs.  Every bond is flexible in the
+force tests; the constrained MD test makes the bonds to hydrogen rigid
+(test1's STRETCHING HEAVY: 14,041 constraints, the protein's through the
+iterative SHAKE/RATTLE of large molecules, the waters' by SETTLE).
 
 Tolerances as in the other parity tests: forces relative RMS <= 1e-5,
 energies <= 1e-6 relative (of the value or of the sum of the shell's term
 magnitudes where the value cancels), stress <= 1e-5 of its norm; FP64
 bonded terms to 1e-10; two MD steps (160 inner steps) agree with the
 oracle's in every energy column to 1e-5 relative and in positions to
-1e-6 A.
+1e-6 A; so do two constrained steps.
 """
 import functools
 import os
@@ -34,12 +36,12 @@ FIX = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "f0_fkb
 
 
 @functools.lru_cache(maxsize=None)
-def f0():
+def f0(rigid_hydrogen=False):
     tp, rst = oracio.split_arrays(dict(np.load(FIX)))
     sh = systems.Shells(rcutm=5.1, rtolm=0.3, rneim=0.4, rcutl=7.8, rtoll=0.3, rneil=0.5, rcuth=10.0, rtolh=0.3,
                         rneih=1.5)
     return oracio.system_from_orac(tp, rst, alphal=0.37, nfft=(48, 48, 48), order=4, shells=sh, ncell=(18, 18, 18),
-                                   fudge=0.83333, lj_fudge=0.5, name="F0_fkbp12")
+                                   fudge=0.83333, lj_fudge=0.5, name="F0_fkbp12", rigid_hydrogen=rigid_hydrogen)
 
 
 def rel_rms(F, Fref):
@@ -98,10 +100,11 @@ def test_f0_intramolecular_parity(pair):
     np.testing.assert_allclose(eg1[2:6], e14, rtol=1e-10, atol=1e-300)
 
 
-def test_f0_md_steps_match_oracle():
+@pytest.mark.parametrize("rigid", [False, True])
+def test_f0_md_steps_match_oracle(rigid):
     from orac_b200.engine import Engine
 
-    s = f0()
+    s = f0(rigid)
     a, b = oracle.Oracle(s.copy()).cself()
     sched = (15.0, 5, 2, 6, "l")
     g = Engine(s.copy())
