@@ -203,7 +203,7 @@ def _components(n, pairs):
 
 
 def system_from_orac(tp, rst, alphal, nfft, order, shells, ncell, fudge=0.83333, lj_fudge=0.5, name="orac",
-                     rigid_hydrogen=False):
+                     rigid_hydrogen=False, move_fast_torsions=True):
     """A System from read_tpgprm / read_rst output with ORAC's conversions:
     charges to program units (src/covchg.f), bonded parameters (src/covbd.f:
     force constants from kcal/mol, angles of bends and harmonic impropers to
@@ -215,7 +215,9 @@ def system_from_orac(tp, rst, alphal, nfft, order, shells, ncell, fudge=0.83333,
     or with rigid_hydrogen every bond to a hydrogen (mass below 1.5 amu) is
     a constraint at its force-field length (ORAC's `STRETCHING HEAVY` with
     the bond lengths adjusted to the force field) and leaves the bond
-    list."""
+    list.  With move_fast_torsions (ORAC's default) the fast proper
+    torsions become cosine impropers as ORAC's MD driver makes them
+    (fast_torsions)."""
     from . import systems
 
     N, G = tp["ntap"], tp["ngrp"]
@@ -291,14 +293,39 @@ def system_from_orac(tp, rst, alphal, nfft, order, shells, ncell, fudge=0.83333,
     sysm.bend_k = be[:, 0] * kconv
     sysm.bend_ub_r0 = be[:, 3].copy()
     sysm.bend_ub_k = be[:, 2] * kconv
-    sysm.tors = tp["ltor"].astype(np.int32)
-    sysm.tors_k = tp["potto"][:, 0] * kconv
-    sysm.tors_n = tp["potto"][:, 1].copy()
-    sysm.itors = tp["litr"].astype(np.int32)
-    sysm.itors_b = it[:, 0] * kconv
-    sysm.itors_a = np.where(it[:, 2] > 0.0, np.radians(it[:, 1]), it[:, 1])
-    sysm.itors_c = it[:, 2].copy()
+    ltor, litr, to = tp["ltor"], tp["litr"], tp["potto"]
+    fast = fast_torsions(ltor, to, mass) if move_fast_torsions else np.zeros(len(ltor), dtype=bool)
+    sysm.tors = ltor[~fast].astype(np.int32)
+    sysm.tors_k = to[~fast, 0] * kconv
+    sysm.tors_n = to[~fast, 1].copy()
+    # moved torsions follow the file's impropers as cosine impropers (c = -1)
+    sysm.itors = np.concatenate([litr, ltor[fast]]).astype(np.int32)
+    sysm.itors_b = np.concatenate([it[:, 0], to[fast, 0]]) * kconv
+    sysm.itors_a = np.concatenate([np.where(it[:, 2] > 0.0, np.radians(it[:, 1]), it[:, 1]), to[fast, 1]])
+    sysm.itors_c = np.concatenate([it[:, 2], np.full(int(fast.sum()), -1.0)])
     return sysm
+
+
+def fast_torsions(ltor, potto, mass):
+    """ORAC's run-time move of "fast" proper torsions into the improper
+    list (src/mtsmd.f:990-1030, on unless the integrator input says
+    `no_adjust_itors`): a torsion whose uncoupled frequency
+    sqrt(tfactor k / mu) n / (2 pi c) exceeds 300 cm^-1 is evaluated by
+    fitors as a cosine improper (potc = -1) at the fastest intramolecular
+    level instead of by fptors.  k is the barrier in kcal/mol, n the signed
+    multiplicity (a negative n never moves), mu = (m1 + m4) sin^2(60 deg)
+    with m = 1 for an end atom whose type name starts with "h" and 12
+    otherwise; the file carries masses, not type names, and here a
+    hydrogen is an atom below 1.5 amu.  The literals keep ORAC's
+    precisions (0.001 and 3.14 are single-precision constants in the
+    Fortran).  Returns a mask over the torsions."""
+    tfactor = 4.0 * 4.184e3 * 1.0e20 / float(np.float32(0.001))
+    m1 = np.where(mass[ltor[:, 0] - 1] < 1.5, 1.0, 12.0)
+    m4 = np.where(mass[ltor[:, 3] - 1] < 1.5, 1.0, 12.0)
+    xmu = (m1 + m4) * math.sin(3.14 / 3.0) ** 2
+    naux = np.rint(potto[:, 1])
+    freq = np.sqrt(tfactor * np.abs(potto[:, 0]) / xmu) * naux / (3.0e10 * 2 * float(np.float32(3.14)))
+    return freq > 300.0
 
 
 def split_arrays(arrs):

@@ -6,10 +6,16 @@ wrote (test2/b-RSTRT/ij4i0000.rst, step 30).  Only the arrays the force
 path needs are kept, in the files' own units and 1-based indices;
 orac_b200.oracio.system_from_orac turns them into a System.
 
+Also builds tests/golden/f0_orac_records.npz: the positions and boxes of
+test2's other two replica-1 restart files (ij4i0001.rst, ij4i0003.rst) and,
+for all three states, the energy record ORAC printed at the step it wrote
+the restart (test2/PAR0001/out0001, matched by box edge and temperature).
+
 Run from the repository root where the reference checkout is present:
     python tests/golden/make_f0.py [reference root]
 """
 import os
+import re
 import sys
 
 import numpy as np
@@ -34,12 +40,64 @@ def build_arrays(root):
     return out
 
 
+# columns of ORAC's energy record (src/prtacc.f, format 12002) kept for the
+# states of the restart files, in kJ/mol (TotTemp in K)
+RECORD_KEYS = ("SlvNonbd", "SlvCoul", "SltCoul", "SltL-J", "SltBond", "SltStr", "SltBen", "SltItor", "SltPtor",
+               "S-SPot", "S-SCoul", "TotTemp")
+RESTARTS = ("ij4i0000.rst", "ij4i0001.rst", "ij4i0003.rst")
+
+
+def parse_records(path):
+    """Every energy record of an ORAC output: (box edge from the XYZ line
+    that follows it, {column: value}, line number)."""
+    lines = open(path).read().splitlines()
+    out, cur = [], None
+    for k, line in enumerate(lines):
+        if "Tstep    =" in line:
+            cur = ({}, k + 1)
+        if cur is not None:
+            for key, val in re.findall(r"(\S+)\s*=\s*(-?[\d.]+)", line):
+                cur[0].setdefault(key, float(val))
+            if line.startswith(" XYZ"):
+                out.append((float(line.split()[1]), cur[0], cur[1]))
+                cur = None
+    return out
+
+
+def build_records(root, ntap):
+    """The replica-1 states that test2 saved as restart files with the
+    energy record ORAC printed for the same step (matched by box edge and
+    temperature): positions and box of each, and the record's columns."""
+    recs = parse_records(os.path.join(root, "test2", "PAR0001", "out0001"))
+    out = {"keys": np.array(RECORD_KEYS), "restarts": np.array(RESTARTS)}
+    vals, where = [], []
+    for k, name in enumerate(RESTARTS):
+        rs = oracio.read_rst(os.path.join(root, "test2", "b-RSTRT", name), ntap)
+        edge = 2.0 * rs["co"][0, 0]
+        hit = [(d, ln) for e, d, ln in recs if abs(e - edge) < 6e-5 and abs(d["TotTemp"] - rs["temp"]) < 6e-3]
+        if len(hit) != 1:
+            raise RuntimeError(f"{name}: {len(hit)} matching records")
+        d, ln = hit[0]
+        vals.append([d[c] for c in RECORD_KEYS])
+        where.append(ln)
+        if k > 0:  # the first state is f0_fkbp12.npz's own
+            out[f"co{k}"] = rs["co"]
+            out[f"xyz{k}"] = rs["xyz"]
+    out["printed"] = np.array(vals)
+    out["out0001_line"] = np.array(where)
+    return out
+
+
 def main():
     root = sys.argv[1] if len(sys.argv) > 1 else DEFAULT_ROOT
     arrs = build_arrays(root)
     path = os.path.join(HERE, "f0_fkbp12.npz")
     np.savez_compressed(path, **arrs)
     print(path, os.path.getsize(path), "bytes")
+    recs = build_records(root, int(arrs["ntap"]))
+    path = os.path.join(HERE, "f0_orac_records.npz")
+    np.savez_compressed(path, **recs)
+    print(path, os.path.getsize(path), "bytes", "records at out0001 lines", list(recs["out0001_line"]))
 
 
 if __name__ == "__main__":

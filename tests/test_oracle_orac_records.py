@@ -1,0 +1,118 @@
+"""The oracle against energies ORAC itself printed: parity pinned on the
+reference's own outputs.
+
+test2 of the reference (solvated FKBP12-ligand, 14,900 atoms) saved three
+restart files of its unscaled replica (b-RSTRT/ij4i0000, 0001, 0003.rst);
+at each of those steps the replica's output (PAR0001/out0001, lines 818,
+903 and 1068) prints an energy record (src/prtacc.f, format 12002) of the
+same state: the restart's box edge and temperature match the record's.
+tests/golden/f0_orac_records.npz holds the three states' positions and
+those records (tests/golden/make_f0.py builds it from the reference's
+files).  The oracle evaluates each state with test2's parameters and the
+record's bookkeeping (src/add_energies.f: with SPME and both species the
+reciprocal energy goes to the solute-solvent columns; each species'
+Coulomb column carries its self energy and the erf corrections of its
+constraints, bonds, 1-3 and fudged 1-4 pairs, src/mts_furier.f:104-130).
+
+- Bonded columns (SltStr, SltBen, SltItor, SltPtor): equal to the printed
+  two decimals at all three states (|d| <= 0.006 kJ/mol), which pins the
+  bonded restatement, the conversion of ORAC's files and ORAC's run-time
+  move of 49 fast proper torsions into the improper list (388 impropers,
+  as the replica's topology table prints at out0001 line 664).
+- Nonbonded columns: SlvNonbd, SlvCoul, SltCoul and SltL-J agree to
+  1e-3 of the value; S-SCoul (solute-solvent real-space Coulomb plus the
+  whole SPME reciprocal energy) is 27-39 kJ/mol (0.7-1.3 %) above the
+  printed value at every state, while the oracle's SPME converges to the
+  direct Ewald sum (test_oracle.py) and the three shells add up to one
+  full-range call exactly; the residual is an open item and the tolerance
+  states it.
+"""
+import functools
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from orac_b200 import oracio, systems, units
+
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+K = units.KJMOL
+
+
+@functools.lru_cache(maxsize=None)
+def records():
+    r = np.load(os.path.join(GOLD, "f0_orac_records.npz"))
+    return {k: r[k] for k in r.files}
+
+
+@functools.lru_cache(maxsize=None)
+def state(k):
+    tp, rst = oracio.split_arrays(dict(np.load(os.path.join(GOLD, "f0_fkbp12.npz"))))
+    if k > 0:
+        r = records()
+        rst = dict(rst, co=r[f"co{k}"], xyz=r[f"xyz{k}"])
+    sh = systems.Shells(rcutm=5.1, rtolm=0.3, rneim=0.4, rcutl=7.8, rtoll=0.3, rneil=0.5, rcuth=10.0, rtolh=0.3,
+                        rneih=1.5)
+    return oracio.system_from_orac(tp, rst, alphal=0.37, nfft=(48, 48, 48), order=4, shells=sh, ncell=(18, 18, 18),
+                                   fudge=0.83333, lj_fudge=0.5, name=f"F0_{k}", rigid_hydrogen=True)
+
+
+def printed(k):
+    r = records()
+    return dict(zip([str(x) for x in r["keys"]], r["printed"][k]))
+
+
+def orac_columns(s):
+    """The oracle's values of the record's columns (kJ/mol)."""
+    o = oracle.Oracle(s.copy())
+    o.update_lists()
+    ue = np.zeros(6)  # LJ slt, slv, slt-slv; Coulomb slt, slv, slt-slv
+    for sh in "mlh":
+        ue += o.shell(sh)[1]
+    erec = o.fft_pme()[1]
+    self_slt, self_slv = o.cself()
+    corr = o.ferrf(s.constraints, 1.0, iz=0)[1] + o.ferrf(s.bonds, 1.0)[1] + o.ferrf(s.bend13, 1.0)[1] \
+        + o.ferrf(s.int14, 1.0 - s.fudge)[1]
+    e14 = o.fnb14()[1]  # LJ slt, slv; Coulomb slt, slv
+    egrp = o.fnbgrp()[1]
+    _, en0 = o.intra_n0()
+    _, et = o.intra_torsions()
+    c = {
+        "SlvCoul": ue[4] + self_slv + corr[1] + e14[3] + egrp[3],
+        "SltCoul": ue[3] + self_slt + corr[0] + e14[2] + egrp[2],
+        "SltL-J": ue[0] + e14[0] + egrp[0],
+        "S-SCoul": ue[5] + erec,
+        "S-SPot": ue[2] + ue[5] + erec,
+        "SltStr": en0["bond"][0],
+        "SltBen": en0["bend"][0],
+        "SltItor": en0["itors"][0],
+        "SltPtor": et[0],
+    }
+    c["SlvNonbd"] = c["SlvCoul"] + ue[1] + e14[1] + egrp[1]
+    return {k: v * K for k, v in c.items()}
+
+
+def test_fast_torsions_are_moved_as_orac_moves_them():
+    s = state(0)
+    assert len(s.itors) == 388 and len(s.tors) == 5732 - 49
+    assert np.all(s.itors_c[339:] == -1.0)
+
+
+@pytest.mark.parametrize("k", [0, 1, 2])
+def test_bonded_columns_equal_the_printed_record(k):
+    c, p = orac_columns(state(k)), printed(k)
+    for col in ("SltStr", "SltBen", "SltItor", "SltPtor"):
+        assert abs(c[col] - p[col]) <= 0.006, (col, c[col], p[col])
+
+
+@pytest.mark.parametrize("k", [0, 1, 2])
+def test_nonbonded_columns_agree_with_the_printed_record(k):
+    c, p = orac_columns(state(k)), printed(k)
+    for col in ("SlvNonbd", "SlvCoul", "SltCoul", "SltL-J"):
+        assert abs(c[col] - p[col]) <= 1e-3 * abs(p[col]), (col, c[col], p[col])
+    # the open residual: the oracle's solute-solvent Coulomb sits above
+    # ORAC's by 0.7-1.3 % at these states
+    d = c["S-SCoul"] - p["S-SCoul"]
+    assert 0.0 < d <= 0.015 * abs(p["S-SCoul"]), (c["S-SCoul"], p["S-SCoul"])
+    assert abs((c["S-SPot"] - c["S-SCoul"]) - (p["S-SPot"] - p["S-SCoul"])) <= 2e-3 * abs(p["S-SPot"] - p["S-SCoul"])
