@@ -41,7 +41,12 @@ def test_f0_fixture_builds_the_real_system():
     assert (s.ss_index == 1).sum() == 1715
     assert int((s.grppt[:, 1] - s.grppt[:, 0] + 1).max()) == 4
     assert abs(s.charge.sum()) < 1e-3 * np.abs(s.charge).sum() / len(s.charge)
-    assert len(s.int14) == 4500 and len(s.tors) == 5732 and len(s.itors) == 339
+    # the file's 5,732 proper and 339 improper torsions; ORAC's MD driver
+    # moves 49 fast propers to the impropers (its topology table: 388)
+    assert len(s.int14) == 4500 and len(s.tors) == 5732 - 49 and len(s.itors) == 388
+    s0 = oracio.system_from_orac(tp, rst, alphal=0.37, nfft=(48, 48, 48), order=4, shells=sh, ncell=(18, 18, 18),
+                                 move_fast_torsions=False)
+    assert len(s0.tors) == 5732 and len(s0.itors) == 339
     # box from the restart: cubic, 54.616 A
     assert np.allclose(np.diag(s.co) * 2.0, 54.616, atol=1e-3)
     # the positions come back through the scaled frame
