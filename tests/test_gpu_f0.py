@@ -100,6 +100,27 @@ def test_f0_intramolecular_parity(pair):
     np.testing.assert_allclose(eg1[2:6], e14, rtol=1e-10, atol=1e-300)
 
 
+def test_f0_bonded_energies_equal_orac_printed_record():
+    """The CUDA bonded levels at F0's state against the energy record ORAC
+    printed for it (test2/PAR0001/out0001 line 818, kept in
+    tests/golden/f0_orac_records.npz), with bonds to hydrogen rigid as in
+    that run: stretching, bending, improper and proper torsion energies equal
+    the printed two decimals."""
+    from orac_b200 import units
+    from orac_b200.engine import Engine
+
+    rec = np.load(os.path.join(os.path.dirname(FIX), "f0_orac_records.npz"))
+    p = dict(zip([str(k) for k in rec["keys"]], rec["printed"][0]))
+    g = Engine(f0(True).copy())
+    _, e0 = g.intra_n0()
+    _, e1 = g.intra_n1()
+    g.close()
+    K = units.KJMOL
+    got = {"SltStr": e0[0] * K, "SltBen": e0[2] * K, "SltItor": e0[4] * K, "SltPtor": e1[0] * K}
+    for col, v in got.items():
+        assert abs(v - p[col]) <= 0.006, (col, v, p[col])
+
+
 @pytest.mark.parametrize("rigid", [False, True])
 def test_f0_md_steps_match_oracle(rigid):
     from orac_b200.engine import Engine
