@@ -116,3 +116,39 @@ def test_nonbonded_columns_agree_with_the_printed_record(k):
     d = c["S-SCoul"] - p["S-SCoul"]
     assert 0.0 < d <= 0.015 * abs(p["S-SCoul"]), (c["S-SCoul"], p["S-SCoul"])
     assert abs((c["S-SPot"] - c["S-SCoul"]) - (p["S-SPot"] - p["S-SCoul"])) <= 2e-3 * abs(p["S-SPot"] - p["S-SCoul"])
+
+
+def test_solute_solvent_real_space_equals_a_direct_pair_sum():
+    """The oracle's real-space solute-solvent Coulomb of the M and L shells
+    at F0's state against a direct sum written from the definitions alone:
+    every solute-solvent atom pair, group centres (mass-weighted) under the
+    minimum image, ORAC's cubic switch of the L shell's outer edge
+    (7.8-8.1 A, src/force.f:164-165) and the A&S erfc with the
+    coefficients of ORAC's DATA statements (src/force.f:123-125)."""
+    s = state(0)
+    x = s.cartesian().T
+    q, g = np.asarray(s.charge), np.asarray(s.atomg) - 1
+    gc = np.zeros((s.ngrp, 3))
+    np.add.at(gc, g, np.asarray(s.pmass)[:, None] * x)
+    off = x - gc[g]
+    box = 2.0 * np.diag(np.asarray(s.co))
+    slt, slv = np.where(s.ss_index == 1)[0], np.where(s.ss_index == 2)[0]
+    rin, r0 = 7.8, 8.1
+
+    def erfc_as(z):
+        t = 1.0 / (1.0 + 0.3275911 * z)
+        return ((((1.0614054 * t - 1.453152) * t + 1.4214137) * t - 0.28449674) * t + 0.2548296) * t * np.exp(-z * z)
+
+    e = 0.0
+    for i in slt:
+        d = gc[g[slv]] - gc[g[i]]
+        d -= box * np.rint(d / box)
+        R = np.sqrt((d ** 2).sum(1))
+        m = R < r0
+        S = np.where(R[m] < rin, 1.0, ((r0 - 3.0 * rin) + 2.0 * R[m]) * (r0 - R[m]) ** 2 / (r0 - rin) ** 3)
+        r = np.sqrt(((d[m] + off[slv[m]] - off[i]) ** 2).sum(1))
+        e += (S * q[i] * q[slv[m]] * erfc_as(s.alphal * r) / r).sum()
+    o = oracle.Oracle(s.copy())
+    o.update_lists()
+    ue = o.shell("m")[1] + o.shell("l")[1]
+    assert abs(ue[5] - e) <= 1e-9 * abs(e), (ue[5] * K, e * K)
