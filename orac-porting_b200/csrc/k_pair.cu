@@ -439,11 +439,13 @@ __global__ void __launch_bounds__(WPB * 32, (MG <= 4 && !EN)
         fix_add(A.ffix + 2 * A.natom + jfirst + b, fbz);
       }
       if (switched) {
-        pconf *= swd;
-        pcoul *= swd;
-        px0 *= swd;
-        px1 *= swd;
-        px2 *= swd;
+        if constexpr (EN) {
+          pconf *= swd;
+          pcoul *= swd;
+          px0 *= swd;
+          px1 *= swd;
+          px2 *= swd;
+        }
         // S'(R) V term: X = -dS/dR / R * V * R_vec on i atoms by mass fraction
         const float sx = -dsw * vsum * dcx, sy = -dsw * vsum * dcy,
                     sz = -dsw * vsum * dcz;
@@ -465,21 +467,23 @@ __global__ void __launch_bounds__(WPB * 32, (MG <= 4 && !EN)
         gy -= sy;
         gz -= sz;
       }
-      const int t = typei + typej - 2;  // 0 slt-slt, 1 slt-slv, 2 slv-slv
-      if (t == 0) {
-        ec0 += pconf;
-        eq0 += pcoul;
-      } else if (t == 1) {
-        ec1 += pconf;
-        eq1 += pcoul;
-      } else {
-        ec2 += pconf;
-        eq2 += pcoul;
+      if constexpr (EN) {
+        const int t = typei + typej - 2;  // 0 slt-slt, 1 slt-slv, 2 slv-slv
+        if (t == 0) {
+          ec0 += pconf;
+          eq0 += pcoul;
+        } else if (t == 1) {
+          ec1 += pconf;
+          eq1 += pcoul;
+        } else {
+          ec2 += pconf;
+          eq2 += pcoul;
+        }
+        ex0 += px0;
+        ex1 += px1;
+        ex2 += px2;
       }
-      ex0 += px0;
-      ex1 += px1;
-      ex2 += px2;
-      if (A.stress && (imx != 0.0 || imy != 0.0 || imz != 0.0)) {
+      if (EN && A.stress && (imx != 0.0 || imy != 0.0 || imz != 0.0)) {
         // j sits at its image xpg_j + img: its virial arm gains co.img
         const float ix = (float)(A.c11 * imx + A.c12 * imy + A.c13 * imz);
         const float iy = (float)(A.c22 * imy + A.c23 * imz);
@@ -524,7 +528,7 @@ __global__ void __launch_bounds__(WPB * 32, (MG <= 4 && !EN)
       const bool inb = valid && band(drj, switched, sw, dsw, swd);
       if constexpr (!COMPACT) {
         if (inb) work(j, msk, mj, cx, cy, cz, imx, imy, imz, switched, sw, dsw, swd);
-        if (A.stress) flush_vimg();
+        if (EN && A.stress) flush_vimg();
       } else {
         // queue the in-band entries; a full queue runs on every lane
         const unsigned bq = __ballot_sync(0xffffffffu, inb);
@@ -536,7 +540,7 @@ __global__ void __launch_bounds__(WPB * 32, (MG <= 4 && !EN)
           geometry(kq, j, msk, mj, drj, cx, cy, cz, imx, imy, imz);
           band(drj, switched, sw, dsw, swd);
           work(j, msk, mj, cx, cy, cz, imx, imy, imz, switched, sw, dsw, swd);
-          if (A.stress) flush_vimg();
+          if (EN && A.stress) flush_vimg();
           __syncwarp();
           if (lane < qn - 32) s_q[warp][lane] = s_q[warp][32 + lane];
           qn -= 32;
@@ -558,7 +562,7 @@ __global__ void __launch_bounds__(WPB * 32, (MG <= 4 && !EN)
         work(j, msk, mj, cx, cy, cz, imx, imy, imz, switched, sw, dsw, swd);
       }
       __syncwarp();
-      if (A.stress) flush_vimg();
+      if (EN && A.stress) flush_vimg();
     }
     if (A.next_on && sl == 0 && gvalid) {
       A.cnt_out[i] = nout;
@@ -599,7 +603,9 @@ __global__ void __launch_bounds__(WPB * 32, (MG <= 4 && !EN)
       if (s2) atomicAdd(A.wcnt + (A.lskip ? 3 : 2), (unsigned long long)s2);
     }
   }
-  if (!A.forces_on || (!EN && !A.stress)) return;
+  // energies and the image virial: the EN build only (a stress request
+  // selects it, pair_launch)
+  if (!EN || !A.forces_on) return;
   // block reduction of energies and image virial
   constexpr int NV = (VAR != VAR_STD && EN) ? 18 : 15;
   double vals[18] = {ec0, ec1, ec2, eq0, eq1, eq2, 0, 0, 0, 0, 0, 0, 0, 0, 0, ex0, ex1, ex2};
@@ -718,8 +724,9 @@ int pair_launch(orac_gpu_ctx* ctx, const PairArgs& a, int maxg) {
   if (nb < 1) nb = 1;
   int slot = -1;
   if (int rc = prof_begin(ctx, &slot)) return rc;
-  const bool hi = a.occ_hi && !a.energy && mgk < 2;
-  switch ((((mgk * 3 + a.variant) * 2 + (a.energy ? 1 : 0)) * 2 + (half ? 1 : 0)) * 2 + (hi ? 1 : 0)) {
+  const bool en = a.energy || a.stress;  // the forces-only build keeps no sums
+  const bool hi = a.occ_hi && !en && mgk < 2;
+  switch ((((mgk * 3 + a.variant) * 2 + (en ? 1 : 0)) * 2 + (half ? 1 : 0)) * 2 + (hi ? 1 : 0)) {
 #define ORAC_KP(MGK, MG, VAR, EN, LPG, HI)                                                     \
   case (((MGK * 3 + VAR) * 2 + (EN ? 1 : 0)) * 2 + (LPG == 16 ? 1 : 0)) * 2 + (HI ? 1 : 0):     \
     orac_launch(k_pair<MG, EN, VAR, LPG, HI>, nb, WPB * 32, smem, ctx->stream, a);                      \
