@@ -192,7 +192,7 @@ __global__ void __launch_bounds__(WPB * 32, (MG <= 4 && !EN)
   __shared__ int s_q[COMPACT ? WPB : 1][64];
   extern __shared__ float2 s_lj[];
   __shared__ float4 s_ai[WPB * SEG][MG];
-  __shared__ int s_ti[WPB * SEG][MG];
+  __shared__ int s_ti[WPB * SEG][MG];  // the i atom's row of the LJ tables (type * ntype)
   __shared__ float s_pm[WPB * SEG][MG];
   __shared__ double s_qd[WPB * SEG][MG];
   __shared__ int s_fi[WPB * SEG][MG];
@@ -238,7 +238,7 @@ __global__ void __launch_bounds__(WPB * 32, (MG <= 4 && !EN)
     const double4 gi = gvalid ? A.gpos[i] : make_double4(0, 0, 0, 0);
     if (sl < ni) {
       s_ai[slot][sl] = A.aoff[ifirst + sl];
-      s_ti[slot][sl] = A.atype[ifirst + sl];
+      s_ti[slot][sl] = A.atype[ifirst + sl] * A.ntype;
       s_pm[slot][sl] = A.apm[ifirst + sl];
       if (EN) s_qd[slot][sl] = A.qd[ifirst + sl];
       if (VAR != VAR_STD) s_fi[slot][sl] = A.vflag[ifirst + sl];
@@ -327,7 +327,11 @@ __global__ void __launch_bounds__(WPB * 32, (MG <= 4 && !EN)
       float gx = 0.f, gy = 0.f, gz = 0.f;  // total force on the j group
       // under lskip_ewald an atom without LJ has no pair to evaluate
       const bool ljonly = VAR != VAR_ALCH && A.lskip && A.ewald;
-      for (int b = 0; b < nj; b++) {
+      // unrolled to the groups' size bound: constant offsets, shifts and
+      // mask bits, and the j atoms' loads issued together
+#pragma unroll
+      for (int b = 0; b < MG; b++) {
+        if (b >= nj) break;
         if (ljonly && !((ljmj >> b) & 1)) continue;
         const float4 ob = A.aoff[jfirst + b];
         const int tb = A.atype[jfirst + b];
@@ -360,7 +364,7 @@ __global__ void __launch_bounds__(WPB * 32, (MG <= 4 && !EN)
             rz = dcz + ai.z - ob.z;
             alch_pair_f32(A, rx * rx + ry * ry + rz * rz, tal, sa.x, sfb.x, eps4, ai.w * ob.w, &qf, &conf, &coul);
           } else {
-            const float2 L = lj[s_ti[slot][a] * A.ntype + tb];
+            const float2 L = lj[s_ti[slot][a] + tb];
             ljon = L.y != 0.f;
             if (A.lskip && !ljon && A.ewald) continue;  // src/force.f:416-417
             npairs++;
@@ -416,7 +420,7 @@ __global__ void __launch_bounds__(WPB * 32, (MG <= 4 && !EN)
               px1 += q0;
               px2 += du;
             } else {
-              pair_energy_fp64(A, erx, ery, erz, A.ljd[s_ti[slot][a] * A.ntype + tb], ljon, s_qd[slot][a] * qbd, &cd,
+              pair_energy_fp64(A, erx, ery, erz, A.ljd[s_ti[slot][a] + tb], ljon, s_qd[slot][a] * qbd, &cd,
                                &qd);
               if (sel) px0 += cd + qd;  // seg_ene
             }
