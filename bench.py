@@ -615,6 +615,29 @@ def profile_window_batch(nwin):
     return 0
 
 
+def profile_f0(nsteps):
+    """`nsteps` MD steps of the test1 system (F0) bracketed for a profiler
+    that starts collecting at cudaProfilerStart (set-up and three warm-up
+    steps stay outside)."""
+    import torch
+
+    from orac_b200.engine import Engine
+
+    wl = F0_WORKLOAD
+    e = Engine(wl["build"]().copy())
+    e.md_setup(wl["dt_h"], wl["lrespa"], wl["mrespa"], wl["nupdte"], wl["rshk"], n1respa=wl["n1respa"],
+               n0respa=wl["n0respa"], econst=0.0)
+    e.md_run(3)
+    torch.cuda.synchronize()
+    torch.cuda.profiler.start()
+    e.md_run(nsteps)
+    torch.cuda.synchronize()
+    torch.cuda.profiler.stop()
+    rc = e.collect()
+    e.close()
+    return rc
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -636,10 +659,15 @@ def main():
     ap.add_argument("--profile-window-batch", type=int, default=0, metavar="N",
                     help="profiling aid, no JSON: N lambda windows batched, 3 steps, then one step bracketed by "
                          "cudaProfilerStart/Stop (ncu --profile-from-start off --graph-profiling graph)")
+    ap.add_argument("--profile-f0", type=int, default=0, metavar="N",
+                    help="profiling aid, no JSON: the test1 system, 3 steps, then N steps bracketed by "
+                         "cudaProfilerStart/Stop (ncu --profile-from-start off)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.profile_window_batch > 0:
         return profile_window_batch(args.profile_window_batch)
+    if args.profile_f0 > 0:
+        return profile_f0(args.profile_f0)
     wl = WORKLOADS[args.workload]
     ws, rank, local = dist_info()
     s = wl["build"]()

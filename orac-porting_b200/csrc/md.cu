@@ -130,6 +130,7 @@ struct MolArgs {
   // accumulators zeroed for the evaluations that follow this drift
   unsigned long long* fz[NLV];
   double dt;
+  double idt;  // 1 / dt, 0 for a zero step
   double tol;
   int* flag;
 };
@@ -464,9 +465,10 @@ __device__ __forceinline__ void cross3(const double* a, const double* b, double*
 }
 
 __device__ bool settle3(double x[SMA][3], const double xo[SMA][3], double v[SMA][3], const double im[SMA],
-                        const double* L2, double dt) {
-  const double mA = 1.0 / im[0], mB = 1.0 / im[1];
-  const double M = mA + 2.0 * mB, wA = mA / M, wB = mB / M;
+                        const double* L2, double idt) {
+  // mass fractions from the inverse masses: mA / (mA + 2 mB) = imB / (imB + 2 imA)
+  const double iM = 1.0 / (im[1] + 2.0 * im[0]);
+  const double wA = im[1] * iM, wB = im[0] * iM;
   const double rc = 0.5 * sqrt(L2[2]);
   const double h2 = L2[0] - rc * rc;
   if (!(h2 > 0.0)) return false;
@@ -487,7 +489,7 @@ __device__ bool settle3(double x[SMA][3], const double xo[SMA][3], double v[SMA]
   cross3(ez, ex, ey);
   const double nz = dot3(ez, ez), nx = dot3(ex, ex), ny = dot3(ey, ey);
   if (!(nz > 0.0 && nx > 0.0 && ny > 0.0)) return false;
-  const double iz = 1.0 / sqrt(nz), ix = 1.0 / sqrt(nx), iy = 1.0 / sqrt(ny);
+  const double iz = rsqrt(nz), ix = rsqrt(nx), iy = rsqrt(ny);
 #pragma unroll
   for (int k = 0; k < 3; k++) {
     ez[k] *= iz;
@@ -519,7 +521,6 @@ __device__ bool settle3(double x[SMA][3], const double xo[SMA][3], double v[SMA]
   const double p[3][3] = {{-a2y * sth, a2y * cth, a2z},
                           {b2x * cth - b2y * sth, b2x * sth + b2y * cth, b2z},
                           {c2x * cth - c2y * sth, c2x * sth + c2y * cth, c2z}};
-  const double idt = dt != 0.0 ? 1.0 / dt : 0.0;
 #pragma unroll
   for (int a = 0; a < 3; a++)
 #pragma unroll
@@ -686,7 +687,7 @@ __global__ void k_drift(const MolArgs A) {
       const double* L2 = A.dss + m.z;
       // isosceles with equal masses at the base: SETTLE, else Newton steps
       const bool iso = im[1] == im[2] && fabs(L2[0] - L2[1]) <= 1e-12 * L2[0];
-      if (!(iso ? settle3(x, xo, v, im, L2, dt) : shake3(x, xo, v, im, L2, dt, A.tol))) atomicOr(A.flag, 1);
+      if (!(iso ? settle3(x, xo, v, im, L2, A.idt) : shake3(x, xo, v, im, L2, dt, A.tol))) atomicOr(A.flag, 1);
       if (!rattle3(x, v, im)) atomicOr(A.flag, 1);
     } else if (nc > 0) {
       if (!shake_small(x, xo, v, im, A.cloc + m.z, A.dss + m.z, nc, dt, A.tol)) atomicOr(A.flag, 1);
@@ -999,6 +1000,7 @@ static MolArgs mol_args(orac_gpu_ctx* ctx, MdState& S, double dt) {
   A.gpos = ctx->d_gpos;
   A.aoff = ctx->d_aoff;
   A.dt = dt;
+  A.idt = dt != 0.0 ? 1.0 / dt : 0.0;
   A.tol = 1e-12;
   A.flag = S.flag;
   return A;
