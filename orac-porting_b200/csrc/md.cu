@@ -335,6 +335,120 @@ __device__ __forceinline__ bool shake_small(double x[SMA][3], const double xo[SM
   return ok;
 }
 
+// Star clusters: a centre atom (local 0) bonded by constraint k to atom k+1
+// (a heavy atom with its hydrogens).  The same Newton SHAKE and exact
+// RATTLE as shake_small / rattle_small with the topology known at compile
+// time: J_kl = 2 (im_0 + [k == l] im_{k+1}) d_k . r0_l.
+template <int NC>
+__device__ __forceinline__ bool solve_n(double A[NC][NC], double b[NC]) {
+#pragma unroll
+  for (int k = 0; k < NC; k++) {
+    if (A[k][k] == 0.0) return false;
+    const double inv = 1.0 / A[k][k];
+#pragma unroll
+    for (int i = k + 1; i < NC; i++) {
+      const double f = A[i][k] * inv;
+#pragma unroll
+      for (int j = k; j < NC; j++) A[i][j] -= f * A[k][j];
+      b[i] -= f * b[k];
+    }
+  }
+#pragma unroll
+  for (int k = NC - 1; k >= 0; k--) {
+    double t = b[k];
+#pragma unroll
+    for (int j = k + 1; j < NC; j++) t -= A[k][j] * b[j];
+    b[k] = t / A[k][k];
+  }
+  return true;
+}
+
+template <int NC>
+__device__ __forceinline__ bool shake_star(double x[SMA][3], const double xo[SMA][3], double v[SMA][3],
+                                           const double im[SMA], const double* L2, double idt, double tol) {
+  double r0[NC][3], lam[NC];
+#pragma unroll
+  for (int k = 0; k < NC; k++) {
+    lam[k] = 0.0;
+#pragma unroll
+    for (int d = 0; d < 3; d++) r0[k][d] = xo[0][d] - xo[k + 1][d];
+  }
+  bool ok = false;
+  for (int it = 0; it < 50; it++) {
+    double dk[NC][3], g[NC], gmax = 0.0;
+#pragma unroll
+    for (int k = 0; k < NC; k++) {
+#pragma unroll
+      for (int d = 0; d < 3; d++) dk[k][d] = x[0][d] - x[k + 1][d];
+      g[k] = -(dot3(dk[k], dk[k]) - L2[k]);
+      gmax = fmax(gmax, fabs(g[k]));
+    }
+    if (gmax < tol) {
+      ok = true;
+      break;
+    }
+    double J[NC][NC];
+#pragma unroll
+    for (int k = 0; k < NC; k++)
+#pragma unroll
+      for (int l = 0; l < NC; l++) J[k][l] = 2.0 * (im[0] + (k == l ? im[k + 1] : 0.0)) * dot3(dk[k], r0[l]);
+    if (!solve_n<NC>(J, g)) return false;
+#pragma unroll
+    for (int l = 0; l < NC; l++) {
+      lam[l] += g[l];
+#pragma unroll
+      for (int d = 0; d < 3; d++) {
+        x[0][d] += g[l] * r0[l][d] * im[0];
+        x[l + 1][d] -= g[l] * r0[l][d] * im[l + 1];
+      }
+    }
+  }
+#pragma unroll
+  for (int l = 0; l < NC; l++)
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      v[0][d] += lam[l] * r0[l][d] * im[0] * idt;
+      v[l + 1][d] -= lam[l] * r0[l][d] * im[l + 1] * idt;
+    }
+  return ok;
+}
+
+template <int NC>
+__device__ __forceinline__ bool rattle_star(const double x[SMA][3], double v[SMA][3], const double im[SMA]) {
+  double r[NC][3], rhs[NC], M[NC][NC];
+#pragma unroll
+  for (int k = 0; k < NC; k++) {
+#pragma unroll
+    for (int d = 0; d < 3; d++) r[k][d] = x[0][d] - x[k + 1][d];
+    rhs[k] = -(r[k][0] * (v[0][0] - v[k + 1][0]) + r[k][1] * (v[0][1] - v[k + 1][1]) +
+               r[k][2] * (v[0][2] - v[k + 1][2]));
+  }
+#pragma unroll
+  for (int k = 0; k < NC; k++)
+#pragma unroll
+    for (int l = 0; l < NC; l++) M[k][l] = (im[0] + (k == l ? im[k + 1] : 0.0)) * dot3(r[k], r[l]);
+  if (!solve_n<NC>(M, rhs)) return false;
+#pragma unroll
+  for (int l = 0; l < NC; l++)
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      v[0][d] += rhs[l] * r[l][d] * im[0];
+      v[l + 1][d] -= rhs[l] * r[l][d] * im[l + 1];
+    }
+  return true;
+}
+
+__device__ __forceinline__ bool rattle_star_n(int nc, const double x[SMA][3], double v[SMA][3],
+                                              const double im[SMA]) {
+  return nc == 1 ? rattle_star<1>(x, v, im) : (nc == 2 ? rattle_star<2>(x, v, im) : rattle_star<3>(x, v, im));
+}
+
+__device__ __forceinline__ bool shake_star_n(int nc, double x[SMA][3], const double xo[SMA][3], double v[SMA][3],
+                                             const double im[SMA], const double* L2, double idt, double tol) {
+  return nc == 1 ? shake_star<1>(x, xo, v, im, L2, idt, tol)
+                 : (nc == 2 ? shake_star<2>(x, xo, v, im, L2, idt, tol) : shake_star<3>(x, xo, v, im, L2, idt, tol));
+}
+
 // Rigid three-atom molecules (the waters) with constraints (0,1), (0,2),
 // (1,2) in this order: the same Newton SHAKE and exact RATTLE as above with
 // the constraint topology fixed at compile time and the 3x3 systems solved
@@ -343,6 +457,8 @@ __device__ __forceinline__ bool shake_small(double x[SMA][3], const double xo[SM
 constexpr int MOL3 = 256;
 // a small molecule none of whose atoms has an intramolecular-level term
 constexpr int NOINTRA = 512;
+// a star cluster (shake_star / rattle_star): centre first, constraints (0, k+1)
+constexpr int STAR = 2048;
 
 __device__ __forceinline__ bool solve3x3(const double J[3][3], const double g[3], double out[3]) {
   const double c00 = J[1][1] * J[2][2] - J[1][2] * J[2][1];
@@ -618,7 +734,9 @@ __global__ void k_kick(const MolArgs A) {
         v[a][0] = v[a][1] = v[a][2] = 0;
       }
     }
-    const bool ok = (m.w & MOL3) ? rattle3(x, v, im) : rattle_small(x, v, im, A.cloc + m.z, m.w & 0xff);
+    const bool ok = (m.w & MOL3)   ? rattle3(x, v, im)
+                    : (m.w & STAR) ? rattle_star_n(m.w & 0xff, x, v, im)
+                                   : rattle_small(x, v, im, A.cloc + m.z, m.w & 0xff);
     if (!ok) atomicOr(A.flag, 1);
 #pragma unroll
     for (int a = 0; a < SMA; a++) {
@@ -670,7 +788,9 @@ __global__ void k_drift(const MolArgs A) {
     const int nc = m.w & 0xff;
     const bool mol3 = (m.w & MOL3) != 0;
     if (A.kick && nc > 0)
-      if (!(mol3 ? rattle3(xo, v, im) : rattle_small(xo, v, im, A.cloc + m.z, nc))) atomicOr(A.flag, 1);
+      if (!(mol3 ? rattle3(xo, v, im)
+                 : ((m.w & STAR) ? rattle_star_n(nc, xo, v, im) : rattle_small(xo, v, im, A.cloc + m.z, nc))))
+        atomicOr(A.flag, 1);
 #pragma unroll
     for (int a = 0; a < SMA; a++) {
       if (a < m.y) {
@@ -689,6 +809,9 @@ __global__ void k_drift(const MolArgs A) {
       const bool iso = im[1] == im[2] && fabs(L2[0] - L2[1]) <= 1e-12 * L2[0];
       if (!(iso ? settle3(x, xo, v, im, L2, A.idt) : shake3(x, xo, v, im, L2, dt, A.tol))) atomicOr(A.flag, 1);
       if (!rattle3(x, v, im)) atomicOr(A.flag, 1);
+    } else if (m.w & STAR) {
+      if (!shake_star_n(nc, x, xo, v, im, A.dss + m.z, A.idt, A.tol)) atomicOr(A.flag, 1);
+      if (!rattle_star_n(nc, x, v, im)) atomicOr(A.flag, 1);
     } else if (nc > 0) {
       if (!shake_small(x, xo, v, im, A.cloc + m.z, A.dss + m.z, nc, dt, A.tol)) atomicOr(A.flag, 1);
       if (!rattle_small(x, v, im, A.cloc + m.z, nc)) atomicOr(A.flag, 1);
@@ -1460,14 +1583,36 @@ int orac_gpu_md_setup(orac_gpu_ctx* ctx, const double* x, const double* y, const
               if (sl >= 0) slot[sl] = k;
             }
           const bool tri = slot[0] >= 0 && slot[1] >= 0 && slot[2] >= 0;
+          // a star: one atom in every constraint and one constraint per
+          // other atom; listed centre first, constraint k to atom k + 1
+          int centre = -1;
+          if (!tri && (int)ks.size() == (int)atoms.size() - 1)
+            for (int a : atoms) {
+              bool all = true;
+              for (int k : ks) all = all && (cnst[2 * k] - 1 == a || cnst[2 * k + 1] - 1 == a);
+              if (all) {
+                centre = a;
+                break;
+              }
+            }
+          if (centre >= 0) {
+            atoms.clear();
+            atoms.push_back(centre);
+            for (int k : ks) atoms.push_back(cnst[2 * k] - 1 == centre ? cnst[2 * k + 1] - 1 : cnst[2 * k] - 1);
+          }
           sm.push_back(make_int4((int)sm_atoms.size(), (int)atoms.size(), (int)cloc.size(),
-                                 (int)ks.size() | CLUSTER | (tri ? MOL3 : 0)));
+                                 (int)ks.size() | CLUSTER | (tri ? MOL3 : 0) | (centre >= 0 ? STAR : 0)));
           smg.push_back(make_int2(0, 0));
           for (int a : atoms) {
             sm_atoms.push_back(a);
             in_cluster[a] = 1;
           }
-          if (tri) {
+          if (centre >= 0) {
+            for (int q = 0; q < (int)ks.size(); q++) {
+              cloc.push_back(make_int2(0, q + 1));
+              cd.push_back(dss[ks[q]]);
+            }
+          } else if (tri) {
             const int2 pr[3] = {make_int2(0, 1), make_int2(0, 2), make_int2(1, 2)};
             for (int q = 0; q < 3; q++) {
               cloc.push_back(pr[q]);
