@@ -103,36 +103,44 @@ __device__ bool torsion_geom(const BondedArgs& A, int4 l, bool absq, double* coa
   const double rsq21 = d21[0] * d21[0] + d21[1] * d21[1] + d21[2] * d21[2];
   const double rsq32 = d32[0] * d32[0] + d32[1] * d32[1] + d32[2] * d32[2];
   const double rsq43 = d43[0] * d43[0] + d43[1] * d43[1] + d43[2] * d43[2];
-  const double rsp21 = sqrt(rsq21), rsp32 = sqrt(rsq32), rsp43 = sqrt(rsq43);
-  const double cb1 = (d21[0] * d32[0] + d21[1] * d32[1] + d21[2] * d32[2]) / (rsp21 * rsp32);
-  const double cb2 = (d43[0] * d32[0] + d43[1] * d32[1] + d43[2] * d32[2]) / (rsp43 * rsp32);
-  const double cb3 = (d21[0] * d43[0] + d21[1] * d43[1] + d21[2] * d43[2]) / (rsp21 * rsp43);
-  const double sb1 = sqrt(absq ? fabs(1.0 - cb1 * cb1) : 1.0 - cb1 * cb1);
-  const double sb2 = sqrt(absq ? fabs(1.0 - cb2 * cb2) : 1.0 - cb2 * cb2);
-  const double sb3 = sqrt(absq ? fabs(1.0 - cb3 * cb3) : 1.0 - cb3 * cb3);
+  // every quotient of the reference's expressions as a product of
+  // reciprocal square roots: 1/|r| for the three bonds and 1/sin for the
+  // three angles (a zero or negative 1 - cos^2 gives inf or NaN, which the
+  // degeneracy test below rejects as it rejects a zero sine)
+  const double ir21 = rsqrt(rsq21), ir32 = rsqrt(rsq32), ir43 = rsqrt(rsq43);
+  const double cb1 = (d21[0] * d32[0] + d21[1] * d32[1] + d21[2] * d32[2]) * (ir21 * ir32);
+  const double cb2 = (d43[0] * d32[0] + d43[1] * d32[1] + d43[2] * d32[2]) * (ir43 * ir32);
+  const double cb3 = (d21[0] * d43[0] + d21[1] * d43[1] + d21[2] * d43[2]) * (ir21 * ir43);
+  const double q1 = absq ? fabs(1.0 - cb1 * cb1) : 1.0 - cb1 * cb1;
+  const double q2 = absq ? fabs(1.0 - cb2 * cb2) : 1.0 - cb2 * cb2;
+  const double q3 = absq ? fabs(1.0 - cb3 * cb3) : 1.0 - cb3 * cb3;
+  const double is1 = rsqrt(q1), is2 = rsqrt(q2), is3 = rsqrt(q3);
+  const double sb1 = q1 * is1, sb2 = q2 * is2, sb3 = q3 * is3;
   const double aux = sb1 * sb2;
   if (!(fabs(aux * sb3) >= 1e-25)) return false;
-  double c = (cb1 * cb2 - cb3) / aux;
+  const double iaux = is1 * is2;
+  double c = (cb1 * cb2 - cb3) * iaux;
   if (c > 1.0 && c < 1.000001) c = 1.0;
   if (c < -1.0 && c > -1.000001) c = -1.0;
-  double aux1 = cb1 * sb2, aux2 = sb1 * cb2;
-  const double auxa = -(aux1 * c + aux2) / aux;
-  const double auxb = -(aux2 * c + aux1) / aux;
-  const double auxc = sb3 / aux;
-  aux1 = rsp21 * rsp32 * sb1;
-  aux2 = rsp32 * rsp43 * sb2;
-  const double aux3 = rsp21 * rsp43 * sb3;
+  const double aux1 = cb1 * sb2, aux2 = sb1 * cb2;
+  const double auxa = -(aux1 * c + aux2) * iaux;
+  const double auxb = -(aux2 * c + aux1) * iaux;
+  const double auxc = sb3 * iaux;
+  const double ia1 = ir21 * ir32 * is1, ia2 = ir32 * ir43 * is2, ia3 = ir21 * ir43 * is3;
+  const double c1a = cb1 * ir21 * ir21 * is1, c1b = cb1 * ir32 * ir32 * is1;
+  const double c2a = cb2 * ir32 * ir32 * is2, c2b = cb2 * ir43 * ir43 * is2;
+  const double c3a = cb3 * ir21 * ir21 * is3, c3b = cb3 * ir43 * ir43 * is3;
 #pragma unroll
   for (int k = 0; k < 3; k++) {
     const double v21 = d21[k], v32 = d32[k], v43 = d43[k];
-    const double b11 = v32 / aux1 - cb1 * v21 / (rsq21 * sb1);
-    const double b13 = -v21 / aux1 + cb1 * v32 / (rsq32 * sb1);
+    const double b11 = v32 * ia1 - c1a * v21;
+    const double b13 = -v21 * ia1 + c1b * v32;
     const double b12 = -b13 - b11;
-    const double b22 = v43 / aux2 - cb2 * v32 / (rsq32 * sb2);
-    const double b24 = -v32 / aux2 + cb2 * v43 / (rsq43 * sb2);
+    const double b22 = v43 * ia2 - c2a * v32;
+    const double b24 = -v32 * ia2 + c2b * v43;
     const double b23 = -b22 - b24;
-    const double b31 = v43 / aux3 - cb3 * v21 / (rsq21 * sb3);
-    const double b33 = v21 / aux3 - cb3 * v43 / (rsq43 * sb3);
+    const double b31 = v43 * ia3 - c3a * v21;
+    const double b33 = v21 * ia3 - c3b * v43;
     g[0][k] = auxa * b11 + auxc * b31;
     g[1][k] = auxa * b12 + auxb * b22 - auxc * b31;
     g[2][k] = auxa * b13 + auxb * b23 + auxc * b33;
@@ -164,6 +172,7 @@ __global__ void k_bonded(const BondedArgs A) {
     pos(A, l.x, ra);
     pos(A, l.y, rb);
     const double x21 = rb[0] - ra[0], y21 = rb[1] - ra[1], z21 = rb[2] - ra[2];
+    // correctly rounded: near its minimum (r - r0)^2 cancels to a few ulp of r
     const double rs21 = sqrt(x21 * x21 + y21 * y21 + z21 * z21);
     const double qforce = -2.0 * p.y * (p.x - rs21) / rs21;
     put(A, l.x, qforce * x21, qforce * y21, qforce * z21);
@@ -186,8 +195,9 @@ __global__ void k_bonded(const BondedArgs A) {
       const double d32[3] = {r3[0] - r2[0], r3[1] - r2[1], r3[2] - r2[2]};
       const double rs12 = d12[0] * d12[0] + d12[1] * d12[1] + d12[2] * d12[2];
       const double rs32 = d32[0] * d32[0] + d32[1] * d32[1] + d32[2] * d32[2];
-      const double dcc2 = sqrt(rs12 * rs32);
-      double cb = (d12[0] * d32[0] + d12[1] * d32[1] + d12[2] * d32[2]) / dcc2;
+      const double ir12 = rsqrt(rs12), ir32 = rsqrt(rs32), idcc2 = ir12 * ir32;
+      const double irs12 = ir12 * ir12, irs32 = ir32 * ir32;
+      double cb = (d12[0] * d32[0] + d12[1] * d32[1] + d12[2] * d32[2]) * idcc2;
       if (fabs(cb) > 1.0) cb = cb > 0 ? 1.0 : -1.0;
       const double sb = sqrt(1.0 - cb * cb);
       const double bb = acos(cb);
@@ -196,8 +206,8 @@ __global__ void k_bonded(const BondedArgs A) {
       double u1[3], u3[3];
 #pragma unroll
       for (int k = 0; k < 3; k++) {
-        u1[k] = d32[k] / dcc2 - cb * d12[k] / rs12;
-        u3[k] = d12[k] / dcc2 - cb * d32[k] / rs32;
+        u1[k] = d32[k] * idcc2 - cb * d12[k] * irs12;
+        u3[k] = d12[k] * idcc2 - cb * d32[k] * irs32;
       }
       put(A, l.x, qforce * u1[0], qforce * u1[1], qforce * u1[2]);
       put(A, l.z, qforce * u3[0], qforce * u3[1], qforce * u3[2]);

@@ -1176,7 +1176,11 @@ static int md_kick(orac_gpu_ctx* ctx, MdState& S, const double* c) {
 // [kick c + RATTLE] + verlet drift of dt (with the N0 half kick when
 // present) + SHAKE + RATTLE, scaled frame and pair-kernel inputs; zeroes the
 // accumulators of the levels in `zmask` (bit l) after reading them
-static int md_drift(orac_gpu_ctx* ctx, MdState& S, double dt, const double* c, int zmask) {
+// groups: the drift precedes a shell evaluation, so the groups of large
+// molecules need their centres (the pair kernels' inputs; the
+// intramolecular levels read atom positions only), as ORAC calls appbou
+// only before the M forces (src/mtsmd.f:2952)
+static int md_drift(orac_gpu_ctx* ctx, MdState& S, double dt, const double* c, int zmask, bool groups = true) {
   if (S.nbig && c) {
     // the RATTLE of large molecules is a separate kernel: kick first
     if (int rc = md_kick(ctx, S, c)) return rc;
@@ -1195,7 +1199,7 @@ static int md_drift(orac_gpu_ctx* ctx, MdState& S, double dt, const double* c, i
     orac_launch(k_rattle_big, (S.nbig + 127) / 128, 128, 0, ctx->stream, big_args(ctx, S, dt, 1e-12));
     CKL();
   }
-  if (S.nfreeg) {
+  if (S.nfreeg && groups) {
     orac_launch(k_free_groups, (S.nfreeg + 31) / 32, 32, 0, ctx->stream, A);
     CKL();
   }
@@ -1367,7 +1371,7 @@ static int md_step(orac_gpu_ctx* ctx, MdState& S, bool update, bool energy) {
     int zmask = 0;
     for (int l = 0; l < NLV; l++)
       if ((k + 1) % per[l] == 0) zmask |= 1 << l;
-    if (int rc = md_drift(ctx, S, dt[LN0], c, zmask)) return rc;
+    if (int rc = md_drift(ctx, S, dt[LN0], c, zmask, (k + 1) % per[LM] == 0)) return rc;
     const bool last = k == K - 1;
     const bool e_now = energy && last;
     const bool due_n1 = S.has_n1 && (k + 1) % per[LN1] == 0;
