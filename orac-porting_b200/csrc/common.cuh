@@ -449,9 +449,11 @@ int small_launch_x(orac_gpu_ctx* ctx, int kind, const double* d_xyz, const int* 
                    int coul_mode, int forces, double* d_f, double* d_e, const int* d_ss, const double* d_q,
                    unsigned long long* d_ffix, const double* d_dq = nullptr, double* d_edq = nullptr);
 // k_bonded.cu: mask of BK_* kinds; forces into d_f (FP64 atomics) or d_ffix
-// (fixed point); d_e[8] (bond, bend, tors, itors) x (slt, slv) or null
+// (fixed point; the proper torsions into d_ffix_tors when given, so one
+// launch serves two r-RESPA levels); d_e[8] (bond, bend, tors, itors) x
+// (slt, slv) or null
 int bonded_launch(orac_gpu_ctx* ctx, int mask, const double* d_x, double* d_f, unsigned long long* d_ffix,
-                  double* d_e);
+                  double* d_e, unsigned long long* d_ffix_tors = nullptr);
 void bonded_free(orac_gpu_ctx* ctx);
 int bonded_set_constraints(orac_gpu_ctx* ctx, const int* cnst, int ncnst);
 // api.cu

@@ -33,17 +33,20 @@ struct BondedArgs {
   const double4* ipar;
   double* f;                  // [3N] FP64 output, or
   unsigned long long* ffix;   // [3N] fixed-point output
+  unsigned long long* ffix_t; // [3N] fixed-point output of the proper torsions (their own r-RESPA level)
   double* e;                  // [8] (bond, bend, tors, itors) x (slt, slv), or null
 };
 
+template <bool TORS = false>
 __device__ __forceinline__ void put(const BondedArgs& A, int a, double fx, double fy, double fz) {
-  if (A.ffix) {
+  unsigned long long* ff = TORS ? A.ffix_t : A.ffix;
+  if (ff) {
     long long q = __double2ll_rn(fx * ORAC_FSCALE);
-    if (q) atomicAdd(A.ffix + a, (unsigned long long)q);
+    if (q) atomicAdd(ff + a, (unsigned long long)q);
     q = __double2ll_rn(fy * ORAC_FSCALE);
-    if (q) atomicAdd(A.ffix + A.N + a, (unsigned long long)q);
+    if (q) atomicAdd(ff + A.N + a, (unsigned long long)q);
     q = __double2ll_rn(fz * ORAC_FSCALE);
-    if (q) atomicAdd(A.ffix + 2 * A.N + a, (unsigned long long)q);
+    if (q) atomicAdd(ff + 2 * A.N + a, (unsigned long long)q);
   } else {
     atomicAdd(A.f + a, fx);
     atomicAdd(A.f + A.N + a, fy);
@@ -262,10 +265,10 @@ __global__ void k_bonded(const BondedArgs A) {
       cheb(n, coa, &tt, &dt);
       const double qforce = sig * dt * p.y;
       e[4 + A.ss[l.x] - 1] += sig * (fabs(p.y) - tt * p.y);
-      put(A, l.x, qforce * g[0][0], qforce * g[0][1], qforce * g[0][2]);
-      put(A, l.y, qforce * g[1][0], qforce * g[1][1], qforce * g[1][2]);
-      put(A, l.z, qforce * g[2][0], qforce * g[2][1], qforce * g[2][2]);
-      put(A, l.w, qforce * g[3][0], qforce * g[3][1], qforce * g[3][2]);
+      put<true>(A, l.x, qforce * g[0][0], qforce * g[0][1], qforce * g[0][2]);
+      put<true>(A, l.y, qforce * g[1][0], qforce * g[1][1], qforce * g[1][2]);
+      put<true>(A, l.z, qforce * g[2][0], qforce * g[2][1], qforce * g[2][2]);
+      put<true>(A, l.w, qforce * g[3][0], qforce * g[3][1], qforce * g[3][2]);
     }
   }
   t -= A.nt;
@@ -337,7 +340,7 @@ __global__ void k_bonded(const BondedArgs A) {
 }  // namespace
 
 int bonded_launch(orac_gpu_ctx* ctx, int mask, const double* d_x, double* d_f, unsigned long long* d_ffix,
-                  double* d_e) {
+                  double* d_e, unsigned long long* d_ffix_tors) {
   const BondedDev& B = ctx->bd;
   BondedArgs A;
   memset(&A, 0, sizeof(A));
@@ -359,6 +362,7 @@ int bonded_launch(orac_gpu_ctx* ctx, int mask, const double* d_x, double* d_f, u
   A.ipar = B.ipar;
   A.f = d_f;
   A.ffix = d_ffix;
+  A.ffix_t = d_ffix_tors ? d_ffix_tors : d_ffix;
   A.e = d_e;
   const int n = B.nb + B.nbend + B.nt + B.nit;
   if (n == 0) return ORAC_OK;

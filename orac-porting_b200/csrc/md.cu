@@ -131,6 +131,7 @@ struct MolArgs {
   unsigned long long* fz[NLV];
   double dt;
   double idt;  // 1 / dt, 0 for a zero step
+  int groups;  // group centres and pair-kernel inputs wanted (a shell evaluation follows)
   double tol;
   int* flag;
 };
@@ -835,7 +836,7 @@ __global__ void k_drift(const MolArgs A) {
         s[a][2] = A.o33 * x[a][2];
       }
     }
-    const int2 gg = A.smg[t];
+    const int2 gg = A.groups ? A.smg[t] : make_int2(0, 0);
     for (int gi = gg.x; gi < gg.x + gg.y; gi++) {
       const int2 mg = A.gmeta[gi];
       double c[3] = {0, 0, 0};
@@ -868,7 +869,7 @@ __global__ void k_drift(const MolArgs A) {
     const int gi = A.drift_groups[t - A.nsm];
     const int2 mg = A.gmeta[gi];
     for (int a = mg.x; a < mg.x + (mg.y & 0xff); a++) drift_atom(A, a, dt);
-    group_centre(A, gi);
+    if (A.groups) group_centre(A, gi);
   } else if (t < A.nsm + A.ndg + A.nda) {
     drift_atom(A, A.drift_atoms[t - A.nsm - A.ndg], dt);
   }
@@ -1124,6 +1125,7 @@ static MolArgs mol_args(orac_gpu_ctx* ctx, MdState& S, double dt) {
   A.aoff = ctx->d_aoff;
   A.dt = dt;
   A.idt = dt != 0.0 ? 1.0 / dt : 0.0;
+  A.groups = 1;
   A.tol = 1e-12;
   A.flag = S.flag;
   return A;
@@ -1187,6 +1189,7 @@ static int md_drift(orac_gpu_ctx* ctx, MdState& S, double dt, const double* c, i
     c = nullptr;
   }
   MolArgs A = mol_args(ctx, S, dt);
+  A.groups = groups ? 1 : 0;
   kick_fill(A, S, c);
   A.fv = S.has_n0 ? S.ffix[LN0] : nullptr;
   for (int l = 0; l < NLV; l++) A.fz[l] = ((zmask >> l) & 1) ? S.ffix[l] : nullptr;
@@ -1298,11 +1301,9 @@ struct SideStream {
 };
 
 // mts_intra_n0 / mts_intra_n1 into their level accumulators
-static int md_forces_intra(orac_gpu_ctx* ctx, MdState& S, int lvl, bool energy) {
+// 1-4 and intra-group pairs of the N1 level (fnb14, fnbgrp)
+static int md_pairs_n1(orac_gpu_ctx* ctx, MdState& S, bool energy) {
   const BondedDev& B = ctx->bd;
-  if (lvl == LN0)
-    return bonded_launch(ctx, BK_BOND | BK_BEND | BK_ITORS, S.x, nullptr, S.ffix[LN0], energy ? S.e + E_BOND : nullptr);
-  if (int rc = bonded_launch(ctx, BK_TORS, S.x, nullptr, S.ffix[LN1], energy ? S.e + E_BOND : nullptr)) return rc;
   if (B.have_pairs) {
     const int coul = ctx->clewld ? 1 : 0;
     if (B.n14 > 0)
@@ -1315,6 +1316,19 @@ static int md_forces_intra(orac_gpu_ctx* ctx, MdState& S, int lvl, bool energy) 
         return rc;
   }
   return ORAC_OK;
+}
+
+// the bonded terms of the N0 level (stretching, bending, impropers) and/or
+// the N1 level (proper torsions) in one launch, each into its accumulator
+static int md_bonded(orac_gpu_ctx* ctx, MdState& S, bool n0, bool n1, bool energy) {
+  const int mask = (n0 ? BK_BOND | BK_BEND | BK_ITORS : 0) | (n1 ? BK_TORS : 0);
+  if (!mask) return ORAC_OK;
+  return bonded_launch(ctx, mask, S.x, nullptr, S.ffix[LN0], energy ? S.e + E_BOND : nullptr, S.ffix[LN1]);
+}
+
+static int md_forces_intra(orac_gpu_ctx* ctx, MdState& S, int lvl, bool energy) {
+  if (int rc = md_bonded(ctx, S, lvl == LN0, lvl == LN1, energy)) return rc;
+  return lvl == LN1 ? md_pairs_n1(ctx, S, energy) : ORAC_OK;
 }
 
 static int md_phony(orac_gpu_ctx* ctx, const ShellRadii& r, char sh) {
@@ -1384,10 +1398,7 @@ static int md_step(orac_gpu_ctx* ctx, MdState& S, bool update, bool energy) {
     if (side) {
       if (int rc = sd.fork()) return rc;
       if (int rc = sd.run([&]() -> int {
-            if (S.has_n0)
-              if (int r2 = md_forces_intra(ctx, S, LN0, e_now)) return r2;
-            if (due_n1)
-              if (int r2 = md_forces_intra(ctx, S, LN1, e_now)) return r2;
+            if (int r2 = md_bonded(ctx, S, S.has_n0, due_n1, e_now)) return r2;
             if (due_m)
               if (int r2 = md_shell_recip(ctx, S, 'm', LM, e_now)) return r2;
             if (due_l)
@@ -1400,6 +1411,9 @@ static int md_step(orac_gpu_ctx* ctx, MdState& S, bool update, bool energy) {
       if (int rc = md_shell_pair(ctx, S, 'm', LM, false, S.e, e_now)) return rc;
     if (due_l)
       if (int rc = md_shell_pair(ctx, S, 'l', LL, false, S.e + 8, e_now)) return rc;
+    // the N1 level's pair terms beside the bonded kernel on the side stream
+    if (due_n1)
+      if (int rc = md_pairs_n1(ctx, S, e_now)) return rc;
     if (side)
       if (int rc = sd.join()) return rc;
   }
