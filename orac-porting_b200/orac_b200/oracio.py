@@ -336,3 +336,32 @@ def split_arrays(arrs):
     rst = dict(co=np.asarray(arrs["co"]), xyz=np.asarray(arrs["xyz"]), v=np.asarray(arrs["v"]),
                nstep=int(arrs["nstep"]))
     return tp, rst
+
+
+def load(tpgprm_path, rst_path, **kw):
+    """A System from ORAC's own files: a topology-parameter file (as ORAC's
+    WRITE_TPGPRM writes it) and a restart file, with the run parameters of
+    system_from_orac as keywords (alphal, nfft, order, shells, ncell, ...)."""
+    tp = read_tpgprm(tpgprm_path)
+    return system_from_orac(tp, read_rst(rst_path, tp["ntap"]), **kw)
+
+
+def write_system_rst(path, s, x, v, nstep=0):
+    """An ORAC restart file of System `s` at Cartesian positions x and
+    velocities v (3, N): the box, the step count, the kinetic temperature
+    (3N minus the constraints minus the three of the centre of mass), and
+    the group and molecule centres of mass that ORAC's restart carries."""
+    x = np.asarray(x, dtype=np.float64)
+    v = np.asarray(v, dtype=np.float64)
+    mass = np.asarray(s.mass, dtype=np.float64)
+    ekin = 0.5 * float((mass * (v * v).sum(0)).sum())
+    ndf = 3 * s.ntap - len(np.asarray(s.constraints).reshape(-1, 2)) - 3
+    temp = units.kinetic_temperature(ekin, ndf) if ndf > 0 else 0.0
+    g = np.asarray(s.atomg) - 1
+    grp = np.zeros((3, s.ngrp))
+    for d in range(3):
+        grp[d] = np.bincount(g, weights=np.asarray(s.pmass) * x[d], minlength=s.ngrp)
+    p = np.asarray(s.atomp) - 1
+    mt = np.bincount(p, weights=mass, minlength=s.nprot)
+    mol = np.stack([np.bincount(p, weights=mass * x[d], minlength=s.nprot) / mt for d in range(3)])
+    write_rst(path, s.co, x, v, nstep=nstep, temp=temp, grp=grp, ngrp=s.ngrp, mol=mol, nprot=s.nprot)

@@ -13,7 +13,12 @@ the device and runs segment requests as they arrive:
   system that is not resident reserves its estimated footprint (evicting
   idle residents, least recently used first, when the budget is short:
   their state goes back to the host System), builds the system's context
-  and starts.  A finished segment leaves its system resident.
+  and starts.  A finished segment leaves its system resident.  With a
+  checkpoint directory, every system whose state leaves the device (evicted,
+  or resident at close) is also written as an ORAC restart file,
+  `<system id>.rst`, which ORAC reads (src/readrs.f) and
+  `oracio.load` / `oracio.read_rst` read back; systems can be submitted
+  from ORAC's own files with `oracio.load`.
 
 The loop is independent of the executor: the unit tests drive it with a
 simulated executor on the CPU.
@@ -24,6 +29,7 @@ import collections
 import ctypes as C
 import dataclasses
 import math
+import os
 import time
 
 import numpy as np
@@ -146,9 +152,11 @@ class Service:
     systems: {system id: host System}; make_engine(system) -> an engine set
     up for MD (orac_b200.engine.Engine after md_setup, or a stand-in with
     .ctx, .footprint(), .collect(), .md_state(), .close());
-    estimate(system) -> bytes to reserve before building."""
+    estimate(system) -> bytes to reserve before building;
+    checkpoint_dir: where evicted and closed systems' states go as ORAC
+    restart files (None: host memory only)."""
 
-    def __init__(self, executor, systems, make_engine, nsteps=500, estimate=estimate_footprint):
+    def __init__(self, executor, systems, make_engine, nsteps=500, estimate=estimate_footprint, checkpoint_dir=None):
         self.ex = executor
         self.systems = systems
         self.make_engine = make_engine
@@ -160,6 +168,8 @@ class Service:
         self.results = []
         self.builds = 0
         self.evictions = 0
+        self.checkpoint_dir = checkpoint_dir
+        self.steps = collections.Counter()  # MD steps each system has run here
 
     # -------------------------------------------------------------- memory
     def _evict_one(self, protect):
@@ -171,6 +181,7 @@ class Service:
         _, sid = min(idle)
         r = self.resident.pop(sid)
         x, v = r.engine.md_state()
+        self.checkpoint(sid, x, v)
         s = self.systems[sid]
         sc = np.linalg.inv(np.asarray(s.co)) @ x
         s.xp0, s.yp0, s.zp0 = sc[0].copy(), sc[1].copy(), sc[2].copy()
@@ -233,6 +244,8 @@ class Service:
         status = f.status
         if status == L.ORAC_OK:
             status = r.engine.collect()
+        if status == L.ORAC_OK:
+            self.steps[req.sid] += self.nsteps
         self.results.append(dict(rid=req.rid, sid=req.sid, natoms=int(self.systems[req.sid].ntap),
                                  t_arrival=f.t_arrival, t_start=f.t_start, t_end=f.t_end,
                                  latency=f.t_end - f.t_arrival, status=status))
@@ -260,8 +273,22 @@ class Service:
                 self.ex.wait(max(0.0, min(idle_wait, nxt)))
         return self.results
 
+    def checkpoint(self, sid, x, v):
+        """Write system `sid` at Cartesian positions x and velocities v as an
+        ORAC restart file in the checkpoint directory (if one is set)."""
+        if self.checkpoint_dir is None:
+            return None
+        from . import oracio
+
+        os.makedirs(self.checkpoint_dir, exist_ok=True)
+        path = os.path.join(self.checkpoint_dir, f"{sid}.rst")
+        oracio.write_system_rst(path, self.systems[sid], x, v, nstep=self.steps[sid])
+        return path
+
     def close(self):
-        for r in self.resident.values():
+        for sid, r in self.resident.items():
+            if self.checkpoint_dir is not None:
+                self.checkpoint(sid, *r.engine.md_state())
             r.engine.close()
             self.ex.unreserve(r.nbytes)
         self.resident.clear()

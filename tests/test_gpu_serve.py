@@ -12,12 +12,13 @@
   and each system's final state matches its uninterrupted run's to 1e-6 A
   (a restart from the saved Cartesian positions and velocities recomputes
   the forces with the energy kernels and re-projects the velocities: the
-  same values to rounding).
+  same values to rounding).  Each evicted system's last state is also in
+  its ORAC restart file in the checkpoint directory.
 """
 import numpy as np
 import pytest
 
-from orac_b200 import serve, systems
+from orac_b200 import oracio, serve, systems
 from orac_b200.engine import Engine
 
 pytestmark = pytest.mark.gpu
@@ -90,7 +91,7 @@ def test_footprint_is_below_the_reserved_estimate():
         assert 0 < fp <= est, (s.ntap, fp, est)
 
 
-def test_service_evicts_within_budget_and_restarts_exactly():
+def test_service_evicts_within_budget_and_restarts_exactly(tmp_path):
     nsteps = 6
     sy = {k: system(k) for k in range(3)}
     base = {k: s.copy() for k, s in sy.items()}
@@ -103,7 +104,7 @@ def test_service_evicts_within_budget_and_restarts_exactly():
     budget = est[1] + est[2] + 1  # two systems resident at most
     srv = serve.Server(budget_bytes=budget, max_active=4, chunk=2)
     svc = serve.Service(srv, sy, lambda s: engine(s, REM[int(s.name[-1])]), nsteps=nsteps,
-                        estimate=lambda s: fp[s.name])
+                        estimate=lambda s: fp[s.name], checkpoint_dir=str(tmp_path))
     arr = [(0.0, 0), (0.0, 1), (0.0, 2), (0.05, 0), (0.05, 1), (0.05, 2)]
     res = svc.run(arr, timeout=300.0)
     assert len(res) == 6 and all(r["status"] == 0 for r in res)
@@ -121,5 +122,8 @@ def test_service_evicts_within_budget_and_restarts_exactly():
         xr, _ = e.md_state()
         e.close()
         assert np.abs(x - xr).max() < 1e-6, (k, np.abs(x - xr).max())
+        if k not in svc.resident:  # evicted: its last state is also an ORAC restart file
+            r = oracio.read_rst(str(tmp_path / f"{k}.rst"), sy[k].ntap)
+            assert np.array_equal(r["xyz"], x) and r["nstep"] == svc.steps[k]
     svc.close()
     srv.close()

@@ -181,3 +181,60 @@ def test_poisson_arrivals_are_seeded_and_have_the_rate():
 def test_fifo_one_at_a_time():
     lat, end = serve.fifo_one_at_a_time([(0.0, 0), (0.5, 1), (3.0, 0)], [1.0, 1.0, 1.0])
     assert np.allclose(lat, [1.0, 1.5, 1.0]) and end == pytest.approx(4.0)
+
+
+class StateEngine(FakeEngine):
+    """A stand-in engine whose state moves with the steps it has run."""
+
+    def md_state(self):
+        x = self.s.cartesian() + 0.01 * self.steps
+        v = np.full((3, self.s.ntap), 0.001 * (1 + self.steps))
+        return x, v
+
+
+def test_evicted_and_closed_systems_are_checkpointed_as_orac_restarts(tmp_path):
+    from orac_b200 import oracio, systems, units
+
+    sy = {k: systems.two_waters(sep=(3.0 + k, 0.0, 0.0)) for k in range(3)}
+    ex = FakeServer(budget=2500, max_active=4, cost=lambda e: 1e-3)
+    svc = serve.Service(ex, sy, lambda s: StateEngine(s, 1000), nsteps=5, estimate=lambda s: 1000,
+                        checkpoint_dir=str(tmp_path))
+    res = svc.run([(0.0, 0), (0.0, 1), (0.0, 2), (0.01, 0), (0.02, 1)], timeout=100.0)
+    assert len(res) == 5 and svc.evictions > 0
+    states = {sid: r.engine.md_state() for sid, r in svc.resident.items()}
+    svc.close()
+    for sid, s in sy.items():
+        r = oracio.read_rst(str(tmp_path / f"{sid}.rst"), s.ntap)
+        assert r["nstep"] == svc.steps[sid] and r["nstep"] % 5 == 0 and r["nstep"] > 0
+        assert np.allclose(r["co"], s.co) and np.allclose(r["oc"], np.linalg.inv(s.co))
+        if sid in states:  # resident at close
+            x, v = states[sid]
+        else:  # evicted: its state went back to the host System too
+            x = s.xyz_restart
+            v = np.stack([s.vx, s.vy, s.vz])
+        assert np.array_equal(r["xyz"], x) and np.array_equal(r["v"], v)
+        ekin = 0.5 * float((np.asarray(s.mass) * (v * v).sum(0)).sum())
+        ndf = 3 * s.ntap - len(np.asarray(s.constraints).reshape(-1, 2)) - 3
+        assert r["temp"] == pytest.approx(units.kinetic_temperature(ekin, ndf), rel=1e-12)
+
+
+def test_orac_restart_round_trip_rebuilds_the_system(tmp_path):
+    """The real system's state written as an ORAC restart and read back
+    rebuilds the same System with the fixture's topology (ORAC's own
+    topology-parameter arrays)."""
+    import os
+
+    from orac_b200 import oracio, systems
+
+    fix = np.load(os.path.join(os.path.dirname(__file__), "golden", "f0_fkbp12.npz"))
+    tp, rst = oracio.split_arrays(dict(fix))
+    sh = systems.Shells(rcutm=5.1, rtolm=0.3, rneim=0.4, rcutl=7.8, rtoll=0.3, rneil=0.5, rcuth=10.0, rtolh=0.3,
+                        rneih=1.5)
+    kw = dict(alphal=0.37, nfft=(48, 48, 48), order=4, shells=sh, ncell=(18, 18, 18))
+    s = oracio.system_from_orac(tp, rst, **kw)
+    path = str(tmp_path / "f0.rst")
+    oracio.write_system_rst(path, s, rst["xyz"], rst["v"], nstep=30)
+    r = oracio.read_rst(path, s.ntap)
+    assert r["nstep"] == 30 and np.array_equal(r["xyz"], rst["xyz"]) and np.array_equal(r["v"], rst["v"])
+    s2 = oracio.system_from_orac(tp, r, **kw)
+    assert np.array_equal(s2.cartesian(), s.cartesian()) and np.array_equal(s2.vx, s.vx)
