@@ -241,6 +241,16 @@ int orac_gpu_set_alchemy(orac_gpu_ctx* ctx, const int* ss_alchemy,
                          const double* rmin, const double* epsm, double qsoft,
                          double ljsoft, int opls);
 
+/* orac_gpu_set_alchemy_shift: the pair form of the alchemy variant, as
+ * mts_forces selects it (src/mts_forces.f:131-146): shifted = 1 gives
+ * force_ALCHEMY_shift (src/force_alchemy_shifted.f:466-520, ORAC's
+ * SHIFT-POT qshift ljshift): LJ evaluated at r + ljshift 2**(1./6.) sigma
+ * alch_fact(1,t) and Coulomb erfc(alpha r) / (r + qshift alch_factq(1,t));
+ * shifted = 0 returns to the soft core of force_alchemy (the default).
+ * Kept across orac_gpu_set_alchemy and orac_gpu_set_lambda calls. */
+int orac_gpu_set_alchemy_shift(orac_gpu_ctx* ctx, int shifted, double qshift,
+                               double ljshift);
+
 /* orac_gpu_set_lambda: cpropar's ladd, lrm, laddq, lrmq and their previous
  * values ladd0..lrmq0 (lam[8] in that order), with intramol / ljintra of
  * alch_set (src/force_alchemy_shifted.f:732-790).  The PME charges become

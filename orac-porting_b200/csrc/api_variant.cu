@@ -150,6 +150,8 @@ void variant_fill(const orac_gpu_ctx* ctx, PairArgs* a) {
     a->at = ctx->at;
     a->qsoft = (float)ctx->at.qsoft;
     a->ljsoft = (float)ctx->at.ljsoft;
+    a->qshift = (float)ctx->at.qshift;
+    a->ljshift_s = (float)ctx->at.ljshift_s;
     for (int k = 0; k < 2; k++)
       for (int t = 0; t < 9; t++) {
         a->af[k][t] = (float)ctx->at.f[k][t];
@@ -225,6 +227,17 @@ int orac_gpu_set_alchemy(orac_gpu_ctx* ctx, const int* ss_alchemy, const double*
   ctx->variant = VAR_ALCH;
   const double zero[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   return orac_gpu_set_lambda(ctx, zero, 0, 0, nullptr);
+}
+
+int orac_gpu_set_alchemy_shift(orac_gpu_ctx* ctx, int shifted, double qshift, double ljshift) {
+  if (!ctx) return ORAC_ERR_PARAM;
+  if (shifted && !(qshift >= 0.0 && ljshift >= 0.0))
+    return ctx_fail(ctx, ORAC_ERR_PARAM, "qshift %g and ljshift %g must be >= 0", qshift, ljshift);
+  ctx->at.shifted = shifted ? 1 : 0;
+  ctx->at.qshift = shifted ? qshift : 0.0;
+  // ORAC's two6 = 2.d0**(1./6.), the exponent a single-precision constant
+  ctx->at.ljshift_s = shifted ? ljshift * std::pow(2.0, (double)(1.0f / 6.0f)) : 0.0;
+  return ORAC_OK;
 }
 
 int orac_gpu_set_lambda(orac_gpu_ctx* ctx, const double* lam, int intramol, int ljintra, const double* dlam) {

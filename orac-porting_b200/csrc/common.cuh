@@ -52,6 +52,11 @@ struct AlchTables {
   double f0[2][9], fq0[2][9];  // previous lambdas
   double df[2][9], dfq[2][9];  // derivatives with respect to the control lambda
   double qsoft, ljsoft;        // SOFT-CORE parameters
+  // the shifted potential of force_ALCHEMY_shift in place of the soft core
+  // (SHIFT-POT qshift ljshift): Coulomb over r + qshift f, LJ at
+  // r + ljshift_s sigma f, ljshift_s = ljshift 2**(1./6.) as ORAC takes it
+  int shifted;
+  double qshift, ljshift_s;
   int opls;                    // sigma = 2 sqrt(rmin_i rmin_j) instead of rmin_i + rmin_j
 };
 
@@ -130,6 +135,7 @@ struct PairArgs {
   const float2* soft;
   const double2* softd;
   float qsoft, ljsoft;
+  float qshift, ljshift_s;  // shifted potential (at.shifted)
   float af[2][9], afq[2][9];  // FP32 copies of the current tables
   AlchTables at;
 };

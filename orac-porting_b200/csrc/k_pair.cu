@@ -87,6 +87,39 @@ __device__ __forceinline__ bool seg_sel(int kind, int fa, int fb) {
 // sum.  t indexes the tables (ss_i + ss_j + 4).
 __device__ __forceinline__ void alch_pair_f32(const PairArgs& A, float r2, int t, float rmi, float rmj, float eps4,
                                               float qq, float* qf, float* conf, float* coul) {
+  if (A.at.shifted) {
+    // force_ALCHEMY_shift (src/force_alchemy_shifted.f:466-520): LJ at the
+    // shifted distance rl, Coulomb erfc(alpha r) over the shifted rq
+    const float ir = rsqrtf(r2), r = r2 * ir;
+    float f = 0.f, uc = 0.f, uq = 0.f;
+    if (eps4 > 1e-12f) {
+      const float sig = A.at.opls ? 2.f * sqrtf(rmi * rmj) : rmi + rmj;
+      const float rl = r + A.ljshift_s * sig * A.af[0][t];
+      const float irl = __fdividef(1.f, rl);
+      const float s2 = sig * sig * irl * irl, x = s2 * s2 * s2;
+      const float sc = A.af[1][t] * eps4;
+      f = sc * (12.f * x * x - 6.f * x) * ir * irl;
+      uc = sc * (x * x - x);
+    }
+    const float irq = __fdividef(1.f, r + A.qshift * A.afq[0][t]);
+    if (!A.lskip) {
+      const float ar = A.alphal * r;
+      const float qt = __fdividef(1.0f, 1.0f + AS_QP * ar);
+      const float ex = __expf(-ar * ar);
+      const float erfcst = ((((AS_A5 * qt + AS_A4) * qt + AS_A3) * qt + AS_A2) * qt + AS_A1) * qt * ex;
+      const float furpar = A.afq[1][t] * qq;
+      uq = furpar * erfcst * irq;
+      // -dU/dr / r of erfc(alpha r) / rq: erfc / (r rq^2) + 2 alpha / sqrt(pi) e / (r rq)
+      f += furpar * (erfcst * irq + A.twrtpi * ar * ex * ir) * irq * ir;
+    } else if (!A.ewald) {
+      uq = A.afq[1][t] * qq * irq;
+      f += uq * irq * ir;
+    }
+    *qf = f;
+    *conf = uc;
+    *coul = uq;
+    return;
+  }
   const float auxa = rsqrtf(r2);
   const float fq1 = A.afq[0][t];
   const float auxaa = rsqrtf(A.qsoft * fq1 * fq1 + r2);
@@ -127,6 +160,41 @@ __device__ __forceinline__ void alch_energy_fp64(const PairArgs& A, double rx, d
                                                  double* c0, double* q0, double* du) {
   const AlchTables& T = A.at;
   const double rsq = rx * rx + ry * ry + rz * rz;
+  if (T.shifted) {
+    // force_ALCHEMY_shift's energies at lambda and lambda0, and dU/dlambda
+    // through the tables: rl = r + c f0, x = (sigma/rl)^6, U = f1 e (x^2 - x),
+    // dx/dlambda = -6 x c df0 / rl; Coulomb f1 g / rq, rq = r + qshift f0
+    const double r = sqrt(rsq);
+    const double epsmin = 4.0 * sqrt(si.y * sj.y);
+    *cd = *qd = *c0 = *q0 = *du = 0.0;
+    if (epsmin > 1.0e-12) {
+      const double sigma = T.opls ? 2.0 * sqrt(si.x * sj.x) : si.x + sj.x;
+      const double c = T.ljshift_s * sigma;
+      const double rl = r + c * T.f[0][t], rl0 = r + c * T.f0[0][t];
+      const double s1 = sigma / rl, s0 = sigma / rl0;
+      const double x = s1 * s1 * s1 * s1 * s1 * s1, x0 = s0 * s0 * s0 * s0 * s0 * s0;
+      *cd = T.f[1][t] * epsmin * (x * x - x);
+      *c0 = T.f0[1][t] * epsmin * (x0 * x0 - x0);
+      *du = T.df[1][t] * epsmin * (x * x - x) +
+            T.f[1][t] * epsmin * (2.0 * x - 1.0) * (-6.0 * x / rl) * c * T.df[0][t];
+    }
+    double g = 0.0;
+    if (!A.lskip) {
+      const double ar = A.alphad * r;
+      const double qt = 1.0 / (1.0 + 0.3275911 * ar);
+      g = qq * ((((1.0614054 * qt - 1.453152) * qt + 1.4214137) * qt - 0.28449674) * qt + 0.2548296) * qt *
+          exp(-ar * ar);
+    } else if (!A.ewald) {
+      g = qq;
+    }
+    if (g != 0.0) {
+      const double rq = r + T.qshift * T.fq[0][t], rq0 = r + T.qshift * T.fq0[0][t];
+      *qd = T.fq[1][t] * g / rq;
+      *q0 = T.fq0[1][t] * g / rq0;
+      *du += T.dfq[1][t] * g / rq - T.fq[1][t] * g / (rq * rq) * T.qshift * T.dfq[0][t];
+    }
+    return;
+  }
   const double auxa = 1.0 / sqrt(rsq);
   const double fq = T.fq[0][t], fq0 = T.fq0[0][t];
   const double auxaa = 1.0 / sqrt(T.qsoft * (fq * fq) + rsq);

@@ -147,14 +147,18 @@ class Engine:
         arr = None if rematom is None else i32(np.asarray(rematom) != 0)
         check(self.ctx, self.lib.orac_gpu_set_rem(self.ctx, arr, int(kind), float(factor)), "set_rem")
 
-    def set_alchemy(self, ss_alchemy, qsoft=0.5, ljsoft=0.5, opls=False):
-        """force_alchemy with ORAC's per-atom soft-core parameters; None: standard."""
+    def set_alchemy(self, ss_alchemy, qsoft=0.5, ljsoft=0.5, opls=False, shifted=False, qshift=0.0, ljshift=0.0):
+        """force_alchemy with ORAC's per-atom soft-core parameters, or with
+        `shifted` force_ALCHEMY_shift (SHIFT-POT qshift ljshift); None:
+        standard."""
         if ss_alchemy is None:
             check(self.ctx, self.lib.orac_gpu_set_alchemy(self.ctx, None, None, None, 0.0, 0.0, 0), "set_alchemy")
             return
         rmin, epsm = self.s.alchemy_params()
         check(self.ctx, self.lib.orac_gpu_set_alchemy(self.ctx, i32(ss_alchemy), f64(rmin), f64(epsm), qsoft, ljsoft,
                                                       int(opls)), "set_alchemy")
+        check(self.ctx, self.lib.orac_gpu_set_alchemy_shift(self.ctx, int(bool(shifted)), float(qshift),
+                                                            float(ljshift)), "set_alchemy_shift")
 
     def set_lambda(self, ladd, lrm, laddq, lrmq, ladd0=None, lrm0=None, laddq0=None, lrmq0=None, intramol=False,
                    ljintra=False, dlam=None):

@@ -73,6 +73,7 @@ def load():
         "orac_gpu_mts_intra_n1": (i, [_P, _D, _D, _D, _D, _D, _D, _D]),
         "orac_gpu_set_rem": (i, [_P, _I, i, d]),
         "orac_gpu_set_alchemy": (i, [_P, _I, _D, _D, d, d, i]),
+        "orac_gpu_set_alchemy_shift": (i, [_P, i, d, d]),
         "orac_gpu_set_lambda": (i, [_P, _D, i, i, _P]),
         "orac_gpu_variant_energies": (i, [_P, _D]),
         "orac_gpu_pme_kspace_static": (i, [_P, i, _P, _P, _D, d, d, d, i, i, i, i, _P, _P, C.c_char_p, i]),

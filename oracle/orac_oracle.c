@@ -554,6 +554,71 @@ static int force_group(const force_args* A, force_ws* W, int i, const int* lst,
   return map;
 }
 
+/* Shifted-potential pair of force_ALCHEMY_shift,
+ * src/force_alchemy_shifted.f:466-520: the LJ distance r + ljshift sigma
+ * two6 alch_fact(1,t) (two6 = 2**(1./6.) with a single-precision
+ * exponent, :178), the Coulomb denominator r + qshift alch_factq(1,t), the
+ * erfc taken at the unshifted r. */
+static void alch_pair_shift(const force_args* A, force_ws* W, int i1, int j, int j1, double xc, double yc,
+                            double zc, double xxcm, double yycm, double zzcm, double rsq, double sigma,
+                            double epsmin, double chrgei, int typeij, int t, double sw) {
+  const orc_variant* V = A->V;
+  const double two6 = pow(2.0, (double)(1.0f / 6.0f));
+  double r = sqrt(rsq);
+  double qforce;
+  if (epsmin > 1.0e-12) {
+    double rl = r + V->ljshift * sigma * two6 * V->fact[0][t];
+    double rl0 = r + V->ljshift * sigma * two6 * V->fact0[0][t];
+    double r6 = pow(sigma / rl, 6.0);
+    double r60 = pow(sigma / rl0, 6.0);
+    double ssvirr = V->fact[1][t] * epsmin * (12.0 * r6 * r6 - 6.0 * r6);
+    double ucon = V->fact[1][t] * epsmin * (r6 * r6 - r6);
+    double ucon0 = V->fact0[1][t] * epsmin * (r60 * r60 - r60);
+    qforce = ssvirr * sw / (r * rl);
+    W->cmap2[j1] += ucon;
+    W->uconf[typeij - 1] += sw * ucon;
+    W->uconf0[typeij - 1] += sw * ucon0;
+  } else {
+    qforce = 0.0;
+  }
+  double rq = r + V->qshift * V->factq[0][t];
+  double rq0 = r + V->qshift * V->factq0[0][t];
+  if (!A->lskip_ewald) {
+    double alphar = A->alphal * r;
+    double qt = 1.0 / (1.0 + AS_QP * alphar);
+    double expcst = exp(-alphar * alphar);
+    double erfcst = ((((AS_A5 * qt + AS_A4) * qt + AS_A3) * qt + AS_A2) * qt + AS_A1) * qt * expcst;
+    double furpar = V->factq[1][t] * chrgei * A->charge[j];
+    double furpar0 = V->factq0[1][t] * chrgei * A->charge[j];
+    W->ucoul[typeij - 1] += sw * furpar * erfcst / rq;
+    W->ucoul0[typeij - 1] += sw * furpar0 * erfcst / rq0;
+    W->cmap2[j1] += furpar * erfcst / rq;
+    qforce += furpar * (erfcst * sw / (rq * rq * r) + A->twrtpi * alphar * expcst * sw / (r * r * rq));
+  } else if (!A->ewald) {
+    double ssvir = V->factq[1][t] * chrgei * A->charge[j] / rq;
+    double ssvir0 = V->factq0[1][t] * chrgei * A->charge[j] / rq0;
+    W->cmap2[j1] += ssvir;
+    W->ucoul[typeij - 1] += ssvir * sw;
+    W->ucoul0[typeij - 1] += ssvir0 * sw;
+    qforce += ssvir * sw / (rq * r);
+  }
+  W->fx[i1] += qforce * xc;
+  W->fy[i1] += qforce * yc;
+  W->fz[i1] += qforce * zc;
+  W->fx[j] -= qforce * xc;
+  W->fy[j] -= qforce * yc;
+  W->fz[j] -= qforce * zc;
+  W->st[0] += qforce * xc * xxcm;
+  W->st[1] += qforce * xc * yycm;
+  W->st[2] += qforce * xc * zzcm;
+  W->st[3] += qforce * yc * xxcm;
+  W->st[4] += qforce * yc * yycm;
+  W->st[5] += qforce * yc * zzcm;
+  W->st[6] += qforce * zc * xxcm;
+  W->st[7] += qforce * zc * yycm;
+  W->st[8] += qforce * zc * zzcm;
+}
+
 /* Soft-core pair of force_alchemy, src/force_alchemy.f:441-531.  j1 is the
  * map slot of the partner group. */
 static inline void alch_pair(const force_args* A, force_ws* W, int i1, int j,
@@ -580,6 +645,10 @@ static inline void alch_pair(const force_args* A, force_ws* W, int i1, int j,
   double zc = co[8] * zg;
   double rsq = xc * xc + yc * yc + zc * zc;
   double auxa = 1.0 / sqrt(rsq);
+  if (V->shifted) {
+    alch_pair_shift(A, W, i1, j, j1, xc, yc, zc, xxcm, yycm, zzcm, rsq, sigma, epsmin, chrgei, typeij, t, sw);
+    return;
+  }
   double fq = V->factq[0][t], fq0 = V->factq0[0][t];
   double auxaa = 1.0 / sqrt(V->qsoft * (fq * fq) + rsq); /* soft core */
   double auxa0 = 1.0 / sqrt(V->qsoft * (fq0 * fq0) + rsq);

@@ -77,7 +77,8 @@ long orc_force(const int* ss_index, const double* xp0, const double* yp0,
                const double* mass, double massinfty, int lskip_ewald,
                int ewald, int nthreads);
 
-/* Variants of the shell kernel selected by mts_forces (src/mts_forces.f:118-153).
+/* Variants of the shell kernel selected by mts_forces (src/mts_forces.f:118-153);
+ * mode 2 with `shifted` is force_ALCHEMY_shift.
  *  mode 1  force_rem (src/force_REM.f): pairs with seg_select(kind, rematom,
  *          i, j) (src/rem.f90:631-645) have their force, and their share of
  *          the S'V switching term, multiplied by rem_factor(3); the energies
@@ -105,6 +106,12 @@ typedef struct {
   double qsoft, ljsoft;
   int opls;                     /* sigma = 2 sqrt(rmin_i rmin_j) if set */
   double fact[2][9], factq[2][9], fact0[2][9], factq0[2][9];
+  /* force_ALCHEMY_shift (src/force_alchemy_shifted.f:466-520, selected by
+   * mts_forces when `shifted`, src/mts_forces.f:131-138): LJ at
+   * r + ljshift sigma 2^(1/6) alch_fact(1,t), Coulomb erfc(alpha r) over
+   * r + qshift alch_factq(1,t), in place of the soft core */
+  int shifted;
+  double qshift, ljshift;
 } orc_variant;
 
 /* force with a variant (NULL or mode 0: force).  extra[4] (may be NULL)

@@ -84,7 +84,8 @@ class Variant(C.Structure):
     _fields_ = [("mode", C.c_int), ("rematom", C.c_void_p), ("rem_kind", C.c_int), ("rem_factor", C.c_double),
                 ("ss_alchemy", C.c_void_p), ("rmin", C.c_void_p), ("epsm", C.c_void_p), ("qsoft", C.c_double),
                 ("ljsoft", C.c_double), ("opls", C.c_int), ("fact", C.c_double * 18), ("factq", C.c_double * 18),
-                ("fact0", C.c_double * 18), ("factq0", C.c_double * 18)]
+                ("fact0", C.c_double * 18), ("factq0", C.c_double * 18), ("shifted", C.c_int),
+                ("qshift", C.c_double), ("ljshift", C.c_double)]
 
 
 def alch_set(ladd, lrm, intramol=False, ljintra=False, qq=False):
@@ -140,9 +141,11 @@ class Oracle:
         v.rem_factor = float(factor)
         self.variant = v
 
-    def set_alchemy(self, ss_alchemy, qsoft=0.5, ljsoft=0.5, opls=False):
+    def set_alchemy(self, ss_alchemy, qsoft=0.5, ljsoft=0.5, opls=False, shifted=False, qshift=0.0, ljshift=0.0):
         """force_alchemy (src/force_alchemy.f) with ORAC's per-atom soft-core
-        parameters (src/mtsmd.f:1298-1303); lambdas start at 0 (all on)."""
+        parameters (src/mtsmd.f:1298-1303), or with `shifted` the
+        shifted potential of force_ALCHEMY_shift (src/force_alchemy_shifted.f,
+        ORAC's SHIFT-POT qshift ljshift); lambdas start at 0 (all on)."""
         rmin, epsm = self.s.alchemy_params()
         self._alch = (_i(ss_alchemy), _f(rmin), _f(epsm))
         v = Variant()
@@ -153,6 +156,9 @@ class Oracle:
         v.qsoft = float(qsoft)
         v.ljsoft = float(ljsoft)
         v.opls = int(opls)
+        v.shifted = int(bool(shifted))
+        v.qshift = float(qshift)
+        v.ljshift = float(ljshift)
         self.variant = v
         self.set_lambda(0.0, 0.0, 0.0, 0.0)
 

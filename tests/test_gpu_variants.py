@@ -1,6 +1,8 @@
 """GPU parity of the shell-kernel variants against the FP64 oracle:
-force_rem (REM segment scaling) and force_alchemy (soft-core alchemy), plus
-the alchemical PME charges and work of do_pmesh_alchemy.
+force_rem (REM segment scaling), force_alchemy (soft-core alchemy) and
+force_ALCHEMY_shift (the shifted potential, selected by
+orac_gpu_set_alchemy_shift), plus the alchemical PME charges and work of
+do_pmesh_alchemy.
 
 Tolerances are those of the standard parity tests: forces relative RMS
 <= 1e-5, energies relative <= 1e-6 of the value or of the sum of the term
@@ -24,6 +26,9 @@ ENERGY_REL = 1e-6
 STRESS_REL = 1e-5
 LAM = dict(ladd=0.3, lrm=0.6, laddq=0.4, lrmq=0.7)
 LAM0 = dict(ladd0=0.2, lrm0=0.5, laddq0=0.35, lrmq0=0.65)
+# the pair forms of the alchemy variant: soft core (force_alchemy) and
+# test4's shifted potential, SHIFT-POT 4.0 0.35 (force_ALCHEMY_shift)
+FORMS = {"soft": {}, "shift": dict(shifted=True, qshift=4.0, ljshift=0.35)}
 
 
 def small_box():
@@ -81,8 +86,9 @@ def pair(name, variant, **kw):
         o.set_rem(s.rematom, kw["kind"], kw["factor"])
         g.set_rem(s.rematom, kw["kind"], kw["factor"])
     else:
-        o.set_alchemy(s.ss_alchemy, 0.5, 0.5)
-        g.set_alchemy(s.ss_alchemy, 0.5, 0.5)
+        form = FORMS[kw.get("form", "soft")]
+        o.set_alchemy(s.ss_alchemy, 0.5, 0.5, **form)
+        g.set_alchemy(s.ss_alchemy, 0.5, 0.5, **form)
         lam = dict(kw.get("lam", LAM))
         lam.update(kw.get("lam0", {}))
         o.set_lambda(**lam)
@@ -113,22 +119,24 @@ def test_rem_shell_parity(name, kind, shell):
     close(xg[0], xr[0], scale, f"{shell} seg_ene")
 
 
+@pytest.mark.parametrize("form", sorted(FORMS))
 @pytest.mark.parametrize("shell", ["m", "l", "h"])
 @pytest.mark.parametrize("name", ["water64", "config1", "polymer_small"])
-def test_alchemy_shell_parity(name, shell):
-    o, g = pair(name, "alch", lam0=LAM0)
+def test_alchemy_shell_parity(name, shell, form):
+    o, g = pair(name, "alch", lam0=LAM0, form=form)
     xr, xg, scale = compare_shell(o, g, shell)
     close(xg[1], xr[1], scale, f"{shell} dwrk")
     close(xg[2], xr[2], scale, f"{shell} U0 LJ")
     close(xg[3], xr[3], scale, f"{shell} U0 Coulomb")
 
 
+@pytest.mark.parametrize("form", sorted(FORMS))
 @pytest.mark.parametrize("shell", ["m", "l", "h"])
 @pytest.mark.parametrize("name", ["water64", "polymer_small"])
-def test_alchemy_dudl_matches_oracle_central_difference(name, shell):
+def test_alchemy_dudl_matches_oracle_central_difference(name, shell, form):
     lam = 0.4
     h = 1e-4
-    o, g = pair(name, "alch", lam=dict(ladd=0.0, lrm=lam, laddq=0.0, lrmq=lam), dlam=[0.0, 1.0, 0.0, 1.0])
+    o, g = pair(name, "alch", lam=dict(ladd=0.0, lrm=lam, laddq=0.0, lrmq=lam), dlam=[0.0, 1.0, 0.0, 1.0], form=form)
     g.shell(shell)
     dudl = g.variant_energies()[4]
     u = []

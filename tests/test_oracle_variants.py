@@ -9,7 +9,10 @@ Pinned by properties the reference's formulas imply:
     are scaled by s in the force but reported unscaled);
   - the REM force is linear in rem_factor, and seg_ene(either) =
     seg_ene(both) + seg_ene(exactly one);
-  - dwrk = U(lambda) - U(lambda0) (src/force_alchemy.f:683-688).
+  - dwrk = U(lambda) - U(lambda0) (src/force_alchemy.f:683-688);
+  - the same for the shifted potential (force_ALCHEMY_shift), which at
+    every lambda 0 is the standard force too and elsewhere differs from the
+    soft core.
 """
 import numpy as np
 import pytest
@@ -48,10 +51,13 @@ def rem_water(seed=0):
 LAM = dict(ladd=0.3, lrm=0.6, laddq=0.4, lrmq=0.7)
 
 
+SHIFT = dict(shifted=True, qshift=4.0, ljshift=0.35)  # test4's SHIFT-POT 4.0 0.35
+
+
 def _oracle(s, variant=None, lam=None, lam0=None, rem=None):
     o = oracle.Oracle(s, nthreads=2)
-    if variant == "alch":
-        o.set_alchemy(s.ss_alchemy, 0.5, 0.5)
+    if variant in ("alch", "shift"):
+        o.set_alchemy(s.ss_alchemy, 0.5, 0.5, **(SHIFT if variant == "shift" else {}))
         lam = lam or dict(ladd=0.0, lrm=0.0, laddq=0.0, lrmq=0.0)
         kw = dict(lam)
         if lam0:
@@ -208,3 +214,39 @@ def test_alchemy_fully_removed_atoms_do_not_interact():
     Fm = F[:, :9].sum(axis=1)
     assert np.allclose(Fm, 0.0, atol=1e-12 * np.abs(F).max())
     assert np.abs(F[:, :9]).max() > 0.0
+
+
+@pytest.mark.parametrize("shell", ["m", "l", "h"])
+def test_shifted_at_zero_lambda_is_the_standard_force(shell):
+    """Removed atoms only, as for the soft core (removed-added pairs never
+    interact); with no shift left the kernels agree to the sigma factor's
+    single-precision 2**(1./6.)."""
+    s = alch_water(added=False)
+    F0, ue0, st0 = _oracle(s).shell(shell)
+    F1, ue1, st1 = _oracle(s, "shift").shell(shell)
+    assert _rel(F1, F0) < 1e-6
+    assert np.allclose(ue1, ue0, rtol=1e-6, atol=1e-9 * np.abs(ue0).max())
+
+
+@pytest.mark.parametrize("shell", ["m", "h"])
+def test_shifted_forces_are_minus_energy_gradient(shell):
+    s = alch_water()
+
+    def make(t):
+        o = _oracle(t, "shift", lam=LAM)
+        o.shell_eval = o.shell(shell)
+        return o
+
+    _fd_check(s, make, lambda o: o.shell_eval[1].sum(), [0, 1, 5, 10, 13, 40])
+
+
+def test_shifted_work_is_energy_difference_and_differs_from_the_soft_core():
+    s = alch_water()
+    lam0 = dict(ladd=0.2, lrm=0.5, laddq=0.35, lrmq=0.65)
+    o = _oracle(s, "shift", lam=LAM, lam0=lam0)
+    F, ue, _ = o.shell("m")
+    dwrk = o.last_extra[1]
+    _, ue_0, _ = _oracle(s, "shift", lam=lam0).shell("m")
+    assert dwrk == pytest.approx(ue.sum() - ue_0.sum(), rel=1e-10)
+    Fs, ues, _ = _oracle(s, "alch", lam=LAM).shell("m")
+    assert _rel(F, Fs) > 1e-3 and abs(ue.sum() - ues.sum()) > 1e-6 * abs(ues.sum())
