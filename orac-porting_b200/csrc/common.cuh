@@ -454,6 +454,12 @@ int small_launch_x(orac_gpu_ctx* ctx, int kind, const double* d_xyz, const int* 
                    int npairs, const double* d_t12, const double* d_t6, double fudge, double lj_fudge,
                    int coul_mode, int forces, double* d_f, double* d_e, const int* d_ss, const double* d_q,
                    unsigned long long* d_ffix, const double* d_dq = nullptr, double* d_edq = nullptr);
+// k_small.cu: ferrf over up to four pair lists in one launch, list k with
+// its own fudge, forces flag (0: energy only) and energy slots d_e[k]
+int ferrf_launch_lists(orac_gpu_ctx* ctx, int nlist, const int* const* d_pairs, const int* npairs,
+                       const double* fudge, const int* forces, double* const* d_e, const double* d_xyz,
+                       const int* d_ss, const double* d_q, unsigned long long* d_ffix, const double* d_dq,
+                       double* d_edq);
 // k_bonded.cu: mask of BK_* kinds; forces into d_f (FP64 atomics) or d_ffix
 // (fixed point; the proper torsions into d_ffix_tors when given, so one
 // launch serves two r-RESPA levels); d_e[8] (bond, bend, tors, itors) x

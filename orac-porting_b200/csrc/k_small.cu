@@ -41,8 +41,7 @@ struct SmallArgs {
   double* edq;
 };
 
-__global__ void k_small(const SmallArgs A) {
-  pdl_enter();
+__device__ __forceinline__ void small_body(const SmallArgs& A) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   double e[4] = {0, 0, 0, 0};
   double dedl = 0.0;
@@ -137,6 +136,23 @@ __global__ void k_small(const SmallArgs A) {
   }
 }
 
+__global__ void k_small(const SmallArgs A) {
+  pdl_enter();
+  small_body(A);
+}
+
+// up to four pair lists of one kind in one launch, blockIdx.y the list:
+// a block never spans two lists, so each keeps its own energy slots
+constexpr int MAX_SEGS = 4;
+struct SmallSegs {
+  SmallArgs s[MAX_SEGS];
+};
+
+__global__ void k_small_segs(const SmallSegs S) {
+  pdl_enter();
+  small_body(S.s[blockIdx.y]);
+}
+
 __global__ void k_self(int n, const double* q, const int* ss, double* e) {
   pdl_enter();
   __shared__ double s[8][2];
@@ -165,10 +181,10 @@ int small_launch(orac_gpu_ctx* ctx, int kind, const double* d_xyz, const int* d_
                         d_f, d_e, d_ss, nullptr, nullptr);
 }
 
-int small_launch_x(orac_gpu_ctx* ctx, int kind, const double* d_xyz, const int* d_pairs, const int* d_ptype,
-                   int npairs, const double* d_t12, const double* d_t6, double fudge, double lj_fudge,
-                   int coul_mode, int forces, double* d_f, double* d_e, const int* d_ss, const double* d_q,
-                   unsigned long long* d_ffix, const double* d_dq, double* d_edq) {
+static SmallArgs small_args(orac_gpu_ctx* ctx, int kind, const double* d_xyz, const int* d_pairs,
+                            const int* d_ptype, int npairs, const double* d_t12, const double* d_t6, double fudge,
+                            double lj_fudge, int coul_mode, int forces, double* d_f, double* d_e, const int* d_ss,
+                            const double* d_q, unsigned long long* d_ffix, const double* d_dq, double* d_edq) {
   SmallArgs A;
   memset(&A, 0, sizeof(A));
   A.kind = kind;
@@ -192,10 +208,38 @@ int small_launch_x(orac_gpu_ctx* ctx, int kind, const double* d_xyz, const int* 
   A.forces = forces;
   A.f = d_f;
   A.e = d_e;
+  return A;
+}
+
+int small_launch_x(orac_gpu_ctx* ctx, int kind, const double* d_xyz, const int* d_pairs, const int* d_ptype,
+                   int npairs, const double* d_t12, const double* d_t6, double fudge, double lj_fudge,
+                   int coul_mode, int forces, double* d_f, double* d_e, const int* d_ss, const double* d_q,
+                   unsigned long long* d_ffix, const double* d_dq, double* d_edq) {
+  const SmallArgs A = small_args(ctx, kind, d_xyz, d_pairs, d_ptype, npairs, d_t12, d_t6, fudge, lj_fudge, coul_mode,
+                                 forces, d_f, d_e, d_ss, d_q, d_ffix, d_dq, d_edq);
   if (npairs > 0) {
     orac_launch(k_small, (npairs + 255) / 256, 256, 0, ctx->stream, A);
     CKL();
   }
+  return ORAC_OK;
+}
+
+int ferrf_launch_lists(orac_gpu_ctx* ctx, int nlist, const int* const* d_pairs, const int* npairs,
+                       const double* fudge, const int* forces, double* const* d_e, const double* d_xyz,
+                       const int* d_ss, const double* d_q, unsigned long long* d_ffix, const double* d_dq,
+                       double* d_edq) {
+  SmallSegs S;
+  memset(&S, 0, sizeof(S));
+  int ns = 0, nmax = 0;
+  for (int k = 0; k < nlist && ns < MAX_SEGS; k++) {
+    if (npairs[k] <= 0) continue;
+    S.s[ns++] = small_args(ctx, 2, d_xyz, d_pairs[k], nullptr, npairs[k], nullptr, nullptr, fudge[k], 1.0, 1,
+                           forces[k], nullptr, d_e[k], d_ss, d_q, d_ffix, d_dq, d_edq);
+    nmax = npairs[k] > nmax ? npairs[k] : nmax;
+  }
+  if (ns == 0) return ORAC_OK;
+  orac_launch(k_small_segs, dim3((nmax + 255) / 256, ns), dim3(256), 0, ctx->stream, S);
+  CKL();
   return ORAC_OK;
 }
 

@@ -1219,23 +1219,15 @@ static int md_ferrf(orac_gpu_ctx* ctx, MdState& S, unsigned long long* f, bool e
   // d/dlambda of the corrections of alchemical charges (ferrf_alchemy)
   const double* dq = (energy && ctx->variant == VAR_ALCH) ? ctx->d_dq : nullptr;
   double* edq = dq ? S.e + E_DUDL + 4 : nullptr;
-  if (B.nb > 0)
-    if (int rc = small_launch_x(ctx, 2, S.x, B.pbond, nullptr, B.nb, nullptr, nullptr, 1.0, 1.0, 1, 1, nullptr,
-                                energy ? S.e + E_ERF : nullptr, B.ss, q, f, dq, edq))
-      return rc;
-  if (energy && B.ncn > 0)
-    if (int rc = small_launch_x(ctx, 2, S.x, B.pcn, nullptr, B.ncn, nullptr, nullptr, 1.0, 1.0, 1, 0, nullptr,
-                                S.e + E_ERF + 4, B.ss, q, nullptr, dq, edq))
-      return rc;
-  if (B.n13 > 0)
-    if (int rc = small_launch_x(ctx, 2, S.x, B.p13, nullptr, B.n13, nullptr, nullptr, 1.0, 1.0, 1, 1, nullptr,
-                                energy ? S.e + E_ERF + 8 : nullptr, B.ss, q, f, dq, edq))
-      return rc;
-  if (B.n14 > 0)
-    if (int rc = small_launch_x(ctx, 2, S.x, B.p14, nullptr, B.n14, nullptr, nullptr, 1.0 - B.fudge, 1.0, 1, 1,
-                                nullptr, energy ? S.e + E_ERF + 12 : nullptr, B.ss, q, f, dq, edq))
-      return rc;
-  return ORAC_OK;
+  // bonds, constraints (energy only, and only when energies are wanted),
+  // 1-3 pairs, 1-4 pairs: one launch, each list into its energy slots
+  const int* lists[4] = {B.pbond, B.pcn, B.p13, B.p14};
+  const int n[4] = {B.nb, energy ? B.ncn : 0, B.n13, B.n14};
+  const double fudge[4] = {1.0, 1.0, 1.0, 1.0 - B.fudge};
+  const int forces[4] = {1, 0, 1, 1};
+  double* e[4] = {energy ? S.e + E_ERF : nullptr, S.e + E_ERF + 4, energy ? S.e + E_ERF + 8 : nullptr,
+                  energy ? S.e + E_ERF + 12 : nullptr};
+  return ferrf_launch_lists(ctx, 4, lists, n, fudge, forces, e, S.x, B.ss, q, f, dq, edq);
 }
 
 // one shell's pair forces into its level accumulator (zeroed by the
