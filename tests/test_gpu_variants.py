@@ -190,17 +190,18 @@ def test_alchemy_pme_dudl_matches_oracle_central_difference():
     assert abs(dudl - fd) <= 1e-5 * abs(fd), (dudl, fd)
 
 
-def test_md_window_dudl_is_derivative_of_potential():
+@pytest.mark.parametrize("form", sorted(FORMS))
+def test_md_window_dudl_is_derivative_of_potential(form):
     """Record column 15 of an alchemical MD window (shells, SPME, erf
     corrections, self term) against the central difference of the oracle's
     potential energy at the same configuration (a 1e-9 fs step leaves the
-    atoms in place)."""
+    atoms in place), with either pair form."""
     from orac_b200.engine import Engine
 
     s = systems.ligand_in_water()
     lam, h = 0.3, 1e-4
     g = Engine(s.copy())
-    g.set_alchemy(s.ss_alchemy)
+    g.set_alchemy(s.ss_alchemy, **FORMS[form])
     g.set_lambda(0.0, lam, 0.0, lam, dlam=[0.0, 1.0, 0.0, 1.0])
     g.md_setup(1e-9, 2, 4, 6, "l")
     rec = g.md_run(1, energy_every=1)
@@ -210,7 +211,7 @@ def test_md_window_dudl_is_derivative_of_potential():
     for sgn in (1, -1):
         lr = lam + sgn * h
         o = oracle.Oracle(s.copy())
-        o.set_alchemy(s.ss_alchemy)
+        o.set_alchemy(s.ss_alchemy, **FORMS[form])
         o.set_lambda(0.0, lr, 0.0, lr)
         o.update_lists()
         esh = sum(o.shell(sh)[1].sum() for sh in "mlh")
