@@ -332,7 +332,11 @@ int orac_gpu_pme_kspace_static(void* stream, int numatoms, const double* xyz,
  * dt_h is the outer (H) time step in fs, lrespa/mrespa/n1respa/n0respa the
  * substeps of the L, M, N1 and N0 levels, nupdte the list-update period in
  * H steps, rshk the shell ('m','l','h') that carries the SPME term; econst is
- * added to the reported total energy (self and constraint corrections). */
+ * added to the reported total energy (self and constraint corrections).
+ * The driver captures its step as CUDA graphs on the first run; a later
+ * orac_gpu_set_lambda, _set_rem, _set_alchemy(_shift), _set_shells,
+ * _set_ewald, _set_box or _set_linked_cell makes the next run capture them
+ * again, so the change takes effect at the next step. */
 int orac_gpu_md_setup(orac_gpu_ctx* ctx, const double* x, const double* y,
                       const double* z, const double* vx, const double* vy,
                       const double* vz, const int* cnst, const double* dss,
@@ -374,7 +378,10 @@ int orac_gpu_md_set_graphs(orac_gpu_ctx* ctx, int on);
  * and their kernels run concurrently.  Replaces running ORAC replicas as
  * separate MPI ranks (src/rem.f90, src/orac_mpi.f90).  The contexts must be
  * set up with orac_gpu_md_setup, share one device, one list-update period
- * and one step index, and must not be driven on their own while batched. */
+ * and one step index, and must not be driven on their own while batched.
+ * The batch holds copies of the step graphs: after a parameter setter on a
+ * member context, orac_gpu_batch_run returns ORAC_ERR_STATE until the batch
+ * is built again. */
 typedef struct orac_gpu_batch orac_gpu_batch;
 int orac_gpu_batch_create(orac_gpu_ctx** ctxs, int n, orac_gpu_batch** out);
 int orac_gpu_batch_run(orac_gpu_batch* b, int nsteps);

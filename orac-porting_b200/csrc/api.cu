@@ -451,6 +451,7 @@ int orac_gpu_set_topology(orac_gpu_ctx* ctx, int ntap, int ngrp, int nprot, cons
 
 int orac_gpu_set_ewald(orac_gpu_ctx* ctx, int clewld, double alphal, int order, int nfft1, int nfft2, int nfft3,
                        double rkcut) {
+  if (ctx) ctx->param_gen++;  // kernels capture these values: step graphs are re-captured
   if (!ctx) return ORAC_ERR_PARAM;
   if (clewld && (alphal <= 0 || order < 3 || order > 12 || nfft1 < order || nfft2 < order || nfft3 < order ||
                  nfft1 > 512 || nfft2 > 512 || nfft3 > 512))
@@ -470,6 +471,7 @@ int orac_gpu_set_ewald(orac_gpu_ctx* ctx, int clewld, double alphal, int order, 
 
 int orac_gpu_set_shells(orac_gpu_ctx* ctx, double rcutm, double rtolm, double rneim, double rcutl, double rtoll,
                         double rneil, double rcuth, double rtolh, double rneih) {
+  if (ctx) ctx->param_gen++;  // kernels capture these values: step graphs are re-captured
   if (!ctx) return ORAC_ERR_PARAM;
   ctx->sh = {rcutm, rtolm, rneim, rcutl, rtoll, rneil, rcuth, rtolh, rneih};
   ctx->have_shells = true;
@@ -477,6 +479,7 @@ int orac_gpu_set_shells(orac_gpu_ctx* ctx, double rcutm, double rtolm, double rn
 }
 
 int orac_gpu_set_linked_cell(orac_gpu_ctx* ctx, int ncx, int ncy, int ncz) {
+  if (ctx) ctx->param_gen++;  // kernels capture these values: step graphs are re-captured
   if (!ctx) return ORAC_ERR_PARAM;
   if (ncx < 0 || ncy < 0 || ncz < 0 || (long)ncx * ncy * ncz > 16 * 1024 * 1024)
     return ctx_fail(ctx, ORAC_ERR_PARAM, "bad linked cell grid");
@@ -487,6 +490,7 @@ int orac_gpu_set_linked_cell(orac_gpu_ctx* ctx, int ncx, int ncy, int ncz) {
 }
 
 int orac_gpu_set_box(orac_gpu_ctx* ctx, const double* co, const double* oc) {
+  if (ctx) ctx->param_gen++;  // kernels capture these values: step graphs are re-captured
   if (!ctx || !co || !oc) return ORAC_ERR_PARAM;
   if (co[1] != 0.0 || co[2] != 0.0 || co[5] != 0.0)
     return ctx_fail(ctx, ORAC_ERR_PARAM, "co must be upper triangular (ORAC's convention)");

@@ -176,6 +176,7 @@ void variant_free(orac_gpu_ctx* ctx) {
 extern "C" {
 
 int orac_gpu_set_rem(orac_gpu_ctx* ctx, const int* rematom, int kind, double rem_factor) {
+  if (ctx) ctx->param_gen++;  // kernels capture these values: step graphs are re-captured
   if (!ctx || !ctx->have_topo) return ctx ? ctx_fail(ctx, ORAC_ERR_STATE, "topology not set") : ORAC_ERR_PARAM;
   CK(cudaSetDevice(ctx->device));
   if (!rematom) {
@@ -196,6 +197,7 @@ int orac_gpu_set_rem(orac_gpu_ctx* ctx, const int* rematom, int kind, double rem
 
 int orac_gpu_set_alchemy(orac_gpu_ctx* ctx, const int* ss_alchemy, const double* rmin, const double* epsm,
                          double qsoft, double ljsoft, int opls) {
+  if (ctx) ctx->param_gen++;  // kernels capture these values: step graphs are re-captured
   if (!ctx || !ctx->have_topo) return ctx ? ctx_fail(ctx, ORAC_ERR_STATE, "topology not set") : ORAC_ERR_PARAM;
   CK(cudaSetDevice(ctx->device));
   if (!ss_alchemy) {
@@ -230,6 +232,7 @@ int orac_gpu_set_alchemy(orac_gpu_ctx* ctx, const int* ss_alchemy, const double*
 }
 
 int orac_gpu_set_alchemy_shift(orac_gpu_ctx* ctx, int shifted, double qshift, double ljshift) {
+  if (ctx) ctx->param_gen++;  // kernels capture these values: step graphs are re-captured
   if (!ctx) return ORAC_ERR_PARAM;
   if (shifted && !(qshift >= 0.0 && ljshift >= 0.0))
     return ctx_fail(ctx, ORAC_ERR_PARAM, "qshift %g and ljshift %g must be >= 0", qshift, ljshift);
@@ -241,6 +244,7 @@ int orac_gpu_set_alchemy_shift(orac_gpu_ctx* ctx, int shifted, double qshift, do
 }
 
 int orac_gpu_set_lambda(orac_gpu_ctx* ctx, const double* lam, int intramol, int ljintra, const double* dlam) {
+  if (ctx) ctx->param_gen++;  // kernels capture these values: step graphs are re-captured
   if (!ctx) return ORAC_ERR_PARAM;
   if (ctx->h_ssal.empty()) return ctx_fail(ctx, ORAC_ERR_STATE, "orac_gpu_set_alchemy first");
   if (!lam) return ctx_fail(ctx, ORAC_ERR_PARAM, "lam is required");

@@ -19,6 +19,7 @@ int md_check_flags(orac_gpu_ctx* ctx);
 
 struct orac_gpu_batch {
   std::vector<orac_gpu_ctx*> ctx;
+  std::vector<unsigned> gen;  // each context's param_gen when the batch was built
   cudaStream_t stream = nullptr;
   cudaGraphExec_t exec[2] = {nullptr, nullptr};
   cudaGraph_t graph[2] = {nullptr, nullptr};
@@ -71,6 +72,7 @@ int orac_gpu_batch_create(orac_gpu_ctx** ctxs, int n, orac_gpu_batch** out) {
       return ORAC_ERR_PARAM;
     }
     b->ctx.push_back(ctxs[k]);
+    b->gen.push_back(ctxs[k]->param_gen);
   }
   if (cudaSetDevice(b->device) != cudaSuccess ||
       cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) {
@@ -118,6 +120,9 @@ int orac_gpu_batch_run(orac_gpu_batch* b, int nsteps) {
   for (auto* c : b->ctx)
     if (md_nupdte(c) != nup || md_step_index(c) != st0 || nup <= 0)
       return bfail(b, ORAC_ERR_STATE, "batched systems need md_setup, one list-update period and one step index");
+  for (size_t k = 0; k < b->ctx.size(); k++)
+    if (b->ctx[k]->param_gen != b->gen[k])
+      return bfail(b, ORAC_ERR_STATE, "a system's parameters changed after the batch was built: build it again");
   for (int s = 0; s < nsteps; s++) {
     const long long step = md_step_index(b->ctx[0]);
     const int kind = (step % nup == 0 && step > 0) ? 1 : 0;

@@ -221,6 +221,10 @@ struct MdState;  // md.cu
 struct orac_gpu_ctx {
   MdState* md = nullptr;
   bool shared_device = false;  // advanced beside other contexts (batch, server)
+  // bumped by every setter whose values kernels take by value (shells,
+  // Ewald, box, cells, variant, lambdas): captured step graphs older than
+  // it are captured again
+  unsigned param_gen = 0;
   std::unordered_map<void*, size_t> dmem;  // live device allocations
   size_t dmem_bytes = 0;
   int device = 0;

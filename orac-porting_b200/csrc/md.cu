@@ -1033,6 +1033,7 @@ struct MdState {
   long long step = 0;
   double econst = 0;
   cudaGraph_t graph = nullptr;
+  unsigned graphs_gen = 0;  // ctx->param_gen when the graphs were captured
   cudaGraphExec_t gexec = nullptr;
   cudaGraph_t graph_u = nullptr;  // step with list update
   cudaGraphExec_t gexec_u = nullptr;
@@ -1825,8 +1826,9 @@ int orac_gpu_md_set_graphs(orac_gpu_ctx* ctx, int on) {
 
 // capture (once) the step graph of one kind: 0 plain step, 1 step with list update
 static int md_capture(orac_gpu_ctx* ctx, MdState& S, int kind) {
-  if ((S.gexec || S.gexec_u) && S.graphs_shared != ctx->shared_device) {
-    // captured for the other device-sharing mode: capture again
+  if ((S.gexec || S.gexec_u) && (S.graphs_shared != ctx->shared_device || S.graphs_gen != ctx->param_gen)) {
+    // captured for the other device-sharing mode, or before a parameter
+    // changed (a new lambda, REM factor, box, ...): capture again
     if (S.gexec) cudaGraphExecDestroy(S.gexec);
     if (S.graph) cudaGraphDestroy(S.graph);
     if (S.gexec_u) cudaGraphExecDestroy(S.gexec_u);
@@ -1835,6 +1837,7 @@ static int md_capture(orac_gpu_ctx* ctx, MdState& S, int kind) {
     S.graph = S.graph_u = nullptr;
   }
   S.graphs_shared = ctx->shared_device;
+  S.graphs_gen = ctx->param_gen;
   cudaGraphExec_t* ge = kind ? &S.gexec_u : &S.gexec;
   cudaGraph_t* gg = kind ? &S.graph_u : &S.graph;
   if (*ge) return ORAC_OK;

@@ -228,3 +228,32 @@ def test_md_window_dudl_is_derivative_of_potential(form):
         u.append(esh + epme + eerf + eself)
     fd = (u[0] - u[1]) / (2 * h)
     assert abs(dudl - fd) <= 1e-5 * abs(fd), (dudl, fd)
+
+
+def test_lambda_change_after_md_setup_reaches_the_step_graphs():
+    """A window moved to a new lambda after md_setup: its next step reports
+    the dU/dlambda of a window set up at that lambda directly (the captured
+    step graphs are captured again when a parameter changes; 1e-9 fs steps
+    leave the atoms in place)."""
+    from orac_b200.engine import Engine
+
+    s = systems.ligand_in_water()
+
+    def window(lam):
+        g = Engine(s.copy())
+        g.set_alchemy(s.ss_alchemy)
+        g.set_lambda(0.0, lam, 0.0, lam, dlam=[0.0, 1.0, 0.0, 1.0])
+        g.md_setup(1e-9, 2, 4, 6, "l")
+        return g
+
+    g = window(0.2)
+    d_a = g.md_run(1, energy_every=1)[0, 15]
+    g.set_lambda(0.0, 0.7, 0.0, 0.7, dlam=[0.0, 1.0, 0.0, 1.0])
+    d_b = g.md_run(1, energy_every=1)[0, 15]
+    g.close()
+    ref = window(0.7)
+    ref.md_run(1, energy_every=1)
+    d_ref = ref.md_run(1, energy_every=1)[0, 15]
+    ref.close()
+    assert abs(d_b - d_a) > 1e-3 * abs(d_a)
+    assert abs(d_b - d_ref) <= 1e-6 * abs(d_ref), (d_b, d_ref)
