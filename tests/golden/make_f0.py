@@ -6,13 +6,14 @@ wrote (test2/b-RSTRT/ij4i0000.rst, step 30).  Only the arrays the force
 path needs are kept, in the files' own units and 1-based indices;
 orac_b200.oracio.system_from_orac turns them into a System.
 
-Also builds tests/golden/f0_orac_records.npz: the positions and boxes of
-test2's other two replica-1 restart files (ij4i0001.rst, ij4i0003.rst) and,
-for all three states, the energy record ORAC printed at the step it wrote
-the restart (test2/PAR0001/out0001, matched by box edge and temperature).
+Also builds tests/golden/f0_orac_records.npz: the positions, velocities and
+boxes of test2's other two replica-1 restart files (ij4i0001.rst,
+ij4i0003.rst) and, for all three states, the energy record ORAC printed at
+the step it wrote the restart (test2/PAR0001/out0001, matched by box edge
+and temperature).
 
-Run from the repository root where the reference checkout is present:
-    python tests/golden/make_f0.py [reference root]
+Run from the repository root with the path of a reference checkout:
+    python tests/golden/make_f0.py <reference root>
 """
 import os
 import re
@@ -26,7 +27,6 @@ from orac_b200 import oracio  # noqa: E402
 
 KEYS_INT = ("ss_index", "nbtype", "grppt", "lbnd", "lbndg", "ltor", "litr", "int14", "type14", "int13", "mapnl")
 KEYS_F = ("chrge", "mass", "potbo", "potbe", "potto", "potit", "pnbd")
-DEFAULT_ROOT = "/root/reference"
 SCALARS = ("ntap", "ngrp", "lbond", "lbend", "ltors", "litor", "lpnbd", "int14p", "int13p", "nmapnl", "iz")
 
 
@@ -67,7 +67,8 @@ def parse_records(path):
 def build_records(root, ntap):
     """The replica-1 states that test2 saved as restart files with the
     energy record ORAC printed for the same step (matched by box edge and
-    temperature): positions and box of each, and the record's columns."""
+    temperature): positions, velocities and box of each, and the record's
+    columns."""
     recs = parse_records(os.path.join(root, "test2", "PAR0001", "out0001"))
     out = {"keys": np.array(RECORD_KEYS), "restarts": np.array(RESTARTS)}
     vals, where = [], []
@@ -83,13 +84,16 @@ def build_records(root, ntap):
         if k > 0:  # the first state is f0_fkbp12.npz's own
             out[f"co{k}"] = rs["co"]
             out[f"xyz{k}"] = rs["xyz"]
+            out[f"v{k}"] = rs["v"]
     out["printed"] = np.array(vals)
     out["out0001_line"] = np.array(where)
     return out
 
 
 def main():
-    root = sys.argv[1] if len(sys.argv) > 1 else DEFAULT_ROOT
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_f0.py <reference root>")
+    root = sys.argv[1]
     arrs = build_arrays(root)
     path = os.path.join(HERE, "f0_fkbp12.npz")
     np.savez_compressed(path, **arrs)
