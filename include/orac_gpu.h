@@ -311,11 +311,14 @@ int orac_gpu_fft_pme_dev(orac_gpu_ctx* ctx, const double* xyz_scaled,
  * means no reciprocal-space cut.  err (may be NULL) receives a message of at
  * most err_len bytes on failure.
  *
- * The first call on a device looks up the scratch array's device address
- * (cudaGetSymbolAddress, with that device current); make that first call
- * before any stream capture.  Every call on a device shares the one array:
- * calls that overlap on the GPU (other streams, other host threads) race and
- * give wrong results — serialise them. */
+ * Every call looks up the scratch array's device address
+ * (cudaGetSymbolAddress, with the device current), so a device context that
+ * is destroyed and created again (cudaDeviceReset) is followed.  The first
+ * lookup on a device may load the library's device code: make the first call
+ * on each device before any stream capture; a first call made while `stream`
+ * is capturing returns ORAC_ERR_STATE.  Every call on a device shares the one
+ * array: calls that overlap on the GPU (other streams, other host threads)
+ * race and give wrong results — serialise them. */
 int orac_gpu_pme_kspace_static(void* stream, int numatoms, const double* xyz,
                                const double* charge, const double* recip,
                                double volume, double ewald_coeff, double rkcut,

@@ -451,12 +451,13 @@ int orac_gpu_set_topology(orac_gpu_ctx* ctx, int ntap, int ngrp, int nprot, cons
 
 int orac_gpu_set_ewald(orac_gpu_ctx* ctx, int clewld, double alphal, int order, int nfft1, int nfft2, int nfft3,
                        double rkcut) {
-  if (ctx) ctx->param_gen++;  // kernels capture these values: step graphs are re-captured
+  ParamGenBump bump(ctx);  // kernels capture these values: step graphs are re-captured
   if (!ctx) return ORAC_ERR_PARAM;
   if (clewld && (alphal <= 0 || order < 3 || order > 12 || nfft1 < order || nfft2 < order || nfft3 < order ||
                  nfft1 > 512 || nfft2 > 512 || nfft3 > 512))
     return ctx_fail(ctx, ORAC_ERR_PARAM, "bad PME parameters alpha=%g order=%d grid=%dx%dx%d", alphal, order, nfft1,
                     nfft2, nfft3);
+  bump.arm();
   ctx->clewld = clewld ? 1 : 0;
   ctx->alphal = alphal;
   ctx->order = order;
@@ -471,18 +472,20 @@ int orac_gpu_set_ewald(orac_gpu_ctx* ctx, int clewld, double alphal, int order, 
 
 int orac_gpu_set_shells(orac_gpu_ctx* ctx, double rcutm, double rtolm, double rneim, double rcutl, double rtoll,
                         double rneil, double rcuth, double rtolh, double rneih) {
-  if (ctx) ctx->param_gen++;  // kernels capture these values: step graphs are re-captured
+  ParamGenBump bump(ctx);  // kernels capture these values: step graphs are re-captured
   if (!ctx) return ORAC_ERR_PARAM;
+  bump.arm();
   ctx->sh = {rcutm, rtolm, rneim, rcutl, rtoll, rneil, rcuth, rtolh, rneih};
   ctx->have_shells = true;
   return ORAC_OK;
 }
 
 int orac_gpu_set_linked_cell(orac_gpu_ctx* ctx, int ncx, int ncy, int ncz) {
-  if (ctx) ctx->param_gen++;  // kernels capture these values: step graphs are re-captured
+  ParamGenBump bump(ctx);  // kernels capture these values: step graphs are re-captured
   if (!ctx) return ORAC_ERR_PARAM;
   if (ncx < 0 || ncy < 0 || ncz < 0 || (long)ncx * ncy * ncz > 16 * 1024 * 1024)
     return ctx_fail(ctx, ORAC_ERR_PARAM, "bad linked cell grid");
+  bump.arm();
   ctx->ncx = ncx;
   ctx->ncy = ncy;
   ctx->ncz = ncz;
@@ -490,10 +493,11 @@ int orac_gpu_set_linked_cell(orac_gpu_ctx* ctx, int ncx, int ncy, int ncz) {
 }
 
 int orac_gpu_set_box(orac_gpu_ctx* ctx, const double* co, const double* oc) {
-  if (ctx) ctx->param_gen++;  // kernels capture these values: step graphs are re-captured
+  ParamGenBump bump(ctx);  // kernels capture these values: step graphs are re-captured
   if (!ctx || !co || !oc) return ORAC_ERR_PARAM;
   if (co[1] != 0.0 || co[2] != 0.0 || co[5] != 0.0)
     return ctx_fail(ctx, ORAC_ERR_PARAM, "co must be upper triangular (ORAC's convention)");
+  bump.arm();
   memcpy(ctx->co, co, sizeof(ctx->co));
   memcpy(ctx->oc, oc, sizeof(ctx->oc));
   ctx->volume = 8.0 * std::fabs(co[0] * co[4] * co[8]);

@@ -176,16 +176,18 @@ void variant_free(orac_gpu_ctx* ctx) {
 extern "C" {
 
 int orac_gpu_set_rem(orac_gpu_ctx* ctx, const int* rematom, int kind, double rem_factor) {
-  if (ctx) ctx->param_gen++;  // kernels capture these values: step graphs are re-captured
+  ParamGenBump bump(ctx);  // kernels capture these values: step graphs are re-captured
   if (!ctx || !ctx->have_topo) return ctx ? ctx_fail(ctx, ORAC_ERR_STATE, "topology not set") : ORAC_ERR_PARAM;
   CK(cudaSetDevice(ctx->device));
   if (!rematom) {
+    bump.arm();
     if (ctx->variant == VAR_REM) ctx->variant = VAR_STD;
     ctx->h_rem.clear();
     return ORAC_OK;
   }
   if (kind < 0 || kind > 2) return ctx_fail(ctx, ORAC_ERR_PARAM, "REM segment kind %d (0, 1 or 2)", kind);
   if (!(rem_factor >= 0.0)) return ctx_fail(ctx, ORAC_ERR_PARAM, "rem_factor %g", rem_factor);
+  bump.arm();
   ctx->h_rem.assign(ctx->N, 0);
   for (int a = 0; a < ctx->N; a++) ctx->h_rem[a] = rematom[a] ? 1 : 0;
   ctx->rem_kind = kind;
@@ -197,10 +199,11 @@ int orac_gpu_set_rem(orac_gpu_ctx* ctx, const int* rematom, int kind, double rem
 
 int orac_gpu_set_alchemy(orac_gpu_ctx* ctx, const int* ss_alchemy, const double* rmin, const double* epsm,
                          double qsoft, double ljsoft, int opls) {
-  if (ctx) ctx->param_gen++;  // kernels capture these values: step graphs are re-captured
+  ParamGenBump bump(ctx);  // kernels capture these values: step graphs are re-captured
   if (!ctx || !ctx->have_topo) return ctx ? ctx_fail(ctx, ORAC_ERR_STATE, "topology not set") : ORAC_ERR_PARAM;
   CK(cudaSetDevice(ctx->device));
   if (!ss_alchemy) {
+    bump.arm();
     if (ctx->variant == VAR_ALCH) ctx->variant = VAR_STD;
     ctx->h_ssal.clear();
     return ORAC_OK;
@@ -218,6 +221,7 @@ int orac_gpu_set_alchemy(orac_gpu_ctx* ctx, const int* ss_alchemy, const double*
     sf[a] = make_float2((float)rmin[a], (float)(2.0 * std::sqrt(epsm[a])));
     sd[a] = make_double2(rmin[a], epsm[a]);
   }
+  bump.arm();
   ctx->h_ssal.assign(ss_alchemy, ss_alchemy + N);
   if (!ctx->d_soft && (dev_alloc(ctx, &ctx->d_soft, N) || dev_alloc(ctx, &ctx->d_softd, N))) return ORAC_ERR_CUDA;
   CK(cudaMemcpy(ctx->d_soft, sf.data(), sizeof(float2) * N, cudaMemcpyHostToDevice));
@@ -232,10 +236,11 @@ int orac_gpu_set_alchemy(orac_gpu_ctx* ctx, const int* ss_alchemy, const double*
 }
 
 int orac_gpu_set_alchemy_shift(orac_gpu_ctx* ctx, int shifted, double qshift, double ljshift) {
-  if (ctx) ctx->param_gen++;  // kernels capture these values: step graphs are re-captured
+  ParamGenBump bump(ctx);  // kernels capture these values: step graphs are re-captured
   if (!ctx) return ORAC_ERR_PARAM;
   if (shifted && !(qshift >= 0.0 && ljshift >= 0.0))
     return ctx_fail(ctx, ORAC_ERR_PARAM, "qshift %g and ljshift %g must be >= 0", qshift, ljshift);
+  bump.arm();
   ctx->at.shifted = shifted ? 1 : 0;
   ctx->at.qshift = shifted ? qshift : 0.0;
   // ORAC's two6 = 2.d0**(1./6.), the exponent a single-precision constant
@@ -244,13 +249,14 @@ int orac_gpu_set_alchemy_shift(orac_gpu_ctx* ctx, int shifted, double qshift, do
 }
 
 int orac_gpu_set_lambda(orac_gpu_ctx* ctx, const double* lam, int intramol, int ljintra, const double* dlam) {
-  if (ctx) ctx->param_gen++;  // kernels capture these values: step graphs are re-captured
+  ParamGenBump bump(ctx);  // kernels capture these values: step graphs are re-captured
   if (!ctx) return ORAC_ERR_PARAM;
   if (ctx->h_ssal.empty()) return ctx_fail(ctx, ORAC_ERR_STATE, "orac_gpu_set_alchemy first");
   if (!lam) return ctx_fail(ctx, ORAC_ERR_PARAM, "lam is required");
   for (int k = 0; k < 8; k++)
     if (!(std::fabs(lam[k]) <= 1.0)) return ctx_fail(ctx, ORAC_ERR_PARAM, "lambda %d = %g outside [-1, 1]", k, lam[k]);
   CK(cudaSetDevice(ctx->device));
+  bump.arm();
   for (int k = 0; k < 8; k++) ctx->lam[k] = lam[k];
   const double d0[4] = {0, 0, 0, 0};
   const double* d = dlam ? dlam : d0;

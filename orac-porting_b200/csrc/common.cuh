@@ -341,6 +341,19 @@ struct orac_gpu_ctx {
   int64_t prof_n = 0;
 };
 
+// Bumps ctx->param_gen when it goes out of scope, once armed: a setter arms
+// it after its arguments have been validated, so a rejected call leaves the
+// captured step graphs (and batches built on them) valid.
+struct ParamGenBump {
+  orac_gpu_ctx* ctx;
+  bool armed = false;
+  explicit ParamGenBump(orac_gpu_ctx* c) : ctx(c) {}
+  void arm() { armed = true; }
+  ~ParamGenBump() {
+    if (armed && ctx) ctx->param_gen++;
+  }
+};
+
 // record the start/end events of one profiled launch (no-op unless prof)
 int prof_begin(orac_gpu_ctx* ctx, int* slot);
 int prof_end(orac_gpu_ctx* ctx, int slot);

@@ -61,7 +61,7 @@ int make_plan(int n, FftPlan* p) {
       p->rad[p->nst++] = r;
       m /= r;
     }
-  if (m != 1 || n > 4096) return -1;
+  if (m != 1 || n > 2048) return -1;  // 3 lines of 2048 complex values fill 48 KB of shared memory
   int ns = 1;
   for (int s = 0; s < p->nst; s++) {
     const int R = p->rad[s];
@@ -593,7 +593,10 @@ int upload_tw(orac_gpu_ctx* ctx, float2** dst, int n) {
 int lines_per_block(int n) {
   // few lines per block: the grids here are small (32^3-96^3), so many
   // small blocks spread a pass over all SMs
-  int B = 3072 / n;  // 2 buffers * B * n * 8 bytes <= 48 KB
+  // (2B + 1) lines of n complex values (two buffers of B lines and the
+  // twiddles) in the 48 KB of shared memory a launch gets without opting in;
+  // make_plan's axis limit keeps B >= 1 inside it
+  int B = (49152 / (8 * n) - 1) / 2;
   if (B > 4) B = 4;
   if (B < 1) B = 1;
   return B;
@@ -768,8 +771,8 @@ int pme_run(orac_gpu_ctx* ctx, int natom, const double* d_cart, const double* d_
 //
 // Host code must never hand orac_static_pme_scratch itself to a kernel: on
 // the host that name is a stand-in, not a device address.  The device address
-// is looked up with cudaGetSymbolAddress once per device, with that device
-// current, on the first call made on it.
+// is looked up with cudaGetSymbolAddress, with the device current, on every
+// call (static_scratch).
 #define ORAC_STATIC_PME_BYTES (5u * 1024u * 1024u + 16u * 1024u)
 static __device__ __align__(256) unsigned char orac_static_pme_scratch[ORAC_STATIC_PME_BYTES];
 
@@ -780,7 +783,7 @@ constexpr long long STATIC_MAX_POINTS = 262144;  // n1*n2*n3 (64^3)
 constexpr int STATIC_MAX_DEVICES = 64;
 
 std::mutex g_static_mu;
-unsigned char* g_static_base[STATIC_MAX_DEVICES];  // device address of the array, per device
+bool g_static_seen[STATIC_MAX_DEVICES];  // devices whose scratch address has been looked up once
 
 struct SplineAt0 {
   double c[MAXORD + 2];
@@ -845,18 +848,34 @@ int static_fail(char* err, int err_len, int code, const char* fmt, ...) {
   return code;
 }
 
-// device address of the scratch array on device dev (which is current)
-int static_scratch(int dev, unsigned char** out, char* err, int err_len) {
+// Device address of the scratch array on device dev (which is current).
+// Looked up on every call: if the process destroys the device's context and
+// a new one is created (cudaDeviceReset, a primary-context reset by another
+// library), the module is loaded again and the array may sit elsewhere, so a
+// saved address could be stale.  The first lookup on a device may load the
+// module, which must not happen inside a stream capture: such a first call
+// is refused with ORAC_ERR_STATE.
+int static_scratch(int dev, cudaStream_t st, unsigned char** out, char* err, int err_len) {
   std::lock_guard<std::mutex> lock(g_static_mu);
-  if (!g_static_base[dev]) {
-    void* p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, orac_static_pme_scratch);
-    if (e != cudaSuccess || !p)
-      return static_fail(err, err_len, ORAC_ERR_CUDA, "cudaGetSymbolAddress of the SPME scratch on device %d: %s",
+  if (!g_static_seen[dev]) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    const cudaError_t e = cudaStreamIsCapturing(st, &cs);
+    if (e != cudaSuccess)
+      return static_fail(err, err_len, ORAC_ERR_STATE, "cudaStreamIsCapturing before the first call on device %d: %s",
                          dev, cudaGetErrorString(e));
-    g_static_base[dev] = (unsigned char*)p;
+    if (cs != cudaStreamCaptureStatusNone)
+      return static_fail(err, err_len, ORAC_ERR_STATE,
+                         "first call on device %d made while its stream is being captured: make one call on the "
+                         "device before any capture",
+                         dev);
   }
-  *out = g_static_base[dev];
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, orac_static_pme_scratch);
+  if (e != cudaSuccess || !p)
+    return static_fail(err, err_len, ORAC_ERR_CUDA, "cudaGetSymbolAddress of the SPME scratch on device %d: %s", dev,
+                       cudaGetErrorString(e));
+  g_static_seen[dev] = true;
+  *out = (unsigned char*)p;
   return ORAC_OK;
 }
 
@@ -917,9 +936,9 @@ extern "C" int orac_gpu_pme_kspace_static(void* stream, int numatoms, const doub
   if (dev < 0 || dev >= STATIC_MAX_DEVICES)
     return static_fail(err, err_len, ORAC_ERR_PARAM, "device %d beyond the %d this entry point tracks", dev,
                        STATIC_MAX_DEVICES);
-  unsigned char* base = nullptr;
-  if (int rc = static_scratch(dev, &base, err, err_len)) return rc;
   cudaStream_t st = (cudaStream_t)stream;
+  unsigned char* base = nullptr;
+  if (int rc = static_scratch(dev, st, &base, err, err_len)) return rc;
   double* eout = (double*)base;
   float2* tw = (float2*)(base + o_tw);
   float* bsp = (float*)(base + o_bsp);
