@@ -441,6 +441,12 @@ int orac_gpu_prof_enable(orac_gpu_ctx* ctx, int on);
 int orac_gpu_prof_read(orac_gpu_ctx* ctx, double* ms_total, int64_t* nlaunch,
                        int reset);
 
+/* FP32 FMA rate of `device` in TFLOP/s (an FMA counts 2), measured by an
+ * FMA-loop kernel that fills every SM (best of three timed launches, about
+ * 20 ms each); ms receives the best launch's time.  The denominator of the
+ * real-space kernel's FP32 roofline. */
+int orac_gpu_fp32_rate(int device, double* tflops, double* ms);
+
 /* Bytes of device memory the context holds (every device allocation it
  * made and has not freed): the footprint a memory-budgeted scheduler
  * admits by. */

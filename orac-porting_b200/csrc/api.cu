@@ -109,16 +109,6 @@ int shell_run(orac_gpu_ctx* ctx, char rshell, const double* d_xyz, const double*
                      SH_STRESS | (energy ? SH_ENERGY : 0));
 }
 
-// lanes per group on the innermost shell, ORAC_KPAIR_LPG_M=32 restores one
-// warp per group
-static int kpair_lpg_inner() {
-  static const int v = [] {
-    const char* e = getenv("ORAC_KPAIR_LPG_M");
-    return (e && atoi(e) == 32) ? 32 : 16;
-  }();
-  return v;
-}
-
 int shell_run_r(orac_gpu_ctx* ctx, char rshell, const ShellRadii& radii, const double* d_xyz, const double* d_grp,
                 const double* d_mol, double* d_f, double* d_e, double* d_stress, int flags) {
   ShellSel s;
@@ -198,8 +188,6 @@ int shell_run_r(orac_gpu_ctx* ctx, char rshell, const ShellRadii& radii, const d
   a.natom = ctx->N;
   a.wcnt = ctx->d_wcnt;
   variant_fill(ctx, &a);
-  // the innermost shell's rows hold about a dozen groups: half a warp each
-  a.lpg = rshell == 'm' ? kpair_lpg_inner() : 32;
   a.occ_hi = ctx->shared_device ? 1 : 0;
   const bool want_e = (flags & SH_ENERGY) && d_e, want_s = (flags & SH_STRESS) && d_stress;
   a.energy = want_e ? 1 : 0;

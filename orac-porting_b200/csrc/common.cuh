@@ -120,9 +120,6 @@ struct PairArgs {
   // 0: skip the image term of the molecular virial and the block reduction
   // (MD without pressure coupling needs neither)
   int stress;
-  // lanes that own one i group: 32, or 16 (two groups per warp) for lists
-  // with short rows; 16 applies to groups of at most 4 atoms
-  int lpg;
   // the context runs beside others (batch, server): the forces-only kernel
   // takes its higher-occupancy build (fewer registers, more warps per SM)
   int occ_hi;

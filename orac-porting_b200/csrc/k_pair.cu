@@ -2,8 +2,7 @@
 // (src/force.f:1-917).
 //
 // One warp owns one i-group (a charge group, <= ORAC_MAXG atoms, staged in
-// shared memory); its 32 lanes walk the group's neighbour-list row, one
-// partner group per lane.  Per partner the lane
+// shared memory) and its neighbour-list row.  Per partner group it
 //   1. forms the group-centre minimum image in FP64 scaled coordinates and
 //      classifies the pair into ORAC's bands (non-switched [rinn0, rout),
 //      switched S on [rout, rout0), 1-S on [rinn, rinn0)), src/force.f:265-333;
@@ -15,9 +14,10 @@
 //      entry's mask, src/force.f:396-731;
 //   4. for switched pairs adds the S'(R) V_ij term distributed by mass
 //      fraction, src/force.f:754-817.
-// i-atom forces stay in registers for the whole row and are warp-reduced
-// once; j-atom forces go to 64-bit fixed-point accumulators with atomics, so
-// the sum is independent of the order of the atomics.
+// Steps 1-2 run a lane per list entry; step 3 a lane per j atom of the
+// in-band entries, queued in shared memory (k_pair below).  Forces go to
+// 64-bit fixed-point accumulators with atomics, so the sum is independent
+// of the order of the atomics.
 // The molecular virial is assembled without per-pair work: ORAC's
 // sum_pairs f (x) (Rm_i - Rm_j - img) equals sum_atoms F_a (x) Rm_a (done in
 // the finalize kernel) plus, for pairs that cross the box, G_ij (x) co.img
@@ -29,7 +29,7 @@ namespace {
 constexpr int WPB = 4;  // warps per block
 constexpr float AS_A1 = 0.2548296f, AS_A2 = -0.28449674f, AS_A3 = 1.4214137f;
 constexpr float AS_A4 = -1.453152f, AS_A5 = 1.0614054f, AS_QP = 0.3275911f;
-constexpr int LJ_SMEM_MAX = 64 * 64;
+constexpr int LJ_SMEM_MAX = 2048;  // staged LJ table entries: 16 KB beside the static queues
 
 __device__ __forceinline__ void fix_add(unsigned long long* p, float v) {
   long long q = __float2ll_rn(v * (float)ORAC_FSCALE);
@@ -231,52 +231,82 @@ __device__ __forceinline__ void alch_energy_fp64(const PairArgs& A, double rx, d
 }
 
 #ifndef ORAC_KPAIR_MINB
-#define ORAC_KPAIR_MINB 6  // resident blocks per SM requested of the half-warp forces-only kernel
-#endif
-#ifndef ORAC_KPAIR_MINB32
-#define ORAC_KPAIR_MINB32 6  // the same for the warp-per-group (compacting) forces-only kernel
+#define ORAC_KPAIR_MINB 6  // resident blocks per SM requested of the forces-only kernel
 #endif
 #ifndef ORAC_KPAIR_MINB_HI
-#define ORAC_KPAIR_MINB_HI 8  // both, for contexts that share the device with others
+#define ORAC_KPAIR_MINB_HI 8  // the same, for contexts that share the device with others
 #endif
 
-// LPG lanes own one i-group: 32 (a warp) for the long rows of the L and H
-// lists, 16 (a half warp, two groups per warp) for the short rows of the M
-// list, where a full warp would leave most lanes idle.
+// Ring capacities of the per-warp queues.  Entries: at most 31 left over
+// from the previous chunk plus 32 new.  Atom slots: at most 31 left over
+// plus 32 entries of MG atoms.
+constexpr int QE = 64;
+template <int MG>
+struct SlotRing {
+  static constexpr int n = (31 + 32 * MG) <= 128 ? 128 : ((31 + 32 * MG) <= 256 ? 256 : 512);
+};
+
+// A slot names one j atom of a queued entry: entry (6 bits), its position t
+// among the entry's slots (3), its atom b in the j group (3), the entry's
+// slot count - 1 (3).
+__device__ __forceinline__ unsigned short slot_pack(int e, int t, int b, int n) {
+  return (unsigned short)(e | (t << 6) | (b << 9) | ((n - 1) << 12));
+}
+
+// One warp owns one i group for a whole list row.
+//
+// Phase 1 (a lane per list entry, 32 entries per chunk): FP64 minimum image
+// and band of the group pair, the next shell's list entry, and, for an
+// in-band entry, its geometry (FP32 centre distance, S, S', and in FP64 what
+// the energies need) into the warp's entry queue and one slot per j atom to
+// evaluate into the slot queue (order kept by ballots and a warp scan).
+//
+// Phase 2 (a lane per j atom): passes of up to 32 slots that hold whole
+// entries.  A lane takes its j atom's offset and charge once and runs over
+// the i atoms (broadcast reads of shared memory): the j
+// atom's force sums in the lane, and goes out with one fixed-point atomic per
+// component, S'(R) V term included; the entry's V is a segmented shuffle sum
+// over the entry's lanes.  The i atoms' forces sum per lane across passes
+// and leave by one warp reduction at the end of the row.
+//
 // HI: the build for contexts sharing the device, where throughput over many
 // concurrent kernels matters more than one launch's latency.
-template <int MG, bool EN, int VAR, int LPG, bool HI>
-__global__ void __launch_bounds__(WPB * 32, (MG <= 4 && !EN)
-                                                ? (HI ? ORAC_KPAIR_MINB_HI
-                                                      : (LPG == 16 ? ORAC_KPAIR_MINB : ORAC_KPAIR_MINB32))
-                                                : 1)
+template <int MG, bool EN, int VAR, bool HI>
+__global__ void __launch_bounds__(WPB * 32, (MG <= 4 && !EN) ? (HI ? ORAC_KPAIR_MINB_HI : ORAC_KPAIR_MINB) : 1)
     k_pair(const PairArgs A) {
   pdl_enter();
-  constexpr int SEG = 32 / LPG;  // groups per warp
-  // long rows (a warp per group): in-band entries are compacted through a
-  // shared queue so the pair work runs on every lane; the short rows of the
-  // half-warp kernel are mostly in band and run where they are
-  constexpr bool COMPACT = LPG == 32;
-  __shared__ int s_q[COMPACT ? WPB : 1][64];
+  constexpr int QS = SlotRing<MG>::n;
+  constexpr unsigned FULL = 0xffffffffu;
   extern __shared__ float2 s_lj[];
-  __shared__ float4 s_ai[WPB * SEG][MG];
-  __shared__ int s_ti[WPB * SEG][MG];  // the i atom's row of the LJ tables (type * ntype)
-  __shared__ float s_pm[WPB * SEG][MG];
-  __shared__ double s_qd[WPB * SEG][MG];
-  __shared__ int s_fi[WPB * SEG][MG];
-  __shared__ float2 s_sf[WPB * SEG][MG];
+  __shared__ float4 s_ai[WPB][MG];
+  __shared__ int s_ti[WPB][MG];  // the i atom's row of the LJ tables (type * ntype)
+  __shared__ float s_pm[WPB][MG];
+  __shared__ double s_qd[WPB][EN ? MG : 1];
+  __shared__ int s_fi[WPB][VAR != VAR_STD ? MG : 1];
+  __shared__ float2 s_sf[WPB][VAR == VAR_ALCH ? MG : 1];
+  // entry queue: centre distance and S, S', j group metadata, skip mask;
+  // FP64 distance and S and the Cartesian image for the energy build
+  __shared__ float4 s_edc[WPB][QE];
+  __shared__ float s_edsw[WPB][QE];
+  __shared__ int2 s_emeta[WPB][QE];
+  __shared__ unsigned long long s_emsk[WPB][QE];
+  __shared__ double4 s_ecd[EN ? WPB : 1][EN ? QE : 1];
+  __shared__ float4 s_eimg[EN ? WPB : 1][EN ? QE : 1];
+  __shared__ unsigned short s_slot[WPB][QS];
   __shared__ double s_red[WPB][ACC_N];
+  __shared__ double s_vimg[WPB][9];
 
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int sub = lane / LPG, sl = lane % LPG, slot = warp * SEG + sub;
+  const unsigned lanes_below = (1u << lane) - 1u;
   const int nt2 = A.ntype * A.ntype;
   const bool staged = nt2 <= LJ_SMEM_MAX;
-  __shared__ double s_vimg[WPB][9];
   if (threadIdx.x < WPB * 9) s_vimg[threadIdx.x / 9][threadIdx.x % 9] = 0.0;
   if (staged)
     for (int k = threadIdx.x; k < nt2; k += blockDim.x) s_lj[k] = A.lj[k];
   __syncthreads();
   const float2* lj = staged ? s_lj : A.lj;
+  // under lskip_ewald an atom without LJ has no pair to evaluate
+  const bool ljonly = VAR != VAR_ALCH && A.lskip && A.ewald;
 
   double ec0 = 0, ec1 = 0, ec2 = 0, eq0 = 0, eq1 = 0, eq2 = 0;
   double ex0 = 0, ex1 = 0, ex2 = 0;  // variant sums (ACC_X)
@@ -298,295 +328,58 @@ __global__ void __launch_bounds__(WPB * 32, (MG <= 4 && !EN)
 
   // every lane of a warp runs the same trip counts, so the warp-wide
   // ballots and shuffles stay convergent
-  for (int pw = blockIdx.x * WPB + warp; pw * SEG < A.ngrp; pw += gridDim.x * WPB) {
-    const int i = pw * SEG + sub;
-    const bool gvalid = i < A.ngrp;
-    const int2 mi = gvalid ? A.gmeta[i] : make_int2(0, 0);
+  for (int i = blockIdx.x * WPB + warp; i < A.ngrp; i += gridDim.x * WPB) {
+    const int2 mi = A.gmeta[i];
     const int ifirst = mi.x, ni = mi.y & 0xff, typei = (mi.y >> 8) & 0xff, ljmi = mi.y >> 16;
-    const double4 gi = gvalid ? A.gpos[i] : make_double4(0, 0, 0, 0);
-    if (sl < ni) {
-      s_ai[slot][sl] = A.aoff[ifirst + sl];
-      s_ti[slot][sl] = A.atype[ifirst + sl] * A.ntype;
-      s_pm[slot][sl] = A.apm[ifirst + sl];
-      if (EN) s_qd[slot][sl] = A.qd[ifirst + sl];
-      if (VAR != VAR_STD) s_fi[slot][sl] = A.vflag[ifirst + sl];
-      if (VAR == VAR_ALCH) s_sf[slot][sl] = A.soft[ifirst + sl];
+    const double4 gi = A.gpos[i];
+    const int row = A.off[i], m = A.cnt[i];
+    if (lane < ni) {
+      s_ai[warp][lane] = A.aoff[ifirst + lane];
+      s_ti[warp][lane] = A.atype[ifirst + lane] * A.ntype;
+      s_pm[warp][lane] = A.apm[ifirst + lane];
+      if (EN) s_qd[warp][lane] = A.qd[ifirst + lane];
+      if (VAR != VAR_STD) s_fi[warp][lane] = A.vflag[ifirst + lane];
+      if (VAR == VAR_ALCH) s_sf[warp][lane] = A.soft[ifirst + lane];
     }
     __syncwarp();
     float fi[MG][3];
 #pragma unroll
     for (int a = 0; a < MG; a++) fi[a][0] = fi[a][1] = fi[a][2] = 0.f;
+    float svx = 0.f, svy = 0.f, svz = 0.f;  // sum of the S'V vectors of this row's switched entries
 
-    const int row = gvalid ? A.off[i] : 0, m = gvalid ? A.cnt[i] : 0;
-    int mmax = m;
-    if (SEG == 2) mmax = max(mmax, __shfl_xor_sync(0xffffffffu, m, 16));
-    // Geometry of list entry k of this row: FP64 minimum image of the group
-    // centres (src/force.f:265-277) and the band of src/force.f:290-333
-    // (non-switched, or switched with S and S'); false when outside.
-    auto geometry = [&](int k, int& j, unsigned long long& msk, int2& mj, double& drj, double& cx, double& cy,
-                        double& cz, double& imx, double& imy, double& imz) {
-      j = A.lj_[row + k];
-      msk = A.lmask[row + k];
-      const double4 gj = A.gpos[j];
-      mj = A.gmeta[j];  // issued with the centre load: the atoms' loads need it
-      double dx = gi.x - gj.x, dy = gi.y - gj.y, dz = gi.z - gj.z;
-      imx = 2.0 * round(0.5 * dx);
-      imy = 2.0 * round(0.5 * dy);
-      imz = 2.0 * round(0.5 * dz);
-      dx -= imx;
-      dy -= imy;
-      dz -= imz;
-      cx = A.c11 * dx + A.c12 * dy + A.c13 * dz;
-      cy = A.c22 * dy + A.c23 * dz;
-      cz = A.c33 * dz;
-      drj = cx * cx + cy * cy + cz * cz;
-    };
-    auto band = [&](double drj, bool& switched, float& sw, float& dsw, double& swd) -> bool {
-      sw = 1.f;
-      dsw = 0.f;
-      swd = 1.0;
-      if (drj >= A.r2inn0 && drj < A.r2out) {
-        switched = false;
-      } else if (drj >= A.r2out && drj < A.r2out0) {
-        // S(R) of src/force.f:311-317 for the forces: FP32 arithmetic on the
-        // two factors taken in FP64, the distance to the band edge (rout0 - R)
-        // and auxa (arsout1 + 2R, where -3 rout and 2R cancel to under a
-        // tenth of their size): FP32 R would leave both with 1e-5 relative
-        // error.  The same expression with or without energies; FP64 where S
-        // enters the energies
-        const double rspd = sqrt(drj);
-        const float rsp = (float)rspd;
-        const float auxa = (float)((A.arsout1 + 2.0 * rspd) * A.diarsout2);
-        const float auxb = (float)(A.rout0 - rspd);
-        sw = auxa * auxb * auxb;
-        dsw = (-2.0f * auxa * auxb + 2.0f * auxb * auxb * A.iarsout2) / rsp;
-        if (EN) {
-          const double auxad = (A.arsout1 + 2.0 * rspd) / A.arsout2;
-          const double auxbd = A.rout0 - rspd;
-          swd = auxad * auxbd * auxbd;
-        }
-        switched = true;
-      } else if (drj >= A.r2inn && drj < A.r2inn0) {
-        const double rspd = sqrt(drj);
-        const float rsp = (float)rspd;
-        const float auxa = (float)((A.arsinn1 + 2.0 * rspd) * A.diarsinn2);
-        const float auxb = (float)(A.rinn0 - rspd);
-        sw = 1.0f - auxa * auxb * auxb;
-        dsw = (2.0f * auxa * auxb - 2.0f * auxb * auxb * A.iarsinn2) / rsp;
-        if (EN) {
-          const double auxad = (A.arsinn1 + 2.0 * rspd) / A.arsinn2;
-          const double auxbd = A.rinn0 - rspd;
-          swd = 1.0 - auxad * auxbd * auxbd;
-        }
-        switched = true;
-      } else {
-        return false;
-      }
-      return true;
-    };
-    // The pair work of one in-band entry: atom pairs, S'V term, energies
-    // and the image virial, into this lane's accumulators.
-    auto work = [&](int j, unsigned long long msk, int2 mj, double cx, double cy, double cz, double imx, double imy,
-                    double imz, bool switched, float sw, float dsw, double swd) {
-      const int jfirst = mj.x, nj = mj.y & 0xff, typej = (mj.y >> 8) & 0xff, ljmj = mj.y >> 16;
-      const float dcx = (float)cx, dcy = (float)cy, dcz = (float)cz;
-      double pconf = 0.0, pcoul = 0.0, px0 = 0.0, px1 = 0.0, px2 = 0.0;
-      float vsum = 0.f;
-      float gx = 0.f, gy = 0.f, gz = 0.f;  // total force on the j group
-      // under lskip_ewald an atom without LJ has no pair to evaluate
-      const bool ljonly = VAR != VAR_ALCH && A.lskip && A.ewald;
-      // unrolled to the groups' size bound: constant offsets, shifts and
-      // mask bits, and the j atoms' loads issued together
-#pragma unroll
-      for (int b = 0; b < MG; b++) {
-        if (b >= nj) break;
-        if (ljonly && !((ljmj >> b) & 1)) continue;
-        const float4 ob = A.aoff[jfirst + b];
-        const int tb = A.atype[jfirst + b];
-        const double qbd = EN ? A.qd[jfirst + b] : 0.0;
-        const int fjb = (VAR != VAR_STD) ? (int)A.vflag[jfirst + b] : 0;
-        const float2 sfb = (VAR == VAR_ALCH) ? A.soft[jfirst + b] : make_float2(0.f, 0.f);
-        float fbx = 0.f, fby = 0.f, fbz = 0.f;
-#pragma unroll
-        for (int a = 0; a < MG; a++) {
-          if (a >= ni) break;
-          if ((msk >> (a * 8 + b)) & 1ull) continue;
-          if (ljonly && !((ljmi >> a) & 1)) continue;
-          const float4 ai = s_ai[slot][a];
-          float qf = 0.f, conf = 0.f, coul = 0.f;
-          float rx, ry, rz;
-          bool ljon = false;
-          int tal = 0;
-          if constexpr (VAR == VAR_ALCH) {
-            // src/force_alchemy.f:412-451: exclusions and fixed-mass pairs
-            // are always skipped; no LJ and no Coulomb skips the pair
-            const int fia = s_fi[slot][a];
-            if (fia & fjb & VF_MINF) continue;
-            const float2 sa = s_sf[slot][a];
-            const float eps4 = sa.y * sfb.y;
-            if (eps4 < 1e-12f && A.lskip && A.ewald) continue;
-            npairs++;
-            tal = (fia >> VF_SSHIFT) + (fjb >> VF_SSHIFT) - 4;
-            rx = dcx + ai.x - ob.x;
-            ry = dcy + ai.y - ob.y;
-            rz = dcz + ai.z - ob.z;
-            alch_pair_f32(A, rx * rx + ry * ry + rz * rz, tal, sa.x, sfb.x, eps4, ai.w * ob.w, &qf, &conf, &coul);
-          } else {
-            const float2 L = lj[s_ti[slot][a] + tb];
-            ljon = L.y != 0.f;
-            if (A.lskip && !ljon && A.ewald) continue;  // src/force.f:416-417
-            npairs++;
-            rx = dcx + ai.x - ob.x;
-            ry = dcy + ai.y - ob.y;
-            rz = dcz + ai.z - ob.z;
-            const float r2 = rx * rx + ry * ry + rz * rz;
-            // 1/r from the hardware reciprocal square root, exp from ex2 and
-            // an approximate reciprocal: a few ulp, far below the pair's FP32
-            // rounding budget, and a fraction of the IEEE sequences' cost
-            const float rinv = rsqrtf(r2);
-            const float rsqi = rinv * rinv;
-            if (ljon) {
-              const float r6 = rsqi * rsqi * rsqi;
-              const float r12 = r6 * r6;
-              qf = (12.0f * L.x * r12 - 6.0f * L.y * r6) * rsqi;
-              conf = L.x * r12 - L.y * r6;
-            }
-            if (!A.lskip) {
-              const float rsp = r2 * rinv;
-              const float ar = A.alphal * rsp;
-              const float qt = __fdividef(1.0f, 1.0f + AS_QP * ar);
-              const float ex = __expf(-ar * ar);
-              const float erfcst =
-                  ((((AS_A5 * qt + AS_A4) * qt + AS_A3) * qt + AS_A2) * qt + AS_A1) *
-                  qt * ex;
-              const float qq = ai.w * ob.w;
-              coul = qq * erfcst * rinv;
-              qf += qq * (erfcst + A.twrtpi * ar * ex) * rsqi * rinv;
-            } else if (!A.ewald) {
-              coul = ai.w * ob.w * rinv;
-              qf += coul * rsqi;
-            }
-          }
-          // force_rem (src/force_REM.f:491-495,634-678): selected pairs scale
-          // their force and their share of the S'V sum
-          const bool sel = (VAR == VAR_REM) && seg_sel(A.rem_kind, s_fi[slot][a], fjb);
-          if (switched) {
-            vsum += sel ? (conf + coul) * A.rem_factor : conf + coul;
-            qf *= sw;
-          }
-          if (sel) qf *= A.rem_factor;
-          if (EN) {
-            const double erx = cx + ((double)ai.x - (double)ob.x);
-            const double ery = cy + ((double)ai.y - (double)ob.y);
-            const double erz = cz + ((double)ai.z - (double)ob.z);
-            double cd, qd;
-            if constexpr (VAR == VAR_ALCH) {
-              double c0, q0, du;
-              alch_energy_fp64(A, erx, ery, erz, A.softd[ifirst + a], A.softd[jfirst + b], s_qd[slot][a] * qbd, tal,
-                               &cd, &qd, &c0, &q0, &du);
-              px0 += c0;
-              px1 += q0;
-              px2 += du;
-            } else {
-              pair_energy_fp64(A, erx, ery, erz, A.ljd[s_ti[slot][a] + tb], ljon, s_qd[slot][a] * qbd, &cd,
-                               &qd);
-              if (sel) px0 += cd + qd;  // seg_ene
-            }
-            pconf += cd;
-            pcoul += qd;
-          }
-          const float fx = qf * rx, fy = qf * ry, fz = qf * rz;
-          fi[a][0] += fx;
-          fi[a][1] += fy;
-          fi[a][2] += fz;
-          fbx -= fx;
-          fby -= fy;
-          fbz -= fz;
-        }
-        gx += fbx;
-        gy += fby;
-        gz += fbz;
-        fix_add(A.ffix + jfirst + b, fbx);
-        fix_add(A.ffix + A.natom + jfirst + b, fby);
-        fix_add(A.ffix + 2 * A.natom + jfirst + b, fbz);
-      }
-      if (switched) {
-        if constexpr (EN) {
-          pconf *= swd;
-          pcoul *= swd;
-          px0 *= swd;
-          px1 *= swd;
-          px2 *= swd;
-        }
-        // S'(R) V term: X = -dS/dR / R * V * R_vec on i atoms by mass fraction
-        const float sx = -dsw * vsum * dcx, sy = -dsw * vsum * dcy,
-                    sz = -dsw * vsum * dcz;
-#pragma unroll
-        for (int a = 0; a < MG; a++) {
-          if (a >= ni) break;
-          const float pm = s_pm[slot][a];
-          fi[a][0] += pm * sx;
-          fi[a][1] += pm * sy;
-          fi[a][2] += pm * sz;
-        }
-        for (int b = 0; b < nj; b++) {
-          const float pm = A.apm[jfirst + b];
-          fix_add(A.ffix + jfirst + b, -pm * sx);
-          fix_add(A.ffix + A.natom + jfirst + b, -pm * sy);
-          fix_add(A.ffix + 2 * A.natom + jfirst + b, -pm * sz);
-        }
-        gx -= sx;
-        gy -= sy;
-        gz -= sz;
-      }
-      if constexpr (EN) {
-        const int t = typei + typej - 2;  // 0 slt-slt, 1 slt-slv, 2 slv-slv
-        if (t == 0) {
-          ec0 += pconf;
-          eq0 += pcoul;
-        } else if (t == 1) {
-          ec1 += pconf;
-          eq1 += pcoul;
-        } else {
-          ec2 += pconf;
-          eq2 += pcoul;
-        }
-        ex0 += px0;
-        ex1 += px1;
-        ex2 += px2;
-      }
-      if (EN && A.stress && (imx != 0.0 || imy != 0.0 || imz != 0.0)) {
-        // j sits at its image xpg_j + img: its virial arm gains co.img
-        const float ix = (float)(A.c11 * imx + A.c12 * imy + A.c13 * imz);
-        const float iy = (float)(A.c22 * imy + A.c23 * imz);
-        const float iz = (float)(A.c33 * imz);
-        vimg[0] += gx * ix;
-        vimg[1] += gx * iy;
-        vimg[2] += gx * iz;
-        vimg[3] += gy * ix;
-        vimg[4] += gy * iy;
-        vimg[5] += gy * iz;
-        vimg[6] += gz * ix;
-        vimg[7] += gz * iy;
-        vimg[8] += gz * iz;
-      }
-    };
     int nout = 0;
-    int qn = 0;  // in-band entries queued for the full-warp pass (COMPACT)
-    for (int base = 0; base < mmax; base += LPG) {
-      const int k = base + sl;
+    int qh = 0, qn = 0;  // entry queue: head, entries pending
+    int sh = 0, sn = 0;  // slot queue: head, slots pending
+    for (int base = 0; base < m; base += 32) {
+      // ---- phase 1: geometry of list entry k (src/force.f:265-333)
+      const int k = base + lane;
       const bool valid = k < m;
       int j = 0;
       unsigned long long msk = 0ull;
       int2 mj = make_int2(0, 0);
-      double drj = 1e300, cx = 0, cy = 0, cz = 0, imx = 0, imy = 0, imz = 0;
-      if (valid) geometry(k, j, msk, mj, drj, cx, cy, cz, imx, imy, imz);
-      if (A.next_on) {
+      double drj = 1e300, cx = 0.0, cy = 0.0, cz = 0.0, imx = 0.0, imy = 0.0, imz = 0.0;
+      if (valid) {
+        j = A.lj_[row + k];
+        msk = A.lmask[row + k];
+        const double4 gj = A.gpos[j];
+        mj = A.gmeta[j];
+        double dx = gi.x - gj.x, dy = gi.y - gj.y, dz = gi.z - gj.z;
+        imx = 2.0 * round(0.5 * dx);
+        imy = 2.0 * round(0.5 * dy);
+        imz = 2.0 * round(0.5 * dz);
+        dx -= imx;
+        dy -= imy;
+        dz -= imz;
+        cx = A.c11 * dx + A.c12 * dy + A.c13 * dz;
+        cy = A.c22 * dy + A.c23 * dz;
+        cz = A.c33 * dz;
+        drj = cx * cx + cy * cy + cz * cz;
+      }
+      if (A.next_on) {  // the next inner shell's list, order kept (src/force.f:279-286)
         const bool keep = valid && drj < A.r2neigh;
-        const unsigned ball = __ballot_sync(0xffffffffu, keep);
-        const unsigned bal = SEG == 2 ? (ball >> (sub * 16)) & 0xffffu : ball;
+        const unsigned bal = __ballot_sync(FULL, keep);
         if (keep) {
-          const int pos = nout + __popc(bal & ((1u << sl) - 1u));
+          const int pos = nout + __popc(bal & lanes_below);
           A.j_out[row + pos] = j;
           A.mask_out[row + pos] = msk;
         }
@@ -594,69 +387,292 @@ __global__ void __launch_bounds__(WPB * 32, (MG <= 4 && !EN)
       }
       nscan += valid ? 1u : 0u;
       if (!A.forces_on) continue;
-      bool switched;
-      float sw, dsw;
-      double swd;
-      const bool inb = valid && band(drj, switched, sw, dsw, swd);
-      if constexpr (!COMPACT) {
-        if (inb) work(j, msk, mj, cx, cy, cz, imx, imy, imz, switched, sw, dsw, swd);
-        if (EN && A.stress) flush_vimg();
-      } else {
-        // queue the in-band entries; a full queue runs on every lane
-        const unsigned bq = __ballot_sync(0xffffffffu, inb);
-        if (inb) s_q[warp][qn + __popc(bq & ((1u << lane) - 1u))] = k;
-        qn += __popc(bq);
-        __syncwarp();
-        if (qn >= 32) {
-          const int kq = s_q[warp][lane];
-          geometry(kq, j, msk, mj, drj, cx, cy, cz, imx, imy, imz);
-          band(drj, switched, sw, dsw, swd);
-          work(j, msk, mj, cx, cy, cz, imx, imy, imz, switched, sw, dsw, swd);
-          if (EN && A.stress) flush_vimg();
-          __syncwarp();
-          if (lane < qn - 32) s_q[warp][lane] = s_q[warp][32 + lane];
-          qn -= 32;
-          __syncwarp();
+      // band: non-switched [rinn0, rout), S on [rout, rout0), 1-S on [rinn, rinn0)
+      bool inb = false;
+      float sw = 1.f, dsw = 0.f;
+      double swd = 1.0;
+      if (valid) {
+        if (drj >= A.r2inn0 && drj < A.r2out) {
+          inb = true;
+        } else if (drj >= A.r2out && drj < A.r2out0) {
+          // S(R) of src/force.f:311-317 for the forces: FP32 arithmetic on the
+          // two factors taken in FP64, the distance to the band edge (rout0 - R)
+          // and auxa (arsout1 + 2R, where -3 rout and 2R cancel to under a
+          // tenth of their size): FP32 R would leave both with 1e-5 relative
+          // error.  FP64 where S enters the energies
+          const double rspd = sqrt(drj);
+          const float rsp = (float)rspd;
+          const float auxa = (float)((A.arsout1 + 2.0 * rspd) * A.diarsout2);
+          const float auxb = (float)(A.rout0 - rspd);
+          sw = auxa * auxb * auxb;
+          dsw = (-2.0f * auxa * auxb + 2.0f * auxb * auxb * A.iarsout2) / rsp;
+          if (EN) {
+            const double auxbd = A.rout0 - rspd;
+            swd = (A.arsout1 + 2.0 * rspd) / A.arsout2 * auxbd * auxbd;
+          }
+          inb = true;
+        } else if (drj >= A.r2inn && drj < A.r2inn0) {
+          const double rspd = sqrt(drj);
+          const float rsp = (float)rspd;
+          const float auxa = (float)((A.arsinn1 + 2.0 * rspd) * A.diarsinn2);
+          const float auxb = (float)(A.rinn0 - rspd);
+          sw = 1.0f - auxa * auxb * auxb;
+          dsw = (2.0f * auxa * auxb - 2.0f * auxb * auxb * A.iarsinn2) / rsp;
+          if (EN) {
+            const double auxbd = A.rinn0 - rspd;
+            swd = 1.0 - (A.arsinn1 + 2.0 * rspd) / A.arsinn2 * auxbd * auxbd;
+          }
+          inb = true;
         }
       }
-    }
-    if constexpr (COMPACT) {
-      if (A.forces_on && lane < qn) {
-        int j, kq = s_q[warp][lane];
-        unsigned long long msk;
-        int2 mj;
-        double drj, cx, cy, cz, imx, imy, imz;
-        bool switched;
-        float sw, dsw;
-        double swd;
-        geometry(kq, j, msk, mj, drj, cx, cy, cz, imx, imy, imz);
-        band(drj, switched, sw, dsw, swd);
-        work(j, msk, mj, cx, cy, cz, imx, imy, imz, switched, sw, dsw, swd);
+      // the j atoms to evaluate: all, or under lskip_ewald those with LJ --
+      // and all atoms of a switched pair, which take the S'V term by mass
+      // fraction whether they have LJ or not
+      unsigned bm = 0u;
+      if (inb) {
+        bm = (1u << (mj.y & 0xff)) - 1u;
+        if (ljonly && dsw == 0.f) bm &= (unsigned)(mj.y >> 16);
       }
+      const int na = __popc(bm);
+      int sc = na;  // inclusive warp scan of the slot counts
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(FULL, sc, o);
+        if (lane >= o) sc += v;
+      }
+      const int tot = __shfl_sync(FULL, sc, 31);
+      const unsigned bq = __ballot_sync(FULL, na > 0);
+      if (na > 0) {
+        const int e = (qh + qn + __popc(bq & lanes_below)) & (QE - 1);
+        s_edc[warp][e] = make_float4((float)cx, (float)cy, (float)cz, sw);
+        s_edsw[warp][e] = dsw;
+        s_emeta[warp][e] = mj;
+        s_emsk[warp][e] = msk;
+        if constexpr (EN) {
+          s_ecd[warp][e] = make_double4(cx, cy, cz, swd);
+          if (A.stress)  // j sits at its image xpg_j + img: its virial arm gains co.img
+            s_eimg[warp][e] = make_float4((float)(A.c11 * imx + A.c12 * imy + A.c13 * imz),
+                                          (float)(A.c22 * imy + A.c23 * imz), (float)(A.c33 * imz), 0.f);
+        }
+        int ps = sh + sn + sc - na;
+        unsigned bb = bm;
+        for (int t = 0; t < na; t++) {
+          const int b = __ffs(bb) - 1;
+          bb &= bb - 1u;
+          s_slot[warp][(ps + t) & (QS - 1)] = slot_pack(e, t, b, na);
+        }
+      }
+      qn += __popc(bq);
+      sn += tot;
       __syncwarp();
-      if (EN && A.stress) flush_vimg();
+
+      // ---- phase 2: passes over whole entries, a lane per j atom
+      const bool last = base + 32 >= m;
+      while (sn >= 32 || (last && sn > 0)) {
+        int L = sn;
+        if (sn > 32) L = 32 - (((int)s_slot[warp][(sh + 32) & (QS - 1)] >> 6) & 7);
+        else if (sn == 32) L = 32;
+        const bool act = lane < L;
+        const unsigned r = act ? (unsigned)s_slot[warp][(sh + lane) & (QS - 1)] : 0u;
+        const int e = r & 63, t = (r >> 6) & 7, b = (r >> 9) & 7, nsl = ((r >> 12) & 7) + 1;
+        float fbx = 0.f, fby = 0.f, fbz = 0.f, vpart = 0.f;
+        float4 dcs = make_float4(0.f, 0.f, 0.f, 1.f);
+        float dswe = 0.f;
+        int jat = 0, typej = 0;
+        if (act) {
+          dcs = s_edc[warp][e];
+          dswe = s_edsw[warp][e];
+          const int2 me = s_emeta[warp][e];
+          const unsigned long long mskb = s_emsk[warp][e] >> b;
+          jat = me.x + b;
+          typej = (me.y >> 8) & 0xff;
+          const float4 ob = A.aoff[jat];
+          const int tb = A.atype[jat];
+          const double qbd = EN ? A.qd[jat] : 0.0;
+          const int fjb = (VAR != VAR_STD) ? (int)A.vflag[jat] : 0;
+          const float2 sfb = (VAR == VAR_ALCH) ? A.soft[jat] : make_float2(0.f, 0.f);
+          const float bx = dcs.x - ob.x, by = dcs.y - ob.y, bz = dcs.z - ob.z;
+          double4 cd = make_double4(0.0, 0.0, 0.0, 1.0);
+          if (EN) cd = s_ecd[warp][e];
+          double pconf = 0.0, pcoul = 0.0, px0 = 0.0, px1 = 0.0, px2 = 0.0;
+#pragma unroll
+          for (int a = 0; a < MG; a++) {
+            if (a >= ni) break;
+            if ((mskb >> (a * 8)) & 1ull) continue;
+            if (ljonly && !((ljmi >> a) & 1)) continue;
+            const float4 ai = s_ai[warp][a];  // a broadcast read
+            const float rx = ai.x + bx, ry = ai.y + by, rz = ai.z + bz;
+            float qf = 0.f, conf = 0.f, coul = 0.f;
+            bool ljon = false;
+            int tal = 0;
+            if constexpr (VAR == VAR_ALCH) {
+              // src/force_alchemy.f:412-451: exclusions and fixed-mass pairs
+              // are always skipped; no LJ and no Coulomb skips the pair
+              const int fia = s_fi[warp][a];
+              if (fia & fjb & VF_MINF) continue;
+              const float2 sa = s_sf[warp][a];
+              const float eps4 = sa.y * sfb.y;
+              if (eps4 < 1e-12f && A.lskip && A.ewald) continue;
+              npairs++;
+              tal = (fia >> VF_SSHIFT) + (fjb >> VF_SSHIFT) - 4;
+              alch_pair_f32(A, rx * rx + ry * ry + rz * rz, tal, sa.x, sfb.x, eps4, ai.w * ob.w, &qf, &conf, &coul);
+            } else {
+              const float2 Lp = lj[s_ti[warp][a] + tb];
+              ljon = Lp.y != 0.f;
+              if (A.lskip && !ljon && A.ewald) continue;  // src/force.f:416-417
+              npairs++;
+              const float r2 = rx * rx + ry * ry + rz * rz;
+              // 1/r from the hardware reciprocal square root, exp from ex2 and
+              // an approximate reciprocal: a few ulp, far below the pair's FP32
+              // rounding budget, and a fraction of the IEEE sequences' cost
+              const float rinv = rsqrtf(r2);
+              const float rsqi = rinv * rinv;
+              if (ljon) {
+                const float r6 = rsqi * rsqi * rsqi;
+                const float r12 = r6 * r6;
+                qf = (12.0f * Lp.x * r12 - 6.0f * Lp.y * r6) * rsqi;
+                conf = Lp.x * r12 - Lp.y * r6;
+              }
+              if (!A.lskip) {
+                const float rsp = r2 * rinv;
+                const float ar = A.alphal * rsp;
+                const float qt = __fdividef(1.0f, 1.0f + AS_QP * ar);
+                const float ex = __expf(-ar * ar);
+                const float erfcst = ((((AS_A5 * qt + AS_A4) * qt + AS_A3) * qt + AS_A2) * qt + AS_A1) * qt * ex;
+                const float qq = ai.w * ob.w;
+                coul = qq * erfcst * rinv;
+                qf += qq * (erfcst + A.twrtpi * ar * ex) * rsqi * rinv;
+              } else if (!A.ewald) {
+                coul = ai.w * ob.w * rinv;
+                qf += coul * rsqi;
+              }
+            }
+            // force_rem (src/force_REM.f:491-495,634-678): selected pairs scale
+            // their force and their share of the S'V sum
+            const bool sel = (VAR == VAR_REM) && seg_sel(A.rem_kind, s_fi[warp][a], fjb);
+            vpart += sel ? (conf + coul) * A.rem_factor : conf + coul;
+            qf *= dcs.w;
+            if (sel) qf *= A.rem_factor;
+            if (EN) {
+              const double erx = cd.x + ((double)ai.x - (double)ob.x);
+              const double ery = cd.y + ((double)ai.y - (double)ob.y);
+              const double erz = cd.z + ((double)ai.z - (double)ob.z);
+              double cdd, qdd;
+              if constexpr (VAR == VAR_ALCH) {
+                double c0, q0, du;
+                alch_energy_fp64(A, erx, ery, erz, A.softd[ifirst + a], A.softd[jat], s_qd[warp][a] * qbd, tal, &cdd,
+                                 &qdd, &c0, &q0, &du);
+                px0 += c0;
+                px1 += q0;
+                px2 += du;
+              } else {
+                pair_energy_fp64(A, erx, ery, erz, A.ljd[s_ti[warp][a] + tb], ljon,
+                                 s_qd[warp][a] * qbd, &cdd, &qdd);
+                if (sel) px0 += cdd + qdd;  // seg_ene
+              }
+              pconf += cdd;
+              pcoul += qdd;
+            }
+            const float fx = qf * rx, fy = qf * ry, fz = qf * rz;
+            fi[a][0] += fx;
+            fi[a][1] += fy;
+            fi[a][2] += fz;
+            fbx -= fx;
+            fby -= fy;
+            fbz -= fz;
+          }
+          if constexpr (EN) {
+            const int tt = typei + typej - 2;  // 0 slt-slt, 1 slt-slv, 2 slv-slv
+            pconf *= cd.w;
+            pcoul *= cd.w;
+            if (tt == 0) {
+              ec0 += pconf;
+              eq0 += pcoul;
+            } else if (tt == 1) {
+              ec1 += pconf;
+              eq1 += pcoul;
+            } else {
+              ec2 += pconf;
+              eq2 += pcoul;
+            }
+            ex0 += px0 * cd.w;
+            ex1 += px1 * cd.w;
+            ex2 += px2 * cd.w;
+          }
+        }
+        // S'(R) V term of switched entries (src/force.f:754-817): V summed
+        // over the entry's lanes, X = -dS/dR / R V R_vec distributed by mass
+        // fraction, on the j atoms here and on the i atoms at the end of the row
+        if (__any_sync(FULL, dswe != 0.f)) {
+          float v = vpart;
+#pragma unroll
+          for (int o = 1; o < MG; o <<= 1) {
+            const float w = __shfl_down_sync(FULL, v, o);
+            if (t + o < nsl) v += w;
+          }
+          const float V = __shfl_sync(FULL, v, (lane - t) & 31);
+          if (act && dswe != 0.f) {
+            const float sx = -dswe * V * dcs.x, sy = -dswe * V * dcs.y, sz = -dswe * V * dcs.z;
+            const float pm = A.apm[jat];
+            fbx -= pm * sx;
+            fby -= pm * sy;
+            fbz -= pm * sz;
+            if (t == 0) {
+              svx += sx;
+              svy += sy;
+              svz += sz;
+            }
+          }
+        }
+        if (act) {
+          fix_add(A.ffix + jat, fbx);
+          fix_add(A.ffix + A.natom + jat, fby);
+          fix_add(A.ffix + 2 * A.natom + jat, fbz);
+        }
+        if (EN && A.stress) {
+          if (act) {
+            const float4 im = s_eimg[warp][e];
+            vimg[0] += fbx * im.x;
+            vimg[1] += fbx * im.y;
+            vimg[2] += fbx * im.z;
+            vimg[3] += fby * im.x;
+            vimg[4] += fby * im.y;
+            vimg[5] += fby * im.z;
+            vimg[6] += fbz * im.x;
+            vimg[7] += fbz * im.y;
+            vimg[8] += fbz * im.z;
+          }
+          flush_vimg();
+        }
+        const int ne = __popc(__ballot_sync(FULL, act && t == 0));
+        sh += L;
+        sn -= L;
+        qh += ne;
+        qn -= ne;
+        __syncwarp();
+      }
     }
-    if (A.next_on && sl == 0 && gvalid) {
+    if (A.next_on && lane == 0) {
       A.cnt_out[i] = nout;
       nkept += (unsigned)nout;
     }
-    if (A.forces_on) {
-      // the segments of a warp may hold groups of different sizes: the
-      // shuffles run to the larger one
-      int nimax = ni;
-      if (SEG == 2) nimax = max(nimax, __shfl_xor_sync(0xffffffffu, ni, 16));
+    if (A.forces_on && m > 0) {
+      // i atoms: pair forces and their share of the row's S'V vectors, one
+      // atomic per component from lanes 0 .. 3 ni - 1
+      const float tsx = seg_sum<32>(svx), tsy = seg_sum<32>(svy), tsz = seg_sum<32>(svz);
+      float val = 0.f;
 #pragma unroll
       for (int a = 0; a < MG; a++) {
-        if (a >= nimax) break;
-        const float sx = seg_sum<LPG>(fi[a][0]);
-        const float sy = seg_sum<LPG>(fi[a][1]);
-        const float sz = seg_sum<LPG>(fi[a][2]);
-        if (sl == 0 && a < ni) {
-          fix_add(A.ffix + ifirst + a, sx);
-          fix_add(A.ffix + A.natom + ifirst + a, sy);
-          fix_add(A.ffix + 2 * A.natom + ifirst + a, sz);
-        }
+        if (a >= ni) break;
+        const float pm = s_pm[warp][a];
+        const float sx = seg_sum<32>(fi[a][0]) + pm * tsx;
+        const float sy = seg_sum<32>(fi[a][1]) + pm * tsy;
+        const float sz = seg_sum<32>(fi[a][2]) + pm * tsz;
+        if (lane == 3 * a) val = sx;
+        if (lane == 3 * a + 1) val = sy;
+        if (lane == 3 * a + 2) val = sz;
       }
+      if (lane < 3 * ni) fix_add(A.ffix + (lane % 3) * A.natom + ifirst + lane / 3, val);
     }
     __syncwarp();
   }
@@ -665,9 +681,9 @@ __global__ void __launch_bounds__(WPB * 32, (MG <= 4 && !EN)
     unsigned s0 = nscan, s1 = nkept, s2 = npairs;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
-      s0 += __shfl_xor_sync(0xffffffffu, s0, o);
-      s1 += __shfl_xor_sync(0xffffffffu, s1, o);
-      s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+      s0 += __shfl_xor_sync(FULL, s0, o);
+      s1 += __shfl_xor_sync(FULL, s1, o);
+      s2 += __shfl_xor_sync(FULL, s2, o);
     }
     if (lane == 0) {
       if (s0) atomicAdd(A.wcnt + 0, (unsigned long long)s0);
@@ -687,16 +703,16 @@ __global__ void __launch_bounds__(WPB * 32, (MG <= 4 && !EN)
       if (lane == 0) s_red[warp][q] = s_vimg[warp][q - 6];
       continue;
     }
-    const double s = warp_sumd(vals[q]);
-    if (lane == 0) s_red[warp][q] = s;
+    const double sred = warp_sumd(vals[q]);
+    if (lane == 0) s_red[warp][q] = sred;
   }
   __syncthreads();
   if (threadIdx.x < NV) {
-    double s = 0;
-    for (int w = 0; w < WPB; w++) s += s_red[w][threadIdx.x];
+    double sacc = 0;
+    for (int w = 0; w < WPB; w++) sacc += s_red[w][threadIdx.x];
     // slots 0..14 = ACC_CONF..ACC_VIMG+8, then ACC_X..ACC_X+2
     const int acc_slot = threadIdx.x < 15 ? (int)threadIdx.x : ACC_X + (int)threadIdx.x - 15;
-    if (s != 0.0) atomicAdd(A.acc + acc_slot, s);
+    if (sacc != 0.0) atomicAdd(A.acc + acc_slot, sacc);
   }
 }
 
@@ -788,40 +804,35 @@ int pair_launch(orac_gpu_ctx* ctx, const PairArgs& a, int maxg) {
     return ctx_fail(ctx, ORAC_ERR_PARAM, "charge group of %d atoms exceeds %d", maxg, ORAC_MAXG);
   if (a.variant < VAR_STD || a.variant > VAR_ALCH) return ctx_fail(ctx, ORAC_ERR_PARAM, "variant %d", a.variant);
   // atoms-per-group bound of the instantiation: 3 (waters, and chains cut
-  // in threes), 4, or 8; half-warp groups only for the two small bounds
+  // in threes), 4, or 8
   const int mgk = maxg <= 3 ? 0 : (maxg <= 4 ? 1 : 2);
-  const bool half = mgk < 2 && a.lpg == 16;
-  const int gpb = WPB * (half ? 2 : 1);  // groups per block
-  int nb = (a.ngrp + gpb - 1) / gpb;
+  int nb = (a.ngrp + WPB - 1) / WPB;  // a warp per i group
   if (nb < 1) nb = 1;
   int slot = -1;
   if (int rc = prof_begin(ctx, &slot)) return rc;
   const bool en = a.energy || a.stress;  // the forces-only build keeps no sums
   const bool hi = a.occ_hi && !en && mgk < 2;
-  switch ((((mgk * 3 + a.variant) * 2 + (en ? 1 : 0)) * 2 + (half ? 1 : 0)) * 2 + (hi ? 1 : 0)) {
-#define ORAC_KP(MGK, MG, VAR, EN, LPG, HI)                                                     \
-  case (((MGK * 3 + VAR) * 2 + (EN ? 1 : 0)) * 2 + (LPG == 16 ? 1 : 0)) * 2 + (HI ? 1 : 0):     \
-    orac_launch(k_pair<MG, EN, VAR, LPG, HI>, nb, WPB * 32, smem, ctx->stream, a);                      \
+  switch (((mgk * 3 + a.variant) * 2 + (en ? 1 : 0)) * 2 + (hi ? 1 : 0)) {
+#define ORAC_KP(MGK, MG, VAR, EN, HI)                                   \
+  case ((MGK * 3 + VAR) * 2 + (EN ? 1 : 0)) * 2 + (HI ? 1 : 0):        \
+    orac_launch(k_pair<MG, EN, VAR, HI>, nb, WPB * 32, smem, ctx->stream, a); \
     break;
-#define ORAC_KP_V(MGK, MG, VAR)                                                                \
-  ORAC_KP(MGK, MG, VAR, false, 32, false)                                                      \
-  ORAC_KP(MGK, MG, VAR, false, 32, true)                                                       \
-  ORAC_KP(MGK, MG, VAR, true, 32, false)                                                       \
-  ORAC_KP(MGK, MG, VAR, false, 16, false)                                                      \
-  ORAC_KP(MGK, MG, VAR, false, 16, true)                                                       \
-  ORAC_KP(MGK, MG, VAR, true, 16, false)
+#define ORAC_KP_V(MGK, MG, VAR)        \
+  ORAC_KP(MGK, MG, VAR, false, false) \
+  ORAC_KP(MGK, MG, VAR, false, true)  \
+  ORAC_KP(MGK, MG, VAR, true, false)
     ORAC_KP_V(0, 3, VAR_STD)
     ORAC_KP_V(0, 3, VAR_REM)
     ORAC_KP_V(0, 3, VAR_ALCH)
     ORAC_KP_V(1, 4, VAR_STD)
     ORAC_KP_V(1, 4, VAR_REM)
     ORAC_KP_V(1, 4, VAR_ALCH)
-    ORAC_KP(2, 8, VAR_STD, false, 32, false)
-    ORAC_KP(2, 8, VAR_STD, true, 32, false)
-    ORAC_KP(2, 8, VAR_REM, false, 32, false)
-    ORAC_KP(2, 8, VAR_REM, true, 32, false)
-    ORAC_KP(2, 8, VAR_ALCH, false, 32, false)
-    ORAC_KP(2, 8, VAR_ALCH, true, 32, false)
+    ORAC_KP(2, 8, VAR_STD, false, false)
+    ORAC_KP(2, 8, VAR_STD, true, false)
+    ORAC_KP(2, 8, VAR_REM, false, false)
+    ORAC_KP(2, 8, VAR_REM, true, false)
+    ORAC_KP(2, 8, VAR_ALCH, false, false)
+    ORAC_KP(2, 8, VAR_ALCH, true, false)
 #undef ORAC_KP_V
 #undef ORAC_KP
   }

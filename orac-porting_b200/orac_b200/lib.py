@@ -97,6 +97,7 @@ def load():
         "orac_gpu_sync": (i, [_P]),
         "orac_gpu_stats": (i, [_P, C.POINTER(i64), C.POINTER(i64)]),
         "orac_gpu_footprint": (i, [_P, C.POINTER(i64)]),
+        "orac_gpu_fp32_rate": (i, [i, C.POINTER(d), C.POINTER(d)]),
         "orac_gpu_server_now": (d, []),
         "orac_gpu_server_create": (i, [i, i64, i, i, C.POINTER(_P)]),
         "orac_gpu_server_destroy": (i, [_P]),
