@@ -2,10 +2,14 @@
 """MD throughput (ns/day) of the B200 r-RESPA nonbonded force path.
 
 One step = one outer r-RESPA step (H = 4 fs: 1 H shell, 2 L shells + SPME,
-8 M shells, drift + SHAKE/RATTLE) of the 3,000-water 31 A box (9,000 atoms,
-alpha 0.35, SPME 32^3 order 4, shells 5.0/7.5/10.0 A, list update every
-6 steps), run by the device-resident driver of liborac_gpu.so with the
-state resident in HBM.  Prints one JSON line.
+8 M shells, drift + SHAKE/RATTLE) of 3,000 rigid waters (9,000 atoms) at
+liquid density (44.7 A box, alpha 0.35, SPME 48^3 order 4, shells
+5.0/7.5/10.0 A, list update every 6 steps; `--workload config1` selects the
+31 A box as specified, three times liquid density), run by the
+device-resident driver of liborac_gpu.so with the state resident in HBM.
+Further legs on the same line: the state's forces and energies against the
+FP64 oracle, 64 batched alchemical windows, ORAC's own test1 system, 128
+uneven HREM replicas and the serving loop.  Prints one JSON line.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -36,7 +40,7 @@ import numpy as np  # noqa: E402
 from orac_b200 import systems, units  # noqa: E402
 
 FS_PER_DAY = 86400.0e15  # fs per day of wall time per 1 fs/s
-FP32_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # 74.4: no measured FP32 peak on this pool
+FP32_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # 74.4: used only if the FMA-rate probe fails
 METRIC = "MD ns/day and p50/p99 segment latency, batched vs plain, at force err<=1e-5"
 
 WORKLOADS = {
@@ -68,6 +72,21 @@ def f0_system():
 # the reference's test1 schedule: 15 fs outer step, L 3 fs (SPME), M 1.5 fs,
 # intramolecular 0.75 / 0.375 fs, list update every 6 steps
 F0_WORKLOAD = dict(build=f0_system, dt_h=15.0, lrespa=5, mrespa=2, n1respa=2, n0respa=2, nupdte=6, rshk="l")
+DUDL_STEPS, DUDL_EVERY = 400, 2  # dU/dlambda sampling of the batched windows
+# the pair-kernel autotuner's choices per device and workload shape
+TUNE_CACHE = os.path.join(ROOT, "orac-porting_b200", "orac_b200", "pair_tuning.txt")
+TUNE_TRIAL = 6
+
+
+def tuned(obj):
+    """Autotune a context or a batch (cached choices are applied without
+    timing): the chosen configuration, its time per step, and whether it was
+    measured in this run or read from the cache."""
+    n0 = len(open(TUNE_CACHE).read().splitlines()) if os.path.exists(TUNE_CACHE) else 0
+    best, ms = obj.tune(trial=TUNE_TRIAL, cache=TUNE_CACHE)
+    n1 = len(open(TUNE_CACHE).read().splitlines()) if os.path.exists(TUNE_CACHE) else 0
+    return {"lpg_m": best[0], "lpg_lh": best[1], "blocks_per_sm": best[2], "ms_per_step": ms,
+            "source": "measured in this run" if n1 > n0 else "cache (orac_b200/pair_tuning.txt)"}
 TEST1_PUBLISHED_NS_DAY = 4.41  # test1/md.out:1061,1063: 58.799 s for 3,000 fs, 8 OpenMP threads, NPT
 
 
@@ -138,6 +157,92 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+def force_check(s, x):
+    """Forces and energies of the Cartesian state x (3, N) through the C ABI
+    (the three shells and SPME, lists built at x) against the FP64 oracle on
+    the same positions: ORAC's check_force metric (relative RMS of the total
+    force, src/pme_code.f:378-396) and the relative error of each energy
+    term (LJ, real-space Coulomb, reciprocal) and of their sum."""
+    import oracle
+    from orac_b200.engine import Engine
+
+    t = s.copy()
+    sc = np.linalg.inv(np.asarray(s.co)) @ np.asarray(x)
+    t.xp0, t.yp0, t.zp0 = sc[0].copy(), sc[1].copy(), sc[2].copy()
+    g, o = Engine(t.copy()), oracle.Oracle(t.copy())
+    try:
+        g.update_lists()
+        o.update_lists()
+        Fg, Fo = np.zeros((3, s.ntap)), np.zeros((3, s.ntap))
+        eg, eo = np.zeros(6), np.zeros(6)
+        for sh in "mlh":
+            F, en, _ = g.shell(sh)
+            Fg += F
+            eg += g.ue6(en)
+            F, ue, _ = o.shell(sh)
+            Fo += F
+            eo += np.asarray(ue)
+        F, rg, _ = g.fft_pme()
+        Fg += F
+        F, ro, _ = o.fft_pme()
+        Fo += F
+    finally:
+        g.close()
+    terms_g = {"lj": eg[:3].sum(), "coul_real": eg[3:].sum(), "reciprocal": rg}
+    terms_o = {"lj": eo[:3].sum(), "coul_real": eo[3:].sum(), "reciprocal": ro}
+    terms_g["total"] = sum(terms_g.values())
+    terms_o["total"] = sum(terms_o.values())
+    rel = {k: abs(terms_g[k] - terms_o[k]) / abs(terms_o[k]) for k in terms_o}
+    return {"force_rel_rms": float(np.sqrt(((Fg - Fo) ** 2).sum() / (Fo ** 2).sum())),
+            "energy_rel_err": max(rel.values()), "energy_rel_err_terms": rel,
+            "energy_kjmol": {k: v * units.KJMOL for k, v in terms_o.items()},
+            "how": "state after the timed steps: M, L, H shells and SPME through the C ABI (lists rebuilt at that "
+                   "state) against the FP64 oracle on the same positions; force = sum of the four"}
+
+
+def drift_fit(rec, dt_h):
+    """Total-energy drift (kJ/mol per ps, least squares) and the RMS of the
+    residual, of energy records."""
+    t = rec[:, 0] * dt_h * 1e-3
+    e = rec[:, 10] * units.KJMOL
+    p = np.polyfit(t, e, 1)
+    return float(p[0]), float(np.std(e - np.polyval(p, t)))
+
+
+def drift_run(wl, s, device):
+    """1,000 outer steps of the workload from its seeded start (NVE, energy
+    record every 10 steps) on the device beside the FP64 oracle's run of the
+    same 1,000 steps (tests/golden/liquid_drift_oracle.npz)."""
+    from orac_b200.engine import Engine
+
+    ref = np.load(os.path.join(ROOT, "tests", "golden", "liquid_drift_oracle.npz"))
+    g = Engine(s.copy(), device=device)
+    g.md_setup(wl["dt_h"], wl["lrespa"], wl["mrespa"], wl["nupdte"], wl["rshk"], econst=econst_of(s, g))
+    rec = g.md_run(int(ref["nsteps"]), energy_every=int(ref["every"]))
+    g.close()
+    dg, fg = drift_fit(rec, wl["dt_h"])
+    do, fo = drift_fit(ref["rec"], float(ref["dt_h"]))
+    return {"steps": int(ref["nsteps"]), "gpu_drift_kjmol_per_ps": dg, "gpu_rms_kjmol": fg,
+            "oracle_drift_kjmol_per_ps": do, "oracle_rms_kjmol": fo,
+            "total_energy_kjmol": float(rec[0, 10] * units.KJMOL),
+            "how": "least-squares slope of the total energy and RMS of its residual over 1,000 outer steps (4 ps) "
+                   "from the seeded start, records every 10 steps; oracle: the FP64 CPU restatement's run of the "
+                   "same steps (fixture made by tests/golden/make_drift.py)"}
+
+
+def fp32_peak(device):
+    """Measured FP32 FMA rate of the device (orac_gpu_fp32_rate), TFLOP/s."""
+    import ctypes as C
+
+    from orac_b200 import lib
+
+    L = lib.load()
+    tf, ms = C.c_double(), C.c_double()
+    if L.orac_gpu_fp32_rate(device, C.byref(tf), C.byref(ms)) != 0 or tf.value <= 0.0:
+        return None
+    return tf.value
+
+
 def measured_peaks():
     try:
         return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -195,6 +300,11 @@ def gpu_arm(args, wl, s, device):
     L = eng.lib
     ec = econst_of(s, eng)
     eng.md_setup(wl["dt_h"], wl["lrespa"], wl["mrespa"], wl["nupdte"], wl["rshk"], econst=ec)
+    ws, rank, local = dist_info()
+    # clocks sampled from the autotuner's and warm-up steps through the timed
+    # steps: the timed region alone is shorter than nvidia-smi's 200 ms period
+    clocks = ClockSampler(device) if rank == 0 else None
+    tuning = tuned(eng)
     L.orac_gpu_prof_enable(eng.ctx, 1)
     stream = torch.cuda.ExternalStream(L.orac_gpu_get_stream(eng.ctx), device=device)
     def ok(rc, what):
@@ -211,13 +321,11 @@ def gpu_arm(args, wl, s, device):
     l0 = C.c_int64()
     L.orac_gpu_stats(eng.ctx, None, C.byref(l0))
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{device}")  # > 126 MB L2
-    ws, rank, local = dist_info()
     if ws > 1:
         import torch.distributed as dist
 
         dist.barrier()
     torch.cuda.synchronize()
-    clocks = ClockSampler(device) if rank == 0 else None
     total_ms = 0.0
     step_ms = []
     for _ in range(args.steps):
@@ -242,13 +350,16 @@ def gpu_arm(args, wl, s, device):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         total_ms = float(t.item())
     clk = clocks.stop() if clocks else None
+    if clk:
+        clk["window"] = "autotuner and warm-up steps through the timed steps"
     l1 = C.c_int64()
     L.orac_gpu_stats(eng.ctx, None, C.byref(l1))
     L.orac_gpu_counters(eng.ctx, cnt, 0)
     pms = C.c_double()
     pn = C.c_int64()
     L.orac_gpu_prof_read(eng.ctx, C.byref(pms), C.byref(pn), 0)
-    res = dict(total_ms=total_ms, step_ms=step_ms, launches=int(l1.value - l0.value), scanned=cnt[0], kept=cnt[1],
+    res = dict(tuning=tuning, total_ms=total_ms, step_ms=step_ms, launches=int(l1.value - l0.value), scanned=cnt[0],
+               kept=cnt[1],
                pairs_ewald=cnt[2], pairs_lj=cnt[3], kpair_ms=pms.value, kpair_n=int(pn.value), clocks=clk,
                kpair_how="CUDA events recorded as graph nodes around every k_pair launch of the timed steps")
     if res["kpair_n"] <= 0:
@@ -298,7 +409,19 @@ def gpu_arm(args, wl, s, device):
     res["e2e_steps"] = e2e_steps
     res["bytes_io"] = 6 * n * 8
     res["G"], res["N"] = s.ngrp, s.ntap
+    res["shell_evals"] = args.steps * (1 + wl["lrespa"] + wl["lrespa"] * wl["mrespa"])
+    xs, _ = eng.md_state()
     eng.close()
+    try:
+        res["force_check"] = force_check(s, xs)
+    except Exception as exc:
+        res["force_check"] = {"error": f"{type(exc).__name__}: {exc}"}
+    res["fp32_peak"] = fp32_peak(device)
+    if args.drift and args.workload == "liquid":
+        try:
+            res["energy_conservation"] = drift_run(wl, s, device)
+        except Exception as exc:
+            res["energy_conservation"] = {"error": f"{type(exc).__name__}: {exc}"}
     if args.batch > 1:
         try:
             res["batched"] = batch_arm(args, wl, s, device, flush)
@@ -309,6 +432,12 @@ def gpu_arm(args, wl, s, device):
             res["orac_test1"] = f0_arm(args, device, flush)
         except Exception as exc:
             res["orac_test1"] = {"error": f"{type(exc).__name__}: {exc}"}
+    if ws == 1 and args.configs:
+        for key, arm in (("config2", config2_arm), ("config1_as_specified", config1_fixed_arm)):
+            try:
+                res[key] = arm(args, device, flush)
+            except Exception as exc:
+                res[key] = {"error": f"{type(exc).__name__}: {exc}"}
     if ws == 1 and args.uneven > 1:
         try:
             res["uneven"] = uneven_arm(args, wl, device, flush)
@@ -369,6 +498,7 @@ def batch_arm(args, wl, s, device, flush):
     nwin = args.batch
     # one window alone (plain)
     e1, _ = window_engine(base, nwin // 2, nwin, device, wl)
+    tune_plain = tuned(e1)
     L = e1.lib
     st1 = torch.cuda.ExternalStream(L.orac_gpu_get_stream(e1.ctx), device=device)
     for _ in range(args.warmup):
@@ -389,20 +519,37 @@ def batch_arm(args, wl, s, device, flush):
         engines.append(e)
         lams.append(lam)
     b = Batch(engines)
+    tune_batch = tuned(b)
     stream = torch.cuda.ExternalStream(b.stream(), device=device)
     b.run(args.warmup)
     step_ms = _timed_steps(lambda: b.run(1, sync=False), stream, flush, args.steps)
     b.sync()
+    # dU/dlambda of every window: energy records written on the device every
+    # DUDL_EVERY steps of a batched sampling run after the timed steps
+    for e in engines:
+        e.md_records(1, reset=True)
+    b.run(DUDL_STEPS, energy_every=DUDL_EVERY)
     b.close()
     dudl = []
     for e in engines:
-        rec = e.md_run(1, energy_every=1)
-        dudl.append(float(rec[0, 15]))
+        rec, n = e.md_records(DUDL_STEPS // DUDL_EVERY)
+        dudl.append(rec[:, 15].copy())
         e.close()
     st = sorted(step_ms)
     return {"systems": nwin, "atoms_per_window": base.ntap, "total_ms": sum(step_ms),
             "step_ms_p50": st[len(st) // 2], "step_ms_p99": st[min(len(st) - 1, int(0.99 * len(st)))],
-            "plain_total_ms": sum(plain_ms), "lambdas": lams, "dudl": dudl}
+            "plain_total_ms": sum(plain_ms), "lambdas": lams, "dudl": dudl,
+            "tuning": {"batch": tune_batch, "plain_window": tune_plain}}
+
+
+def block_mean_err(x, nblocks=10):
+    """Mean and its standard error from the spread of nblocks block means
+    (correlated samples of one trajectory)."""
+    x = np.asarray(x, dtype=np.float64)
+    nb = max(2, min(nblocks, len(x)))
+    m = len(x) // nb
+    blocks = x[:m * nb].reshape(nb, m).mean(axis=1)
+    return float(x.mean()), float(blocks.std(ddof=1) / np.sqrt(nb))
 
 
 def build_pool(specs):
@@ -457,6 +604,7 @@ def uneven_arm(args, wl, device, flush):
             raise RuntimeError(L.orac_gpu_last_error(e.ctx).decode())
         plain_ms.append(sum(ms) / len(ms))
     b = Batch(engines)
+    tune_batch = tuned(b)
     stream = torch.cuda.ExternalStream(b.stream(), device=device)
     b.run(args.warmup)
     nb = max(3, min(args.steps, 20))
@@ -479,7 +627,7 @@ def uneven_arm(args, wl, device, flush):
             "ms_per_step": sum(step_ms) / nb, "step_ms_p50": st[len(st) // 2],
             "step_ms_p99": st[min(len(st) - 1, int(0.99 * len(st)))],
             "plain_value": pval, "plain_ms_per_step_sum": sum(plain_ms), "speedup_vs_plain": bval / pval,
-            "device_bytes": footprint, "status_ok": all(x == 0 for x in status),
+            "device_bytes": footprint, "status_ok": all(x == 0 for x in status), "tuning": tune_batch,
             "host_build_s": t_build, "setup_s": t_setup,
             "how": f"one graph launch per H step advances all {n} systems (orac_gpu_batch_run), {nb} timed steps; "
                    f"plain = each system alone, {kp} timed steps each, summed (one at a time)"}
@@ -591,6 +739,103 @@ def f0_arm(args, device, flush):
     return out
 
 
+def config2_arm(args, device, flush):
+    """The solvated chain of the second workload: a 1,700-atom bonded chain
+    in 7,000 waters (22,700 atoms, 62 A box, SPME 64^3 order 5), FP32 pair
+    forces with fixed-point sums, FP64 integration; the chain's bonds,
+    bends and torsions on the N0/N1 levels (0.5 fs M step split 2 x 2).
+    MD rate of the device-resident driver, and the state's forces and
+    energies against the FP64 oracle."""
+    import torch
+
+    from orac_b200.engine import Engine
+
+    wl = dict(WORKLOADS["liquid"], n1respa=2, n0respa=2)
+    s = systems.config2_polymer()
+    e = Engine(s.copy(), device=device)
+    e.md_setup(wl["dt_h"], wl["lrespa"], wl["mrespa"], wl["nupdte"], wl["rshk"], n1respa=wl["n1respa"],
+               n0respa=wl["n0respa"], econst=0.0)
+    L = e.lib
+    st = torch.cuda.ExternalStream(L.orac_gpu_get_stream(e.ctx), device=device)
+    for _ in range(args.warmup):
+        L.orac_gpu_md_run_async(e.ctx, 1)
+    if e.collect():
+        raise RuntimeError(L.orac_gpu_last_error(e.ctx).decode())
+    k = max(3, min(args.steps, 20))
+    ms = _timed_steps(lambda: L.orac_gpu_md_run_async(e.ctx, 1), st, flush, k)
+    if e.collect():
+        raise RuntimeError(L.orac_gpu_last_error(e.ctx).decode())
+    x, _ = e.md_state()
+    e.close()
+    out = {"workload": f"1,700-atom bonded chain in 7,000 waters ({s.ntap} atoms), 62 A box, SPME 64^3 order 5, "
+                       "alpha 0.35, shells 5.0/7.5/10.0 A, r-RESPA 4/2/0.5 fs with the chain's bonded terms at "
+                       "0.25/0.125 fs, NVE",
+           "value": ns_per_day(k, wl["dt_h"], sum(ms) / 1e3), "unit": "ns/day", "ms_per_step": sum(ms) / k,
+           "steps": k}
+    try:
+        out["force_check"] = force_check(s, x)
+    except Exception as exc:
+        out["force_check"] = {"error": f"{type(exc).__name__}: {exc}"}
+    return out
+
+
+def config1_fixed_arm(args, device, flush):
+    """The 3,000-water box as specified (31 A, three times liquid density):
+    its dynamics heat and stop converging SHAKE within tens of steps, so its
+    rate is the force-evaluation rate on a fixed list at the seeded state --
+    every shell (M, L, H) and SPME, forces only, device-resident inputs."""
+    import ctypes as C
+
+    import torch
+
+    from orac_b200.engine import Engine
+
+    s = systems.config1_water()
+    e = Engine(s.copy(), device=device)
+    e.update_lists()
+    L = e.lib
+    dev = torch.device(f"cuda:{device}")
+    x = torch.tensor(np.concatenate([s.xp0, s.yp0, s.zp0]), dtype=torch.float64, device=dev)
+    g = torch.tensor(np.concatenate(s.group_centres()), dtype=torch.float64, device=dev)
+    m = torch.tensor(np.concatenate(s.molecule_centres()), dtype=torch.float64, device=dev)
+    f = torch.zeros(3 * s.ntap, dtype=torch.float64, device=dev)
+    eer = torch.zeros(1, dtype=torch.float64, device=dev)
+    vir = torch.zeros(9, dtype=torch.float64, device=dev)
+    st = torch.cuda.ExternalStream(L.orac_gpu_get_stream(e.ctx), device=device)
+
+    def one():
+        for sh in "mlh":
+            rc = L.orac_gpu_mts_forces_dev(e.ctx, sh.encode(), x.data_ptr(), g.data_ptr(), m.data_ptr(), f.data_ptr(),
+                                           None, None)
+            if rc:
+                raise RuntimeError(L.orac_gpu_last_error(e.ctx).decode())
+        rc = L.orac_gpu_fft_pme_dev(e.ctx, x.data_ptr(), m.data_ptr(), f.data_ptr(), eer.data_ptr(), vir.data_ptr())
+        if rc:
+            raise RuntimeError(L.orac_gpu_last_error(e.ctx).decode())
+
+    for _ in range(args.warmup):
+        one()
+    cnt = (C.c_int64 * 4)()
+    L.orac_gpu_counters(e.ctx, cnt, 1)
+    k = max(3, min(args.steps, 20))
+    ms = _timed_steps(one, st, flush, k)
+    L.orac_gpu_counters(e.ctx, cnt, 0)
+    e.close()
+    secs = sum(ms) / 1e3
+    out = {"workload": "3,000 rigid waters in the 31.0 A box as specified (9,000 atoms, 3x liquid density), SPME 32^3 "
+                       "order 4, alpha 0.35, shells 5.0/7.5/10.0 A, list fixed at the seeded state",
+           "force_evals_per_s": k / secs, "ms_per_force_eval": 1e3 * secs / k,
+           "pair_evals_per_s": (cnt[2] + cnt[3]) / secs,
+           "how": "one force evaluation = M, L and H shells plus SPME (forces only, device buffers, "
+                  "orac_gpu_mts_forces_dev / orac_gpu_fft_pme_dev), CUDA events on the context stream, L2 flushed "
+                  "before each"}
+    try:
+        out["force_check"] = force_check(s, s.cartesian())
+    except Exception as exc:
+        out["force_check"] = {"error": f"{type(exc).__name__}: {exc}"}
+    return out
+
+
 def profile_window_batch(nwin):
     """One batched step of `nwin` lambda windows bracketed for a profiler
     that starts collecting at cudaProfilerStart (the windows' set-up and
@@ -656,6 +901,9 @@ def main():
     ap.add_argument("--serve", type=float, default=3.0, help="seconds of Poisson arrivals of the serving leg (0: skip)")
     ap.add_argument("--serve-systems", type=int, default=16, help="systems the serving requests draw from")
     ap.add_argument("--no-f0", dest="f0", action="store_false", help="skip the ORAC test1 system leg")
+    ap.add_argument("--no-drift", dest="drift", action="store_false", help="skip the 1,000-step energy drift run")
+    ap.add_argument("--no-configs", dest="configs", action="store_false",
+                    help="skip the solvated-chain MD leg and the 31 A fixed-list leg")
     ap.add_argument("--profile-window-batch", type=int, default=0, metavar="N",
                     help="profiling aid, no JSON: N lambda windows batched, 3 steps, then one step bracketed by "
                          "cudaProfilerStart/Stop (ncu --profile-from-start off --graph-profiling graph)")
@@ -711,25 +959,39 @@ def main():
     secs = res["total_ms"] / 1e3
     value = ws * ns_per_day(args.steps, wl["dt_h"], secs)
     peaks = measured_peaks()
-    # dominant kernel: the real-space shell kernel (all shells)
+    # dominant kernel: the real-space shell kernel (all shells).  It is bound
+    # by FP32 issue (LJ + A&S erfc per atom pair, no contraction): the
+    # roofline is its pair FLOP rate against the device's measured FP32 FMA
+    # rate; the HBM view beside it shows it is far from the memory bound.
     n_l = max(1, res["kpair_n"])
     kp_s = res["kpair_ms"] / 1e3
+    npair = res["pairs_ewald"] + res["pairs_lj"]
     flops = 60.0 * res["pairs_ewald"] + 36.0 * res["pairs_lj"]
-    bytes_alg = 12.0 * (res["scanned"] + res["kept"]) + n_l * (40.0 * res["G"] + 48.0 * res["N"])
-    hbm_peak = peaks.get("hbm_gbs")
-    achieved_gbs = bytes_alg / kp_s / 1e9 if kp_s > 0 else 0.0
-    roofline = {"kernel": "k_pair (real-space r-RESPA shell kernel, all shells)", "bound": "hbm",
-                "achieved": achieved_gbs, "peak": hbm_peak if hbm_peak else 6650.0, "unit": "GB/s",
-                "frac": achieved_gbs / (hbm_peak if hbm_peak else 6650.0),
-                "peak_source": "measured" if hbm_peak else "fallback",
-                "traffic": ncu_traffic(), "bytes_per_launch": bytes_alg / n_l, "launches": res["kpair_n"],
+    fp32 = res.get("fp32_peak")
+    fp32_peak_v = fp32 if fp32 else FP32_NOMINAL_TFLOPS
+    achieved_tf = flops / kp_s / 1e12 if kp_s > 0 else 0.0
+    roofline = {"kernel": "k_pair (real-space r-RESPA shell kernel, all shells)", "bound": "fp32",
+                "achieved": achieved_tf, "peak": fp32_peak_v, "unit": "TFLOP/s", "frac": achieved_tf / fp32_peak_v,
+                "peak_source": ("measured (FP32 FMA-loop kernel, orac_gpu_fp32_rate, this run)" if fp32
+                                else "nominal 148 SM x 128 lanes x 2 x 1.965 GHz"),
+                "traffic": ncu_traffic(), "pair_evaluations_per_launch": npair / n_l,
+                "flops_per_pair": "60 LJ+Ewald, 36 LJ-only (FMA = 2)", "launches": res["kpair_n"],
                 "avg_launch_us": 1e6 * kp_s / n_l, "timing": res["kpair_how"],
-                "fp32_view": {"achieved": flops / kp_s / 1e12 if kp_s > 0 else 0.0, "unit": "TFLOP/s",
-                              "peak": FP32_NOMINAL_TFLOPS, "peak_source": "nominal (no measured FP32 peak)",
-                              "frac": (flops / kp_s / 1e12) / FP32_NOMINAL_TFLOPS if kp_s > 0 else 0.0,
-                              "pair_evaluations": res["pairs_ewald"] + res["pairs_lj"],
-                              "flops_per_pair": "60 LJ+Ewald, 36 LJ-only"},
                 "share_of_step": res["kpair_ms"] / res["total_ms"] if res["total_ms"] else None}
+    hbm_peak = peaks.get("hbm_gbs")
+    bytes_alg = 12.0 * (res["scanned"] + res["kept"]) + n_l * (40.0 * res["G"] + 48.0 * res["N"])
+    achieved_gbs = bytes_alg / kp_s / 1e9 if kp_s > 0 else 0.0
+    roofline_hbm = {"kernel": roofline["kernel"], "bound": "hbm", "achieved": achieved_gbs,
+                    "peak": hbm_peak if hbm_peak else 6650.0, "unit": "GB/s",
+                    "frac": achieved_gbs / (hbm_peak if hbm_peak else 6650.0),
+                    "peak_source": "measured" if hbm_peak else "fallback", "traffic": ncu_traffic(),
+                    "bytes_per_launch": bytes_alg / n_l,
+                    "bytes_counted": "12 B per list entry scanned or kept, 40 B per group, 48 B per atom"}
+    rates = {"pair_evals_per_s": npair / (res["total_ms"] / 1e3),
+             "shell_evals_per_s": res["shell_evals"] / (res["total_ms"] / 1e3),
+             "how": "pair evaluations (non-excluded atom pairs in a shell's band, device counters) and "
+                    "real-space shell evaluations (mts_forces calls: 8 M, 2 L, 1 H per 4-fs step) per second "
+                    "of the timed steps"}
     cpu = None
     if not args.no_cpu_baseline:
         t, done, cores = cpu_run(wl, s, 200, 1, budget_s=args.cpu_budget)
@@ -740,17 +1002,26 @@ def main():
     st = sorted(res["step_ms"])
     out = dict(base, value=value, ms_per_step=res["total_ms"] / args.steps,
                step_ms_p50=st[len(st) // 2], step_ms_p99=st[min(len(st) - 1, int(0.99 * len(st)))],
-               roofline=roofline, cpu_baseline=cpu,
+               roofline=roofline, roofline_hbm=roofline_hbm, force_evals=rates, cpu_baseline=cpu,
                e2e={"value": e2e_val, "unit": "ns/day", "h2d_bytes_per_step": res["bytes_io"],
                     "d2h_bytes_per_step": res["bytes_io"],
                     "how": "orac_gpu_md_set_state (pinned host -> device), one step, orac_gpu_md_get_state "
                            "(device -> pinned host, with the status flags), orac_gpu_md_collect, wall clock"},
-               gpu_launches=res["launches"], clocks=res["clocks"])
+               gpu_launches=res["launches"], clocks=res["clocks"], tuning=res["tuning"])
+    for key in ("force_check", "energy_conservation"):
+        if key in res:
+            out[key] = res[key]
     if "batched" in res:
         bt = res["batched"]
         bval = ns_per_day(args.steps, wl["dt_h"], bt["total_ms"] / 1e3) * bt["systems"]
         pval = ns_per_day(args.steps, wl["dt_h"], bt["plain_total_ms"] / 1e3)
-        d = np.array(bt["dudl"])
+        stats = [block_mean_err(x) for x in bt["dudl"]]
+        mean = np.array([m for m, _ in stats]) * units.KJMOL
+        err = np.array([e for _, e in stats]) * units.KJMOL
+        lam = np.asarray(bt["lambdas"])
+        wts = np.gradient(lam) * 0.0  # trapezoid weights
+        wts[1:] += 0.5 * np.diff(lam)
+        wts[:-1] += 0.5 * np.diff(lam)
         out["batched"] = {
             "workload": f"{bt['systems']} alchemical lambda windows (lambda_k = k/{bt['systems'] - 1}) of a 40-atom "
                         f"flexible ligand in the liquid water box ({bt['atoms_per_window']} atoms per window), "
@@ -759,14 +1030,24 @@ def main():
             "ms_per_step": bt["total_ms"] / args.steps, "step_ms_p50": bt["step_ms_p50"],
             "step_ms_p99": bt["step_ms_p99"], "plain_window_value": pval,
             "speedup_vs_plain": bval / pval,
-            "dudl_kjmol": {"first": float(d[0]) * units.KJMOL, "mid": float(d[len(d) // 2]) * units.KJMOL,
-                           "last": float(d[-1]) * units.KJMOL,
-                           "trapezoid_dG": float(np.trapezoid(d, bt["lambdas"])) * units.KJMOL},
+            "dudl_kjmol": {"lambda": [round(float(x), 5) for x in lam], "mean": [float(x) for x in mean],
+                           "stderr": [float(x) for x in err], "samples_per_window": len(bt["dudl"][0]),
+                           "trapezoid_dG": float((wts * mean).sum()),
+                           "trapezoid_dG_stderr": float(np.sqrt(((wts * err) ** 2).sum())),
+                           "how": f"energy records on the device every {DUDL_EVERY} steps of a batched run of "
+                                  f"{DUDL_STEPS} steps (orac_gpu_batch_run_energy) after the timed steps; mean and "
+                                  "standard error from 10 block means per window",
+                           "note": "the workload scales the ligand's LJ and charges by the same lambda; past "
+                                   "lambda ~0.2 the soft core (qsoft lambda^2) no longer keeps water charges off "
+                                   "the ligand's, and dU/dlambda grows to 1e4 kJ/mol: the estimate is not a "
+                                   "converged free energy"},
+            "tuning": bt["tuning"],
             "how": "one graph launch per H step advances every window (orac_gpu_batch_run); plain = one window "
-                   "alone through the same driver; dU/dlambda from an energy step at the end of each window"}
+                   "alone through the same driver; both with the real-space kernel's launch configuration chosen by "
+                   "the autotuner (orac_gpu_batch_tune / orac_gpu_tune)"}
     elif "batched_error" in res:
         out["batched"] = {"error": res["batched_error"]}
-    for key in ("orac_test1", "uneven", "served"):
+    for key in ("orac_test1", "config2", "config1_as_specified", "uneven", "served"):
         if key in res:
             out[key] = res[key]
     print(json.dumps(out))

@@ -374,6 +374,16 @@ int orac_gpu_md_set_state(orac_gpu_ctx* ctx, const double* x, const double* y,
 /* 0 = launch every kernel of a step directly, 1 = replay captured graphs. */
 int orac_gpu_md_set_graphs(orac_gpu_ctx* ctx, int on);
 
+/* Energy records kept on the device.  Every energy step (md_run's
+ * energy_every, or orac_gpu_batch_run_energy) writes one record of
+ * 16 doubles (the layout orac_gpu_md_run returns, with [0] the
+ * record's number) into a ring of the newest 2,048 records of the context.
+ * Copies the newest min(max, kept) records, oldest first, to out; n_total
+ * receives the number written since the last reset; reset != 0 clears the
+ * count.  Synchronises the context's stream. */
+int orac_gpu_md_records(orac_gpu_ctx* ctx, int max, double* out,
+                        int64_t* n_total, int reset);
+
 /* Batched systems ----------------------------------------------------------
  * Many independent systems (replicas, HREM states, alchemical windows), one
  * context each, advanced together: the batch splices every context's step
@@ -388,6 +398,9 @@ int orac_gpu_md_set_graphs(orac_gpu_ctx* ctx, int on);
 typedef struct orac_gpu_batch orac_gpu_batch;
 int orac_gpu_batch_create(orac_gpu_ctx** ctxs, int n, orac_gpu_batch** out);
 int orac_gpu_batch_run(orac_gpu_batch* b, int nsteps);
+/* The same with an energy record (orac_gpu_md_records) of every system on
+ * every energy_every-th step (0: none), each a captured energy step. */
+int orac_gpu_batch_run_energy(orac_gpu_batch* b, int nsteps, int energy_every);
 int orac_gpu_batch_sync(orac_gpu_batch* b);
 int orac_gpu_batch_destroy(orac_gpu_batch* b);
 const char* orac_gpu_batch_last_error(const orac_gpu_batch* b);
@@ -425,6 +438,29 @@ int orac_gpu_server_poll(orac_gpu_server* s, int max, int64_t* tickets,
 /* pending, running, finished not yet polled, submitted, finished,
  * reserved bytes, peak reserved bytes, steps launched */
 int orac_gpu_server_stats(orac_gpu_server* s, int64_t* out8);
+
+/* Launch configuration of the real-space kernel (no counterpart in the
+ * reference) ---------------------------------------------------------------
+ * Lanes per i group on the M shell and on the L/H shells (16 or 32; 16 only
+ * for groups of at most 4 atoms) and resident blocks per SM of its
+ * forces-only build (5, 6 or 8); 0 selects the default of the context's mode
+ * (alone 32, 32, 6; batched or served 16, 32, 8).  Forces, energies and
+ * trajectories do not depend on it: only speed does. */
+int orac_gpu_set_pair_tuning(orac_gpu_ctx* ctx, int lpg_m, int lpg_lh,
+                             int minb);
+/* The configuration in effect (lpg_m, lpg_lh, minb). */
+int orac_gpu_get_pair_tuning(orac_gpu_ctx* ctx, int* out3);
+/* Autotuner: every candidate configuration runs `trial` outer steps of the
+ * context (or of the batch, all members alike) after `trial` warm-up steps,
+ * timed with CUDA events; the fastest is applied, returned in out3 with its
+ * time per step, and appended to the text file cache_path (may be NULL) under
+ * the device name and the workload's shape (systems, atoms, group size,
+ * variants).  Unless force != 0, a shape already in the file is applied
+ * without timing.  The trial steps advance the systems. */
+int orac_gpu_tune(orac_gpu_ctx* ctx, int trial, const char* cache_path,
+                  int force, int* out3, double* ms_per_step);
+int orac_gpu_batch_tune(orac_gpu_batch* b, int trial, const char* cache_path,
+                        int force, int* out3, double* ms_per_step);
 
 /* Measurement (no counterpart in the reference, which times with wall
  * clocks in src/timer.f) ---------------------------------------------------

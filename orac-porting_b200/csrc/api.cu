@@ -188,7 +188,15 @@ int shell_run_r(orac_gpu_ctx* ctx, char rshell, const ShellRadii& radii, const d
   a.natom = ctx->N;
   a.wcnt = ctx->d_wcnt;
   variant_fill(ctx, &a);
-  a.occ_hi = ctx->shared_device ? 1 : 0;
+  // launch configuration: the tuned one, or the mode's default -- the
+  // innermost shell's rows hold about a dozen groups: beside other contexts
+  // half a warp each (fewer instructions per row) and 8 blocks per SM, alone
+  // a warp each (twice the warps to hide one launch's latency) and 6
+  if (rshell == 'm')
+    a.lpg = ctx->tune_lpg_m ? ctx->tune_lpg_m : (ctx->shared_device ? 16 : 32);
+  else
+    a.lpg = ctx->tune_lpg_lh ? ctx->tune_lpg_lh : 32;
+  a.minb = ctx->tune_minb ? ctx->tune_minb : (ctx->shared_device ? 8 : 6);
   const bool want_e = (flags & SH_ENERGY) && d_e, want_s = (flags & SH_STRESS) && d_stress;
   a.energy = want_e ? 1 : 0;
   a.stress = want_s ? 1 : 0;

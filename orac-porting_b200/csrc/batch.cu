@@ -6,13 +6,14 @@
 // replicas (HREM states, alchemical windows) as separate MPI ranks
 // (src/rem.f90, src/orac_mpi.f90).
 #include "common.cuh"
+#include "tune.cuh"
 
 struct MdState;
 
-// md.cu: captured step graph of a context (kind 0: plain step, 1: step with
-// list update); captures it on first use
+// md.cu: captured step graph of a context (kind bit 0: the step updates the
+// lists, bit 1: it writes an energy record); captures it on first use
 int md_step_graph(orac_gpu_ctx* ctx, int kind, cudaGraph_t* out);
-int md_advance(orac_gpu_ctx* ctx, int nsteps);
+int md_advance(orac_gpu_ctx* ctx, int nsteps, int kind);
 long long md_step_index(orac_gpu_ctx* ctx);
 int md_nupdte(orac_gpu_ctx* ctx);
 int md_check_flags(orac_gpu_ctx* ctx);
@@ -21,8 +22,8 @@ struct orac_gpu_batch {
   std::vector<orac_gpu_ctx*> ctx;
   std::vector<unsigned> gen;  // each context's param_gen when the batch was built
   cudaStream_t stream = nullptr;
-  cudaGraphExec_t exec[2] = {nullptr, nullptr};
-  cudaGraph_t graph[2] = {nullptr, nullptr};
+  cudaGraphExec_t exec[4] = {nullptr, nullptr, nullptr, nullptr};
+  cudaGraph_t graph[4] = {nullptr, nullptr, nullptr, nullptr};
   char err[512] = {0};
   int device = 0;
 };
@@ -99,7 +100,7 @@ int orac_gpu_batch_destroy(orac_gpu_batch* b) {
   if (!b) return ORAC_OK;
   cudaSetDevice(b->device);
   if (b->stream) cudaStreamSynchronize(b->stream);
-  for (int k = 0; k < 2; k++) {
+  for (int k = 0; k < 4; k++) {
     if (b->exec[k]) cudaGraphExecDestroy(b->exec[k]);
     if (b->graph[k]) cudaGraphDestroy(b->graph[k]);
   }
@@ -110,9 +111,11 @@ int orac_gpu_batch_destroy(orac_gpu_batch* b) {
 }
 
 // Advance every system of the batch by nsteps outer steps with one graph
-// launch per step.  All systems must have been set up with orac_gpu_md_setup
-// and share the list-update period and the current step index.
-int orac_gpu_batch_run(orac_gpu_batch* b, int nsteps) {
+// launch per step; with energy_every > 0 every energy_every-th step also
+// writes each system's energy record (orac_gpu_md_records).  All systems
+// must have been set up with orac_gpu_md_setup and share the list-update
+// period and the current step index.
+static int batch_run(orac_gpu_batch* b, int nsteps, int energy_every) {
   if (!b) return ORAC_ERR_PARAM;
   if (cudaSetDevice(b->device) != cudaSuccess) return bfail(b, ORAC_ERR_CUDA, "cudaSetDevice");
   const int nup = md_nupdte(b->ctx[0]);
@@ -125,11 +128,89 @@ int orac_gpu_batch_run(orac_gpu_batch* b, int nsteps) {
       return bfail(b, ORAC_ERR_STATE, "a system's parameters changed after the batch was built: build it again");
   for (int s = 0; s < nsteps; s++) {
     const long long step = md_step_index(b->ctx[0]);
-    const int kind = (step % nup == 0 && step > 0) ? 1 : 0;
+    int kind = (step % nup == 0 && step > 0) ? 1 : 0;
+    if (energy_every > 0 && (s + 1) % energy_every == 0) kind |= 2;
     if (int rc = build_kind(b, kind)) return rc;
     if (cudaGraphLaunch(b->exec[kind], b->stream) != cudaSuccess) return bfail(b, ORAC_ERR_CUDA, "cudaGraphLaunch");
-    for (auto* c : b->ctx) md_advance(c, 1);
+    for (auto* c : b->ctx) md_advance(c, 1, kind);
   }
+  return ORAC_OK;
+}
+
+int orac_gpu_batch_run(orac_gpu_batch* b, int nsteps) { return batch_run(b, nsteps, 0); }
+
+int orac_gpu_batch_run_energy(orac_gpu_batch* b, int nsteps, int energy_every) {
+  if (energy_every < 0) return bfail(b, ORAC_ERR_PARAM, "energy_every < 0");
+  return batch_run(b, nsteps, energy_every);
+}
+
+// Drop the parent graphs (built again on the next run from the members'
+// current step graphs) and take the members' parameter generations.
+static void batch_reset_graphs(orac_gpu_batch* b) {
+  cudaStreamSynchronize(b->stream);
+  for (int k = 0; k < 4; k++) {
+    if (b->exec[k]) cudaGraphExecDestroy(b->exec[k]);
+    if (b->graph[k]) cudaGraphDestroy(b->graph[k]);
+    b->exec[k] = nullptr;
+    b->graph[k] = nullptr;
+  }
+  for (size_t k = 0; k < b->ctx.size(); k++) b->gen[k] = b->ctx[k]->param_gen;
+}
+
+// The autotuner on the batch: every candidate configuration (the same for
+// all members) runs `trial` batched steps after `trial` warm-up steps that
+// capture its graphs, timed with CUDA events on the batch's stream.
+int orac_gpu_batch_tune(orac_gpu_batch* b, int trial, const char* cache_path, int force, int* out3,
+                        double* ms_per_step) {
+  if (!b || trial < 1) return ORAC_ERR_PARAM;
+  if (cudaSetDevice(b->device) != cudaSuccess) return bfail(b, ORAC_ERR_CUDA, "cudaSetDevice");
+  const std::string sig = tune_signature(b->ctx, "batch");
+  PairTune best{0, 0, 0};
+  double best_ms = 0.0;
+  if (!force && tune_cache_find(cache_path, sig, &best, &best_ms)) {
+    for (auto* c : b->ctx) tune_apply(c, best);
+    batch_reset_graphs(b);
+  } else {
+    int maxg = 0;
+    for (auto* c : b->ctx) maxg = c->maxg > maxg ? c->maxg : maxg;
+    std::vector<PairTune> cand;
+    tune_candidates(maxg, &cand);
+    cudaEvent_t e0, e1;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)
+      return bfail(b, ORAC_ERR_CUDA, "cudaEventCreate");
+    int rc = ORAC_OK;
+    for (const PairTune& c : cand) {
+      for (auto* x : b->ctx) tune_apply(x, c);
+      batch_reset_graphs(b);
+      if ((rc = batch_run(b, trial, 0)) || (rc = orac_gpu_batch_sync(b))) break;
+      cudaEventRecord(e0, b->stream);
+      if ((rc = batch_run(b, trial, 0))) break;
+      cudaEventRecord(e1, b->stream);
+      if ((rc = orac_gpu_batch_sync(b))) break;
+      float ms = 0.f;
+      if (cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {
+        rc = bfail(b, ORAC_ERR_CUDA, "cudaEventElapsedTime");
+        break;
+      }
+      const double per = ms / trial;
+      if (best.lpg_m == 0 || per < best_ms) {
+        best = c;
+        best_ms = per;
+      }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+    for (auto* c : b->ctx) tune_apply(c, best);
+    batch_reset_graphs(b);
+    tune_cache_add(cache_path, sig, best, best_ms);
+  }
+  if (out3) {
+    out3[0] = best.lpg_m;
+    out3[1] = best.lpg_lh;
+    out3[2] = best.minb;
+  }
+  if (ms_per_step) *ms_per_step = best_ms;
   return ORAC_OK;
 }
 

@@ -120,9 +120,11 @@ struct PairArgs {
   // 0: skip the image term of the molecular virial and the block reduction
   // (MD without pressure coupling needs neither)
   int stress;
-  // the context runs beside others (batch, server): the forces-only kernel
-  // takes its higher-occupancy build (fewer registers, more warps per SM)
-  int occ_hi;
+  // lanes that own one i group: 32, or 16 (two groups per warp) for lists
+  // with short rows; 16 applies to groups of at most 4 atoms
+  int lpg;
+  // resident blocks per SM of the forces-only build (5, 6 or 8)
+  int minb;
   // variant (VAR_*); REM: seg_select kind and rem_factor(3)
   int variant;
   const unsigned char* vflag;  // [N]
@@ -222,6 +224,12 @@ struct orac_gpu_ctx {
   // Ewald, box, cells, variant, lambdas): captured step graphs older than
   // it are captured again
   unsigned param_gen = 0;
+  // pair-kernel launch configuration (orac_gpu_set_pair_tuning, the
+  // autotuner): lanes per i group on the M shell and on the L/H shells,
+  // resident blocks per SM; 0 = the default for the context's mode (alone:
+  // 32, 32, 6; beside other contexts: 16, 32, 8).  Results do not depend on
+  // it (fixed-point sums)
+  int tune_lpg_m = 0, tune_lpg_lh = 0, tune_minb = 0;
   std::unordered_map<void*, size_t> dmem;  // live device allocations
   size_t dmem_bytes = 0;
   int device = 0;

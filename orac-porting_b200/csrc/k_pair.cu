@@ -31,6 +31,8 @@ constexpr float AS_A1 = 0.2548296f, AS_A2 = -0.28449674f, AS_A3 = 1.4214137f;
 constexpr float AS_A4 = -1.453152f, AS_A5 = 1.0614054f, AS_QP = 0.3275911f;
 constexpr int LJ_SMEM_MAX = 2048;  // staged LJ table entries: 16 KB beside the static queues
 
+__device__ __forceinline__ long long to_fix(float v) { return __float2ll_rn(v * (float)ORAC_FSCALE); }
+
 __device__ __forceinline__ void fix_add(unsigned long long* p, float v) {
   long long q = __float2ll_rn(v * (float)ORAC_FSCALE);
   if (q != 0) atomicAdd(p, (unsigned long long)q);
@@ -42,6 +44,37 @@ __device__ __forceinline__ float seg_sum(float v) {
 #pragma unroll
   for (int o = W / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   return v;
+}
+
+// Sum of P values over the aligned runs of W lanes, scattered: at each
+// shuffle step a lane keeps half of its values and receives the matching
+// half of its partner's, so P - 1 shuffles (plus log2(W / P) for the last
+// value) replace P full butterflies.  Returns the segment's total of value
+// rs_index<W, P>(lane % W).
+template <int W, int P, typename T>
+__device__ __forceinline__ T reduce_scatter(T (&v)[P], int sl) {
+#pragma unroll
+  for (int h = P / 2, o = W / 2; h >= 1; h >>= 1, o >>= 1) {
+    const bool up = (sl & o) != 0;
+#pragma unroll
+    for (int k = 0; k < h; k++) {
+      const T send = up ? v[k] : v[k + h];
+      const T keep = up ? v[k + h] : v[k];
+      v[k] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+    }
+  }
+  T r = v[0];
+#pragma unroll
+  for (int o = W / P / 2; o >= 1; o >>= 1) r += __shfl_xor_sync(0xffffffffu, r, o);
+  return r;
+}
+
+template <int W, int P>
+__device__ __forceinline__ int rs_index(int sl) {
+  int idx = 0;
+#pragma unroll
+  for (int o = W / 2, h = P / 2; h >= 1; o >>= 1, h >>= 1) idx += (sl & o) ? h : 0;
+  return idx;
 }
 
 __device__ __forceinline__ double warp_sumd(double v) {
@@ -230,20 +263,15 @@ __device__ __forceinline__ void alch_energy_fp64(const PairArgs& A, double rx, d
   }
 }
 
-#ifndef ORAC_KPAIR_MINB
-#define ORAC_KPAIR_MINB 6  // resident blocks per SM requested of the forces-only kernel
-#endif
-#ifndef ORAC_KPAIR_MINB_HI
-#define ORAC_KPAIR_MINB_HI 8  // the same, for contexts that share the device with others
-#endif
 
-// Ring capacities of the per-warp queues.  Entries: at most 31 left over
-// from the previous chunk plus 32 new.  Atom slots: at most 31 left over
-// plus 32 entries of MG atoms.
-constexpr int QE = 64;
-template <int MG>
-struct SlotRing {
-  static constexpr int n = (31 + 32 * MG) <= 128 ? 128 : ((31 + 32 * MG) <= 256 ? 256 : 512);
+// Ring capacities of the per-group queues (LPG lanes own one i group).
+// Entries: at most LPG - 1 left over from the previous chunk plus LPG new.
+// Atom slots: at most LPG - 1 left over plus LPG entries of MG atoms.
+template <int MG, int LPG>
+struct Rings {
+  static constexpr int QE = 2 * LPG;
+  static constexpr int need = LPG - 1 + LPG * MG;
+  static constexpr int QS = need <= 64 ? 64 : (need <= 128 ? 128 : (need <= 256 ? 256 : 512));
 };
 
 // A slot names one j atom of a queued entry: entry (6 bits), its position t
@@ -253,51 +281,57 @@ __device__ __forceinline__ unsigned short slot_pack(int e, int t, int b, int n) 
   return (unsigned short)(e | (t << 6) | (b << 9) | ((n - 1) << 12));
 }
 
-// One warp owns one i group for a whole list row.
+// LPG lanes own one i group for a whole list row: 32 (a warp) for the long
+// rows of the L and H lists, 16 (two groups per warp) for the short rows of
+// the M list, where a full warp would leave most lanes idle.
 //
-// Phase 1 (a lane per list entry, 32 entries per chunk): FP64 minimum image
+// Phase 1 (a lane per list entry, LPG entries per chunk): FP64 minimum image
 // and band of the group pair, the next shell's list entry, and, for an
 // in-band entry, its geometry (FP32 centre distance, S, S', and in FP64 what
-// the energies need) into the warp's entry queue and one slot per j atom to
-// evaluate into the slot queue (order kept by ballots and a warp scan).
+// the energies need) into the group's entry queue and one slot per j atom to
+// evaluate into its slot queue (order kept by ballots and a segment scan).
 //
-// Phase 2 (a lane per j atom): passes of up to 32 slots that hold whole
+// Phase 2 (a lane per j atom): passes of up to LPG slots that hold whole
 // entries.  A lane takes its j atom's offset and charge once and runs over
-// the i atoms (broadcast reads of shared memory): the j
-// atom's force sums in the lane, and goes out with one fixed-point atomic per
-// component, S'(R) V term included; the entry's V is a segmented shuffle sum
-// over the entry's lanes.  The i atoms' forces sum per lane across passes
-// and leave by one warp reduction at the end of the row.
+// the i atoms (broadcast reads of shared memory): the j atom's force sums in
+// the lane, and goes out with one fixed-point atomic per component, S'(R) V
+// term included; the entry's V is a segmented shuffle sum over the entry's
+// lanes.  The i atoms' forces sum per lane across passes and leave by one
+// segment reduction at the end of the row.
 //
-// HI: the build for contexts sharing the device, where throughput over many
-// concurrent kernels matters more than one launch's latency.
-template <int MG, bool EN, int VAR, bool HI>
-__global__ void __launch_bounds__(WPB * 32, (MG <= 4 && !EN) ? (HI ? ORAC_KPAIR_MINB_HI : ORAC_KPAIR_MINB) : 1)
-    k_pair(const PairArgs A) {
+// MINB: resident blocks per SM the forces-only build is compiled for (5, 6
+// or 8; fewer registers per thread the more blocks); a context alone favours
+// one launch's latency, contexts sharing the device more warps per SM.
+template <int MG, bool EN, int VAR, int LPG, int MINB>
+__global__ void __launch_bounds__(WPB * 32, MINB) k_pair(const PairArgs A) {
   pdl_enter();
-  constexpr int QS = SlotRing<MG>::n;
+  constexpr int SEG = 32 / LPG;  // groups per warp
+  constexpr int QE = Rings<MG, LPG>::QE, QS = Rings<MG, LPG>::QS;
+  constexpr int NQ = WPB * SEG;  // groups per block
   constexpr unsigned FULL = 0xffffffffu;
   extern __shared__ float2 s_lj[];
-  __shared__ float4 s_ai[WPB][MG];
-  __shared__ int s_ti[WPB][MG];  // the i atom's row of the LJ tables (type * ntype)
-  __shared__ float s_pm[WPB][MG];
-  __shared__ double s_qd[WPB][EN ? MG : 1];
-  __shared__ int s_fi[WPB][VAR != VAR_STD ? MG : 1];
-  __shared__ float2 s_sf[WPB][VAR == VAR_ALCH ? MG : 1];
+  __shared__ float4 s_ai[NQ][MG];
+  __shared__ int s_ti[NQ][MG];  // the i atom's row of the LJ tables (type * ntype)
+  __shared__ float s_pm[NQ][MG];
+  __shared__ double s_qd[NQ][EN ? MG : 1];
+  __shared__ int s_fi[NQ][VAR != VAR_STD ? MG : 1];
+  __shared__ float2 s_sf[NQ][VAR == VAR_ALCH ? MG : 1];
   // entry queue: centre distance and S, S', j group metadata, skip mask;
   // FP64 distance and S and the Cartesian image for the energy build
-  __shared__ float4 s_edc[WPB][QE];
-  __shared__ float s_edsw[WPB][QE];
-  __shared__ int2 s_emeta[WPB][QE];
-  __shared__ unsigned long long s_emsk[WPB][QE];
-  __shared__ double4 s_ecd[EN ? WPB : 1][EN ? QE : 1];
-  __shared__ float4 s_eimg[EN ? WPB : 1][EN ? QE : 1];
-  __shared__ unsigned short s_slot[WPB][QS];
+  __shared__ float4 s_edc[NQ][QE];
+  __shared__ float s_edsw[NQ][QE];
+  __shared__ int2 s_emeta[NQ][QE];
+  __shared__ unsigned long long s_emsk[NQ][QE];
+  __shared__ double4 s_ecd[EN ? NQ : 1][EN ? QE : 1];
+  __shared__ float4 s_eimg[EN ? NQ : 1][EN ? QE : 1];
+  __shared__ unsigned short s_slot[NQ][QS];
   __shared__ double s_red[WPB][ACC_N];
   __shared__ double s_vimg[WPB][9];
 
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const unsigned lanes_below = (1u << lane) - 1u;
+  const int sub = lane / LPG, sl = lane % LPG, q = warp * SEG + sub;
+  const unsigned below = (1u << sl) - 1u;  // lanes of this segment below this one
+  const int seg0 = sub * LPG;              // first lane of this segment
   const int nt2 = A.ntype * A.ntype;
   const bool staged = nt2 <= LJ_SMEM_MAX;
   if (threadIdx.x < WPB * 9) s_vimg[threadIdx.x / 9][threadIdx.x % 9] = 0.0;
@@ -307,6 +341,8 @@ __global__ void __launch_bounds__(WPB * 32, (MG <= 4 && !EN) ? (HI ? ORAC_KPAIR_
   const float2* lj = staged ? s_lj : A.lj;
   // under lskip_ewald an atom without LJ has no pair to evaluate
   const bool ljonly = VAR != VAR_ALCH && A.lskip && A.ewald;
+  // this segment's bits of a warp ballot
+  auto segbits = [&](unsigned b) -> unsigned { return SEG == 1 ? b : (b >> seg0) & 0xffffu; };
 
   double ec0 = 0, ec1 = 0, ec2 = 0, eq0 = 0, eq1 = 0, eq2 = 0;
   double ex0 = 0, ex1 = 0, ex2 = 0;  // variant sums (ACC_X)
@@ -316,43 +352,49 @@ __global__ void __launch_bounds__(WPB * 32, (MG <= 4 && !EN) ? (HI ? ORAC_KPAIR_
   // the terms cancel heavily, so no FP32 sums across lanes)
   float vimg[9];
 #pragma unroll
-  for (int q = 0; q < 9; q++) vimg[q] = 0.f;
+  for (int c = 0; c < 9; c++) vimg[c] = 0.f;
   auto flush_vimg = [&]() {  // every lane of the warp calls it
 #pragma unroll
-    for (int q = 0; q < 9; q++) {
-      const double t = warp_sumd((double)vimg[q]);
-      if (lane == 0) s_vimg[warp][q] += t;
-      vimg[q] = 0.f;
+    for (int c = 0; c < 9; c++) {
+      const double t = warp_sumd((double)vimg[c]);
+      if (lane == 0) s_vimg[warp][c] += t;
+      vimg[c] = 0.f;
     }
   };
 
   // every lane of a warp runs the same trip counts, so the warp-wide
   // ballots and shuffles stay convergent
-  for (int i = blockIdx.x * WPB + warp; i < A.ngrp; i += gridDim.x * WPB) {
-    const int2 mi = A.gmeta[i];
+  for (int pw = blockIdx.x * WPB + warp; pw * SEG < A.ngrp; pw += gridDim.x * WPB) {
+    const int i = pw * SEG + sub;
+    const bool gvalid = i < A.ngrp;
+    const int2 mi = gvalid ? A.gmeta[i] : make_int2(0, 0);
     const int ifirst = mi.x, ni = mi.y & 0xff, typei = (mi.y >> 8) & 0xff, ljmi = mi.y >> 16;
-    const double4 gi = A.gpos[i];
-    const int row = A.off[i], m = A.cnt[i];
-    if (lane < ni) {
-      s_ai[warp][lane] = A.aoff[ifirst + lane];
-      s_ti[warp][lane] = A.atype[ifirst + lane] * A.ntype;
-      s_pm[warp][lane] = A.apm[ifirst + lane];
-      if (EN) s_qd[warp][lane] = A.qd[ifirst + lane];
-      if (VAR != VAR_STD) s_fi[warp][lane] = A.vflag[ifirst + lane];
-      if (VAR == VAR_ALCH) s_sf[warp][lane] = A.soft[ifirst + lane];
+    const double4 gi = gvalid ? A.gpos[i] : make_double4(0.0, 0.0, 0.0, 0.0);
+    const int row = gvalid ? A.off[i] : 0, m = gvalid ? A.cnt[i] : 0;
+    int mmax = m;
+    if (SEG == 2) mmax = max(mmax, __shfl_xor_sync(FULL, m, 16));
+    if (sl < ni) {
+      s_ai[q][sl] = A.aoff[ifirst + sl];
+      s_ti[q][sl] = A.atype[ifirst + sl] * A.ntype;
+      s_pm[q][sl] = A.apm[ifirst + sl];
+      if (EN) s_qd[q][sl] = A.qd[ifirst + sl];
+      if (VAR != VAR_STD) s_fi[q][sl] = A.vflag[ifirst + sl];
+      if (VAR == VAR_ALCH) s_sf[q][sl] = A.soft[ifirst + sl];
     }
     __syncwarp();
-    float fi[MG][3];
+    // the i atoms' forces of this lane's pairs and S'V shares, in fixed
+    // point: integer sums are exact, so the row's total does not depend on
+    // which lane took which j atom (half or full warps, any block shape)
+    long long fiq[MG][3];
 #pragma unroll
-    for (int a = 0; a < MG; a++) fi[a][0] = fi[a][1] = fi[a][2] = 0.f;
-    float svx = 0.f, svy = 0.f, svz = 0.f;  // sum of the S'V vectors of this row's switched entries
+    for (int a = 0; a < MG; a++) fiq[a][0] = fiq[a][1] = fiq[a][2] = 0ll;
 
     int nout = 0;
     int qh = 0, qn = 0;  // entry queue: head, entries pending
     int sh = 0, sn = 0;  // slot queue: head, slots pending
-    for (int base = 0; base < m; base += 32) {
+    for (int base = 0; base < mmax; base += LPG) {
       // ---- phase 1: geometry of list entry k (src/force.f:265-333)
-      const int k = base + lane;
+      const int k = base + sl;
       const bool valid = k < m;
       int j = 0;
       unsigned long long msk = 0ull;
@@ -377,9 +419,9 @@ __global__ void __launch_bounds__(WPB * 32, (MG <= 4 && !EN) ? (HI ? ORAC_KPAIR_
       }
       if (A.next_on) {  // the next inner shell's list, order kept (src/force.f:279-286)
         const bool keep = valid && drj < A.r2neigh;
-        const unsigned bal = __ballot_sync(FULL, keep);
+        const unsigned bal = segbits(__ballot_sync(FULL, keep));
         if (keep) {
-          const int pos = nout + __popc(bal & lanes_below);
+          const int pos = nout + __popc(bal & below);
           A.j_out[row + pos] = j;
           A.mask_out[row + pos] = msk;
         }
@@ -392,37 +434,37 @@ __global__ void __launch_bounds__(WPB * 32, (MG <= 4 && !EN) ? (HI ? ORAC_KPAIR_
       float sw = 1.f, dsw = 0.f;
       double swd = 1.0;
       if (valid) {
-        if (drj >= A.r2inn0 && drj < A.r2out) {
-          inb = true;
-        } else if (drj >= A.r2out && drj < A.r2out0) {
-          // S(R) of src/force.f:311-317 for the forces: FP32 arithmetic on the
-          // two factors taken in FP64, the distance to the band edge (rout0 - R)
-          // and auxa (arsout1 + 2R, where -3 rout and 2R cancel to under a
-          // tenth of their size): FP32 R would leave both with 1e-5 relative
-          // error.  FP64 where S enters the energies
-          const double rspd = sqrt(drj);
-          const float rsp = (float)rspd;
-          const float auxa = (float)((A.arsout1 + 2.0 * rspd) * A.diarsout2);
-          const float auxb = (float)(A.rout0 - rspd);
-          sw = auxa * auxb * auxb;
-          dsw = (-2.0f * auxa * auxb + 2.0f * auxb * auxb * A.iarsout2) / rsp;
+        const bool sw_out = drj >= A.r2out && drj < A.r2out0;
+        const bool sw_in = drj >= A.r2inn && drj < A.r2inn0;
+        inb = (drj >= A.r2inn0 && drj < A.r2out) || sw_out || sw_in;
+        if (sw_out || sw_in) {
+          // S(R) of src/force.f:311-317 for the forces: FP32 arithmetic on
+          // the two factors taken in FP64, the distance to the band edge
+          // (edge - R) and auxa (ars1 + 2R, where -3 r and 2R cancel to under
+          // a tenth of their size): FP32 R would leave both with 1e-5
+          // relative error.  R in FP64 from an FP32 reciprocal square root
+          // and one Newton step (relative error ~1e-14); the outer band
+          // gives S = auxa auxb^2, the inner one 1 - auxa auxb^2, both from
+          // the same code with the band's constants.  FP64 where S enters
+          // the energies.
+          const double edge = sw_out ? A.rout0 : A.rinn0;
+          const double ars1 = sw_out ? A.arsout1 : A.arsinn1;
+          const double iars2 = sw_out ? A.diarsout2 : A.diarsinn2;
+          const float iars2f = sw_out ? A.iarsout2 : A.iarsinn2;
+          const float sgn = sw_out ? 1.f : -1.f;
+          double y = (double)rsqrtf((float)drj);
+          y = y * (1.5 - 0.5 * drj * y * y);
+          const double rspd = drj * y;
+          const float auxa = (float)((ars1 + 2.0 * rspd) * iars2);
+          const float auxb = (float)(edge - rspd);
+          const float s3 = auxa * auxb * auxb;
+          sw = sw_out ? s3 : 1.0f - s3;
+          dsw = sgn * (-2.0f * auxa * auxb + 2.0f * auxb * auxb * iars2f) * (float)y;
           if (EN) {
-            const double auxbd = A.rout0 - rspd;
-            swd = (A.arsout1 + 2.0 * rspd) / A.arsout2 * auxbd * auxbd;
+            const double auxbd = edge - rspd;
+            const double s3d = (ars1 + 2.0 * rspd) * iars2 * auxbd * auxbd;
+            swd = sw_out ? s3d : 1.0 - s3d;
           }
-          inb = true;
-        } else if (drj >= A.r2inn && drj < A.r2inn0) {
-          const double rspd = sqrt(drj);
-          const float rsp = (float)rspd;
-          const float auxa = (float)((A.arsinn1 + 2.0 * rspd) * A.diarsinn2);
-          const float auxb = (float)(A.rinn0 - rspd);
-          sw = 1.0f - auxa * auxb * auxb;
-          dsw = (2.0f * auxa * auxb - 2.0f * auxb * auxb * A.iarsinn2) / rsp;
-          if (EN) {
-            const double auxbd = A.rinn0 - rspd;
-            swd = 1.0 - (A.arsinn1 + 2.0 * rspd) / A.arsinn2 * auxbd * auxbd;
-          }
-          inb = true;
         }
       }
       // the j atoms to evaluate: all, or under lskip_ewald those with LJ --
@@ -434,32 +476,32 @@ __global__ void __launch_bounds__(WPB * 32, (MG <= 4 && !EN) ? (HI ? ORAC_KPAIR_
         if (ljonly && dsw == 0.f) bm &= (unsigned)(mj.y >> 16);
       }
       const int na = __popc(bm);
-      int sc = na;  // inclusive warp scan of the slot counts
+      int sc = na;  // inclusive scan of the slot counts over the segment
 #pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
+      for (int o = 1; o < LPG; o <<= 1) {
         const int v = __shfl_up_sync(FULL, sc, o);
-        if (lane >= o) sc += v;
+        if (sl >= o) sc += v;
       }
-      const int tot = __shfl_sync(FULL, sc, 31);
-      const unsigned bq = __ballot_sync(FULL, na > 0);
+      const int tot = __shfl_sync(FULL, sc, seg0 + LPG - 1);
+      const unsigned bq = segbits(__ballot_sync(FULL, na > 0));
       if (na > 0) {
-        const int e = (qh + qn + __popc(bq & lanes_below)) & (QE - 1);
-        s_edc[warp][e] = make_float4((float)cx, (float)cy, (float)cz, sw);
-        s_edsw[warp][e] = dsw;
-        s_emeta[warp][e] = mj;
-        s_emsk[warp][e] = msk;
+        const int e = (qh + qn + __popc(bq & below)) & (QE - 1);
+        s_edc[q][e] = make_float4((float)cx, (float)cy, (float)cz, sw);
+        s_edsw[q][e] = dsw;
+        s_emeta[q][e] = mj;
+        s_emsk[q][e] = msk;
         if constexpr (EN) {
-          s_ecd[warp][e] = make_double4(cx, cy, cz, swd);
+          s_ecd[q][e] = make_double4(cx, cy, cz, swd);
           if (A.stress)  // j sits at its image xpg_j + img: its virial arm gains co.img
-            s_eimg[warp][e] = make_float4((float)(A.c11 * imx + A.c12 * imy + A.c13 * imz),
-                                          (float)(A.c22 * imy + A.c23 * imz), (float)(A.c33 * imz), 0.f);
+            s_eimg[q][e] = make_float4((float)(A.c11 * imx + A.c12 * imy + A.c13 * imz),
+                                       (float)(A.c22 * imy + A.c23 * imz), (float)(A.c33 * imz), 0.f);
         }
-        int ps = sh + sn + sc - na;
+        const int ps = sh + sn + sc - na;
         unsigned bb = bm;
         for (int t = 0; t < na; t++) {
           const int b = __ffs(bb) - 1;
           bb &= bb - 1u;
-          s_slot[warp][(ps + t) & (QS - 1)] = slot_pack(e, t, b, na);
+          s_slot[q][(ps + t) & (QS - 1)] = slot_pack(e, t, b, na);
         }
       }
       qn += __popc(bq);
@@ -467,23 +509,28 @@ __global__ void __launch_bounds__(WPB * 32, (MG <= 4 && !EN) ? (HI ? ORAC_KPAIR_
       __syncwarp();
 
       // ---- phase 2: passes over whole entries, a lane per j atom
-      const bool last = base + 32 >= m;
-      while (sn >= 32 || (last && sn > 0)) {
-        int L = sn;
-        if (sn > 32) L = 32 - (((int)s_slot[warp][(sh + 32) & (QS - 1)] >> 6) & 7);
-        else if (sn == 32) L = 32;
-        const bool act = lane < L;
-        const unsigned r = act ? (unsigned)s_slot[warp][(sh + lane) & (QS - 1)] : 0u;
+      const bool last = base + LPG >= m;
+      for (;;) {
+        const bool want = sn >= LPG || (last && sn > 0);
+        if (!__any_sync(FULL, want)) break;
+        int L = 0;
+        if (want) {
+          L = sn;
+          if (sn > LPG) L = LPG - (((int)s_slot[q][(sh + LPG) & (QS - 1)] >> 6) & 7);
+          else if (sn == LPG) L = LPG;
+        }
+        const bool act = sl < L;
+        const unsigned r = act ? (unsigned)s_slot[q][(sh + sl) & (QS - 1)] : 0u;
         const int e = r & 63, t = (r >> 6) & 7, b = (r >> 9) & 7, nsl = ((r >> 12) & 7) + 1;
         float fbx = 0.f, fby = 0.f, fbz = 0.f, vpart = 0.f;
         float4 dcs = make_float4(0.f, 0.f, 0.f, 1.f);
         float dswe = 0.f;
         int jat = 0, typej = 0;
         if (act) {
-          dcs = s_edc[warp][e];
-          dswe = s_edsw[warp][e];
-          const int2 me = s_emeta[warp][e];
-          const unsigned long long mskb = s_emsk[warp][e] >> b;
+          dcs = s_edc[q][e];
+          dswe = s_edsw[q][e];
+          const int2 me = s_emeta[q][e];
+          const unsigned long long mskb = s_emsk[q][e] >> b;
           jat = me.x + b;
           typej = (me.y >> 8) & 0xff;
           const float4 ob = A.aoff[jat];
@@ -493,14 +540,14 @@ __global__ void __launch_bounds__(WPB * 32, (MG <= 4 && !EN) ? (HI ? ORAC_KPAIR_
           const float2 sfb = (VAR == VAR_ALCH) ? A.soft[jat] : make_float2(0.f, 0.f);
           const float bx = dcs.x - ob.x, by = dcs.y - ob.y, bz = dcs.z - ob.z;
           double4 cd = make_double4(0.0, 0.0, 0.0, 1.0);
-          if (EN) cd = s_ecd[warp][e];
+          if (EN) cd = s_ecd[q][e];
           double pconf = 0.0, pcoul = 0.0, px0 = 0.0, px1 = 0.0, px2 = 0.0;
 #pragma unroll
           for (int a = 0; a < MG; a++) {
             if (a >= ni) break;
             if ((mskb >> (a * 8)) & 1ull) continue;
             if (ljonly && !((ljmi >> a) & 1)) continue;
-            const float4 ai = s_ai[warp][a];  // a broadcast read
+            const float4 ai = s_ai[q][a];  // a broadcast read
             const float rx = ai.x + bx, ry = ai.y + by, rz = ai.z + bz;
             float qf = 0.f, conf = 0.f, coul = 0.f;
             bool ljon = false;
@@ -508,16 +555,16 @@ __global__ void __launch_bounds__(WPB * 32, (MG <= 4 && !EN) ? (HI ? ORAC_KPAIR_
             if constexpr (VAR == VAR_ALCH) {
               // src/force_alchemy.f:412-451: exclusions and fixed-mass pairs
               // are always skipped; no LJ and no Coulomb skips the pair
-              const int fia = s_fi[warp][a];
+              const int fia = s_fi[q][a];
               if (fia & fjb & VF_MINF) continue;
-              const float2 sa = s_sf[warp][a];
+              const float2 sa = s_sf[q][a];
               const float eps4 = sa.y * sfb.y;
               if (eps4 < 1e-12f && A.lskip && A.ewald) continue;
               npairs++;
               tal = (fia >> VF_SSHIFT) + (fjb >> VF_SSHIFT) - 4;
               alch_pair_f32(A, rx * rx + ry * ry + rz * rz, tal, sa.x, sfb.x, eps4, ai.w * ob.w, &qf, &conf, &coul);
             } else {
-              const float2 Lp = lj[s_ti[warp][a] + tb];
+              const float2 Lp = lj[s_ti[q][a] + tb];
               ljon = Lp.y != 0.f;
               if (A.lskip && !ljon && A.ewald) continue;  // src/force.f:416-417
               npairs++;
@@ -549,7 +596,7 @@ __global__ void __launch_bounds__(WPB * 32, (MG <= 4 && !EN) ? (HI ? ORAC_KPAIR_
             }
             // force_rem (src/force_REM.f:491-495,634-678): selected pairs scale
             // their force and their share of the S'V sum
-            const bool sel = (VAR == VAR_REM) && seg_sel(A.rem_kind, s_fi[warp][a], fjb);
+            const bool sel = (VAR == VAR_REM) && seg_sel(A.rem_kind, s_fi[q][a], fjb);
             vpart += sel ? (conf + coul) * A.rem_factor : conf + coul;
             qf *= dcs.w;
             if (sel) qf *= A.rem_factor;
@@ -560,23 +607,22 @@ __global__ void __launch_bounds__(WPB * 32, (MG <= 4 && !EN) ? (HI ? ORAC_KPAIR_
               double cdd, qdd;
               if constexpr (VAR == VAR_ALCH) {
                 double c0, q0, du;
-                alch_energy_fp64(A, erx, ery, erz, A.softd[ifirst + a], A.softd[jat], s_qd[warp][a] * qbd, tal, &cdd,
+                alch_energy_fp64(A, erx, ery, erz, A.softd[ifirst + a], A.softd[jat], s_qd[q][a] * qbd, tal, &cdd,
                                  &qdd, &c0, &q0, &du);
                 px0 += c0;
                 px1 += q0;
                 px2 += du;
               } else {
-                pair_energy_fp64(A, erx, ery, erz, A.ljd[s_ti[warp][a] + tb], ljon,
-                                 s_qd[warp][a] * qbd, &cdd, &qdd);
+                pair_energy_fp64(A, erx, ery, erz, A.ljd[s_ti[q][a] + tb], ljon, s_qd[q][a] * qbd, &cdd, &qdd);
                 if (sel) px0 += cdd + qdd;  // seg_ene
               }
               pconf += cdd;
               pcoul += qdd;
             }
             const float fx = qf * rx, fy = qf * ry, fz = qf * rz;
-            fi[a][0] += fx;
-            fi[a][1] += fy;
-            fi[a][2] += fz;
+            fiq[a][0] += to_fix(fx);
+            fiq[a][1] += to_fix(fy);
+            fiq[a][2] += to_fix(fz);
             fbx -= fx;
             fby -= fy;
             fbz -= fz;
@@ -617,10 +663,15 @@ __global__ void __launch_bounds__(WPB * 32, (MG <= 4 && !EN) ? (HI ? ORAC_KPAIR_
             fbx -= pm * sx;
             fby -= pm * sy;
             fbz -= pm * sz;
-            if (t == 0) {
-              svx += sx;
-              svy += sy;
-              svz += sz;
+            if (t == 0) {  // the i atoms' share, by mass fraction
+#pragma unroll
+              for (int a = 0; a < MG; a++) {
+                if (a >= ni) break;
+                const float pmi = s_pm[q][a];
+                fiq[a][0] += to_fix(pmi * sx);
+                fiq[a][1] += to_fix(pmi * sy);
+                fiq[a][2] += to_fix(pmi * sz);
+              }
             }
           }
         }
@@ -631,7 +682,7 @@ __global__ void __launch_bounds__(WPB * 32, (MG <= 4 && !EN) ? (HI ? ORAC_KPAIR_
         }
         if (EN && A.stress) {
           if (act) {
-            const float4 im = s_eimg[warp][e];
+            const float4 im = s_eimg[q][e];
             vimg[0] += fbx * im.x;
             vimg[1] += fbx * im.y;
             vimg[2] += fbx * im.z;
@@ -644,7 +695,7 @@ __global__ void __launch_bounds__(WPB * 32, (MG <= 4 && !EN) ? (HI ? ORAC_KPAIR_
           }
           flush_vimg();
         }
-        const int ne = __popc(__ballot_sync(FULL, act && t == 0));
+        const int ne = __popc(segbits(__ballot_sync(FULL, act && t == 0)));
         sh += L;
         sn -= L;
         qh += ne;
@@ -652,27 +703,28 @@ __global__ void __launch_bounds__(WPB * 32, (MG <= 4 && !EN) ? (HI ? ORAC_KPAIR_
         __syncwarp();
       }
     }
-    if (A.next_on && lane == 0) {
+    if (A.next_on && sl == 0 && gvalid) {
       A.cnt_out[i] = nout;
       nkept += (unsigned)nout;
     }
-    if (A.forces_on && m > 0) {
-      // i atoms: pair forces and their share of the row's S'V vectors, one
-      // atomic per component from lanes 0 .. 3 ni - 1
-      const float tsx = seg_sum<32>(svx), tsy = seg_sum<32>(svy), tsz = seg_sum<32>(svz);
-      float val = 0.f;
+    if (A.forces_on) {
+      // i atoms: the fixed-point sums of the segment's lanes by one
+      // reduce-scatter; the lane holding component c of atom a adds it
+      constexpr int P = 3 * MG <= 16 ? 16 : 32;
+      long long v[P];
 #pragma unroll
       for (int a = 0; a < MG; a++) {
-        if (a >= ni) break;
-        const float pm = s_pm[warp][a];
-        const float sx = seg_sum<32>(fi[a][0]) + pm * tsx;
-        const float sy = seg_sum<32>(fi[a][1]) + pm * tsy;
-        const float sz = seg_sum<32>(fi[a][2]) + pm * tsz;
-        if (lane == 3 * a) val = sx;
-        if (lane == 3 * a + 1) val = sy;
-        if (lane == 3 * a + 2) val = sz;
+        v[3 * a] = fiq[a][0];
+        v[3 * a + 1] = fiq[a][1];
+        v[3 * a + 2] = fiq[a][2];
       }
-      if (lane < 3 * ni) fix_add(A.ffix + (lane % 3) * A.natom + ifirst + lane / 3, val);
+#pragma unroll
+      for (int k = 3 * MG; k < P; k++) v[k] = 0ll;
+      const long long tot_v = reduce_scatter<LPG, P>(v, sl);
+      const int idx = rs_index<LPG, P>(sl);
+      const bool owner = (LPG / P <= 1) || (sl % (LPG / P)) == 0;  // one lane per value
+      if (gvalid && m > 0 && owner && idx < 3 * ni && tot_v != 0)
+        atomicAdd(A.ffix + (idx % 3) * A.natom + ifirst + idx / 3, (unsigned long long)tot_v);
     }
     __syncwarp();
   }
@@ -698,13 +750,13 @@ __global__ void __launch_bounds__(WPB * 32, (MG <= 4 && !EN) ? (HI ? ORAC_KPAIR_
   constexpr int NV = (VAR != VAR_STD && EN) ? 18 : 15;
   double vals[18] = {ec0, ec1, ec2, eq0, eq1, eq2, 0, 0, 0, 0, 0, 0, 0, 0, 0, ex0, ex1, ex2};
 #pragma unroll
-  for (int q = 0; q < NV; q++) {
-    if (q >= 6 && q < 15) {
-      if (lane == 0) s_red[warp][q] = s_vimg[warp][q - 6];
+  for (int c = 0; c < NV; c++) {
+    if (c >= 6 && c < 15) {
+      if (lane == 0) s_red[warp][c] = s_vimg[warp][c - 6];
       continue;
     }
-    const double sred = warp_sumd(vals[q]);
-    if (lane == 0) s_red[warp][q] = sred;
+    const double sred = warp_sumd(vals[c]);
+    if (lane == 0) s_red[warp][c] = sred;
   }
   __syncthreads();
   if (threadIdx.x < NV) {
@@ -804,37 +856,49 @@ int pair_launch(orac_gpu_ctx* ctx, const PairArgs& a, int maxg) {
     return ctx_fail(ctx, ORAC_ERR_PARAM, "charge group of %d atoms exceeds %d", maxg, ORAC_MAXG);
   if (a.variant < VAR_STD || a.variant > VAR_ALCH) return ctx_fail(ctx, ORAC_ERR_PARAM, "variant %d", a.variant);
   // atoms-per-group bound of the instantiation: 3 (waters, and chains cut
-  // in threes), 4, or 8
+  // in threes), 4, or 8; half-warp groups and the occupancy classes only
+  // for the two small bounds
   const int mgk = maxg <= 3 ? 0 : (maxg <= 4 ? 1 : 2);
-  int nb = (a.ngrp + WPB - 1) / WPB;  // a warp per i group
+  const bool half = mgk < 2 && a.lpg == 16;
+  const int gpb = WPB * (half ? 2 : 1);  // groups per block
+  int nb = (a.ngrp + gpb - 1) / gpb;
   if (nb < 1) nb = 1;
   int slot = -1;
   if (int rc = prof_begin(ctx, &slot)) return rc;
   const bool en = a.energy || a.stress;  // the forces-only build keeps no sums
-  const bool hi = a.occ_hi && !en && mgk < 2;
-  switch (((mgk * 3 + a.variant) * 2 + (en ? 1 : 0)) * 2 + (hi ? 1 : 0)) {
-#define ORAC_KP(MGK, MG, VAR, EN, HI)                                   \
-  case ((MGK * 3 + VAR) * 2 + (EN ? 1 : 0)) * 2 + (HI ? 1 : 0):        \
-    orac_launch(k_pair<MG, EN, VAR, HI>, nb, WPB * 32, smem, ctx->stream, a); \
+  // occupancy class of the forces-only build: 0, 1, 2 = 5, 6, 8 blocks per SM
+  const int occ = (en || mgk == 2) ? 0 : (a.minb <= 5 ? 0 : (a.minb <= 7 ? 1 : 2));
+  switch ((((mgk * 3 + a.variant) * 2 + (en ? 1 : 0)) * 2 + (half ? 1 : 0)) * 3 + occ) {
+#define ORAC_KP(MGK, MG, VAR, EN, LPG, OCC, MINB)                                               \
+  case (((MGK * 3 + VAR) * 2 + (EN ? 1 : 0)) * 2 + (LPG == 16 ? 1 : 0)) * 3 + OCC:             \
+    orac_launch(k_pair<MG, EN, VAR, LPG, MINB>, nb, WPB * 32, smem, ctx->stream, a);            \
     break;
-#define ORAC_KP_V(MGK, MG, VAR)        \
-  ORAC_KP(MGK, MG, VAR, false, false) \
-  ORAC_KP(MGK, MG, VAR, false, true)  \
-  ORAC_KP(MGK, MG, VAR, true, false)
+#define ORAC_KP_L(MGK, MG, VAR, LPG)       \
+  ORAC_KP(MGK, MG, VAR, false, LPG, 0, 5)  \
+  ORAC_KP(MGK, MG, VAR, false, LPG, 1, 6)  \
+  ORAC_KP(MGK, MG, VAR, false, LPG, 2, 8)  \
+  ORAC_KP(MGK, MG, VAR, true, LPG, 0, 1)
+#define ORAC_KP_V(MGK, MG, VAR) \
+  ORAC_KP_L(MGK, MG, VAR, 32)   \
+  ORAC_KP_L(MGK, MG, VAR, 16)
     ORAC_KP_V(0, 3, VAR_STD)
     ORAC_KP_V(0, 3, VAR_REM)
     ORAC_KP_V(0, 3, VAR_ALCH)
     ORAC_KP_V(1, 4, VAR_STD)
     ORAC_KP_V(1, 4, VAR_REM)
     ORAC_KP_V(1, 4, VAR_ALCH)
-    ORAC_KP(2, 8, VAR_STD, false, false)
-    ORAC_KP(2, 8, VAR_STD, true, false)
-    ORAC_KP(2, 8, VAR_REM, false, false)
-    ORAC_KP(2, 8, VAR_REM, true, false)
-    ORAC_KP(2, 8, VAR_ALCH, false, false)
-    ORAC_KP(2, 8, VAR_ALCH, true, false)
+    ORAC_KP(2, 8, VAR_STD, false, 32, 0, 1)
+    ORAC_KP(2, 8, VAR_STD, true, 32, 0, 1)
+    ORAC_KP(2, 8, VAR_REM, false, 32, 0, 1)
+    ORAC_KP(2, 8, VAR_REM, true, 32, 0, 1)
+    ORAC_KP(2, 8, VAR_ALCH, false, 32, 0, 1)
+    ORAC_KP(2, 8, VAR_ALCH, true, 32, 0, 1)
 #undef ORAC_KP_V
+#undef ORAC_KP_L
 #undef ORAC_KP
+    default:
+      return ctx_fail(ctx, ORAC_ERR_PARAM, "no pair-kernel build for %d atoms per group, lpg %d, %d blocks per SM",
+                      maxg, a.lpg, a.minb);
   }
   CKL();
   return prof_end(ctx, slot);

@@ -970,6 +970,44 @@ __global__ void k_rattle_big(const ConsArgs A) {
   atomicOr(A.flag, 1);
 }
 
+// The energy record of an energy step (ORAC_MD_REC doubles, the layout
+// orac_gpu_md_run returns) into the context's ring: [0] record number,
+// [1] kinetic, [2..7] M, L, H LJ and Coulomb, [8] SPME, [9] the constant
+// (self energy), [10] total, [11] status flags, [12] bonded, [13] 1-4 and
+// intra-group pairs, [14] erf corrections, [15] dU/dlambda.
+__global__ void k_record(const double* __restrict__ e, const int* __restrict__ flag, double econst, double self_dudl,
+                         int alch, double* __restrict__ ring, int cap, unsigned long long* __restrict__ n) {
+  pdl_enter();
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const unsigned long long k = *n;
+  double* r = ring + (size_t)ORAC_MD_REC * (size_t)(k % (unsigned long long)cap);
+  r[0] = (double)(k + 1);
+  r[1] = e[40];
+  r[2] = e[4] + e[0] + e[6];
+  r[3] = e[5] + e[1] + e[7];
+  r[4] = e[12] + e[8] + e[14];
+  r[5] = e[13] + e[9] + e[15];
+  r[6] = e[20] + e[16] + e[22];
+  r[7] = e[21] + e[17] + e[23];
+  r[8] = 0.5 * e[24];
+  r[9] = econst;
+  double b = 0.0, p = 0.0, c = 0.0, d = 0.0;
+  for (int q = 41; q < 49; q++) b += e[q];  // bonded (E_BOND..E_14)
+  for (int q = 49; q < 57; q++) p += e[q];  // 1-4 and intra-group (E_14..E_ERF)
+  for (int q = 57; q < 73; q++) c += e[q];  // erf corrections (E_ERF..E_DUDL)
+  if (alch) {
+    for (int q = 73; q < 78; q++) d += e[q];
+    d += self_dudl;
+  }
+  r[12] = b;
+  r[13] = p;
+  r[14] = c;
+  r[15] = d;
+  r[10] = r[1] + r[2] + r[3] + r[4] + r[5] + r[6] + r[7] + r[8] + r[9] + r[12] + r[13] + r[14];
+  r[11] = (double)*flag;
+  *n = k + 1;
+}
+
 __global__ void k_ekin(int N, const double* __restrict__ v, const double* __restrict__ invm, double* __restrict__ out) {
   pdl_enter();
   __shared__ double s[8];
@@ -1032,15 +1070,19 @@ struct MdState {
   char rshk = 'l';
   long long step = 0;
   double econst = 0;
-  cudaGraph_t graph = nullptr;
+  // captured step graphs by kind: bit 0 list update, bit 1 energy record
+  cudaGraph_t graph[4] = {nullptr, nullptr, nullptr, nullptr};
+  cudaGraphExec_t gexec[4] = {nullptr, nullptr, nullptr, nullptr};
   unsigned graphs_gen = 0;  // ctx->param_gen when the graphs were captured
-  cudaGraphExec_t gexec = nullptr;
-  cudaGraph_t graph_u = nullptr;  // step with list update
-  cudaGraphExec_t gexec_u = nullptr;
   bool graphs_shared = false;  // ctx->shared_device when the graphs were captured
   bool use_graph = true;
-  int pslot[2][2] = {{0, 0}, {0, 0}};  // profiling event slots of each graph
-  int64_t kpg[2] = {0, 0};             // kernels per captured graph
+  int pslot[4][2] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};  // profiling event slots of each graph
+  int64_t kpg[4] = {0, 0, 0, 0};                       // kernels per captured graph
+  // energy records of the energy steps (MD_REC doubles each, k_record): a
+  // ring of rec_cap records on the device and the count written so far
+  double* rec = nullptr;
+  unsigned long long* rec_n = nullptr;
+  int rec_cap = 0;
   int last_kind = -1;                  // graph of the last queued step
   // second stream of the step: work that depends only on the drifted
   // positions and adds into its own level accumulators (intramolecular
@@ -1062,10 +1104,10 @@ static MdState* md_of(orac_gpu_ctx* ctx) {
 void md_destroy(orac_gpu_ctx* ctx) {
   MdState* S = ctx->md;
   if (!S) return;
-  if (S->gexec) cudaGraphExecDestroy(S->gexec);
-  if (S->graph) cudaGraphDestroy(S->graph);
-  if (S->gexec_u) cudaGraphExecDestroy(S->gexec_u);
-  if (S->graph_u) cudaGraphDestroy(S->graph_u);
+  for (int k = 0; k < 4; k++) {
+    if (S->gexec[k]) cudaGraphExecDestroy(S->gexec[k]);
+    if (S->graph[k]) cudaGraphDestroy(S->graph[k]);
+  }
   if (S->h_flag) cudaFreeHost(S->h_flag);
   if (S->ev_fork) cudaEventDestroy(S->ev_fork);
   if (S->ev_join) cudaEventDestroy(S->ev_join);
@@ -1074,7 +1116,7 @@ void md_destroy(orac_gpu_ctx* ctx) {
                   S->ffix[4],
                   S->invm,      S->pm,       S->sm,          S->smg,       S->cloc,    S->cdss,    S->free_atoms,
                   S->free_groups, S->bstart, S->bcab,        S->bdss,      S->e,       S->flag,
-                  S->drift_groups, S->drift_atoms, S->sm_atoms};
+                  S->drift_groups, S->drift_atoms, S->sm_atoms, S->rec, S->rec_n};
   for (void* p : ptrs)
     if (p) dev_free(ctx, p);
   delete S;
@@ -1151,6 +1193,9 @@ static ConsArgs big_args(orac_gpu_ctx* ctx, MdState& S, double dt, double tol) {
 }
 
 enum { E_BOND = 41, E_14 = 49, E_GRP = 53, E_ERF = 57, E_DUDL = 73, E_N = 80 };
+
+// energy records kept on the device per context (the newest MD_REC_CAP)
+constexpr int MD_REC_CAP = 2048;
 
 // kick of the level accumulators with velocity factors c[l] (0: skip) + RATTLE
 static void kick_fill(MolArgs& A, MdState& S, const double* c) {
@@ -1432,6 +1477,9 @@ static int md_step(orac_gpu_ctx* ctx, MdState& S, bool update, bool energy) {
     CK(cudaMemsetAsync(S.e + 40, 0, sizeof(double), ctx->stream));
     orac_launch(k_ekin, 64, 256, 0, ctx->stream, ctx->N, S.v, S.invm, S.e + 40);
     CKL();
+    orac_launch(k_record, 1, 32, 0, ctx->stream, S.e, S.flag, S.econst, ctx->self_dudl,
+                (ctx->variant == VAR_ALCH && ctx->d_dq) ? 1 : 0, S.rec, S.rec_cap, S.rec_n);
+    CKL();
   }
   return ORAC_OK;
 }
@@ -1474,7 +1522,8 @@ int orac_gpu_md_setup(orac_gpu_ctx* ctx, const double* x, const double* y, const
   if (dev_alloc(ctx, &S.x, 3 * (size_t)N) || dev_alloc(ctx, &S.v, 3 * (size_t)N) ||
       dev_alloc(ctx, &S.xo, 3 * (size_t)N) || dev_alloc(ctx, &S.ffix[0], 3 * (size_t)N) ||
       dev_alloc(ctx, &S.ffix[1], 3 * (size_t)N) || dev_alloc(ctx, &S.ffix[2], 3 * (size_t)N) ||
-      dev_alloc(ctx, &S.invm, N) || dev_alloc(ctx, &S.pm, N) || dev_alloc(ctx, &S.e, 96) ||
+      dev_alloc(ctx, &S.invm, N) || dev_alloc(ctx, &S.pm, N) || dev_alloc(ctx, &S.e, 96) || dev_alloc(ctx, &S.rec, (size_t)ORAC_MD_REC * MD_REC_CAP) ||
+      dev_alloc(ctx, &S.rec_n, 1) ||
       dev_alloc(ctx, &S.flag, 4))
     return ORAC_ERR_CUDA;
   {
@@ -1486,6 +1535,8 @@ int orac_gpu_md_setup(orac_gpu_ctx* ctx, const double* x, const double* y, const
         (S.has_n0 && dev_alloc(ctx, &S.ffix[LN0], 3 * (size_t)N)))
       return ORAC_ERR_CUDA;
     CK(cudaMemset(S.e, 0, sizeof(double) * 96));
+    CK(cudaMemset(S.rec_n, 0, sizeof(unsigned long long)));
+    S.rec_cap = MD_REC_CAP;
   }
   if (int rc = bonded_set_constraints(ctx, cnst, ncnst)) return rc;
   const double* src[2][3] = {{x, y, z}, {vx, vy, vz}};
@@ -1816,6 +1867,26 @@ int orac_gpu_md_set_state(orac_gpu_ctx* ctx, const double* x, const double* y, c
   return copy_runs(ctx, dst, src, cudaMemcpyHostToDevice);
 }
 
+int orac_gpu_md_records(orac_gpu_ctx* ctx, int max, double* out, int64_t* n_total, int reset) {
+  if (!ctx || max < 0 || (max > 0 && !out)) return ORAC_ERR_PARAM;
+  MdState& S = *md_of(ctx);
+  if (!S.ready) return ctx_fail(ctx, ORAC_ERR_STATE, "md_setup not called");
+  CK(cudaSetDevice(ctx->device));
+  CK(cudaStreamSynchronize(ctx->stream));
+  unsigned long long n = 0;
+  CK(cudaMemcpy(&n, S.rec_n, sizeof(n), cudaMemcpyDeviceToHost));
+  if (n_total) *n_total = (int64_t)n;
+  const unsigned long long kept = n < (unsigned long long)S.rec_cap ? n : (unsigned long long)S.rec_cap;
+  const unsigned long long take = kept < (unsigned long long)max ? kept : (unsigned long long)max;
+  for (unsigned long long k = 0; k < take; k++) {  // oldest of the newest `take` first
+    const unsigned long long idx = (n - take + k) % (unsigned long long)S.rec_cap;
+    CK(cudaMemcpy(out + ORAC_MD_REC * k, S.rec + ORAC_MD_REC * idx, sizeof(double) * ORAC_MD_REC,
+                  cudaMemcpyDeviceToHost));
+  }
+  if (reset) CK(cudaMemset(S.rec_n, 0, sizeof(unsigned long long)));
+  return ORAC_OK;
+}
+
 int orac_gpu_md_set_graphs(orac_gpu_ctx* ctx, int on) {
   if (!ctx) return ORAC_ERR_PARAM;
   md_of(ctx)->use_graph = on != 0;
@@ -1826,25 +1897,25 @@ int orac_gpu_md_set_graphs(orac_gpu_ctx* ctx, int on) {
 
 // capture (once) the step graph of one kind: 0 plain step, 1 step with list update
 static int md_capture(orac_gpu_ctx* ctx, MdState& S, int kind) {
-  if ((S.gexec || S.gexec_u) && (S.graphs_shared != ctx->shared_device || S.graphs_gen != ctx->param_gen)) {
+  bool any = false;
+  for (int k = 0; k < 4; k++) any = any || S.gexec[k];
+  if (any && (S.graphs_shared != ctx->shared_device || S.graphs_gen != ctx->param_gen)) {
     // captured for the other device-sharing mode, or before a parameter
     // changed (a new lambda, REM factor, box, ...): capture again
-    if (S.gexec) cudaGraphExecDestroy(S.gexec);
-    if (S.graph) cudaGraphDestroy(S.graph);
-    if (S.gexec_u) cudaGraphExecDestroy(S.gexec_u);
-    if (S.graph_u) cudaGraphDestroy(S.graph_u);
-    S.gexec = S.gexec_u = nullptr;
-    S.graph = S.graph_u = nullptr;
+    for (int k = 0; k < 4; k++) {
+      if (S.gexec[k]) cudaGraphExecDestroy(S.gexec[k]);
+      if (S.graph[k]) cudaGraphDestroy(S.graph[k]);
+      S.gexec[k] = nullptr;
+      S.graph[k] = nullptr;
+    }
   }
   S.graphs_shared = ctx->shared_device;
   S.graphs_gen = ctx->param_gen;
-  cudaGraphExec_t* ge = kind ? &S.gexec_u : &S.gexec;
-  cudaGraph_t* gg = kind ? &S.graph_u : &S.graph;
-  if (*ge) return ORAC_OK;
+  if (S.gexec[kind]) return ORAC_OK;
   const int64_t l0 = ctx->launches;
   S.pslot[kind][0] = ctx->prof_next;
   CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
-  const int rc = md_step(ctx, S, kind == 1, false);
+  const int rc = md_step(ctx, S, (kind & 1) != 0, (kind & 2) != 0);
   cudaGraph_t g = nullptr;
   const cudaError_t ce = cudaStreamEndCapture(ctx->stream, &g);
   if (rc) {
@@ -1852,8 +1923,8 @@ static int md_capture(orac_gpu_ctx* ctx, MdState& S, int kind) {
     return rc;
   }
   CK(ce);
-  *gg = g;
-  CK(cudaGraphInstantiate(ge, g, 0));
+  S.graph[kind] = g;
+  CK(cudaGraphInstantiate(&S.gexec[kind], g, 0));
   S.pslot[kind][1] = ctx->prof_next;
   S.kpg[kind] = ctx->launches - l0;
   ctx->launches = l0;
@@ -1864,15 +1935,16 @@ static int md_capture(orac_gpu_ctx* ctx, MdState& S, int kind) {
 int md_step_graph(orac_gpu_ctx* ctx, int kind, cudaGraph_t* out) {
   MdState& S = *md_of(ctx);
   if (!S.ready) return ctx_fail(ctx, ORAC_ERR_STATE, "md_setup not called");
+  if (kind < 0 || kind > 3) return ctx_fail(ctx, ORAC_ERR_PARAM, "step graph kind %d", kind);
   if (int rc = md_capture(ctx, S, kind)) return rc;
-  *out = kind ? S.graph_u : S.graph;
+  *out = S.graph[kind];
   return ORAC_OK;
 }
 
-int md_advance(orac_gpu_ctx* ctx, int nsteps) {
+int md_advance(orac_gpu_ctx* ctx, int nsteps, int kind) {
   MdState& S = *md_of(ctx);
   S.step += nsteps;
-  ctx->launches += S.kpg[0] * nsteps;
+  ctx->launches += S.kpg[kind & 3] * nsteps;
   return ORAC_OK;
 }
 
@@ -1899,9 +1971,8 @@ static int md_run_impl(orac_gpu_ctx* ctx, int nsteps, int energy_every, double* 
     const bool energy = energy_every > 0 && ((k + 1) % energy_every == 0);
     if (S.use_graph && !energy) {
       const int kind = update ? 1 : 0;
-      cudaGraphExec_t* ge = update ? &S.gexec_u : &S.gexec;
       if (int rc = md_capture(ctx, S, kind)) return rc;
-      CK(cudaGraphLaunch(*ge, ctx->stream));
+      CK(cudaGraphLaunch(S.gexec[kind], ctx->stream));
       ctx->launches += S.kpg[kind];
       S.last_kind = kind;
       if (ctx->prof && !async) {

@@ -298,6 +298,35 @@ class Engine:
         check(self.ctx, self.lib.orac_gpu_md_run(self.ctx, nsteps, energy_every, rec), "md_run")
         return rec[:nrec * R].reshape(-1, R)
 
+    def set_pair_tuning(self, lpg_m=0, lpg_lh=0, minb=0):
+        """Launch configuration of the real-space kernel (0: the mode's default)."""
+        check(self.ctx, self.lib.orac_gpu_set_pair_tuning(self.ctx, lpg_m, lpg_lh, minb), "set_pair_tuning")
+
+    def pair_tuning(self):
+        out = (C.c_int * 3)()
+        check(self.ctx, self.lib.orac_gpu_get_pair_tuning(self.ctx, out), "get_pair_tuning")
+        return tuple(out)
+
+    def tune(self, trial=6, cache=None, force=False):
+        """Autotune the real-space kernel on this context's MD steps
+        (orac_gpu_tune): ((lpg_m, lpg_lh, minb), ms per step)."""
+        out = (C.c_int * 3)()
+        ms = C.c_double()
+        path = cache.encode() if cache else None
+        check(self.ctx, self.lib.orac_gpu_tune(self.ctx, trial, path, int(force), out, C.byref(ms)), "tune")
+        return tuple(out), ms.value
+
+    def md_records(self, max_records=2048, reset=False):
+        """The energy records kept on the device (orac_gpu_md_records): the
+        newest up to max_records, oldest first, and the number written."""
+        R = self.MD_REC
+        out = np.zeros(max(1, max_records) * R)
+        n = C.c_int64()
+        check(self.ctx, self.lib.orac_gpu_md_records(self.ctx, max_records, out.ctypes.data, C.byref(n),
+                                                     int(reset)), "md_records")
+        k = min(n.value, max_records, 2048)
+        return out[:k * R].reshape(-1, R), n.value
+
     def md_state(self):
         n = self.s.ntap
         a = [np.zeros(n) for _ in range(6)]
@@ -343,13 +372,27 @@ class Batch:
         if rc != L.ORAC_OK:
             raise L.OracGpuError(f"{what}: {L.ERRORS.get(rc, rc)} {self.lib.orac_gpu_batch_last_error(self.h).decode()}")
 
-    def run(self, nsteps, sync=True):
-        self._check(self.lib.orac_gpu_batch_run(self.h, nsteps), "batch_run")
+    def run(self, nsteps, sync=True, energy_every=0):
+        """nsteps H steps of every system; with energy_every > 0 every
+        energy_every-th step writes each system's energy record."""
+        if energy_every:
+            self._check(self.lib.orac_gpu_batch_run_energy(self.h, nsteps, energy_every), "batch_run_energy")
+        else:
+            self._check(self.lib.orac_gpu_batch_run(self.h, nsteps), "batch_run")
         if sync:
             self.sync()
 
     def sync(self):
         self._check(self.lib.orac_gpu_batch_sync(self.h), "batch_sync")
+
+    def tune(self, trial=6, cache=None, force=False):
+        """Autotune the real-space kernel on the batched steps
+        (orac_gpu_batch_tune): ((lpg_m, lpg_lh, minb), ms per batched step)."""
+        out = (C.c_int * 3)()
+        ms = C.c_double()
+        path = cache.encode() if cache else None
+        self._check(self.lib.orac_gpu_batch_tune(self.h, trial, path, int(force), out, C.byref(ms)), "batch_tune")
+        return tuple(out), ms.value
 
     def stream(self):
         return self.lib.orac_gpu_batch_stream(self.h)

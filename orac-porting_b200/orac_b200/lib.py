@@ -87,6 +87,8 @@ def load():
         "orac_gpu_get_stream": (_P, [_P]),
         "orac_gpu_batch_create": (i, [C.POINTER(_P), i, C.POINTER(_P)]),
         "orac_gpu_batch_run": (i, [_P, i]),
+        "orac_gpu_batch_run_energy": (i, [_P, i, i]),
+        "orac_gpu_md_records": (i, [_P, i, _P, C.POINTER(i64), i]),
         "orac_gpu_batch_sync": (i, [_P]),
         "orac_gpu_batch_destroy": (i, [_P]),
         "orac_gpu_batch_last_error": (C.c_char_p, [_P]),
@@ -98,6 +100,10 @@ def load():
         "orac_gpu_stats": (i, [_P, C.POINTER(i64), C.POINTER(i64)]),
         "orac_gpu_footprint": (i, [_P, C.POINTER(i64)]),
         "orac_gpu_fp32_rate": (i, [i, C.POINTER(d), C.POINTER(d)]),
+        "orac_gpu_set_pair_tuning": (i, [_P, i, i, i]),
+        "orac_gpu_get_pair_tuning": (i, [_P, C.POINTER(i)]),
+        "orac_gpu_tune": (i, [_P, i, C.c_char_p, i, C.POINTER(i), C.POINTER(d)]),
+        "orac_gpu_batch_tune": (i, [_P, i, C.c_char_p, i, C.POINTER(i), C.POINTER(d)]),
         "orac_gpu_server_now": (d, []),
         "orac_gpu_server_create": (i, [i, i64, i, i, C.POINTER(_P)]),
         "orac_gpu_server_destroy": (i, [_P]),

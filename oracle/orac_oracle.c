@@ -1740,3 +1740,176 @@ void orc_fnbgrp(const int* ss_index, const double* xp0, const double* yp0,
   ue[2] = ucoul[0];
   ue[3] = ucoul[1];
 }
+
+/* The per-atom lambdas of ORAC's alchemical species (src/mtsmd.f:746-754,
+ * src/initialize_lambda.f:30-52): added atoms carry ladd, removed atoms
+ * -lrm, all others 0; the coupling of an atom is 1 - |lambda|. */
+void orc_alch_atom_lambdas(int nato, const int* ss_alchemy, double ladd, double lrm, double* lam) {
+  for (int i = 0; i < nato; i++) lam[i] = ss_alchemy[i] == 2 ? ladd : (ss_alchemy[i] == -2 ? -lrm : 0.0);
+}
+
+/* listqq of src/initialize_lambda.f:62-139: every pair of alchemical atoms
+ * (added or removed) that is no 1-2 (bond or constraint), 1-3 or 1-4 pair,
+ * as (ia, ib, facQ) 1-based, facQ = 1 for atoms of one species, 0 for an
+ * added-removed pair.  The excluded pairs come as one 1-based list of
+ * nexcl pairs.  Returns the number of entries written (at most cap). */
+int orc_alch_listqq(int nato, const int* ss_alchemy, const int* excl, int nexcl, int* out3, int cap) {
+  int nat = 0;
+  for (int i = 0; i < nato; i++) nat += (ss_alchemy[i] == 2 || ss_alchemy[i] == -2);
+  int* iat = (int*)malloc(sizeof(int) * (nat > 0 ? nat : 1));
+  int k = 0;
+  /* ORAC's order: added atoms first, then removed ones */
+  for (int i = 0; i < nato; i++)
+    if (ss_alchemy[i] == 2) iat[k++] = i + 1;
+  for (int i = 0; i < nato; i++)
+    if (ss_alchemy[i] == -2) iat[k++] = i + 1;
+  int n = 0;
+  for (int a = 0; a < nat - 1; a++)
+    for (int b = a + 1; b < nat; b++) {
+      const int ia = iat[a], ib = iat[b];
+      int skip = 0;
+      for (int l = 0; l < nexcl && !skip; l++)
+        skip = (excl[2 * l] == ia && excl[2 * l + 1] == ib) || (excl[2 * l] == ib && excl[2 * l + 1] == ia);
+      if (skip) continue;
+      if (n < cap) {
+        out3[3 * n] = ia;
+        out3[3 * n + 1] = ib;
+        out3[3 * n + 2] = ss_alchemy[ia - 1] == ss_alchemy[ib - 1] ? 1 : 0;
+      }
+      n++;
+    }
+  free(iat);
+  return n;
+}
+
+/* ferrf_alchemy_add, src/ferrf_alchemy_add.f (the branch without the erf
+ * tables, ORAC's default): the reciprocal sum of the scaled charges
+ * (1 - |lq|) Q gives every listqq pair (1-|lq_a|)(1-|lq_b|) Q_a Q_b erf/r;
+ * this subtracts factl Q_a Q_b erf(alpha r)/r with factl = that product -
+ * facQ, so that atoms of one species keep their full Coulomb (facQ 1) and
+ * added and removed atoms do not see each other (facQ 0).  With intramol
+ * the pairs of one species are skipped.  fs receives the energies (solute,
+ * solvent), *dwrk the work U(lambda) - U(lambda0). */
+void orc_ferrf_alchemy_add(const int* ss_index, double alphal, const double* charge, const double* lambdaq,
+                           const double* lambdaq0, const double* x0, const double* y0, const double* z0,
+                           const int* list3, int nlist, int intramol, double* fs, double* dwrk, double* fpx,
+                           double* fpy, double* fpz) {
+  double twrtpi = 2.0 / sqrt(PI_D);
+  double fsr[2] = {0, 0}, en0 = 0.0;
+  for (int i = 0; i < nlist; i++) {
+    int ia = list3[3 * i] - 1, ib = list3[3 * i + 1] - 1;
+    double facq = (double)list3[3 * i + 2];
+    if (intramol && list3[3 * i + 2] != 0) continue;
+    int type = ss_index[ia];
+    double factl = (1.0 - fabs(lambdaq[ia])) * (1.0 - fabs(lambdaq[ib])) - facq;
+    double factl0 = (1.0 - fabs(lambdaq0[ia])) * (1.0 - fabs(lambdaq0[ib])) - facq;
+    double furpar = factl * charge[ia] * charge[ib];
+    double furpar0 = factl0 * charge[ia] * charge[ib];
+    double xab = x0[ia] - x0[ib], yab = y0[ia] - y0[ib], zab = z0[ia] - z0[ib];
+    double rsq = xab * xab + yab * yab + zab * zab;
+    double rsp = sqrt(rsq);
+    double alphar = alphal * rsp;
+    double qt = 1.0 / (1.0 + AS_QP * alphar);
+    double expcst = exp(-alphar * alphar);
+    double erfcst = ((((AS_A5 * qt + AS_A4) * qt + AS_A3) * qt + AS_A2) * qt + AS_A1) * qt * expcst;
+    double erfst = 1.0 - erfcst;
+    double qforce = -furpar * (erfst - twrtpi * alphar * expcst) / (rsp * rsq);
+    fsr[type - 1] -= furpar * erfst / rsp;
+    en0 -= furpar0 * erfst / rsp;
+    fpx[ia] += qforce * xab;
+    fpy[ia] += qforce * yab;
+    fpz[ia] += qforce * zab;
+    fpx[ib] -= qforce * xab;
+    fpy[ib] -= qforce * yab;
+    fpz[ib] -= qforce * zab;
+  }
+  fs[0] = fsr[0];
+  fs[1] = fsr[1];
+  *dwrk = fsr[0] + fsr[1] - en0;
+}
+
+/* the coupling factors of one 1-4 pair in fnb14_alchemy (src/fnb14_alchemy.f:
+ * 149-177 for LJ, 252-289 for the charges): an alchemical atom with
+ * lambda 0 counts as normal; one alchemical atom: 1 - |lambda|; two of one
+ * lambda: full (and, for the charges, the erf term that restores the full
+ * Coulomb the scaled reciprocal sum lacks, 1 - the product of the
+ * couplings); two of different lambdas: none (and the reciprocal sum's
+ * product subtracted) */
+static void alch14_factors(double li, double lj, int charges, double* f, double* f2) {
+  *f2 = 0.0;
+  if (li == 0.0 && lj != 0.0) {
+    *f = 1.0 - fabs(lj);
+  } else if (li != 0.0 && lj == 0.0) {
+    *f = 1.0 - fabs(li);
+  } else if (li == 0.0 && lj == 0.0) {
+    *f = 1.0;
+  } else if (li != lj) {
+    *f = 0.0;
+    if (charges) *f2 = -(1.0 - fabs(li)) * (1.0 - fabs(lj));
+  } else {
+    *f = 1.0;
+    if (charges) *f2 = 1.0 - (1.0 - fabs(li)) * (1.0 - fabs(lj));
+  }
+}
+
+/* fnb14_alchemy, src/fnb14_alchemy.f:225-341 (the Ewald branch): 1-4 pairs
+ * with LJ scaled by alch_fact and Coulomb fudge Q_i Q_j [alch_factq erfc/r
+ * + alch_factq2 erf/r], at lambda and lambda0 for the work.  ORAC scales
+ * only the repulsive term of the LJ force by alch_fact (its energy by
+ * alch_fact whole); restated as written.  ue: LJ slt, slv, Coulomb slt,
+ * slv; *dwrk: U(lambda) - U(lambda0). */
+void orc_fnb14_alchemy(const int* ss_index, const double* xp0, const double* yp0, const double* zp0,
+                       const double* charge, const double* ecc12, const double* ecc6, double alphal,
+                       const int* int14, int int14p, const int* type14, double fudge, double lj_fudge,
+                       const double* lambda, const double* lambdaq, const double* lambda0, const double* lambdaq0,
+                       double* fpx, double* fpy, double* fpz, double* ue, double* dwrk) {
+  double uconf[2] = {0, 0}, ucoul[2] = {0, 0}, uconf0[2] = {0, 0}, ucoul0[2] = {0, 0};
+  double twrtpi = 2.0 / sqrt(PI_D);
+  for (int i = 0; i < int14p; i++) {
+    int i1 = int14[2 * i] - 1, i2 = int14[2 * i + 1] - 1;
+    double af, af0, aq, aq0, aq2, aq20, dum;
+    alch14_factors(lambda[i1], lambda[i2], 0, &af, &dum);
+    alch14_factors(lambda0[i1], lambda0[i2], 0, &af0, &dum);
+    alch14_factors(lambdaq[i1], lambdaq[i2], 1, &aq, &aq2);
+    alch14_factors(lambdaq0[i1], lambdaq0[i2], 1, &aq0, &aq20);
+    int type = ss_index[i1];
+    int lij = type14[i] - 1;
+    double xa = xp0[i1] - xp0[i2], ya = yp0[i1] - yp0[i2], za = zp0[i1] - zp0[i2];
+    double rsq = xa * xa + ya * ya + za * za;
+    double rsp = sqrt(rsq);
+    double rsqi = 1.0 / rsq;
+    double rspqi = rsqi / rsp;
+    double r6 = rsqi * rsqi * rsqi;
+    double r12 = r6 * r6;
+    double ssvir = af * 12.0 * ecc12[lij] * r12 - 6.0 * ecc6[lij] * r6;
+    double qforce = lj_fudge * ssvir * rsqi;
+    double aux = lj_fudge * (ecc12[lij] * r12 - ecc6[lij] * r6);
+    uconf[type - 1] += af * aux;
+    uconf0[type - 1] += af0 * aux;
+    double alphar = alphal * rsp;
+    double qt = 1.0 / (1.0 + AS_QP * alphar);
+    double expcst = exp(-alphar * alphar);
+    double erfcst = ((((AS_A5 * qt + AS_A4) * qt + AS_A3) * qt + AS_A2) * qt + AS_A1) * qt * expcst;
+    double qq = fudge * charge[i1] * charge[i2];
+    double furpar = aq * qq, furpar0 = aq0 * qq;
+    double erff = 1.0 - erfcst;
+    double furpar2 = aq2 * qq, furpar20 = aq20 * qq;
+    ucoul[type - 1] += furpar * erfcst / rsp + furpar2 * erff / rsp;
+    ucoul0[type - 1] += furpar0 * erfcst / rsp + furpar20 * erff / rsp;
+    double a1 = (erfcst + twrtpi * alphar * expcst) * rspqi;
+    double a2 = (erff - twrtpi * alphar * expcst) * rspqi;
+    qforce += furpar * a1 + furpar2 * a2;
+    fpx[i1] += qforce * xa;
+    fpy[i1] += qforce * ya;
+    fpz[i1] += qforce * za;
+    fpx[i2] -= qforce * xa;
+    fpy[i2] -= qforce * ya;
+    fpz[i2] -= qforce * za;
+  }
+  ue[0] = uconf[0];
+  ue[1] = uconf[1];
+  ue[2] = ucoul[0];
+  ue[3] = ucoul[1];
+  *dwrk = 0.0;
+  for (int k = 0; k < 2; k++) *dwrk += uconf[k] + ucoul[k] - (uconf0[k] + ucoul0[k]);
+}

@@ -244,6 +244,22 @@ void orc_md_set_intra(void* h, int nb, const int* lbnd, const double* r0,
                       double fudge, int ningrp, const int* ingrp, int n13,
                       const int* int13, int n1respa, int n0respa);
 
+/* ORAC's intra-alchemical corrections (orac_oracle.c): per-atom lambdas of
+ * the species, the listqq of src/initialize_lambda.f, ferrf_alchemy_add
+ * (src/ferrf_alchemy_add.f) and fnb14_alchemy's Ewald branch
+ * (src/fnb14_alchemy.f). */
+void orc_alch_atom_lambdas(int nato, const int* ss_alchemy, double ladd, double lrm, double* lam);
+int orc_alch_listqq(int nato, const int* ss_alchemy, const int* excl, int nexcl, int* out3, int cap);
+void orc_ferrf_alchemy_add(const int* ss_index, double alphal, const double* charge, const double* lambdaq,
+                           const double* lambdaq0, const double* x0, const double* y0, const double* z0,
+                           const int* list3, int nlist, int intramol, double* fs, double* dwrk, double* fpx,
+                           double* fpy, double* fpz);
+void orc_fnb14_alchemy(const int* ss_index, const double* xp0, const double* yp0, const double* zp0,
+                       const double* charge, const double* ecc12, const double* ecc6, double alphal,
+                       const int* int14, int int14p, const int* type14, double fudge, double lj_fudge,
+                       const double* lambda, const double* lambdaq, const double* lambda0, const double* lambdaq0,
+                       double* fpx, double* fpy, double* fpz, double* ue, double* dwrk);
+
 #ifdef __cplusplus
 }
 #endif

@@ -117,3 +117,37 @@ def test_md_flexible_chain_energy_conservation():
     etot, ekin = rec[:, 10], rec[:, 1]
     assert np.isfinite(etot).all()
     assert (etot.max() - etot.min()) < 5e-3 * ekin.mean(), (etot.min(), etot.max(), ekin.mean())
+
+
+def _drift(rec):
+    """Total-energy drift (kJ/mol per ps, least squares) and the RMS of the
+    residual about that line, of energy records of 4-fs steps."""
+    from orac_b200 import units
+
+    t = rec[:, 0] * 4.0e-3
+    e = rec[:, 10] * units.KJMOL
+    p = np.polyfit(t, e, 1)
+    return float(p[0]), float(np.std(e - np.polyval(p, t)))
+
+
+def test_energy_conservation_over_1000_steps_matches_the_oracle():
+    """1,000 outer steps (4 ps) of the liquid box from its seeded start, NVE:
+    the GPU's total-energy drift and fluctuation against the FP64 oracle's
+    over the same run (tests/golden/liquid_drift_oracle.npz, made by
+    tests/golden/make_drift.py).  The trajectories separate after a few
+    hundred steps, so the two are compared as statistics: drift within
+    3 kJ/mol/ps of the oracle's (the total is about 4.3e4 kJ/mol), residual
+    fluctuation within a factor 2."""
+    import os
+
+    ref = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "liquid_drift_oracle.npz"))
+    s = systems.config1_liquid()
+    g = Engine(s.copy())
+    g.md_setup(SCHED["dt_h"], SCHED["lrespa"], SCHED["mrespa"], SCHED["nupdte"], SCHED["rshk"], econst=econst(s))
+    rec = g.md_run(int(ref["nsteps"]), energy_every=int(ref["every"]))
+    g.close()
+    assert np.all(rec[:, 11] == 0)
+    d_g, f_g = _drift(rec)
+    d_o, f_o = _drift(ref["rec"])
+    assert abs(d_g - d_o) <= 3.0, (d_g, d_o)
+    assert 0.5 * f_o <= f_g <= 2.0 * f_o, (f_g, f_o)
