@@ -73,6 +73,7 @@ def f0_system():
 # intramolecular 0.75 / 0.375 fs, list update every 6 steps
 F0_WORKLOAD = dict(build=f0_system, dt_h=15.0, lrespa=5, mrespa=2, n1respa=2, n0respa=2, nupdte=6, rshk="l")
 DUDL_STEPS, DUDL_EVERY = 400, 2  # dU/dlambda sampling of the batched windows
+SERVE_PLAIN_SAMPLE = 8  # serving requests also run one at a time, to check the plain model
 # the pair-kernel autotuner's choices per device and workload shape
 TUNE_CACHE = os.path.join(ROOT, "orac-porting_b200", "orac_b200", "pair_tuning.txt")
 TUNE_TRIAL = 6
@@ -664,6 +665,24 @@ def serve_arm(args, wl, device):
         t_step[k] = (time.perf_counter() - t0) / 10
         e.close()
     arrivals = serve.poisson_arrivals(20.0, args.serve, len(specs), seed=11)
+    # the plain path run for real on the first requests, one at a time (each
+    # system's context built beforehand, as the model assumes): their
+    # 500-step service times against the model's 500 x measured step time
+    sample = arrivals[:SERVE_PLAIN_SAMPLE]
+    measured, modelled = [], []
+    for _, sid in sample:
+        e = uneven_engine(syst[sid].copy(), specs[sid], device, wl)
+        L = e.lib
+        for _ in range(3):
+            L.orac_gpu_md_run_async(e.ctx, 1)
+        e.collect()
+        t0 = time.perf_counter()
+        L.orac_gpu_md_run_async(e.ctx, nsteps)
+        if e.collect():
+            raise RuntimeError(L.orac_gpu_last_error(e.ctx).decode())
+        measured.append(time.perf_counter() - t0)
+        modelled.append(nsteps * t_step[sid])
+        e.close()
     srv = serve.Server(device=device, budget_bytes=150e9, max_active=32, chunk=4)
     svc = serve.Service(srv, pop, lambda s: uneven_engine(s, specs[int(s.name[len("served"):])], device, wl),
                         nsteps=nsteps)
@@ -693,6 +712,10 @@ def serve_arm(args, wl, device):
             "speedup_vs_plain": (sim_ns / span) / (sim_ns / pspan),
             "status_ok": all(r["status"] == 0 for r in res), "builds": svc.builds, "evictions": svc.evictions,
             "peak_reserved_gb": stats["peak_reserved"] / 1e9,
+            "plain_check": {"requests": len(sample), "service_s_measured": measured, "service_s_model": modelled,
+                            "measured_over_model": sum(measured) / sum(modelled),
+                            "how": "the first requests' systems run one at a time through the plain driver, 500 steps "
+                                   "each (wall clock, context built beforehand as in the model)"},
             "how": "native executor (orac_gpu_server_*): per-system streams, 4 step graphs per chunk, pump thread; "
                    "latency = segment end - arrival (host monotonic clock); plain = first-come-first-served single "
                    "server with each request taking 500 x the system's measured single-system step time"}

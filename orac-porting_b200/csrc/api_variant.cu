@@ -126,6 +126,24 @@ int upload_alch_charges(orac_gpu_ctx* ctx, const double* dlam) {
   CK(cudaMemcpy(ctx->d_qc, qc.data(), sizeof(double) * N, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(ctx->d_q0, q0.data(), sizeof(double) * N, cudaMemcpyHostToDevice));
   ctx->q0_differs = qc != q0;
+  {
+    // per-atom lambdas of fnb14_alchemy / ferrf_alchemy_add and the
+    // derivatives of their couplings 1 - |lambda| (added: ladd, removed:
+    // -lrm, src/mtsmd.f:746-754)
+    std::vector<double4> l4(N);
+    const double d0[4] = {0, 0, 0, 0};
+    const double* d = dlam ? dlam : d0;
+    for (int a = 0; a < N; a++) {
+      const int ss = ctx->h_ssal[a];
+      const double ll = ss == 2 ? ctx->lam[0] : (ss == -2 ? -ctx->lam[1] : 0.0);
+      const double lq = ss == 2 ? ctx->lam[2] : (ss == -2 ? -ctx->lam[3] : 0.0);
+      const double sl = ss == 2 ? (ctx->lam[0] < 0 ? -1.0 : 1.0) * d[0] : (ss == -2 ? (ctx->lam[1] < 0 ? -1.0 : 1.0) * d[1] : 0.0);
+      const double sq = ss == 2 ? (ctx->lam[2] < 0 ? -1.0 : 1.0) * d[2] : (ss == -2 ? (ctx->lam[3] < 0 ? -1.0 : 1.0) * d[3] : 0.0);
+      l4[a] = make_double4(ll, lq, -sl, -sq);
+    }
+    if (!ctx->d_lam4 && dev_alloc(ctx, &ctx->d_lam4, N)) return ORAC_ERR_CUDA;
+    CK(cudaMemcpy(ctx->d_lam4, l4.data(), sizeof(double4) * N, cudaMemcpyHostToDevice));
+  }
   if (dlam) {
     if (!ctx->d_dq && dev_alloc(ctx, &ctx->d_dq, N)) return ORAC_ERR_CUDA;
     CK(cudaMemcpy(ctx->d_dq, dq.data(), sizeof(double) * N, cudaMemcpyHostToDevice));
@@ -167,8 +185,47 @@ int variant_out_launch(orac_gpu_ctx* ctx, int forces_on) {
   return ORAC_OK;
 }
 
+// listqq of src/initialize_lambda.f:62-139 from the species and the
+// context's pair lists: every pair of alchemical atoms that is no bond,
+// constraint, 1-3 or 1-4 pair, facQ 1 within a species, 0 across.  Built
+// when the MD driver is set up (the constraints are known then) and again
+// when the species change.
+int alch_listqq_build(orac_gpu_ctx* ctx) {
+  const BondedDev& B = ctx->bd;
+  std::vector<int> iat;  // ORAC's order: added atoms, then removed ones
+  for (int a = 0; a < ctx->N; a++)
+    if (ctx->h_ssal.size() == (size_t)ctx->N && ctx->h_ssal[a] == 2) iat.push_back(a + 1);
+  for (int a = 0; a < ctx->N; a++)
+    if (ctx->h_ssal.size() == (size_t)ctx->N && ctx->h_ssal[a] == -2) iat.push_back(a + 1);
+  std::unordered_map<long long, char> excl;
+  auto key = [](int i, int j) { return i < j ? ((long long)i << 32) | (unsigned)j : ((long long)j << 32) | (unsigned)i; };
+  const int* lists[4] = {B.pbond, B.pcn, B.p13, B.p14};
+  const int n[4] = {B.nb, B.ncn, B.n13, B.n14};
+  for (int k = 0; k < 4; k++) {
+    if (!lists[k] || n[k] <= 0) continue;
+    std::vector<int> h(2 * (size_t)n[k]);
+    CK(cudaMemcpy(h.data(), lists[k], sizeof(int) * h.size(), cudaMemcpyDeviceToHost));
+    for (int q = 0; q < n[k]; q++) excl[key(h[2 * q], h[2 * q + 1])] = 1;
+  }
+  std::vector<int> out;
+  for (size_t a = 0; a + 1 < iat.size(); a++)
+    for (size_t b = a + 1; b < iat.size(); b++) {
+      if (excl.count(key(iat[a], iat[b]))) continue;
+      out.push_back(iat[a]);
+      out.push_back(iat[b]);
+      out.push_back(ctx->h_ssal[iat[a] - 1] == ctx->h_ssal[iat[b] - 1] ? 1 : 0);
+    }
+  ctx->nlistqq = (int)(out.size() / 3);
+  if (ctx->nlistqq > 0) {
+    if (dev_alloc(ctx, &ctx->d_listqq, out.size())) return ORAC_ERR_CUDA;
+    CK(cudaMemcpy(ctx->d_listqq, out.data(), sizeof(int) * out.size(), cudaMemcpyHostToDevice));
+  }
+  return ORAC_OK;
+}
+
 void variant_free(orac_gpu_ctx* ctx) {
-  void* p[] = {ctx->d_vflag, ctx->d_soft, ctx->d_softd, ctx->d_qc, ctx->d_q0, ctx->d_xtra, ctx->d_dq};
+  void* p[] = {ctx->d_vflag, ctx->d_soft, ctx->d_softd, ctx->d_qc, ctx->d_q0, ctx->d_xtra, ctx->d_dq,
+               ctx->d_lam4, ctx->d_listqq};
   for (void* q : p)
     if (q) dev_free(ctx, q);
 }
@@ -223,6 +280,7 @@ int orac_gpu_set_alchemy(orac_gpu_ctx* ctx, const int* ss_alchemy, const double*
   }
   bump.arm();
   ctx->h_ssal.assign(ss_alchemy, ss_alchemy + N);
+  ctx->nlistqq = -1;  // the species changed: listqq is built again
   if (!ctx->d_soft && (dev_alloc(ctx, &ctx->d_soft, N) || dev_alloc(ctx, &ctx->d_softd, N))) return ORAC_ERR_CUDA;
   CK(cudaMemcpy(ctx->d_soft, sf.data(), sizeof(float2) * N, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(ctx->d_softd, sd.data(), sizeof(double2) * N, cudaMemcpyHostToDevice));
@@ -258,6 +316,7 @@ int orac_gpu_set_lambda(orac_gpu_ctx* ctx, const double* lam, int intramol, int 
   CK(cudaSetDevice(ctx->device));
   bump.arm();
   for (int k = 0; k < 8; k++) ctx->lam[k] = lam[k];
+  ctx->alch_intramol = intramol ? 1 : 0;
   const double d0[4] = {0, 0, 0, 0};
   const double* d = dlam ? dlam : d0;
   AlchTables& T = ctx->at;

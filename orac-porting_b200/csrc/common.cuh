@@ -326,6 +326,13 @@ struct orac_gpu_ctx {
   double* d_q0 = nullptr;  // [N] PME charges at lambda0
   double* d_dq = nullptr;  // [N] d(PME charge)/d(control lambda), or null
   double self_dudl = 0.0;  // d(self energy)/d(control lambda) (cself_alchemy)
+  // ORAC's intra-alchemical corrections (fnb14_alchemy, ferrf_alchemy_add):
+  // per atom (lambda LJ, lambda charge, d(1-|lambda LJ|)/dlambda,
+  // d(1-|lambda charge|)/dlambda), and listqq (ia, ib, facQ, 1-based)
+  double4* d_lam4 = nullptr;
+  int* d_listqq = nullptr;
+  int nlistqq = -1;  // -1: not built for the current species
+  int alch_intramol = 0;
   std::vector<unsigned char> h_rem;   // REM segment atoms
   bool q0_differs = false;            // lambda0 charges differ from lambda charges
   double pme_dwrk = 0.0;              // eer(lambda) - eer(lambda0) of the last fft_pme
@@ -470,6 +477,9 @@ int small_launch(orac_gpu_ctx* ctx, int kind, const double* d_xyz,
                  double lj_fudge, int coul_mode, int forces, double* d_f,
                  double* d_e, const int* d_ss);
 int self_launch(orac_gpu_ctx* ctx, const int* d_ss, double* d_e);
+int alch_intra_launch(orac_gpu_ctx* ctx, int kind, const double* d_xyz, unsigned long long* d_ffix, double* d_e,
+                      double* d_edq);
+int alch_listqq_build(orac_gpu_ctx* ctx);
 // the same with explicit charges (null: the topology's) and an optional
 // fixed-point force output (the MD driver's level accumulators)
 int small_launch_x(orac_gpu_ctx* ctx, int kind, const double* d_xyz, const int* d_pairs, const int* d_ptype,

@@ -20,7 +20,7 @@ __device__ __forceinline__ double warp_sumd(double v) {
 }
 
 struct SmallArgs {
-  int kind;  // 0 fnb14, 1 fnbgrp, 2 ferrf
+  int kind;  // 0 fnb14, 1 fnbgrp, 2 ferrf, 3 fnb14_alchemy, 4 ferrf_alchemy_add
   int n;     // pairs
   int natom;
   const double* xyz;  // [3N] Cartesian
@@ -39,14 +39,56 @@ struct SmallArgs {
   // ferrf: d/dlambda of the correction for charges q(lambda) with dq/dlambda
   const double* dq;
   double* edq;
+  // fnb14_alchemy, ferrf_alchemy_add: per atom (lambda LJ, lambda charge,
+  // d(1-|lambda LJ|)/dlambda, d(1-|lambda charge|)/dlambda); the charges
+  // q are the full ones; intramol skips same-species listqq pairs
+  const double4* lam4;
+  int intramol;
 };
+
+// Coupling factors of one pair of fnb14_alchemy (src/fnb14_alchemy.f:
+// 149-177, 252-289) from the atoms' lambdas li, lj with the derivatives
+// di, dj of their couplings 1-|l|: f scales the erfc (or LJ) term, f2 the
+// erf term of the charges; df, df2 their derivatives.  An alchemical atom
+// at lambda 0 counts as normal; one alchemical atom: its coupling; two of
+// one lambda: full, with f2 = 1 - the product of couplings; two of
+// different lambdas: none, f2 = - that product.
+__device__ __forceinline__ void alch14_factors(double li, double lj, double di, double dj, bool charges, double* f,
+                                               double* df, double* f2, double* df2) {
+  const double ci = 1.0 - fabs(li), cj = 1.0 - fabs(lj);
+  *f2 = 0.0;
+  *df2 = 0.0;
+  *df = 0.0;
+  if (li == 0.0 && lj != 0.0) {
+    *f = cj;
+    *df = dj;
+  } else if (li != 0.0 && lj == 0.0) {
+    *f = ci;
+    *df = di;
+  } else if (li == 0.0 && lj == 0.0) {
+    *f = 1.0;
+  } else if (li != lj) {
+    *f = 0.0;
+    if (charges) {
+      *f2 = -ci * cj;
+      *df2 = -(di * cj + ci * dj);
+    }
+  } else {
+    *f = 1.0;
+    if (charges) {
+      *f2 = 1.0 - ci * cj;
+      *df2 = -(di * cj + ci * dj);
+    }
+  }
+}
 
 __device__ __forceinline__ void small_body(const SmallArgs& A) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   double e[4] = {0, 0, 0, 0};
   double dedl = 0.0;
   if (t < A.n) {
-    const int i1 = A.pairs[2 * t] - 1, i2 = A.pairs[2 * t + 1] - 1;
+    const int stride = A.kind == 4 ? 3 : 2;  // listqq carries facQ
+    const int i1 = A.pairs[stride * t] - 1, i2 = A.pairs[stride * t + 1] - 1;
     const int type = A.ss[i1] - 1;
     const double xa = A.xyz[i1] - A.xyz[i2];
     const double ya = A.xyz[A.natom + i1] - A.xyz[A.natom + i2];
@@ -55,7 +97,54 @@ __device__ __forceinline__ void small_body(const SmallArgs& A) {
     const double rsp = sqrt(rsq);
     const double rsqi = 1.0 / rsq;
     double qforce = 0.0;
-    if (A.kind == 2) {
+    bool skip = false;
+    if (A.kind == 4) {
+      // ferrf_alchemy_add (src/ferrf_alchemy_add.f): the reciprocal sum of
+      // the scaled charges gave the pair c_a c_b Q_a Q_b erf/r; subtract
+      // (c_a c_b - facQ) of it, so one species keeps its full Coulomb
+      // (facQ 1) and added and removed atoms do not see each other (0)
+      const int facq = A.pairs[3 * t + 2];
+      skip = A.intramol && facq != 0;
+      if (!skip) {
+        const double4 la = A.lam4[i1], lb = A.lam4[i2];
+        const double ca = 1.0 - fabs(la.y), cb = 1.0 - fabs(lb.y);
+        const double qab = A.q[i1] * A.q[i2];
+        const double furpar = (ca * cb - (double)facq) * qab;
+        const double alphar = A.alpha * rsp;
+        const double qt = 1.0 / (1.0 + AS_QP * alphar);
+        const double expcst = exp(-alphar * alphar);
+        const double erfcst = ((((AS_A5 * qt + AS_A4) * qt + AS_A3) * qt + AS_A2) * qt + AS_A1) * qt * expcst;
+        const double erfst = 1.0 - erfcst;
+        e[type] -= furpar * erfst / rsp;
+        qforce = -furpar * (erfst - A.twrtpi * alphar * expcst) / (rsp * rsq);
+        dedl = -(la.w * cb + ca * lb.w) * qab * erfst / rsp;
+      }
+    } else if (A.kind == 3) {
+      // fnb14_alchemy, Ewald branch (src/fnb14_alchemy.f:225-341); ORAC
+      // scales only the repulsive term of the LJ force by alch_fact (its
+      // energy by alch_fact whole), restated as written
+      const double4 la = A.lam4[i1], lb = A.lam4[i2];
+      double af, daf, dum, ddum, aq, daq, aq2, daq2;
+      alch14_factors(la.x, lb.x, la.z, lb.z, false, &af, &daf, &dum, &ddum);
+      alch14_factors(la.y, lb.y, la.w, lb.w, true, &aq, &daq, &aq2, &daq2);
+      const int lij = A.ptype[t] - 1;
+      const double rspqi = rsqi / rsp;
+      const double r6 = rsqi * rsqi * rsqi;
+      const double r12 = r6 * r6;
+      const double ssvir = af * 12.0 * A.tab12[lij] * r12 - 6.0 * A.tab6[lij] * r6;
+      qforce = A.lj_fudge * ssvir * rsqi;
+      const double elj = A.lj_fudge * (A.tab12[lij] * r12 - A.tab6[lij] * r6);
+      e[type] += af * elj;
+      const double alphar = A.alpha * rsp;
+      const double qt = 1.0 / (1.0 + AS_QP * alphar);
+      const double expcst = exp(-alphar * alphar);
+      const double erfcst = ((((AS_A5 * qt + AS_A4) * qt + AS_A3) * qt + AS_A2) * qt + AS_A1) * qt * expcst;
+      const double erff = 1.0 - erfcst;
+      const double qq = A.fudge * A.q[i1] * A.q[i2];
+      e[2 + type] += qq * (aq * erfcst + aq2 * erff) / rsp;
+      qforce += qq * (aq * (erfcst + A.twrtpi * alphar * expcst) + aq2 * (erff - A.twrtpi * alphar * expcst)) * rspqi;
+      dedl = daf * elj + qq * (daq * erfcst + daq2 * erff) / rsp;
+    } else if (A.kind == 2) {
       // ferrf: subtract fudge q q erf(alpha r)/r
       const double furpar = (A.forces ? A.fudge : 1.0) * A.q[i1] * A.q[i2];
       const double alphar = A.alpha * rsp;
@@ -98,7 +187,8 @@ __device__ __forceinline__ void small_body(const SmallArgs& A) {
         qforce += sv * rsqi;
       }
     }
-    if (A.forces && A.ffix) {
+    if (skip) {
+    } else if (A.forces && A.ffix) {
       const double fv[3] = {qforce * xa, qforce * ya, qforce * za};
 #pragma unroll
       for (int d = 0; d < 3; d++) {
@@ -199,7 +289,9 @@ static SmallArgs small_args(orac_gpu_ctx* ctx, int kind, const double* d_xyz, co
   A.ss = d_ss;
   A.ffix = d_ffix;
   A.dq = (kind == 2 && d_edq) ? d_dq : nullptr;
-  A.edq = A.dq ? d_edq : nullptr;
+  A.edq = (A.dq || kind >= 3) ? d_edq : nullptr;
+  A.lam4 = ctx->d_lam4;
+  A.intramol = ctx->alch_intramol;
   A.alpha = ctx->alphal;
   A.fudge = fudge;
   A.lj_fudge = lj_fudge;
@@ -241,6 +333,23 @@ int ferrf_launch_lists(orac_gpu_ctx* ctx, int nlist, const int* const* d_pairs, 
   orac_launch(k_small_segs, dim3((nmax + 255) / 256, ns), dim3(256), 0, ctx->stream, S);
   CKL();
   return ORAC_OK;
+}
+
+// fnb14_alchemy over the 1-4 list (kind 3) or ferrf_alchemy_add over listqq
+// (kind 4), forces into the fixed-point accumulator, energies into d_e (4
+// or 2 slots), dU/dlambda into d_edq
+int alch_intra_launch(orac_gpu_ctx* ctx, int kind, const double* d_xyz, unsigned long long* d_ffix, double* d_e,
+                      double* d_edq) {
+  const BondedDev& B = ctx->bd;
+  if (!ctx->d_lam4) return ORAC_OK;
+  if (kind == 3) {
+    if (B.n14 <= 0) return ORAC_OK;
+    return small_launch_x(ctx, 3, d_xyz, B.p14, B.t14, B.n14, B.e1412, B.e146, B.fudge, B.lj_fudge, 1, 1, nullptr,
+                          d_e, B.ss, ctx->d_aqd, d_ffix, nullptr, d_edq);
+  }
+  if (ctx->nlistqq <= 0) return ORAC_OK;
+  return small_launch_x(ctx, 4, d_xyz, ctx->d_listqq, nullptr, ctx->nlistqq, nullptr, nullptr, 1.0, 1.0, 1, 1,
+                        nullptr, d_e, B.ss, ctx->d_aqd, d_ffix, nullptr, d_edq);
 }
 
 int self_launch(orac_gpu_ctx* ctx, const int* d_ss, double* d_e) {

@@ -995,8 +995,9 @@ __global__ void k_record(const double* __restrict__ e, const int* __restrict__ f
   for (int q = 41; q < 49; q++) b += e[q];  // bonded (E_BOND..E_14)
   for (int q = 49; q < 57; q++) p += e[q];  // 1-4 and intra-group (E_14..E_ERF)
   for (int q = 57; q < 73; q++) c += e[q];  // erf corrections (E_ERF..E_DUDL)
+  c += e[80] + e[81];                       // ferrf_alchemy_add (E_AQQ)
   if (alch) {
-    for (int q = 73; q < 78; q++) d += e[q];
+    for (int q = 73; q < 80; q++) d += e[q];
     d += self_dudl;
   }
   r[12] = b;
@@ -1192,7 +1193,10 @@ static ConsArgs big_args(orac_gpu_ctx* ctx, MdState& S, double dt, double tol) {
   return A;
 }
 
-enum { E_BOND = 41, E_14 = 49, E_GRP = 53, E_ERF = 57, E_DUDL = 73, E_N = 80 };
+// dU/dlambda slots: E_DUDL + 0..2 shells, +3 SPME, +4 erf corrections,
+// +5 fnb14_alchemy, +6 ferrf_alchemy_add; E_AQQ: ferrf_alchemy_add's
+// energies (solute, solvent)
+enum { E_BOND = 41, E_14 = 49, E_GRP = 53, E_ERF = 57, E_DUDL = 73, E_AQQ = 80, E_N = 82 };
 
 // energy records kept on the device per context (the newest MD_REC_CAP)
 constexpr int MD_REC_CAP = 2048;
@@ -1340,11 +1344,31 @@ struct SideStream {
 
 // mts_intra_n0 / mts_intra_n1 into their level accumulators
 // 1-4 and intra-group pairs of the N1 level (fnb14, fnbgrp)
+// ORAC's intra-alchemical corrections apply with alchemy and Ewald
+// (src/mts_intra_n1.f:81-85, src/mtsmd.f:3035-3041)
+static bool md_alch_intra(const orac_gpu_ctx* ctx) {
+  return ctx->variant == VAR_ALCH && ctx->clewld && ctx->d_lam4;
+}
+
+// ferrf_alchemy_add over listqq after the M shell (src/mtsmd.f:3035-3041)
+static int md_alch_m(orac_gpu_ctx* ctx, MdState& S, bool energy) {
+  if (!md_alch_intra(ctx)) return ORAC_OK;
+  if (ctx->nlistqq < 0)
+    if (int rc = alch_listqq_build(ctx)) return rc;
+  return alch_intra_launch(ctx, 4, S.x, S.ffix[LM], energy ? S.e + E_AQQ : nullptr,
+                           energy ? S.e + E_DUDL + 6 : nullptr);
+}
+
 static int md_pairs_n1(orac_gpu_ctx* ctx, MdState& S, bool energy) {
   const BondedDev& B = ctx->bd;
   if (B.have_pairs) {
     const int coul = ctx->clewld ? 1 : 0;
-    if (B.n14 > 0)
+    if (B.n14 > 0 && md_alch_intra(ctx)) {
+      // fnb14_alchemy in place of fnb14 (src/mts_intra_n1.f:81-85)
+      if (int rc = alch_intra_launch(ctx, 3, S.x, S.ffix[LN1], energy ? S.e + E_14 : nullptr,
+                                     energy ? S.e + E_DUDL + 5 : nullptr))
+        return rc;
+    } else if (B.n14 > 0)
       if (int rc = small_launch_x(ctx, 0, S.x, B.p14, B.t14, B.n14, B.e1412, B.e146, B.fudge, B.lj_fudge, coul, 1,
                                   nullptr, energy ? S.e + E_14 : nullptr, B.ss, nullptr, S.ffix[LN1]))
         return rc;
@@ -1445,8 +1469,10 @@ static int md_step(orac_gpu_ctx* ctx, MdState& S, bool update, bool energy) {
           }))
         return rc;
     }
-    if (due_m)
+    if (due_m) {
       if (int rc = md_shell_pair(ctx, S, 'm', LM, false, S.e, e_now)) return rc;
+      if (int rc = md_alch_m(ctx, S, e_now)) return rc;
+    }
     if (due_l)
       if (int rc = md_shell_pair(ctx, S, 'l', LL, false, S.e + 8, e_now)) return rc;
     // the N1 level's pair terms beside the bonded kernel on the side stream
@@ -1789,7 +1815,9 @@ int orac_gpu_md_setup(orac_gpu_ctx* ctx, const double* x, const double* y, const
     r2.rtoll = 0.0;
     if (int rc = md_phony(ctx, r2, 'l')) return rc;
   }
+  if (ctx->variant == VAR_ALCH) ctx->nlistqq = -1;  // built with this setup's constraints
   if (int rc = md_forces_shell(ctx, S, 'm', LM, true, S.e, true)) return rc;
+  if (int rc = md_alch_m(ctx, S, false)) return rc;
   if (int rc = md_forces_shell(ctx, S, 'l', LL, true, S.e + 8, true)) return rc;
   if (int rc = md_forces_shell(ctx, S, 'h', LH, true, S.e + 16, true)) return rc;
   for (int l = LN1; l <= LN0; l++) {
@@ -1912,6 +1940,9 @@ static int md_capture(orac_gpu_ctx* ctx, MdState& S, int kind) {
   S.graphs_shared = ctx->shared_device;
   S.graphs_gen = ctx->param_gen;
   if (S.gexec[kind]) return ORAC_OK;
+  // listqq is built with synchronous copies: never inside the capture
+  if (md_alch_intra(ctx) && ctx->nlistqq < 0)
+    if (int rc = alch_listqq_build(ctx)) return rc;
   const int64_t l0 = ctx->launches;
   S.pslot[kind][0] = ctx->prof_next;
   CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
@@ -2010,9 +2041,11 @@ static int md_run_impl(orac_gpu_ctx* ctx, int nsteps, int energy_every, double* 
       for (int q = E_BOND; q < E_14; q++) r[12] += e[q];
       for (int q = E_14; q < E_ERF; q++) r[13] += e[q];
       for (int q = E_ERF; q < E_DUDL; q++) r[14] += e[q];
-      // dU/dlambda of the alchemical windows: shells, PME, erf corrections, self term
+      r[14] += e[E_AQQ] + e[E_AQQ + 1];
+      // dU/dlambda of the alchemical windows: shells, PME, erf corrections,
+      // fnb14_alchemy, ferrf_alchemy_add, self term
       if (ctx->variant == VAR_ALCH && ctx->d_dq) {
-        for (int q = E_DUDL; q < E_DUDL + 5; q++) r[15] += e[q];
+        for (int q = E_DUDL; q < E_DUDL + 7; q++) r[15] += e[q];
         r[15] += ctx->self_dudl;
       }
       r[10] = r[1] + r[2] + r[3] + r[4] + r[5] + r[6] + r[7] + r[8] + r[9] + r[12] + r[13] + r[14];

@@ -74,6 +74,13 @@ def lib():
         L.orc_fnb14.argtypes = [_I, _D, _D, _D, _D, C.c_int, _D, _D, C.c_int, C.c_int, C.c_double, _I, C.c_int,
                                 _I, C.c_double, C.c_double, _D, _D, _D, _D]
         L.orc_fnbgrp.argtypes = [_I, _D, _D, _D, _D, _I, _D, _D, C.c_int, C.c_double, _I, C.c_int, _D, _D, _D, _D]
+        L.orc_alch_atom_lambdas.argtypes = [C.c_int, _I, C.c_double, C.c_double, _D]
+        L.orc_alch_listqq.restype = C.c_int
+        L.orc_alch_listqq.argtypes = [C.c_int, _I, _I, C.c_int, _I, C.c_int]
+        L.orc_ferrf_alchemy_add.argtypes = [_I, C.c_double, _D, _D, _D, _D, _D, _D, _I, C.c_int, C.c_int, _D, _D,
+                                            _D, _D, _D]
+        L.orc_fnb14_alchemy.argtypes = [_I, _D, _D, _D, _D, _D, _D, C.c_double, _I, C.c_int, _I, C.c_double,
+                                        C.c_double, _D, _D, _D, _D, _D, _D, _D, _D, _D]
         _lib = L
     return _lib
 
@@ -414,6 +421,56 @@ class Oracle:
         self.L.orc_fnbgrp(_i(s.ss_index), _f(r[0]), _f(r[1]), _f(r[2]), _f(s.charge), _i(s.nbtype), _f(s.ecc12),
                           _f(s.ecc6), int(self.ewald), s.alphal, p, len(p) // 2, fx, fy, fz, ue)
         return np.stack([fx, fy, fz]), ue
+
+
+    # ------------------------------------------- intra-alchemical terms
+    def alch_lambdas(self, ss_alchemy, ladd, lrm):
+        """Per-atom lambdas of the species (added ladd, removed -lrm)."""
+        lam = np.zeros(self.s.ntap)
+        self.L.orc_alch_atom_lambdas(self.s.ntap, _i(ss_alchemy), float(ladd), float(lrm), lam)
+        return lam
+
+    def alch_listqq(self, ss_alchemy):
+        """listqq (src/initialize_lambda.f:62-139): (ia, ib, facQ) 1-based
+        for the pairs of alchemical atoms beyond 1-4."""
+        s = self.s
+        excl = [np.asarray(a).reshape(-1, 2) for a in (s.bonds, s.constraints, s.bend13, s.int14) if len(a)]
+        ex = _i(np.concatenate(excl).ravel()) if excl else _i(np.zeros(0))
+        nal = int(np.sum(np.abs(np.asarray(ss_alchemy)) == 2))
+        cap = max(1, nal * (nal - 1) // 2)
+        out = np.zeros(3 * cap, np.int32)
+        n = self.L.orc_alch_listqq(s.ntap, _i(ss_alchemy), ex, len(ex) // 2, out, cap)
+        return out[:3 * n].reshape(-1, 3)
+
+    def ferrf_alchemy_add(self, listqq, lamq, lamq0=None, intramol=False):
+        """ferrf_alchemy_add (src/ferrf_alchemy_add.f) with the full charges:
+        (F, (E slt, E slv), U(lambda) - U(lambda0))."""
+        s = self.s
+        r = self.cartesian()
+        f = [np.zeros(s.ntap) for _ in range(3)]
+        fs = np.zeros(2)
+        dw = np.zeros(1)
+        lq0 = lamq if lamq0 is None else lamq0
+        lst = _i(np.asarray(listqq).ravel())
+        self.L.orc_ferrf_alchemy_add(_i(s.ss_index), s.alphal, _f(s.charge), _f(lamq), _f(lq0), _f(r[0]), _f(r[1]),
+                                     _f(r[2]), lst, len(lst) // 3, int(intramol), fs, dw, *f)
+        return np.stack(f), fs, float(dw[0])
+
+    def fnb14_alchemy(self, lam, lamq, lam0=None, lamq0=None):
+        """fnb14_alchemy's Ewald branch (src/fnb14_alchemy.f:225-341) with
+        the full charges: (F, (LJ slt, slv, Coulomb slt, slv), work)."""
+        s = self.s
+        r = self.cartesian()
+        f = [np.zeros(s.ntap) for _ in range(3)]
+        ue = np.zeros(4)
+        dw = np.zeros(1)
+        l0 = lam if lam0 is None else lam0
+        lq0 = lamq if lamq0 is None else lamq0
+        p = _i(s.int14.ravel())
+        self.L.orc_fnb14_alchemy(_i(s.ss_index), _f(r[0]), _f(r[1]), _f(r[2]), _f(s.charge), _f(s.ecc1412),
+                                 _f(s.ecc146), s.alphal, p, len(p) // 2, _i(s.type14), s.fudge, 1.0, _f(lam),
+                                 _f(lamq), _f(l0), _f(lq0), *f, ue, dw)
+        return np.stack(f), ue, float(dw[0])
 
 
 class OracleMD:

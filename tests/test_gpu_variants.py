@@ -193,9 +193,11 @@ def test_alchemy_pme_dudl_matches_oracle_central_difference():
 @pytest.mark.parametrize("form", sorted(FORMS))
 def test_md_window_dudl_is_derivative_of_potential(form):
     """Record column 15 of an alchemical MD window (shells, SPME, erf
-    corrections, self term) against the central difference of the oracle's
-    potential energy at the same configuration (a 1e-9 fs step leaves the
-    atoms in place), with either pair form."""
+    corrections, self term, and ORAC's intra-alchemical corrections:
+    fnb14_alchemy's 1-4 pairs and ferrf_alchemy_add over listqq) against the
+    central difference of the oracle's potential energy at the same
+    configuration (a 1e-9 fs step leaves the atoms in place), with either
+    pair form."""
     from orac_b200.engine import Engine
 
     s = systems.ligand_in_water()
@@ -225,7 +227,10 @@ def test_md_window_dudl_is_derivative_of_potential(form):
             if len(pairs):
                 eerf += ot.ferrf(np.asarray(pairs).reshape(-1, 2), fudge, iz=iz)[1].sum()
         eself = ot.cself()[0]
-        u.append(esh + epme + eerf + eself)
+        lam_at = o.alch_lambdas(s.ss_alchemy, 0.0, lr)
+        e14 = o.fnb14_alchemy(lam_at, lam_at)[1].sum()
+        eqq = o.ferrf_alchemy_add(o.alch_listqq(s.ss_alchemy), lam_at)[1].sum()
+        u.append(esh + epme + eerf + eself + e14 + eqq)
     fd = (u[0] - u[1]) / (2 * h)
     assert abs(dudl - fd) <= 1e-5 * abs(fd), (dudl, fd)
 
@@ -257,3 +262,38 @@ def test_lambda_change_after_md_setup_reaches_the_step_graphs():
     ref.close()
     assert abs(d_b - d_a) > 1e-3 * abs(d_a)
     assert abs(d_b - d_ref) <= 1e-6 * abs(d_ref), (d_b, d_ref)
+
+
+def test_intra_alchemical_corrections_energies_match_oracle():
+    """ORAC's intra-alchemical corrections in an alchemical MD window at
+    lambda 0.45: record column 13 (1-4 and intra-group pairs, fnb14_alchemy
+    for the 1-4 pairs) and column 14 (erf corrections of the scaled charges
+    plus ferrf_alchemy_add over listqq) against the oracle's restatements at
+    the same configuration (1e-9 fs step), relative 1e-9 (both FP64)."""
+    from orac_b200.engine import Engine
+
+    s = systems.ligand_in_water()
+    lam = 0.45
+    g = Engine(s.copy())
+    g.set_alchemy(s.ss_alchemy)
+    g.set_lambda(0.0, lam, 0.0, lam, dlam=[0.0, 1.0, 0.0, 1.0])
+    g.md_setup(1e-9, 2, 4, 6, "l")
+    rec = g.md_run(1, energy_every=1)[0]
+    g.close()
+    o = oracle.Oracle(s.copy())
+    lam_at = o.alch_lambdas(s.ss_alchemy, 0.0, lam)
+    e14 = o.fnb14_alchemy(lam_at, lam_at)[1].sum() + o.fnbgrp()[1].sum()
+    assert abs(rec[13] - e14) <= 1e-9 * abs(e14), (rec[13], e14)
+    a = s.intra_lists()
+    t = s.copy()
+    t.charge = np.where(s.ss_alchemy == -2, 1.0 - lam, 1.0) * s.charge
+    ot = oracle.Oracle(t)
+    eerf = 0.0
+    for pairs, fudge, iz in ((a["lbnd"], 1.0, 1), (t.constraints.ravel(), 1.0, 0), (a["int13"], 1.0, 1),
+                             (a["int14"], 1.0 - s.fudge, 1)):
+        if len(pairs):
+            eerf += ot.ferrf(np.asarray(pairs).reshape(-1, 2), fudge, iz=iz)[1].sum()
+    lst = o.alch_listqq(s.ss_alchemy)
+    assert len(lst) > 500
+    eqq = o.ferrf_alchemy_add(lst, lam_at)[1].sum()
+    assert abs(rec[14] - (eerf + eqq)) <= 1e-9 * (abs(eerf) + abs(eqq)), (rec[14], eerf, eqq)
