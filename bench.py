@@ -74,6 +74,7 @@ def f0_system():
 F0_WORKLOAD = dict(build=f0_system, dt_h=15.0, lrespa=5, mrespa=2, n1respa=2, n0respa=2, nupdte=6, rshk="l")
 DUDL_STEPS, DUDL_EVERY = 400, 2  # dU/dlambda sampling of the batched windows
 SERVE_PLAIN_SAMPLE = 8  # serving requests also run one at a time, to check the plain model
+HREM_N, HREM_EVERY, HREM_INTERVALS = 16, 15, 6  # replica-exchange leg
 # the pair-kernel autotuner's choices per device and workload shape
 TUNE_CACHE = os.path.join(ROOT, "orac-porting_b200", "orac_b200", "pair_tuning.txt")
 TUNE_TRIAL = 6
@@ -433,6 +434,11 @@ def gpu_arm(args, wl, s, device):
             res["orac_test1"] = f0_arm(args, device, flush)
         except Exception as exc:
             res["orac_test1"] = {"error": f"{type(exc).__name__}: {exc}"}
+    if ws == 1 and args.hrem:
+        try:
+            res["hrem"] = hrem_arm(args, wl, device)
+        except Exception as exc:
+            res["hrem"] = {"error": f"{type(exc).__name__}: {exc}"}
     if ws == 1 and args.configs:
         for key, arm in (("config2", config2_arm), ("config1_as_specified", config1_fixed_arm)):
             try:
@@ -762,6 +768,69 @@ def f0_arm(args, device, flush):
     return out
 
 
+def hrem_arm(args, wl, device):
+    """Hamiltonian replica exchange as ORAC's test2 runs it, batched on one
+    GPU: HREM_N replicas of one solvated-chain system (about 20k atoms,
+    solute 8%), solute scaling on a geometric ladder from 1 to 0.3
+    (rem_factor(3) on the pairs touching the solute, seg_select kind 0),
+    300 K, an exchange attempt every 15 steps (60 fs) by ORAC's rule on
+    the replicas' segment energies recorded on the device.  Timed by wall
+    clock over the exchange intervals (steps, records, decisions and factor
+    writes all inside); plain = one replica alone through the same driver."""
+    import torch
+
+    from orac_b200 import hrem
+
+    s = systems.solvated_chains(20000, 4242, solute_frac=0.08, name="hrem20k")
+    ladder = hrem.ladder_geometric(HREM_N, 0.3)
+    kT = units.BOLTZ * 300.0 / units.UNITE
+
+    def make(f):
+        return uneven_engine(s.copy(), {"rem_factor": float(f)}, device, wl)
+
+    e1 = make(1.0)
+    L = e1.lib
+    for _ in range(3):
+        L.orac_gpu_md_run_async(e1.ctx, 1)
+    e1.collect()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    L.orac_gpu_md_run_async(e1.ctx, HREM_EVERY * HREM_INTERVALS)
+    if e1.collect():
+        raise RuntimeError(L.orac_gpu_last_error(e1.ctx).decode())
+    plain_s = time.perf_counter() - t0
+    e1.close()
+    engines = [make(f) for f in ladder]
+    h = hrem.HremBatch(engines, ladder, kT, seed=2)
+    tune = tuned(h.batch)
+    h.interval(HREM_EVERY)  # warm-up interval (captures the energy-step graphs)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(HREM_INTERVALS):
+        h.interval(HREM_EVERY)
+    secs = time.perf_counter() - t0
+    acc = h.acceptance()
+    ens = h.ens.tolist()
+    h.close()
+    status = [e.collect() for e in engines]
+    for e in engines:
+        e.close()
+    steps = HREM_EVERY * HREM_INTERVALS
+    val = ns_per_day(steps * HREM_N, wl["dt_h"], secs)
+    pval = ns_per_day(steps, wl["dt_h"], plain_s)
+    return {"workload": f"{HREM_N} replicas of one solvated-chain system ({s.ntap} atoms, solute {int(s.rematom.sum())} "
+                        "atoms), solute scaling 1..0.3 geometric as rem_factor(3) (seg_select kind 0), 300 K, "
+                        f"exchange attempts every {HREM_EVERY} steps ({HREM_EVERY * wl['dt_h']:g} fs)",
+            "replicas": HREM_N, "value": val, "unit": "ns/day (aggregate over replicas)",
+            "plain_value": pval, "speedup_vs_plain": val / pval, "exchanges": HREM_INTERVALS + 1,
+            "acceptance_by_pair": [float(a) for a in acc], "final_ensembles": ens,
+            "status_ok": all(x == 0 for x in status), "tuning": tune,
+            "how": "one graph launch per step advances every replica; each interval ends with an energy step whose "
+                   "device record holds the segment energies; ORAC's decision (orac_gpu_rem_exchange) on the host; "
+                   "accepted swaps rewrite rem_factor on the device (no graph capture); wall clock over "
+                   f"{HREM_INTERVALS} intervals"}
+
+
 def config2_arm(args, device, flush):
     """The solvated chain of the second workload: a 1,700-atom bonded chain
     in 7,000 waters (22,700 atoms, 62 A box, SPME 64^3 order 5), FP32 pair
@@ -925,6 +994,7 @@ def main():
     ap.add_argument("--serve-systems", type=int, default=16, help="systems the serving requests draw from")
     ap.add_argument("--no-f0", dest="f0", action="store_false", help="skip the ORAC test1 system leg")
     ap.add_argument("--no-drift", dest="drift", action="store_false", help="skip the 1,000-step energy drift run")
+    ap.add_argument("--no-hrem", dest="hrem", action="store_false", help="skip the replica-exchange leg")
     ap.add_argument("--no-configs", dest="configs", action="store_false",
                     help="skip the solvated-chain MD leg and the 31 A fixed-list leg")
     ap.add_argument("--profile-window-batch", type=int, default=0, metavar="N",
@@ -1070,7 +1140,7 @@ def main():
                    "the autotuner (orac_gpu_batch_tune / orac_gpu_tune)"}
     elif "batched_error" in res:
         out["batched"] = {"error": res["batched_error"]}
-    for key in ("orac_test1", "config2", "config1_as_specified", "uneven", "served"):
+    for key in ("orac_test1", "config2", "config1_as_specified", "hrem", "uneven", "served"):
         if key in res:
             out[key] = res[key]
     print(json.dumps(out))

@@ -230,6 +230,13 @@ int orac_gpu_mts_intra_n1(orac_gpu_ctx* ctx, const double* x, const double* y,
  * selected pairs.  rematom = NULL returns to the standard kernel. */
 int orac_gpu_set_rem(orac_gpu_ctx* ctx, const int* rematom, int kind,
                      double rem_factor);
+/* A new rem_factor(3) for the context's REM segment, enqueued on `stream`
+ * (NULL: the context's own) so that it takes effect between steps in
+ * stream order: the pair kernel reads it from device memory, so a replica
+ * exchange needs no graph capture (no counterpart in the reference, whose
+ * replicas keep rem_factor in a module variable). */
+int orac_gpu_set_rem_factor_async(orac_gpu_ctx* ctx, double rem_factor,
+                                  void* stream);
 
 /* orac_gpu_set_alchemy: force_alchemy (src/force_alchemy.f), soft-core
  * GROMOS-like form.  ss_alchemy[ntap] (cpropar): 1 normal, 2 added, -2
@@ -401,6 +408,25 @@ int orac_gpu_batch_run(orac_gpu_batch* b, int nsteps);
 /* The same with an energy record (orac_gpu_md_records) of every system on
  * every energy_every-th step (0: none), each a captured energy step. */
 int orac_gpu_batch_run_energy(orac_gpu_batch* b, int nsteps, int energy_every);
+/* Every member's rem_factor(3) (factors[k] for member k), on the batch's
+ * stream. */
+int orac_gpu_batch_set_rem_factors(orac_gpu_batch* b, const double* factors);
+
+/* Replica exchange: ORAC's decision (rem_exchange, src/rem.f90:371-537) for
+ * n replicas over the n ensembles of a scaling ladder (ladder[e] =
+ * rem_factor(3) of ensemble e).  ens[r] is the 0-based ensemble replica r
+ * runs (a permutation; updated in place), pot[r] its segment energy (record
+ * column 15 of its last energy step) and kT in the same units.  On
+ * exchange step step_rem the pairs (p, p + 1) with p + 1 + step_rem odd
+ * attempt a swap: delta = (ladder[p+1] - ladder[p]) (pot of the replica at
+ * p + 1 - pot of the replica at p) / kT, accepted when delta >= 0 or
+ * random <= exp(delta), one random number in [0, 1) for all pairs (ORAC's
+ * broadcast one).  accepted[p] (may be NULL) is 1 where pair (p, p + 1)
+ * swapped.  Host only: every rank of a multi-GPU run reaches the same
+ * decision from the all-gathered energies. */
+int orac_gpu_rem_exchange(int n, const double* ladder, int* ens,
+                          const double* pot, double kT, long long step_rem,
+                          double random, int* accepted);
 int orac_gpu_batch_sync(orac_gpu_batch* b);
 int orac_gpu_batch_destroy(orac_gpu_batch* b);
 const char* orac_gpu_batch_last_error(const orac_gpu_batch* b);

@@ -161,7 +161,7 @@ void variant_fill(const orac_gpu_ctx* ctx, PairArgs* a) {
   if (ctx->variant == VAR_STD) return;
   a->vflag = ctx->d_vflag;
   a->rem_kind = ctx->rem_kind;
-  a->rem_factor = (float)ctx->rem_factor;
+  a->remf = ctx->d_remf;
   if (ctx->variant == VAR_ALCH) {
     a->soft = ctx->d_soft;
     a->softd = ctx->d_softd;
@@ -225,7 +225,7 @@ int alch_listqq_build(orac_gpu_ctx* ctx) {
 
 void variant_free(orac_gpu_ctx* ctx) {
   void* p[] = {ctx->d_vflag, ctx->d_soft, ctx->d_softd, ctx->d_qc, ctx->d_q0, ctx->d_xtra, ctx->d_dq,
-               ctx->d_lam4, ctx->d_listqq};
+               ctx->d_lam4, ctx->d_listqq, ctx->d_remf};
   for (void* q : p)
     if (q) dev_free(ctx, q);
 }
@@ -249,8 +249,25 @@ int orac_gpu_set_rem(orac_gpu_ctx* ctx, const int* rematom, int kind, double rem
   for (int a = 0; a < ctx->N; a++) ctx->h_rem[a] = rematom[a] ? 1 : 0;
   ctx->rem_kind = kind;
   ctx->rem_factor = rem_factor;
+  {
+    const float f = (float)rem_factor;
+    if (!ctx->d_remf && dev_alloc(ctx, &ctx->d_remf, 1)) return ORAC_ERR_CUDA;
+    CK(cudaMemcpy(ctx->d_remf, &f, sizeof(float), cudaMemcpyHostToDevice));
+  }
   if (int rc = build_vflag(ctx)) return rc;
   ctx->variant = VAR_REM;
+  return ORAC_OK;
+}
+
+int orac_gpu_set_rem_factor_async(orac_gpu_ctx* ctx, double rem_factor, void* stream) {
+  if (!ctx) return ORAC_ERR_PARAM;
+  if (ctx->variant != VAR_REM || !ctx->d_remf) return ctx_fail(ctx, ORAC_ERR_STATE, "orac_gpu_set_rem first");
+  if (!(rem_factor >= 0.0)) return ctx_fail(ctx, ORAC_ERR_PARAM, "rem_factor %g", rem_factor);
+  CK(cudaSetDevice(ctx->device));
+  ctx->rem_factor = rem_factor;
+  ctx->h_remf = (float)rem_factor;  // staged: the copy reads it when the stream gets there
+  CK(cudaMemcpyAsync(ctx->d_remf, &ctx->h_remf, sizeof(float), cudaMemcpyHostToDevice,
+                     stream ? (cudaStream_t)stream : ctx->stream));
   return ORAC_OK;
 }
 

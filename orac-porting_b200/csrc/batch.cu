@@ -8,6 +8,8 @@
 #include "common.cuh"
 #include "tune.cuh"
 
+#include <cmath>
+
 struct MdState;
 
 // md.cu: captured step graph of a context (kind bit 0: the step updates the
@@ -224,5 +226,48 @@ int orac_gpu_batch_sync(orac_gpu_batch* b) {
 }
 
 void* orac_gpu_batch_stream(orac_gpu_batch* b) { return b ? (void*)b->stream : nullptr; }
+
+// The rem_factor(3) of every member on the batch's stream (ordered with its
+// step graphs): what a replica exchange changes.
+int orac_gpu_batch_set_rem_factors(orac_gpu_batch* b, const double* factors) {
+  if (!b || !factors) return ORAC_ERR_PARAM;
+  if (cudaSetDevice(b->device) != cudaSuccess) return bfail(b, ORAC_ERR_CUDA, "cudaSetDevice");
+  for (size_t k = 0; k < b->ctx.size(); k++)
+    if (int rc = orac_gpu_set_rem_factor_async(b->ctx[k], factors[k], b->stream))
+      return bfail(b, rc, orac_gpu_last_error(b->ctx[k]));
+  return ORAC_OK;
+}
+
+// ORAC's replica-exchange decision (rem_exchange, src/rem.f90:371-537) for
+// n replicas and n ensembles of the scaling ladder.  On exchange step
+// step_rem the pairs of ensembles (p, p + 1) whose 1-based lower index plus
+// step_rem is odd attempt a swap; with pot the replicas' segment energies
+// and kT in the same units, delta = (ladder[p+1] - ladder[p]) (pot of the
+// replica at p + 1 - pot of the replica at p) / kT, accepted when delta >= 0
+// or random <= exp(delta) -- one random number for every pair, as ORAC's
+// root broadcasts one.  An accepted pair trades ensembles.
+int orac_gpu_rem_exchange(int n, const double* ladder, int* ens, const double* pot, double kT, long long step_rem,
+                          double random, int* accepted) {
+  if (n < 1 || !ladder || !ens || !pot || !(kT > 0.0)) return ORAC_ERR_PARAM;
+  std::vector<int> rep_of(n, -1);
+  for (int r = 0; r < n; r++) {
+    if (ens[r] < 0 || ens[r] >= n || rep_of[ens[r]] >= 0) return ORAC_ERR_PARAM;  // not a permutation
+    rep_of[ens[r]] = r;
+  }
+  for (int p = 0; p + 1 < n; p++) {
+    if (accepted) accepted[p] = 0;
+    if (((step_rem + p + 1) & 1LL) == 0) continue;  // ensemble p + 1 (1-based p) is no lower partner now
+    const int lo = rep_of[p], hi = rep_of[p + 1];
+    const double delta = (ladder[p + 1] - ladder[p]) * (pot[hi] - pot[lo]) / kT;
+    if (delta >= 0.0 || random <= std::exp(delta)) {
+      ens[lo] = p + 1;
+      ens[hi] = p;
+      rep_of[p] = hi;
+      rep_of[p + 1] = lo;
+      if (accepted) accepted[p] = 1;
+    }
+  }
+  return ORAC_OK;
+}
 
 }  // extern "C"

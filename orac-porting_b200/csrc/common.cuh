@@ -129,7 +129,9 @@ struct PairArgs {
   int variant;
   const unsigned char* vflag;  // [N]
   int rem_kind;
-  float rem_factor;
+  // rem_factor(3) in device memory: a replica exchange rewrites it without
+  // capturing the step graphs again
+  const float* remf;
   // alchemy: per-atom (rmin, 2 sqrt(epsm)) in FP32, (rmin, epsm) in FP64
   const float2* soft;
   const double2* softd;
@@ -316,6 +318,8 @@ struct orac_gpu_ctx {
   std::vector<unsigned char> h_vflag;
   int rem_kind = 0;
   double rem_factor = 1.0;
+  float* d_remf = nullptr;  // [1] rem_factor on the device (the pair kernel reads it)
+  float h_remf = 1.0f;      // host copy staged for orac_gpu_set_rem_factor_async
   float2* d_soft = nullptr;    // [N]
   double2* d_softd = nullptr;  // [N]
   AlchTables at{};
@@ -479,6 +483,25 @@ int small_launch(orac_gpu_ctx* ctx, int kind, const double* d_xyz,
 int self_launch(orac_gpu_ctx* ctx, const int* d_ss, double* d_e);
 int alch_intra_launch(orac_gpu_ctx* ctx, int kind, const double* d_xyz, unsigned long long* d_ffix, double* d_e,
                       double* d_edq);
+// one short list of small_launch_set (kinds of k_small: 0 fnb14, 1 fnbgrp,
+// 2 ferrf, 3 fnb14_alchemy, 4 ferrf_alchemy_add)
+struct SmallSpec {
+  int kind;
+  const double* xyz;
+  const int* pairs;
+  const int* ptype;
+  int npairs;
+  const double* t12;
+  const double* t6;
+  double fudge, lj_fudge;
+  int coul_mode;
+  double* e;
+  const int* ss;
+  const double* q;
+  unsigned long long* ffix;
+  double* edq;
+};
+int small_launch_set(orac_gpu_ctx* ctx, int n, const SmallSpec* specs);
 int alch_listqq_build(orac_gpu_ctx* ctx);
 // the same with explicit charges (null: the topology's) and an optional
 // fixed-point force output (the MD driver's level accumulators)

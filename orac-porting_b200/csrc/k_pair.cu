@@ -341,6 +341,7 @@ __global__ void __launch_bounds__(WPB * 32, MINB) k_pair(const PairArgs A) {
   const float2* lj = staged ? s_lj : A.lj;
   // under lskip_ewald an atom without LJ has no pair to evaluate
   const bool ljonly = VAR != VAR_ALCH && A.lskip && A.ewald;
+  const float remf = VAR == VAR_REM ? __ldg(A.remf) : 1.f;  // rem_factor(3)
   // this segment's bits of a warp ballot
   auto segbits = [&](unsigned b) -> unsigned { return SEG == 1 ? b : (b >> seg0) & 0xffffu; };
 
@@ -597,9 +598,9 @@ __global__ void __launch_bounds__(WPB * 32, MINB) k_pair(const PairArgs A) {
             // force_rem (src/force_REM.f:491-495,634-678): selected pairs scale
             // their force and their share of the S'V sum
             const bool sel = (VAR == VAR_REM) && seg_sel(A.rem_kind, s_fi[q][a], fjb);
-            vpart += sel ? (conf + coul) * A.rem_factor : conf + coul;
+            vpart += sel ? (conf + coul) * remf : conf + coul;
             qf *= dcs.w;
-            if (sel) qf *= A.rem_factor;
+            if (sel) qf *= remf;
             if (EN) {
               const double erx = cd.x + ((double)ai.x - (double)ob.x);
               const double ery = cd.y + ((double)ai.y - (double)ob.y);

@@ -335,6 +335,28 @@ int ferrf_launch_lists(orac_gpu_ctx* ctx, int nlist, const int* const* d_pairs, 
   return ORAC_OK;
 }
 
+// Up to MAX_SEGS short lists of any kinds in one launch (blockIdx.y the
+// list), each with its own fixed-point accumulator, energy slots and
+// dU/dlambda slot: the N1 level's 1-4 and intra-group pairs and, on M
+// steps, ferrf_alchemy_add's listqq share one launch.
+int small_launch_set(orac_gpu_ctx* ctx, int n, const SmallSpec* specs) {
+  SmallSegs S;
+  memset(&S, 0, sizeof(S));
+  int ns = 0, nmax = 0;
+  for (int k = 0; k < n && ns < MAX_SEGS; k++) {
+    const SmallSpec& p = specs[k];
+    if (p.npairs <= 0) continue;
+    S.s[ns] = small_args(ctx, p.kind, p.xyz, p.pairs, p.ptype, p.npairs, p.t12, p.t6, p.fudge, p.lj_fudge,
+                         p.coul_mode, 1, nullptr, p.e, p.ss, p.q, p.ffix, nullptr, p.edq);
+    ns++;
+    nmax = p.npairs > nmax ? p.npairs : nmax;
+  }
+  if (ns == 0) return ORAC_OK;
+  orac_launch(k_small_segs, dim3((nmax + 255) / 256, ns), dim3(256), 0, ctx->stream, S);
+  CKL();
+  return ORAC_OK;
+}
+
 // fnb14_alchemy over the 1-4 list (kind 3) or ferrf_alchemy_add over listqq
 // (kind 4), forces into the fixed-point accumulator, energies into d_e (4
 // or 2 slots), dU/dlambda into d_edq

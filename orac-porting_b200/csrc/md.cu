@@ -974,9 +974,10 @@ __global__ void k_rattle_big(const ConsArgs A) {
 // orac_gpu_md_run returns) into the context's ring: [0] record number,
 // [1] kinetic, [2..7] M, L, H LJ and Coulomb, [8] SPME, [9] the constant
 // (self energy), [10] total, [11] status flags, [12] bonded, [13] 1-4 and
-// intra-group pairs, [14] erf corrections, [15] dU/dlambda.
+// intra-group pairs, [14] erf corrections, [15] dU/dlambda (alchemy) or the
+// REM segment's nonbonded energy (REM).
 __global__ void k_record(const double* __restrict__ e, const int* __restrict__ flag, double econst, double self_dudl,
-                         int alch, double* __restrict__ ring, int cap, unsigned long long* __restrict__ n) {
+                         int var, double* __restrict__ ring, int cap, unsigned long long* __restrict__ n) {
   pdl_enter();
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   const unsigned long long k = *n;
@@ -996,9 +997,11 @@ __global__ void k_record(const double* __restrict__ e, const int* __restrict__ f
   for (int q = 49; q < 57; q++) p += e[q];  // 1-4 and intra-group (E_14..E_ERF)
   for (int q = 57; q < 73; q++) c += e[q];  // erf corrections (E_ERF..E_DUDL)
   c += e[80] + e[81];                       // ferrf_alchemy_add (E_AQQ)
-  if (alch) {
+  if (var == 2) {  // alchemy: dU/dlambda of every term
     for (int q = 73; q < 80; q++) d += e[q];
     d += self_dudl;
+  } else if (var == 1) {  // REM: the segment energy of the three shells (rem_pot(3))
+    for (int q = 73; q < 76; q++) d += e[q];
   }
   r[12] = b;
   r[13] = p;
@@ -1292,6 +1295,8 @@ static int md_shell_pair(orac_gpu_ctx* ctx, MdState& S, char sh, int lvl, bool z
   const bool dudl = energy && ctx->variant == VAR_ALCH && ctx->d_dq;
   if (dudl)  // the shell's dU/dlambda (k_variant_out)
     CK(cudaMemcpyAsync(S.e + E_DUDL + lvl, ctx->d_xtra + 4, sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+  if (energy && ctx->variant == VAR_REM)  // the shell's REM segment energy (seg_ene)
+    CK(cudaMemcpyAsync(S.e + E_DUDL + lvl, ctx->d_xtra, sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
   return ORAC_OK;
 }
 
@@ -1350,34 +1355,41 @@ static bool md_alch_intra(const orac_gpu_ctx* ctx) {
   return ctx->variant == VAR_ALCH && ctx->clewld && ctx->d_lam4;
 }
 
-// ferrf_alchemy_add over listqq after the M shell (src/mtsmd.f:3035-3041)
+// The N1 level's pair terms (fnb14 -- fnb14_alchemy with alchemy and Ewald,
+// src/mts_intra_n1.f:81-85 -- and fnbgrp) in one launch, and, when the step
+// ends an M step too (with_m), ferrf_alchemy_add over listqq into the M
+// accumulator (src/mtsmd.f:3035-3041): every M step is an N1 step, so the
+// correction costs no launch of its own.
+static int md_pairs_n1(orac_gpu_ctx* ctx, MdState& S, bool energy, bool with_m = false) {
+  const BondedDev& B = ctx->bd;
+  SmallSpec sp[3];
+  int n = 0;
+  const int coul = ctx->clewld ? 1 : 0;
+  const bool alch = md_alch_intra(ctx);
+  if (B.have_pairs && B.n14 > 0)
+    sp[n++] = {alch ? 3 : 0, S.x, B.p14, B.t14, B.n14, B.e1412, B.e146, B.fudge, B.lj_fudge, coul,
+               energy ? S.e + E_14 : nullptr, B.ss, ctx->d_aqd, S.ffix[LN1],
+               (alch && energy) ? S.e + E_DUDL + 5 : nullptr};
+  if (B.have_pairs && B.ningrp > 0)
+    sp[n++] = {1, S.x, B.pgrp, B.nbt, B.ningrp, B.e12, B.e6, 1.0, 1.0, coul, energy ? S.e + E_GRP : nullptr, B.ss,
+               ctx->d_aqd, S.ffix[LN1], nullptr};
+  if (with_m && alch) {
+    if (ctx->nlistqq < 0)
+      if (int rc = alch_listqq_build(ctx)) return rc;
+    if (ctx->nlistqq > 0)
+      sp[n++] = {4, S.x, ctx->d_listqq, nullptr, ctx->nlistqq, nullptr, nullptr, 1.0, 1.0, 1,
+                 energy ? S.e + E_AQQ : nullptr, B.ss, ctx->d_aqd, S.ffix[LM], energy ? S.e + E_DUDL + 6 : nullptr};
+  }
+  return small_launch_set(ctx, n, sp);
+}
+
+// ferrf_alchemy_add on an M step of a system without N1 pair terms
 static int md_alch_m(orac_gpu_ctx* ctx, MdState& S, bool energy) {
-  if (!md_alch_intra(ctx)) return ORAC_OK;
+  if (!md_alch_intra(ctx) || S.has_n1) return ORAC_OK;
   if (ctx->nlistqq < 0)
     if (int rc = alch_listqq_build(ctx)) return rc;
   return alch_intra_launch(ctx, 4, S.x, S.ffix[LM], energy ? S.e + E_AQQ : nullptr,
                            energy ? S.e + E_DUDL + 6 : nullptr);
-}
-
-static int md_pairs_n1(orac_gpu_ctx* ctx, MdState& S, bool energy) {
-  const BondedDev& B = ctx->bd;
-  if (B.have_pairs) {
-    const int coul = ctx->clewld ? 1 : 0;
-    if (B.n14 > 0 && md_alch_intra(ctx)) {
-      // fnb14_alchemy in place of fnb14 (src/mts_intra_n1.f:81-85)
-      if (int rc = alch_intra_launch(ctx, 3, S.x, S.ffix[LN1], energy ? S.e + E_14 : nullptr,
-                                     energy ? S.e + E_DUDL + 5 : nullptr))
-        return rc;
-    } else if (B.n14 > 0)
-      if (int rc = small_launch_x(ctx, 0, S.x, B.p14, B.t14, B.n14, B.e1412, B.e146, B.fudge, B.lj_fudge, coul, 1,
-                                  nullptr, energy ? S.e + E_14 : nullptr, B.ss, nullptr, S.ffix[LN1]))
-        return rc;
-    if (B.ningrp > 0)
-      if (int rc = small_launch_x(ctx, 1, S.x, B.pgrp, B.nbt, B.ningrp, B.e12, B.e6, 1.0, 1.0, coul, 1, nullptr,
-                                  energy ? S.e + E_GRP : nullptr, B.ss, nullptr, S.ffix[LN1]))
-        return rc;
-  }
-  return ORAC_OK;
 }
 
 // the bonded terms of the N0 level (stretching, bending, impropers) and/or
@@ -1390,7 +1402,7 @@ static int md_bonded(orac_gpu_ctx* ctx, MdState& S, bool n0, bool n1, bool energ
 
 static int md_forces_intra(orac_gpu_ctx* ctx, MdState& S, int lvl, bool energy) {
   if (int rc = md_bonded(ctx, S, lvl == LN0, lvl == LN1, energy)) return rc;
-  return lvl == LN1 ? md_pairs_n1(ctx, S, energy) : ORAC_OK;
+  return lvl == LN1 ? md_pairs_n1(ctx, S, energy, true) : ORAC_OK;
 }
 
 static int md_phony(orac_gpu_ctx* ctx, const ShellRadii& r, char sh) {
@@ -1471,13 +1483,13 @@ static int md_step(orac_gpu_ctx* ctx, MdState& S, bool update, bool energy) {
     }
     if (due_m) {
       if (int rc = md_shell_pair(ctx, S, 'm', LM, false, S.e, e_now)) return rc;
-      if (int rc = md_alch_m(ctx, S, e_now)) return rc;
+      if (int rc = md_alch_m(ctx, S, e_now)) return rc;  // only without N1 pairs (else with them)
     }
     if (due_l)
       if (int rc = md_shell_pair(ctx, S, 'l', LL, false, S.e + 8, e_now)) return rc;
     // the N1 level's pair terms beside the bonded kernel on the side stream
     if (due_n1)
-      if (int rc = md_pairs_n1(ctx, S, e_now)) return rc;
+      if (int rc = md_pairs_n1(ctx, S, e_now, due_m)) return rc;
     if (side)
       if (int rc = sd.join()) return rc;
   }
@@ -1504,7 +1516,8 @@ static int md_step(orac_gpu_ctx* ctx, MdState& S, bool update, bool energy) {
     orac_launch(k_ekin, 64, 256, 0, ctx->stream, ctx->N, S.v, S.invm, S.e + 40);
     CKL();
     orac_launch(k_record, 1, 32, 0, ctx->stream, S.e, S.flag, S.econst, ctx->self_dudl,
-                (ctx->variant == VAR_ALCH && ctx->d_dq) ? 1 : 0, S.rec, S.rec_cap, S.rec_n);
+                (ctx->variant == VAR_ALCH && ctx->d_dq) ? 2 : (ctx->variant == VAR_REM ? 1 : 0), S.rec, S.rec_cap,
+                S.rec_n);
     CKL();
   }
   return ORAC_OK;
@@ -1817,7 +1830,7 @@ int orac_gpu_md_setup(orac_gpu_ctx* ctx, const double* x, const double* y, const
   }
   if (ctx->variant == VAR_ALCH) ctx->nlistqq = -1;  // built with this setup's constraints
   if (int rc = md_forces_shell(ctx, S, 'm', LM, true, S.e, true)) return rc;
-  if (int rc = md_alch_m(ctx, S, false)) return rc;
+  if (int rc = md_alch_m(ctx, S, false)) return rc;  // (systems without N1 pairs; else with the N1 level below)
   if (int rc = md_forces_shell(ctx, S, 'l', LL, true, S.e + 8, true)) return rc;
   if (int rc = md_forces_shell(ctx, S, 'h', LH, true, S.e + 16, true)) return rc;
   for (int l = LN1; l <= LN0; l++) {
@@ -2044,6 +2057,8 @@ static int md_run_impl(orac_gpu_ctx* ctx, int nsteps, int energy_every, double* 
       r[14] += e[E_AQQ] + e[E_AQQ + 1];
       // dU/dlambda of the alchemical windows: shells, PME, erf corrections,
       // fnb14_alchemy, ferrf_alchemy_add, self term
+      if (ctx->variant == VAR_REM)  // REM: the shells' segment energy (rem_pot(3))
+        for (int q = E_DUDL; q < E_DUDL + 3; q++) r[15] += e[q];
       if (ctx->variant == VAR_ALCH && ctx->d_dq) {
         for (int q = E_DUDL; q < E_DUDL + 7; q++) r[15] += e[q];
         r[15] += ctx->self_dudl;

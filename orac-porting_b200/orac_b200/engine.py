@@ -298,6 +298,10 @@ class Engine:
         check(self.ctx, self.lib.orac_gpu_md_run(self.ctx, nsteps, energy_every, rec), "md_run")
         return rec[:nrec * R].reshape(-1, R)
 
+    def set_rem_factor_async(self, factor, stream=None):
+        """A new rem_factor(3), in stream order (orac_gpu_set_rem_factor_async)."""
+        check(self.ctx, self.lib.orac_gpu_set_rem_factor_async(self.ctx, float(factor), stream), "set_rem_factor_async")
+
     def set_pair_tuning(self, lpg_m=0, lpg_lh=0, minb=0):
         """Launch configuration of the real-space kernel (0: the mode's default)."""
         check(self.ctx, self.lib.orac_gpu_set_pair_tuning(self.ctx, lpg_m, lpg_lh, minb), "set_pair_tuning")
@@ -384,6 +388,12 @@ class Batch:
 
     def sync(self):
         self._check(self.lib.orac_gpu_batch_sync(self.h), "batch_sync")
+
+    def set_rem_factors(self, factors):
+        """Every member's rem_factor(3), on the batch's stream
+        (orac_gpu_batch_set_rem_factors)."""
+        self._check(self.lib.orac_gpu_batch_set_rem_factors(self.h, np.ascontiguousarray(factors, dtype=np.float64)),
+                    "batch_set_rem_factors")
 
     def tune(self, trial=6, cache=None, force=False):
         """Autotune the real-space kernel on the batched steps

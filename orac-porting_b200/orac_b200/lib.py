@@ -88,6 +88,9 @@ def load():
         "orac_gpu_batch_create": (i, [C.POINTER(_P), i, C.POINTER(_P)]),
         "orac_gpu_batch_run": (i, [_P, i]),
         "orac_gpu_batch_run_energy": (i, [_P, i, i]),
+        "orac_gpu_batch_set_rem_factors": (i, [_P, _D]),
+        "orac_gpu_set_rem_factor_async": (i, [_P, d, _P]),
+        "orac_gpu_rem_exchange": (i, [i, _D, _I, _D, d, C.c_longlong, d, _I]),
         "orac_gpu_md_records": (i, [_P, i, _P, C.POINTER(i64), i]),
         "orac_gpu_batch_sync": (i, [_P]),
         "orac_gpu_batch_destroy": (i, [_P]),
