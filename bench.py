@@ -74,7 +74,7 @@ def f0_system():
 F0_WORKLOAD = dict(build=f0_system, dt_h=15.0, lrespa=5, mrespa=2, n1respa=2, n0respa=2, nupdte=6, rshk="l")
 DUDL_STEPS, DUDL_EVERY = 400, 2  # dU/dlambda sampling of the batched windows
 SERVE_PLAIN_SAMPLE = 8  # serving requests also run one at a time, to check the plain model
-HREM_N, HREM_EVERY, HREM_INTERVALS = 16, 15, 6  # replica-exchange leg
+HREM_N, HREM_EVERY, HREM_INTERVALS = 16, 15, 10  # replica-exchange leg
 # the pair-kernel autotuner's choices per device and workload shape
 TUNE_CACHE = os.path.join(ROOT, "orac-porting_b200", "orac_b200", "pair_tuning.txt")
 TUNE_TRIAL = 6
@@ -412,6 +412,10 @@ def gpu_arm(args, wl, s, device):
     res["bytes_io"] = 6 * n * 8
     res["G"], res["N"] = s.ngrp, s.ntap
     res["shell_evals"] = args.steps * (1 + wl["lrespa"] + wl["lrespa"] * wl["mrespa"])
+    try:
+        res["step_breakdown"] = step_breakdown(eng, flush, max(5, min(args.steps, 20)))
+    except Exception as exc:
+        res["step_breakdown"] = {"error": f"{type(exc).__name__}: {exc}"}
     xs, _ = eng.md_state()
     eng.close()
     try:
@@ -458,6 +462,55 @@ def gpu_arm(args, wl, s, device):
     return res
 
 
+PROF_FAMILIES = ("pair", "drift_kick", "spme", "bonded")
+
+
+def step_breakdown(eng, flush, nsteps):
+    """Device time per step of each kernel family, from CUDA events that
+    bracket every launch of the family inside the captured step graphs (the
+    pair kernel, the drift and kick kernels, one SPME evaluation from spread
+    to gather, the bonded kernel), over nsteps further steps after the timed
+    ones, L2 flushed before each.  The SPME evaluations run on the step's
+    second stream, beside the pair kernels: the families' times can add up
+    to more than the step."""
+    import ctypes as C
+
+    import torch
+
+    L = eng.lib
+    L.orac_gpu_prof_enable(eng.ctx, (1 << len(PROF_FAMILIES)) - 1)
+    stream = torch.cuda.ExternalStream(L.orac_gpu_get_stream(eng.ctx), device=flush.device)
+    for _ in range(2):  # captures the instrumented graphs
+        L.orac_gpu_md_run_async(eng.ctx, 1)
+        L.orac_gpu_md_collect(eng.ctx)
+    L.orac_gpu_prof_read(eng.ctx, None, None, 1)
+    status = []
+
+    def one():
+        # the events of a replayed step graph are read when the step is collected
+        L.orac_gpu_md_run_async(eng.ctx, 1)
+        status.append(L.orac_gpu_md_collect(eng.ctx))
+
+    step_ms = _timed_steps(one, stream, flush, nsteps)
+    if any(status):
+        raise RuntimeError(L.orac_gpu_last_error(eng.ctx).decode())
+    out = {"steps": nsteps, "ms_per_step": sum(step_ms) / nsteps,
+           "how": "CUDA events recorded as graph nodes around each launch of the family (the event nodes break the "
+                  "launches' programmatic overlap, so this step is a little slower than the timed one)"}
+    for f, name in enumerate(PROF_FAMILIES):
+        ms = C.c_double()
+        n = C.c_int64()
+        L.orac_gpu_prof_read_family(eng.ctx, f, C.byref(ms), C.byref(n), 0)
+        if n.value < 0:
+            out[name] = {"error": "some event pairs could not be timed"}
+            continue
+        out[name] = {"ms_per_step": ms.value / nsteps, "launches_per_step": n.value / nsteps,
+                     "us_per_launch": 1e3 * ms.value / n.value if n.value else None,
+                     "share_of_step": ms.value / sum(step_ms) if step_ms else None}
+    L.orac_gpu_prof_enable(eng.ctx, 0)
+    return out
+
+
 def _timed_steps(run_one, stream, flush, steps):
     """CUDA-event time of each of `steps` calls of run_one on `stream`, L2
     flushed before each."""
@@ -477,15 +530,28 @@ def _timed_steps(run_one, stream, flush, steps):
     return out
 
 
+def window_lambdas(lam):
+    """The two-stage removal path of ORAC's NE runs (test3/test4's schedule
+    switches the charges off first, then the LJ): control lambda in [0, 0.5]
+    takes lrmq from 0 to 1 with lrm = 0, lambda in [0.5, 1] takes lrm from
+    0 to 1 with the charges off.  (ladd, lrm, laddq, lrmq) and their
+    derivatives with respect to lambda."""
+    if lam <= 0.5:
+        return (0.0, 0.0, 0.0, 2.0 * lam), [0.0, 0.0, 0.0, 2.0]
+    return (0.0, 2.0 * lam - 1.0, 0.0, 1.0), [0.0, 2.0, 0.0, 0.0]
+
+
 def window_engine(base, k, nwin, device, wl):
-    """Lambda window k: the ligand removed at lambda = k / (nwin - 1) (lrm =
-    lrmq = lambda, soft core 0.5 0.5), dU/dlambda of that control lambda."""
+    """Lambda window k at lambda = k / (nwin - 1) on the two-stage removal
+    path (window_lambdas; soft core 0.5 0.5), dU/dlambda of that control
+    lambda."""
     from orac_b200.engine import Engine
 
     lam = k / (nwin - 1)
     e = Engine(base.copy(), device=device)
     e.set_alchemy(base.ss_alchemy, 0.5, 0.5)
-    e.set_lambda(0.0, lam, 0.0, lam, dlam=[0.0, 1.0, 0.0, 1.0])
+    lv, dl = window_lambdas(lam)
+    e.set_lambda(*lv, dlam=dl)
     e.md_setup(wl["dt_h"], wl["lrespa"], wl["mrespa"], wl["nupdte"], wl["rshk"], econst=0.0)
     return e, lam
 
@@ -493,7 +559,7 @@ def window_engine(base, k, nwin, device, wl):
 def batch_arm(args, wl, s, device, flush):
     """The alchemical lambda-window batch: `args.batch` windows of the
     40-atom ligand in the liquid water box (lambda_k = k / (B - 1) on the
-    ligand's LJ and charges) advanced by one graph launch per outer step
+    two-stage removal path: charges, then LJ) advanced by one graph launch per outer step
     (orac_gpu_batch_run); the plain reference is one window alone on the
     same driver.  Every window ends with an energy step that yields its
     dU/dlambda."""
@@ -770,8 +836,9 @@ def f0_arm(args, device, flush):
 
 def hrem_arm(args, wl, device):
     """Hamiltonian replica exchange as ORAC's test2 runs it, batched on one
-    GPU: HREM_N replicas of one solvated-chain system (about 20k atoms,
-    solute 8%), solute scaling on a geometric ladder from 1 to 0.3
+    GPU: HREM_N replicas of one solvated-chain system (about 20k atoms, a
+    70-atom solute chain, the size of test2's ligand + TYR27 segment),
+    solute scaling on a geometric ladder from 1 to 0.6 as in test2
     (rem_factor(3) on the pairs touching the solute, seg_select kind 0),
     300 K, an exchange attempt every 15 steps (60 fs) by ORAC's rule on
     the replicas' segment energies recorded on the device.  Timed by wall
@@ -781,8 +848,8 @@ def hrem_arm(args, wl, device):
 
     from orac_b200 import hrem
 
-    s = systems.solvated_chains(20000, 4242, solute_frac=0.08, name="hrem20k")
-    ladder = hrem.ladder_geometric(HREM_N, 0.3)
+    s = systems.solvated_chains(20000, 4242, solute_frac=70 / 20000, name="hrem20k")
+    ladder = hrem.ladder_geometric(HREM_N, 0.6)
     kT = units.BOLTZ * 300.0 / units.UNITE
 
     def make(f):
@@ -819,7 +886,7 @@ def hrem_arm(args, wl, device):
     val = ns_per_day(steps * HREM_N, wl["dt_h"], secs)
     pval = ns_per_day(steps, wl["dt_h"], plain_s)
     return {"workload": f"{HREM_N} replicas of one solvated-chain system ({s.ntap} atoms, solute {int(s.rematom.sum())} "
-                        "atoms), solute scaling 1..0.3 geometric as rem_factor(3) (seg_select kind 0), 300 K, "
+                        "atoms), solute scaling 1..0.6 geometric as rem_factor(3) (seg_select kind 0), 300 K, "
                         f"exchange attempts every {HREM_EVERY} steps ({HREM_EVERY * wl['dt_h']:g} fs)",
             "replicas": HREM_N, "value": val, "unit": "ns/day (aggregate over replicas)",
             "plain_value": pval, "speedup_vs_plain": val / pval, "exchanges": HREM_INTERVALS + 1,
@@ -1101,7 +1168,7 @@ def main():
                     "how": "orac_gpu_md_set_state (pinned host -> device), one step, orac_gpu_md_get_state "
                            "(device -> pinned host, with the status flags), orac_gpu_md_collect, wall clock"},
                gpu_launches=res["launches"], clocks=res["clocks"], tuning=res["tuning"])
-    for key in ("force_check", "energy_conservation"):
+    for key in ("force_check", "energy_conservation", "step_breakdown"):
         if key in res:
             out[key] = res[key]
     if "batched" in res:
@@ -1116,7 +1183,8 @@ def main():
         wts[1:] += 0.5 * np.diff(lam)
         wts[:-1] += 0.5 * np.diff(lam)
         out["batched"] = {
-            "workload": f"{bt['systems']} alchemical lambda windows (lambda_k = k/{bt['systems'] - 1}) of a 40-atom "
+            "workload": f"{bt['systems']} alchemical lambda windows (lambda_k = k/{bt['systems'] - 1}, charges "
+                        "then LJ switched off) of a 40-atom "
                         f"flexible ligand in the liquid water box ({bt['atoms_per_window']} atoms per window), "
                         "soft-core force_alchemy, SPME of the scaled charges, bonded N0/N1 levels",
             "systems": bt["systems"], "value": bval, "unit": "ns/day (aggregate over windows)",
@@ -1130,10 +1198,10 @@ def main():
                            "how": f"energy records on the device every {DUDL_EVERY} steps of a batched run of "
                                   f"{DUDL_STEPS} steps (orac_gpu_batch_run_energy) after the timed steps; mean and "
                                   "standard error from 10 block means per window",
-                           "note": "the workload scales the ligand's LJ and charges by the same lambda; past "
-                                   "lambda ~0.2 the soft core (qsoft lambda^2) no longer keeps water charges off "
-                                   "the ligand's, and dU/dlambda grows to 1e4 kJ/mol: the estimate is not a "
-                                   "converged free energy"},
+                           "note": "lambda in [0, 0.5] switches the ligand's charges off (lrmq = 2 lambda), "
+                                   "[0.5, 1] its LJ (lrm = 2 lambda - 1), ORAC's NE order; each window starts "
+                                   "from the same unequilibrated state and samples a few ps, so the sum is a "
+                                   "short-run estimate, not a converged free energy"},
             "tuning": bt["tuning"],
             "how": "one graph launch per H step advances every window (orac_gpu_batch_run); plain = one window "
                    "alone through the same driver; both with the real-space kernel's launch configuration chosen by "

@@ -496,12 +496,19 @@ void* orac_gpu_get_stream(orac_gpu_ctx* ctx);
  * scanned, entries kept for the next shell, atom pairs evaluated with Ewald,
  * atom pairs evaluated LJ-only. */
 int orac_gpu_counters(orac_gpu_ctx* ctx, int64_t* out4, int reset);
-/* With profiling on, every real-space kernel launch is bracketed by CUDA
- * events (also inside captured graphs); prof_read returns the summed device
- * time in ms and the number of launches timed. */
+/* Launch profiler: `on` is a mask of kernel families, bit 0 the real-space
+ * pair kernel, bit 1 the integrator's drift and kick kernels, bit 2 one SPME
+ * evaluation (spread to gather as one interval), bit 3 the bonded kernel
+ * (on = 1 profiles the pair kernel alone).  Each launch of a profiled
+ * family is bracketed by CUDA events, also inside captured graphs (a new
+ * mask captures the step graphs again).  prof_read returns the pair
+ * kernel's summed device time in ms and number of launches timed;
+ * prof_read_family the same for family 0..3.  reset clears every family. */
 int orac_gpu_prof_enable(orac_gpu_ctx* ctx, int on);
 int orac_gpu_prof_read(orac_gpu_ctx* ctx, double* ms_total, int64_t* nlaunch,
                        int reset);
+int orac_gpu_prof_read_family(orac_gpu_ctx* ctx, int family, double* ms_total,
+                              int64_t* nlaunch, int reset);
 
 /* FP32 FMA rate of `device` in TFLOP/s (an FMA counts 2), measured by an
  * FMA-loop kernel that fills every SM (best of three timed launches, about

@@ -579,24 +579,36 @@ int orac_gpu_counters(orac_gpu_ctx* ctx, int64_t* out4, int reset) {
 
 int orac_gpu_prof_enable(orac_gpu_ctx* ctx, int on) {
   if (!ctx) return ORAC_ERR_PARAM;
+  if (on < 0 || on >= (1 << PROF_NFAM)) return ctx_fail(ctx, ORAC_ERR_PARAM, "profile mask %d", on);
   if (on && ctx->prof_ev.empty()) {
-    ctx->prof_ev.resize(2048);
+    ctx->prof_ev.resize(4096);
+    ctx->prof_fam.assign(ctx->prof_ev.size() / 2, 0);
     for (auto& e : ctx->prof_ev) CK(cudaEventCreate(&e));
   }
-  ctx->prof = on != 0;
+  // the event records are nodes of the captured step graphs: a new mask
+  // captures them again
+  if (on != ctx->prof) ctx->param_gen++;
+  ctx->prof = on;
+  return ORAC_OK;
+}
+
+int orac_gpu_prof_read_family(orac_gpu_ctx* ctx, int family, double* ms_total, int64_t* nlaunch, int reset) {
+  if (!ctx) return ORAC_ERR_PARAM;
+  if (family < 0 || family >= PROF_NFAM) return ctx_fail(ctx, ORAC_ERR_PARAM, "profile family %d", family);
+  if (ms_total) *ms_total = ctx->prof_ms[family];
+  if (nlaunch) *nlaunch = ctx->prof_bad ? -1 : ctx->prof_n[family];  // -1: some launches could not be timed
+  if (reset) {
+    for (int f = 0; f < PROF_NFAM; f++) {
+      ctx->prof_ms[f] = 0;
+      ctx->prof_n[f] = 0;
+    }
+    ctx->prof_bad = false;
+  }
   return ORAC_OK;
 }
 
 int orac_gpu_prof_read(orac_gpu_ctx* ctx, double* ms_total, int64_t* nlaunch, int reset) {
-  if (!ctx) return ORAC_ERR_PARAM;
-  if (ms_total) *ms_total = ctx->prof_ms;
-  if (nlaunch) *nlaunch = ctx->prof_bad ? -1 : ctx->prof_n;  // -1: some launches could not be timed
-  if (reset) {
-    ctx->prof_ms = 0;
-    ctx->prof_n = 0;
-    ctx->prof_bad = false;
-  }
-  return ORAC_OK;
+  return orac_gpu_prof_read_family(ctx, PROF_PAIR, ms_total, nlaunch, reset);
 }
 
 int orac_gpu_stats(orac_gpu_ctx* ctx, int64_t* list_pairs, int64_t* launches) {

@@ -146,9 +146,11 @@ int orac_gpu_batch_run_energy(orac_gpu_batch* b, int nsteps, int energy_every) {
   return batch_run(b, nsteps, energy_every);
 }
 
-// Drop the parent graphs (built again on the next run from the members'
-// current step graphs) and take the members' parameter generations.
-static void batch_reset_graphs(orac_gpu_batch* b) {
+// Drop the parent graphs and take the members' parameter generations.
+// With `eager` the plain and list-update kinds are built again at once from
+// the members' current step graphs, so that no step of a later run pays for
+// a capture; otherwise each kind is built on its first use.
+static int batch_reset_graphs(orac_gpu_batch* b, bool eager) {
   cudaStreamSynchronize(b->stream);
   for (int k = 0; k < 4; k++) {
     if (b->exec[k]) cudaGraphExecDestroy(b->exec[k]);
@@ -157,6 +159,10 @@ static void batch_reset_graphs(orac_gpu_batch* b) {
     b->graph[k] = nullptr;
   }
   for (size_t k = 0; k < b->ctx.size(); k++) b->gen[k] = b->ctx[k]->param_gen;
+  if (eager)
+    for (int kind = 0; kind < 2; kind++)
+      if (int rc = build_kind(b, kind)) return rc;
+  return ORAC_OK;
 }
 
 // The autotuner on the batch: every candidate configuration (the same for
@@ -171,7 +177,7 @@ int orac_gpu_batch_tune(orac_gpu_batch* b, int trial, const char* cache_path, in
   double best_ms = 0.0;
   if (!force && tune_cache_find(cache_path, sig, &best, &best_ms)) {
     for (auto* c : b->ctx) tune_apply(c, best);
-    batch_reset_graphs(b);
+    if (int rc = batch_reset_graphs(b, true)) return rc;
   } else {
     int maxg = 0;
     for (auto* c : b->ctx) maxg = c->maxg > maxg ? c->maxg : maxg;
@@ -183,7 +189,7 @@ int orac_gpu_batch_tune(orac_gpu_batch* b, int trial, const char* cache_path, in
     int rc = ORAC_OK;
     for (const PairTune& c : cand) {
       for (auto* x : b->ctx) tune_apply(x, c);
-      batch_reset_graphs(b);
+      if ((rc = batch_reset_graphs(b, false))) break;
       if ((rc = batch_run(b, trial, 0)) || (rc = orac_gpu_batch_sync(b))) break;
       cudaEventRecord(e0, b->stream);
       if ((rc = batch_run(b, trial, 0))) break;
@@ -204,7 +210,7 @@ int orac_gpu_batch_tune(orac_gpu_batch* b, int trial, const char* cache_path, in
     cudaEventDestroy(e1);
     if (rc) return rc;
     for (auto* c : b->ctx) tune_apply(c, best);
-    batch_reset_graphs(b);
+    if (int rc2 = batch_reset_graphs(b, true)) return rc2;
     tune_cache_add(cache_path, sig, best, best_ms);
   }
   if (out3) {

@@ -38,6 +38,11 @@ enum {
   ACC_N = 27
 };
 
+// Kernel families that the launch profiler brackets with CUDA events: the
+// real-space pair kernel, the drift and kick kernels of the integrator, one
+// SPME evaluation (spread to gather, as one interval), the bonded kernel.
+enum { PROF_PAIR = 0, PROF_DRIFT = 1, PROF_PME = 2, PROF_BONDED = 3, PROF_NFAM = 4 };
+
 // Shell-kernel variants, the dispatch of src/mts_forces.f:118-153.
 enum { VAR_STD = 0, VAR_REM = 1, VAR_ALCH = 2 };
 
@@ -349,12 +354,13 @@ struct orac_gpu_ctx {
   // measurement: work counters of the pair kernel and CUDA events around
   // its launches (recorded into captured graphs as event nodes)
   unsigned long long* d_wcnt = nullptr;  // [4]
-  bool prof = false;
+  int prof = 0;           // mask of the profiled kernel families (PROF_*)
   bool prof_bad = false;  // an event pair could not be timed
   std::vector<cudaEvent_t> prof_ev;  // pairs (start, end)
+  std::vector<int> prof_fam;         // family of each slot
   int prof_next = 0;
-  double prof_ms = 0;
-  int64_t prof_n = 0;
+  double prof_ms[PROF_NFAM] = {0, 0, 0, 0};
+  int64_t prof_n[PROF_NFAM] = {0, 0, 0, 0};
 };
 
 // Bumps ctx->param_gen when it goes out of scope, once armed: a setter arms
@@ -370,10 +376,12 @@ struct ParamGenBump {
   }
 };
 
-// record the start/end events of one profiled launch (no-op unless prof)
-int prof_begin(orac_gpu_ctx* ctx, int* slot);
+// record the start/end events of one profiled launch of a family (no-op
+// unless that family is profiled)
+int prof_begin(orac_gpu_ctx* ctx, int* slot, int family = PROF_PAIR);
 int prof_end(orac_gpu_ctx* ctx, int slot);
-// sum the elapsed time of slots [a, b) into prof_ms / prof_n (after a sync)
+// sum the elapsed time of slots [a, b) into prof_ms / prof_n of their
+// families (after a sync)
 int prof_collect(orac_gpu_ctx* ctx, int a, int b);
 
 // shell-kernel variants (api_variant.cu)

@@ -917,11 +917,12 @@ static int prof_record(orac_gpu_ctx* ctx, cudaEvent_t ev) {
   return ORAC_OK;
 }
 
-int prof_begin(orac_gpu_ctx* ctx, int* slot) {
+int prof_begin(orac_gpu_ctx* ctx, int* slot, int family) {
   *slot = -1;
-  if (!ctx->prof) return ORAC_OK;
+  if (!(ctx->prof & (1 << family))) return ORAC_OK;
   if (2 * (ctx->prof_next + 1) > (int)ctx->prof_ev.size()) return ORAC_OK;  // pool exhausted: not profiled
   *slot = ctx->prof_next++;
+  ctx->prof_fam[*slot] = family;
   return prof_record(ctx, ctx->prof_ev[2 * *slot]);
 }
 
@@ -938,8 +939,9 @@ int prof_collect(orac_gpu_ctx* ctx, int a, int b) {
       ctx->prof_bad = true;
       continue;
     }
-    ctx->prof_ms += ms;
-    ctx->prof_n++;
+    const int f = ctx->prof_fam[s];
+    ctx->prof_ms[f] += ms;
+    ctx->prof_n[f]++;
   }
   return ORAC_OK;
 }

@@ -708,170 +708,229 @@ __device__ __forceinline__ void group_centre(const MolArgs& A, int gi) {
   }
 }
 
-// correc (v += f dt/2m) from the fixed-point level accumulators, then RATTLE.
+// correc (v += f dt/2m) from the fixed-point level accumulators, then RATTLE,
+// for one small molecule (W3: a rigid three-site one, in registers)
+template <bool W3>
+__device__ __forceinline__ void kick_molecule(const MolArgs& A, const int4 m) {
+  const int N = A.N;
+  const int na = W3 ? 3 : m.y;
+  int gat[SMA];
+  double im[SMA];
+#pragma unroll
+  for (int a = 0; a < SMA; a++) {
+    gat[a] = a < na ? sm_atom(A, m, a) : 0;
+    im[a] = a < na ? __ldg(&A.invm[gat[a]]) : 0.0;
+  }
+  pdl_enter();
+  double x[SMA][3], v[SMA][3];
+  const int nlev = (m.w & NOINTRA) ? LN1 : NLV;
+#pragma unroll
+  for (int a = 0; a < SMA; a++) {
+    if (a < na) {
+      const int g = gat[a];
+#pragma unroll
+      for (int d = 0; d < 3; d++) {
+        x[a][d] = A.x[d * N + g];
+        v[a][d] = A.v[d * N + g] + kick_dv(A, d * N + g, nlev) * im[a];
+      }
+    } else {
+#pragma unroll
+      for (int d = 0; d < 3; d++) x[a][d] = v[a][d] = 0.0;
+    }
+  }
+  bool ok;
+  if constexpr (W3)
+    ok = rattle3(x, v, im);
+  else
+    ok = (m.w & STAR) ? rattle_star_n(m.w & 0xff, x, v, im) : rattle_small(x, v, im, A.cloc + m.z, m.w & 0xff);
+  if (!ok) atomicOr(A.flag, 1);
+#pragma unroll
+  for (int a = 0; a < SMA; a++) {
+    if (a < na) {
+      const int g = gat[a];
+#pragma unroll
+      for (int d = 0; d < 3; d++) A.v[d * N + g] = v[a][d];
+    }
+  }
+}
+
 // Threads [0, nsm) take one small molecule each, the rest one free atom.
 __global__ void k_kick(const MolArgs A) {
-  pdl_enter();
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int N = A.N;
   if (t < A.nsm) {
-    const int4 m = A.sm[t];
-    double x[SMA][3], v[SMA][3], im[SMA];
-#pragma unroll
-    for (int a = 0; a < SMA; a++) {
-      if (a < m.y) {
-        const int g = sm_atom(A, m, a);
-        im[a] = A.invm[g];
-        x[a][0] = A.x[g];
-        x[a][1] = A.x[N + g];
-        x[a][2] = A.x[2 * N + g];
-        const int nlev = (m.w & NOINTRA) ? LN1 : NLV;
-        v[a][0] = A.v[g] + kick_dv(A, g, nlev) * im[a];
-        v[a][1] = A.v[N + g] + kick_dv(A, N + g, nlev) * im[a];
-        v[a][2] = A.v[2 * N + g] + kick_dv(A, 2 * N + g, nlev) * im[a];
-      } else {
-        im[a] = 0;
-        x[a][0] = x[a][1] = x[a][2] = 0;
-        v[a][0] = v[a][1] = v[a][2] = 0;
-      }
-    }
-    const bool ok = (m.w & MOL3)   ? rattle3(x, v, im)
-                    : (m.w & STAR) ? rattle_star_n(m.w & 0xff, x, v, im)
-                                   : rattle_small(x, v, im, A.cloc + m.z, m.w & 0xff);
-    if (!ok) atomicOr(A.flag, 1);
-#pragma unroll
-    for (int a = 0; a < SMA; a++) {
-      if (a < m.y) {
-        const int g = sm_atom(A, m, a);
-        A.v[g] = v[a][0];
-        A.v[N + g] = v[a][1];
-        A.v[2 * N + g] = v[a][2];
-      }
-    }
+    const int4 m = __ldg(&A.sm[t]);
+    if (m.w & MOL3)
+      kick_molecule<true>(A, m);
+    else
+      kick_molecule<false>(A, m);
   } else if (t < A.nsm + A.nfree) {
+    pdl_enter();
     const int g = A.free_atoms[t - A.nsm];
     const double im = A.invm[g];
     A.v[g] += kick_dv(A, g) * im;
     A.v[N + g] += kick_dv(A, N + g) * im;
     A.v[2 * N + g] += kick_dv(A, 2 * N + g) * im;
+  } else {
+    pdl_enter();
   }
 }
 
-// verlet drift (src/verlet.f) + SHAKE + RATTLE of small molecules, then
-// the scaled frame, group centres (appbou) and the pair-kernel inputs of
-// their groups; free atoms drift here and get their groups in k_free_groups.
-__global__ void k_drift(const MolArgs A) {
-  pdl_enter();
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+// One small constrained molecule (thread t): verlet drift (src/verlet.f) +
+// SHAKE + RATTLE, then the scaled frame, group centres (appbou) and the
+// pair-kernel inputs of its groups.  W3: a rigid three-site molecule
+// (SETTLE or Newton SHAKE), whose arrays are indexed by constants only and
+// stay in registers; otherwise the general clusters, whose solvers index by
+// constraint and keep their arrays in local memory.
+template <bool W3>
+__device__ __forceinline__ void drift_molecule(const MolArgs& A, int t, const int4 m) {
   const int N = A.N;
   const double dt = A.dt;
+  const int na = W3 ? 3 : m.y;
+  // The molecule's topology, masses, charges and constraint lengths are
+  // written by no kernel: they are loaded together, before the wait for the
+  // preceding grid, so that one memory round trip covers them.
+  const int2 gg = A.groups ? __ldg(&A.smg[t]) : make_int2(0, 0);
+  const int2 mg0 = gg.y > 0 ? __ldg(&A.gmeta[gg.x]) : make_int2(0, 0);
+  const int nlev = (m.w & NOINTRA) ? LN1 : NLV;
+  int gat[SMA];
+  double im[SMA], pmv[SMA];
+  float qv[SMA];
+#pragma unroll
+  for (int a = 0; a < SMA; a++) {
+    gat[a] = a < na ? sm_atom(A, m, a) : 0;
+    im[a] = a < na ? __ldg(&A.invm[gat[a]]) : 0.0;
+    pmv[a] = (a < na && gg.y > 0) ? __ldg(&A.pm[m.x + a]) : 0.0;
+    qv[a] = (a < na && gg.y > 0) ? __ldg(&A.q[m.x + a]) : 0.f;
+  }
+  double L2v[3] = {0.0, 0.0, 0.0};
+  if constexpr (W3)
+#pragma unroll
+    for (int k = 0; k < 3; k++) L2v[k] = __ldg(&A.dss[m.z + k]);
+  pdl_enter();
+  double x[SMA][3], xo[SMA][3], v[SMA][3], fh[SMA][3];
+  // positions, velocities, the kick's level forces and the verlet step's
+  // N0 force (as 0.5 dt f / m), all issued before any arithmetic
+  const bool vf = A.fv && nlev == NLV;
+#pragma unroll
+  for (int a = 0; a < SMA; a++) {
+    if (a < na) {
+      const int g = gat[a];
+#pragma unroll
+      for (int d = 0; d < 3; d++) {
+        xo[a][d] = A.x[d * N + g];
+        v[a][d] = A.v[d * N + g];
+        if (A.kick) v[a][d] += kick_dv(A, d * N + g, nlev) * im[a];
+        fh[a][d] = vf ? fixd(A.fv[d * N + g]) : 0.0;
+      }
+    } else {
+#pragma unroll
+      for (int d = 0; d < 3; d++) x[a][d] = xo[a][d] = v[a][d] = fh[a][d] = 0.0;
+    }
+  }
+  const int nc = m.w & 0xff;
+  if (A.kick && nc > 0) {
+    bool ok;
+    if constexpr (W3)
+      ok = rattle3(xo, v, im);
+    else
+      ok = (m.w & STAR) ? rattle_star_n(nc, xo, v, im) : rattle_small(xo, v, im, A.cloc + m.z, nc);
+    if (!ok) atomicOr(A.flag, 1);
+  }
+#pragma unroll
+  for (int a = 0; a < SMA; a++) {
+    if (a < na) {
+#pragma unroll
+      for (int d = 0; d < 3; d++) {
+        const double f = fh[a][d];
+        x[a][d] = xo[a][d] + dt * v[a][d] + f * 0.5 * dt * dt * im[a];
+        v[a][d] += f * 0.5 * dt * im[a];
+      }
+    }
+  }
+  if constexpr (W3) {
+    // isosceles with equal masses at the base: SETTLE, else Newton steps
+    const bool iso = im[1] == im[2] && fabs(L2v[0] - L2v[1]) <= 1e-12 * L2v[0];
+    if (!(iso ? settle3(x, xo, v, im, L2v, A.idt) : shake3(x, xo, v, im, L2v, dt, A.tol))) atomicOr(A.flag, 1);
+    if (!rattle3(x, v, im)) atomicOr(A.flag, 1);
+  } else if (m.w & STAR) {
+    if (!shake_star_n(nc, x, xo, v, im, A.dss + m.z, A.idt, A.tol)) atomicOr(A.flag, 1);
+    if (!rattle_star_n(nc, x, v, im)) atomicOr(A.flag, 1);
+  } else if (nc > 0) {
+    if (!shake_small(x, xo, v, im, A.cloc + m.z, A.dss + m.z, nc, dt, A.tol)) atomicOr(A.flag, 1);
+    if (!rattle_small(x, v, im, A.cloc + m.z, nc)) atomicOr(A.flag, 1);
+  }
+  double s[SMA][3];
+#pragma unroll
+  for (int a = 0; a < SMA; a++) {
+    if (a < na) {
+      const int g = gat[a];
+#pragma unroll
+      for (int d = 0; d < 3; d++) {
+        A.x[d * N + g] = x[a][d];
+        A.xo[d * N + g] = xo[a][d];
+        A.v[d * N + g] = v[a][d];
+#pragma unroll
+        for (int l = 0; l < NLV; l++)
+          if (l < nlev && A.fz[l]) A.fz[l][d * N + g] = 0ull;
+      }
+      s[a][0] = A.o11 * x[a][0] + A.o12 * x[a][1] + A.o13 * x[a][2];
+      s[a][1] = A.o22 * x[a][1] + A.o23 * x[a][2];
+      s[a][2] = A.o33 * x[a][2];
+    }
+  }
+  for (int gi = gg.x; gi < gg.x + gg.y; gi++) {
+    const int2 mg = gi == gg.x ? mg0 : __ldg(&A.gmeta[gi]);
+    double c[3] = {0, 0, 0};
+#pragma unroll
+    for (int a = 0; a < SMA; a++) {
+      const int ga = m.x + a;
+      if (a < na && ga >= mg.x && ga < mg.x + (mg.y & 0xff)) {
+        const double w = pmv[a];
+        c[0] += w * s[a][0];
+        c[1] += w * s[a][1];
+        c[2] += w * s[a][2];
+      }
+    }
+    A.grp[gi] = c[0];
+    A.grp[A.G + gi] = c[1];
+    A.grp[2 * A.G + gi] = c[2];
+    A.gpos[gi] = make_double4(c[0], c[1], c[2], 0.0);
+#pragma unroll
+    for (int a = 0; a < SMA; a++) {
+      const int ga = m.x + a;
+      if (a < na && ga >= mg.x && ga < mg.x + (mg.y & 0xff)) {
+        const double dx = s[a][0] - c[0], dy = s[a][1] - c[1], dz = s[a][2] - c[2];
+        A.aoff[ga] = make_float4((float)(A.c11 * dx + A.c12 * dy + A.c13 * dz), (float)(A.c22 * dy + A.c23 * dz),
+                                 (float)(A.c33 * dz), qv[a]);
+      }
+    }
+  }
+}
+
+// verlet drift + SHAKE + RATTLE of small molecules (drift_molecule); free
+// atoms drift here and get their groups in k_free_groups.
+__global__ void k_drift(const MolArgs A) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const double dt = A.dt;
   if (t < A.nsm) {
-    const int4 m = A.sm[t];
-    double x[SMA][3], xo[SMA][3], v[SMA][3], im[SMA];
-    const int nlev = (m.w & NOINTRA) ? LN1 : NLV;
-#pragma unroll
-    for (int a = 0; a < SMA; a++) {
-      if (a < m.y) {
-        const int g = sm_atom(A, m, a);
-        im[a] = A.invm[g];
-#pragma unroll
-        for (int d = 0; d < 3; d++) {
-          xo[a][d] = A.x[d * N + g];
-          v[a][d] = A.v[d * N + g];
-          if (A.kick) v[a][d] += kick_dv(A, d * N + g, nlev) * im[a];
-        }
-      } else {
-        im[a] = 0;
-#pragma unroll
-        for (int d = 0; d < 3; d++) x[a][d] = xo[a][d] = v[a][d] = 0.0;
-      }
-    }
-    const int nc = m.w & 0xff;
-    const bool mol3 = (m.w & MOL3) != 0;
-    if (A.kick && nc > 0)
-      if (!(mol3 ? rattle3(xo, v, im)
-                 : ((m.w & STAR) ? rattle_star_n(nc, xo, v, im) : rattle_small(xo, v, im, A.cloc + m.z, nc))))
-        atomicOr(A.flag, 1);
-#pragma unroll
-    for (int a = 0; a < SMA; a++) {
-      if (a < m.y) {
-        const int g = sm_atom(A, m, a);
-#pragma unroll
-        for (int d = 0; d < 3; d++) {
-          const double f = (A.fv && nlev == NLV) ? fixd(A.fv[d * N + g]) : 0.0;
-          x[a][d] = xo[a][d] + dt * v[a][d] + f * 0.5 * dt * dt * im[a];
-          v[a][d] += f * 0.5 * dt * im[a];
-        }
-      }
-    }
-    if (mol3) {
-      const double* L2 = A.dss + m.z;
-      // isosceles with equal masses at the base: SETTLE, else Newton steps
-      const bool iso = im[1] == im[2] && fabs(L2[0] - L2[1]) <= 1e-12 * L2[0];
-      if (!(iso ? settle3(x, xo, v, im, L2, A.idt) : shake3(x, xo, v, im, L2, dt, A.tol))) atomicOr(A.flag, 1);
-      if (!rattle3(x, v, im)) atomicOr(A.flag, 1);
-    } else if (m.w & STAR) {
-      if (!shake_star_n(nc, x, xo, v, im, A.dss + m.z, A.idt, A.tol)) atomicOr(A.flag, 1);
-      if (!rattle_star_n(nc, x, v, im)) atomicOr(A.flag, 1);
-    } else if (nc > 0) {
-      if (!shake_small(x, xo, v, im, A.cloc + m.z, A.dss + m.z, nc, dt, A.tol)) atomicOr(A.flag, 1);
-      if (!rattle_small(x, v, im, A.cloc + m.z, nc)) atomicOr(A.flag, 1);
-    }
-    double s[SMA][3];
-#pragma unroll
-    for (int a = 0; a < SMA; a++) {
-      if (a < m.y) {
-        const int g = sm_atom(A, m, a);
-#pragma unroll
-        for (int d = 0; d < 3; d++) {
-          A.x[d * N + g] = x[a][d];
-          A.xo[d * N + g] = xo[a][d];
-          A.v[d * N + g] = v[a][d];
-#pragma unroll
-          for (int l = 0; l < NLV; l++)
-            if (l < nlev && A.fz[l]) A.fz[l][d * N + g] = 0ull;
-        }
-        s[a][0] = A.o11 * x[a][0] + A.o12 * x[a][1] + A.o13 * x[a][2];
-        s[a][1] = A.o22 * x[a][1] + A.o23 * x[a][2];
-        s[a][2] = A.o33 * x[a][2];
-      }
-    }
-    const int2 gg = A.groups ? A.smg[t] : make_int2(0, 0);
-    for (int gi = gg.x; gi < gg.x + gg.y; gi++) {
-      const int2 mg = A.gmeta[gi];
-      double c[3] = {0, 0, 0};
-#pragma unroll
-      for (int a = 0; a < SMA; a++) {
-        const int ga = m.x + a;
-        if (a < m.y && ga >= mg.x && ga < mg.x + (mg.y & 0xff)) {
-          const double w = A.pm[ga];
-          c[0] += w * s[a][0];
-          c[1] += w * s[a][1];
-          c[2] += w * s[a][2];
-        }
-      }
-      A.grp[gi] = c[0];
-      A.grp[A.G + gi] = c[1];
-      A.grp[2 * A.G + gi] = c[2];
-      A.gpos[gi] = make_double4(c[0], c[1], c[2], 0.0);
-#pragma unroll
-      for (int a = 0; a < SMA; a++) {
-        const int ga = m.x + a;
-        if (a < m.y && ga >= mg.x && ga < mg.x + (mg.y & 0xff)) {
-          const double dx = s[a][0] - c[0], dy = s[a][1] - c[1], dz = s[a][2] - c[2];
-          A.aoff[ga] = make_float4((float)(A.c11 * dx + A.c12 * dy + A.c13 * dz), (float)(A.c22 * dy + A.c23 * dz),
-                                   (float)(A.c33 * dz), A.q[ga]);
-        }
-      }
-    }
+    const int4 m = __ldg(&A.sm[t]);
+    if (m.w & MOL3)
+      drift_molecule<true>(A, t, m);
+    else
+      drift_molecule<false>(A, t, m);
   } else if (t < A.nsm + A.ndg) {
+    pdl_enter();
     // a group of an unconstrained molecule: its atoms, then its centre
     const int gi = A.drift_groups[t - A.nsm];
     const int2 mg = A.gmeta[gi];
     for (int a = mg.x; a < mg.x + (mg.y & 0xff); a++) drift_atom(A, a, dt);
     if (A.groups) group_centre(A, gi);
   } else if (t < A.nsm + A.ndg + A.nda) {
+    pdl_enter();
     drift_atom(A, A.drift_atoms[t - A.nsm - A.ndg], dt);
+  } else {
+    pdl_enter();
   }
 }
 
@@ -1219,8 +1278,11 @@ static int md_kick(orac_gpu_ctx* ctx, MdState& S, const double* c) {
   kick_fill(A, S, c);
   if (!A.kick) return ORAC_OK;
   const int n = S.nsm + S.nfree;
+  int slot = -1;
+  if (int rc = prof_begin(ctx, &slot, PROF_DRIFT)) return rc;
   orac_launch(k_kick, (n + 31) / 32, 32, 0, ctx->stream, A);
   CKL();
+  if (int rc = prof_end(ctx, slot)) return rc;
   if (S.nbig) {
     orac_launch(k_rattle_big, (S.nbig + 127) / 128, 128, 0, ctx->stream, big_args(ctx, S, 0.0, 1e-12));
     CKL();
@@ -1247,8 +1309,11 @@ static int md_drift(orac_gpu_ctx* ctx, MdState& S, double dt, const double* c, i
   A.fv = S.has_n0 ? S.ffix[LN0] : nullptr;
   for (int l = 0; l < NLV; l++) A.fz[l] = ((zmask >> l) & 1) ? S.ffix[l] : nullptr;
   const int n = S.nsm + S.ndg + S.nda;
+  int slot = -1;
+  if (int rc = prof_begin(ctx, &slot, PROF_DRIFT)) return rc;
   orac_launch(k_drift, (n + 31) / 32, 32, 0, ctx->stream, A);
   CKL();
+  if (int rc = prof_end(ctx, slot)) return rc;
   if (S.nbig) {
     orac_launch(k_shake_big, (S.nbig + 127) / 128, 128, 0, ctx->stream, big_args(ctx, S, dt, 1e-8));
     CKL();
@@ -1311,9 +1376,12 @@ static int md_shell_recip(orac_gpu_ctx* ctx, MdState& S, char sh, int lvl, bool 
   double recip[9];
   for (int i = 0; i < 3; i++)
     for (int j = 0; j < 3; j++) recip[i + 3 * j] = 0.5 * ctx->oc[j + 3 * i];  // src/fft_pme.f:47-51
+  int slot = -1;
+  if (int rc = prof_begin(ctx, &slot, PROF_PME)) return rc;
   if (int rc = pme_run(ctx, ctx->N, S.x, ctx->pme_q(), recip, ctx->volume, ctx->alphal, nullptr, S.e + 24, nullptr,
                        nullptr, f, dudl ? ctx->d_dq : nullptr, dudl ? S.e + E_DUDL + 3 : nullptr))
     return rc;
+  if (int rc = prof_end(ctx, slot)) return rc;
   return md_ferrf(ctx, S, f, energy);
 }
 
@@ -1397,7 +1465,11 @@ static int md_alch_m(orac_gpu_ctx* ctx, MdState& S, bool energy) {
 static int md_bonded(orac_gpu_ctx* ctx, MdState& S, bool n0, bool n1, bool energy) {
   const int mask = (n0 ? BK_BOND | BK_BEND | BK_ITORS : 0) | (n1 ? BK_TORS : 0);
   if (!mask) return ORAC_OK;
-  return bonded_launch(ctx, mask, S.x, nullptr, S.ffix[LN0], energy ? S.e + E_BOND : nullptr, S.ffix[LN1]);
+  int slot = -1;
+  if (int rc = prof_begin(ctx, &slot, PROF_BONDED)) return rc;
+  if (int rc = bonded_launch(ctx, mask, S.x, nullptr, S.ffix[LN0], energy ? S.e + E_BOND : nullptr, S.ffix[LN1]))
+    return rc;
+  return prof_end(ctx, slot);
 }
 
 static int md_forces_intra(orac_gpu_ctx* ctx, MdState& S, int lvl, bool energy) {
@@ -2015,7 +2087,10 @@ static int md_run_impl(orac_gpu_ctx* ctx, int nsteps, int energy_every, double* 
     const bool energy = energy_every > 0 && ((k + 1) % energy_every == 0);
     if (S.use_graph && !energy) {
       const int kind = update ? 1 : 0;
+      // both kinds at once: the first list-update step of a run then pays
+      // for no capture
       if (int rc = md_capture(ctx, S, kind)) return rc;
+      if (int rc = md_capture(ctx, S, kind ^ 1)) return rc;
       CK(cudaGraphLaunch(S.gexec[kind], ctx->stream));
       ctx->launches += S.kpg[kind];
       S.last_kind = kind;

@@ -99,6 +99,7 @@ def load():
         "orac_gpu_counters": (i, [_P, C.POINTER(i64), i]),
         "orac_gpu_prof_enable": (i, [_P, i]),
         "orac_gpu_prof_read": (i, [_P, C.POINTER(d), C.POINTER(i64), i]),
+        "orac_gpu_prof_read_family": (i, [_P, i, C.POINTER(d), C.POINTER(i64), i]),
         "orac_gpu_sync": (i, [_P]),
         "orac_gpu_stats": (i, [_P, C.POINTER(i64), C.POINTER(i64)]),
         "orac_gpu_footprint": (i, [_P, C.POINTER(i64)]),
