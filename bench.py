@@ -69,6 +69,33 @@ def f0_system():
                                    fudge=0.83333, lj_fudge=0.5, name="F0_fkbp12", rigid_hydrogen=True)
 
 
+def f0_test4_system(k):
+    """F0 at test2's restart state k (0 ij4i0000, 1 ij4i0001, 2 ij4i0003)
+    with the reference's test4 parameters: shells 5.0/8.1/12.5 A, SPME alpha
+    0.37 on 48 x 49 x 48 order 4, bonds to hydrogen rigid, the ligand (atoms
+    1-52) the removed alchemical species."""
+    from orac_b200 import oracio
+
+    gold = os.path.join(ROOT, "tests", "golden")
+    tp, rst = oracio.split_arrays(dict(np.load(os.path.join(gold, "f0_fkbp12.npz"))))
+    if k > 0:
+        r = np.load(os.path.join(gold, "f0_orac_records.npz"))
+        rst = dict(rst, co=r[f"co{k}"], xyz=r[f"xyz{k}"], v=r[f"v{k}"])
+    sh = systems.Shells(rcutm=5.0, rtolm=0.3, rneim=0.5, rcutl=8.1, rtoll=0.3, rneil=0.5, rcuth=12.5, rtolh=0.3,
+                        rneih=1.5)
+    s = oracio.system_from_orac(tp, rst, alphal=0.37, nfft=(48, 49, 48), order=4, shells=sh, ncell=(18, 18, 18),
+                                fudge=0.83333, lj_fudge=0.5, name=f"F0_test4_{k}", rigid_hydrogen=True)
+    ss = np.ones(s.ntap, np.int32)
+    ss[:52] = -2
+    s.ss_alchemy = ss
+    return s
+
+
+# test4's NE run: 15/3/1.5/0.75/0.375 fs, lists every 60 fs, the shifted
+# potential SHIFT-POT 4.0 0.35, the 1.5 ps schedule of 15.off
+NE_WORKLOAD = dict(dt_h=15.0, lrespa=5, mrespa=2, n1respa=2, n0respa=2, nupdte=4, rshk="l")
+NE_WALKERS = 12  # the three restart states, four velocity draws each
+
 # the reference's test1 schedule: 15 fs outer step, L 3 fs (SPME), M 1.5 fs,
 # intramolecular 0.75 / 0.375 fs, list update every 6 steps
 F0_WORKLOAD = dict(build=f0_system, dt_h=15.0, lrespa=5, mrespa=2, n1respa=2, n0respa=2, nupdte=6, rshk="l")
@@ -443,6 +470,11 @@ def gpu_arm(args, wl, s, device):
             res["hrem"] = hrem_arm(args, wl, device)
         except Exception as exc:
             res["hrem"] = {"error": f"{type(exc).__name__}: {exc}"}
+    if ws == 1 and args.ne:
+        try:
+            res["ne_swarm"] = ne_arm(args, device)
+        except Exception as exc:
+            res["ne_swarm"] = {"error": f"{type(exc).__name__}: {exc}"}
     if ws == 1 and args.configs:
         for key, arm in (("config2", config2_arm), ("config1_as_specified", config1_fixed_arm)):
             try:
@@ -898,6 +930,92 @@ def hrem_arm(args, wl, device):
                    f"{HREM_INTERVALS} intervals"}
 
 
+def ne_arm(args, device):
+    """The non-equilibrium work swarm of the reference's test4: walkers on
+    F0 switch the ligand off along test4's 1.5 ps schedule (charges over
+    0.6 ps, then the LJ) with the shifted potential, the lambdas moved and
+    the work summed on the device (orac_gpu_md_set_schedule); all walkers
+    advance by one graph launch per 15-fs step.  Walkers start from test2's
+    three restart states (the states of test4's walkers 1, 2 and 4) with
+    their own velocities and with three perturbed copies each (every
+    velocity scaled by 1 + 0.01 N(0, 1)).  Timed by wall clock over the
+    whole schedule; plain = one walker alone through the same driver."""
+    import torch
+
+    from orac_b200.engine import Batch, Engine
+
+    d = np.load(os.path.join(ROOT, "tests", "golden", "ne_test4.npz"))
+    sch = d["schedule"]
+    wl = NE_WORKLOAD
+    nsteps = int(round(1000.0 * sch[-1, 0] / wl["dt_h"]))
+    kT = units.BOLTZ * 300.0 / units.UNITE
+
+    def make(k, draw):
+        s = f0_test4_system(k)
+        if draw:
+            rng = np.random.default_rng(1000 * k + draw)
+            f = 1.0 + 0.01 * rng.standard_normal(s.ntap)
+            s.vx, s.vy, s.vz = s.vx * f, s.vy * f, s.vz * f
+        e = Engine(s, device=device)
+        e.set_alchemy(s.ss_alchemy, 0.5, 0.5, shifted=True, qshift=4.0, ljshift=0.35)
+        e.set_lambda(0.0, 0.0, 0.0, 0.0)
+        e.set_schedule(sch[:, 0] * 1000.0, sch[:, 1], sch[:, 2], sch[:, 3], sch[:, 4])
+        e.md_setup(wl["dt_h"], wl["lrespa"], wl["mrespa"], wl["nupdte"], wl["rshk"], n1respa=wl["n1respa"],
+                   n0respa=wl["n0respa"])
+        return e
+
+    e1 = make(0, 0)
+    L = e1.lib
+    L.orac_gpu_md_run_async(e1.ctx, 1)  # captures the step graphs
+    if e1.collect():
+        raise RuntimeError(L.orac_gpu_last_error(e1.ctx).decode())
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    L.orac_gpu_md_run_async(e1.ctx, nsteps - 1)
+    if e1.collect():
+        raise RuntimeError(L.orac_gpu_last_error(e1.ctx).decode())
+    plain_s = time.perf_counter() - t0
+    w_plain = e1.md_work()[0]
+    e1.close()
+    walkers = [(k, draw) for draw in range(NE_WALKERS // 3) for k in range(3)]
+    engines = [make(k, draw) for k, draw in walkers]
+    b = Batch(engines)
+    tune = tuned(b)
+    b.run(1)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    b.run(nsteps - 1)
+    secs = time.perf_counter() - t0
+    b.close()
+    works = []
+    for e in engines:
+        works.append(e.md_work()[0] * units.KJMOL)
+        if e.collect():
+            raise RuntimeError(L.orac_gpu_last_error(e.ctx).decode())
+        e.close()
+    works = np.array(works)
+    wk = works / (kT * units.KJMOL)
+    jar = -kT * units.KJMOL * (np.log(np.mean(np.exp(-(wk - wk.min())))) - wk.min())
+    orac_final = {f"walker{w}": float(d[f"wrk{w}"][-1, 5]) for w in (1, 2, 4)}
+    val = ns_per_day((nsteps - 1) * len(engines), wl["dt_h"], secs)
+    pval = ns_per_day(nsteps - 1, wl["dt_h"], plain_s)
+    return {"workload": f"{len(engines)} NE walkers on F0 (14,900 atoms), test4's schedule 15.off "
+                        "(1.5 ps: charges off over 0.6 ps, LJ over 0.9 ps), shifted potential 4.0/0.35, shells "
+                        "5.0/8.1/12.5 A, SPME 48x49x48, r-RESPA 15/3/1.5/0.75/0.375 fs, NVE",
+            "walkers": len(engines), "steps": nsteps, "value": val, "unit": "ns/day (aggregate over walkers)",
+            "plain_value": pval, "speedup_vs_plain": val / pval,
+            "work_kjmol": [float(x) for x in works],
+            "work_same_starts_as_orac": {"walker1": float(works[0]), "walker2": float(works[1]),
+                                         "walker4": float(works[2])},
+            "orac_printed_final_work_kjmol": orac_final,
+            "plain_walker1_work_kjmol": float(w_plain * units.KJMOL),
+            "jarzynski_dG_kjmol": float(jar), "mean_work_kjmol": float(works.mean()), "tuning": tune,
+            "how": "work per walker summed on the device as ORAC sums it (orac_gpu_md_work); ORAC's final works are "
+                   "the last line of test4/PAR000k/1.5.wrk (NPT with thermostats and a COM restraint: the "
+                   "trajectories part after ~0.1 ps, so the finals agree only in size); wall clock over the "
+                   "schedule after one captured step"}
+
+
 def config2_arm(args, device, flush):
     """The solvated chain of the second workload: a 1,700-atom bonded chain
     in 7,000 waters (22,700 atoms, 62 A box, SPME 64^3 order 5), FP32 pair
@@ -1062,6 +1180,7 @@ def main():
     ap.add_argument("--no-f0", dest="f0", action="store_false", help="skip the ORAC test1 system leg")
     ap.add_argument("--no-drift", dest="drift", action="store_false", help="skip the 1,000-step energy drift run")
     ap.add_argument("--no-hrem", dest="hrem", action="store_false", help="skip the replica-exchange leg")
+    ap.add_argument("--no-ne", dest="ne", action="store_false", help="skip the non-equilibrium work-swarm leg")
     ap.add_argument("--no-configs", dest="configs", action="store_false",
                     help="skip the solvated-chain MD leg and the 31 A fixed-list leg")
     ap.add_argument("--profile-window-batch", type=int, default=0, metavar="N",
@@ -1208,7 +1327,7 @@ def main():
                    "the autotuner (orac_gpu_batch_tune / orac_gpu_tune)"}
     elif "batched_error" in res:
         out["batched"] = {"error": res["batched_error"]}
-    for key in ("orac_test1", "config2", "config1_as_specified", "hrem", "uneven", "served"):
+    for key in ("orac_test1", "config2", "config1_as_specified", "hrem", "ne_swarm", "uneven", "served"):
         if key in res:
             out[key] = res[key]
     print(json.dumps(out))

@@ -391,6 +391,32 @@ int orac_gpu_md_set_graphs(orac_gpu_ctx* ctx, int on);
 int orac_gpu_md_records(orac_gpu_ctx* ctx, int max, double* out,
                         int64_t* n_total, int reset);
 
+/* Non-equilibrium alchemical runs (ORAC's steered alchemy, the NE work
+ * swarms of test3/test4: STEER_PATH ALCHEMY with time_steer) ------------
+ * orac_gpu_md_set_schedule replaces the alchemy file ORAC reads
+ * (src/alchemic.f's timerec, ladded, laddedq, lremoved, lremovedq): ntimes
+ * points (2..64) of increasing times in fs and the four lambdas there.
+ * Call it after orac_gpu_set_alchemy and before orac_gpu_md_setup; the run
+ * then starts at time t0 with the lambdas as ORAC sets them on a restart
+ * (src/mtsmd.f:722-758).  Before every M shell the lambdas move to the
+ * schedule's values at rtime = t0 + (N0 steps so far) x (N0 step), on the
+ * device, as src/mtsmd.f:2963-2999 moves them; each M step adds ORAC's
+ * work terms (src/mtsmd.f:3042-3044).  ljintra as orac_gpu_set_lambda's;
+ * intramol is the last orac_gpu_set_lambda call's.  ntimes = 0 removes the
+ * schedule (before the next md_setup). */
+int orac_gpu_md_set_schedule(orac_gpu_ctx* ctx, int ntimes, const double* times,
+                             const double* ladded, const double* laddedq,
+                             const double* lremoved, const double* lremovedq,
+                             double t0, int ljintra);
+/* out[14]: the work so far (internal energy units), rtime (fs), ladd lrm
+ * laddq lrmq, and the held terms dwrkm dwrkl dwrkh dwrkrc_m dwrkrc_l
+ * dwrkrc_h dwrk_al dwrk14.  Synchronises the context's stream. */
+int orac_gpu_md_work(orac_gpu_ctx* ctx, double* out);
+/* (rtime, work) after each M step, the newest min(max, 8192) oldest first;
+ * n_total receives the number of M steps recorded. */
+int orac_gpu_md_work_trace(orac_gpu_ctx* ctx, int max, double* out,
+                           int64_t* n_total);
+
 /* Batched systems ----------------------------------------------------------
  * Many independent systems (replicas, HREM states, alchemical windows), one
  * context each, advanced together: the batch splices every context's step

@@ -5,34 +5,10 @@
 // (src/mts_forces.f:118-153).
 #include <cmath>
 
+#include "alch.cuh"
 #include "common.cuh"
 
 namespace {
-
-// alch_set: [0][t+4] soft-core shift, [1][t+4] scale
-void alch_set(double f[2][9], double ladd, double lrm, int intramol, int ljintra, int qq) {
-  for (int k = 0; k < 2; k++)
-    for (int t = 0; t < 9; t++) f[k][t] = 0.0;
-  const double la = std::fabs(ladd), lr = std::fabs(lrm);
-  auto put = [&](int t, double a, double b) {
-    f[0][t + 4] = a;
-    f[1][t + 4] = b;
-  };
-  put(2, 0.0, 1.0);
-  put(3, la, 1.0 - la);
-  put(-1, lr, 1.0 - lr);
-  if (intramol && qq) {
-    put(4, la * la, 1.0 - la * la);
-    put(-4, lr * lr, 1.0 - lr * lr);
-  } else if (intramol && !ljintra) {
-    put(4, la, 1.0 - la);
-    put(-4, lr, 1.0 - lr);
-  } else {
-    put(4, 0.0, 1.0);
-    put(-4, 0.0, 1.0);
-  }
-  put(0, 0.0, 0.0);
-}
 
 // derivative of alch_set's tables with respect to a control lambda that
 // moves ladd and lrm at rates dla and dlr (d|l|/dl taken as +1 at l = 0)
@@ -54,14 +30,6 @@ void alch_set_d(double d[2][9], double ladd, double lrm, double dla, double dlr,
     put(4, sa * dla, -sa * dla);
     put(-4, sr * dlr, -sr * dlr);
   }
-}
-
-// chrgec of mts_furier_alchemy (src/mts_furier_alchemy.f:75-88)
-double scaled_charge(double q, double lq) {
-  const double a = std::fabs(lq);
-  if (a == 1.0) return 0.0;
-  if (a == 0.0) return q;
-  return (1.0 - a) * q;
 }
 
 __global__ void k_variant_out(const double* __restrict__ acc, int variant, int forces_on, double* __restrict__ x) {
@@ -156,6 +124,27 @@ int upload_alch_charges(orac_gpu_ctx* ctx, const double* dlam) {
 
 }  // namespace
 
+int alch_upload_tables(orac_gpu_ctx* ctx) {
+  AlchDyn D;
+  const AlchTables& T = ctx->at;
+  for (int k = 0; k < 2; k++)
+    for (int t = 0; t < 9; t++) {
+      D.f[k][t] = T.f[k][t];
+      D.fq[k][t] = T.fq[k][t];
+      D.f0[k][t] = T.f0[k][t];
+      D.fq0[k][t] = T.fq0[k][t];
+      D.df[k][t] = T.df[k][t];
+      D.dfq[k][t] = T.dfq[k][t];
+    }
+  alch_dyn_f32(&D);
+  if (!ctx->d_ad && dev_alloc(ctx, &ctx->d_ad, 1)) return ORAC_ERR_CUDA;
+  // stream-ordered: a step graph still running reads the old tables
+  CK(cudaMemcpyAsync(ctx->d_ad, &D, sizeof(D), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return ORAC_OK;
+}
+
+
 void variant_fill(const orac_gpu_ctx* ctx, PairArgs* a) {
   a->variant = ctx->variant;
   if (ctx->variant == VAR_STD) return;
@@ -170,11 +159,7 @@ void variant_fill(const orac_gpu_ctx* ctx, PairArgs* a) {
     a->ljsoft = (float)ctx->at.ljsoft;
     a->qshift = (float)ctx->at.qshift;
     a->ljshift_s = (float)ctx->at.ljshift_s;
-    for (int k = 0; k < 2; k++)
-      for (int t = 0; t < 9; t++) {
-        a->af[k][t] = (float)ctx->at.f[k][t];
-        a->afq[k][t] = (float)ctx->at.fq[k][t];
-      }
+    a->ad = ctx->d_ad;
   }
 }
 
@@ -225,7 +210,7 @@ int alch_listqq_build(orac_gpu_ctx* ctx) {
 
 void variant_free(orac_gpu_ctx* ctx) {
   void* p[] = {ctx->d_vflag, ctx->d_soft, ctx->d_softd, ctx->d_qc, ctx->d_q0, ctx->d_xtra, ctx->d_dq,
-               ctx->d_lam4, ctx->d_listqq, ctx->d_remf};
+               ctx->d_lam4, ctx->d_listqq, ctx->d_remf, ctx->d_ad, ctx->d_lam40, ctx->d_ne, ctx->d_ne_alist};
   for (void* q : p)
     if (q) dev_free(ctx, q);
 }
@@ -343,6 +328,7 @@ int orac_gpu_set_lambda(orac_gpu_ctx* ctx, const double* lam, int intramol, int 
   alch_set(T.fq0, lam[6], lam[7], intramol, ljintra, 1);
   alch_set_d(T.df, lam[0], lam[1], d[0], d[1], intramol, ljintra, 0);
   alch_set_d(T.dfq, lam[2], lam[3], d[2], d[3], intramol, ljintra, 1);
+  if (int rc = alch_upload_tables(ctx)) return rc;
   return upload_alch_charges(ctx, dlam);
 }
 

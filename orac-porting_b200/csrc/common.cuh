@@ -65,6 +65,16 @@ struct AlchTables {
   int opls;                    // sigma = 2 sqrt(rmin_i rmin_j) instead of rmin_i + rmin_j
 };
 
+// The lambda-dependent tables of the alchemy variant in device memory, read
+// by the pair kernel on every launch: a lambda changed on the device (a
+// non-equilibrium schedule) or by orac_gpu_set_lambda needs no new graph.
+// FP32 copies of the current tables for the force path, FP64 tables for
+// the energies, the work and dU/dlambda.
+struct AlchDyn {
+  float af[2][9], afq[2][9];
+  double f[2][9], fq[2][9], f0[2][9], fq0[2][9], df[2][9], dfq[2][9];
+};
+
 // A group-pair list in CSR form with fixed row capacities: row i occupies
 // [off[i], off[i+1]) and holds cnt[i] entries.  Nested shell lists reuse the
 // rows of their parent list.
@@ -142,8 +152,8 @@ struct PairArgs {
   const double2* softd;
   float qsoft, ljsoft;
   float qshift, ljshift_s;  // shifted potential (at.shifted)
-  float af[2][9], afq[2][9];  // FP32 copies of the current tables
-  AlchTables at;
+  const AlchDyn* ad;        // the lambda tables (device memory)
+  AlchTables at;            // the constants (qsoft, ljsoft, shifted, opls, shifts)
 };
 
 // Bonded intramolecular terms (orac_gpu_set_bonded / _set_intra_pairs), the
@@ -223,6 +233,34 @@ struct ApiScratch {
 };
 
 struct MdState;  // md.cu
+
+// A non-equilibrium alchemical run (ne.cu): the schedule as set (host) and
+// the lambda state and work on the device.
+constexpr int NE_MAXT = 64;       // schedule points
+constexpr int NE_REC_CAP = 8192;  // (rtime, work) records, one per M step
+struct NeHost {
+  bool on = false;
+  std::vector<double> trec, sch[4];  // times (fs); ladded laddedq lremoved lremovedq
+  double t0 = 0.0;
+  int ljintra = 0;
+};
+struct NeDev {
+  int ntimes;
+  double trec[NE_MAXT], sch[4][NE_MAXT];
+  double t0, tn0, rtime;
+  long long ninn0;     // N0 steps since t0
+  double g[4], g0[4];  // ladd lrm laddq lrmq and their previous values
+  double pa[4], pr[4]; // added / removed atoms: lambda, lambdaq, lambda0, lambdaq0
+  int intramol, ljintra;
+  double selfc;        // alpha / sqrt(pi) (1 - erfc(kcut / (2 alpha)))
+  double dself;        // cself_alchemy's dwrk at the current charges
+  // work terms dwrkm dwrkl dwrkh dwrkrc_m dwrkrc_l dwrkrc_h dwrk_al dwrk14:
+  // held (dw) and of the evaluations of the current M step (dwn)
+  double dw[8], dwn[8];
+  double wrk;
+  long long nrec;
+  double rec[NE_REC_CAP][2];
+};
 
 struct orac_gpu_ctx {
   MdState* md = nullptr;
@@ -339,6 +377,12 @@ struct orac_gpu_ctx {
   // per atom (lambda LJ, lambda charge, d(1-|lambda LJ|)/dlambda,
   // d(1-|lambda charge|)/dlambda), and listqq (ia, ib, facQ, 1-based)
   double4* d_lam4 = nullptr;
+  double4* d_lam40 = nullptr;  // lambda0, lambdaq0 per atom (non-equilibrium runs)
+  AlchDyn* d_ad = nullptr;  // the lambda tables the pair kernel reads
+  NeHost ne;                 // a non-equilibrium schedule (ne.cu)
+  NeDev* d_ne = nullptr;
+  int4* d_ne_alist = nullptr;  // alchemical atoms: (atom, +1 added / -1 removed, ss_index, 0)
+  int ne_nal = 0;
   int* d_listqq = nullptr;
   int nlistqq = -1;  // -1: not built for the current species
   int alch_intramol = 0;
@@ -508,8 +552,16 @@ struct SmallSpec {
   const double* q;
   unsigned long long* ffix;
   double* edq;
+  double* work;  // fnb14_alchemy / ferrf_alchemy_add: U(lambda) - U(lambda0) (null: none)
 };
 int small_launch_set(orac_gpu_ctx* ctx, int n, const SmallSpec* specs);
+// ne.cu: the schedule's state at md_setup, and the launches of the MD step
+int ne_init(orac_gpu_ctx* ctx, double tn0);
+int ne_lambda_launch(orac_gpu_ctx* ctx, int n0steps);
+int ne_sum_launch(orac_gpu_ctx* ctx, int commit);
+int ne_recip_launch(orac_gpu_ctx* ctx, const double* eq, const double* e0, const double* fq, const double* f0,
+                    int slot, bool direct);
+int md_nupdte(orac_gpu_ctx* ctx);
 int alch_listqq_build(orac_gpu_ctx* ctx);
 // the same with explicit charges (null: the topology's) and an optional
 // fixed-point force output (the MD driver's level accumulators)

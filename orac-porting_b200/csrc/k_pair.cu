@@ -118,8 +118,9 @@ __device__ __forceinline__ bool seg_sel(int kind, int fa, int fb) {
 // Soft-core pair of force_alchemy (src/force_alchemy.f:441-531) in FP32:
 // qf is the force over r, conf/coul the scaled energies that enter the S'V
 // sum.  t indexes the tables (ss_i + ss_j + 4).
-__device__ __forceinline__ void alch_pair_f32(const PairArgs& A, float r2, int t, float rmi, float rmj, float eps4,
-                                              float qq, float* qf, float* conf, float* coul) {
+__device__ __forceinline__ void alch_pair_f32(const PairArgs& A, const float (*af)[9], const float (*afq)[9], float r2,
+                                              int t, float rmi, float rmj, float eps4, float qq, float* qf,
+                                              float* conf, float* coul) {
   if (A.at.shifted) {
     // force_ALCHEMY_shift (src/force_alchemy_shifted.f:466-520): LJ at the
     // shifted distance rl, Coulomb erfc(alpha r) over the shifted rq
@@ -127,25 +128,25 @@ __device__ __forceinline__ void alch_pair_f32(const PairArgs& A, float r2, int t
     float f = 0.f, uc = 0.f, uq = 0.f;
     if (eps4 > 1e-12f) {
       const float sig = A.at.opls ? 2.f * sqrtf(rmi * rmj) : rmi + rmj;
-      const float rl = r + A.ljshift_s * sig * A.af[0][t];
+      const float rl = r + A.ljshift_s * sig * af[0][t];
       const float irl = __fdividef(1.f, rl);
       const float s2 = sig * sig * irl * irl, x = s2 * s2 * s2;
-      const float sc = A.af[1][t] * eps4;
+      const float sc = af[1][t] * eps4;
       f = sc * (12.f * x * x - 6.f * x) * ir * irl;
       uc = sc * (x * x - x);
     }
-    const float irq = __fdividef(1.f, r + A.qshift * A.afq[0][t]);
+    const float irq = __fdividef(1.f, r + A.qshift * afq[0][t]);
     if (!A.lskip) {
       const float ar = A.alphal * r;
       const float qt = __fdividef(1.0f, 1.0f + AS_QP * ar);
       const float ex = __expf(-ar * ar);
       const float erfcst = ((((AS_A5 * qt + AS_A4) * qt + AS_A3) * qt + AS_A2) * qt + AS_A1) * qt * ex;
-      const float furpar = A.afq[1][t] * qq;
+      const float furpar = afq[1][t] * qq;
       uq = furpar * erfcst * irq;
       // -dU/dr / r of erfc(alpha r) / rq: erfc / (r rq^2) + 2 alpha / sqrt(pi) e / (r rq)
       f += furpar * (erfcst * irq + A.twrtpi * ar * ex * ir) * irq * ir;
     } else if (!A.ewald) {
-      uq = A.afq[1][t] * qq * irq;
+      uq = afq[1][t] * qq * irq;
       f += uq * irq * ir;
     }
     *qf = f;
@@ -154,16 +155,16 @@ __device__ __forceinline__ void alch_pair_f32(const PairArgs& A, float r2, int t
     return;
   }
   const float auxa = rsqrtf(r2);
-  const float fq1 = A.afq[0][t];
+  const float fq1 = afq[0][t];
   const float auxaa = rsqrtf(A.qsoft * fq1 * fq1 + r2);
   float f = 0.f, uc = 0.f, uq = 0.f;
   if (eps4 > 1e-12f) {
     const float sig = A.at.opls ? 2.f * sqrtf(rmi * rmj) : rmi + rmj;
     const float s2 = sig * sig;
     const float r6 = __fdividef(r2 * r2 * r2, s2 * s2 * s2);
-    const float gp1 = __fdividef(1.f, A.ljsoft * A.af[0][t] + r6);
+    const float gp1 = __fdividef(1.f, A.ljsoft * af[0][t] + r6);
     const float gp2 = gp1 * gp1;
-    const float sc = A.af[1][t] * eps4;
+    const float sc = af[1][t] * eps4;
     f = sc * (2.f * gp1 * gp2 - gp2) * 6.f * r6 * auxa * auxa;
     uc = sc * (gp2 - gp1);
   }
@@ -173,11 +174,11 @@ __device__ __forceinline__ void alch_pair_f32(const PairArgs& A, float r2, int t
     const float qt = __fdividef(1.0f, 1.0f + AS_QP * ar);
     const float ex = __expf(-ar * ar);
     const float erfcst = ((((AS_A5 * qt + AS_A4) * qt + AS_A3) * qt + AS_A2) * qt + AS_A1) * qt * ex;
-    const float furpar = A.afq[1][t] * qq;
+    const float furpar = afq[1][t] * qq;
     uq = furpar * erfcst * auxaa;
     f += uq * auxaa * auxaa + furpar * A.twrtpi * ar * ex * auxa * auxa * auxaa;
   } else if (!A.ewald) {
-    uq = A.afq[1][t] * qq * auxaa;
+    uq = afq[1][t] * qq * auxaa;
     f += uq * auxaa * auxaa;
   }
   *qf = f;
@@ -192,6 +193,7 @@ __device__ __forceinline__ void alch_energy_fp64(const PairArgs& A, double rx, d
                                                  double2 sj, double qq, int t, double* cd, double* qd,
                                                  double* c0, double* q0, double* du) {
   const AlchTables& T = A.at;
+  const AlchDyn& D = *A.ad;
   const double rsq = rx * rx + ry * ry + rz * rz;
   if (T.shifted) {
     // force_ALCHEMY_shift's energies at lambda and lambda0, and dU/dlambda
@@ -203,13 +205,13 @@ __device__ __forceinline__ void alch_energy_fp64(const PairArgs& A, double rx, d
     if (epsmin > 1.0e-12) {
       const double sigma = T.opls ? 2.0 * sqrt(si.x * sj.x) : si.x + sj.x;
       const double c = T.ljshift_s * sigma;
-      const double rl = r + c * T.f[0][t], rl0 = r + c * T.f0[0][t];
+      const double rl = r + c * D.f[0][t], rl0 = r + c * D.f0[0][t];
       const double s1 = sigma / rl, s0 = sigma / rl0;
       const double x = s1 * s1 * s1 * s1 * s1 * s1, x0 = s0 * s0 * s0 * s0 * s0 * s0;
-      *cd = T.f[1][t] * epsmin * (x * x - x);
-      *c0 = T.f0[1][t] * epsmin * (x0 * x0 - x0);
-      *du = T.df[1][t] * epsmin * (x * x - x) +
-            T.f[1][t] * epsmin * (2.0 * x - 1.0) * (-6.0 * x / rl) * c * T.df[0][t];
+      *cd = D.f[1][t] * epsmin * (x * x - x);
+      *c0 = D.f0[1][t] * epsmin * (x0 * x0 - x0);
+      *du = D.df[1][t] * epsmin * (x * x - x) +
+            D.f[1][t] * epsmin * (2.0 * x - 1.0) * (-6.0 * x / rl) * c * D.df[0][t];
     }
     double g = 0.0;
     if (!A.lskip) {
@@ -221,15 +223,15 @@ __device__ __forceinline__ void alch_energy_fp64(const PairArgs& A, double rx, d
       g = qq;
     }
     if (g != 0.0) {
-      const double rq = r + T.qshift * T.fq[0][t], rq0 = r + T.qshift * T.fq0[0][t];
-      *qd = T.fq[1][t] * g / rq;
-      *q0 = T.fq0[1][t] * g / rq0;
-      *du += T.dfq[1][t] * g / rq - T.fq[1][t] * g / (rq * rq) * T.qshift * T.dfq[0][t];
+      const double rq = r + T.qshift * D.fq[0][t], rq0 = r + T.qshift * D.fq0[0][t];
+      *qd = D.fq[1][t] * g / rq;
+      *q0 = D.fq0[1][t] * g / rq0;
+      *du += D.dfq[1][t] * g / rq - D.fq[1][t] * g / (rq * rq) * T.qshift * D.dfq[0][t];
     }
     return;
   }
   const double auxa = 1.0 / sqrt(rsq);
-  const double fq = T.fq[0][t], fq0 = T.fq0[0][t];
+  const double fq = D.fq[0][t], fq0 = D.fq0[0][t];
   const double auxaa = 1.0 / sqrt(T.qsoft * (fq * fq) + rsq);
   const double auxa0 = 1.0 / sqrt(T.qsoft * (fq0 * fq0) + rsq);
   const double epsmin = 4.0 * sqrt(si.y * sj.y);
@@ -238,14 +240,14 @@ __device__ __forceinline__ void alch_energy_fp64(const PairArgs& A, double rx, d
     const double sigma = T.opls ? 2.0 * sqrt(si.x * sj.x) : si.x + sj.x;
     const double s2 = sigma * sigma;
     const double r6 = rsq * rsq * rsq / (s2 * s2 * s2);
-    const double gp1 = 1.0 / (T.ljsoft * T.f[0][t] + r6);
+    const double gp1 = 1.0 / (T.ljsoft * D.f[0][t] + r6);
     const double gp2 = gp1 * gp1;
-    const double gp10 = 1.0 / (T.ljsoft * T.f0[0][t] + r6);
+    const double gp10 = 1.0 / (T.ljsoft * D.f0[0][t] + r6);
     const double gp20 = gp10 * gp10;
     const double auxc = epsmin * (gp2 - gp1);
-    *cd = T.f[1][t] * auxc;
-    *c0 = T.f0[1][t] * epsmin * (gp20 - gp10);
-    *du = T.df[1][t] * auxc + T.f[1][t] * epsmin * (gp2 - 2.0 * gp1 * gp2) * T.ljsoft * T.df[0][t];
+    *cd = D.f[1][t] * auxc;
+    *c0 = D.f0[1][t] * epsmin * (gp20 - gp10);
+    *du = D.df[1][t] * auxc + D.f[1][t] * epsmin * (gp2 - 2.0 * gp1 * gp2) * T.ljsoft * D.df[0][t];
   }
   double g = 0.0;  // charge-pair kernel without its scale and soft core
   if (!A.lskip) {
@@ -257,9 +259,9 @@ __device__ __forceinline__ void alch_energy_fp64(const PairArgs& A, double rx, d
     g = qq;
   }
   if (g != 0.0) {
-    *qd = T.fq[1][t] * g * auxaa;
-    *q0 = T.fq0[1][t] * g * auxa0;
-    *du += T.dfq[1][t] * g * auxaa - T.fq[1][t] * g * T.qsoft * fq * T.dfq[0][t] * auxaa * auxaa * auxaa;
+    *qd = D.fq[1][t] * g * auxaa;
+    *q0 = D.fq0[1][t] * g * auxa0;
+    *du += D.dfq[1][t] * g * auxaa - D.fq[1][t] * g * T.qsoft * fq * D.dfq[0][t] * auxaa * auxaa * auxaa;
   }
 }
 
@@ -327,6 +329,7 @@ __global__ void __launch_bounds__(WPB * 32, MINB) k_pair(const PairArgs A) {
   __shared__ unsigned short s_slot[NQ][QS];
   __shared__ double s_red[WPB][ACC_N];
   __shared__ double s_vimg[WPB][9];
+  __shared__ float s_af[VAR == VAR_ALCH ? 2 : 1][9], s_afq[VAR == VAR_ALCH ? 2 : 1][9];
 
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int sub = lane / LPG, sl = lane % LPG, q = warp * SEG + sub;
@@ -337,6 +340,12 @@ __global__ void __launch_bounds__(WPB * 32, MINB) k_pair(const PairArgs A) {
   if (threadIdx.x < WPB * 9) s_vimg[threadIdx.x / 9][threadIdx.x % 9] = 0.0;
   if (staged)
     for (int k = threadIdx.x; k < nt2; k += blockDim.x) s_lj[k] = A.lj[k];
+  if constexpr (VAR == VAR_ALCH) {  // the current lambda tables
+    if (threadIdx.x < 18) {
+      s_af[threadIdx.x / 9][threadIdx.x % 9] = A.ad->af[threadIdx.x / 9][threadIdx.x % 9];
+      s_afq[threadIdx.x / 9][threadIdx.x % 9] = A.ad->afq[threadIdx.x / 9][threadIdx.x % 9];
+    }
+  }
   __syncthreads();
   const float2* lj = staged ? s_lj : A.lj;
   // under lskip_ewald an atom without LJ has no pair to evaluate
@@ -563,7 +572,8 @@ __global__ void __launch_bounds__(WPB * 32, MINB) k_pair(const PairArgs A) {
               if (eps4 < 1e-12f && A.lskip && A.ewald) continue;
               npairs++;
               tal = (fia >> VF_SSHIFT) + (fjb >> VF_SSHIFT) - 4;
-              alch_pair_f32(A, rx * rx + ry * ry + rz * rz, tal, sa.x, sfb.x, eps4, ai.w * ob.w, &qf, &conf, &coul);
+              alch_pair_f32(A, s_af, s_afq, rx * rx + ry * ry + rz * rz, tal, sa.x, sfb.x, eps4, ai.w * ob.w, &qf, &conf,
+                            &coul);
             } else {
               const float2 Lp = lj[s_ti[q][a] + tb];
               ljon = Lp.y != 0.f;

@@ -731,6 +731,9 @@ int pme_run(orac_gpu_ctx* ctx, int natom, const double* d_cart, const double* d_
   sm = (2 * (size_t)G.B + 1) * n3 * sizeof(float2);
   orac_launch(k_fft<ZC>, nb, FFT_THREADS, sm, ctx->stream, G);
   CKL();
+  // the energy alone (the second charge set of a non-equilibrium step's
+  // work): no potential back on the grid, no gather
+  if (!d_f && !d_ffix && !d_edq && !(d_sxyz && d_mol)) return ORAC_OK;
   {
     // y inverse
     make_plan(n2, &G.P);

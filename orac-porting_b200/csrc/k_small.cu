@@ -44,6 +44,10 @@ struct SmallArgs {
   // q are the full ones; intramol skips same-species listqq pairs
   const double4* lam4;
   int intramol;
+  // the work U(lambda) - U(lambda0) of fnb14_alchemy / ferrf_alchemy_add
+  // (their dwrk) with the lambda0 of each atom in lam40, into *work
+  const double4* lam40;
+  double* work;
 };
 
 // Coupling factors of one pair of fnb14_alchemy (src/fnb14_alchemy.f:
@@ -85,7 +89,7 @@ __device__ __forceinline__ void alch14_factors(double li, double lj, double di, 
 __device__ __forceinline__ void small_body(const SmallArgs& A) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   double e[4] = {0, 0, 0, 0};
-  double dedl = 0.0;
+  double dedl = 0.0, wk = 0.0;
   if (t < A.n) {
     const int stride = A.kind == 4 ? 3 : 2;  // listqq carries facQ
     const int i1 = A.pairs[stride * t] - 1, i2 = A.pairs[stride * t + 1] - 1;
@@ -118,6 +122,11 @@ __device__ __forceinline__ void small_body(const SmallArgs& A) {
         e[type] -= furpar * erfst / rsp;
         qforce = -furpar * (erfst - A.twrtpi * alphar * expcst) / (rsp * rsq);
         dedl = -(la.w * cb + ca * lb.w) * qab * erfst / rsp;
+        if (A.work) {
+          const double4 la0 = A.lam40[i1], lb0 = A.lam40[i2];
+          const double furpar0 = ((1.0 - fabs(la0.y)) * (1.0 - fabs(lb0.y)) - (double)facq) * qab;
+          wk = -furpar * erfst / rsp + furpar0 * erfst / rsp;
+        }
       }
     } else if (A.kind == 3) {
       // fnb14_alchemy, Ewald branch (src/fnb14_alchemy.f:225-341); ORAC
@@ -144,6 +153,13 @@ __device__ __forceinline__ void small_body(const SmallArgs& A) {
       e[2 + type] += qq * (aq * erfcst + aq2 * erff) / rsp;
       qforce += qq * (aq * (erfcst + A.twrtpi * alphar * expcst) + aq2 * (erff - A.twrtpi * alphar * expcst)) * rspqi;
       dedl = daf * elj + qq * (daq * erfcst + daq2 * erff) / rsp;
+      if (A.work) {
+        const double4 la0 = A.lam40[i1], lb0 = A.lam40[i2];
+        double af0, aq0, aq20;
+        alch14_factors(la0.x, lb0.x, 0.0, 0.0, false, &af0, &dum, &ddum, &ddum);
+        alch14_factors(la0.y, lb0.y, 0.0, 0.0, true, &aq0, &dum, &aq20, &ddum);
+        wk = (af * elj + qq * (aq * erfcst + aq2 * erff) / rsp) - (af0 * elj + qq * (aq0 * erfcst + aq20 * erff) / rsp);
+      }
     } else if (A.kind == 2) {
       // ferrf: subtract fudge q q erf(alpha r)/r
       const double furpar = (A.forces ? A.fudge : 1.0) * A.q[i1] * A.q[i2];
@@ -198,7 +214,7 @@ __device__ __forceinline__ void small_body(const SmallArgs& A) {
           atomicAdd(A.ffix + d * A.natom + i2, (unsigned long long)(-q));
         }
       }
-    } else if (A.forces) {
+    } else if (A.forces && A.f) {
       atomicAdd(A.f + i1, qforce * xa);
       atomicAdd(A.f + A.natom + i1, qforce * ya);
       atomicAdd(A.f + 2 * A.natom + i1, qforce * za);
@@ -223,6 +239,10 @@ __device__ __forceinline__ void small_body(const SmallArgs& A) {
   if (A.edq) {
     const double x = warp_sumd(dedl);
     if (lane == 0 && x != 0.0) atomicAdd(A.edq, x);
+  }
+  if (A.work) {
+    const double x = warp_sumd(wk);
+    if (lane == 0 && x != 0.0) atomicAdd(A.work, x);
   }
 }
 
@@ -348,6 +368,10 @@ int small_launch_set(orac_gpu_ctx* ctx, int n, const SmallSpec* specs) {
     if (p.npairs <= 0) continue;
     S.s[ns] = small_args(ctx, p.kind, p.xyz, p.pairs, p.ptype, p.npairs, p.t12, p.t6, p.fudge, p.lj_fudge,
                          p.coul_mode, 1, nullptr, p.e, p.ss, p.q, p.ffix, nullptr, p.edq);
+    if (p.work && p.kind >= 3) {
+      S.s[ns].lam40 = ctx->d_lam40;
+      S.s[ns].work = p.work;
+    }
     ns++;
     nmax = p.npairs > nmax ? p.npairs : nmax;
   }

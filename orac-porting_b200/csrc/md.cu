@@ -1259,6 +1259,9 @@ static ConsArgs big_args(orac_gpu_ctx* ctx, MdState& S, double dt, double tol) {
 // +5 fnb14_alchemy, +6 ferrf_alchemy_add; E_AQQ: ferrf_alchemy_add's
 // energies (solute, solvent)
 enum { E_BOND = 41, E_14 = 49, E_GRP = 53, E_ERF = 57, E_DUDL = 73, E_AQQ = 80, E_N = 82 };
+// scratch of non-equilibrium runs: the SPME sums of chrge0, the erf
+// corrections of chrgec and of chrge0, a shell's energies off energy steps
+enum { E_NE0 = 82, E_NEQ = 98, E_NEQ0 = 114, E_NESH = 130, E_ALL = 160 };
 
 // energy records kept on the device per context (the newest MD_REC_CAP)
 constexpr int MD_REC_CAP = 2048;
@@ -1331,6 +1334,11 @@ static int md_drift(orac_gpu_ctx* ctx, MdState& S, double dt, const double* c, i
 // (mts_furier, src/mts_furier.f:85-141): bonds and 1-3 pairs with forces,
 // 1-4 pairs with fudgec = 1 - fudge (src/mtsmd.f:474), constraints energy
 // only (their forces would be removed by the constraints)
+// a non-equilibrium schedule drives the lambdas (ne.cu)
+static bool md_ne(const orac_gpu_ctx* ctx) { return ctx->ne.on && ctx->d_ne && ctx->variant == VAR_ALCH; }
+// the work term of a level's shell: 0 M, 1 L, 2 H (+3: its reciprocal sum)
+static int ne_term(int lvl) { return lvl == LM ? 0 : (lvl == LL ? 1 : 2); }
+
 static int md_ferrf(orac_gpu_ctx* ctx, MdState& S, unsigned long long* f, bool energy) {
   const BondedDev& B = ctx->bd;
   const double* q = ctx->pme_q();
@@ -1353,10 +1361,18 @@ static int md_ferrf(orac_gpu_ctx* ctx, MdState& S, unsigned long long* f, bool e
 static int md_shell_pair(orac_gpu_ctx* ctx, MdState& S, char sh, int lvl, bool zero, double* e, bool energy) {
   unsigned long long* f = S.ffix[lvl];
   if (zero) CK(cudaMemsetAsync(f, 0, sizeof(unsigned long long) * 3 * ctx->N, ctx->stream));
-  const int flags = SH_PREPPED | SH_FIXED_OUT | (energy ? SH_ENERGY : 0);
+  // along a schedule every shell evaluates its energies: force_alchemy's
+  // dwrk, U(lambda) - U(lambda0) over the shell's pairs, is a work term
+  const bool ne = md_ne(ctx);
+  const int flags = SH_PREPPED | SH_FIXED_OUT | ((energy || ne) ? SH_ENERGY : 0);
   if (int rc = shell_run_r(ctx, sh, ctx->sh, ctx->d_xyz, ctx->d_grp, ctx->d_mol, reinterpret_cast<double*>(f),
-                           energy ? e : nullptr, nullptr, flags))
+                           energy ? e : (ne ? S.e + E_NESH : nullptr), nullptr, flags))
     return rc;
+  if (ne) {  // the H shell's term is held at once (the step's last work sum came before it)
+    const int t = ne_term(lvl);
+    double* dst = lvl == LH ? &ctx->d_ne->dw[t] : &ctx->d_ne->dwn[t];
+    CK(cudaMemcpyAsync(dst, ctx->d_xtra + 1, sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+  }
   const bool dudl = energy && ctx->variant == VAR_ALCH && ctx->d_dq;
   if (dudl)  // the shell's dU/dlambda (k_variant_out)
     CK(cudaMemcpyAsync(S.e + E_DUDL + lvl, ctx->d_xtra + 4, sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
@@ -1382,7 +1398,29 @@ static int md_shell_recip(orac_gpu_ctx* ctx, MdState& S, char sh, int lvl, bool 
                        nullptr, f, dudl ? ctx->d_dq : nullptr, dudl ? S.e + E_DUDL + 3 : nullptr))
     return rc;
   if (int rc = prof_end(ctx, slot)) return rc;
-  return md_ferrf(ctx, S, f, energy);
+  if (!md_ne(ctx)) return md_ferrf(ctx, S, f, energy);
+  // along a schedule: mts_furier_alchemy's dwrk (src/mts_furier_alchemy.f:
+  // 112-186), the SPME sum, erf corrections and self term of chrgec minus
+  // those of chrge0; a second SPME of chrge0 gives its energy only
+  const BondedDev& B = ctx->bd;
+  const int* lists[4] = {B.pbond, B.pcn, B.p13, B.p14};
+  const int n[4] = {B.nb, B.ncn, B.n13, B.n14};
+  const double fudge[4] = {1.0, 1.0, 1.0, 1.0 - B.fudge};
+  const int forces[4] = {1, 0, 1, 1};
+  double* eq[4] = {S.e + E_NEQ, S.e + E_NEQ + 4, S.e + E_NEQ + 8, S.e + E_NEQ + 12};
+  double* e0[4] = {S.e + E_NEQ0, S.e + E_NEQ0 + 4, S.e + E_NEQ0 + 8, S.e + E_NEQ0 + 12};
+  CK(cudaMemsetAsync(S.e + E_NEQ, 0, sizeof(double) * 32, ctx->stream));
+  if (int rc = ferrf_launch_lists(ctx, 4, lists, n, fudge, forces, eq, S.x, B.ss, ctx->d_qc, f, nullptr, nullptr))
+    return rc;
+  if (energy)  // the energy record's erf corrections
+    CK(cudaMemcpyAsync(S.e + E_ERF, S.e + E_NEQ, sizeof(double) * 16, cudaMemcpyDeviceToDevice, ctx->stream));
+  if (int rc = pme_run(ctx, ctx->N, S.x, ctx->d_q0, recip, ctx->volume, ctx->alphal, nullptr, S.e + E_NE0, nullptr,
+                       nullptr, nullptr, nullptr, nullptr))
+    return rc;
+  if (int rc = ferrf_launch_lists(ctx, 4, lists, n, fudge, forces, e0, S.x, B.ss, ctx->d_q0, nullptr, nullptr,
+                                  nullptr))
+    return rc;
+  return ne_recip_launch(ctx, S.e + 24, S.e + E_NE0, S.e + E_NEQ, S.e + E_NEQ0, 3 + ne_term(lvl), lvl == LH);
 }
 
 static int md_forces_shell(orac_gpu_ctx* ctx, MdState& S, char sh, int lvl, bool zero, double* e, bool energy) {
@@ -1434,14 +1472,20 @@ static int md_pairs_n1(orac_gpu_ctx* ctx, MdState& S, bool energy, bool with_m =
   int n = 0;
   const int coul = ctx->clewld ? 1 : 0;
   const bool alch = md_alch_intra(ctx);
-  if (B.have_pairs && B.n14 > 0)
+  const bool ne = md_ne(ctx);
+  if (B.have_pairs && B.n14 > 0) {
     sp[n++] = {alch ? 3 : 0, S.x, B.p14, B.t14, B.n14, B.e1412, B.e146, B.fudge, B.lj_fudge, coul,
                energy ? S.e + E_14 : nullptr, B.ss, ctx->d_aqd, S.ffix[LN1],
                (alch && energy) ? S.e + E_DUDL + 5 : nullptr};
+    if (ne && alch) {  // fnb14_alchemy's dwrk of this evaluation is dwrk14 (src/mtsmd.f:2903)
+      CK(cudaMemsetAsync(&ctx->d_ne->dwn[7], 0, sizeof(double), ctx->stream));
+      sp[n - 1].work = &ctx->d_ne->dwn[7];
+    }
+  }
   if (B.have_pairs && B.ningrp > 0)
     sp[n++] = {1, S.x, B.pgrp, B.nbt, B.ningrp, B.e12, B.e6, 1.0, 1.0, coul, energy ? S.e + E_GRP : nullptr, B.ss,
                ctx->d_aqd, S.ffix[LN1], nullptr};
-  if (with_m && alch) {
+  if (with_m && alch && !ne) {
     if (ctx->nlistqq < 0)
       if (int rc = alch_listqq_build(ctx)) return rc;
     if (ctx->nlistqq > 0)
@@ -1453,7 +1497,16 @@ static int md_pairs_n1(orac_gpu_ctx* ctx, MdState& S, bool energy, bool with_m =
 
 // ferrf_alchemy_add on an M step of a system without N1 pair terms
 static int md_alch_m(orac_gpu_ctx* ctx, MdState& S, bool energy) {
-  if (!md_alch_intra(ctx) || S.has_n1) return ORAC_OK;
+  if (!md_alch_intra(ctx) || (S.has_n1 && !md_ne(ctx))) return ORAC_OK;
+  if (md_ne(ctx)) {  // ferrf_alchemy_add's dwrk is dwrk_al (src/mtsmd.f:3035-3041)
+    if (ctx->nlistqq < 0)
+      if (int rc = alch_listqq_build(ctx)) return rc;
+    if (ctx->nlistqq <= 0) return ORAC_OK;
+    SmallSpec sp = {4, S.x, ctx->d_listqq, nullptr, ctx->nlistqq, nullptr, nullptr, 1.0, 1.0, 1,
+                    energy ? S.e + E_AQQ : nullptr, ctx->bd.ss, ctx->d_aqd, S.ffix[LM], nullptr,
+                    &ctx->d_ne->dwn[6]};
+    return small_launch_set(ctx, 1, &sp);
+  }
   if (ctx->nlistqq < 0)
     if (int rc = alch_listqq_build(ctx)) return rc;
   return alch_intra_launch(ctx, 4, S.x, S.ffix[LM], energy ? S.e + E_AQQ : nullptr,
@@ -1541,6 +1594,15 @@ static int md_step(orac_gpu_ctx* ctx, MdState& S, bool update, bool energy) {
     // exact fixed-point atomics), and all are joined before the next drift
     const bool side = S.has_n0 || due_n1 || (due_m && md_has_recip(ctx, S, 'm')) ||
                       (due_l && md_has_recip(ctx, S, 'l'));
+    // along a schedule the M step's order is ORAC's: the N1 level's pairs
+    // with the old lambdas, the lambda update, then every shell and
+    // reciprocal sum with the new ones (src/mtsmd.f:2900-3060)
+    const bool ne_m = md_ne(ctx) && due_m;
+    if (ne_m) {
+      if (due_n1)
+        if (int rc = md_pairs_n1(ctx, S, e_now, false)) return rc;
+      if (int rc = ne_lambda_launch(ctx, per[LM])) return rc;
+    }
     if (side) {
       if (int rc = sd.fork()) return rc;
       if (int rc = sd.run([&]() -> int {
@@ -1560,10 +1622,20 @@ static int md_step(orac_gpu_ctx* ctx, MdState& S, bool update, bool energy) {
     if (due_l)
       if (int rc = md_shell_pair(ctx, S, 'l', LL, false, S.e + 8, e_now)) return rc;
     // the N1 level's pair terms beside the bonded kernel on the side stream
-    if (due_n1)
+    if (due_n1 && !ne_m)
       if (int rc = md_pairs_n1(ctx, S, e_now, due_m)) return rc;
     if (side)
       if (int rc = sd.join()) return rc;
+    if (ne_m) {
+      // the M step's work, then the terms evaluated here become the held
+      // ones: M shell, listqq, 1-4, and the L shell and the reciprocal sums
+      // of the levels evaluated at this step
+      int commit = 1 | (1 << 6) | (1 << 7);
+      if (due_l) commit |= 1 << 1;
+      if (md_has_recip(ctx, S, 'm')) commit |= 1 << 3;
+      if (due_l && md_has_recip(ctx, S, 'l')) commit |= 1 << 4;
+      if (int rc = ne_sum_launch(ctx, commit)) return rc;
+    }
   }
   {
     const bool side = md_has_recip(ctx, S, 'h');
@@ -1633,7 +1705,7 @@ int orac_gpu_md_setup(orac_gpu_ctx* ctx, const double* x, const double* y, const
   if (dev_alloc(ctx, &S.x, 3 * (size_t)N) || dev_alloc(ctx, &S.v, 3 * (size_t)N) ||
       dev_alloc(ctx, &S.xo, 3 * (size_t)N) || dev_alloc(ctx, &S.ffix[0], 3 * (size_t)N) ||
       dev_alloc(ctx, &S.ffix[1], 3 * (size_t)N) || dev_alloc(ctx, &S.ffix[2], 3 * (size_t)N) ||
-      dev_alloc(ctx, &S.invm, N) || dev_alloc(ctx, &S.pm, N) || dev_alloc(ctx, &S.e, 96) || dev_alloc(ctx, &S.rec, (size_t)ORAC_MD_REC * MD_REC_CAP) ||
+      dev_alloc(ctx, &S.invm, N) || dev_alloc(ctx, &S.pm, N) || dev_alloc(ctx, &S.e, E_ALL) || dev_alloc(ctx, &S.rec, (size_t)ORAC_MD_REC * MD_REC_CAP) ||
       dev_alloc(ctx, &S.rec_n, 1) ||
       dev_alloc(ctx, &S.flag, 4))
     return ORAC_ERR_CUDA;
@@ -1645,7 +1717,7 @@ int orac_gpu_md_setup(orac_gpu_ctx* ctx, const double* x, const double* y, const
     if ((S.has_n1 && dev_alloc(ctx, &S.ffix[LN1], 3 * (size_t)N)) ||
         (S.has_n0 && dev_alloc(ctx, &S.ffix[LN0], 3 * (size_t)N)))
       return ORAC_ERR_CUDA;
-    CK(cudaMemset(S.e, 0, sizeof(double) * 96));
+    CK(cudaMemset(S.e, 0, sizeof(double) * E_ALL));
     CK(cudaMemset(S.rec_n, 0, sizeof(unsigned long long)));
     S.rec_cap = MD_REC_CAP;
   }
@@ -1901,6 +1973,11 @@ int orac_gpu_md_setup(orac_gpu_ctx* ctx, const double* x, const double* y, const
     if (int rc = md_phony(ctx, r2, 'l')) return rc;
   }
   if (ctx->variant == VAR_ALCH) ctx->nlistqq = -1;  // built with this setup's constraints
+  if (ctx->ne.on && ctx->variant == VAR_ALCH) {
+    // the schedule's starting lambdas before the first forces
+    const double tn0 = S.dth / ((double)S.lrespa * S.mrespa * S.n1respa * S.n0respa);
+    if (int rc = ne_init(ctx, tn0)) return rc;
+  }
   if (int rc = md_forces_shell(ctx, S, 'm', LM, true, S.e, true)) return rc;
   if (int rc = md_alch_m(ctx, S, false)) return rc;  // (systems without N1 pairs; else with the N1 level below)
   if (int rc = md_forces_shell(ctx, S, 'l', LL, true, S.e + 8, true)) return rc;

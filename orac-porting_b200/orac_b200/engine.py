@@ -331,6 +331,30 @@ class Engine:
         k = min(n.value, max_records, 2048)
         return out[:k * R].reshape(-1, R), n.value
 
+    def set_schedule(self, times_fs, ladded, laddedq, lremoved, lremovedq, t0=0.0, ljintra=False):
+        """A non-equilibrium alchemical run (orac_gpu_md_set_schedule): the
+        lambdas follow the schedule from t0 (fs) on; before md_setup."""
+        sch = [f64(times_fs), f64(ladded), f64(laddedq), f64(lremoved), f64(lremovedq)]
+        self._schedule = sch
+        check(self.ctx, self.lib.orac_gpu_md_set_schedule(self.ctx, len(sch[0]), *[a.ctypes.data for a in sch],
+                                                          float(t0), int(ljintra)), "md_set_schedule")
+
+    def md_work(self):
+        """(work, rtime, (ladd, lrm, laddq, lrmq), held terms[8]) of the
+        schedule's run (orac_gpu_md_work); work in internal energy units."""
+        out = np.zeros(14)
+        check(self.ctx, self.lib.orac_gpu_md_work(self.ctx, out.ctypes.data), "md_work")
+        return float(out[0]), float(out[1]), tuple(out[2:6]), out[6:14].copy()
+
+    def md_work_trace(self, max_records=8192):
+        """(rtime, work) after each M step, oldest first, and the count."""
+        out = np.zeros(2 * max(1, max_records))
+        n = C.c_int64()
+        check(self.ctx, self.lib.orac_gpu_md_work_trace(self.ctx, max_records, out.ctypes.data, C.byref(n)),
+              "md_work_trace")
+        k = min(n.value, max_records, 8192)
+        return out[:2 * k].reshape(-1, 2), n.value
+
     def md_state(self):
         n = self.s.ntap
         a = [np.zeros(n) for _ in range(6)]

@@ -92,6 +92,9 @@ def load():
         "orac_gpu_set_rem_factor_async": (i, [_P, d, _P]),
         "orac_gpu_rem_exchange": (i, [i, _D, _I, _D, d, C.c_longlong, d, _I]),
         "orac_gpu_md_records": (i, [_P, i, _P, C.POINTER(i64), i]),
+        "orac_gpu_md_set_schedule": (i, [_P, i, _P, _P, _P, _P, _P, d, i]),
+        "orac_gpu_md_work": (i, [_P, _P]),
+        "orac_gpu_md_work_trace": (i, [_P, i, _P, C.POINTER(i64)]),
         "orac_gpu_batch_sync": (i, [_P]),
         "orac_gpu_batch_destroy": (i, [_P]),
         "orac_gpu_batch_last_error": (C.c_char_p, [_P]),

@@ -19,6 +19,8 @@
 
 #include "orac_oracle.h"
 
+static const double PI_MD = 3.14159265358979323846; /* setuns.f:35 4*atan(1) */
+
 typedef struct {
   int ntap, ngrp, nprot, ma;
   const int *ss, *nbtype, *type, *atomg, *atomp, *grppt, *mapnl;
@@ -54,7 +56,123 @@ typedef struct {
   int n1respa, n0respa, has_n0, has_n1;
   double *fn0, *fn1;
   double e_bonded, e_tors, e_14grp, e_ferrf;
+  /* Alchemy in the loop (force_alchemy in the shells, do_pmesh_alchemy and
+   * ferrf_alchemy over the scaled charges, cself_alchemy, fnb14_alchemy on
+   * the N1 level, ferrf_alchemy_add over listqq after every M shell) and,
+   * with a schedule, the lambdas of a non-equilibrium run (alchemic,
+   * src/alchemic.f; the update of src/mtsmd.f:2963-2999) with ORAC's work
+   * sum (src/mtsmd.f:3042-3044). */
+  int alch, ne;
+  orc_variant V;
+  int* ssal;
+  double *rmin, *epsm;
+  int intramol, ljintra;
+  double gl[4], gl0[4]; /* ladd lrm laddq lrmq and ladd0 lrm0 laddq0 lrmq0 (cpropar) */
+  double *lam, *lamq, *lam0, *lamq0; /* per atom: lambda, lambdaq, lambda0, lambdaq0 */
+  double *qc, *q0;                   /* chrgec, chrge0 of mts_furier_alchemy */
+  int nlistqq;
+  int* listqq;
+  int ntimes;
+  double *trec, *sch[4]; /* timerec (fs); ladded laddedq lremoved lremovedq */
+  double t0, rtime;
+  long ninn0;
+  /* dwrkm dwrkl dwrkh dwrkrc_m dwrkrc_l dwrkrc_h dwrk_al dwrk14, and the sum */
+  double dw[8], wrk;
 } orc_md;
+
+/* the charge of mts_furier_alchemy (src/mts_furier_alchemy.f:96-111) */
+static double alch_charge(double q, double lq) {
+  const double a = fabs(lq);
+  if (a == 1.0) return 0.0;
+  if (a == 0.0) return q;
+  return (1.0 - a) * q;
+}
+
+static void alch_refresh(orc_md* M) {
+  orc_alch_set(M->V.fact, M->gl[0], M->gl[1], M->intramol, M->ljintra, 0);
+  orc_alch_set(M->V.factq, M->gl[2], M->gl[3], M->intramol, M->ljintra, 1);
+  orc_alch_set(M->V.fact0, M->gl0[0], M->gl0[1], M->intramol, M->ljintra, 0);
+  orc_alch_set(M->V.factq0, M->gl0[2], M->gl0[3], M->intramol, M->ljintra, 1);
+  for (int a = 0; a < M->ntap; a++) {
+    M->qc[a] = alch_charge(M->charge[a], M->lamq[a]);
+    M->q0[a] = alch_charge(M->charge[a], M->lamq0[a]);
+  }
+}
+
+/* alchemic (src/alchemic.f): the lambdas of the time slice that holds
+ * rtime, linear in time; the last slice that holds it wins; before the
+ * first point ladd = laddq = 1, lrm = lrmq = 0; after the last point its
+ * values.  sch: ladded laddedq lremoved lremovedq (ntimes each); g = ladd
+ * lrm laddq lrmq. */
+void orc_alchemic(int ntimes, const double* trec, const double* ladded, const double* laddedq,
+                  const double* lremoved, const double* lremovedq, double rtime, double* g) {
+  g[0] = 1.0;
+  g[1] = 0.0;
+  g[2] = 1.0;
+  g[3] = 0.0;
+  int i0 = -1;
+  for (int i = 0; i + 1 < ntimes; i++)
+    if (rtime >= trec[i] && rtime <= trec[i + 1]) i0 = i;
+  if (i0 >= 0) {
+    const double ts = trec[i0 + 1] - trec[i0];
+    const double va = (ladded[i0 + 1] - ladded[i0]) / ts, vr = (lremoved[i0 + 1] - lremoved[i0]) / ts;
+    const double vaq = (laddedq[i0 + 1] - laddedq[i0]) / ts, vrq = (lremovedq[i0 + 1] - lremovedq[i0]) / ts;
+    const double dt = rtime - trec[i0];
+    g[0] = ladded[i0] + va * dt;
+    g[1] = lremoved[i0] + vr * dt;
+    g[2] = laddedq[i0] + vaq * dt;
+    g[3] = lremovedq[i0] + vrq * dt;
+  }
+  if (rtime > trec[ntimes - 1]) {
+    const int n = ntimes - 1;
+    g[0] = ladded[n];
+    g[1] = lremoved[n];
+    g[2] = laddedq[n];
+    g[3] = lremovedq[n];
+  }
+}
+
+static void alchemic(const orc_md* M, double rtime, double* g) {
+  orc_alchemic(M->ntimes, M->trec, M->sch[0], M->sch[1], M->sch[2], M->sch[3], rtime, g);
+}
+
+/* the lambda update before an M shell (src/mtsmd.f:2963-2999): the
+ * previous values become lambda0, the schedule gives the new ones; the
+ * per-atom lambdas of the added (removed) atoms move only while ladd or
+ * laddq differ from 1 (lrm or lrmq from 0) */
+static void ne_update(orc_md* M) {
+  for (int k = 0; k < 4; k++) M->gl0[k] = M->gl[k];
+  alchemic(M, M->rtime, M->gl);
+  const int add = M->gl[0] != 1.0 || M->gl[2] != 1.0;
+  const int rm = M->gl[1] != 0.0 || M->gl[3] != 0.0;
+  for (int a = 0; a < M->ntap; a++) {
+    if (M->ssal[a] == 2 && add) {
+      M->lam0[a] = M->lam[a];
+      M->lamq0[a] = M->lamq[a];
+      M->lam[a] = M->gl[0];
+      M->lamq[a] = M->gl[2];
+    } else if (M->ssal[a] == -2 && rm) {
+      M->lam0[a] = M->lam[a];
+      M->lam[a] = -M->gl[1];
+      M->lamq0[a] = M->lamq[a];
+      M->lamq[a] = -M->gl[3];
+    }
+  }
+  alch_refresh(M);
+}
+
+/* cself_alchemy (src/cself_alchemy.f): the solute self energy of chrgec
+ * minus that of chrge0 */
+static double alch_self_work(const orc_md* M) {
+  double s = 0.0, s0 = 0.0;
+  for (int a = 0; a < M->ntap; a++)
+    if (M->ss[a] == 1) {
+      s += M->qc[a] * M->qc[a];
+      s0 += M->q0[a] * M->q0[a];
+    }
+  const double f = M->alphal / sqrt(PI_MD) * (1.0 - orc_erfc_as(M->rkcut / (2.0 * M->alphal)));
+  return -s * f + s0 * f;
+}
 
 #define ORC_MD_REC 16
 
@@ -80,22 +198,25 @@ static void md_coords(orc_md* M) {
   free(mt);
 }
 
-/* one call of force with explicit radii, like mts_forces (src/mts_forces.f) */
+/* one call of force with explicit radii, like mts_forces (src/mts_forces.f);
+ * with alchemy force_alchemy, its dwrk into *dwrk (may be null) */
 static long md_force(orc_md* M, const int* in, int* out, long capout, double rneigh, double rinn, double rout,
-                     double rtolinn, double rtolout, double* f, double* ue) {
+                     double rtolinn, double rtolout, double* f, double* ue, double* dwrk) {
   int N = M->ntap, G = M->ngrp;
   double st[9] = {0};
   double uel[6];
+  double extra[5] = {0, 0, 0, 0, 0};
   int lskip = orc_decide_force(rinn, M->alphal);
   double* tmp = (double*)calloc(3 * (size_t)N, sizeof(double));
-  long n = orc_force(M->ss, M->s, M->s + N, M->s + 2 * N, M->g, M->g + G, M->g + 2 * G, M->charge, M->nbtype,
-                     M->type, M->ma, N, M->atomg, M->m, M->m + M->nprot, M->m + 2 * M->nprot, M->atomp, M->co,
-                     M->ecc12, M->ecc6, M->alphal, M->mapnl, G, M->grppt, uel, tmp, tmp + N, tmp + 2 * N, st, in,
-                     out, capout, rneigh, rinn, rout, rtolinn, rtolout, M->pmass, 1, M->mass, M->massinfty, lskip, 1,
-                     M->nthreads);
+  long n = orc_force_ex(M->ss, M->s, M->s + N, M->s + 2 * N, M->g, M->g + G, M->g + 2 * G, M->charge, M->nbtype,
+                        M->type, M->ma, N, M->atomg, M->m, M->m + M->nprot, M->m + 2 * M->nprot, M->atomp, M->co,
+                        M->ecc12, M->ecc6, M->alphal, M->mapnl, G, M->grppt, uel, tmp, tmp + N, tmp + 2 * N, st, in,
+                        out, capout, rneigh, rinn, rout, rtolinn, rtolout, M->pmass, 1, M->mass, M->massinfty, lskip,
+                        1, M->nthreads, M->alch ? &M->V : NULL, M->alch ? extra : NULL);
   if (f)
     for (long k = 0; k < 3 * (long)N; k++) f[k] += tmp[k];
   if (ue) memcpy(ue, uel, sizeof(uel));
+  if (dwrk) *dwrk = extra[1];
   free(tmp);
   return n;
 }
@@ -116,13 +237,13 @@ static int md_lists(orc_md* M) {
     M->capl = M->caph;
     M->ll = (int*)realloc(M->ll, sizeof(int) * M->capl);
   }
-  if (md_force(M, M->lh, M->ll, M->capl, r[5], r[3], r[3], r[4], 0.0, NULL, NULL) < 0) return -1;
+  if (md_force(M, M->lh, M->ll, M->capl, r[5], r[3], r[3], r[4], 0.0, NULL, NULL, NULL) < 0) return -1;
   /* phony 'l' with rcutl=rcutm, rtoll=0: ro=rcutm ri=rcutm rto=0 rti=rtolm rni=rneim */
   if (M->capm < M->caph) {
     M->capm = M->caph;
     M->lm = (int*)realloc(M->lm, sizeof(int) * M->capm);
   }
-  if (md_force(M, M->ll, M->lm, M->capm, r[2], r[0], r[0], r[1], 0.0, NULL, NULL) < 0) return -1;
+  if (md_force(M, M->ll, M->lm, M->capm, r[2], r[0], r[0], r[1], 0.0, NULL, NULL, NULL) < 0) return -1;
   return 0;
 }
 
@@ -133,33 +254,40 @@ static int md_rattle(orc_md* M);
 /* The erf corrections of mts_furier (src/mts_furier.f:85-141) for the
  * excluded pairs: bonds and bends with forces, the 1-4 pairs with
  * fudgec = 1 - fudge (src/mtsmd.f:474), constraints energy only. */
-static void md_ferrf(orc_md* M, double* f) {
+static double md_ferrf_q(orc_md* M, const double* q, double* f);
+
+static void md_ferrf(orc_md* M, double* f) { M->e_ferrf = md_ferrf_q(M, M->alch ? M->qc : M->charge, f); }
+
+/* the corrections with charges q, forces into f (null: energy only);
+ * returns their energy */
+static double md_ferrf_q(orc_md* M, const double* q, double* f) {
   int N = M->ntap;
-  double fs[2], dummy_e = 0.0;
+  double fs[2], dummy_e = 0.0, e = 0.0;
   double* scratch = (double*)calloc(3 * (size_t)N, sizeof(double));
-  M->e_ferrf = 0.0;
+  if (!f) f = scratch;
   if (M->nb > 0) {
-    orc_ferrf(M->ss, M->alphal, M->charge, 1.0, M->x, M->x + N, M->x + 2 * N, 1, M->lbnd, M->nb, fs, f, f + N,
+    orc_ferrf(M->ss, M->alphal, q, 1.0, M->x, M->x + N, M->x + 2 * N, 1, M->lbnd, M->nb, fs, f, f + N,
               f + 2 * N);
-    M->e_ferrf += fs[0] + fs[1];
+    e += fs[0] + fs[1];
   }
   if (M->ncnst > 0) {
-    orc_ferrf(M->ss, M->alphal, M->charge, 1.0, M->x, M->x + N, M->x + 2 * N, 0, M->cnst, M->ncnst, fs, scratch,
+    orc_ferrf(M->ss, M->alphal, q, 1.0, M->x, M->x + N, M->x + 2 * N, 0, M->cnst, M->ncnst, fs, scratch,
               scratch + N, scratch + 2 * N);
-    M->e_ferrf += fs[0] + fs[1];
+    e += fs[0] + fs[1];
   }
   if (M->n13 > 0) {
-    orc_ferrf(M->ss, M->alphal, M->charge, 1.0, M->x, M->x + N, M->x + 2 * N, 1, M->int13, M->n13, fs, f, f + N,
+    orc_ferrf(M->ss, M->alphal, q, 1.0, M->x, M->x + N, M->x + 2 * N, 1, M->int13, M->n13, fs, f, f + N,
               f + 2 * N);
-    M->e_ferrf += fs[0] + fs[1];
+    e += fs[0] + fs[1];
   }
   if (M->n14 > 0) {
-    orc_ferrf(M->ss, M->alphal, M->charge, 1.0 - M->fudge, M->x, M->x + N, M->x + 2 * N, 1, M->int14, M->n14, fs,
+    orc_ferrf(M->ss, M->alphal, q, 1.0 - M->fudge, M->x, M->x + N, M->x + 2 * N, 1, M->int14, M->n14, fs,
               f, f + N, f + 2 * N);
-    M->e_ferrf += fs[0] + fs[1];
+    e += fs[0] + fs[1];
   }
   (void)dummy_e;
   free(scratch);
+  return e;
 }
 
 /* mts_intra_n0: fpbond + fpbend + fitors (src/mts_intra_n0.f:73-100) */
@@ -198,7 +326,13 @@ static void md_intra_n1(orc_md* M) {
     orc_fptors(M->ss, M->ltor, M->nt, x, y, z, M->tpota, M->tpotb, ue, fx, fy, fz);
     M->e_tors = ue[0] + ue[1];
   }
-  if (M->n14 > 0) {
+  if (M->n14 > 0 && M->alch) {
+    /* fnb14_alchemy with Ewald (src/mts_intra_n1.f:81-85): its dwrk is
+     * dwrk14 (src/mtsmd.f:2903) */
+    orc_fnb14_alchemy(M->ss, x, y, z, M->charge, M->ecc1412, M->ecc146, M->alphal, M->int14, M->n14, M->type14,
+                      M->fudge, 1.0, M->lam, M->lamq, M->lam0, M->lamq0, fx, fy, fz, ue, &M->dw[7]);
+    M->e_14grp += ue[0] + ue[1] + ue[2] + ue[3];
+  } else if (M->n14 > 0) {
     orc_fnb14(M->ss, x, y, z, M->charge, N, M->ecc1412, M->ecc146, 1, 1, M->alphal, M->int14, M->n14, M->type14,
               M->fudge, 1.0, fx, fy, fz, ue);
     M->e_14grp += ue[0] + ue[1] + ue[2] + ue[3];
@@ -213,27 +347,50 @@ static void md_intra_n1(orc_md* M) {
 static void md_forces(orc_md* M, char sh, double* f) {
   int N = M->ntap;
   double* r = M->sh;
+  const int lv = sh == 'm' ? 0 : (sh == 'l' ? 1 : 2);
   memset(f, 0, sizeof(double) * 3 * N);
   if (sh == 'm') {
-    md_force(M, M->lm, NULL, 0, 0.0, 0.0, r[0], 0.0, r[1], f, M->e[0]);
+    md_force(M, M->lm, NULL, 0, 0.0, 0.0, r[0], 0.0, r[1], f, M->e[0], &M->dw[0]);
   } else if (sh == 'l') {
-    md_force(M, M->ll, M->lm, M->capm, r[2], r[0], r[3], r[1], r[4], f, M->e[1]);
+    md_force(M, M->ll, M->lm, M->capm, r[2], r[0], r[3], r[1], r[4], f, M->e[1], &M->dw[1]);
   } else {
-    md_force(M, M->lh, M->ll, M->capl, r[5], r[3], r[6], r[4], r[7], f, M->e[2]);
+    md_force(M, M->lh, M->ll, M->capl, r[5], r[3], r[6], r[4], r[7], f, M->e[2], &M->dw[2]);
   }
+  if (sh == 'm' && M->alch && M->nlistqq > 0) {
+    /* ferrf_alchemy_add after the M shell (src/mtsmd.f:3035-3041) */
+    double fs[2];
+    orc_ferrf_alchemy_add(M->ss, M->alphal, M->charge, M->lamq, M->lamq0, M->x, M->x + N, M->x + 2 * N, M->listqq,
+                          M->nlistqq, M->intramol, fs, &M->dw[6], f, f + N, f + 2 * N);
+  }
+  /* the work of the M step, before the M level's reciprocal sum */
+  if (sh == 'm' && M->ne)
+    for (int k = 0; k < 8; k++) M->wrk += M->dw[k];
   if (M->rshk == sh) {
     double st[9] = {0};
-    orc_fft_pme(N, M->s, M->s + N, M->s + 2 * N, M->m, M->m + M->nprot, M->m + 2 * M->nprot, M->charge, M->co,
-                M->oc, M->volume, M->alphal, M->order, M->n1, M->n2, M->n3, &M->eer, f, f + N, f + 2 * N, st,
-                M->atomp, 0, M->rkcut, M->nthreads);
+    const double* q = M->alch ? M->qc : M->charge;
+    orc_fft_pme(N, M->s, M->s + N, M->s + 2 * N, M->m, M->m + M->nprot, M->m + 2 * M->nprot, q, M->co, M->oc,
+                M->volume, M->alphal, M->order, M->n1, M->n2, M->n3, &M->eer, f, f + N, f + 2 * N, st, M->atomp, 0,
+                M->rkcut, M->nthreads);
     md_ferrf(M, f);
+    if (M->ne) {
+      /* mts_furier_alchemy's dwrk (src/mts_furier_alchemy.f:112-186): the
+       * reciprocal sum, the erf corrections and the self term of chrgec
+       * minus those of chrge0 */
+      double eer0 = 0.0;
+      double* scr = (double*)calloc(3 * (size_t)N, sizeof(double));
+      orc_fft_pme(N, M->s, M->s + N, M->s + 2 * N, M->m, M->m + M->nprot, M->m + 2 * M->nprot, M->q0, M->co,
+                  M->oc, M->volume, M->alphal, M->order, M->n1, M->n2, M->n3, &eer0, scr, scr + N, scr + 2 * N, st,
+                  M->atomp, 0, M->rkcut, M->nthreads);
+      free(scr);
+      M->dw[3 + lv] = (M->eer - eer0) + (M->e_ferrf - md_ferrf_q(M, M->q0, NULL)) + alch_self_work(M);
+    }
   }
 }
 
 static void md_refresh_m(orc_md* M) {
   double* r = M->sh;
   /* phony 'l' with rcutl = rcutm: ro=rcutm rto=rtoll ri=rcutm rti=rtolm rni=rneim */
-  md_force(M, M->ll, M->lm, M->capm, r[2], r[0], r[0], r[1], r[4], NULL, NULL);
+  md_force(M, M->ll, M->lm, M->capm, r[2], r[0], r[0], r[1], r[4], NULL, NULL, NULL);
 }
 
 static void md_kick(orc_md* M, const double* f, double dt) {
@@ -616,6 +773,10 @@ int orc_md_run(void* h, int nsteps, int energy_every, double* rec) {
             fail |= md_shake(M, tn0);
             fail |= md_rattle(M);
             md_coords(M);
+            if (M->ne) { /* rtime = oldtime + ninn0 tn0 (src/mtsmd.f:2751) */
+              M->ninn0++;
+              M->rtime = M->t0 + (double)M->ninn0 * tn0;
+            }
             if (M->has_n0) {
               md_intra_n0(M);
               fail |= md_kick_r(M, M->fn0, tn0);
@@ -626,6 +787,7 @@ int orc_md_run(void* h, int nsteps, int energy_every, double* rec) {
             fail |= md_kick_r(M, M->fn1, tn1);
           }
         }
+        if (M->ne) ne_update(M);
         md_forces(M, 'm', M->fm);
         fail |= md_kick_r(M, M->fm, tm);
       }
@@ -655,6 +817,108 @@ int orc_md_run(void* h, int nsteps, int energy_every, double* rec) {
     }
   }
   return fail ? 1 : 0;
+}
+
+/* Alchemy in the loop: force_alchemy (soft core, or with shifted the
+ * shifted potential of force_ALCHEMY_shift), lam8 = ladd lrm laddq lrmq and
+ * ladd0 lrm0 laddq0 lrmq0 (the per-atom lambdas follow: added ladd / laddq,
+ * removed -lrm / -lrmq), listqq (ia, ib, facQ; 1-based) of the
+ * intra-alchemical Coulomb correction. */
+void orc_md_set_alchemy(void* h, const int* ss_alchemy, const double* rmin, const double* epsm, double qsoft,
+                        double ljsoft, int opls, int shifted, double qshift, double ljshift, int intramol,
+                        int ljintra, const double* lam8, const int* listqq, int nlistqq) {
+  orc_md* M = (orc_md*)h;
+  const int N = M->ntap;
+  M->alch = 1;
+  M->ssal = dup_i(ss_alchemy, N);
+  M->rmin = dup_d(rmin, N);
+  M->epsm = dup_d(epsm, N);
+  memset(&M->V, 0, sizeof(M->V));
+  M->V.mode = 2;
+  M->V.ss_alchemy = M->ssal;
+  M->V.rmin = M->rmin;
+  M->V.epsm = M->epsm;
+  M->V.qsoft = qsoft;
+  M->V.ljsoft = ljsoft;
+  M->V.opls = opls;
+  M->V.shifted = shifted;
+  M->V.qshift = qshift;
+  M->V.ljshift = ljshift;
+  M->intramol = intramol;
+  M->ljintra = ljintra;
+  for (int k = 0; k < 4; k++) {
+    M->gl[k] = lam8[k];
+    M->gl0[k] = lam8[4 + k];
+  }
+  M->lam = (double*)calloc(N, sizeof(double));
+  M->lamq = (double*)calloc(N, sizeof(double));
+  M->lam0 = (double*)calloc(N, sizeof(double));
+  M->lamq0 = (double*)calloc(N, sizeof(double));
+  M->qc = (double*)calloc(N, sizeof(double));
+  M->q0 = (double*)calloc(N, sizeof(double));
+  for (int a = 0; a < N; a++) {
+    if (M->ssal[a] == 2) {
+      M->lam[a] = M->gl[0];
+      M->lamq[a] = M->gl[2];
+      M->lam0[a] = M->gl0[0];
+      M->lamq0[a] = M->gl0[2];
+    } else if (M->ssal[a] == -2) {
+      M->lam[a] = -M->gl[1];
+      M->lamq[a] = -M->gl[3];
+      M->lam0[a] = -M->gl0[1];
+      M->lamq0[a] = -M->gl0[3];
+    }
+  }
+  M->nlistqq = nlistqq;
+  M->listqq = nlistqq > 0 ? dup_i(listqq, 3 * (size_t)nlistqq) : NULL;
+  alch_refresh(M);
+}
+
+/* A non-equilibrium run: the lambdas follow the schedule (times in fs,
+ * ntimes points) from time t0 on, set as ORAC sets them when it restarts a
+ * steered run (src/mtsmd.f:722-758: lambda = lambda0 = the schedule's
+ * values at t0 for the species whose values there are not 0 (the added
+ * atoms start at 1, the removed ones at 0 otherwise)), the work is zeroed. */
+void orc_md_set_schedule(void* h, int ntimes, const double* trec, const double* ladded, const double* laddedq,
+                         const double* lremoved, const double* lremovedq, double t0) {
+  orc_md* M = (orc_md*)h;
+  const int N = M->ntap;
+  M->ne = 1;
+  M->ntimes = ntimes;
+  M->trec = dup_d(trec, ntimes);
+  M->sch[0] = dup_d(ladded, ntimes);
+  M->sch[1] = dup_d(laddedq, ntimes);
+  M->sch[2] = dup_d(lremoved, ntimes);
+  M->sch[3] = dup_d(lremovedq, ntimes);
+  M->t0 = t0;
+  M->rtime = t0;
+  M->ninn0 = 0;
+  alchemic(M, t0, M->gl);
+  for (int k = 0; k < 4; k++) M->gl0[k] = M->gl[k];
+  const int add = M->gl[0] != 0.0 || M->gl[2] != 0.0;
+  const int rm = M->gl[1] != 0.0 || M->gl[3] != 0.0;
+  for (int a = 0; a < N; a++) {
+    if (M->ssal[a] == 2) {
+      M->lam[a] = M->lam0[a] = add ? M->gl[0] : 1.0;
+      M->lamq[a] = M->lamq0[a] = add ? M->gl[2] : 1.0;
+    } else if (M->ssal[a] == -2) {
+      M->lam[a] = M->lam0[a] = rm ? -M->gl[1] : 0.0;
+      M->lamq[a] = M->lamq0[a] = rm ? -M->gl[3] : 0.0;
+    }
+  }
+  for (int k = 0; k < 8; k++) M->dw[k] = 0.0;
+  M->wrk = 0.0;
+  alch_refresh(M);
+}
+
+/* out[0] the work so far, out[1] rtime, out[2..5] ladd lrm laddq lrmq,
+ * out[6..13] the latest work terms */
+void orc_md_work(void* h, double* out) {
+  orc_md* M = (orc_md*)h;
+  out[0] = M->wrk;
+  out[1] = M->rtime;
+  for (int k = 0; k < 4; k++) out[2 + k] = M->gl[k];
+  for (int k = 0; k < 8; k++) out[6 + k] = M->dw[k];
 }
 
 void orc_md_get_state(void* h, double* x, double* v) {
@@ -687,5 +951,8 @@ void orc_md_destroy(void* h) {
   void* extra[] = {M->lbnd, M->r0, M->kb, M->lbndg, M->bendpot, M->ltor, M->tpota, M->tpotb, M->litr, M->ipota,
                    M->ipotb, M->ipotc, M->int14, M->type14, M->ecc1412, M->ecc146, M->ingrp, M->int13, M->fn0, M->fn1};
   for (unsigned k = 0; k < sizeof(extra) / sizeof(extra[0]); k++) free(extra[k]);
+  void* alch[] = {M->ssal, M->rmin, M->epsm, M->lam, M->lamq, M->lam0, M->lamq0, M->qc, M->q0, M->listqq,
+                  M->trec, M->sch[0], M->sch[1], M->sch[2], M->sch[3]};
+  for (unsigned k = 0; k < sizeof(alch) / sizeof(alch[0]); k++) free(alch[k]);
   free(M);
 }

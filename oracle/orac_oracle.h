@@ -260,7 +260,12 @@ void orc_fnb14_alchemy(const int* ss_index, const double* xp0, const double* yp0
                        const double* lambda, const double* lambdaq, const double* lambda0, const double* lambdaq0,
                        double* fpx, double* fpy, double* fpz, double* ue, double* dwrk);
 
+/* alchemic (src/alchemic.f), orac_md.c */
+void orc_alchemic(int ntimes, const double* trec, const double* ladded, const double* laddedq,
+                  const double* lremoved, const double* lremovedq, double rtime, double* g);
+
 #ifdef __cplusplus
 }
 #endif
+
 #endif

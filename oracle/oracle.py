@@ -524,6 +524,38 @@ class OracleMD:
                                len(a["ecc1412"]), s.fudge, len(a["ingrp"]) // 2, a["ingrp"], len(a["int13"]) // 2,
                                a["int13"], n1respa, n0respa)
 
+    def set_alchemy(self, ss_alchemy, lam8, qsoft=0.5, ljsoft=0.5, opls=False, shifted=False, qshift=0.0,
+                    ljshift=0.0, intramol=False, ljintra=False):
+        """Alchemy in the loop (force_alchemy, do_pmesh_alchemy, ferrf over
+        the scaled charges, fnb14_alchemy, ferrf_alchemy_add over listqq):
+        lam8 = ladd lrm laddq lrmq ladd0 lrm0 laddq0 lrmq0."""
+        L, s = self.L, self.s
+        vp = C.c_void_p
+        rmin, epsm = s.alchemy_params()
+        lq = Oracle(s, nthreads=1).alch_listqq(ss_alchemy)
+        self._keep["alch"] = (_i(ss_alchemy), _f(rmin), _f(epsm), _f(lam8), _i(lq.ravel()))
+        a = self._keep["alch"]
+        L.orc_md_set_alchemy.argtypes = [vp, _I, _D, _D, C.c_double, C.c_double, C.c_int, C.c_int, C.c_double,
+                                         C.c_double, C.c_int, C.c_int, _D, _I, C.c_int]
+        L.orc_md_set_alchemy(self.h, a[0], a[1], a[2], qsoft, ljsoft, int(opls), int(bool(shifted)), qshift,
+                             ljshift, int(intramol), int(ljintra), a[3], a[4], len(lq))
+
+    def set_schedule(self, times_fs, ladded, laddedq, lremoved, lremovedq, t0=0.0):
+        """A non-equilibrium run (alchemic): the lambdas follow the schedule
+        from t0 (fs) on, the work starts at 0."""
+        L = self.L
+        sch = [_f(times_fs), _f(ladded), _f(laddedq), _f(lremoved), _f(lremovedq)]
+        self._keep["schedule"] = sch
+        L.orc_md_set_schedule.argtypes = [C.c_void_p, C.c_int, _D, _D, _D, _D, _D, C.c_double]
+        L.orc_md_set_schedule(self.h, len(sch[0]), *sch, float(t0))
+
+    def work(self):
+        """(work, rtime, (ladd, lrm, laddq, lrmq), latest work terms[8])."""
+        out = np.zeros(14)
+        self.L.orc_md_work.argtypes = [C.c_void_p, _D]
+        self.L.orc_md_work(self.h, out)
+        return float(out[0]), float(out[1]), tuple(out[2:6]), out[6:14].copy()
+
     def run(self, nsteps, energy_every=0):
         R = self.REC
         nrec = nsteps // energy_every if energy_every else 0
