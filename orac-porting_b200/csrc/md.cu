@@ -1368,11 +1368,9 @@ static int md_shell_pair(orac_gpu_ctx* ctx, MdState& S, char sh, int lvl, bool z
   if (int rc = shell_run_r(ctx, sh, ctx->sh, ctx->d_xyz, ctx->d_grp, ctx->d_mol, reinterpret_cast<double*>(f),
                            energy ? e : (ne ? S.e + E_NESH : nullptr), nullptr, flags))
     return rc;
-  if (ne) {  // the H shell's term is held at once (the step's last work sum came before it)
-    const int t = ne_term(lvl);
-    double* dst = lvl == LH ? &ctx->d_ne->dw[t] : &ctx->d_ne->dwn[t];
-    CK(cudaMemcpyAsync(dst, ctx->d_xtra + 1, sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
-  }
+  if (ne)  // pending until the M step's work sum commits it
+    CK(cudaMemcpyAsync(&ctx->d_ne->dwn[ne_term(lvl)], ctx->d_xtra + 1, sizeof(double), cudaMemcpyDeviceToDevice,
+                       ctx->stream));
   const bool dudl = energy && ctx->variant == VAR_ALCH && ctx->d_dq;
   if (dudl)  // the shell's dU/dlambda (k_variant_out)
     CK(cudaMemcpyAsync(S.e + E_DUDL + lvl, ctx->d_xtra + 4, sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
@@ -1420,7 +1418,7 @@ static int md_shell_recip(orac_gpu_ctx* ctx, MdState& S, char sh, int lvl, bool 
   if (int rc = ferrf_launch_lists(ctx, 4, lists, n, fudge, forces, e0, S.x, B.ss, ctx->d_q0, nullptr, nullptr,
                                   nullptr))
     return rc;
-  return ne_recip_launch(ctx, S.e + 24, S.e + E_NE0, S.e + E_NEQ, S.e + E_NEQ0, 3 + ne_term(lvl), lvl == LH);
+  return ne_recip_launch(ctx, S.e + 24, S.e + E_NE0, S.e + E_NEQ, S.e + E_NEQ0, 3 + ne_term(lvl), false);
 }
 
 static int md_forces_shell(orac_gpu_ctx* ctx, MdState& S, char sh, int lvl, bool zero, double* e, bool energy) {
@@ -1592,8 +1590,11 @@ static int md_step(orac_gpu_ctx* ctx, MdState& S, bool update, bool energy) {
     // intramolecular levels and SPME beside the shell pair kernels: each
     // adds into its own level accumulator (SPME into the pair kernel's, by
     // exact fixed-point atomics), and all are joined before the next drift
+    // the last drift also ends the H step: the H shell (after the L shell,
+    // whose list it rewrites) and its reciprocal sum join the same fork, so
+    // the H pair kernel overlaps the L level's SPME
     const bool side = S.has_n0 || due_n1 || (due_m && md_has_recip(ctx, S, 'm')) ||
-                      (due_l && md_has_recip(ctx, S, 'l'));
+                      (due_l && md_has_recip(ctx, S, 'l')) || (last && md_has_recip(ctx, S, 'h'));
     // along a schedule the M step's order is ORAC's: the N1 level's pairs
     // with the old lambdas, the lambda update, then every shell and
     // reciprocal sum with the new ones (src/mtsmd.f:2900-3060)
@@ -1611,6 +1612,8 @@ static int md_step(orac_gpu_ctx* ctx, MdState& S, bool update, bool energy) {
               if (int r2 = md_shell_recip(ctx, S, 'm', LM, e_now)) return r2;
             if (due_l)
               if (int r2 = md_shell_recip(ctx, S, 'l', LL, e_now)) return r2;
+            if (last)
+              if (int r2 = md_shell_recip(ctx, S, 'h', LH, energy)) return r2;
             return ORAC_OK;
           }))
         return rc;
@@ -1621,6 +1624,13 @@ static int md_step(orac_gpu_ctx* ctx, MdState& S, bool update, bool energy) {
     }
     if (due_l)
       if (int rc = md_shell_pair(ctx, S, 'l', LL, false, S.e + 8, e_now)) return rc;
+    if (last) {
+      if (int rc = md_shell_pair(ctx, S, 'h', LH, false, S.e + 16, energy)) return rc;
+      // the M list again from the new L list (src/mtsmd.f:3287-3295)
+      ShellRadii r = ctx->sh;
+      r.rcutl = r.rcutm;
+      if (int rc = md_phony(ctx, r, 'l')) return rc;
+    }
     // the N1 level's pair terms beside the bonded kernel on the side stream
     if (due_n1 && !ne_m)
       if (int rc = md_pairs_n1(ctx, S, e_now, due_m)) return rc;
@@ -1632,23 +1642,12 @@ static int md_step(orac_gpu_ctx* ctx, MdState& S, bool update, bool energy) {
       // of the levels evaluated at this step
       int commit = 1 | (1 << 6) | (1 << 7);
       if (due_l) commit |= 1 << 1;
+      if (last) commit |= 1 << 2;
       if (md_has_recip(ctx, S, 'm')) commit |= 1 << 3;
       if (due_l && md_has_recip(ctx, S, 'l')) commit |= 1 << 4;
+      if (last && md_has_recip(ctx, S, 'h')) commit |= 1 << 5;
       if (int rc = ne_sum_launch(ctx, commit)) return rc;
     }
-  }
-  {
-    const bool side = md_has_recip(ctx, S, 'h');
-    if (side) {
-      if (int rc = sd.fork()) return rc;
-      if (int rc = sd.run([&]() -> int { return md_shell_recip(ctx, S, 'h', LH, energy); })) return rc;
-    }
-    if (int rc = md_shell_pair(ctx, S, 'h', LH, false, S.e + 16, energy)) return rc;
-    ShellRadii r = ctx->sh;
-    r.rcutl = r.rcutm;
-    if (int rc = md_phony(ctx, r, 'l')) return rc;
-    if (side)
-      if (int rc = sd.join()) return rc;
   }
   {
     double c[NLV];
