@@ -200,6 +200,8 @@ int shell_run_r(orac_gpu_ctx* ctx, char rshell, const ShellRadii& radii, const d
   const bool want_e = (flags & SH_ENERGY) && d_e, want_s = (flags & SH_STRESS) && d_stress;
   a.energy = want_e ? 1 : 0;
   a.stress = want_s ? 1 : 0;
+  // the forces-only build sums force_alchemy's dwrk where a schedule asks
+  a.dwrk = (a.variant == VAR_ALCH && !want_e && !want_s) ? ctx->pair_dwrk : nullptr;
   if (flags & SH_FIXED_OUT) a.ffix = reinterpret_cast<unsigned long long*>(d_f);
   if (want_e || want_s) CK(cudaMemsetAsync(ctx->d_acc, 0, ACC_N * sizeof(double), ctx->stream));
   if (!(flags & SH_PREPPED))

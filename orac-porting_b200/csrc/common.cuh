@@ -45,6 +45,9 @@ enum { PROF_PAIR = 0, PROF_DRIFT = 1, PROF_PME = 2, PROF_BONDED = 3, PROF_NFAM =
 
 // Shell-kernel variants, the dispatch of src/mts_forces.f:118-153.
 enum { VAR_STD = 0, VAR_REM = 1, VAR_ALCH = 2 };
+// the pair kernel's build of the alchemy variant that also sums
+// force_alchemy's dwrk in a forces-only launch (a non-equilibrium schedule)
+constexpr int VAR_ALCHW = 3;
 
 // Per-atom variant flags (d_vflag): bit 0 REM segment atom, bit 1 mass at or
 // above massinfty, bits 4..7 ss_alchemy + 4.
@@ -153,6 +156,7 @@ struct PairArgs {
   float qsoft, ljsoft;
   float qshift, ljshift_s;  // shifted potential (at.shifted)
   const AlchDyn* ad;        // the lambda tables (device memory)
+  double* dwrk;             // forces-only launches under a schedule: dwrk accumulates here
   AlchTables at;            // the constants (qsoft, ljsoft, shifted, opls, shifts)
 };
 
@@ -379,6 +383,7 @@ struct orac_gpu_ctx {
   double4* d_lam4 = nullptr;
   double4* d_lam40 = nullptr;  // lambda0, lambdaq0 per atom (non-equilibrium runs)
   AlchDyn* d_ad = nullptr;  // the lambda tables the pair kernel reads
+  double* pair_dwrk = nullptr;  // set around a forces-only shell whose dwrk a schedule needs
   NeHost ne;                 // a non-equilibrium schedule (ne.cu)
   NeDev* d_ne = nullptr;
   int4* d_ne_alist = nullptr;  // alchemical atoms: (atom, +1 added / -1 removed, ss_index, 0)

@@ -307,6 +307,8 @@ __device__ __forceinline__ unsigned short slot_pack(int e, int t, int b, int n) 
 template <int MG, bool EN, int VAR, int LPG, int MINB>
 __global__ void __launch_bounds__(WPB * 32, MINB) k_pair(const PairArgs A) {
   pdl_enter();
+  // the alchemy variant, and its build that also sums force_alchemy's dwrk
+  constexpr bool ALCH = VAR == VAR_ALCH || VAR == VAR_ALCHW;
   constexpr int SEG = 32 / LPG;  // groups per warp
   constexpr int QE = Rings<MG, LPG>::QE, QS = Rings<MG, LPG>::QS;
   constexpr int NQ = WPB * SEG;  // groups per block
@@ -317,7 +319,7 @@ __global__ void __launch_bounds__(WPB * 32, MINB) k_pair(const PairArgs A) {
   __shared__ float s_pm[NQ][MG];
   __shared__ double s_qd[NQ][EN ? MG : 1];
   __shared__ int s_fi[NQ][VAR != VAR_STD ? MG : 1];
-  __shared__ float2 s_sf[NQ][VAR == VAR_ALCH ? MG : 1];
+  __shared__ float2 s_sf[NQ][ALCH ? MG : 1];
   // entry queue: centre distance and S, S', j group metadata, skip mask;
   // FP64 distance and S and the Cartesian image for the energy build
   __shared__ float4 s_edc[NQ][QE];
@@ -329,7 +331,7 @@ __global__ void __launch_bounds__(WPB * 32, MINB) k_pair(const PairArgs A) {
   __shared__ unsigned short s_slot[NQ][QS];
   __shared__ double s_red[WPB][ACC_N];
   __shared__ double s_vimg[WPB][9];
-  __shared__ float s_af[VAR == VAR_ALCH ? 2 : 1][9], s_afq[VAR == VAR_ALCH ? 2 : 1][9];
+  __shared__ float s_af[ALCH ? 2 : 1][9], s_afq[ALCH ? 2 : 1][9];
 
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int sub = lane / LPG, sl = lane % LPG, q = warp * SEG + sub;
@@ -340,7 +342,7 @@ __global__ void __launch_bounds__(WPB * 32, MINB) k_pair(const PairArgs A) {
   if (threadIdx.x < WPB * 9) s_vimg[threadIdx.x / 9][threadIdx.x % 9] = 0.0;
   if (staged)
     for (int k = threadIdx.x; k < nt2; k += blockDim.x) s_lj[k] = A.lj[k];
-  if constexpr (VAR == VAR_ALCH) {  // the current lambda tables
+  if constexpr (ALCH) {  // the current lambda tables
     if (threadIdx.x < 18) {
       s_af[threadIdx.x / 9][threadIdx.x % 9] = A.ad->af[threadIdx.x / 9][threadIdx.x % 9];
       s_afq[threadIdx.x / 9][threadIdx.x % 9] = A.ad->afq[threadIdx.x / 9][threadIdx.x % 9];
@@ -349,13 +351,17 @@ __global__ void __launch_bounds__(WPB * 32, MINB) k_pair(const PairArgs A) {
   __syncthreads();
   const float2* lj = staged ? s_lj : A.lj;
   // under lskip_ewald an atom without LJ has no pair to evaluate
-  const bool ljonly = VAR != VAR_ALCH && A.lskip && A.ewald;
+  const bool ljonly = !ALCH && A.lskip && A.ewald;
   const float remf = VAR == VAR_REM ? __ldg(A.remf) : 1.f;  // rem_factor(3)
   // this segment's bits of a warp ballot
   auto segbits = [&](unsigned b) -> unsigned { return SEG == 1 ? b : (b >> seg0) & 0xffffu; };
 
   double ec0 = 0, ec1 = 0, ec2 = 0, eq0 = 0, eq1 = 0, eq2 = 0;
   double ex0 = 0, ex1 = 0, ex2 = 0;  // variant sums (ACC_X)
+  // force_alchemy's dwrk of a forces-only launch under a schedule (A.dwrk):
+  // U(lambda) - U(lambda0) of the alchemical pairs, FP64 on the FP32 pair
+  // geometry (the other pairs' terms are equal at lambda and lambda0)
+  double wk = 0.0;
   unsigned npairs = 0, nscan = 0, nkept = 0;
   // image term of the molecular virial: each pass's per-lane FP32 terms are
   // summed over the warp in FP64 into this warp's accumulator (stress only;
@@ -389,7 +395,7 @@ __global__ void __launch_bounds__(WPB * 32, MINB) k_pair(const PairArgs A) {
       s_pm[q][sl] = A.apm[ifirst + sl];
       if (EN) s_qd[q][sl] = A.qd[ifirst + sl];
       if (VAR != VAR_STD) s_fi[q][sl] = A.vflag[ifirst + sl];
-      if (VAR == VAR_ALCH) s_sf[q][sl] = A.soft[ifirst + sl];
+      if (ALCH) s_sf[q][sl] = A.soft[ifirst + sl];
     }
     __syncwarp();
     // the i atoms' forces of this lane's pairs and S'V shares, in fixed
@@ -547,7 +553,7 @@ __global__ void __launch_bounds__(WPB * 32, MINB) k_pair(const PairArgs A) {
           const int tb = A.atype[jat];
           const double qbd = EN ? A.qd[jat] : 0.0;
           const int fjb = (VAR != VAR_STD) ? (int)A.vflag[jat] : 0;
-          const float2 sfb = (VAR == VAR_ALCH) ? A.soft[jat] : make_float2(0.f, 0.f);
+          const float2 sfb = ALCH ? A.soft[jat] : make_float2(0.f, 0.f);
           const float bx = dcs.x - ob.x, by = dcs.y - ob.y, bz = dcs.z - ob.z;
           double4 cd = make_double4(0.0, 0.0, 0.0, 1.0);
           if (EN) cd = s_ecd[q][e];
@@ -562,7 +568,7 @@ __global__ void __launch_bounds__(WPB * 32, MINB) k_pair(const PairArgs A) {
             float qf = 0.f, conf = 0.f, coul = 0.f;
             bool ljon = false;
             int tal = 0;
-            if constexpr (VAR == VAR_ALCH) {
+            if constexpr (ALCH) {
               // src/force_alchemy.f:412-451: exclusions and fixed-mass pairs
               // are always skipped; no LJ and no Coulomb skips the pair
               const int fia = s_fi[q][a];
@@ -574,6 +580,14 @@ __global__ void __launch_bounds__(WPB * 32, MINB) k_pair(const PairArgs A) {
               tal = (fia >> VF_SSHIFT) + (fjb >> VF_SSHIFT) - 4;
               alch_pair_f32(A, s_af, s_afq, rx * rx + ry * ry + rz * rz, tal, sa.x, sfb.x, eps4, ai.w * ob.w, &qf, &conf,
                             &coul);
+              if constexpr (VAR == VAR_ALCHW) {
+                if (tal != 6) {  // 6: two normal atoms
+                  double cdd, qdd, c0, q0, du;
+                  alch_energy_fp64(A, (double)rx, (double)ry, (double)rz, A.softd[ifirst + a], A.softd[jat],
+                                   A.qd[ifirst + a] * A.qd[jat], tal, &cdd, &qdd, &c0, &q0, &du);
+                  wk += ((cdd + qdd) - (c0 + q0)) * (double)dcs.w;
+                }
+              }
             } else {
               const float2 Lp = lj[s_ti[q][a] + tb];
               ljon = Lp.y != 0.f;
@@ -616,7 +630,7 @@ __global__ void __launch_bounds__(WPB * 32, MINB) k_pair(const PairArgs A) {
               const double ery = cd.y + ((double)ai.y - (double)ob.y);
               const double erz = cd.z + ((double)ai.z - (double)ob.z);
               double cdd, qdd;
-              if constexpr (VAR == VAR_ALCH) {
+              if constexpr (ALCH) {
                 double c0, q0, du;
                 alch_energy_fp64(A, erx, ery, erz, A.softd[ifirst + a], A.softd[jat], s_qd[q][a] * qbd, tal, &cdd,
                                  &qdd, &c0, &q0, &du);
@@ -754,6 +768,10 @@ __global__ void __launch_bounds__(WPB * 32, MINB) k_pair(const PairArgs A) {
       if (s2) atomicAdd(A.wcnt + (A.lskip ? 3 : 2), (unsigned long long)s2);
     }
   }
+  if constexpr (VAR == VAR_ALCHW) {
+    const double w = warp_sumd(wk);
+    if (lane == 0 && w != 0.0) atomicAdd(A.dwrk, w);
+  }
   // energies and the image virial: the EN build only (a stress request
   // selects it, pair_launch)
   if (!EN || !A.forces_on) return;
@@ -866,6 +884,8 @@ int pair_launch(orac_gpu_ctx* ctx, const PairArgs& a, int maxg) {
   if (maxg > ORAC_MAXG)
     return ctx_fail(ctx, ORAC_ERR_PARAM, "charge group of %d atoms exceeds %d", maxg, ORAC_MAXG);
   if (a.variant < VAR_STD || a.variant > VAR_ALCH) return ctx_fail(ctx, ORAC_ERR_PARAM, "variant %d", a.variant);
+  // the alchemy build that sums force_alchemy's dwrk (forces only)
+  const int var = (a.variant == VAR_ALCH && a.dwrk && !a.energy && !a.stress) ? VAR_ALCHW : a.variant;
   // atoms-per-group bound of the instantiation: 3 (waters, and chains cut
   // in threes), 4, or 8; half-warp groups and the occupancy classes only
   // for the two small bounds
@@ -879,9 +899,9 @@ int pair_launch(orac_gpu_ctx* ctx, const PairArgs& a, int maxg) {
   const bool en = a.energy || a.stress;  // the forces-only build keeps no sums
   // occupancy class of the forces-only build: 0, 1, 2 = 5, 6, 8 blocks per SM
   const int occ = (en || mgk == 2) ? 0 : (a.minb <= 5 ? 0 : (a.minb <= 7 ? 1 : 2));
-  switch ((((mgk * 3 + a.variant) * 2 + (en ? 1 : 0)) * 2 + (half ? 1 : 0)) * 3 + occ) {
+  switch ((((mgk * 4 + var) * 2 + (en ? 1 : 0)) * 2 + (half ? 1 : 0)) * 3 + occ) {
 #define ORAC_KP(MGK, MG, VAR, EN, LPG, OCC, MINB)                                               \
-  case (((MGK * 3 + VAR) * 2 + (EN ? 1 : 0)) * 2 + (LPG == 16 ? 1 : 0)) * 3 + OCC:             \
+  case (((MGK * 4 + VAR) * 2 + (EN ? 1 : 0)) * 2 + (LPG == 16 ? 1 : 0)) * 3 + OCC:             \
     orac_launch(k_pair<MG, EN, VAR, LPG, MINB>, nb, WPB * 32, smem, ctx->stream, a);            \
     break;
 #define ORAC_KP_L(MGK, MG, VAR, LPG)       \
@@ -892,6 +912,13 @@ int pair_launch(orac_gpu_ctx* ctx, const PairArgs& a, int maxg) {
 #define ORAC_KP_V(MGK, MG, VAR) \
   ORAC_KP_L(MGK, MG, VAR, 32)   \
   ORAC_KP_L(MGK, MG, VAR, 16)
+#define ORAC_KP_W(MGK, MG)                         \
+  ORAC_KP(MGK, MG, VAR_ALCHW, false, 32, 0, 5)     \
+  ORAC_KP(MGK, MG, VAR_ALCHW, false, 32, 1, 6)     \
+  ORAC_KP(MGK, MG, VAR_ALCHW, false, 32, 2, 8)     \
+  ORAC_KP(MGK, MG, VAR_ALCHW, false, 16, 0, 5)     \
+  ORAC_KP(MGK, MG, VAR_ALCHW, false, 16, 1, 6)     \
+  ORAC_KP(MGK, MG, VAR_ALCHW, false, 16, 2, 8)
     ORAC_KP_V(0, 3, VAR_STD)
     ORAC_KP_V(0, 3, VAR_REM)
     ORAC_KP_V(0, 3, VAR_ALCH)
@@ -904,6 +931,10 @@ int pair_launch(orac_gpu_ctx* ctx, const PairArgs& a, int maxg) {
     ORAC_KP(2, 8, VAR_REM, true, 32, 0, 1)
     ORAC_KP(2, 8, VAR_ALCH, false, 32, 0, 1)
     ORAC_KP(2, 8, VAR_ALCH, true, 32, 0, 1)
+    ORAC_KP_W(0, 3)
+    ORAC_KP_W(1, 4)
+    ORAC_KP(2, 8, VAR_ALCHW, false, 32, 0, 1)
+#undef ORAC_KP_W
 #undef ORAC_KP_V
 #undef ORAC_KP_L
 #undef ORAC_KP

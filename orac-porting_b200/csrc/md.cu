@@ -1361,16 +1361,23 @@ static int md_ferrf(orac_gpu_ctx* ctx, MdState& S, unsigned long long* f, bool e
 static int md_shell_pair(orac_gpu_ctx* ctx, MdState& S, char sh, int lvl, bool zero, double* e, bool energy) {
   unsigned long long* f = S.ffix[lvl];
   if (zero) CK(cudaMemsetAsync(f, 0, sizeof(unsigned long long) * 3 * ctx->N, ctx->stream));
-  // along a schedule every shell evaluates its energies: force_alchemy's
-  // dwrk, U(lambda) - U(lambda0) over the shell's pairs, is a work term
+  // along a schedule force_alchemy's dwrk, U(lambda) - U(lambda0) over the
+  // shell's pairs, is a work term: an energy evaluation yields it with the
+  // energies, a forces-only one sums it over the alchemical pairs; either
+  // way it stays pending until the M step's work sum commits it
   const bool ne = md_ne(ctx);
-  const int flags = SH_PREPPED | SH_FIXED_OUT | ((energy || ne) ? SH_ENERGY : 0);
-  if (int rc = shell_run_r(ctx, sh, ctx->sh, ctx->d_xyz, ctx->d_grp, ctx->d_mol, reinterpret_cast<double*>(f),
-                           energy ? e : (ne ? S.e + E_NESH : nullptr), nullptr, flags))
-    return rc;
-  if (ne)  // pending until the M step's work sum commits it
-    CK(cudaMemcpyAsync(&ctx->d_ne->dwn[ne_term(lvl)], ctx->d_xtra + 1, sizeof(double), cudaMemcpyDeviceToDevice,
-                       ctx->stream));
+  double* pend = ne ? &ctx->d_ne->dwn[ne_term(lvl)] : nullptr;
+  if (ne && !energy) {
+    CK(cudaMemsetAsync(pend, 0, sizeof(double), ctx->stream));
+    ctx->pair_dwrk = pend;
+  }
+  const int flags = SH_PREPPED | SH_FIXED_OUT | (energy ? SH_ENERGY : 0);
+  const int rc0 = shell_run_r(ctx, sh, ctx->sh, ctx->d_xyz, ctx->d_grp, ctx->d_mol, reinterpret_cast<double*>(f),
+                              energy ? e : nullptr, nullptr, flags);
+  ctx->pair_dwrk = nullptr;
+  if (rc0) return rc0;
+  if (ne && energy)
+    CK(cudaMemcpyAsync(pend, ctx->d_xtra + 1, sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
   const bool dudl = energy && ctx->variant == VAR_ALCH && ctx->d_dq;
   if (dudl)  // the shell's dU/dlambda (k_variant_out)
     CK(cudaMemcpyAsync(S.e + E_DUDL + lvl, ctx->d_xtra + 4, sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));

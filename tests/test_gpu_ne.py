@@ -24,9 +24,10 @@ TIMES = [0.0, 40.0, 80.0]
 LAMS = dict(ladded=[1.0, 1.0, 1.0], laddedq=[1.0, 1.0, 1.0], lremoved=[0.0, 0.0, 1.0], lremovedq=[0.0, 1.0, 1.0])
 FORMS = {"soft": {}, "shift": dict(shifted=True, qshift=4.0, ljshift=0.35)}
 # work: FP32 pair forces move the trajectory off the FP64 one by ~1e-7 A
-# per step; the work follows to this relative tolerance, with an absolute
-# floor of 1e-4 kJ/mol (internal units 10 J/mol)
-WORK_RTOL, WORK_ATOL = 2e-5, 1e-5
+# per step, and the shells' work terms of forces-only steps take the FP32
+# pair geometry; the work follows to this relative tolerance, with an
+# absolute floor of 1e-3 kJ/mol (the internal energy unit is 1e4 kJ/mol)
+WORK_RTOL, WORK_ATOL = 2e-5, 1e-7
 
 
 def pair(form, s=None):
@@ -58,10 +59,11 @@ def test_ne_work_and_trajectory_match_the_oracle(form):
         np.testing.assert_allclose(wg, wo, rtol=WORK_RTOL, atol=WORK_ATOL, err_msg=f"work after step {step}")
         np.testing.assert_allclose(dg, do, rtol=1e-4, atol=WORK_ATOL, err_msg=f"work terms after step {step}")
         works.append(wo)
-    # the charges and the LJ came off: work was done, and it stops growing
-    # once the schedule ends
-    assert abs(works[9]) > 1.0 and abs(works[19] - works[9]) > 1.0
-    assert abs(works[23] - works[20]) < 1e-6 * max(1.0, abs(works[23]))
+    # the charges and the LJ came off: work was done (tens of kJ/mol in
+    # each stage), and it stops once the schedule has ended and the held
+    # terms have been evaluated again
+    assert abs(works[9]) > 1e-3 and abs(works[19] - works[9]) > 1e-3
+    assert works[23] == works[21]
     xg, _ = g.md_state()
     xo, _ = o.state()
     assert np.abs(xg - xo).max() < 1e-4
@@ -76,7 +78,7 @@ def test_ne_swarm_in_one_batch_matches_each_alone():
     """A swarm of NE trajectories from different starting velocities, as
     test3/test4's MPI walkers, advanced by one graph launch per step: each
     walker's state equals its run alone bitwise (fixed-point forces), its
-    work to 1e-12 (FP64 energy sums in atomics of a varying order)."""
+    work to 1e-9 (FP64 work sums in atomics of a varying order)."""
     base = systems.ligand_in_water()
     walkers = []
     for k in range(3):
@@ -108,7 +110,7 @@ def test_ne_swarm_in_one_batch_matches_each_alone():
     for k, g in enumerate(engines):
         w = g.md_work()[0]
         x, _ = g.md_state()
-        assert abs(w - alone[k][0]) <= 1e-12 * abs(alone[k][0]), (k, w, alone[k][0])
+        assert abs(w - alone[k][0]) <= 1e-9 * abs(alone[k][0]), (k, w, alone[k][0])
         assert np.array_equal(x, alone[k][1]), k
         g.close()
     assert len({round(a[0], 6) for a in alone}) == 3  # the walkers differ
