@@ -356,78 +356,6 @@ __global__ void __launch_bounds__(FFT_THREADS) k_fft(const GridArgs A) {
   }
 }
 
-// The x and y passes of one z plane in one block (the whole plane in shared
-// memory): forward, r2c along x of the plane's n2 lines then c2c along y of
-// its h1 columns; inverse, c2c along y then c2r along x.  The same Stockham
-// passes on the same data as k_fft<XF> + k_fft<YF> (k_fft<YI> + k_fft<XI>),
-// so the grids are bitwise the same, with one launch and one trip through
-// global memory instead of two.  A.P is the x plan, Py the y plan.
-constexpr int XY_THREADS = 256;
-
-template <bool FWD>
-__global__ void __launch_bounds__(XY_THREADS) k_fft_xy(const GridArgs A, const FftPlan Py, const float2* tw2) {
-  pdl_enter();
-  extern __shared__ float2 sm[];
-  const int n1 = A.n1, n2 = A.n2, h1 = A.h1, k = blockIdx.x;
-  const int np = n1 * n2;
-  float2* a = sm;
-  float2* b = sm + np;
-  float2* tx = sm + 2 * np;
-  float2* ty = tx + n1;
-  for (int e = threadIdx.x; e < n1; e += blockDim.x) tx[e] = A.tw[e];
-  for (int e = threadIdx.x; e < n2; e += blockDim.x) ty[e] = tw2[e];
-  if (FWD) {
-    const size_t g0 = (size_t)k * np;
-    for (int e = threadIdx.x; e < np; e += blockDim.x) {
-      const long long q = (long long)A.qfix[g0 + e];
-      a[e] = make_float2((float)((double)q * (1.0 / ORAC_QSCALE)), 0.f);
-    }
-    __syncthreads();
-    float2* res = fft_smem(a, b, n2, A.P, tx, -1);  // lines j of n1
-    float2* col = res == a ? b : a;
-    for (int e = threadIdx.x; e < h1 * n2; e += blockDim.x) {
-      const int i = qdiv(e, Py.mn), j = e - i * n2;
-      col[i * n2 + j] = res[j * n1 + i];
-    }
-    __syncthreads();
-    float2* out = fft_smem(col, res, h1, Py, ty, -1);  // lines i of n2
-    for (int e = threadIdx.x; e < h1 * n2; e += blockDim.x) {
-      const int j = e / h1, i = e - j * h1;
-      A.cg[((size_t)k * n2 + j) * h1 + i] = out[i * n2 + j];
-    }
-  } else {
-    for (int e = threadIdx.x; e < h1 * n2; e += blockDim.x) {
-      const int j = e / h1, i = e - j * h1;
-      a[i * n2 + j] = A.cg[((size_t)k * n2 + j) * h1 + i];
-    }
-    __syncthreads();
-    float2* res = fft_smem(a, b, h1, Py, ty, +1);  // lines i of n2
-    float2* row = res == a ? b : a;
-    // Hermitian extension of each x line (c2r)
-    for (int e = threadIdx.x; e < np; e += blockDim.x) {
-      const int j = qdiv(e, A.P.mn), i = e - j * n1;
-      float2 v;
-      if (i < h1) {
-        v = res[i * n2 + j];
-      } else {
-        v = res[(n1 - i) * n2 + j];
-        v.y = -v.y;
-      }
-      row[e] = v;
-    }
-    __syncthreads();
-    float2* out = fft_smem(row, res, n2, A.P, tx, +1);  // lines j of n1
-    const size_t g0 = (size_t)k * np;
-    for (int e = threadIdx.x; e < np; e += blockDim.x) A.rg[g0 + e] = out[e].x;
-  }
-}
-
-// shared memory of k_fft_xy: two planes and both axes' twiddles
-size_t xy_smem(int n1, int n2) { return (2 * (size_t)n1 * n2 + n1 + n2) * sizeof(float2); }
-// the fused passes are taken where the plane fits the shared memory a block
-// can opt into
-constexpr size_t XY_SMEM_MAX = 200 * 1024;
-
 struct AtomArgs {
   int natom, order, n1, n2, n3;
   const double* xyz;  // [3N] Cartesian
@@ -700,13 +628,6 @@ int pme_setup(orac_gpu_ctx* ctx, int n1, int n2, int n3, int order) {
   const size_t ng = (size_t)n1 * n2 * n3;
   if (dev_alloc(ctx, &P.qfix, ng) || dev_alloc(ctx, &P.rgrid, ng) || dev_alloc(ctx, &P.cgrid, (size_t)P.h1 * n2 * n3))
     return ORAC_ERR_CUDA;
-  const size_t xs = xy_smem(n1, n2);
-  if (xs <= XY_SMEM_MAX && xs > 48 * 1024) {
-    // the largest plane any context of the device may take (an attribute of
-    // the function on the device, shared by its contexts)
-    CK(cudaFuncSetAttribute(k_fft_xy<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)XY_SMEM_MAX));
-    CK(cudaFuncSetAttribute(k_fft_xy<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)XY_SMEM_MAX));
-  }
   return ORAC_OK;
 }
 
@@ -784,16 +705,7 @@ int pme_run(orac_gpu_ctx* ctx, int natom, const double* d_cart, const double* d_
   G.eout = d_eout;
   int nb;
   size_t sm;
-  const bool fused = xy_smem(n1, n2) <= XY_SMEM_MAX;
-  FftPlan Py;
-  make_plan(n2, &Py);
-  if (fused) {
-    // x and y forward, one z plane per block
-    make_plan(n1, &G.P);
-    G.tw = P.tw1;
-    orac_launch(k_fft_xy<true>, n3, XY_THREADS, xy_smem(n1, n2), ctx->stream, G, Py, (const float2*)P.tw2);
-    CKL();
-  } else {
+  {
     // x forward (r2c)
     make_plan(n1, &G.P);
     G.tw = P.tw1;
@@ -822,13 +734,7 @@ int pme_run(orac_gpu_ctx* ctx, int natom, const double* d_cart, const double* d_
   // the energy alone (the second charge set of a non-equilibrium step's
   // work): no potential back on the grid, no gather
   if (!d_f && !d_ffix && !d_edq && !(d_sxyz && d_mol)) return ORAC_OK;
-  if (fused) {
-    // y and x inverse, one z plane per block
-    make_plan(n1, &G.P);
-    G.tw = P.tw1;
-    orac_launch(k_fft_xy<false>, n3, XY_THREADS, xy_smem(n1, n2), ctx->stream, G, Py, (const float2*)P.tw2);
-    CKL();
-  } else {
+  {
     // y inverse
     make_plan(n2, &G.P);
     G.tw = P.tw2;
