@@ -829,13 +829,16 @@ __device__ __forceinline__ void drift_molecule(const MolArgs& A, int t, const in
     }
   }
   const int nc = m.w & 0xff;
-  if (A.kick && nc > 0) {
-    bool ok;
-    if constexpr (W3)
-      ok = rattle3(xo, v, im);
-    else
-      ok = (m.w & STAR) ? rattle_star_n(nc, xo, v, im) : rattle_small(xo, v, im, A.cloc + m.z, nc);
-    if (!ok) atomicOr(A.flag, 1);
+  // RATTLE of the kicked velocities (rattle_correc after correc).  A rigid
+  // three-site molecule skips it: SETTLE and the Newton SHAKE move the
+  // atoms along the old bonds only, so a velocity change along those bonds
+  // leaves the constrained positions, and the velocities (x_new - x_old)/dt
+  // they leave, as they were (to rounding)
+  if constexpr (!W3) {
+    if (A.kick && nc > 0) {
+      const bool ok = (m.w & STAR) ? rattle_star_n(nc, xo, v, im) : rattle_small(xo, v, im, A.cloc + m.z, nc);
+      if (!ok) atomicOr(A.flag, 1);
+    }
   }
 #pragma unroll
   for (int a = 0; a < SMA; a++) {
