@@ -143,6 +143,8 @@ struct PairArgs {
   int lpg;
   // resident blocks per SM of the forces-only build (5, 6 or 8)
   int minb;
+  // warps per row (1, or 2 for whole-warp rows without a next-shell list)
+  int split;
   // variant (VAR_*); REM: seg_select kind and rem_factor(3)
   int variant;
   const unsigned char* vflag;  // [N]

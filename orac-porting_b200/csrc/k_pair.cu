@@ -380,13 +380,23 @@ __global__ void __launch_bounds__(WPB * 32, MINB) k_pair(const PairArgs A) {
 
   // every lane of a warp runs the same trip counts, so the warp-wide
   // ballots and shuffles stay convergent
-  for (int pw = blockIdx.x * WPB + warp; pw * SEG < A.ngrp; pw += gridDim.x * WPB) {
-    const int i = pw * SEG + sub;
+  // a row split between two warps (A.split = 2, whole-warp rows of a
+  // launch that writes no next-shell list): each takes a chunk-aligned half
+  // of the entries, and both add the i atoms' forces by exact fixed-point
+  // atomics, so the row's result does not change; its chain is half as long
+  const int split = SEG == 1 ? A.split : 1;
+  for (int pw = blockIdx.x * WPB + warp; pw * SEG < A.ngrp * split; pw += gridDim.x * WPB) {
+    const int gw = split == 2 ? pw >> 1 : pw;
+    const int part = pw - gw * split;
+    const int i = gw * SEG + sub;
     const bool gvalid = i < A.ngrp;
     const int2 mi = gvalid ? A.gmeta[i] : make_int2(0, 0);
     const int ifirst = mi.x, ni = mi.y & 0xff, typei = (mi.y >> 8) & 0xff, ljmi = mi.y >> 16;
     const double4 gi = gvalid ? A.gpos[i] : make_double4(0.0, 0.0, 0.0, 0.0);
-    const int row = gvalid ? A.off[i] : 0, m = gvalid ? A.cnt[i] : 0;
+    const int row = gvalid ? A.off[i] : 0, mrow = gvalid ? A.cnt[i] : 0;
+    // this warp's entries [k0, m) of the row
+    const int chunk = split == 2 ? ((mrow + 1) / 2 + LPG - 1) / LPG * LPG : mrow;
+    const int k0 = min(mrow, part * chunk), m = min(mrow, k0 + chunk);
     int mmax = m;
     if (SEG == 2) mmax = max(mmax, __shfl_xor_sync(FULL, m, 16));
     if (sl < ni) {
@@ -408,7 +418,7 @@ __global__ void __launch_bounds__(WPB * 32, MINB) k_pair(const PairArgs A) {
     int nout = 0;
     int qh = 0, qn = 0;  // entry queue: head, entries pending
     int sh = 0, sn = 0;  // slot queue: head, slots pending
-    for (int base = 0; base < mmax; base += LPG) {
+    for (int base = k0; base < mmax; base += LPG) {
       // ---- phase 1: geometry of list entry k (src/force.f:265-333)
       const int k = base + sl;
       const bool valid = k < m;
@@ -892,7 +902,9 @@ int pair_launch(orac_gpu_ctx* ctx, const PairArgs& a, int maxg) {
   const int mgk = maxg <= 3 ? 0 : (maxg <= 4 ? 1 : 2);
   const bool half = mgk < 2 && a.lpg == 16;
   const int gpb = WPB * (half ? 2 : 1);  // groups per block
-  int nb = (a.ngrp + gpb - 1) / gpb;
+  if (a.split != 1 && (a.split != 2 || half || a.next_on))
+    return ctx_fail(ctx, ORAC_ERR_PARAM, "row split %d with %s", a.split, a.next_on ? "a next-shell list" : "lpg 16");
+  int nb = (a.ngrp * a.split + gpb - 1) / gpb;
   if (nb < 1) nb = 1;
   int slot = -1;
   if (int rc = prof_begin(ctx, &slot)) return rc;
