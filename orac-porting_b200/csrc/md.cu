@@ -708,11 +708,18 @@ __device__ __forceinline__ void group_centre(const MolArgs& A, int gi) {
   }
 }
 
+// The molecule kinds of the drift and kick kernels: the solvers of a rigid
+// three-site molecule and of a star cluster index their arrays by
+// constants, so those arrays stay in registers; the general solvers index
+// them by constraint (local memory)
+enum { MK_GENERAL = 0, MK_W3 = 1, MK_STAR = 2 };
+
 // correc (v += f dt/2m) from the fixed-point level accumulators, then RATTLE,
-// for one small molecule (W3: a rigid three-site one, in registers)
-template <bool W3>
+// for one small molecule of kind KIND
+template <int KIND>
 __device__ __forceinline__ void kick_molecule(const MolArgs& A, const int4 m) {
   const int N = A.N;
+  constexpr bool W3 = KIND == MK_W3;
   const int na = W3 ? 3 : m.y;
   int gat[SMA];
   double im[SMA];
@@ -741,8 +748,10 @@ __device__ __forceinline__ void kick_molecule(const MolArgs& A, const int4 m) {
   bool ok;
   if constexpr (W3)
     ok = rattle3(x, v, im);
+  else if constexpr (KIND == MK_STAR)
+    ok = rattle_star_n(m.w & 0xff, x, v, im);
   else
-    ok = (m.w & STAR) ? rattle_star_n(m.w & 0xff, x, v, im) : rattle_small(x, v, im, A.cloc + m.z, m.w & 0xff);
+    ok = rattle_small(x, v, im, A.cloc + m.z, m.w & 0xff);
   if (!ok) atomicOr(A.flag, 1);
 #pragma unroll
   for (int a = 0; a < SMA; a++) {
@@ -761,9 +770,11 @@ __global__ void k_kick(const MolArgs A) {
   if (t < A.nsm) {
     const int4 m = __ldg(&A.sm[t]);
     if (m.w & MOL3)
-      kick_molecule<true>(A, m);
+      kick_molecule<MK_W3>(A, m);
+    else if (m.w & STAR)
+      kick_molecule<MK_STAR>(A, m);
     else
-      kick_molecule<false>(A, m);
+      kick_molecule<MK_GENERAL>(A, m);
   } else if (t < A.nsm + A.nfree) {
     pdl_enter();
     const int g = A.free_atoms[t - A.nsm];
@@ -778,12 +789,12 @@ __global__ void k_kick(const MolArgs A) {
 
 // One small constrained molecule (thread t): verlet drift (src/verlet.f) +
 // SHAKE + RATTLE, then the scaled frame, group centres (appbou) and the
-// pair-kernel inputs of its groups.  W3: a rigid three-site molecule
-// (SETTLE or Newton SHAKE), whose arrays are indexed by constants only and
-// stay in registers; otherwise the general clusters, whose solvers index by
-// constraint and keep their arrays in local memory.
-template <bool W3>
+// pair-kernel inputs of its groups, for a molecule of kind KIND (a rigid
+// three-site molecule: SETTLE or Newton SHAKE; a star cluster; the general
+// small molecule).
+template <int KIND>
 __device__ __forceinline__ void drift_molecule(const MolArgs& A, int t, const int4 m) {
+  constexpr bool W3 = KIND == MK_W3;
   const int N = A.N;
   const double dt = A.dt;
   const int na = W3 ? 3 : m.y;
@@ -836,7 +847,11 @@ __device__ __forceinline__ void drift_molecule(const MolArgs& A, int t, const in
   // they leave, as they were (to rounding)
   if constexpr (!W3) {
     if (A.kick && nc > 0) {
-      const bool ok = (m.w & STAR) ? rattle_star_n(nc, xo, v, im) : rattle_small(xo, v, im, A.cloc + m.z, nc);
+      bool ok;
+      if constexpr (KIND == MK_STAR)
+        ok = rattle_star_n(nc, xo, v, im);
+      else
+        ok = rattle_small(xo, v, im, A.cloc + m.z, nc);
       if (!ok) atomicOr(A.flag, 1);
     }
   }
@@ -856,7 +871,7 @@ __device__ __forceinline__ void drift_molecule(const MolArgs& A, int t, const in
     const bool iso = im[1] == im[2] && fabs(L2v[0] - L2v[1]) <= 1e-12 * L2v[0];
     if (!(iso ? settle3(x, xo, v, im, L2v, A.idt) : shake3(x, xo, v, im, L2v, dt, A.tol))) atomicOr(A.flag, 1);
     if (!rattle3(x, v, im)) atomicOr(A.flag, 1);
-  } else if (m.w & STAR) {
+  } else if constexpr (KIND == MK_STAR) {
     if (!shake_star_n(nc, x, xo, v, im, A.dss + m.z, A.idt, A.tol)) atomicOr(A.flag, 1);
     if (!rattle_star_n(nc, x, v, im)) atomicOr(A.flag, 1);
   } else if (nc > 0) {
@@ -919,9 +934,11 @@ __global__ void k_drift(const MolArgs A) {
   if (t < A.nsm) {
     const int4 m = __ldg(&A.sm[t]);
     if (m.w & MOL3)
-      drift_molecule<true>(A, t, m);
+      drift_molecule<MK_W3>(A, t, m);
+    else if (m.w & STAR)
+      drift_molecule<MK_STAR>(A, t, m);
     else
-      drift_molecule<false>(A, t, m);
+      drift_molecule<MK_GENERAL>(A, t, m);
   } else if (t < A.nsm + A.ndg) {
     pdl_enter();
     // a group of an unconstrained molecule: its atoms, then its centre
