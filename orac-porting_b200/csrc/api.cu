@@ -197,9 +197,11 @@ int shell_run_r(orac_gpu_ctx* ctx, char rshell, const ShellRadii& radii, const d
   else
     a.lpg = ctx->tune_lpg_lh ? ctx->tune_lpg_lh : 32;
   a.minb = ctx->tune_minb ? ctx->tune_minb : (ctx->shared_device ? 8 : 6);
-  // the M shell of a context alone: a row's entries split between two
-  // warps (twice the warps in flight; the shell writes no next list)
-  a.split = (rshell == 'm' && a.lpg == 32 && !a.next_on && !ctx->shared_device) ? 2 : 1;
+  // a row's entries split between two warps: only where twice the warps
+  // still fit in one wave (a launch of the M shell, which writes no next
+  // list, on a system of at most 1,024 groups); beyond that the second
+  // wave costs more than the shorter chains save
+  a.split = (rshell == 'm' && a.lpg == 32 && !a.next_on && !ctx->shared_device && ctx->G <= 1024) ? 2 : 1;
   const bool want_e = (flags & SH_ENERGY) && d_e, want_s = (flags & SH_STRESS) && d_stress;
   a.energy = want_e ? 1 : 0;
   a.stress = want_s ? 1 : 0;
