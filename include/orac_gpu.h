@@ -387,7 +387,10 @@ int orac_gpu_md_set_graphs(orac_gpu_ctx* ctx, int on);
  * record's number) into a ring of the newest 2,048 records of the context.
  * Copies the newest min(max, kept) records, oldest first, to out; n_total
  * receives the number written since the last reset; reset != 0 clears the
- * count.  Synchronises the context's stream. */
+ * count.  Column 15 holds dU/dlambda for alchemical windows
+ * (orac_gpu_set_lambda with dlam), the segment energy for REM contexts and
+ * the work so far under a non-equilibrium schedule.  Synchronises the
+ * context's stream. */
 int orac_gpu_md_records(orac_gpu_ctx* ctx, int max, double* out,
                         int64_t* n_total, int reset);
 

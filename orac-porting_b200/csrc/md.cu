@@ -1056,7 +1056,8 @@ __global__ void k_rattle_big(const ConsArgs A) {
 // intra-group pairs, [14] erf corrections, [15] dU/dlambda (alchemy) or the
 // REM segment's nonbonded energy (REM).
 __global__ void k_record(const double* __restrict__ e, const int* __restrict__ flag, double econst, double self_dudl,
-                         int var, double* __restrict__ ring, int cap, unsigned long long* __restrict__ n) {
+                         int var, double* __restrict__ ring, int cap, unsigned long long* __restrict__ n,
+                         const NeDev* __restrict__ ne) {
   pdl_enter();
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   const unsigned long long k = *n;
@@ -1081,6 +1082,8 @@ __global__ void k_record(const double* __restrict__ e, const int* __restrict__ f
     d += self_dudl;
   } else if (var == 1) {  // REM: the segment energy of the three shells (rem_pot(3))
     for (int q = 73; q < 76; q++) d += e[q];
+  } else if (var == 3) {  // a non-equilibrium schedule: the work so far (wrk_alchemy)
+    d = ne->wrk;
   }
   r[12] = b;
   r[13] = p;
@@ -1685,9 +1688,9 @@ static int md_step(orac_gpu_ctx* ctx, MdState& S, bool update, bool energy) {
     CK(cudaMemsetAsync(S.e + 40, 0, sizeof(double), ctx->stream));
     orac_launch(k_ekin, 64, 256, 0, ctx->stream, ctx->N, S.v, S.invm, S.e + 40);
     CKL();
-    orac_launch(k_record, 1, 32, 0, ctx->stream, S.e, S.flag, S.econst, ctx->self_dudl,
-                (ctx->variant == VAR_ALCH && ctx->d_dq) ? 2 : (ctx->variant == VAR_REM ? 1 : 0), S.rec, S.rec_cap,
-                S.rec_n);
+    const int var = md_ne(ctx) ? 3 : ((ctx->variant == VAR_ALCH && ctx->d_dq) ? 2 : (ctx->variant == VAR_REM ? 1 : 0));
+    orac_launch(k_record, 1, 32, 0, ctx->stream, S.e, S.flag, S.econst, ctx->self_dudl, var, S.rec, S.rec_cap,
+                S.rec_n, (const NeDev*)ctx->d_ne);
     CKL();
   }
   return ORAC_OK;
@@ -2240,6 +2243,9 @@ static int md_run_impl(orac_gpu_ctx* ctx, int nsteps, int energy_every, double* 
       if (ctx->variant == VAR_ALCH && ctx->d_dq) {
         for (int q = E_DUDL; q < E_DUDL + 7; q++) r[15] += e[q];
         r[15] += ctx->self_dudl;
+      }
+      if (md_ne(ctx)) {  // a non-equilibrium schedule: the work so far (wrk_alchemy)
+        CK(cudaMemcpy(&r[15], &ctx->d_ne->wrk, sizeof(double), cudaMemcpyDeviceToHost));
       }
       r[10] = r[1] + r[2] + r[3] + r[4] + r[5] + r[6] + r[7] + r[8] + r[9] + r[12] + r[13] + r[14];
       r[11] = (double)flag;

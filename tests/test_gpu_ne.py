@@ -74,6 +74,9 @@ def test_ne_work_and_trajectory_match_the_oracle(form):
     assert n == 24 * 8
     np.testing.assert_allclose(np.diff(tr[:, 0]), 0.5, rtol=0, atol=1e-12)
     assert tr[-1, 1] == wg
+    # an energy step's record carries the work in column 15
+    rec = g.md_run(1, energy_every=1)
+    assert rec[0, 15] == g.md_work()[0]
 
 
 def test_ne_swarm_in_one_batch_matches_each_alone():
