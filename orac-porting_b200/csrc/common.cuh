@@ -216,6 +216,7 @@ struct PmePlan {
   unsigned long long* qfix = nullptr;  // [n1*n2*n3] fixed-point charge grid
   float2* cgrid = nullptr;             // [h1*n2*n3] complex grid
   float* rgrid = nullptr;              // [n1*n2*n3] real grid after c2r
+  float2* cgsave = nullptr;            // [h1*n2*n3] a kept transformed grid (non-equilibrium work)
   float4* theta = nullptr;             // per atom spline data cache
   int natom_cap = 0;
 };
@@ -389,6 +390,7 @@ struct orac_gpu_ctx {
   NeHost ne;                 // a non-equilibrium schedule (ne.cu)
   NeDev* d_ne = nullptr;
   int4* d_ne_alist = nullptr;  // alchemical atoms: (atom, +1 added / -1 removed, ss_index, 0)
+  double* d_ne_dq = nullptr;   // chrgec - chrge0 per atom
   int ne_nal = 0;
   int* d_listqq = nullptr;
   int nlistqq = -1;  // -1: not built for the current species
@@ -532,7 +534,9 @@ int pme_run(orac_gpu_ctx* ctx, int natom, const double* d_cart /*3N*/,
             double alpha, double* d_f /*3N accumulated*/, double* d_eout,
             const double* d_sxyz, const double* d_mol,
             unsigned long long* d_ffix = nullptr /*3N fixed point instead of d_f*/,
-            const double* d_dq = nullptr, double* d_edq = nullptr /*sum phi_i dq_i, accumulated*/);
+            const double* d_dq = nullptr, double* d_edq = nullptr /*sum phi_i dq_i, accumulated*/,
+            float2* d_save = nullptr /*keep the transformed grid (h1 n2 n3)*/,
+            const float2* d_cross = nullptr /*energy difference against a kept grid, no forces*/);
 // k_small.cu: kind 0 fnb14, 1 fnbgrp, 2 ferrf; d_e[4]
 int small_launch(orac_gpu_ctx* ctx, int kind, const double* d_xyz,
                  const int* d_pairs, const int* d_ptype, int npairs,
@@ -566,8 +570,7 @@ int small_launch_set(orac_gpu_ctx* ctx, int n, const SmallSpec* specs);
 int ne_init(orac_gpu_ctx* ctx, double tn0);
 int ne_lambda_launch(orac_gpu_ctx* ctx, int n0steps);
 int ne_sum_launch(orac_gpu_ctx* ctx, int commit);
-int ne_recip_launch(orac_gpu_ctx* ctx, const double* eq, const double* e0, const double* fq, const double* f0,
-                    int slot, bool direct);
+int ne_recip_launch(orac_gpu_ctx* ctx, const double* ed, const double* fq, const double* f0, int slot, bool direct);
 int md_nupdte(orac_gpu_ctx* ctx);
 int alch_listqq_build(orac_gpu_ctx* ctx);
 // the same with explicit charges (null: the topology's) and an optional

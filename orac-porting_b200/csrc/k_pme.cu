@@ -200,6 +200,11 @@ struct GridArgs {
   float fac, pivol;  // pi^2/alpha^2, pi*volume
   double rkcut2;
   double* eout;  // [7] energy, v11 v22 v33 v12 v13 v23
+  // the z pass keeps the transformed grid (save), or, given the transformed
+  // grid S of other charges (cross), sums the energy difference
+  // |S|^2 - |S - T|^2 = 2 Re(S conj T) - |T|^2 of this grid T and stops
+  float2* save;
+  const float2* cross;
 };
 
 enum { XF = 0, YF = 1, ZC = 2, YI = 3, XI = 4 };
@@ -292,13 +297,19 @@ __global__ void __launch_bounds__(FFT_THREADS) k_fft(const GridArgs A) {
       const double mh3 = A.r31 * m1 + A.r32 * m2 + A.r33 * m3;
       const double msq = mh1 * mh1 + mh2 * mh2 + mh3 * mh3;
       float2 q = res[e];
+      const size_t gi = ((size_t)kk * A.n2 + j0) * A.h1 + i0 + l;  // the element's place in cg
+      if (A.save) A.save[gi] = q;
       float eterm = 0.f;
       if (msq <= A.rkcut2) {
         const float fm = (float)msq;
         const float denom = A.pivol * A.bsp1[k1 - 1] * A.bsp2[k2 - 1] * A.bsp3[k3 - 1] * fm;
         eterm = expf(-A.fac * fm) / denom;
         const double vterm = 2.0 * ((double)A.fac * msq + 1.0) / msq;
-        const double q2 = (double)q.x * q.x + (double)q.y * q.y;
+        double q2 = (double)q.x * q.x + (double)q.y * q.y;
+        if (A.cross) {
+          const float2 c = A.cross[gi];
+          q2 = 2.0 * ((double)q.x * c.x + (double)q.y * c.y) - q2;
+        }
         double struc2;
         double f12 = 1, f13 = 1, f23 = 1;
         if (k1 == 1 || (k1 == ndim1 && (A.n1 % 2) == 0)) {
@@ -330,6 +341,7 @@ __global__ void __launch_bounds__(FFT_THREADS) k_fft(const GridArgs A) {
     }
     __syncthreads();
     block_reduce_add<7>(acc, A.eout);
+    if (A.cross) return;  // the energy difference alone
     float2* other = (res == a) ? b : a;
     res = fft_smem(res, other, nl, A.P, tws, +1);
   }
@@ -633,7 +645,8 @@ int pme_setup(orac_gpu_ctx* ctx, int n1, int n2, int n3, int order) {
 
 int pme_run(orac_gpu_ctx* ctx, int natom, const double* d_cart, const double* d_q, const double* recip,
             double volume, double alpha, double* d_f, double* d_eout, const double* d_sxyz, const double* d_mol,
-            unsigned long long* d_ffix, const double* d_dq, double* d_edq) {
+            unsigned long long* d_ffix, const double* d_dq, double* d_edq, float2* d_save,
+            const float2* d_cross) {
   PmePlan& P = ctx->pme;
   if (!P.qfix) return ctx_fail(ctx, ORAC_ERR_STATE, "PME not set up");
   const int n1 = P.n1, n2 = P.n2, n3 = P.n3, h1 = P.h1;
@@ -703,6 +716,8 @@ int pme_run(orac_gpu_ctx* ctx, int natom, const double* d_cart, const double* d_
   G.pivol = (float)(pif * volume);
   G.rkcut2 = 0.25 * ctx->rkcut * ctx->rkcut / (pif * pif);
   G.eout = d_eout;
+  G.save = d_save;
+  G.cross = d_cross;
   int nb;
   size_t sm;
   {
@@ -733,7 +748,7 @@ int pme_run(orac_gpu_ctx* ctx, int natom, const double* d_cart, const double* d_
   CKL();
   // the energy alone (the second charge set of a non-equilibrium step's
   // work): no potential back on the grid, no gather
-  if (!d_f && !d_ffix && !d_edq && !(d_sxyz && d_mol)) return ORAC_OK;
+  if (d_cross || (!d_f && !d_ffix && !d_edq && !(d_sxyz && d_mol))) return ORAC_OK;
   {
     // y inverse
     make_plan(n2, &G.P);

@@ -1422,14 +1422,17 @@ static int md_shell_recip(orac_gpu_ctx* ctx, MdState& S, char sh, int lvl, bool 
     for (int j = 0; j < 3; j++) recip[i + 3 * j] = 0.5 * ctx->oc[j + 3 * i];  // src/fft_pme.f:47-51
   int slot = -1;
   if (int rc = prof_begin(ctx, &slot, PROF_PME)) return rc;
+  // along a schedule the transformed grid of chrgec is kept for the work
+  float2* keep = md_ne(ctx) ? ctx->pme.cgsave : nullptr;
   if (int rc = pme_run(ctx, ctx->N, S.x, ctx->pme_q(), recip, ctx->volume, ctx->alphal, nullptr, S.e + 24, nullptr,
-                       nullptr, f, dudl ? ctx->d_dq : nullptr, dudl ? S.e + E_DUDL + 3 : nullptr))
+                       nullptr, f, dudl ? ctx->d_dq : nullptr, dudl ? S.e + E_DUDL + 3 : nullptr, keep))
     return rc;
   if (int rc = prof_end(ctx, slot)) return rc;
   if (!md_ne(ctx)) return md_ferrf(ctx, S, f, energy);
   // along a schedule: mts_furier_alchemy's dwrk (src/mts_furier_alchemy.f:
   // 112-186), the SPME sum, erf corrections and self term of chrgec minus
-  // those of chrge0; a second SPME of chrge0 gives its energy only
+  // those of chrge0; a second SPME, of chrgec - chrge0 against the kept
+  // grid of chrgec, gives the SPME difference (energy only)
   const BondedDev& B = ctx->bd;
   const int* lists[4] = {B.pbond, B.pcn, B.p13, B.p14};
   const int n[4] = {B.nb, B.ncn, B.n13, B.n14};
@@ -1442,13 +1445,13 @@ static int md_shell_recip(orac_gpu_ctx* ctx, MdState& S, char sh, int lvl, bool 
     return rc;
   if (energy)  // the energy record's erf corrections
     CK(cudaMemcpyAsync(S.e + E_ERF, S.e + E_NEQ, sizeof(double) * 16, cudaMemcpyDeviceToDevice, ctx->stream));
-  if (int rc = pme_run(ctx, ctx->N, S.x, ctx->d_q0, recip, ctx->volume, ctx->alphal, nullptr, S.e + E_NE0, nullptr,
-                       nullptr, nullptr, nullptr, nullptr))
+  if (int rc = pme_run(ctx, ctx->N, S.x, ctx->d_ne_dq, recip, ctx->volume, ctx->alphal, nullptr, S.e + E_NE0,
+                       nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, ctx->pme.cgsave))
     return rc;
   if (int rc = ferrf_launch_lists(ctx, 4, lists, n, fudge, forces, e0, S.x, B.ss, ctx->d_q0, nullptr, nullptr,
                                   nullptr))
     return rc;
-  return ne_recip_launch(ctx, S.e + 24, S.e + E_NE0, S.e + E_NEQ, S.e + E_NEQ0, 3 + ne_term(lvl), false);
+  return ne_recip_launch(ctx, S.e + E_NE0, S.e + E_NEQ, S.e + E_NEQ0, 3 + ne_term(lvl), false);
 }
 
 static int md_forces_shell(orac_gpu_ctx* ctx, MdState& S, char sh, int lvl, bool zero, double* e, bool energy) {

@@ -68,7 +68,8 @@ __host__ __device__ void ne_tables(const NeDev& ne, AlchDyn* D) {
 // solute self term's work (cself_alchemy).
 __global__ void k_ne_lambda(NeDev* __restrict__ ne, AlchDyn* __restrict__ ad, int nal, const int4* __restrict__ alist,
                             const double* __restrict__ q, double* __restrict__ qc, double* __restrict__ q0,
-                            double4* __restrict__ lam4, double4* __restrict__ lam40, int n0steps) {
+                            double* __restrict__ dqc, double4* __restrict__ lam4, double4* __restrict__ lam40,
+                            int n0steps) {
   pdl_enter();
   __shared__ double cls[2][4];
   __shared__ double red[32];
@@ -107,6 +108,7 @@ __global__ void k_ne_lambda(NeDev* __restrict__ ne, AlchDyn* __restrict__ ad, in
     const double c1 = scaled_charge(qa, c[1]), c0 = scaled_charge(qa, c[3]);
     qc[a.x] = c1;
     q0[a.x] = c0;
+    dqc[a.x] = c1 - c0;
     lam4[a.x] = make_double4(c[0], c[1], 0.0, 0.0);
     lam40[a.x] = make_double4(c[2], c[3], 0.0, 0.0);
     if (a.z == 1) s += c1 * c1 - c0 * c0;
@@ -139,14 +141,17 @@ __global__ void k_ne_sum(NeDev* __restrict__ ne, int commit) {
 }
 
 // mts_furier_alchemy's dwrk at one reciprocal evaluation
-// (src/mts_furier_alchemy.f:112-186): the SPME energies of chrgec and
-// chrge0 (eout[0] holds twice each), the erf corrections of both (16 slots
-// each) and the self term; into the pending slot, or the held one (direct).
-__global__ void k_ne_recip(NeDev* __restrict__ ne, const double* __restrict__ eq, const double* __restrict__ e0,
-                           const double* __restrict__ fq, const double* __restrict__ f0, int slot, int direct) {
+// (src/mts_furier_alchemy.f:112-186): the SPME energy of chrgec minus that
+// of chrge0, summed directly as 2 Re(S conj T) - |T|^2 over the transformed
+// grids S of chrgec and T of chrgec - chrge0 (ed[0] holds twice it; the
+// difference of two FP32 energies would lose it to rounding), the erf
+// corrections of both charge sets (16 slots each) and the self term; into
+// the pending slot, or the held one (direct).
+__global__ void k_ne_recip(NeDev* __restrict__ ne, const double* __restrict__ ed, const double* __restrict__ fq,
+                           const double* __restrict__ f0, int slot, int direct) {
   pdl_enter();
   if (threadIdx.x != 0) return;
-  double d = 0.5 * (eq[0] - e0[0]);
+  double d = 0.5 * ed[0];
   for (int k = 0; k < 16; k++) d += fq[k] - f0[k];
   d += ne->dself;
   if (direct)
@@ -159,7 +164,7 @@ __global__ void k_ne_recip(NeDev* __restrict__ ne, const double* __restrict__ eq
 
 int ne_lambda_launch(orac_gpu_ctx* ctx, int n0steps) {
   orac_launch(k_ne_lambda, 1, 256, 0, ctx->stream, ctx->d_ne, ctx->d_ad, ctx->ne_nal, ctx->d_ne_alist, ctx->d_aqd,
-              ctx->d_qc, ctx->d_q0, ctx->d_lam4, ctx->d_lam40, n0steps);
+              ctx->d_qc, ctx->d_q0, ctx->d_ne_dq, ctx->d_lam4, ctx->d_lam40, n0steps);
   CKL();
   return ORAC_OK;
 }
@@ -170,9 +175,8 @@ int ne_sum_launch(orac_gpu_ctx* ctx, int commit) {
   return ORAC_OK;
 }
 
-int ne_recip_launch(orac_gpu_ctx* ctx, const double* eq, const double* e0, const double* fq, const double* f0,
-                    int slot, bool direct) {
-  orac_launch(k_ne_recip, 1, 32, 0, ctx->stream, ctx->d_ne, eq, e0, fq, f0, slot, direct ? 1 : 0);
+int ne_recip_launch(orac_gpu_ctx* ctx, const double* ed, const double* fq, const double* f0, int slot, bool direct) {
+  orac_launch(k_ne_recip, 1, 32, 0, ctx->stream, ctx->d_ne, ed, fq, f0, slot, direct ? 1 : 0);
   CKL();
   return ORAC_OK;
 }
@@ -252,6 +256,11 @@ int ne_init(orac_gpu_ctx* ctx, double tn0) {
   if (!ctx->d_lam4 && dev_alloc(ctx, &ctx->d_lam4, N)) return ORAC_ERR_CUDA;
   if (!ctx->d_lam40 && dev_alloc(ctx, &ctx->d_lam40, N)) return ORAC_ERR_CUDA;
   if (!ctx->d_ne && dev_alloc(ctx, &ctx->d_ne, 1)) return ORAC_ERR_CUDA;
+  if (!ctx->d_ne_dq && dev_alloc(ctx, &ctx->d_ne_dq, N)) return ORAC_ERR_CUDA;
+  {
+    const PmePlan& P = ctx->pme;
+    if (P.qfix && !P.cgsave && dev_alloc(ctx, &ctx->pme.cgsave, (size_t)P.h1 * P.n2 * P.n3)) return ORAC_ERR_CUDA;
+  }
   if (dev_alloc(ctx, &ctx->d_ne_alist, al.size())) return ORAC_ERR_CUDA;
   ctx->ne_nal = (int)al.size();
   if (ctx->d_dq) {  // no control-lambda derivative along a schedule
@@ -261,6 +270,11 @@ int ne_init(orac_gpu_ctx* ctx, double tn0) {
   ctx->q0_differs = qc != q0;
   CK(cudaMemcpy(ctx->d_qc, qc.data(), sizeof(double) * N, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(ctx->d_q0, q0.data(), sizeof(double) * N, cudaMemcpyHostToDevice));
+  {
+    std::vector<double> dq(N);
+    for (int a = 0; a < N; a++) dq[a] = qc[a] - q0[a];
+    CK(cudaMemcpy(ctx->d_ne_dq, dq.data(), sizeof(double) * N, cudaMemcpyHostToDevice));
+  }
   CK(cudaMemcpy(ctx->d_lam4, l4.data(), sizeof(double4) * N, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(ctx->d_lam40, l40.data(), sizeof(double4) * N, cudaMemcpyHostToDevice));
   if (!al.empty()) CK(cudaMemcpy(ctx->d_ne_alist, al.data(), sizeof(int4) * al.size(), cudaMemcpyHostToDevice));

@@ -23,12 +23,12 @@ SCHED = dict(dt_h=4.0, lrespa=2, mrespa=4, nupdte=1000, rshk="l", n1respa=2, n0r
 TIMES = [0.0, 40.0, 80.0]
 LAMS = dict(ladded=[1.0, 1.0, 1.0], laddedq=[1.0, 1.0, 1.0], lremoved=[0.0, 0.0, 1.0], lremovedq=[0.0, 1.0, 1.0])
 FORMS = {"soft": {}, "shift": dict(shifted=True, qshift=4.0, ljshift=0.35)}
-# work (ORAC's internal energy unit, 1e4 kJ/mol): the reciprocal terms are
-# differences of two SPME energies of FP32 FFTs, each good to ~1e-7 units
-# (1e-3 kJ/mol) of the ~0.5-unit reciprocal energy, and the trajectory
-# leaves the FP64 one by ~1e-7 A per step; the work follows to an absolute
-# 2e-6 units (0.02 kJ/mol) or 2e-5 of its value
-WORK_RTOL, WORK_ATOL = 2e-5, 2e-6
+# work (ORAC's internal energy unit, 1e4 kJ/mol): the trajectory leaves
+# the FP64 one by ~1e-7 A per step, and the reciprocal term comes from FP32
+# FFTs (summed as a cross term of the two transformed grids, not as the
+# difference of two energies); the work follows to an absolute 1e-8 units
+# (1e-4 kJ/mol) or 1e-5 of its value
+WORK_RTOL, WORK_ATOL = 1e-5, 1e-8
 
 
 def pair(form, s=None):
