@@ -570,7 +570,7 @@ int small_launch_set(orac_gpu_ctx* ctx, int n, const SmallSpec* specs);
 int ne_init(orac_gpu_ctx* ctx, double tn0);
 int ne_lambda_launch(orac_gpu_ctx* ctx, int n0steps);
 int ne_sum_launch(orac_gpu_ctx* ctx, int commit);
-int ne_recip_launch(orac_gpu_ctx* ctx, const double* ed, const double* fq, const double* f0, int slot, bool direct);
+int ne_recip_launch(orac_gpu_ctx* ctx, const double* ed, const double* fq, const double* f0, int slot);
 int md_nupdte(orac_gpu_ctx* ctx);
 int alch_listqq_build(orac_gpu_ctx* ctx);
 // the same with explicit charges (null: the topology's) and an optional

@@ -390,29 +390,45 @@ struct AtomArgs {
   double* edq;
 };
 
-// fill_bspline restated in FP32 (src/pme_fftw3.f90:518-576)
-__device__ __forceinline__ void bspline(float w, int order, float* c, float* d) {
+// fill_bspline restated in FP32 (src/pme_fftw3.f90:518-576).  P > 0: the
+// order fixed at compile time (every loop unrolled, the arrays in
+// registers); P = 0: the run-time order.  Both do the same operations.
+constexpr int MAXORD = 12;
+
+template <int P>
+__device__ __forceinline__ void bspline(float w, int order_rt, float* c, float* d) {
+  const int order = P > 0 ? P : order_rt;
   c[order - 1] = 0.f;
   c[1] = w;
   c[0] = 1.f - w;
-  for (int k = 3; k <= order - 1; k++) {
+#pragma unroll
+  for (int k = 3; k <= (P > 0 ? P : MAXORD) - 1; k++) {
+    if (P == 0 && k > order - 1) break;
     const float div = 1.f / (k - 1);
     c[k - 1] = div * w * c[k - 2];
+#pragma unroll
     for (int j = 1; j <= k - 2; j++) c[k - j - 1] = div * ((w + j) * c[k - j - 2] + (k - j - w) * c[k - j - 1]);
     c[0] = div * (1.f - w) * c[0];
   }
   d[0] = -c[0];
-  for (int j = 2; j <= order; j++) d[j - 1] = c[j - 2] - c[j - 1];
+#pragma unroll
+  for (int j = 2; j <= (P > 0 ? P : MAXORD); j++) {
+    if (P == 0 && j > order) break;
+    d[j - 1] = c[j - 2] - c[j - 1];
+  }
   {
     const int k = order;
     const float div = 1.f / (k - 1);
     c[k - 1] = div * w * c[k - 2];
-    for (int j = 1; j <= k - 2; j++) c[k - j - 1] = div * ((w + j) * c[k - j - 2] + (k - j - w) * c[k - j - 1]);
+#pragma unroll
+    for (int j = 1; j <= (P > 0 ? P : MAXORD) - 2; j++) {
+      if (P == 0 && j > k - 2) break;
+      c[k - j - 1] = div * ((w + j) * c[k - j - 2] + (k - j - w) * c[k - j - 1]);
+    }
     c[0] = div * (1.f - w) * c[0];
   }
 }
 
-constexpr int MAXORD = 12;
 
 __device__ __forceinline__ void frac_coord(const AtomArgs& A, int t, double* fr) {
   const double x = A.xyz[t], y = A.xyz[A.natom + t], z = A.xyz[2 * A.natom + t];
@@ -435,27 +451,37 @@ __device__ __forceinline__ int gidx(int k0, int n) {
   return k;
 }
 
-// one thread per (atom, i3 plane)
+// one thread per (atom, i3 plane); P > 0: the order at compile time (the
+// spline arrays in registers), 0: A.order
+template <int P>
 __global__ void k_spread(const AtomArgs A) {
   pdl_enter();
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  const int p = A.order;
+  const int p = P > 0 ? P : A.order;
   if (t >= A.natom * p) return;
   const int at = t / p, i3 = t - at * p;
   double fr[3];
   frac_coord(A, at, fr);
   if (!frac_ok(A, fr)) return;  // non-finite coordinates never index the grid
   float th1[MAXORD], th2[MAXORD], th3[MAXORD], d[MAXORD];
-  bspline((float)(fr[0] - (int)fr[0]), p, th1, d);
-  bspline((float)(fr[1] - (int)fr[1]), p, th2, d);
-  bspline((float)(fr[2] - (int)fr[2]), p, th3, d);
+  bspline<P>((float)(fr[0] - (int)fr[0]), p, th1, d);
+  bspline<P>((float)(fr[1] - (int)fr[1]), p, th2, d);
+  bspline<P>((float)(fr[2] - (int)fr[2]), p, th3, d);
+  float t3 = 0.f;  // th3[i3], selected without a run-time index
+#pragma unroll
+  for (int k = 0; k < (P > 0 ? P : MAXORD); k++)
+    if (k == i3) t3 = th3[k];
   const float qa = (float)A.q[at];
   const int kk = gidx((int)fr[2] - p + 1 + i3, A.n3);
-  for (int i2 = 0; i2 < p; i2++) {
+#pragma unroll
+  for (int i2 = 0; i2 < (P > 0 ? P : MAXORD); i2++) {
+    if (P == 0 && i2 >= p) break;
     const int jj = gidx((int)fr[1] - p + 1 + i2, A.n2);
-    const float prod = th2[i2] * th3[i3] * qa;
+    const float prod = th2[i2] * t3 * qa;
     unsigned long long* row = A.qfix + ((size_t)kk * A.n2 + jj) * A.n1;
-    for (int i1 = 0; i1 < p; i1++) {
+#pragma unroll
+    for (int i1 = 0; i1 < (P > 0 ? P : MAXORD); i1++) {
+      if (P == 0 && i1 >= p) break;
       const int ii = gidx((int)fr[0] - p + 1 + i1, A.n1);
       const long long v = __double2ll_rn((double)(th1[i1] * prod) * ORAC_QSCALE);
       if (v) atomicAdd(row + ii, (unsigned long long)v);
@@ -467,11 +493,12 @@ __global__ void k_spread(const AtomArgs A) {
 // of the p^3 grid points; the partial sums meet by shuffles.
 constexpr int GATHER_LANES = 4;
 
+template <int P>
 __global__ void k_gather(const AtomArgs A) {
   pdl_enter();
   const int gt = blockIdx.x * blockDim.x + threadIdx.x;
   const int t = gt / GATHER_LANES, sub = gt % GATHER_LANES;
-  const int p = A.order;
+  const int p = P > 0 ? P : A.order;
   double st[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
   double dphi = 0.0;
   double fr[3] = {0, 0, 0};
@@ -480,16 +507,25 @@ __global__ void k_gather(const AtomArgs A) {
   float f1 = 0.f, f2 = 0.f, f3 = 0.f, phi = 0.f;
   if (active) {
     float th1[MAXORD], th2[MAXORD], th3[MAXORD], d1[MAXORD], d2[MAXORD], d3[MAXORD];
-    bspline((float)(fr[0] - (int)fr[0]), p, th1, d1);
-    bspline((float)(fr[1] - (int)fr[1]), p, th2, d2);
-    bspline((float)(fr[2] - (int)fr[2]), p, th3, d3);
-    for (int i3 = sub; i3 < p; i3 += GATHER_LANES) {
+    bspline<P>((float)(fr[0] - (int)fr[0]), p, th1, d1);
+    bspline<P>((float)(fr[1] - (int)fr[1]), p, th2, d2);
+    bspline<P>((float)(fr[2] - (int)fr[2]), p, th3, d3);
+    // the lane's planes i3 = sub, sub + GATHER_LANES, ... (a compile-time
+    // loop over every plane, so the arrays are indexed by constants)
+#pragma unroll
+    for (int i3 = 0; i3 < (P > 0 ? P : MAXORD); i3++) {
+      if (P == 0 && i3 >= p) break;
+      if (i3 % GATHER_LANES != sub) continue;
       const int kk = gidx((int)fr[2] - p + 1 + i3, A.n3);
-      for (int i2 = 0; i2 < p; i2++) {
+#pragma unroll
+      for (int i2 = 0; i2 < (P > 0 ? P : MAXORD); i2++) {
+        if (P == 0 && i2 >= p) break;
         const int jj = gidx((int)fr[1] - p + 1 + i2, A.n2);
         const float* row = A.rg + ((size_t)kk * A.n2 + jj) * A.n1;
         float s1 = 0.f, s2 = 0.f, s3 = 0.f;
-        for (int i1 = 0; i1 < p; i1++) {
+#pragma unroll
+        for (int i1 = 0; i1 < (P > 0 ? P : MAXORD); i1++) {
+          if (P == 0 && i1 >= p) break;
           const float qv = row[gidx((int)fr[0] - p + 1 + i1, A.n1)];
           s1 += d1[i1] * qv;
           s2 += th1[i1] * qv;
@@ -602,6 +638,17 @@ int upload_tw(orac_gpu_ctx* ctx, float2** dst, int n) {
   return ORAC_OK;
 }
 
+// the builds of the spread and gather kernels for the common orders
+using AtomKernel = void (*)(AtomArgs);
+AtomKernel spread_kernel(int order) {
+  return order == 4 ? k_spread<4> : order == 5 ? k_spread<5> : order == 6 ? k_spread<6> : order == 8 ? k_spread<8>
+                                                                                                      : k_spread<0>;
+}
+AtomKernel gather_kernel(int order) {
+  return order == 4 ? k_gather<4> : order == 5 ? k_gather<5> : order == 6 ? k_gather<6> : order == 8 ? k_gather<8>
+                                                                                                      : k_gather<0>;
+}
+
 int lines_per_block(int n) {
   // few lines per block: the grids here are small (32^3-96^3), so many
   // small blocks spread a pass over all SMs
@@ -688,7 +735,7 @@ int pme_run(orac_gpu_ctx* ctx, int natom, const double* d_cart, const double* d_
   A.dq = d_edq ? d_dq : nullptr;
   A.edq = d_edq;
   const int nsp = natom * P.order;
-  orac_launch(k_spread, (nsp + 255) / 256, 256, 0, ctx->stream, A);
+  orac_launch(spread_kernel(P.order), (nsp + 255) / 256, 256, 0, ctx->stream, A);
   CKL();
   GridArgs G;
   memset(&G, 0, sizeof(G));
@@ -767,7 +814,7 @@ int pme_run(orac_gpu_ctx* ctx, int natom, const double* d_cart, const double* d_
     orac_launch(k_fft<XI>, nb, FFT_THREADS, sm, ctx->stream, G);
     CKL();
   }
-  orac_launch(k_gather, (GATHER_LANES * natom + 127) / 128, 128, 0, ctx->stream, A);
+  orac_launch(gather_kernel(P.order), (GATHER_LANES * natom + 127) / 128, 128, 0, ctx->stream, A);
   CKL();
   return ORAC_OK;
 }
@@ -998,7 +1045,7 @@ extern "C" int orac_gpu_pme_kspace_static(void* stream, int numatoms, const doub
   A.f = d_force;
   A.eout = eout;
   const int nsp = numatoms * order;
-  orac_launch(k_spread, (nsp + 255) / 256, 256, 0, st, A);
+  orac_launch(spread_kernel(order), (nsp + 255) / 256, 256, 0, st, A);
 
   GridArgs G;
   memset(&G, 0, sizeof(G));
@@ -1053,7 +1100,7 @@ extern "C" int orac_gpu_pme_kspace_static(void* stream, int numatoms, const doub
   G.tw = tws[0];
   G.B = lines_per_block(nfft1);
   orac_launch(k_fft<XI>, (nfft2 * nfft3 + G.B - 1) / G.B, FFT_THREADS, (2 * (size_t)G.B + 1) * nfft1 * sizeof(float2), st, G);
-  orac_launch(k_gather, (GATHER_LANES * numatoms + 127) / 128, 128, 0, st, A);
+  orac_launch(gather_kernel(order), (GATHER_LANES * numatoms + 127) / 128, 128, 0, st, A);
   orac_launch(k_static_finish, 1, 32, 0, st, eout, d_energy);
   ce = cudaGetLastError();
   if (ce != cudaSuccess) return static_fail(err, err_len, ORAC_ERR_CUDA, "SPME launch: %s", cudaGetErrorString(ce));

@@ -1451,7 +1451,7 @@ static int md_shell_recip(orac_gpu_ctx* ctx, MdState& S, char sh, int lvl, bool 
   if (int rc = ferrf_launch_lists(ctx, 4, lists, n, fudge, forces, e0, S.x, B.ss, ctx->d_q0, nullptr, nullptr,
                                   nullptr))
     return rc;
-  return ne_recip_launch(ctx, S.e + E_NE0, S.e + E_NEQ, S.e + E_NEQ0, 3 + ne_term(lvl), false);
+  return ne_recip_launch(ctx, S.e + E_NE0, S.e + E_NEQ, S.e + E_NEQ0, 3 + ne_term(lvl));
 }
 
 static int md_forces_shell(orac_gpu_ctx* ctx, MdState& S, char sh, int lvl, bool zero, double* e, bool energy) {

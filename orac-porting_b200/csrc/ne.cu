@@ -146,18 +146,14 @@ __global__ void k_ne_sum(NeDev* __restrict__ ne, int commit) {
 // grids S of chrgec and T of chrgec - chrge0 (ed[0] holds twice it; the
 // difference of two FP32 energies would lose it to rounding), the erf
 // corrections of both charge sets (16 slots each) and the self term; into
-// the pending slot, or the held one (direct).
+// the pending slot (the M step's work sum commits it).
 __global__ void k_ne_recip(NeDev* __restrict__ ne, const double* __restrict__ ed, const double* __restrict__ fq,
-                           const double* __restrict__ f0, int slot, int direct) {
+                           const double* __restrict__ f0, int slot) {
   pdl_enter();
   if (threadIdx.x != 0) return;
   double d = 0.5 * ed[0];
   for (int k = 0; k < 16; k++) d += fq[k] - f0[k];
-  d += ne->dself;
-  if (direct)
-    ne->dw[slot] = d;
-  else
-    ne->dwn[slot] = d;
+  ne->dwn[slot] = d + ne->dself;
 }
 
 }  // namespace
@@ -175,8 +171,8 @@ int ne_sum_launch(orac_gpu_ctx* ctx, int commit) {
   return ORAC_OK;
 }
 
-int ne_recip_launch(orac_gpu_ctx* ctx, const double* ed, const double* fq, const double* f0, int slot, bool direct) {
-  orac_launch(k_ne_recip, 1, 32, 0, ctx->stream, ctx->d_ne, ed, fq, f0, slot, direct ? 1 : 0);
+int ne_recip_launch(orac_gpu_ctx* ctx, const double* ed, const double* fq, const double* f0, int slot) {
+  orac_launch(k_ne_recip, 1, 32, 0, ctx->stream, ctx->d_ne, ed, fq, f0, slot);
   CKL();
   return ORAC_OK;
 }
