@@ -163,6 +163,16 @@ __device__ __forceinline__ double warp_sumd(double v) {
   return v;
 }
 
+// e[B + type] += v with a constant index (type 0 solute, 1 solvent): the
+// energy array stays in registers
+template <int B>
+__device__ __forceinline__ void eadd(double* e, int type, double v) {
+  if (type == 0)
+    e[B] += v;
+  else
+    e[B + 1] += v;
+}
+
 __global__ void k_bonded(const BondedArgs A) {
   pdl_enter();
   int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -180,7 +190,7 @@ __global__ void k_bonded(const BondedArgs A) {
     const double qforce = -2.0 * p.y * (p.x - rs21) / rs21;
     put(A, l.x, qforce * x21, qforce * y21, qforce * z21);
     put(A, l.y, -qforce * x21, -qforce * y21, -qforce * z21);
-    e[0 + A.ss[l.x] - 1] += p.y * (rs21 - p.x) * (rs21 - p.x);
+    eadd<0>(e, A.ss[l.x] - 1, p.y * (rs21 - p.x) * (rs21 - p.x));
   }
   t -= A.nb;
   if ((A.mask & BK_BEND) && t >= 0 && t < A.nbend) {
@@ -216,7 +226,7 @@ __global__ void k_bonded(const BondedArgs A) {
       put(A, l.z, qforce * u3[0], qforce * u3[1], qforce * u3[2]);
       put(A, l.y, -qforce * (u1[0] + u3[0]), -qforce * (u1[1] + u3[1]), -qforce * (u1[2] + u3[2]));
       const int ty = A.ss[l.x] - 1;
-      e[2 + ty] += linear ? 2.0 * potb * (cb + 1.0) : potb * (bb - pota) * (bb - pota);
+      eadd<2>(e, ty, linear ? 2.0 * potb * (cb + 1.0) : potb * (bb - pota) * (bb - pota));
       if (fabs(potd) > 1e-5 && (fabs(pote) < 1e-5 || fabs(potf) > 1e-5)) {
         // Urey-Bradley 1-3 spring
         const double d31[3] = {r3[0] - r1[0], r3[1] - r1[1], r3[2] - r1[2]};
@@ -224,7 +234,7 @@ __global__ void k_bonded(const BondedArgs A) {
         const double q = -2.0 * potd * (potc - rsp31) / rsp31;
         put(A, l.x, q * d31[0], q * d31[1], q * d31[2]);
         put(A, l.z, -q * d31[0], -q * d31[1], -q * d31[2]);
-        e[2 + ty] += potd * (rsp31 - potc) * (rsp31 - potc);
+        eadd<2>(e, ty, potd * (rsp31 - potc) * (rsp31 - potc));
       }
       bool coupling = false;
       double k12 = 0, rr1 = 0, rr2 = 0;
@@ -248,7 +258,7 @@ __global__ void k_bonded(const BondedArgs A) {
         put(A, l.x, -pf * a1[0], -pf * a1[1], -pf * a1[2]);
         put(A, l.y, pf * a1[0] + qf * a2[0], pf * a1[1] + qf * a2[1], pf * a1[2] + qf * a2[2]);
         put(A, l.z, -qf * a2[0], -qf * a2[1], -qf * a2[2]);
-        e[2 + ty] += k12 * (rsp12 - rr1) * (rsp32 - rr2);
+        eadd<2>(e, ty, k12 * (rsp12 - rr1) * (rsp32 - rr2));
       }
     }
   }
@@ -264,7 +274,7 @@ __global__ void k_bonded(const BondedArgs A) {
     if (fabs(p.y) >= 1e-12 && n >= 1 && n <= 8 && torsion_geom(A, l, true, &coa, g, &sgn)) {
       cheb(n, coa, &tt, &dt);
       const double qforce = sig * dt * p.y;
-      e[4 + A.ss[l.x] - 1] += sig * (fabs(p.y) - tt * p.y);
+      eadd<4>(e, A.ss[l.x] - 1, sig * (fabs(p.y) - tt * p.y));
       put<true>(A, l.x, qforce * g[0][0], qforce * g[0][1], qforce * g[0][2]);
       put<true>(A, l.y, qforce * g[1][0], qforce * g[1][1], qforce * g[1][2]);
       put<true>(A, l.z, qforce * g[2][0], qforce * g[2][1], qforce * g[2][2]);
@@ -313,7 +323,7 @@ __global__ void k_bonded(const BondedArgs A) {
         }
       }
       if (ok) {
-        e[6 + A.ss[l.x] - 1] += enrg;
+        eadd<6>(e, A.ss[l.x] - 1, enrg);
         put(A, l.x, qforce * g[0][0], qforce * g[0][1], qforce * g[0][2]);
         put(A, l.y, qforce * g[1][0], qforce * g[1][1], qforce * g[1][2]);
         put(A, l.z, qforce * g[2][0], qforce * g[2][1], qforce * g[2][2]);
