@@ -86,6 +86,15 @@ __device__ __forceinline__ void alch14_factors(double li, double lj, double di, 
   }
 }
 
+// e[B + type] += v with a constant index (type 0 solute, 1 solvent)
+template <int B>
+__device__ __forceinline__ void eadd(double* e, int type, double v) {
+  if (type == 0)
+    e[B] += v;
+  else
+    e[B + 1] += v;
+}
+
 __device__ __forceinline__ void small_body(const SmallArgs& A) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   double e[4] = {0, 0, 0, 0};
@@ -119,7 +128,7 @@ __device__ __forceinline__ void small_body(const SmallArgs& A) {
         const double expcst = exp(-alphar * alphar);
         const double erfcst = ((((AS_A5 * qt + AS_A4) * qt + AS_A3) * qt + AS_A2) * qt + AS_A1) * qt * expcst;
         const double erfst = 1.0 - erfcst;
-        e[type] -= furpar * erfst / rsp;
+        eadd<0>(e, type, -(furpar * erfst / rsp));
         qforce = -furpar * (erfst - A.twrtpi * alphar * expcst) / (rsp * rsq);
         dedl = -(la.w * cb + ca * lb.w) * qab * erfst / rsp;
         if (A.work) {
@@ -143,14 +152,14 @@ __device__ __forceinline__ void small_body(const SmallArgs& A) {
       const double ssvir = af * 12.0 * A.tab12[lij] * r12 - 6.0 * A.tab6[lij] * r6;
       qforce = A.lj_fudge * ssvir * rsqi;
       const double elj = A.lj_fudge * (A.tab12[lij] * r12 - A.tab6[lij] * r6);
-      e[type] += af * elj;
+      eadd<0>(e, type, af * elj);
       const double alphar = A.alpha * rsp;
       const double qt = 1.0 / (1.0 + AS_QP * alphar);
       const double expcst = exp(-alphar * alphar);
       const double erfcst = ((((AS_A5 * qt + AS_A4) * qt + AS_A3) * qt + AS_A2) * qt + AS_A1) * qt * expcst;
       const double erff = 1.0 - erfcst;
       const double qq = A.fudge * A.q[i1] * A.q[i2];
-      e[2 + type] += qq * (aq * erfcst + aq2 * erff) / rsp;
+      eadd<2>(e, type, qq * (aq * erfcst + aq2 * erff) / rsp);
       qforce += qq * (aq * (erfcst + A.twrtpi * alphar * expcst) + aq2 * (erff - A.twrtpi * alphar * expcst)) * rspqi;
       dedl = daf * elj + qq * (daq * erfcst + daq2 * erff) / rsp;
       if (A.work) {
@@ -168,7 +177,7 @@ __device__ __forceinline__ void small_body(const SmallArgs& A) {
       const double expcst = exp(-alphar * alphar);
       const double erfcst = ((((AS_A5 * qt + AS_A4) * qt + AS_A3) * qt + AS_A2) * qt + AS_A1) * qt * expcst;
       const double erfst = 1.0 - erfcst;
-      e[type] -= furpar * erfst / rsp;
+      eadd<0>(e, type, -(furpar * erfst / rsp));
       qforce = -furpar * (erfst - A.twrtpi * alphar * expcst) / (rsp * rsq);
       if (A.dq)
         dedl = -(A.forces ? A.fudge : 1.0) * (A.dq[i1] * A.q[i2] + A.q[i1] * A.dq[i2]) * erfst / rsp;
@@ -187,7 +196,7 @@ __device__ __forceinline__ void small_body(const SmallArgs& A) {
       const double r12 = r6 * r6;
       const double ssvir = 12.0 * A.tab12[lij] * r12 - 6.0 * A.tab6[lij] * r6;
       qforce = lf * ssvir * rsqi;
-      e[type] += lf * (A.tab12[lij] * r12 - A.tab6[lij] * r6);
+      eadd<0>(e, type, lf * (A.tab12[lij] * r12 - A.tab6[lij] * r6));
       const double furpar = qf * A.q[i1] * A.q[i2];
       if (A.coul_mode) {
         const double rspqi = rsqi / rsp;
@@ -195,11 +204,11 @@ __device__ __forceinline__ void small_body(const SmallArgs& A) {
         const double qt = 1.0 / (1.0 + AS_QP * alphar);
         const double expcst = exp(-alphar * alphar);
         const double erfcst = ((((AS_A5 * qt + AS_A4) * qt + AS_A3) * qt + AS_A2) * qt + AS_A1) * qt * expcst;
-        e[2 + type] += furpar * erfcst / rsp;
+        eadd<2>(e, type, furpar * erfcst / rsp);
         qforce += furpar * (erfcst + A.twrtpi * alphar * expcst) * rspqi;
       } else {
         const double sv = furpar / rsp;
-        e[2 + type] += sv;
+        eadd<2>(e, type, sv);
         qforce += sv * rsqi;
       }
     }
