@@ -1198,7 +1198,7 @@ void md_destroy(orac_gpu_ctx* ctx) {
   if (S->ev_fork) cudaEventDestroy(S->ev_fork);
   if (S->ev_join) cudaEventDestroy(S->ev_join);
   if (S->side) cudaStreamDestroy(S->side);
-  void* ptrs[] = {S->x,         S->v,        S->xo,          S->ffix[0],   S->ffix[1], S->ffix[2], S->ffix[3],
+  void* ptrs[] = {S->x,         S->xo,          S->ffix[0],   S->ffix[1], S->ffix[2], S->ffix[3],
                   S->ffix[4],
                   S->invm,      S->pm,       S->sm,          S->smg,       S->cloc,    S->cdss,    S->free_atoms,
                   S->free_groups, S->bstart, S->bcab,        S->bdss,      S->e,       S->flag,
@@ -1734,13 +1734,16 @@ int orac_gpu_md_setup(orac_gpu_ctx* ctx, const double* x, const double* y, const
   CK(cudaMallocHost((void**)&S.h_flag, sizeof(int)));
   CK(cudaEventCreateWithFlags(&S.ev_fork, cudaEventDisableTiming));
   CK(cudaEventCreateWithFlags(&S.ev_join, cudaEventDisableTiming));
-  if (dev_alloc(ctx, &S.x, 3 * (size_t)N) || dev_alloc(ctx, &S.v, 3 * (size_t)N) ||
+  // positions and velocities in one allocation, back to back: a state
+  // transfer to or from a packed host buffer is one copy each way
+  if (dev_alloc(ctx, &S.x, 6 * (size_t)N) ||
       dev_alloc(ctx, &S.xo, 3 * (size_t)N) || dev_alloc(ctx, &S.ffix[0], 3 * (size_t)N) ||
       dev_alloc(ctx, &S.ffix[1], 3 * (size_t)N) || dev_alloc(ctx, &S.ffix[2], 3 * (size_t)N) ||
       dev_alloc(ctx, &S.invm, N) || dev_alloc(ctx, &S.pm, N) || dev_alloc(ctx, &S.e, E_ALL) || dev_alloc(ctx, &S.rec, (size_t)ORAC_MD_REC * MD_REC_CAP) ||
       dev_alloc(ctx, &S.rec_n, 1) ||
       dev_alloc(ctx, &S.flag, 4))
     return ORAC_ERR_CUDA;
+  S.v = S.x + 3 * (size_t)N;
   {
     // intramolecular levels (mts_intra_n0 / mts_intra_n1) when the topology has terms for them
     const BondedDev& B = ctx->bd;
