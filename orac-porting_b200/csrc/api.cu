@@ -170,7 +170,7 @@ int shell_run_r(orac_gpu_ctx* ctx, char rshell, const ShellRadii& radii, const d
   a.qd = ctx->d_aqd;
   a.twrtpi = (float)(2.0 / std::sqrt(4.0 * std::atan(1.0)));
   a.forces_on = (s.iz == 1 && rinn0 < rout) ? 1 : 0;  // src/force.f:288,848
-  a.next_on = (a.r2inn > 1.0e-5 && s.out >= 0) ? 1 : 0;  // src/force.f:279,337
+  a.next_on = (a.r2inn > 1.0e-5 && s.out >= 0 && !(flags & SH_NO_NEXT)) ? 1 : 0;  // src/force.f:279,337
   a.lskip = ctx->clewld ? (erfc_as(ctx->alphal * rinn) < 10.0e-4) : 1;  // decide_force
   a.ewald = ctx->clewld;
   a.off = Lin.off;

@@ -201,7 +201,8 @@ enum {
   SH_ENERGY = 1,    // FP64 pair energies into the energy outputs
   SH_STRESS = 2,    // molecular virial (finalize + image term)
   SH_PREPPED = 4,   // gpos/aoff already written and the force accumulator zeroed
-  SH_FIXED_OUT = 8  // d_f is a fixed-point accumulator: skip finalize
+  SH_FIXED_OUT = 8, // d_f is a fixed-point accumulator: skip finalize
+  SH_NO_NEXT = 16   // write no next-shell list (a later pass rebuilds it)
 };
 
 struct PmePlan {

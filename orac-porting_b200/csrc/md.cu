@@ -1176,6 +1176,9 @@ struct MdState {
   // kernels; fork and join by events (captured as graph edges)
   cudaStream_t side = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  // a third stream for the L and H shells of the step's last drift
+  cudaStream_t side2 = nullptr;
+  cudaEvent_t ev_fork2 = nullptr, ev_join2 = nullptr;
   // status flags read back through pinned memory; flag_step is the step
   // count at the last read-back that followed a synchronisation
   int* h_flag = nullptr;
@@ -1198,6 +1201,9 @@ void md_destroy(orac_gpu_ctx* ctx) {
   if (S->ev_fork) cudaEventDestroy(S->ev_fork);
   if (S->ev_join) cudaEventDestroy(S->ev_join);
   if (S->side) cudaStreamDestroy(S->side);
+  if (S->ev_fork2) cudaEventDestroy(S->ev_fork2);
+  if (S->ev_join2) cudaEventDestroy(S->ev_join2);
+  if (S->side2) cudaStreamDestroy(S->side2);
   void* ptrs[] = {S->x,         S->xo,          S->ffix[0],   S->ffix[1], S->ffix[2], S->ffix[3],
                   S->ffix[4],
                   S->invm,      S->pm,       S->sm,          S->smg,       S->cloc,    S->cdss,    S->free_atoms,
@@ -1381,7 +1387,8 @@ static int md_ferrf(orac_gpu_ctx* ctx, MdState& S, unsigned long long* f, bool e
 
 // one shell's pair forces into its level accumulator (zeroed by the
 // preceding drift, or here when `zero`)
-static int md_shell_pair(orac_gpu_ctx* ctx, MdState& S, char sh, int lvl, bool zero, double* e, bool energy) {
+static int md_shell_pair(orac_gpu_ctx* ctx, MdState& S, char sh, int lvl, bool zero, double* e, bool energy,
+                         bool no_next = false) {
   unsigned long long* f = S.ffix[lvl];
   if (zero) CK(cudaMemsetAsync(f, 0, sizeof(unsigned long long) * 3 * ctx->N, ctx->stream));
   // along a schedule force_alchemy's dwrk, U(lambda) - U(lambda0) over the
@@ -1394,7 +1401,7 @@ static int md_shell_pair(orac_gpu_ctx* ctx, MdState& S, char sh, int lvl, bool z
     CK(cudaMemsetAsync(pend, 0, sizeof(double), ctx->stream));
     ctx->pair_dwrk = pend;
   }
-  const int flags = SH_PREPPED | SH_FIXED_OUT | (energy ? SH_ENERGY : 0);
+  const int flags = SH_PREPPED | SH_FIXED_OUT | (energy ? SH_ENERGY : 0) | (no_next ? SH_NO_NEXT : 0);
   const int rc0 = shell_run_r(ctx, sh, ctx->sh, ctx->d_xyz, ctx->d_grp, ctx->d_mol, reinterpret_cast<double*>(f),
                               energy ? e : nullptr, nullptr, flags);
   ctx->pair_dwrk = nullptr;
@@ -1463,21 +1470,22 @@ static int md_forces_shell(orac_gpu_ctx* ctx, MdState& S, char sh, int lvl, bool
 // the side stream while the shell pair kernels run on the context's own.
 struct SideStream {
   orac_gpu_ctx* ctx;
-  MdState& S;
+  cudaStream_t side;
+  cudaEvent_t ev_fork, ev_join;
   int fork() {
-    CK(cudaEventRecord(S.ev_fork, ctx->stream));
-    CK(cudaStreamWaitEvent(S.side, S.ev_fork, 0));
+    CK(cudaEventRecord(ev_fork, ctx->stream));
+    CK(cudaStreamWaitEvent(side, ev_fork, 0));
     return ORAC_OK;
   }
   int join() {
-    CK(cudaEventRecord(S.ev_join, S.side));
-    CK(cudaStreamWaitEvent(ctx->stream, S.ev_join, 0));
+    CK(cudaEventRecord(ev_join, side));
+    CK(cudaStreamWaitEvent(ctx->stream, ev_join, 0));
     return ORAC_OK;
   }
   template <typename F>
   int run(F&& fn) {  // every launcher uses ctx->stream: point it at the side stream meanwhile
     cudaStream_t own = ctx->stream;
-    ctx->stream = S.side;
+    ctx->stream = side;
     const int rc = fn();
     ctx->stream = own;
     return rc;
@@ -1596,7 +1604,8 @@ static int md_step(orac_gpu_ctx* ctx, MdState& S, bool update, bool energy) {
   const int n0 = S.n0respa, n1 = S.n1respa;
   const int per[NLV] = {S.lrespa * S.mrespa * n1 * n0, S.mrespa * n1 * n0, n1 * n0, n0, 1};
   const int K = per[LH];
-  SideStream sd{ctx, S};
+  SideStream sd{ctx, S.side, S.ev_fork, S.ev_join};
+  SideStream sd2{ctx, S.side2, S.ev_fork2, S.ev_join2};
   double dt[NLV];
   dt[LH] = S.dth;
   dt[LL] = dt[LH] / S.lrespa;
@@ -1651,14 +1660,32 @@ static int md_step(orac_gpu_ctx* ctx, MdState& S, bool update, bool energy) {
           }))
         return rc;
     }
+    // the last drift of a step without energies: the L shell (its M list
+    // is rebuilt below anyway, so it writes none) and then the H shell (which
+    // rewrites the L list) on a third stream beside the M shell; the M list
+    // is rebuilt from the new L list once both are done.  The shells of an
+    // energy step share the energy accumulators and run one after another.
+    const bool split3 = last && !energy;
+    if (split3) {
+      if (int rc = sd2.fork()) return rc;
+      if (int rc = sd2.run([&]() -> int {
+            if (int r2 = md_shell_pair(ctx, S, 'l', LL, false, S.e + 8, false, true)) return r2;
+            return md_shell_pair(ctx, S, 'h', LH, false, S.e + 16, false);
+          }))
+        return rc;
+    }
     if (due_m) {
       if (int rc = md_shell_pair(ctx, S, 'm', LM, false, S.e, e_now)) return rc;
       if (int rc = md_alch_m(ctx, S, e_now)) return rc;  // only without N1 pairs (else with them)
     }
-    if (due_l)
+    if (due_l && !split3)
       if (int rc = md_shell_pair(ctx, S, 'l', LL, false, S.e + 8, e_now)) return rc;
     if (last) {
-      if (int rc = md_shell_pair(ctx, S, 'h', LH, false, S.e + 16, energy)) return rc;
+      if (split3) {
+        if (int rc = sd2.join()) return rc;
+      } else if (int rc = md_shell_pair(ctx, S, 'h', LH, false, S.e + 16, energy)) {
+        return rc;
+      }
       // the M list again from the new L list (src/mtsmd.f:3287-3295)
       ShellRadii r = ctx->sh;
       r.rcutl = r.rcutm;
@@ -1734,6 +1761,9 @@ int orac_gpu_md_setup(orac_gpu_ctx* ctx, const double* x, const double* y, const
   CK(cudaMallocHost((void**)&S.h_flag, sizeof(int)));
   CK(cudaEventCreateWithFlags(&S.ev_fork, cudaEventDisableTiming));
   CK(cudaEventCreateWithFlags(&S.ev_join, cudaEventDisableTiming));
+  CK(cudaStreamCreateWithFlags(&S.side2, cudaStreamNonBlocking));
+  CK(cudaEventCreateWithFlags(&S.ev_fork2, cudaEventDisableTiming));
+  CK(cudaEventCreateWithFlags(&S.ev_join2, cudaEventDisableTiming));
   // positions and velocities in one allocation, back to back: a state
   // transfer to or from a packed host buffer is one copy each way
   if (dev_alloc(ctx, &S.x, 6 * (size_t)N) ||
