@@ -389,7 +389,8 @@ int orac_gpu_md_set_graphs(orac_gpu_ctx* ctx, int on);
  * receives the number written since the last reset; reset != 0 clears the
  * count.  Column 15 holds dU/dlambda for alchemical windows
  * (orac_gpu_set_lambda with dlam), the segment energy for REM contexts and
- * the work so far under a non-equilibrium schedule.  Synchronises the
+ * the work so far under a non-equilibrium schedule, otherwise the
+ * thermostats' energy under Nose-Hoover thermostats.  Synchronises the
  * context's stream. */
 int orac_gpu_md_records(orac_gpu_ctx* ctx, int max, double* out,
                         int64_t* n_total, int reset);
@@ -419,6 +420,27 @@ int orac_gpu_md_work(orac_gpu_ctx* ctx, double* out);
  * n_total receives the number of M steps recorded. */
 int orac_gpu_md_work_trace(orac_gpu_ctx* ctx, int max, double* out,
                            int64_t* n_total);
+
+/* Nose-Hoover thermostats (ORAC's THERMOS, NVT) ------------------------------
+ * orac_gpu_md_set_thermostat replaces THERMOS / TEMPERATURE of ORAC's input
+ * (src/find_thermos.f, src/cov_thermos.f): the temperature temp (K) and the
+ * frequencies (cm^-1) of the three thermostats, on the molecules' centres of
+ * mass, the solute atoms and the solvent atoms (ss_index 1 and 2) relative to
+ * their molecule's centre of mass.  Call it before orac_gpu_md_setup; temp
+ * <= 0 removes the thermostats.  The M level of every step then runs ORAC's
+ * thermostat sequence (src/mtsmd.f:2556-2618, 2932, 3109-3170).  Molecules
+ * whose constraints need the iterative solver (a connected set of more than
+ * 4 atoms or 3 constraints) are refused at md_setup.  Energy records carry
+ * the thermostats' energy in column 15 (unless a schedule's work is there)
+ * and add it to the total (column 10), the extended system's conserved
+ * energy.  This replaces rank 3 of ORAC's ensembles only in part: the
+ * Parrinello-Rahman barostat (ISOSTRESS, cpress) is not built. */
+int orac_gpu_md_set_thermostat(orac_gpu_ctx* ctx, double temp, double nu_com,
+                               double nu_solute, double nu_solvent);
+/* out[13]: eta[3], etap[3] (1/fs), Q[3], ndf[3], the thermostats' energy
+ * (internal units), thermostats ordered centres of mass, solute, solvent.
+ * Synchronises the context's stream. */
+int orac_gpu_md_thermostat(orac_gpu_ctx* ctx, double* out);
 
 /* Batched systems ----------------------------------------------------------
  * Many independent systems (replicas, HREM states, alchemical windows), one

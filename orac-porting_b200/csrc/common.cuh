@@ -270,6 +270,15 @@ struct NeDev {
   double rec[NE_REC_CAP][2];
 };
 
+// ORAC's Nose-Hoover thermostats (THERMOS): the temperature and the
+// frequencies (cm^-1) of the centre-of-mass, solute and solvent thermostats,
+// set before md_setup; the MD state keeps the thermostats on the device
+struct ThermoHost {
+  bool on = false;
+  double temp = 0.0;
+  double nu[3] = {0.0, 0.0, 0.0};
+};
+
 struct orac_gpu_ctx {
   MdState* md = nullptr;
   bool shared_device = false;  // advanced beside other contexts (batch, server)
@@ -388,6 +397,7 @@ struct orac_gpu_ctx {
   double4* d_lam40 = nullptr;  // lambda0, lambdaq0 per atom (non-equilibrium runs)
   AlchDyn* d_ad = nullptr;  // the lambda tables the pair kernel reads
   double* pair_dwrk = nullptr;  // set around a forces-only shell whose dwrk a schedule needs
+  ThermoHost thermo;         // Nose-Hoover thermostats of the MD loop (md.cu)
   NeHost ne;                 // a non-equilibrium schedule (ne.cu)
   NeDev* d_ne = nullptr;
   int4* d_ne_alist = nullptr;  // alchemical atoms: (atom, +1 added / -1 removed, ss_index, 0)

@@ -1049,15 +1049,23 @@ __global__ void k_rattle_big(const ConsArgs A) {
   atomicOr(A.flag, 1);
 }
 
+struct ThermoDev {
+  double eta[3], etap[3], s[3];  // s = exp(-tm/4 etap): the scales of the sandwiches
+  double q[3], ndfkt[3];
+  double tm, tm4;
+  unsigned int count;  // blocks of the pass done; the last one updates the thermostats
+};
+
 // The energy record of an energy step (ORAC_MD_REC doubles, the layout
 // orac_gpu_md_run returns) into the context's ring: [0] record number,
 // [1] kinetic, [2..7] M, L, H LJ and Coulomb, [8] SPME, [9] the constant
 // (self energy), [10] total, [11] status flags, [12] bonded, [13] 1-4 and
-// intra-group pairs, [14] erf corrections, [15] dU/dlambda (alchemy) or the
-// REM segment's nonbonded energy (REM).
+// intra-group pairs, [14] erf corrections, [15] dU/dlambda (alchemy), the
+// REM segment's nonbonded energy (REM), the work of a non-equilibrium run or
+// the thermostats' energy (Nose-Hoover, which [10] then includes).
 __global__ void k_record(const double* __restrict__ e, const int* __restrict__ flag, double econst, double self_dudl,
                          int var, double* __restrict__ ring, int cap, unsigned long long* __restrict__ n,
-                         const NeDev* __restrict__ ne) {
+                         const NeDev* __restrict__ ne, const ThermoDev* __restrict__ th) {
   pdl_enter();
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   const unsigned long long k = *n;
@@ -1090,6 +1098,12 @@ __global__ void k_record(const double* __restrict__ e, const int* __restrict__ f
   r[14] = c;
   r[15] = d;
   r[10] = r[1] + r[2] + r[3] + r[4] + r[5] + r[6] + r[7] + r[8] + r[9] + r[12] + r[13] + r[14];
+  if (th) {  // the thermostats' energy (comp_thermos_energy): the extended system's total
+    double et = 0.0;
+    for (int k = 0; k < 3; k++) et += th->ndfkt[k] * th->eta[k] + 0.5 * th->q[k] * th->etap[k] * th->etap[k];
+    r[10] += et;
+    if (var != 3) r[15] = et;
+  }
   r[11] = (double)*flag;
   *n = k + 1;
 }
@@ -1108,6 +1122,414 @@ __global__ void k_ekin(int N, const double* __restrict__ v, const double* __rest
     for (int k = 0; k < (int)(blockDim.x >> 5); k++) x += s[k];
     atomicAdd(out, x);
   }
+}
+
+// ---------------------------------------------------------------------------
+// ORAC's Nose-Hoover thermostats (THERMOS) at the M level
+// (src/mtsmd.f:2556-2618, 2932, 3109-3170).  ORAC keeps each molecule's
+// centre-of-mass velocity V apart from its atoms' velocities u relative to
+// it (comp_fcm, src/comp_fcm.f); the driver keeps atomic velocities v = V + u
+// and splits them where a thermostat acts.  The M half kick at either end
+// of an M step sits between two scalings (correc_exp_scale): V by
+// s_c = exp(-tm/4 etap1), u by s_k = exp(-tm/4 etap_k) (k 2: solute, 3:
+// solvent), so with c = tm/2 and F the molecule's M force
+//   v <- s_k (s_k (v - V) + c (f/m - F/M)) + s_c (s_c V + c F/M),
+// then RATTLE (its impulses move no centre of mass and it commutes with the
+// split scaling, so one projection after the sandwich is the same).  The
+// thermostats' velocities follow comp_thermos_forces + correc_etap twice at
+// each end of the M step: etap_k += tm/4 (tto_k - ndf_k kT) / Q_k with
+// tto = sum M V^2 over molecules, sum m u^2 over solute and over solvent
+// atoms, taken after the end sandwich (K1) and before the start sandwich
+// (K2, after the L and H kicks that come between them).
+
+// sums per molecule outside the small molecules (k_mol_sums): m v, then the
+// forces of the levels N0, N1, M, L, H (sum of f)
+constexpr int TH_NS = 18;
+constexpr int TH_BLOCK = 128;
+
+struct ThermoArgs {
+  int N, nsm, nfree, nbm;
+  const int4* sm;
+  const int2* cloc;
+  const int* sm_atoms;
+  const int* free_atoms;
+  const double* x;
+  double* v;
+  const double* invm;
+  const int* cls;       // [N] 1 solute, 2 solvent: the thermostat of the atom's relative velocity
+  const int* abm;       // [N] molecule of the atom among those outside small molecules, or -1
+  const int2* brange;   // [nbm] first atom, atoms
+  const double* bmass;  // [nbm]
+  double* msum;         // [nbm][TH_NS]
+  double* vcur;         // [nbm][3] centre-of-mass velocity left by the end pass
+  const unsigned long long* f[NLV];
+  // end pass: the end half kicks of N0 (c0) and N1 (c1), the end sandwich
+  // with the M half kick cm, K1; then kicks of L (cl) and H (ch) and K2.
+  // start pass: the start sandwich with the scales the end pass left.
+  double c0, c1, cm, cl, ch;
+  int end, k2, start;
+  ThermoDev* th;
+  double* part;  // [blocks][6]: K1 and K2 of each block
+  int* flag;
+};
+
+__device__ __forceinline__ double fixf(const unsigned long long* f, int i) { return f ? fixd(f[i]) : 0.0; }
+
+// the q-th level of the sums: N0, N1, M, L, H
+__device__ __forceinline__ int th_level(int q) { return LN0 - q; }
+
+__global__ void __launch_bounds__(TH_BLOCK) k_mol_sums(const ThermoArgs A) {
+  const int2 r = __ldg(&A.brange[blockIdx.x]);
+  pdl_enter();
+  const int N = A.N;
+  double s[TH_NS];
+#pragma unroll
+  for (int j = 0; j < TH_NS; j++) s[j] = 0.0;
+  for (int a = r.x + threadIdx.x; a < r.x + r.y; a += blockDim.x) {
+    const double m = 1.0 / A.invm[a];
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      s[d] += m * A.v[d * N + a];
+#pragma unroll
+      for (int q = 0; q < 5; q++) s[3 + 3 * q + d] += fixf(A.f[th_level(q)], d * N + a);
+    }
+  }
+  __shared__ double sh[TH_BLOCK / 32][TH_NS];
+#pragma unroll
+  for (int j = 0; j < TH_NS; j++) {
+    double x = s[j];
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5][j] = x;
+  }
+  __syncthreads();
+  if (threadIdx.x < TH_NS) {
+    double x = 0.0;
+    for (int w = 0; w < TH_BLOCK / 32; w++) x += sh[w][threadIdx.x];
+    A.msum[blockIdx.x * TH_NS + threadIdx.x] = x;
+  }
+}
+
+// centre-of-mass velocity of molecule p (outside the small molecules) at the
+// stages of the end pass, from its sums: Va after the end kicks, V1 after
+// the end sandwich, V2 after the L and H kicks; FM its M force
+struct BigStages {
+  double Va[3], V1[3], V2[3], FM[3], iM;
+};
+
+__device__ __forceinline__ void big_stages(const ThermoArgs& A, int p, const double* sc, BigStages& B) {
+  const double* S = A.msum + (size_t)p * TH_NS;
+  B.iM = 1.0 / A.bmass[p];
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    B.Va[d] = S[d] * B.iM + (A.c0 * S[3 + d] + A.c1 * S[6 + d]) * B.iM;
+    B.FM[d] = S[9 + d];
+    B.V1[d] = A.end ? sc[0] * (sc[0] * B.Va[d] + A.cm * B.FM[d] * B.iM) : B.Va[d];
+    B.V2[d] = B.V1[d] + (A.cl * S[12 + d] + A.ch * S[15 + d]) * B.iM;
+  }
+}
+
+// the sandwich of one velocity component: relative part by sk, centre of
+// mass by sc, M half kick cm of force f (mass 1/im) within a molecule of
+// velocity V, M force F and mass 1/iM
+__device__ __forceinline__ double sandwich(double v, double f, double im, double V, double F, double iM, double sk,
+                                           double sc, double cm) {
+  return sk * (sk * (v - V) + cm * (f * im - F * iM)) + sc * (sc * V + cm * F * iM);
+}
+
+// atom a of entry m (a cluster lists its atoms in sm_atoms)
+__device__ __forceinline__ int th_atom(const ThermoArgs& A, const int4& m, int a) {
+  return (m.w & CLUSTER) ? A.sm_atoms[m.x + a] : m.x + a;
+}
+
+template <int KIND>
+__device__ __forceinline__ bool th_rattle(const ThermoArgs& A, const int4& m, const double x[SMA][3], double v[SMA][3],
+                                          const double im[SMA]) {
+  const int nc = m.w & 0xff;
+  if constexpr (KIND == MK_W3)
+    return rattle3(x, v, im);
+  else if constexpr (KIND == MK_STAR)
+    return rattle_star_n(nc, x, v, im);
+  else
+    return rattle_small(const_cast<double(*)[3]>(x), v, im, A.cloc + m.z, nc);
+}
+
+// one small molecule or constraint cluster (entry m) of kind KIND: the end
+// pass (K1, K2 partial sums) or the start pass
+template <int KIND>
+__device__ __forceinline__ void thermo_entry(const ThermoArgs& A, const int4 m, double k1[3], double k2[3]) {
+  const int N = A.N;
+  constexpr bool W3 = KIND == MK_W3;
+  const int na = W3 ? 3 : m.y;
+  const bool big = (m.w & CLUSTER) != 0;
+  int gat[SMA];
+  double im[SMA];
+#pragma unroll
+  for (int a = 0; a < SMA; a++) {
+    gat[a] = a < na ? th_atom(A, m, a) : 0;
+    im[a] = a < na ? __ldg(&A.invm[gat[a]]) : 0.0;
+  }
+  const int c = __ldg(&A.cls[gat[0]]);
+  const int p = big ? __ldg(&A.abm[gat[0]]) : -1;
+  pdl_enter();
+  double x[SMA][3], v[SMA][3];
+  double M = 0.0;
+#pragma unroll
+  for (int a = 0; a < SMA; a++) {
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      x[a][d] = a < na ? A.x[d * N + gat[a]] : 0.0;
+      v[a][d] = a < na ? A.v[d * N + gat[a]] : 0.0;
+    }
+    if (a < na) M += 1.0 / im[a];
+  }
+  const double sc = A.th->s[0], sk = A.th->s[c];
+  // centre-of-mass velocity and M force of a small molecule from its atoms
+  auto com = [&](double V[3]) {
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      double t = 0.0;
+#pragma unroll
+      for (int a = 0; a < SMA; a++)
+        if (a < na) t += v[a][d] / im[a];
+      V[d] = t / M;
+    }
+  };
+  auto fsum = [&](double F[3]) {
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      double t = 0.0;
+#pragma unroll
+      for (int a = 0; a < SMA; a++)
+        if (a < na) t += fixf(A.f[LM], d * N + gat[a]);
+      F[d] = t;
+    }
+  };
+  // relative kinetic term sum m |v - V|^2 and, for a small molecule, M |V|^2
+  auto kin = [&](const double V[3], double k[3]) {
+    double u2 = 0.0;
+#pragma unroll
+    for (int a = 0; a < SMA; a++)
+      if (a < na) {
+        double t = 0.0;
+#pragma unroll
+        for (int d = 0; d < 3; d++) t += (v[a][d] - V[d]) * (v[a][d] - V[d]);
+        u2 += t / im[a];
+      }
+    k[c] += u2;
+    if (!big) k[0] += M * (V[0] * V[0] + V[1] * V[1] + V[2] * V[2]);
+  };
+  bool ok = true;
+  if (A.start) {
+    double V[3], F[3];
+    if (big) {
+#pragma unroll
+      for (int d = 0; d < 3; d++) {
+        V[d] = A.vcur[3 * p + d];
+        F[d] = A.msum[(size_t)p * TH_NS + 9 + d];
+      }
+    } else {
+      com(V);
+      fsum(F);
+    }
+    const double iM = big ? 1.0 / A.bmass[p] : 1.0 / M;
+#pragma unroll
+    for (int a = 0; a < SMA; a++)
+      if (a < na)
+#pragma unroll
+        for (int d = 0; d < 3; d++)
+          v[a][d] = sandwich(v[a][d], fixf(A.f[LM], d * N + gat[a]), im[a], V[d], F[d], iM, sk, sc, A.cm);
+    ok = th_rattle<KIND>(A, m, x, v, im);
+  } else {
+    BigStages B;
+    if (big) big_stages(A, p, A.th->s, B);
+    if (A.end) {
+#pragma unroll
+      for (int a = 0; a < SMA; a++)
+        if (a < na)
+#pragma unroll
+          for (int d = 0; d < 3; d++)
+            v[a][d] += (A.c0 * fixf(A.f[LN0], d * N + gat[a]) + A.c1 * fixf(A.f[LN1], d * N + gat[a])) * im[a];
+      double Va[3], F[3];
+      if (big) {
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+          Va[d] = B.Va[d];
+          F[d] = B.FM[d];
+        }
+      } else {
+        com(Va);
+        fsum(F);
+      }
+      const double iM = big ? B.iM : 1.0 / M;
+#pragma unroll
+      for (int a = 0; a < SMA; a++)
+        if (a < na)
+#pragma unroll
+          for (int d = 0; d < 3; d++)
+            v[a][d] = sandwich(v[a][d], fixf(A.f[LM], d * N + gat[a]), im[a], Va[d], F[d], iM, sk, sc, A.cm);
+      ok = th_rattle<KIND>(A, m, x, v, im);
+      double V1[3];
+      if (big) {
+#pragma unroll
+        for (int d = 0; d < 3; d++) V1[d] = B.V1[d];
+      } else {
+        com(V1);
+      }
+      kin(V1, k1);
+    }
+    if (A.cl != 0.0 || A.ch != 0.0) {
+#pragma unroll
+      for (int a = 0; a < SMA; a++)
+        if (a < na)
+#pragma unroll
+          for (int d = 0; d < 3; d++)
+            v[a][d] += (A.cl * fixf(A.f[LL], d * N + gat[a]) + A.ch * fixf(A.f[LH], d * N + gat[a])) * im[a];
+      ok = th_rattle<KIND>(A, m, x, v, im) && ok;
+    }
+    if (A.k2) {
+      double V2[3];
+      if (big) {
+#pragma unroll
+        for (int d = 0; d < 3; d++) V2[d] = B.V2[d];
+      } else {
+        com(V2);
+      }
+      kin(V2, k2);
+    }
+  }
+  if (!ok) atomicOr(A.flag, 1);
+#pragma unroll
+  for (int a = 0; a < SMA; a++)
+    if (a < na)
+#pragma unroll
+      for (int d = 0; d < 3; d++) A.v[d * N + gat[a]] = v[a][d];
+}
+
+// correc_etap (src/correc_etap.f) with tto from comp_thermos_forces
+__device__ __forceinline__ void th_etap(ThermoDev& T, const double K[3]) {
+  for (int k = 0; k < 3; k++) {
+    if (fabs(T.q[k]) > 1.0e-7)
+      T.etap[k] += T.tm4 * (K[k] - T.ndfkt[k]) / T.q[k];
+    else
+      T.etap[k] = 0.0;
+  }
+}
+
+// Threads [0, nsm) take one small molecule or constraint cluster each,
+// [nsm, nsm + nfree) one atom outside them, the next nbm one molecule
+// outside the small ones (its centre-of-mass terms).  In the end pass each
+// block leaves its K1 and K2 sums in part; the last block to finish adds
+// them in block order (the same result at every run) and moves the
+// thermostats: eta += tm etap (verlet_free_eta, once per M step), etap
+// twice from K1 (the end of the M step), twice from K2 (the start of the
+// next), and the scales of the next sandwiches.
+__global__ void __launch_bounds__(TH_BLOCK) k_thermo(const ThermoArgs A) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int N = A.N;
+  double k1[3] = {0.0, 0.0, 0.0}, k2[3] = {0.0, 0.0, 0.0};
+  if (t < A.nsm) {
+    const int4 m = __ldg(&A.sm[t]);
+    if (m.w & MOL3)
+      thermo_entry<MK_W3>(A, m, k1, k2);
+    else if (m.w & STAR)
+      thermo_entry<MK_STAR>(A, m, k1, k2);
+    else
+      thermo_entry<MK_GENERAL>(A, m, k1, k2);
+  } else if (t < A.nsm + A.nfree) {
+    const int g = __ldg(&A.free_atoms[t - A.nsm]);
+    const double im = __ldg(&A.invm[g]);
+    const int c = __ldg(&A.cls[g]);
+    const int p = __ldg(&A.abm[g]);
+    pdl_enter();
+    const double sc = A.th->s[0], sk = A.th->s[c];
+    double v[3];
+#pragma unroll
+    for (int d = 0; d < 3; d++) v[d] = A.v[d * N + g];
+    if (A.start) {
+#pragma unroll
+      for (int d = 0; d < 3; d++)
+        v[d] = sandwich(v[d], fixf(A.f[LM], d * N + g), im, A.vcur[3 * p + d], A.msum[(size_t)p * TH_NS + 9 + d],
+                        1.0 / A.bmass[p], sk, sc, A.cm);
+    } else {
+      BigStages B;
+      big_stages(A, p, A.th->s, B);
+      if (A.end) {
+        double u2 = 0.0;
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+          v[d] += (A.c0 * fixf(A.f[LN0], d * N + g) + A.c1 * fixf(A.f[LN1], d * N + g)) * im;
+          v[d] = sandwich(v[d], fixf(A.f[LM], d * N + g), im, B.Va[d], B.FM[d], B.iM, sk, sc, A.cm);
+          u2 += (v[d] - B.V1[d]) * (v[d] - B.V1[d]);
+        }
+        k1[c] += u2 / im;
+      }
+      double u2 = 0.0;
+#pragma unroll
+      for (int d = 0; d < 3; d++) {
+        v[d] += (A.cl * fixf(A.f[LL], d * N + g) + A.ch * fixf(A.f[LH], d * N + g)) * im;
+        u2 += (v[d] - B.V2[d]) * (v[d] - B.V2[d]);
+      }
+      if (A.k2) k2[c] += u2 / im;
+    }
+#pragma unroll
+    for (int d = 0; d < 3; d++) A.v[d * N + g] = v[d];
+  } else if (t < A.nsm + A.nfree + A.nbm) {
+    pdl_enter();
+    if (!A.start) {
+      const int p = t - A.nsm - A.nfree;
+      BigStages B;
+      big_stages(A, p, A.th->s, B);
+      const double M = A.bmass[p];
+      if (A.end) k1[0] += M * (B.V1[0] * B.V1[0] + B.V1[1] * B.V1[1] + B.V1[2] * B.V1[2]);
+      if (A.k2) k2[0] += M * (B.V2[0] * B.V2[0] + B.V2[1] * B.V2[1] + B.V2[2] * B.V2[2]);
+#pragma unroll
+      for (int d = 0; d < 3; d++) A.vcur[3 * p + d] = B.V2[d];
+    }
+  } else {
+    pdl_enter();
+  }
+  if (A.start) return;
+  __shared__ double red[6][TH_BLOCK / 32];
+  __shared__ bool last;
+  double kk[6] = {k1[0], k1[1], k1[2], k2[0], k2[1], k2[2]};
+#pragma unroll
+  for (int j = 0; j < 6; j++) {
+    double x = kk[j];
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    if ((threadIdx.x & 31) == 0) red[j][threadIdx.x >> 5] = x;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int j = 0; j < 6; j++) {
+      double x = 0.0;
+      for (int w = 0; w < TH_BLOCK / 32; w++) x += red[j][w];
+      A.part[6 * blockIdx.x + j] = x;
+    }
+    __threadfence();
+    last = atomicAdd(&A.th->count, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last || threadIdx.x != 0) return;
+  __threadfence();
+  const volatile double* P = A.part;
+  double K1[3] = {0.0, 0.0, 0.0}, K2[3] = {0.0, 0.0, 0.0};
+  for (unsigned b = 0; b < gridDim.x; b++)
+    for (int j = 0; j < 3; j++) {
+      K1[j] += P[6 * b + j];
+      K2[j] += P[6 * b + 3 + j];
+    }
+  ThermoDev& T = *A.th;
+  if (A.end) {
+    for (int k = 0; k < 3; k++) T.eta[k] += T.tm * T.etap[k];
+    th_etap(T, K1);
+    th_etap(T, K1);
+  }
+  if (A.k2) {
+    th_etap(T, K2);
+    th_etap(T, K2);
+  }
+  for (int k = 0; k < 3; k++) T.s[k] = exp(-T.tm4 * T.etap[k]);
+  T.count = 0;
 }
 
 }  // namespace
@@ -1183,6 +1605,19 @@ struct MdState {
   // count at the last read-back that followed a synchronisation
   int* h_flag = nullptr;
   long long flag_step = -1;
+  // Nose-Hoover thermostats (k_thermo): device state, per-block partial
+  // sums, the molecules outside the small ones (ranges, masses, sums,
+  // centre-of-mass velocities), the atoms' thermostat and molecule
+  ThermoDev* th = nullptr;
+  int th_blocks = 0, nbm = 0;
+  double* tpart = nullptr;
+  int2* brange = nullptr;
+  double* bmass = nullptr;
+  double* msum = nullptr;
+  double* vcur = nullptr;
+  int* tcls = nullptr;
+  int* abm = nullptr;
+  int th_ndf[3] = {0, 0, 0};
 };
 
 static MdState* md_of(orac_gpu_ctx* ctx) {
@@ -1208,7 +1643,8 @@ void md_destroy(orac_gpu_ctx* ctx) {
                   S->ffix[4],
                   S->invm,      S->pm,       S->sm,          S->smg,       S->cloc,    S->cdss,    S->free_atoms,
                   S->free_groups, S->bstart, S->bcab,        S->bdss,      S->e,       S->flag,
-                  S->drift_groups, S->drift_atoms, S->sm_atoms, S->rec, S->rec_n};
+                  S->drift_groups, S->drift_atoms, S->sm_atoms, S->rec, S->rec_n, S->th, S->tpart,
+                  S->brange, S->bmass, S->msum, S->vcur, S->tcls, S->abm};
   for (void* p : ptrs)
     if (p) dev_free(ctx, p);
   delete S;
@@ -1357,6 +1793,52 @@ static int md_drift(orac_gpu_ctx* ctx, MdState& S, double dt, const double* c, i
     CKL();
   }
   return ORAC_OK;
+}
+
+// a thermostat pass (k_thermo; ThermoArgs has the coefficients), an end
+// pass after the sums of the molecules outside the small ones (k_mol_sums)
+static int md_thermo(orac_gpu_ctx* ctx, MdState& S, bool start, bool end, bool k2, double c0, double c1, double cm,
+                     double cl, double ch) {
+  ThermoArgs A;
+  memset(&A, 0, sizeof(A));
+  A.N = ctx->N;
+  A.nsm = S.nsm;
+  A.nfree = S.nfree;
+  A.nbm = S.nbm;
+  A.sm = S.sm;
+  A.cloc = S.cloc;
+  A.sm_atoms = S.sm_atoms;
+  A.free_atoms = S.free_atoms;
+  A.x = S.x;
+  A.v = S.v;
+  A.invm = S.invm;
+  A.cls = S.tcls;
+  A.abm = S.abm;
+  A.brange = S.brange;
+  A.bmass = S.bmass;
+  A.msum = S.msum;
+  A.vcur = S.vcur;
+  for (int l = 0; l < NLV; l++) A.f[l] = S.ffix[l];
+  A.c0 = c0;
+  A.c1 = c1;
+  A.cm = cm;
+  A.cl = cl;
+  A.ch = ch;
+  A.end = end;
+  A.k2 = k2;
+  A.start = start;
+  A.th = S.th;
+  A.part = S.tpart;
+  A.flag = S.flag;
+  int slot = -1;
+  if (int rc = prof_begin(ctx, &slot, PROF_DRIFT)) return rc;
+  if (!start && S.nbm) {
+    orac_launch(k_mol_sums, S.nbm, TH_BLOCK, 0, ctx->stream, A);
+    CKL();
+  }
+  orac_launch(k_thermo, S.th_blocks, TH_BLOCK, 0, ctx->stream, A);
+  CKL();
+  return prof_end(ctx, slot);
 }
 
 // erf corrections of the excluded pairs at the reciprocal level
@@ -1621,6 +2103,18 @@ static int md_step(orac_gpu_ctx* ctx, MdState& S, bool update, bool energy) {
       for (int l = LL; l < LN0; l++)
         if (k % per[l] == 0) c[l] = dt[l];
     }
+    if (S.th && k % per[LM] == 0) {
+      // an M step starts: the end of the previous one (its N0 and N1 end
+      // half kicks and the M sandwich, K1), the L kicks at an L boundary
+      // (the H and L start kicks at the step's start), K2, then the start
+      // sandwich; the drift keeps the N1 start half kick
+      const bool first = k == 0;
+      if (int rc = md_thermo(ctx, S, false, !first, true, first ? 0.0 : 0.5 * dt[LN0], first ? 0.0 : 0.5 * dt[LN1],
+                             0.5 * dt[LM], c[LL], c[LH]))
+        return rc;
+      if (int rc = md_thermo(ctx, S, true, false, false, 0, 0, 0.5 * dt[LM], 0, 0)) return rc;
+      for (int l = 0; l < NLV; l++) c[l] = l == LN1 ? 0.5 * dt[LN1] : 0.0;
+    }
     int zmask = 0;
     for (int l = 0; l < NLV; l++)
       if ((k + 1) % per[l] == 0) zmask |= 1 << l;
@@ -1709,7 +2203,12 @@ static int md_step(orac_gpu_ctx* ctx, MdState& S, bool update, bool energy) {
       if (int rc = ne_sum_launch(ctx, commit)) return rc;
     }
   }
-  {
+  if (S.th) {
+    // the last M step's end (K1) and the end half kicks of L and H
+    if (int rc = md_thermo(ctx, S, false, true, false, 0.5 * dt[LN0], 0.5 * dt[LN1], 0.5 * dt[LM], 0.5 * dt[LL],
+                           0.5 * dt[LH]))
+      return rc;
+  } else {
     double c[NLV];
     for (int l = 0; l < NLV; l++) c[l] = 0.5 * dt[l];
     if (int rc = md_kick(ctx, S, c)) return rc;
@@ -1720,13 +2219,79 @@ static int md_step(orac_gpu_ctx* ctx, MdState& S, bool update, bool energy) {
     CKL();
     const int var = md_ne(ctx) ? 3 : ((ctx->variant == VAR_ALCH && ctx->d_dq) ? 2 : (ctx->variant == VAR_REM ? 1 : 0));
     orac_launch(k_record, 1, 32, 0, ctx->stream, S.e, S.flag, S.econst, ctx->self_dudl, var, S.rec, S.rec_cap,
-                S.rec_n, (const NeDev*)ctx->d_ne);
+                S.rec_n, (const NeDev*)ctx->d_ne, (const ThermoDev*)S.th);
     CKL();
   }
   return ORAC_OK;
 }
 
 static int md_run_impl(orac_gpu_ctx* ctx, int nsteps, int energy_every, double* rec, bool async);
+
+// THERMOS (src/find_thermos.f, src/cov_thermos.f): degrees of freedom 3 per
+// molecule (centres of mass), 3 per atom less 3 per molecule less the
+// constraints (solute; solvent); Q = 2 ndf k T / (2 pi c nu)^2, zero for a
+// class without atoms or with one degree of freedom
+static int thermo_setup(orac_gpu_ctx* ctx, MdState& S, const std::vector<int>& ma0, const std::vector<int>& mna,
+                        const std::vector<char>& small, int ncnst, const int* cnst, double tm) {
+  if (S.nbig)
+    return ctx_fail(ctx, ORAC_ERR_PARAM, "thermostats with constraint sets solved iteratively (more than %d atoms "
+                                         "or %d constraints joined) are not supported", SMA, SMC);
+  const int N = ctx->N, P = ctx->P;
+  std::vector<int> cls(N), abm(N, -1);
+  std::vector<int2> br;
+  std::vector<double> bm;
+  int nat[3] = {0, 0, 0}, nmol[3] = {0, 0, 0}, ncn[3] = {0, 0, 0};
+  for (int a = 0; a < N; a++) {
+    cls[a] = ctx->h_ss[a] == 1 ? 1 : 2;
+    nat[cls[a]]++;
+  }
+  for (int p = 0; p < P; p++) {
+    if (mna[p] <= 0) continue;
+    nmol[cls[ma0[p]]]++;
+    if (small[p]) continue;
+    double m = 0.0;
+    for (int a = ma0[p]; a < ma0[p] + mna[p]; a++) {
+      abm[a] = (int)br.size();
+      m += ctx->h_mass[a];
+    }
+    br.push_back(make_int2(ma0[p], mna[p]));
+    bm.push_back(m);
+  }
+  for (int k = 0; k < ncnst; k++) ncn[cls[cnst[2 * k] - 1]]++;
+  int ndf[3] = {3 * P, 3 * nat[1] - 3 * nmol[1] - ncn[1], 3 * nat[2] - 3 * nmol[2] - ncn[2]};
+  const double avogad = 6.022140857e23, boltz = 1.38064852e-23;  // src/setuns.f:37-38
+  const double unitm = 1.0 / (avogad * 1000.0), unitl = 1.0e-10, unite = unitm * (unitl / 1.0e-15) * (unitl / 1.0e-15);
+  const double c = 2.0 * 3.14159265358979323846 * 2.997925e10;
+  ThermoDev T;
+  memset(&T, 0, sizeof(T));
+  for (int k = 0; k < 3; k++) {
+    const bool exist = k == 0 || nat[k] > 0;
+    const double om = ctx->thermo.nu[k] * c;
+    T.q[k] = exist ? 2.0 * ndf[k] * boltz * ctx->thermo.temp / (om * om) / (unitm * unitl * unitl) : 0.0;
+    if (ndf[k] == 1) T.q[k] = 0.0;
+    T.ndfkt[k] = ndf[k] * boltz * ctx->thermo.temp / unite;
+    T.s[k] = 1.0;
+    S.th_ndf[k] = ndf[k];
+  }
+  T.tm = tm;
+  T.tm4 = 0.25 * tm;
+  S.nbm = (int)br.size();
+  S.th_blocks = (S.nsm + S.nfree + S.nbm + TH_BLOCK - 1) / TH_BLOCK;
+  if (dev_alloc(ctx, &S.th, 1) || dev_alloc(ctx, &S.tpart, 6 * (size_t)S.th_blocks) || dev_alloc(ctx, &S.tcls, N) ||
+      dev_alloc(ctx, &S.abm, N))
+    return ORAC_ERR_CUDA;
+  CK(cudaMemcpy(S.th, &T, sizeof(T), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(S.tcls, cls.data(), sizeof(int) * N, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(S.abm, abm.data(), sizeof(int) * N, cudaMemcpyHostToDevice));
+  if (S.nbm) {
+    if (dev_alloc(ctx, &S.brange, S.nbm) || dev_alloc(ctx, &S.bmass, S.nbm) ||
+        dev_alloc(ctx, &S.msum, (size_t)TH_NS * S.nbm) || dev_alloc(ctx, &S.vcur, 3 * (size_t)S.nbm))
+      return ORAC_ERR_CUDA;
+    CK(cudaMemcpy(S.brange, br.data(), sizeof(int2) * S.nbm, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(S.bmass, bm.data(), sizeof(double) * S.nbm, cudaMemcpyHostToDevice));
+  }
+  return ORAC_OK;
+}
 
 // The six N-double arrays of a state transfer as few copies as possible:
 // arrays that follow each other in memory on both sides go as one copy.
@@ -1994,6 +2559,8 @@ int orac_gpu_md_setup(orac_gpu_ctx* ctx, const double* x, const double* y, const
     UPV(S.bdss, bd);
   }
 #undef UPV
+  if (ctx->thermo.on)
+    if (int rc = thermo_setup(ctx, S, ma0, mna, small, ncnst, cnst, dt_h / lrespa / mrespa)) return rc;
   S.dth = dt_h;
   S.lrespa = lrespa;
   S.mrespa = mrespa;
@@ -2067,6 +2634,47 @@ int orac_gpu_md_setup(orac_gpu_ctx* ctx, const double* x, const double* y, const
 // Coul), U_L (LJ, Coul), U_H (LJ, Coul), E_rec, econst, total, flag,
 // bonded (bonds, bends, torsions, impropers), 1-4 + intra-group, erf
 // corrections, 0.
+int orac_gpu_md_set_thermostat(orac_gpu_ctx* ctx, double temp, double nu_com, double nu_solute,
+                               double nu_solvent) {
+  ParamGenBump bump(ctx);  // the step graphs gain the thermostat passes
+  if (!ctx) return ORAC_ERR_PARAM;
+  if (md_nupdte(ctx) > 0) return ctx_fail(ctx, ORAC_ERR_STATE, "set the thermostats before orac_gpu_md_setup");
+  if (temp <= 0.0) {
+    ctx->thermo.on = false;
+    bump.arm();
+    return ORAC_OK;
+  }
+  const double nu[3] = {nu_com, nu_solute, nu_solvent};
+  for (double x : nu)
+    if (!(x > 0.0 && std::isfinite(x))) return ctx_fail(ctx, ORAC_ERR_PARAM, "thermostat frequency %g cm^-1", x);
+  if (!std::isfinite(temp)) return ctx_fail(ctx, ORAC_ERR_PARAM, "temperature");
+  bump.arm();
+  ctx->thermo.on = true;
+  ctx->thermo.temp = temp;
+  for (int k = 0; k < 3; k++) ctx->thermo.nu[k] = nu[k];
+  return ORAC_OK;
+}
+
+int orac_gpu_md_thermostat(orac_gpu_ctx* ctx, double* out) {
+  if (!ctx || !out) return ORAC_ERR_PARAM;
+  MdState* S = ctx->md;
+  if (!S || !S->ready || !S->th) return ctx_fail(ctx, ORAC_ERR_STATE, "no thermostats (md_set_thermostat, md_setup)");
+  CK(cudaSetDevice(ctx->device));
+  ThermoDev T;
+  CK(cudaMemcpyAsync(&T, S->th, sizeof(T), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  double e = 0.0;
+  for (int k = 0; k < 3; k++) {
+    out[k] = T.eta[k];
+    out[3 + k] = T.etap[k];
+    out[6 + k] = T.q[k];
+    out[9 + k] = S->th_ndf[k];
+    e += T.ndfkt[k] * T.eta[k] + 0.5 * T.q[k] * T.etap[k] * T.etap[k];
+  }
+  out[12] = e;
+  return ORAC_OK;
+}
+
 int orac_gpu_md_run(orac_gpu_ctx* ctx, int nsteps, int energy_every, double* rec) {
   return md_run_impl(ctx, nsteps, energy_every, rec, false);
 }
@@ -2284,6 +2892,14 @@ static int md_run_impl(orac_gpu_ctx* ctx, int nsteps, int energy_every, double* 
         CK(cudaMemcpy(&r[15], &ctx->d_ne->wrk, sizeof(double), cudaMemcpyDeviceToHost));
       }
       r[10] = r[1] + r[2] + r[3] + r[4] + r[5] + r[6] + r[7] + r[8] + r[9] + r[12] + r[13] + r[14];
+      if (S.th) {  // the thermostats' energy, in the total (the extended system's)
+        ThermoDev T;
+        CK(cudaMemcpy(&T, S.th, sizeof(T), cudaMemcpyDeviceToHost));
+        double et = 0.0;
+        for (int q = 0; q < 3; q++) et += T.ndfkt[q] * T.eta[q] + 0.5 * T.q[q] * T.etap[q] * T.etap[q];
+        r[10] += et;
+        if (!md_ne(ctx)) r[15] = et;
+      }
       r[11] = (double)flag;
     }
   }

@@ -346,6 +346,19 @@ class Engine:
         check(self.ctx, self.lib.orac_gpu_md_work(self.ctx, out.ctypes.data), "md_work")
         return float(out[0]), float(out[1]), tuple(out[2:6]), out[6:14].copy()
 
+    def set_thermostat(self, temp, nu_com, nu_solute, nu_solvent):
+        """ORAC's THERMOS (orac_gpu_md_set_thermostat): Nose-Hoover
+        thermostats of the molecular centres of mass, the solute and the
+        solvent at temp (K), frequencies in cm^-1; before md_setup."""
+        check(self.ctx, self.lib.orac_gpu_md_set_thermostat(self.ctx, float(temp), float(nu_com), float(nu_solute),
+                                                            float(nu_solvent)), "md_set_thermostat")
+
+    def md_thermostat(self):
+        """(eta[3], etap[3], Q[3], ndf[3], energy) of the three thermostats."""
+        out = np.zeros(13)
+        check(self.ctx, self.lib.orac_gpu_md_thermostat(self.ctx, out.ctypes.data), "md_thermostat")
+        return out[0:3].copy(), out[3:6].copy(), out[6:9].copy(), out[9:12].astype(int), float(out[12])
+
     def md_work_trace(self, max_records=8192):
         """(rtime, work) after each M step, oldest first, and the count."""
         out = np.zeros(2 * max(1, max_records))

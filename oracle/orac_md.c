@@ -1,8 +1,9 @@
 /*
  * ORACLE — test infrastructure only.
  *
- * FP64 CPU restatement of the NVE r-RESPA step loop of ORAC's mtsmd
- * (src/mtsmd.f:2390-3540) over the restated force routines of
+ * FP64 CPU restatement of the r-RESPA step loop of ORAC's mtsmd
+ * (src/mtsmd.f:2390-3540), NVE or with ORAC's Nose-Hoover thermostats at
+ * the M level (NVT), over the restated force routines of
  * orac_oracle.c: kicks as correc (src/correc.f), drift as verlet
  * (src/verlet.f), SHAKE/RATTLE as the iterative branches of
  * src/rattle_verlet.f and src/rattle_correc.f (tolerance 1e-8 A^2,
@@ -78,6 +79,14 @@ typedef struct {
   long ninn0;
   /* dwrkm dwrkl dwrkh dwrkrc_m dwrkrc_l dwrkrc_h dwrk_al dwrk14, and the sum */
   double dw[8], wrk;
+  /* ORAC's three Nose-Hoover thermostats (THERMOS: molecular centres of
+   * mass, solute, solvent), coupled at the M level
+   * (src/mtsmd.f:2556-2592, 3109-3170): thermostat masses, ndf kT, the
+   * coordinates eta and velocities etap, the molecules' masses */
+  int thermo;
+  double qmass[3], ndfkt[3], eta[3], etap[3];
+  int ndf[3];
+  double* tmass;
 } orc_md;
 
 /* the charge of mts_furier_alchemy (src/mts_furier_alchemy.f:96-111) */
@@ -565,6 +574,78 @@ static int md_rattle(orc_md* M) {
   return fail;
 }
 
+/* Nose-Hoover thermostats.  ORAC keeps the molecules' centre-of-mass
+ * velocities apart from the atoms' velocities relative to them
+ * (comp_fcm, src/comp_fcm.f); the oracle keeps atomic velocities and
+ * splits them when a thermostat acts, which is the same state: v = V + u
+ * with V the molecule's centre-of-mass velocity. */
+static void thermo_com(const orc_md* M, double* vc) {
+  const int N = M->ntap, P = M->nprot;
+  memset(vc, 0, sizeof(double) * 3 * P);
+  for (int a = 0; a < N; a++) {
+    const int p = M->atomp[a] - 1;
+    for (int d = 0; d < 3; d++) vc[3 * p + d] += M->mass[a] * M->v[d * N + a];
+  }
+  for (int p = 0; p < P; p++)
+    for (int d = 0; d < 3; d++) vc[3 * p + d] /= M->tmass[p];
+}
+
+/* comp_thermos_forces (src/comp_thermos_forces.f), then correc_etap
+ * (src/correc_etap.f): tto = sum M V^2 over molecules (thermostat 1) and
+ * sum m u^2 over solute (2) and solvent (3) atoms; etap += dt (tto - ndf
+ * kT) / Q, or 0 for a massless thermostat */
+static void thermo_etap(orc_md* M, double dt) {
+  const int N = M->ntap, P = M->nprot;
+  double* vc = (double*)malloc(sizeof(double) * 3 * (P + 1));
+  thermo_com(M, vc);
+  double tto[3] = {0.0, 0.0, 0.0};
+  for (int p = 0; p < P; p++)
+    tto[0] += M->tmass[p] * (vc[3 * p] * vc[3 * p] + vc[3 * p + 1] * vc[3 * p + 1] + vc[3 * p + 2] * vc[3 * p + 2]);
+  for (int a = 0; a < N; a++) {
+    const int p = M->atomp[a] - 1;
+    double u2 = 0.0;
+    for (int d = 0; d < 3; d++) {
+      const double u = M->v[d * N + a] - vc[3 * p + d];
+      u2 += u * u;
+    }
+    tto[M->ss[a] == 1 ? 1 : 2] += M->mass[a] * u2;
+  }
+  free(vc);
+  for (int k = 0; k < 3; k++) {
+    if (fabs(M->qmass[k]) > 1.0e-7)
+      M->etap[k] += dt * (tto[k] - M->ndfkt[k]) / M->qmass[k];
+    else
+      M->etap[k] = 0.0;
+  }
+}
+
+/* correc_exp_scale (src/correc_exp_scale.f): centre-of-mass velocities by
+ * exp(-dt etap1), solute and solvent atoms' relative velocities by
+ * exp(-dt etap2), exp(-dt etap3) */
+static void thermo_scale(orc_md* M, double dt) {
+  const int N = M->ntap, P = M->nprot;
+  double* vc = (double*)malloc(sizeof(double) * 3 * (P + 1));
+  thermo_com(M, vc);
+  const double sc = exp(-dt * M->etap[0]), s2 = exp(-dt * M->etap[1]), s3 = exp(-dt * M->etap[2]);
+  for (int a = 0; a < N; a++) {
+    const int p = M->atomp[a] - 1;
+    const double sk = M->ss[a] == 1 ? s2 : s3;
+    for (int d = 0; d < 3; d++) {
+      const double V = vc[3 * p + d];
+      M->v[d * N + a] = sk * (M->v[d * N + a] - V) + sc * V;
+    }
+  }
+  free(vc);
+}
+
+/* comp_thermos_energy (src/comp_thermos_energy.f): sum ndf kT eta +
+ * 1/2 Q etap^2, internal units */
+static double thermo_energy(const orc_md* M) {
+  double e = 0.0;
+  for (int k = 0; k < 3; k++) e += M->ndfkt[k] * M->eta[k] + 0.5 * M->qmass[k] * M->etap[k] * M->etap[k];
+  return e;
+}
+
 static int md_kick_r(orc_md* M, const double* f, double dt) {
   md_kick(M, f, dt);
   return md_rattle(M);
@@ -756,7 +837,14 @@ int orc_md_run(void* h, int nsteps, int energy_every, double* rec) {
     for (int il = 0; il < M->lrespa; il++) {
       fail |= md_kick_r(M, M->fl, tl);
       for (int im = 0; im < M->mrespa; im++) {
+        const double tm4 = 0.25 * tm;
+        if (M->thermo) {
+          thermo_etap(M, tm4);
+          thermo_etap(M, tm4);
+          thermo_scale(M, tm4);
+        }
         fail |= md_kick_r(M, M->fm, tm);
+        if (M->thermo) thermo_scale(M, tm4);
         const double tn1 = tm / M->n1respa, tn0 = tn1 / M->n0respa;
         for (int i1 = 0; i1 < M->n1respa; i1++) {
           if (M->has_n1) fail |= md_kick_r(M, M->fn1, tn1);
@@ -787,9 +875,17 @@ int orc_md_run(void* h, int nsteps, int energy_every, double* rec) {
             fail |= md_kick_r(M, M->fn1, tn1);
           }
         }
+        if (M->thermo) /* verlet_free_eta */
+          for (int q = 0; q < 3; q++) M->eta[q] += tm * M->etap[q];
         if (M->ne) ne_update(M);
         md_forces(M, 'm', M->fm);
+        if (M->thermo) thermo_scale(M, tm4);
         fail |= md_kick_r(M, M->fm, tm);
+        if (M->thermo) {
+          thermo_scale(M, tm4);
+          thermo_etap(M, tm4);
+          thermo_etap(M, tm4);
+        }
       }
       md_forces(M, 'l', M->fl);
       fail |= md_kick_r(M, M->fl, tl);
@@ -811,8 +907,13 @@ int orc_md_run(void* h, int nsteps, int energy_every, double* rec) {
       r[12] = M->e_bonded + M->e_tors;
       r[13] = M->e_14grp;
       r[14] = M->e_ferrf;
-      r[15] = 0.0;
+      r[15] = M->ne ? M->wrk : 0.0;
       r[10] = r[1] + r[2] + r[3] + r[4] + r[5] + r[6] + r[7] + r[8] + r[9] + r[12] + r[13] + r[14];
+      if (M->thermo) { /* the extended system's conserved energy */
+        const double et = thermo_energy(M);
+        r[10] += et;
+        if (!M->ne) r[15] = et;
+      }
       r[11] = fail;
     }
   }
@@ -921,6 +1022,58 @@ void orc_md_work(void* h, double* out) {
   for (int k = 0; k < 8; k++) out[6 + k] = M->dw[k];
 }
 
+/* THERMOS (src/find_thermos.f, src/cov_thermos.f): temperature temp (K)
+ * and the three thermostats' frequencies nu (cm^-1: centres of mass,
+ * solute, solvent).  ndf: 3 per molecule for the centres of mass; 3 per
+ * atom less 3 per molecule less the constraints for solute and solvent.
+ * Q = 2 ndf k T / (2 pi c nu)^2, zero for a class without atoms or with one
+ * degree of freedom; eta = etap = 0. */
+void orc_md_set_thermostat(void* h, double temp, const double* nu) {
+  orc_md* M = (orc_md*)h;
+  const int N = M->ntap, P = M->nprot;
+  const double avogad = 6.022140857e23, boltz = 1.38064852e-23;
+  const double unitm = 1.0 / (avogad * 1000.0), unitl = 1.0e-10, unite = unitm * (unitl / 1.0e-15) * (unitl / 1.0e-15);
+  const double c = 2.0 * PI_MD * 2.997925e10;
+  free(M->tmass);
+  M->tmass = (double*)calloc(P + 1, sizeof(double));
+  int* cls = (int*)calloc(P + 1, sizeof(int));
+  int nat[3] = {0, 0, 0}, nmol[3] = {0, 0, 0}, ncn[3] = {0, 0, 0};
+  for (int a = 0; a < N; a++) {
+    const int p = M->atomp[a] - 1, k = M->ss[a] == 1 ? 1 : 2;
+    M->tmass[p] += M->mass[a];
+    nat[k]++;
+    if (!cls[p]) {
+      cls[p] = k;
+      nmol[k]++;
+    }
+  }
+  for (int q = 0; q < M->ncnst; q++) ncn[M->ss[M->cnst[2 * q] - 1] == 1 ? 1 : 2]++;
+  free(cls);
+  M->ndf[0] = 3 * P;
+  for (int k = 1; k < 3; k++) M->ndf[k] = 3 * nat[k] - 3 * nmol[k] - ncn[k];
+  for (int k = 0; k < 3; k++) {
+    const int exist = k == 0 || nat[k] > 0;
+    const double om = nu[k] * c;
+    M->qmass[k] = exist ? 2.0 * M->ndf[k] * boltz * temp / (om * om) / (unitm * unitl * unitl) : 0.0;
+    if (M->ndf[k] == 1) M->qmass[k] = 0.0;
+    M->ndfkt[k] = M->ndf[k] * boltz * temp / unite;
+    M->eta[k] = M->etap[k] = 0.0;
+  }
+  M->thermo = 1;
+}
+
+/* out: eta[3], etap[3], Q[3], ndf[3], the thermostats' energy */
+void orc_md_thermostat(void* h, double* out) {
+  orc_md* M = (orc_md*)h;
+  for (int k = 0; k < 3; k++) {
+    out[k] = M->eta[k];
+    out[3 + k] = M->etap[k];
+    out[6 + k] = M->qmass[k];
+    out[9 + k] = M->ndf[k];
+  }
+  out[12] = thermo_energy(M);
+}
+
 void orc_md_get_state(void* h, double* x, double* v) {
   orc_md* M = (orc_md*)h;
   memcpy(x, M->x, sizeof(double) * 3 * M->ntap);
@@ -948,6 +1101,7 @@ void orc_md_destroy(void* h) {
   free(M->lh);
   free(M->ll);
   free(M->lm);
+  free(M->tmass);
   void* extra[] = {M->lbnd, M->r0, M->kb, M->lbndg, M->bendpot, M->ltor, M->tpota, M->tpotb, M->litr, M->ipota,
                    M->ipotb, M->ipotc, M->int14, M->type14, M->ecc1412, M->ecc146, M->ingrp, M->int13, M->fn0, M->fn1};
   for (unsigned k = 0; k < sizeof(extra) / sizeof(extra[0]); k++) free(extra[k]);

@@ -244,6 +244,12 @@ void orc_md_set_intra(void* h, int nb, const int* lbnd, const double* r0,
                       double fudge, int ningrp, const int* ingrp, int n13,
                       const int* int13, int n1respa, int n0respa);
 
+/* ORAC's Nose-Hoover thermostats in the MD loop (THERMOS): temperature (K)
+ * and frequencies nu[3] (cm^-1) of the centre-of-mass, solute and solvent
+ * thermostats; the state out[13]: eta[3], etap[3], Q[3], ndf[3], energy. */
+void orc_md_set_thermostat(void* h, double temp, const double* nu);
+void orc_md_thermostat(void* h, double* out);
+
 /* ORAC's intra-alchemical corrections (orac_oracle.c): per-atom lambdas of
  * the species, the listqq of src/initialize_lambda.f, ferrf_alchemy_add
  * (src/ferrf_alchemy_add.f) and fnb14_alchemy's Ewald branch

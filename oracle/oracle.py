@@ -549,6 +549,19 @@ class OracleMD:
         L.orc_md_set_schedule.argtypes = [C.c_void_p, C.c_int, _D, _D, _D, _D, _D, C.c_double]
         L.orc_md_set_schedule(self.h, len(sch[0]), *sch, float(t0))
 
+    def set_thermostat(self, temp, nu_com, nu_solute, nu_solvent):
+        """ORAC's THERMOS: Nose-Hoover thermostats of the molecular centres
+        of mass, the solute and the solvent at temp (K), frequencies in cm^-1."""
+        self.L.orc_md_set_thermostat.argtypes = [C.c_void_p, C.c_double, _D]
+        self.L.orc_md_set_thermostat(self.h, float(temp), _f([nu_com, nu_solute, nu_solvent]))
+
+    def thermostat(self):
+        """(eta[3], etap[3], Q[3], ndf[3], energy) of the three thermostats."""
+        out = np.zeros(13)
+        self.L.orc_md_thermostat.argtypes = [C.c_void_p, _D]
+        self.L.orc_md_thermostat(self.h, out)
+        return out[0:3].copy(), out[3:6].copy(), out[6:9].copy(), out[9:12].astype(int), float(out[12])
+
     def work(self):
         """(work, rtime, (ladd, lrm, laddq, lrmq), latest work terms[8])."""
         out = np.zeros(14)
