@@ -1143,9 +1143,11 @@ __global__ void k_ekin(int N, const double* __restrict__ v, const double* __rest
 // (K2, after the L and H kicks that come between them).
 
 // sums per molecule outside the small molecules (k_mol_sums): m v, then the
-// forces of the levels N0, N1, M, L, H (sum of f)
+// forces of the levels N0, N1, M, L, H (sum of f), all in the fixed point of
+// the force accumulators (integer sums: exact, the same in any order)
 constexpr int TH_NS = 18;
 constexpr int TH_BLOCK = 128;
+constexpr int TH_CHUNK = 256;  // atoms of one molecule per block of k_mol_sums
 
 struct ThermoArgs {
   int N, nsm, nfree, nbm;
@@ -1158,9 +1160,9 @@ struct ThermoArgs {
   const double* invm;
   const int* cls;       // [N] 1 solute, 2 solvent: the thermostat of the atom's relative velocity
   const int* abm;       // [N] molecule of the atom among those outside small molecules, or -1
-  const int2* brange;   // [nbm] first atom, atoms
+  const int4* bchunk;   // k_mol_sums blocks: molecule, first atom, atoms (at most TH_CHUNK)
   const double* bmass;  // [nbm]
-  double* msum;         // [nbm][TH_NS]
+  unsigned long long* msum;  // [nbm][TH_NS] fixed point
   double* vcur;         // [nbm][3] centre-of-mass velocity left by the end pass
   const unsigned long long* f[NLV];
   // end pass: the end half kicks of N0 (c0) and N1 (c1), the end sandwich
@@ -1168,6 +1170,7 @@ struct ThermoArgs {
   // start pass: the start sandwich with the scales the end pass left.
   double c0, c1, cm, cl, ch;
   int end, k2, start;
+  int lvmask;  // levels k_mol_sums sums (bit q: N0, N1, M, L, H)
   ThermoDev* th;
   double* part;  // [blocks][6]: K1 and K2 of each block
   int* flag;
@@ -1178,34 +1181,41 @@ __device__ __forceinline__ double fixf(const unsigned long long* f, int i) { ret
 // the q-th level of the sums: N0, N1, M, L, H
 __device__ __forceinline__ int th_level(int q) { return LN0 - q; }
 
+// sum j of molecule p
+__device__ __forceinline__ double msv(const ThermoArgs& A, int p, int j) { return fixd(A.msum[(size_t)p * TH_NS + j]); }
+
+// one block per chunk of at most TH_CHUNK atoms of one molecule: the
+// chunk's integer sums, added into the molecule's by one atomic each
 __global__ void __launch_bounds__(TH_BLOCK) k_mol_sums(const ThermoArgs A) {
-  const int2 r = __ldg(&A.brange[blockIdx.x]);
+  const int4 c = __ldg(&A.bchunk[blockIdx.x]);
   pdl_enter();
   const int N = A.N;
-  double s[TH_NS];
+  unsigned long long s[TH_NS];
 #pragma unroll
-  for (int j = 0; j < TH_NS; j++) s[j] = 0.0;
-  for (int a = r.x + threadIdx.x; a < r.x + r.y; a += blockDim.x) {
+  for (int j = 0; j < TH_NS; j++) s[j] = 0ull;
+  for (int a = c.y + threadIdx.x; a < c.y + c.z; a += blockDim.x) {
     const double m = 1.0 / A.invm[a];
 #pragma unroll
     for (int d = 0; d < 3; d++) {
-      s[d] += m * A.v[d * N + a];
+      s[d] += (unsigned long long)__double2ll_rn(m * A.v[d * N + a] * ORAC_FSCALE);
 #pragma unroll
-      for (int q = 0; q < 5; q++) s[3 + 3 * q + d] += fixf(A.f[th_level(q)], d * N + a);
+      for (int q = 0; q < 5; q++)
+        if ((A.lvmask >> q) & 1) s[3 + 3 * q + d] += A.f[th_level(q)][d * N + a];
     }
   }
-  __shared__ double sh[TH_BLOCK / 32][TH_NS];
+  __shared__ unsigned long long sh[TH_BLOCK / 32][TH_NS];
 #pragma unroll
   for (int j = 0; j < TH_NS; j++) {
-    double x = s[j];
+    unsigned long long x = s[j];
     for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
     if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5][j] = x;
   }
   __syncthreads();
-  if (threadIdx.x < TH_NS) {
-    double x = 0.0;
-    for (int w = 0; w < TH_BLOCK / 32; w++) x += sh[w][threadIdx.x];
-    A.msum[blockIdx.x * TH_NS + threadIdx.x] = x;
+  const int j = threadIdx.x;
+  if (j < TH_NS && (j < 3 || ((A.lvmask >> ((j - 3) / 3)) & 1))) {
+    unsigned long long x = 0ull;
+    for (int w = 0; w < TH_BLOCK / 32; w++) x += sh[w][j];
+    atomicAdd(&A.msum[(size_t)c.x * TH_NS + j], x);
   }
 }
 
@@ -1217,14 +1227,13 @@ struct BigStages {
 };
 
 __device__ __forceinline__ void big_stages(const ThermoArgs& A, int p, const double* sc, BigStages& B) {
-  const double* S = A.msum + (size_t)p * TH_NS;
   B.iM = 1.0 / A.bmass[p];
 #pragma unroll
   for (int d = 0; d < 3; d++) {
-    B.Va[d] = S[d] * B.iM + (A.c0 * S[3 + d] + A.c1 * S[6 + d]) * B.iM;
-    B.FM[d] = S[9 + d];
+    B.Va[d] = msv(A, p, d) * B.iM + (A.c0 * msv(A, p, 3 + d) + A.c1 * msv(A, p, 6 + d)) * B.iM;
+    B.FM[d] = msv(A, p, 9 + d);
     B.V1[d] = A.end ? sc[0] * (sc[0] * B.Va[d] + A.cm * B.FM[d] * B.iM) : B.Va[d];
-    B.V2[d] = B.V1[d] + (A.cl * S[12 + d] + A.ch * S[15 + d]) * B.iM;
+    B.V2[d] = B.V1[d] + (A.cl * msv(A, p, 12 + d) + A.ch * msv(A, p, 15 + d)) * B.iM;
   }
 }
 
@@ -1325,7 +1334,7 @@ __device__ __forceinline__ void thermo_entry(const ThermoArgs& A, const int4 m, 
 #pragma unroll
       for (int d = 0; d < 3; d++) {
         V[d] = A.vcur[3 * p + d];
-        F[d] = A.msum[(size_t)p * TH_NS + 9 + d];
+        F[d] = msv(A, p, 9 + d);
       }
     } else {
       com(V);
@@ -1448,7 +1457,7 @@ __global__ void __launch_bounds__(TH_BLOCK) k_thermo(const ThermoArgs A) {
     if (A.start) {
 #pragma unroll
       for (int d = 0; d < 3; d++)
-        v[d] = sandwich(v[d], fixf(A.f[LM], d * N + g), im, A.vcur[3 * p + d], A.msum[(size_t)p * TH_NS + 9 + d],
+        v[d] = sandwich(v[d], fixf(A.f[LM], d * N + g), im, A.vcur[3 * p + d], msv(A, p, 9 + d),
                         1.0 / A.bmass[p], sk, sc, A.cm);
     } else {
       BigStages B;
@@ -1611,9 +1620,10 @@ struct MdState {
   ThermoDev* th = nullptr;
   int th_blocks = 0, nbm = 0;
   double* tpart = nullptr;
-  int2* brange = nullptr;
+  int4* bchunk = nullptr;
+  int nchunk = 0;
   double* bmass = nullptr;
-  double* msum = nullptr;
+  unsigned long long* msum = nullptr;
   double* vcur = nullptr;
   int* tcls = nullptr;
   int* abm = nullptr;
@@ -1644,7 +1654,7 @@ void md_destroy(orac_gpu_ctx* ctx) {
                   S->invm,      S->pm,       S->sm,          S->smg,       S->cloc,    S->cdss,    S->free_atoms,
                   S->free_groups, S->bstart, S->bcab,        S->bdss,      S->e,       S->flag,
                   S->drift_groups, S->drift_atoms, S->sm_atoms, S->rec, S->rec_n, S->th, S->tpart,
-                  S->brange, S->bmass, S->msum, S->vcur, S->tcls, S->abm};
+                  S->bchunk, S->bmass, S->msum, S->vcur, S->tcls, S->abm};
   for (void* p : ptrs)
     if (p) dev_free(ctx, p);
   delete S;
@@ -1814,7 +1824,7 @@ static int md_thermo(orac_gpu_ctx* ctx, MdState& S, bool start, bool end, bool k
   A.invm = S.invm;
   A.cls = S.tcls;
   A.abm = S.abm;
-  A.brange = S.brange;
+  A.bchunk = S.bchunk;
   A.bmass = S.bmass;
   A.msum = S.msum;
   A.vcur = S.vcur;
@@ -1832,8 +1842,11 @@ static int md_thermo(orac_gpu_ctx* ctx, MdState& S, bool start, bool end, bool k
   A.flag = S.flag;
   int slot = -1;
   if (int rc = prof_begin(ctx, &slot, PROF_DRIFT)) return rc;
+  A.lvmask = (c0 != 0.0 && S.ffix[LN0] ? 1 : 0) | (c1 != 0.0 && S.ffix[LN1] ? 2 : 0) | 4 | (cl != 0.0 ? 8 : 0) |
+             (ch != 0.0 ? 16 : 0);
   if (!start && S.nbm) {
-    orac_launch(k_mol_sums, S.nbm, TH_BLOCK, 0, ctx->stream, A);
+    CK(cudaMemsetAsync(S.msum, 0, sizeof(unsigned long long) * TH_NS * (size_t)S.nbm, ctx->stream));
+    orac_launch(k_mol_sums, S.nchunk, TH_BLOCK, 0, ctx->stream, A);
     CKL();
   }
   orac_launch(k_thermo, S.th_blocks, TH_BLOCK, 0, ctx->stream, A);
@@ -2238,7 +2251,7 @@ static int thermo_setup(orac_gpu_ctx* ctx, MdState& S, const std::vector<int>& m
                                          "or %d constraints joined) are not supported", SMA, SMC);
   const int N = ctx->N, P = ctx->P;
   std::vector<int> cls(N), abm(N, -1);
-  std::vector<int2> br;
+  std::vector<int4> br;
   std::vector<double> bm;
   int nat[3] = {0, 0, 0}, nmol[3] = {0, 0, 0}, ncn[3] = {0, 0, 0};
   for (int a = 0; a < N; a++) {
@@ -2250,11 +2263,13 @@ static int thermo_setup(orac_gpu_ctx* ctx, MdState& S, const std::vector<int>& m
     nmol[cls[ma0[p]]]++;
     if (small[p]) continue;
     double m = 0.0;
+    const int b = (int)bm.size();
     for (int a = ma0[p]; a < ma0[p] + mna[p]; a++) {
-      abm[a] = (int)br.size();
+      abm[a] = b;
       m += ctx->h_mass[a];
     }
-    br.push_back(make_int2(ma0[p], mna[p]));
+    for (int a = ma0[p]; a < ma0[p] + mna[p]; a += TH_CHUNK)
+      br.push_back(make_int4(b, a, std::min(TH_CHUNK, ma0[p] + mna[p] - a), 0));
     bm.push_back(m);
   }
   for (int k = 0; k < ncnst; k++) ncn[cls[cnst[2 * k] - 1]]++;
@@ -2275,7 +2290,8 @@ static int thermo_setup(orac_gpu_ctx* ctx, MdState& S, const std::vector<int>& m
   }
   T.tm = tm;
   T.tm4 = 0.25 * tm;
-  S.nbm = (int)br.size();
+  S.nbm = (int)bm.size();
+  S.nchunk = (int)br.size();
   S.th_blocks = (S.nsm + S.nfree + S.nbm + TH_BLOCK - 1) / TH_BLOCK;
   if (dev_alloc(ctx, &S.th, 1) || dev_alloc(ctx, &S.tpart, 6 * (size_t)S.th_blocks) || dev_alloc(ctx, &S.tcls, N) ||
       dev_alloc(ctx, &S.abm, N))
@@ -2284,10 +2300,10 @@ static int thermo_setup(orac_gpu_ctx* ctx, MdState& S, const std::vector<int>& m
   CK(cudaMemcpy(S.tcls, cls.data(), sizeof(int) * N, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(S.abm, abm.data(), sizeof(int) * N, cudaMemcpyHostToDevice));
   if (S.nbm) {
-    if (dev_alloc(ctx, &S.brange, S.nbm) || dev_alloc(ctx, &S.bmass, S.nbm) ||
+    if (dev_alloc(ctx, &S.bchunk, S.nchunk) || dev_alloc(ctx, &S.bmass, S.nbm) ||
         dev_alloc(ctx, &S.msum, (size_t)TH_NS * S.nbm) || dev_alloc(ctx, &S.vcur, 3 * (size_t)S.nbm))
       return ORAC_ERR_CUDA;
-    CK(cudaMemcpy(S.brange, br.data(), sizeof(int2) * S.nbm, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(S.bchunk, br.data(), sizeof(int4) * S.nchunk, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(S.bmass, bm.data(), sizeof(double) * S.nbm, cudaMemcpyHostToDevice));
   }
   return ORAC_OK;
