@@ -1155,16 +1155,18 @@ def profile_window_batch(nwin):
     return 0
 
 
-def profile_f0(nsteps):
+def profile_f0(nsteps, thermostats=False):
     """`nsteps` MD steps of the test1 system (F0) bracketed for a profiler
     that starts collecting at cudaProfilerStart (set-up and three warm-up
-    steps stay outside)."""
+    steps stay outside); with thermostats, test1's THERMOS."""
     import torch
 
     from orac_b200.engine import Engine
 
     wl = F0_WORKLOAD
     e = Engine(wl["build"]().copy())
+    if thermostats:
+        e.set_thermostat(*TEST1_THERMOS)
     e.md_setup(wl["dt_h"], wl["lrespa"], wl["mrespa"], wl["nupdte"], wl["rshk"], n1respa=wl["n1respa"],
                n0respa=wl["n0respa"], econst=0.0)
     e.md_run(3)
@@ -1207,12 +1209,14 @@ def main():
     ap.add_argument("--profile-f0", type=int, default=0, metavar="N",
                     help="profiling aid, no JSON: the test1 system, 3 steps, then N steps bracketed by "
                          "cudaProfilerStart/Stop (ncu --profile-from-start off)")
+    ap.add_argument("--profile-thermostats", action="store_true",
+                    help="with --profile-f0: test1's Nose-Hoover thermostats (THERMOS 298 K, 10 cm^-1)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.profile_window_batch > 0:
         return profile_window_batch(args.profile_window_batch)
     if args.profile_f0 > 0:
-        return profile_f0(args.profile_f0)
+        return profile_f0(args.profile_f0, args.profile_thermostats)
     wl = WORKLOADS[args.workload]
     ws, rank, local = dist_info()
     s = wl["build"]()

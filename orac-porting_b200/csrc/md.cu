@@ -81,6 +81,26 @@ __device__ __forceinline__ bool solve3(double A[SMC][SMC], double b[SMC], int n)
   return true;
 }
 
+struct ThermoDev {
+  double eta[3], etap[3], s[3];  // s = exp(-tm/4 etap): the scales of the sandwiches
+  double q[3], ndfkt[3];
+  double tm, tm4;
+  unsigned int count;  // blocks of the pass done; the last one updates the thermostats
+};
+
+// sums per molecule outside the small molecules (k_mol_sums): m v, then the
+// forces of the levels N0, N1, M, L, H (sum of f), all in the fixed point of
+// the force accumulators (integer sums: exact, the same in any order)
+constexpr int TH_NS = 18;
+
+// the M half kick cm of force f (mass 1/im) between the two scalings of a
+// thermostat sandwich: the velocity relative to the molecule's centre of
+// mass (V; M force F, mass 1/iM) by sk, the centre of mass by sc
+__device__ __forceinline__ double sandwich(double v, double f, double im, double V, double F, double iM, double sk,
+                                           double sc, double cm) {
+  return sk * (sk * (v - V) + cm * (f * im - F * iM)) + sc * (sc * V + cm * F * iM);
+}
+
 struct MolArgs {
   int N;
   // small constrained molecules
@@ -134,6 +154,17 @@ struct MolArgs {
   int groups;  // group centres and pair-kernel inputs wanted (a shell evaluation follows)
   double tol;
   int* flag;
+  // the start sandwich of an M step under thermostats (k_drift<true>): the
+  // thermostats' scales, each atom's thermostat (1 solute, 2 solvent) and
+  // molecule outside the small ones, those molecules' centre-of-mass
+  // velocities, sums and masses, tm/2
+  const ThermoDev* th;
+  const int* tcls;
+  const int* abm;
+  const double* vcur;
+  const unsigned long long* msum;
+  const double* bmass;
+  double tcm;
 };
 
 // a constraint cluster of a large molecule (the atoms joined by one
@@ -661,14 +692,26 @@ __device__ __forceinline__ double kick_dv(const MolArgs& A, int i, int nlev = NL
 
 // free atom i (SoA component index d*N + g): kick, verlet half kick of the N0
 // force and drift, zeroing of the level accumulators that restart here
+template <bool TH>
 __device__ __forceinline__ void drift_atom(const MolArgs& A, int g, double dt) {
   const int N = A.N;
   const double im = A.invm[g];
+  int p = 0;
+  double sc = 1.0, sk = 1.0, iM = 0.0;
+  if constexpr (TH) {
+    p = A.abm[g];
+    sc = A.th->s[0];
+    sk = A.th->s[A.tcls[g]];
+    iM = 1.0 / A.bmass[p];
+  }
 #pragma unroll
   for (int d = 0; d < 3; d++) {
     const int i = d * N + g;
     const double f = A.fv ? fixd(A.fv[i]) : 0.0;
     double v = A.v[i];
+    if constexpr (TH)
+      v = sandwich(v, fixd(A.fk[LM][i]), im, A.vcur[3 * p + d], fixd(A.msum[(size_t)p * TH_NS + 9 + d]), iM, sk, sc,
+                   A.tcm);
     if (A.kick) v += kick_dv(A, i) * im;
     const double xo = A.x[i];
     A.xo[i] = xo;
@@ -792,7 +835,7 @@ __global__ void k_kick(const MolArgs A) {
 // pair-kernel inputs of its groups, for a molecule of kind KIND (a rigid
 // three-site molecule: SETTLE or Newton SHAKE; a star cluster; the general
 // small molecule).
-template <int KIND>
+template <int KIND, bool TH>
 __device__ __forceinline__ void drift_molecule(const MolArgs& A, int t, const int4 m) {
   constexpr bool W3 = KIND == MK_W3;
   const int N = A.N;
@@ -831,13 +874,50 @@ __device__ __forceinline__ void drift_molecule(const MolArgs& A, int t, const in
       for (int d = 0; d < 3; d++) {
         xo[a][d] = A.x[d * N + g];
         v[a][d] = A.v[d * N + g];
-        if (A.kick) v[a][d] += kick_dv(A, d * N + g, nlev) * im[a];
+        if (!TH && A.kick) v[a][d] += kick_dv(A, d * N + g, nlev) * im[a];
         fh[a][d] = vf ? fixd(A.fv[d * N + g]) : 0.0;
       }
     } else {
 #pragma unroll
       for (int d = 0; d < 3; d++) x[a][d] = xo[a][d] = v[a][d] = fh[a][d] = 0.0;
     }
+  }
+  if constexpr (TH) {
+    // the M step's start sandwich under thermostats, then the kick
+    const bool big = (m.w & CLUSTER) != 0;
+    const int p = big ? A.abm[gat[0]] : 0;
+    const double sc = A.th->s[0], sk = A.th->s[A.tcls[gat[0]]];
+    double M = 0.0;
+#pragma unroll
+    for (int a = 0; a < SMA; a++)
+      if (a < na) M += 1.0 / im[a];
+    double V[3], F[3];
+    const double iM = big ? 1.0 / A.bmass[p] : 1.0 / M;
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      if (big) {
+        V[d] = A.vcur[3 * p + d];
+        F[d] = fixd(A.msum[(size_t)p * TH_NS + 9 + d]);
+      } else {
+        double tv = 0.0, tf = 0.0;
+#pragma unroll
+        for (int a = 0; a < SMA; a++)
+          if (a < na) {
+            tv += v[a][d] / im[a];
+            tf += fixd(A.fk[LM][d * N + gat[a]]);
+          }
+        V[d] = tv / M;
+        F[d] = tf;
+      }
+    }
+#pragma unroll
+    for (int a = 0; a < SMA; a++)
+      if (a < na)
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+          v[a][d] = sandwich(v[a][d], fixd(A.fk[LM][d * N + gat[a]]), im[a], V[d], F[d], iM, sk, sc, A.tcm);
+          if (A.kick) v[a][d] += kick_dv(A, d * N + gat[a], nlev) * im[a];
+        }
   }
   const int nc = m.w & 0xff;
   // RATTLE of the kicked velocities (rattle_correc after correc).  A rigid
@@ -846,7 +926,7 @@ __device__ __forceinline__ void drift_molecule(const MolArgs& A, int t, const in
   // leaves the constrained positions, and the velocities (x_new - x_old)/dt
   // they leave, as they were (to rounding)
   if constexpr (!W3) {
-    if (A.kick && nc > 0) {
+    if ((A.kick || TH) && nc > 0) {
       bool ok;
       if constexpr (KIND == MK_STAR)
         ok = rattle_star_n(nc, xo, v, im);
@@ -928,27 +1008,28 @@ __device__ __forceinline__ void drift_molecule(const MolArgs& A, int t, const in
 
 // verlet drift + SHAKE + RATTLE of small molecules (drift_molecule); free
 // atoms drift here and get their groups in k_free_groups.
+template <bool TH>
 __global__ void k_drift(const MolArgs A) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const double dt = A.dt;
   if (t < A.nsm) {
     const int4 m = __ldg(&A.sm[t]);
     if (m.w & MOL3)
-      drift_molecule<MK_W3>(A, t, m);
+      drift_molecule<MK_W3, TH>(A, t, m);
     else if (m.w & STAR)
-      drift_molecule<MK_STAR>(A, t, m);
+      drift_molecule<MK_STAR, TH>(A, t, m);
     else
-      drift_molecule<MK_GENERAL>(A, t, m);
+      drift_molecule<MK_GENERAL, TH>(A, t, m);
   } else if (t < A.nsm + A.ndg) {
     pdl_enter();
     // a group of an unconstrained molecule: its atoms, then its centre
     const int gi = A.drift_groups[t - A.nsm];
     const int2 mg = A.gmeta[gi];
-    for (int a = mg.x; a < mg.x + (mg.y & 0xff); a++) drift_atom(A, a, dt);
+    for (int a = mg.x; a < mg.x + (mg.y & 0xff); a++) drift_atom<TH>(A, a, dt);
     if (A.groups) group_centre(A, gi);
   } else if (t < A.nsm + A.ndg + A.nda) {
     pdl_enter();
-    drift_atom(A, A.drift_atoms[t - A.nsm - A.ndg], dt);
+    drift_atom<TH>(A, A.drift_atoms[t - A.nsm - A.ndg], dt);
   } else {
     pdl_enter();
   }
@@ -1049,12 +1130,6 @@ __global__ void k_rattle_big(const ConsArgs A) {
   atomicOr(A.flag, 1);
 }
 
-struct ThermoDev {
-  double eta[3], etap[3], s[3];  // s = exp(-tm/4 etap): the scales of the sandwiches
-  double q[3], ndfkt[3];
-  double tm, tm4;
-  unsigned int count;  // blocks of the pass done; the last one updates the thermostats
-};
 
 // The energy record of an energy step (ORAC_MD_REC doubles, the layout
 // orac_gpu_md_run returns) into the context's ring: [0] record number,
@@ -1142,12 +1217,11 @@ __global__ void k_ekin(int N, const double* __restrict__ v, const double* __rest
 // atoms, taken after the end sandwich (K1) and before the start sandwich
 // (K2, after the L and H kicks that come between them).
 
-// sums per molecule outside the small molecules (k_mol_sums): m v, then the
-// forces of the levels N0, N1, M, L, H (sum of f), all in the fixed point of
-// the force accumulators (integer sums: exact, the same in any order)
-constexpr int TH_NS = 18;
-constexpr int TH_BLOCK = 128;
-constexpr int TH_CHUNK = 256;  // atoms of one molecule per block of k_mol_sums
+// one warp per block of k_thermo (its threads' chains are long: the blocks
+// spread over the SMs); k_mol_sums takes 64 atoms of one molecule per block
+constexpr int TH_BLOCK = 32;
+constexpr int TS_BLOCK = 64;
+constexpr int TH_CHUNK = 64;
 
 struct ThermoArgs {
   int N, nsm, nfree, nbm;
@@ -1165,11 +1239,11 @@ struct ThermoArgs {
   unsigned long long* msum;  // [nbm][TH_NS] fixed point
   double* vcur;         // [nbm][3] centre-of-mass velocity left by the end pass
   const unsigned long long* f[NLV];
-  // end pass: the end half kicks of N0 (c0) and N1 (c1), the end sandwich
-  // with the M half kick cm, K1; then kicks of L (cl) and H (ch) and K2.
-  // start pass: the start sandwich with the scales the end pass left.
+  // the end half kicks of N0 (c0) and N1 (c1), the end sandwich with the M
+  // half kick cm, K1; then kicks of L (cl) and H (ch) and K2 (the start
+  // sandwich follows in the drift, k_drift<true>)
   double c0, c1, cm, cl, ch;
-  int end, k2, start;
+  int end, k2;
   int lvmask;  // levels k_mol_sums sums (bit q: N0, N1, M, L, H)
   ThermoDev* th;
   double* part;  // [blocks][6]: K1 and K2 of each block
@@ -1186,7 +1260,7 @@ __device__ __forceinline__ double msv(const ThermoArgs& A, int p, int j) { retur
 
 // one block per chunk of at most TH_CHUNK atoms of one molecule: the
 // chunk's integer sums, added into the molecule's by one atomic each
-__global__ void __launch_bounds__(TH_BLOCK) k_mol_sums(const ThermoArgs A) {
+__global__ void __launch_bounds__(TS_BLOCK) k_mol_sums(const ThermoArgs A) {
   const int4 c = __ldg(&A.bchunk[blockIdx.x]);
   pdl_enter();
   const int N = A.N;
@@ -1203,7 +1277,7 @@ __global__ void __launch_bounds__(TH_BLOCK) k_mol_sums(const ThermoArgs A) {
         if ((A.lvmask >> q) & 1) s[3 + 3 * q + d] += A.f[th_level(q)][d * N + a];
     }
   }
-  __shared__ unsigned long long sh[TH_BLOCK / 32][TH_NS];
+  __shared__ unsigned long long sh[TS_BLOCK / 32][TH_NS];
 #pragma unroll
   for (int j = 0; j < TH_NS; j++) {
     unsigned long long x = s[j];
@@ -1214,7 +1288,7 @@ __global__ void __launch_bounds__(TH_BLOCK) k_mol_sums(const ThermoArgs A) {
   const int j = threadIdx.x;
   if (j < TH_NS && (j < 3 || ((A.lvmask >> ((j - 3) / 3)) & 1))) {
     unsigned long long x = 0ull;
-    for (int w = 0; w < TH_BLOCK / 32; w++) x += sh[w][j];
+    for (int w = 0; w < TS_BLOCK / 32; w++) x += sh[w][j];
     atomicAdd(&A.msum[(size_t)c.x * TH_NS + j], x);
   }
 }
@@ -1237,14 +1311,6 @@ __device__ __forceinline__ void big_stages(const ThermoArgs& A, int p, const dou
   }
 }
 
-// the sandwich of one velocity component: relative part by sk, centre of
-// mass by sc, M half kick cm of force f (mass 1/im) within a molecule of
-// velocity V, M force F and mass 1/iM
-__device__ __forceinline__ double sandwich(double v, double f, double im, double V, double F, double iM, double sk,
-                                           double sc, double cm) {
-  return sk * (sk * (v - V) + cm * (f * im - F * iM)) + sc * (sc * V + cm * F * iM);
-}
-
 // atom a of entry m (a cluster lists its atoms in sm_atoms)
 __device__ __forceinline__ int th_atom(const ThermoArgs& A, const int4& m, int a) {
   return (m.w & CLUSTER) ? A.sm_atoms[m.x + a] : m.x + a;
@@ -1262,8 +1328,8 @@ __device__ __forceinline__ bool th_rattle(const ThermoArgs& A, const int4& m, co
     return rattle_small(const_cast<double(*)[3]>(x), v, im, A.cloc + m.z, nc);
 }
 
-// one small molecule or constraint cluster (entry m) of kind KIND: the end
-// pass (K1, K2 partial sums) or the start pass
+// one small molecule or constraint cluster (entry m) of kind KIND: its share
+// of the pass and of K1 and K2
 template <int KIND>
 __device__ __forceinline__ void thermo_entry(const ThermoArgs& A, const int4 m, double k1[3], double k2[3]) {
   const int N = A.N;
@@ -1328,27 +1394,7 @@ __device__ __forceinline__ void thermo_entry(const ThermoArgs& A, const int4 m, 
     if (!big) k[0] += M * (V[0] * V[0] + V[1] * V[1] + V[2] * V[2]);
   };
   bool ok = true;
-  if (A.start) {
-    double V[3], F[3];
-    if (big) {
-#pragma unroll
-      for (int d = 0; d < 3; d++) {
-        V[d] = A.vcur[3 * p + d];
-        F[d] = msv(A, p, 9 + d);
-      }
-    } else {
-      com(V);
-      fsum(F);
-    }
-    const double iM = big ? 1.0 / A.bmass[p] : 1.0 / M;
-#pragma unroll
-    for (int a = 0; a < SMA; a++)
-      if (a < na)
-#pragma unroll
-        for (int d = 0; d < 3; d++)
-          v[a][d] = sandwich(v[a][d], fixf(A.f[LM], d * N + gat[a]), im[a], V[d], F[d], iM, sk, sc, A.cm);
-    ok = th_rattle<KIND>(A, m, x, v, im);
-  } else {
+  {
     BigStages B;
     if (big) big_stages(A, p, A.th->s, B);
     if (A.end) {
@@ -1426,8 +1472,8 @@ __device__ __forceinline__ void th_etap(ThermoDev& T, const double K[3]) {
 
 // Threads [0, nsm) take one small molecule or constraint cluster each,
 // [nsm, nsm + nfree) one atom outside them, the next nbm one molecule
-// outside the small ones (its centre-of-mass terms).  In the end pass each
-// block leaves its K1 and K2 sums in part; the last block to finish adds
+// outside the small ones (its centre-of-mass terms).  Each block leaves its
+// K1 and K2 sums in part; the last block to finish adds
 // them in block order (the same result at every run) and moves the
 // thermostats: eta += tm etap (verlet_free_eta, once per M step), etap
 // twice from K1 (the end of the M step), twice from K2 (the start of the
@@ -1454,12 +1500,7 @@ __global__ void __launch_bounds__(TH_BLOCK) k_thermo(const ThermoArgs A) {
     double v[3];
 #pragma unroll
     for (int d = 0; d < 3; d++) v[d] = A.v[d * N + g];
-    if (A.start) {
-#pragma unroll
-      for (int d = 0; d < 3; d++)
-        v[d] = sandwich(v[d], fixf(A.f[LM], d * N + g), im, A.vcur[3 * p + d], msv(A, p, 9 + d),
-                        1.0 / A.bmass[p], sk, sc, A.cm);
-    } else {
+    {
       BigStages B;
       big_stages(A, p, A.th->s, B);
       if (A.end) {
@@ -1484,7 +1525,7 @@ __global__ void __launch_bounds__(TH_BLOCK) k_thermo(const ThermoArgs A) {
     for (int d = 0; d < 3; d++) A.v[d * N + g] = v[d];
   } else if (t < A.nsm + A.nfree + A.nbm) {
     pdl_enter();
-    if (!A.start) {
+    {
       const int p = t - A.nsm - A.nfree;
       BigStages B;
       big_stages(A, p, A.th->s, B);
@@ -1497,7 +1538,6 @@ __global__ void __launch_bounds__(TH_BLOCK) k_thermo(const ThermoArgs A) {
   } else {
     pdl_enter();
   }
-  if (A.start) return;
   __shared__ double red[6][TH_BLOCK / 32];
   __shared__ bool last;
   double kk[6] = {k1[0], k1[1], k1[2], k2[0], k2[1], k2[2]};
@@ -1518,15 +1558,21 @@ __global__ void __launch_bounds__(TH_BLOCK) k_thermo(const ThermoArgs A) {
     last = atomicAdd(&A.th->count, 1u) == gridDim.x - 1;
   }
   __syncthreads();
-  if (!last || threadIdx.x != 0) return;
+  if (!last) return;
   __threadfence();
+  // the blocks' sums: lane l adds blocks l, l + 32, ... in order, then a
+  // fixed butterfly over the lanes (the same result at every run)
   const volatile double* P = A.part;
-  double K1[3] = {0.0, 0.0, 0.0}, K2[3] = {0.0, 0.0, 0.0};
-  for (unsigned b = 0; b < gridDim.x; b++)
-    for (int j = 0; j < 3; j++) {
-      K1[j] += P[6 * b + j];
-      K2[j] += P[6 * b + 3 + j];
-    }
+  double K[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  if (threadIdx.x < 32)
+    for (unsigned b = threadIdx.x; b < gridDim.x; b += 32)
+#pragma unroll
+      for (int j = 0; j < 6; j++) K[j] += P[6 * b + j];
+#pragma unroll
+  for (int j = 0; j < 6; j++)
+    for (int o = 16; o > 0; o >>= 1) K[j] += __shfl_xor_sync(0xffffffffu, K[j], o);
+  if (threadIdx.x != 0) return;
+  const double K1[3] = {K[0], K[1], K[2]}, K2[3] = {K[3], K[4], K[5]};
   ThermoDev& T = *A.th;
   if (A.end) {
     for (int k = 0; k < 3; k++) T.eta[k] += T.tm * T.etap[k];
@@ -1628,6 +1674,7 @@ struct MdState {
   int* tcls = nullptr;
   int* abm = nullptr;
   int th_ndf[3] = {0, 0, 0};
+  double th_tm = 0.0;  // the M step
 };
 
 static MdState* md_of(orac_gpu_ctx* ctx) {
@@ -1775,7 +1822,10 @@ static int md_kick(orac_gpu_ctx* ctx, MdState& S, const double* c) {
 // molecules need their centres (the pair kernels' inputs; the
 // intramolecular levels read atom positions only), as ORAC calls appbou
 // only before the M forces (src/mtsmd.f:2952)
-static int md_drift(orac_gpu_ctx* ctx, MdState& S, double dt, const double* c, int zmask, bool groups = true) {
+// tstart: the drift opens an M step under thermostats and applies its start
+// sandwich (k_drift<true>) before the kick
+static int md_drift(orac_gpu_ctx* ctx, MdState& S, double dt, const double* c, int zmask, bool groups = true,
+                    bool tstart = false) {
   if (S.nbig && c) {
     // the RATTLE of large molecules is a separate kernel: kick first
     if (int rc = md_kick(ctx, S, c)) return rc;
@@ -1786,10 +1836,23 @@ static int md_drift(orac_gpu_ctx* ctx, MdState& S, double dt, const double* c, i
   kick_fill(A, S, c);
   A.fv = S.has_n0 ? S.ffix[LN0] : nullptr;
   for (int l = 0; l < NLV; l++) A.fz[l] = ((zmask >> l) & 1) ? S.ffix[l] : nullptr;
+  if (tstart) {
+    A.fk[LM] = S.ffix[LM];
+    A.th = S.th;
+    A.tcls = S.tcls;
+    A.abm = S.abm;
+    A.vcur = S.vcur;
+    A.msum = S.msum;
+    A.bmass = S.bmass;
+    A.tcm = 0.5 * S.th_tm;
+  }
   const int n = S.nsm + S.ndg + S.nda;
   int slot = -1;
   if (int rc = prof_begin(ctx, &slot, PROF_DRIFT)) return rc;
-  orac_launch(k_drift, (n + 31) / 32, 32, 0, ctx->stream, A);
+  if (tstart)
+    orac_launch(k_drift<true>, (n + 31) / 32, 32, 0, ctx->stream, A);
+  else
+    orac_launch(k_drift<false>, (n + 31) / 32, 32, 0, ctx->stream, A);
   CKL();
   if (int rc = prof_end(ctx, slot)) return rc;
   if (S.nbig) {
@@ -1805,10 +1868,10 @@ static int md_drift(orac_gpu_ctx* ctx, MdState& S, double dt, const double* c, i
   return ORAC_OK;
 }
 
-// a thermostat pass (k_thermo; ThermoArgs has the coefficients), an end
-// pass after the sums of the molecules outside the small ones (k_mol_sums)
-static int md_thermo(orac_gpu_ctx* ctx, MdState& S, bool start, bool end, bool k2, double c0, double c1, double cm,
-                     double cl, double ch) {
+// a thermostat pass (k_thermo; ThermoArgs has the coefficients) after the
+// sums of the molecules outside the small ones (k_mol_sums)
+static int md_thermo(orac_gpu_ctx* ctx, MdState& S, bool end, bool k2, double c0, double c1, double cm, double cl,
+                     double ch) {
   ThermoArgs A;
   memset(&A, 0, sizeof(A));
   A.N = ctx->N;
@@ -1836,7 +1899,6 @@ static int md_thermo(orac_gpu_ctx* ctx, MdState& S, bool start, bool end, bool k
   A.ch = ch;
   A.end = end;
   A.k2 = k2;
-  A.start = start;
   A.th = S.th;
   A.part = S.tpart;
   A.flag = S.flag;
@@ -1844,9 +1906,9 @@ static int md_thermo(orac_gpu_ctx* ctx, MdState& S, bool start, bool end, bool k
   if (int rc = prof_begin(ctx, &slot, PROF_DRIFT)) return rc;
   A.lvmask = (c0 != 0.0 && S.ffix[LN0] ? 1 : 0) | (c1 != 0.0 && S.ffix[LN1] ? 2 : 0) | 4 | (cl != 0.0 ? 8 : 0) |
              (ch != 0.0 ? 16 : 0);
-  if (!start && S.nbm) {
+  if (S.nbm) {
     CK(cudaMemsetAsync(S.msum, 0, sizeof(unsigned long long) * TH_NS * (size_t)S.nbm, ctx->stream));
-    orac_launch(k_mol_sums, S.nchunk, TH_BLOCK, 0, ctx->stream, A);
+    orac_launch(k_mol_sums, S.nchunk, TS_BLOCK, 0, ctx->stream, A);
     CKL();
   }
   orac_launch(k_thermo, S.th_blocks, TH_BLOCK, 0, ctx->stream, A);
@@ -2116,22 +2178,22 @@ static int md_step(orac_gpu_ctx* ctx, MdState& S, bool update, bool energy) {
       for (int l = LL; l < LN0; l++)
         if (k % per[l] == 0) c[l] = dt[l];
     }
-    if (S.th && k % per[LM] == 0) {
+    const bool tstart = S.th && k % per[LM] == 0;
+    if (tstart) {
       // an M step starts: the end of the previous one (its N0 and N1 end
       // half kicks and the M sandwich, K1), the L kicks at an L boundary
-      // (the H and L start kicks at the step's start), K2, then the start
-      // sandwich; the drift keeps the N1 start half kick
+      // (the H and L start kicks at the step's start), K2; the drift then
+      // applies the start sandwich and the N1 start half kick
       const bool first = k == 0;
-      if (int rc = md_thermo(ctx, S, false, !first, true, first ? 0.0 : 0.5 * dt[LN0], first ? 0.0 : 0.5 * dt[LN1],
+      if (int rc = md_thermo(ctx, S, !first, true, first ? 0.0 : 0.5 * dt[LN0], first ? 0.0 : 0.5 * dt[LN1],
                              0.5 * dt[LM], c[LL], c[LH]))
         return rc;
-      if (int rc = md_thermo(ctx, S, true, false, false, 0, 0, 0.5 * dt[LM], 0, 0)) return rc;
       for (int l = 0; l < NLV; l++) c[l] = l == LN1 ? 0.5 * dt[LN1] : 0.0;
     }
     int zmask = 0;
     for (int l = 0; l < NLV; l++)
       if ((k + 1) % per[l] == 0) zmask |= 1 << l;
-    if (int rc = md_drift(ctx, S, dt[LN0], c, zmask, (k + 1) % per[LM] == 0)) return rc;
+    if (int rc = md_drift(ctx, S, dt[LN0], c, zmask, (k + 1) % per[LM] == 0, tstart)) return rc;
     const bool last = k == K - 1;
     const bool e_now = energy && last;
     const bool due_n1 = S.has_n1 && (k + 1) % per[LN1] == 0;
@@ -2218,7 +2280,7 @@ static int md_step(orac_gpu_ctx* ctx, MdState& S, bool update, bool energy) {
   }
   if (S.th) {
     // the last M step's end (K1) and the end half kicks of L and H
-    if (int rc = md_thermo(ctx, S, false, true, false, 0.5 * dt[LN0], 0.5 * dt[LN1], 0.5 * dt[LM], 0.5 * dt[LL],
+    if (int rc = md_thermo(ctx, S, true, false, 0.5 * dt[LN0], 0.5 * dt[LN1], 0.5 * dt[LM], 0.5 * dt[LL],
                            0.5 * dt[LH]))
       return rc;
   } else {
@@ -2290,6 +2352,7 @@ static int thermo_setup(orac_gpu_ctx* ctx, MdState& S, const std::vector<int>& m
   }
   T.tm = tm;
   T.tm4 = 0.25 * tm;
+  S.th_tm = tm;
   S.nbm = (int)bm.size();
   S.nchunk = (int)br.size();
   S.th_blocks = (S.nsm + S.nfree + S.nbm + TH_BLOCK - 1) / TH_BLOCK;
