@@ -376,7 +376,9 @@ int bonded_launch(orac_gpu_ctx* ctx, int mask, const double* d_x, double* d_f, u
   A.e = d_e;
   const int n = B.nb + B.nbend + B.nt + B.nit;
   if (n == 0) return ORAC_OK;
-  orac_launch(k_bonded, (n + 255) / 256, 256, 0, ctx->stream, A);
+  // 64 threads a block: the terms of one launch spread over four times the
+  // SMs (each thread's FP64 chain sets the time, not the issue rate)
+  orac_launch(k_bonded, (n + 63) / 64, 64, 0, ctx->stream, A);
   CKL();
   return ORAC_OK;
 }

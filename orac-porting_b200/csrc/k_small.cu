@@ -359,7 +359,7 @@ int ferrf_launch_lists(orac_gpu_ctx* ctx, int nlist, const int* const* d_pairs, 
     nmax = npairs[k] > nmax ? npairs[k] : nmax;
   }
   if (ns == 0) return ORAC_OK;
-  orac_launch(k_small_segs, dim3((nmax + 255) / 256, ns), dim3(256), 0, ctx->stream, S);
+  orac_launch(k_small_segs, dim3((nmax + 63) / 64, ns), dim3(64), 0, ctx->stream, S);
   CKL();
   return ORAC_OK;
 }
@@ -385,7 +385,7 @@ int small_launch_set(orac_gpu_ctx* ctx, int n, const SmallSpec* specs) {
     nmax = p.npairs > nmax ? p.npairs : nmax;
   }
   if (ns == 0) return ORAC_OK;
-  orac_launch(k_small_segs, dim3((nmax + 255) / 256, ns), dim3(256), 0, ctx->stream, S);
+  orac_launch(k_small_segs, dim3((nmax + 63) / 64, ns), dim3(64), 0, ctx->stream, S);
   CKL();
   return ORAC_OK;
 }
