@@ -441,6 +441,11 @@ int orac_gpu_md_set_thermostat(orac_gpu_ctx* ctx, double temp, double nu_com,
  * (internal units), thermostats ordered centres of mass, solute, solvent.
  * Synchronises the context's stream. */
 int orac_gpu_md_thermostat(orac_gpu_ctx* ctx, double* out);
+/* A restart's thermostat state (ORAC's restart records gh = eta and vh =
+ * etap, src/readrs.f:247-251): eta[3] and etap[3] in the order above, after
+ * orac_gpu_md_setup.  Synchronises the context's stream. */
+int orac_gpu_md_set_thermostat_state(orac_gpu_ctx* ctx, const double* eta,
+                                     const double* etap);
 
 /* Batched systems ----------------------------------------------------------
  * Many independent systems (replicas, HREM states, alchemical windows), one

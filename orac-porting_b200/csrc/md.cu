@@ -2734,6 +2734,26 @@ int orac_gpu_md_set_thermostat(orac_gpu_ctx* ctx, double temp, double nu_com, do
   return ORAC_OK;
 }
 
+int orac_gpu_md_set_thermostat_state(orac_gpu_ctx* ctx, const double* eta, const double* etap) {
+  if (!ctx || !eta || !etap) return ORAC_ERR_PARAM;
+  MdState* S = ctx->md;
+  if (!S || !S->ready || !S->th) return ctx_fail(ctx, ORAC_ERR_STATE, "no thermostats (md_set_thermostat, md_setup)");
+  for (int k = 0; k < 3; k++)
+    if (!std::isfinite(eta[k]) || !std::isfinite(etap[k])) return ctx_fail(ctx, ORAC_ERR_PARAM, "thermostat state");
+  CK(cudaSetDevice(ctx->device));
+  ThermoDev T;
+  CK(cudaMemcpyAsync(&T, S->th, sizeof(T), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  for (int k = 0; k < 3; k++) {
+    T.eta[k] = eta[k];
+    T.etap[k] = etap[k];
+    T.s[k] = std::exp(-T.tm4 * etap[k]);
+  }
+  CK(cudaMemcpyAsync(S->th, &T, sizeof(T), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return ORAC_OK;
+}
+
 int orac_gpu_md_thermostat(orac_gpu_ctx* ctx, double* out) {
   if (!ctx || !out) return ORAC_ERR_PARAM;
   MdState* S = ctx->md;

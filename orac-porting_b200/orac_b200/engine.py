@@ -359,6 +359,13 @@ class Engine:
         check(self.ctx, self.lib.orac_gpu_md_thermostat(self.ctx, out.ctypes.data), "md_thermostat")
         return out[0:3].copy(), out[3:6].copy(), out[6:9].copy(), out[9:12].astype(int), float(out[12])
 
+    def set_thermostat_state(self, eta, etap):
+        """A restart's thermostat coordinates and velocities
+        (orac_gpu_md_set_thermostat_state); after md_setup."""
+        e, p = f64(eta), f64(etap)
+        check(self.ctx, self.lib.orac_gpu_md_set_thermostat_state(self.ctx, e.ctypes.data, p.ctypes.data),
+              "md_set_thermostat_state")
+
     def md_work_trace(self, max_records=8192):
         """(rtime, work) after each M step, oldest first, and the count."""
         out = np.zeros(2 * max(1, max_records))

@@ -97,6 +97,7 @@ def load():
         "orac_gpu_md_work_trace": (i, [_P, i, _P, C.POINTER(i64)]),
         "orac_gpu_md_set_thermostat": (i, [_P, d, d, d, d]),
         "orac_gpu_md_thermostat": (i, [_P, _P]),
+        "orac_gpu_md_set_thermostat_state": (i, [_P, _P, _P]),
         "orac_gpu_batch_sync": (i, [_P]),
         "orac_gpu_batch_destroy": (i, [_P]),
         "orac_gpu_batch_last_error": (C.c_char_p, [_P]),

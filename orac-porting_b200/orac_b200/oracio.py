@@ -155,14 +155,31 @@ def read_rst(path, ntap=None):
     big = r.floats(6 * n + 3 * ngrp + 6 * nprot)
     x = big[:3 * n].reshape(3, n)
     vel = big[3 * n:6 * n].reshape(3, n)
-    return dict(co=co, oc=oc, nstep=nstep, temp=temp, ntap=n, ngrp=ngrp, nprot=nprot, xyz=x, v=vel)
+    out = dict(co=co, oc=oc, nstep=nstep, temp=temp, ntap=n, ngrp=ngrp, nprot=nprot, xyz=x, v=vel)
+    # the thermostats' state when the run had them (src/readrs.f:240-251:
+    # vpx1, the averages, then hoover and cpress, and with hoover nh, gh =
+    # eta, vh = etap, vh1); older or shorter files end before it
+    try:
+        r.floats(3 * n)
+        n1, n2 = (int(v) for v in r.read(2))
+        r.floats(n1 + n2)
+        hoover = r.read(2)[0].upper().startswith(("T", ".T"))
+        if hoover:
+            nh = int(r.read(1)[0])
+            g = r.floats(3 * nh)
+            out["eta"], out["etap"] = g[:nh].copy(), g[nh:2 * nh].copy()
+    except (EOFError, ValueError, IndexError):
+        pass
+    return out
 
 
-def write_rst(path, co, xyz, v, nstep=0, temp=0.0, grp=None, ngrp=0, mol=None, nprot=0):
-    """A restart file with the records ORAC reads (src/readrs.f:216-244):
+def write_rst(path, co, xyz, v, nstep=0, temp=0.0, grp=None, ngrp=0, mol=None, nprot=0, thermostat=None):
+    """A restart file with the records ORAC reads (src/readrs.f:216-251):
     box, step and temperature, sizes, positions, velocities (twice, as
     src/dumprs.f writes vpx and vpx1), group and molecule centres (zero when
-    not given), no running averages, no thermostat or barostat state."""
+    not given), no running averages, no barostat state; thermostat = (eta,
+    etap) of the three Nose-Hoover thermostats writes hoover and ORAC's gh,
+    vh and vh1 records (vh1 as etap)."""
     co = np.asarray(co, dtype=np.float64)
     oc = np.linalg.inv(co)
     n = xyz.shape[1]
@@ -179,7 +196,13 @@ def write_rst(path, co, xyz, v, nstep=0, temp=0.0, grp=None, ngrp=0, mol=None, n
         f.write(rec(np.concatenate([xyz.ravel(), v.ravel(), grp.ravel(), mol.ravel(), np.zeros(3 * nprot)])))
         f.write(rec(v.ravel()))
         f.write("0 0\n\n")
-        f.write("F F\n")
+        if thermostat is None:
+            f.write("F F\n")
+        else:
+            eta, etap = (np.asarray(t, dtype=np.float64).ravel() for t in thermostat)
+            f.write("T F\n")
+            f.write(f"{len(eta)}\n")
+            f.write(rec(np.concatenate([eta, etap, etap])))
         f.write("F\n")
 
 

@@ -1062,6 +1062,15 @@ void orc_md_set_thermostat(void* h, double temp, const double* nu) {
   M->thermo = 1;
 }
 
+/* a restart's thermostat state (src/readrs.f:247-251: gh = eta, vh = etap) */
+void orc_md_set_thermostat_state(void* h, const double* eta, const double* etap) {
+  orc_md* M = (orc_md*)h;
+  for (int k = 0; k < 3; k++) {
+    M->eta[k] = eta[k];
+    M->etap[k] = etap[k];
+  }
+}
+
 /* out: eta[3], etap[3], Q[3], ndf[3], the thermostats' energy */
 void orc_md_thermostat(void* h, double* out) {
   orc_md* M = (orc_md*)h;

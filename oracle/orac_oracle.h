@@ -249,6 +249,7 @@ void orc_md_set_intra(void* h, int nb, const int* lbnd, const double* r0,
  * thermostats; the state out[13]: eta[3], etap[3], Q[3], ndf[3], energy. */
 void orc_md_set_thermostat(void* h, double temp, const double* nu);
 void orc_md_thermostat(void* h, double* out);
+void orc_md_set_thermostat_state(void* h, const double* eta, const double* etap);
 
 /* ORAC's intra-alchemical corrections (orac_oracle.c): per-atom lambdas of
  * the species, the listqq of src/initialize_lambda.f, ferrf_alchemy_add

@@ -555,6 +555,11 @@ class OracleMD:
         self.L.orc_md_set_thermostat.argtypes = [C.c_void_p, C.c_double, _D]
         self.L.orc_md_set_thermostat(self.h, float(temp), _f([nu_com, nu_solute, nu_solvent]))
 
+    def set_thermostat_state(self, eta, etap):
+        """A restart's thermostat coordinates and velocities."""
+        self.L.orc_md_set_thermostat_state.argtypes = [C.c_void_p, _D, _D]
+        self.L.orc_md_set_thermostat_state(self.h, _f(eta), _f(etap))
+
     def thermostat(self):
         """(eta[3], etap[3], Q[3], ndf[3], energy) of the three thermostats."""
         out = np.zeros(13)

@@ -144,3 +144,41 @@ def test_thermostat_setter_errors():
     with pytest.raises(OracGpuError):
         g.md_thermostat()  # NVE: no thermostats
     g.close()
+
+
+def test_nvt_restart_continues_the_run(tmp_path):
+    """An ORAC restart file of a thermostatted run (positions, velocities, the
+    hoover records gh = eta, vh = etap) written after 4 steps and read into a
+    new context continues the run: 4 + 3 steps against 7 in one go (the
+    restarted context builds its lists again; the pair set and the
+    fixed-point forces are the same)."""
+    from test_oracle_nvt import restored
+
+    from orac_b200 import oracio
+
+    s = chain()
+
+    def make(sys_):
+        g = Engine(sys_)
+        g.set_thermostat(300.0, 50.0, 50.0, 50.0)
+        g.md_setup(SCHED["dt_h"], SCHED["lrespa"], SCHED["mrespa"], SCHED["nupdte"], SCHED["rshk"],
+                   n1respa=SCHED["n1respa"], n0respa=SCHED["n0respa"])
+        return g
+
+    a = make(s.copy())
+    a.md_run(4)
+    x, v = a.md_state()
+    eta, etap, _, _, _ = a.md_thermostat()
+    p = str(tmp_path / "nvt.rst")
+    oracio.write_rst(p, s.co, x, v, nstep=4, temp=300.0, thermostat=(eta, etap))
+    a.md_run(3)
+    r = oracio.read_rst(p, s.ntap)
+    b = make(restored(s, r["xyz"], r["v"]))
+    b.set_thermostat_state(r["eta"], r["etap"])
+    b.md_run(3)
+    xa, _ = a.md_state()
+    xb, _ = b.md_state()
+    assert np.abs(xa - xb).max() < 1e-8
+    np.testing.assert_allclose(b.md_thermostat()[1], a.md_thermostat()[1], rtol=1e-8)
+    a.close()
+    b.close()

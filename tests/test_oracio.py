@@ -77,3 +77,22 @@ def test_restart_round_trip(tmp_path):
     r = oracio.read_rst(p, 50)
     assert np.array_equal(r["co"], co) and np.array_equal(r["xyz"], x) and np.array_equal(r["v"], v)
     assert r["nstep"] == 7 and r["temp"] == 300.5 and (r["ngrp"], r["nprot"]) == (4, 2)
+
+
+def test_restart_round_trip_with_thermostats(tmp_path):
+    """A thermostatted run's restart carries ORAC's hoover records (gh = eta,
+    vh = etap, vh1), src/readrs.f:247-251; a restart without them reads as
+    before."""
+    rng = np.random.default_rng(4)
+    co = np.diag([20.0, 20.0, 20.0])
+    x = rng.uniform(-10, 10, (3, 12))
+    v = rng.normal(0, 0.01, (3, 12))
+    eta, etap = np.array([1e-3, -2e-4, 5e-3]), np.array([3e-5, -1e-6, 2e-4])
+    p = str(tmp_path / "t.rst")
+    oracio.write_rst(p, co, x, v, nstep=3, temp=298.0, thermostat=(eta, etap))
+    r = oracio.read_rst(p, 12)
+    assert np.array_equal(r["eta"], eta) and np.array_equal(r["etap"], etap)
+    assert np.array_equal(r["xyz"], x) and np.array_equal(r["v"], v)
+    q = str(tmp_path / "n.rst")
+    oracio.write_rst(q, co, x, v)
+    assert "eta" not in oracio.read_rst(q, 12)

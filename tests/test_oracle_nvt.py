@@ -71,3 +71,38 @@ def test_stiff_thermostats_cool_the_box_and_conserve_the_extended_energy(chain):
     dt = np.abs(rt[:, 10] - rt[0, 10]).max()
     assert dt < dn + 2e-4, (dt, dn)
     assert (th[0] > 0).all() and (th[1] > 0).all()  # a hot box: every thermostat pulls
+
+
+def restored(s, x, v):
+    """The system at a restart's positions (Cartesian, 3 x N) and velocities."""
+    r = s.copy()
+    sc = np.linalg.solve(r.co, x)
+    r.xp0, r.yp0, r.zp0 = sc[0].copy(), sc[1].copy(), sc[2].copy()
+    r.xyz_restart = x.copy()
+    r.vx, r.vy, r.vz = v[0].copy(), v[1].copy(), v[2].copy()
+    return r
+
+
+def test_restart_with_the_thermostat_state_continues_the_run(chain):
+    """Positions, velocities and ORAC's thermostat records of a restart
+    (src/readrs.f:247-251) continue the run: 4 + 3 steps against 7 in one go."""
+    def make(s):
+        o = oracle.OracleMD(s, SCHED["dt_h"], SCHED["lrespa"], SCHED["mrespa"], SCHED["nupdte"], SCHED["rshk"],
+                            n1respa=SCHED["n1respa"], n0respa=SCHED["n0respa"])
+        o.set_thermostat(300.0, 50.0, 50.0, 50.0)
+        return o
+
+    a = make(chain.copy())
+    a.run(4)
+    x, v = a.state()
+    eta, etap, _, _, _ = a.thermostat()
+    a.run(3)
+    b = make(restored(chain, x, v))
+    b.set_thermostat_state(eta, etap)
+    b.run(3)
+    xa, _ = a.state()
+    xb, _ = b.state()
+    assert np.abs(xa - xb).max() < 1e-8
+    np.testing.assert_allclose(b.thermostat()[1], a.thermostat()[1], rtol=1e-8)
+    a.close()
+    b.close()
