@@ -10,7 +10,8 @@ device-resident driver of liborac_gpu.so with the state resident in HBM.
 Further legs on the same line: the state's forces and energies against the
 FP64 oracle, a per-kernel-family breakdown of the step, a 1,000-step energy
 drift against the oracle's, 64 batched alchemical windows, ORAC's own test1
-system, the 22,700-atom solvated chain and the as-specified 31 A box,
+system (NVE, and with test1's Nose-Hoover thermostats), the 22,700-atom
+solvated chain and the as-specified 31 A box,
 replica exchange of 16 batched replicas, test4's non-equilibrium work swarm
 on ORAC's system, 128 uneven HREM replicas and the serving loop.  Prints
 one JSON line.
