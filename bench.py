@@ -601,6 +601,8 @@ def batch_arm(args, wl, s, device, flush):
     (orac_gpu_batch_run); the plain reference is one window alone on the
     same driver.  Every window ends with an energy step that yields its
     dU/dlambda."""
+    import ctypes as C
+
     import torch
 
     from orac_b200.engine import Batch
@@ -633,8 +635,18 @@ def batch_arm(args, wl, s, device, flush):
     tune_batch = tuned(b)
     stream = torch.cuda.ExternalStream(b.stream(), device=device)
     b.run(args.warmup)
+    b.sync()
+    cnt = (C.c_int64 * 4)()
+    for e in engines:
+        e.lib.orac_gpu_counters(e.ctx, cnt, 1)
     step_ms = _timed_steps(lambda: b.run(1, sync=False), stream, flush, args.steps)
     b.sync()
+    # pair evaluations of every window over the timed steps (device counters)
+    pairs_ewald = pairs_lj = 0
+    for e in engines:
+        e.lib.orac_gpu_counters(e.ctx, cnt, 0)
+        pairs_ewald += int(cnt[2])
+        pairs_lj += int(cnt[3])
     # dU/dlambda of every window: energy records written on the device every
     # DUDL_EVERY steps of a batched sampling run after the timed steps
     for e in engines:
@@ -649,7 +661,8 @@ def batch_arm(args, wl, s, device, flush):
     st = sorted(step_ms)
     return {"systems": nwin, "atoms_per_window": base.ntap, "total_ms": sum(step_ms),
             "step_ms_p50": st[len(st) // 2], "step_ms_p99": st[min(len(st) - 1, int(0.99 * len(st)))],
-            "plain_total_ms": sum(plain_ms), "lambdas": lams, "dudl": dudl,
+            "plain_total_ms": sum(plain_ms), "lambdas": lams, "dudl": dudl, "pairs_ewald": pairs_ewald,
+            "pairs_lj": pairs_lj,
             "tuning": {"batch": tune_batch, "plain_window": tune_plain}}
 
 
@@ -1324,6 +1337,18 @@ def main():
         wts = np.gradient(lam) * 0.0  # trapezoid weights
         wts[1:] += 0.5 * np.diff(lam)
         wts[:-1] += 0.5 * np.diff(lam)
+        # the pair kernel's FP32 rate with the device full: every window's
+        # pair FLOPs over the whole batched step time (the step also runs
+        # SPME, drifts and the bonded levels, so this bounds k_pair's rate
+        # from below)
+        bflop = 60.0 * bt["pairs_ewald"] + 36.0 * bt["pairs_lj"]
+        btf = bflop / (bt["total_ms"] / 1e3) / 1e12
+        device_full = {"pair_evals_per_s": (bt["pairs_ewald"] + bt["pairs_lj"]) / (bt["total_ms"] / 1e3),
+                       "achieved_tflops": btf, "peak_tflops": roofline.get("peak"),
+                       "frac_of_fp32": btf / roofline["peak"] if roofline.get("peak") else None,
+                       "how": "pair FLOPs of all windows (60 per LJ+Ewald pair, 36 per LJ-only pair, device "
+                              "counters) over the whole batched step time, against the same measured FP32 FMA rate "
+                              "as roofline: a lower bound on k_pair's own rate with the device full"}
         out["batched"] = {
             "workload": f"{bt['systems']} alchemical lambda windows (lambda_k = k/{bt['systems'] - 1}, charges "
                         "then LJ switched off) of a 40-atom "
@@ -1345,6 +1370,7 @@ def main():
                                    "from the same unequilibrated state and samples a few ps, so the sum is a "
                                    "short-run estimate, not a converged free energy"},
             "tuning": bt["tuning"],
+            "device_full": device_full,
             "how": "one graph launch per H step advances every window (orac_gpu_batch_run); plain = one window "
                    "alone through the same driver; both with the real-space kernel's launch configuration chosen by "
                    "the autotuner (orac_gpu_batch_tune / orac_gpu_tune)"}
