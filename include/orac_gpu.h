@@ -389,8 +389,8 @@ int orac_gpu_md_set_graphs(orac_gpu_ctx* ctx, int on);
  * receives the number written since the last reset; reset != 0 clears the
  * count.  Column 15 holds dU/dlambda for alchemical windows
  * (orac_gpu_set_lambda with dlam), the segment energy for REM contexts and
- * the work so far under a non-equilibrium schedule, otherwise the
- * thermostats' energy under Nose-Hoover thermostats.  Synchronises the
+ * the work so far under a non-equilibrium schedule, and for other contexts
+ * the thermostats' energy under Nose-Hoover thermostats.  Synchronises the
  * context's stream. */
 int orac_gpu_md_records(orac_gpu_ctx* ctx, int max, double* out,
                         int64_t* n_total, int reset);
@@ -430,10 +430,10 @@ int orac_gpu_md_work_trace(orac_gpu_ctx* ctx, int max, double* out,
  * <= 0 removes the thermostats.  The M level of every step then runs ORAC's
  * thermostat sequence (src/mtsmd.f:2556-2618, 2932, 3109-3170).  Molecules
  * whose constraints need the iterative solver (a connected set of more than
- * 4 atoms or 3 constraints) are refused at md_setup.  Energy records carry
- * the thermostats' energy in column 15 (unless a schedule's work is there)
- * and add it to the total (column 10), the extended system's conserved
- * energy.  This replaces rank 3 of ORAC's ensembles only in part: the
+ * 4 atoms or 3 constraints) are refused at md_setup.  Energy records add
+ * the thermostats' energy to the total (column 10), the extended system's
+ * conserved energy, and carry it in column 15 where that column has no other
+ * use (no alchemy, REM or schedule).  This replaces rank 3 of ORAC's ensembles only in part: the
  * Parrinello-Rahman barostat (ISOSTRESS, cpress) is not built. */
 int orac_gpu_md_set_thermostat(orac_gpu_ctx* ctx, double temp, double nu_com,
                                double nu_solute, double nu_solvent);

@@ -1136,8 +1136,9 @@ __global__ void k_rattle_big(const ConsArgs A) {
 // [1] kinetic, [2..7] M, L, H LJ and Coulomb, [8] SPME, [9] the constant
 // (self energy), [10] total, [11] status flags, [12] bonded, [13] 1-4 and
 // intra-group pairs, [14] erf corrections, [15] dU/dlambda (alchemy), the
-// REM segment's nonbonded energy (REM), the work of a non-equilibrium run or
-// the thermostats' energy (Nose-Hoover, which [10] then includes).
+// REM segment's nonbonded energy (REM), the work of a non-equilibrium run, or
+// for a standard context the thermostats' energy (Nose-Hoover thermostats
+// add it to [10] in every case).
 __global__ void k_record(const double* __restrict__ e, const int* __restrict__ flag, double econst, double self_dudl,
                          int var, double* __restrict__ ring, int cap, unsigned long long* __restrict__ n,
                          const NeDev* __restrict__ ne, const ThermoDev* __restrict__ th) {
@@ -1177,7 +1178,7 @@ __global__ void k_record(const double* __restrict__ e, const int* __restrict__ f
     double et = 0.0;
     for (int k = 0; k < 3; k++) et += th->ndfkt[k] * th->eta[k] + 0.5 * th->q[k] * th->etap[k] * th->etap[k];
     r[10] += et;
-    if (var != 3) r[15] = et;
+    if (var == 0) r[15] = et;  // where the column has no other use
   }
   r[11] = (double)*flag;
   *n = k + 1;
@@ -2997,7 +2998,8 @@ static int md_run_impl(orac_gpu_ctx* ctx, int nsteps, int energy_every, double* 
         double et = 0.0;
         for (int q = 0; q < 3; q++) et += T.ndfkt[q] * T.eta[q] + 0.5 * T.q[q] * T.etap[q] * T.etap[q];
         r[10] += et;
-        if (!md_ne(ctx)) r[15] = et;
+        // in column 15 where it has no other use (no alchemy, REM or schedule)
+        if (ctx->variant != VAR_REM && !(ctx->variant == VAR_ALCH && ctx->d_dq) && !md_ne(ctx)) r[15] = et;
       }
       r[11] = (double)flag;
     }

@@ -912,7 +912,7 @@ int orc_md_run(void* h, int nsteps, int energy_every, double* rec) {
       if (M->thermo) { /* the extended system's conserved energy */
         const double et = thermo_energy(M);
         r[10] += et;
-        if (!M->ne) r[15] = et;
+        if (!M->ne && !M->alch) r[15] = et;
       }
       r[11] = fail;
     }

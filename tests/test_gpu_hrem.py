@@ -88,3 +88,39 @@ def test_hrem_forced_acceptance_swaps_every_attempted_pair():
     assert enss[0].tolist() == [0, 2, 1, 3]
     assert enss[1].tolist() == [1, 3, 0, 2]
     assert np.all(acc == 1.0)
+
+
+def test_hrem_with_thermostats_keeps_the_segment_energy_in_its_column():
+    """test2 runs its replicas with ORAC's thermostats: under them the energy
+    record's column 15 still holds the REM segment energy (the thermostats'
+    energy goes into the total only), so the exchange reads the same quantity
+    -- a massive thermostat (1 cm^-1) leaves it at the NVE run's to 1e-7 after
+    one step -- and a thermostatted HREM batch exchanges as the NVE one."""
+    s = system()
+
+    def make(factor, thermo):
+        e = Engine(s.copy())
+        e.set_rem(s.rematom, 0, factor)
+        if thermo:
+            e.set_thermostat(300.0, *thermo)
+        e.md_setup(SCHED["dt_h"], SCHED["lrespa"], SCHED["mrespa"], SCHED["nupdte"], SCHED["rshk"])
+        return e
+
+    a, b = make(0.8, None), make(0.8, (1.0, 1.0, 1.0))
+    ra = a.md_run(1, energy_every=1)
+    rb = b.md_run(1, energy_every=1)
+    et = b.md_thermostat()[4]
+    assert rb[0, 15] != et
+    np.testing.assert_allclose(rb[0, 15], ra[0, 15], rtol=1e-7)
+    np.testing.assert_allclose(rb[0, 10], ra[0, 10] + et, rtol=1e-7)
+    a.close()
+    b.close()
+    ladder = hrem.ladder_geometric(4, 0.7)
+    engines = [make(f, (10.0, 10.0, 10.0)) for f in ladder]
+    h = hrem.HremBatch(engines, ladder, KT_300, seed=5)
+    for _ in range(3):
+        p = h.interval(3)
+        assert np.all(np.isfinite(p)) and sorted(h.ens.tolist()) == [0, 1, 2, 3]
+    h.close()
+    for e in engines:
+        e.close()
