@@ -104,7 +104,8 @@ NE_WALKERS = 12  # the three restart states, four velocity draws each
 # the reference's test1 schedule: 15 fs outer step, L 3 fs (SPME), M 1.5 fs,
 # intramolecular 0.75 / 0.375 fs, list update every 6 steps
 F0_WORKLOAD = dict(build=f0_system, dt_h=15.0, lrespa=5, mrespa=2, n1respa=2, n0respa=2, nupdte=6, rshk="l")
-TEST1_THERMOS = (298.0, 10.0, 10.0, 10.0)  # test1/md.in: TEMPERATURE 298, THERMOS solute/solvent/cofm 10 cm^-1
+# test1/md.in and test2/rem.in: TEMPERATURE 298, THERMOS solute/solvent/cofm 10 cm^-1
+TEST1_THERMOS = (298.0, 10.0, 10.0, 10.0)
 DUDL_STEPS, DUDL_EVERY = 400, 2  # dU/dlambda sampling of the batched windows
 SERVE_PLAIN_SAMPLE = 8  # serving requests also run one at a time, to check the plain model
 HREM_N, HREM_EVERY, HREM_INTERVALS = 16, 15, 10  # replica-exchange leg
@@ -687,11 +688,13 @@ def build_pool(specs):
         return list(ex.map(systems.build_spec, specs, chunksize=1))
 
 
-def uneven_engine(s, spec, device, wl):
+def uneven_engine(s, spec, device, wl, thermostats=None):
     from orac_b200.engine import Engine
 
     e = Engine(s, device=device)
     e.set_rem(s.rematom, 0, spec["rem_factor"])  # seg_select kind 0: pairs touching the solute
+    if thermostats:
+        e.set_thermostat(*thermostats)
     e.md_setup(wl["dt_h"], wl["lrespa"], wl["mrespa"], wl["nupdte"], wl["rshk"], econst=0.0)
     return e
 
@@ -904,7 +907,8 @@ def hrem_arm(args, wl, device):
     70-atom solute chain, the size of test2's ligand + TYR27 segment),
     solute scaling on a geometric ladder from 1 to 0.6 as in test2
     (rem_factor(3) on the pairs touching the solute, seg_select kind 0),
-    300 K, an exchange attempt every 15 steps (60 fs) by ORAC's rule on
+    test2's Nose-Hoover thermostats (298 K, 10 cm^-1; ORAC's run adds the
+    barostat), an exchange attempt every 15 steps (60 fs) by ORAC's rule on
     the replicas' segment energies recorded on the device.  Timed by wall
     clock over the exchange intervals (steps, records, decisions and factor
     writes all inside); plain = one replica alone through the same driver."""
@@ -914,10 +918,10 @@ def hrem_arm(args, wl, device):
 
     s = systems.solvated_chains(20000, 4242, solute_frac=70 / 20000, name="hrem20k")
     ladder = hrem.ladder_geometric(HREM_N, 0.6)
-    kT = units.BOLTZ * 300.0 / units.UNITE
+    kT = units.BOLTZ * TEST1_THERMOS[0] / units.UNITE
 
     def make(f):
-        return uneven_engine(s.copy(), {"rem_factor": float(f)}, device, wl)
+        return uneven_engine(s.copy(), {"rem_factor": float(f)}, device, wl, thermostats=TEST1_THERMOS)
 
     e1 = make(1.0)
     L = e1.lib
@@ -950,7 +954,8 @@ def hrem_arm(args, wl, device):
     val = ns_per_day(steps * HREM_N, wl["dt_h"], secs)
     pval = ns_per_day(steps, wl["dt_h"], plain_s)
     return {"workload": f"{HREM_N} replicas of one solvated-chain system ({s.ntap} atoms, solute {int(s.rematom.sum())} "
-                        "atoms), solute scaling 1..0.6 geometric as rem_factor(3) (seg_select kind 0), 300 K, "
+                        "atoms), solute scaling 1..0.6 geometric as rem_factor(3) (seg_select kind 0), test2's "
+                        "Nose-Hoover thermostats (298 K, 10 cm^-1 each; no barostat), "
                         f"exchange attempts every {HREM_EVERY} steps ({HREM_EVERY * wl['dt_h']:g} fs)",
             "replicas": HREM_N, "value": val, "unit": "ns/day (aggregate over replicas)",
             "plain_value": pval, "speedup_vs_plain": val / pval, "exchanges": HREM_INTERVALS + 1,
