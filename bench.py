@@ -809,7 +809,7 @@ def serve_arm(args, wl, device):
         measured.append(time.perf_counter() - t0)
         modelled.append(nsteps * t_step[sid])
         e.close()
-    srv = serve.Server(device=device, budget_bytes=150e9, max_active=32, chunk=4)
+    srv = serve.Server(device=device, budget_bytes=150e9, max_active=32, chunk=args.serve_chunk)
     svc = serve.Service(srv, pop, lambda s: uneven_engine(s, specs[int(s.name[len("served"):])], device, wl),
                         nsteps=nsteps)
     res = svc.run(arrivals, timeout=900.0)
@@ -842,7 +842,8 @@ def serve_arm(args, wl, device):
                             "measured_over_model": sum(measured) / sum(modelled),
                             "how": "the first requests' systems run one at a time through the plain driver, 500 steps "
                                    "each (wall clock, context built beforehand as in the model)"},
-            "how": "native executor (orac_gpu_server_*): per-system streams, 4 step graphs per chunk, pump thread; "
+            "how": f"native executor (orac_gpu_server_*): per-system streams, {args.serve_chunk} step graphs per chunk, "
+                   "pump thread; "
                    "latency = segment end - arrival (host monotonic clock); plain = first-come-first-served single "
                    "server with each request taking 500 x the system's measured single-system step time"}
 
@@ -1216,6 +1217,7 @@ def main():
     ap.add_argument("--uneven", type=int, default=128, help="systems of the uneven HREM batch (0/1: skip)")
     ap.add_argument("--serve", type=float, default=3.0, help="seconds of Poisson arrivals of the serving leg (0: skip)")
     ap.add_argument("--serve-systems", type=int, default=16, help="systems the serving requests draw from")
+    ap.add_argument("--serve-chunk", type=int, default=4, help="captured steps the serving executor queues at a time")
     ap.add_argument("--no-f0", dest="f0", action="store_false", help="skip the ORAC test1 system leg")
     ap.add_argument("--no-drift", dest="drift", action="store_false", help="skip the 1,000-step energy drift run")
     ap.add_argument("--no-hrem", dest="hrem", action="store_false", help="skip the replica-exchange leg")
