@@ -106,6 +106,7 @@ NE_WALKERS = 12  # the three restart states, four velocity draws each
 F0_WORKLOAD = dict(build=f0_system, dt_h=15.0, lrespa=5, mrespa=2, n1respa=2, n0respa=2, nupdte=6, rshk="l")
 # test1/md.in and test2/rem.in: TEMPERATURE 298, THERMOS solute/solvent/cofm 10 cm^-1
 TEST1_THERMOS = (298.0, 10.0, 10.0, 10.0)
+NVT_LIQUID = (300.0, 20.0, 20.0, 20.0)  # test3/test4's THERMOS (300 K, 20 cm^-1)
 DUDL_STEPS, DUDL_EVERY = 400, 2  # dU/dlambda sampling of the batched windows
 SERVE_PLAIN_SAMPLE = 8  # serving requests also run one at a time, to check the plain model
 HREM_N, HREM_EVERY, HREM_INTERVALS = 16, 15, 10  # replica-exchange leg
@@ -453,6 +454,10 @@ def gpu_arm(args, wl, s, device):
     xs, _ = eng.md_state()
     eng.close()
     try:
+        res["nvt"] = nvt_arm(args, wl, s, device, flush)
+    except Exception as exc:
+        res["nvt"] = {"error": f"{type(exc).__name__}: {exc}"}
+    try:
         res["force_check"] = force_check(s, xs)
     except Exception as exc:
         res["force_check"] = {"error": f"{type(exc).__name__}: {exc}"}
@@ -548,6 +553,35 @@ def step_breakdown(eng, flush, nsteps):
                      "share_of_step": ms.value / sum(step_ms) if step_ms else None}
     L.orac_gpu_prof_enable(eng.ctx, 0)
     return out
+
+
+def nvt_arm(args, wl, s, device, flush):
+    """The plain workload with Nose-Hoover thermostats (ORAC's THERMOS at
+    300 K, 20 cm^-1 each, as test3/test4 couple them): the same steps timed
+    the same way, and the thermostats' state at the end."""
+    import torch
+
+    from orac_b200.engine import Engine
+
+    e = Engine(s.copy(), device=device)
+    e.set_thermostat(*NVT_LIQUID)
+    e.md_setup(wl["dt_h"], wl["lrespa"], wl["mrespa"], wl["nupdte"], wl["rshk"], econst=0.0)
+    L = e.lib
+    st = torch.cuda.ExternalStream(L.orac_gpu_get_stream(e.ctx), device=device)
+    for _ in range(args.warmup):
+        L.orac_gpu_md_run_async(e.ctx, 1)
+    if e.collect():
+        raise RuntimeError(L.orac_gpu_last_error(e.ctx).decode())
+    ms = _timed_steps(lambda: L.orac_gpu_md_run_async(e.ctx, 1), st, flush, args.steps)
+    if e.collect():
+        raise RuntimeError(L.orac_gpu_last_error(e.ctx).decode())
+    eta, etap, q, ndf, et = e.md_thermostat()
+    e.close()
+    return {"value": ns_per_day(args.steps, wl["dt_h"], sum(ms) / 1e3), "unit": "ns/day",
+            "ms_per_step": sum(ms) / args.steps,
+            "thermostats": f"Nose-Hoover (ORAC's THERMOS) at {NVT_LIQUID[0]:g} K, centres of mass, solute and "
+                           f"solvent at {NVT_LIQUID[1]:g} cm^-1",
+            "etap": [float(x) for x in etap], "ndf": [int(x) for x in ndf]}
 
 
 def _timed_steps(run_one, stream, flush, steps):
@@ -1330,7 +1364,7 @@ def main():
                     "how": "orac_gpu_md_set_state (pinned host -> device), one step, orac_gpu_md_get_state "
                            "(device -> pinned host, with the status flags), orac_gpu_md_collect, wall clock"},
                gpu_launches=res["launches"], clocks=res["clocks"], tuning=res["tuning"])
-    for key in ("force_check", "energy_conservation", "step_breakdown"):
+    for key in ("force_check", "energy_conservation", "step_breakdown", "nvt"):
         if key in res:
             out[key] = res[key]
     if "batched" in res:
