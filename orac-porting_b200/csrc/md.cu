@@ -1238,7 +1238,7 @@ struct ThermoArgs {
   const int4* bchunk;   // k_mol_sums blocks: molecule, first atom, atoms (at most TH_CHUNK)
   const double* bmass;  // [nbm]
   unsigned long long* msum;  // [nbm][TH_NS] fixed point
-  double* vcur;         // [nbm][3] centre-of-mass velocity left by the end pass
+  double* vcur;         // [nbm][3] centre-of-mass velocity the pass leaves (the drift's start sandwich reads it)
   const unsigned long long* f[NLV];
   // the end half kicks of N0 (c0) and N1 (c1), the end sandwich with the M
   // half kick cm, K1; then kicks of L (cl) and H (ch) and K2 (the start
@@ -1295,7 +1295,7 @@ __global__ void __launch_bounds__(TS_BLOCK) k_mol_sums(const ThermoArgs A) {
 }
 
 // centre-of-mass velocity of molecule p (outside the small molecules) at the
-// stages of the end pass, from its sums: Va after the end kicks, V1 after
+// stages of the pass, from its sums: Va after the end kicks, V1 after
 // the end sandwich, V2 after the L and H kicks; FM its M force
 struct BigStages {
   double Va[3], V1[3], V2[3], FM[3], iM;
