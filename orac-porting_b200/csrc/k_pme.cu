@@ -510,12 +510,22 @@ __global__ void k_gather(const AtomArgs A) {
     bspline<P>((float)(fr[0] - (int)fr[0]), p, th1, d1);
     bspline<P>((float)(fr[1] - (int)fr[1]), p, th2, d2);
     bspline<P>((float)(fr[2] - (int)fr[2]), p, th3, d3);
-    // the lane's planes i3 = sub, sub + GATHER_LANES, ... (a compile-time
-    // loop over every plane, so the arrays are indexed by constants)
+    // the lane's planes i3 = sub, sub + GATHER_LANES, ...: the plane's
+    // spline values picked from the arrays by constant indices, so every
+    // lane of the warp runs its own plane at once (a loop over all planes
+    // that skipped the others' ran each plane with a quarter of the lanes)
+    constexpr int PP = P > 0 ? P : MAXORD;
 #pragma unroll
-    for (int i3 = 0; i3 < (P > 0 ? P : MAXORD); i3++) {
-      if (P == 0 && i3 >= p) break;
-      if (i3 % GATHER_LANES != sub) continue;
+    for (int c = 0; c < (PP + GATHER_LANES - 1) / GATHER_LANES; c++) {
+      const int i3 = sub + c * GATHER_LANES;
+      if (i3 >= p) break;
+      float t3 = 0.f, dd3 = 0.f;
+#pragma unroll
+      for (int q = 0; q < PP; q++)
+        if (q == i3) {
+          t3 = th3[q];
+          dd3 = d3[q];
+        }
       const int kk = gidx((int)fr[2] - p + 1 + i3, A.n3);
 #pragma unroll
       for (int i2 = 0; i2 < (P > 0 ? P : MAXORD); i2++) {
@@ -531,10 +541,10 @@ __global__ void k_gather(const AtomArgs A) {
           s2 += th1[i1] * qv;
         }
         s3 = s2;
-        phi += s2 * th2[i2] * th3[i3];
-        f1 += s1 * th2[i2] * th3[i3];
-        f2 += s2 * d2[i2] * th3[i3];
-        f3 += s3 * th2[i2] * d3[i3];
+        phi += s2 * th2[i2] * t3;
+        f1 += s1 * th2[i2] * t3;
+        f2 += s2 * d2[i2] * t3;
+        f3 += s3 * th2[i2] * dd3;
       }
     }
   }
