@@ -8,9 +8,10 @@ orac_b200.oracio.system_from_orac turns them into a System.
 
 Also builds tests/golden/f0_orac_records.npz: the positions, velocities and
 boxes of test2's other two replica-1 restart files (ij4i0001.rst,
-ij4i0003.rst) and, for all three states, the energy record ORAC printed at
-the step it wrote the restart (test2/PAR0001/out0001, matched by box edge
-and temperature).
+ij4i0003.rst) and, for all three states, the Nose-Hoover thermostats'
+state the restart carries and the energy record ORAC printed at the step it
+wrote the restart (test2/PAR0001/out0001, matched by box edge and
+temperature).
 
 Run from the repository root with the path of a reference checkout:
     python tests/golden/make_f0.py <reference root>
@@ -85,6 +86,10 @@ def build_records(root, ntap):
             out[f"co{k}"] = rs["co"]
             out[f"xyz{k}"] = rs["xyz"]
             out[f"v{k}"] = rs["v"]
+        # the three Nose-Hoover thermostats' coordinates and velocities the
+        # restart carries (src/readrs.f:247-251: gh, vh)
+        out[f"eta{k}"] = rs["eta"]
+        out[f"etap{k}"] = rs["etap"]
     out["printed"] = np.array(vals)
     out["out0001_line"] = np.array(where)
     return out

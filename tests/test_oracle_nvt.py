@@ -106,3 +106,32 @@ def test_restart_with_the_thermostat_state_continues_the_run(chain):
     np.testing.assert_allclose(b.thermostat()[1], a.thermostat()[1], rtol=1e-8)
     a.close()
     b.close()
+
+
+def test_f0_test4_with_the_restart_thermostats_matches_what_orac_printed():
+    """test4's walker 1 on ORAC's system with test4's THERMOS (300 K, 20
+    cm^-1) started from the thermostats' state ORAC wrote into its restart
+    (tests/golden/f0_orac_records.npz: eta, etap of test2's ij4i0000.rst):
+    the work after 60 fs against the first line of ORAC's 1.5.wrk (ORAC's
+    run adds the barostat and a COM restraint: 0.4%, as the NVE run)."""
+    import os
+
+    from test_oracle_ne import F0_FORM, F0_MD, F0_WALKERS, f0_test4
+
+    here = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+    d = np.load(os.path.join(here, "ne_test4.npz"))
+    r = np.load(os.path.join(here, "f0_orac_records.npz"))
+    sched = d["schedule"]
+    s = f0_test4(0)
+    o = oracle.OracleMD(s.copy(), F0_MD["dt_h"], F0_MD["lrespa"], F0_MD["mrespa"], F0_MD["nupdte"], F0_MD["rshk"],
+                        n1respa=F0_MD["n1respa"], n0respa=F0_MD["n0respa"])
+    o.set_alchemy(s.ss_alchemy, [0.0] * 8, **F0_FORM)
+    o.set_schedule(sched[:, 0] * 1000.0, sched[:, 1], sched[:, 2], sched[:, 3], sched[:, 4])
+    o.set_thermostat(300.0, 20.0, 20.0, 20.0)
+    o.set_thermostat_state(r["eta0"], r["etap0"])
+    o.run(4)
+    w = o.work()[0]
+    eta, etap, _, _, _ = o.thermostat()
+    o.close()
+    np.testing.assert_allclose(w * units.KJMOL, d[f"wrk{F0_WALKERS[0]}"][0, 5], rtol=4e-3)
+    assert np.all(eta != r["eta0"])  # the thermostats moved from ORAC's state
