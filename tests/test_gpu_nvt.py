@@ -182,3 +182,45 @@ def test_nvt_restart_continues_the_run(tmp_path):
     np.testing.assert_allclose(b.md_thermostat()[1], a.md_thermostat()[1], rtol=1e-8)
     a.close()
     b.close()
+
+
+def test_nvt_ne_f0_from_orac_thermostat_state_matches_the_oracle():
+    """test4's walker 1 on ORAC's system: the non-equilibrium schedule with
+    test4's THERMOS (300 K, 20 cm^-1) started from the thermostats' state of
+    ORAC's restart file; the GPU's work, lambdas and thermostats against the
+    oracle's after each of 4 outer steps (60 fs)."""
+    import os
+
+    from test_oracle_ne import F0_FORM, F0_MD, f0_test4
+
+    here = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+    d = np.load(os.path.join(here, "ne_test4.npz"))
+    r = np.load(os.path.join(here, "f0_orac_records.npz"))
+    sched = d["schedule"]
+    args = (sched[:, 0] * 1000.0, sched[:, 1], sched[:, 2], sched[:, 3], sched[:, 4])
+    s = f0_test4(0)
+    g = Engine(s.copy())
+    g.set_alchemy(s.ss_alchemy, 0.5, 0.5, **F0_FORM)
+    g.set_lambda(0.0, 0.0, 0.0, 0.0)
+    g.set_schedule(*args)
+    g.set_thermostat(300.0, 20.0, 20.0, 20.0)
+    g.md_setup(F0_MD["dt_h"], F0_MD["lrespa"], F0_MD["mrespa"], F0_MD["nupdte"], F0_MD["rshk"],
+               n1respa=F0_MD["n1respa"], n0respa=F0_MD["n0respa"])
+    g.set_thermostat_state(r["eta0"], r["etap0"])
+    o = oracle.OracleMD(s.copy(), F0_MD["dt_h"], F0_MD["lrespa"], F0_MD["mrespa"], F0_MD["nupdte"], F0_MD["rshk"],
+                        n1respa=F0_MD["n1respa"], n0respa=F0_MD["n0respa"])
+    o.set_alchemy(s.ss_alchemy, [0.0] * 8, **F0_FORM)
+    o.set_schedule(*args)
+    o.set_thermostat(300.0, 20.0, 20.0, 20.0)
+    o.set_thermostat_state(r["eta0"], r["etap0"])
+    for step in range(4):
+        g.md_run(1)
+        o.run(1)
+        wg, tg, lg, _ = g.md_work()
+        wo, to, lo, _ = o.work()
+        assert tg == to and lg == lo
+        np.testing.assert_allclose(wg, wo, rtol=1e-5, atol=1e-8, err_msg=f"work after step {step}")
+        pg, po = g.md_thermostat()[1], o.thermostat()[1]
+        np.testing.assert_allclose(pg, po, rtol=RTOL, atol=RTOL * np.abs(po).max(), err_msg=f"etap after step {step}")
+    g.close()
+    o.close()
