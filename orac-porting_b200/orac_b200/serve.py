@@ -198,6 +198,35 @@ class Service:
                 return False
         return True
 
+    def prewarm(self, sids=None):
+        """Build the contexts of the given systems (all by default) before
+        requests arrive, as far as the budget holds them without evicting,
+        and capture their step graphs with one step each (a step the
+        segments' counts leave out).  Returns the number built."""
+        n = 0
+        for sid in (self.systems if sids is None else sids):
+            if sid in self.resident:
+                continue
+            s = self.systems[sid]
+            need = int(self.estimate(s))
+            if not self.ex.reserve(need):
+                break
+            eng = self.make_engine(s)
+            self.builds += 1
+            actual = int(eng.footprint())
+            if actual > need and not self.ex.reserve(actual - need):
+                eng.close()
+                self.ex.unreserve(need)
+                break
+            if actual < need:
+                self.ex.unreserve(need - actual)
+            run = getattr(eng, "md_run", None)
+            if run is not None:
+                run(1)
+            self.resident[sid] = _Resident(eng, actual)
+            n += 1
+        return n
+
     # ------------------------------------------------------------ requests
     def _start(self, req, r):
         r.busy = True
