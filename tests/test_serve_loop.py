@@ -238,3 +238,16 @@ def test_orac_restart_round_trip_rebuilds_the_system(tmp_path):
     assert r["nstep"] == 30 and np.array_equal(r["xyz"], rst["xyz"]) and np.array_equal(r["v"], rst["v"])
     s2 = oracio.system_from_orac(tp, r, **kw)
     assert np.array_equal(s2.cartesian(), s.cartesian()) and np.array_equal(s2.vx, s.vx)
+
+
+def test_prewarm_builds_what_the_budget_holds_and_requests_start_without_builds():
+    """Service.prewarm builds the systems' contexts before requests arrive,
+    within the budget and without evicting; requests for them then start
+    without a build."""
+    svc, ex, systems = make_service(budget=1200 * (1000 + 2000) + 10)
+    assert svc.prewarm() == 2  # the largest system does not fit beside them
+    assert svc.builds == 2 and svc.evictions == 0 and ex.reserved <= ex.budget
+    res = svc.run([(0.0, 0), (0.001, 1), (0.002, 0)], timeout=100.0)
+    assert len(res) == 3 and svc.builds == 2
+    svc2, ex2, _ = make_service(budget=10 ** 9)
+    assert svc2.prewarm() == 3 and svc2.prewarm() == 0  # built once
