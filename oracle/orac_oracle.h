@@ -6,13 +6,21 @@
  * load this library, and only as the checker.  The product (liborac_gpu.so)
  * never links, loads or calls it.
  *
- * Parity status: UNPINNED against reference outputs.  The reference ships no
- * force- or energy-per-call vectors (its tests are four chaotic full MD runs)
- * and it cannot be built here (Fortran + FFTW + MPI, none installed).  The
- * restatement is instead checked by properties the reference's algorithm must
- * satisfy: forces = -dE/dx by finite differences, PME against a direct Ewald
- * k-sum, the NaCl Madelung constant, the FFT against numpy.fft, and the
- * linked-cell list against a brute-force pair search.
+ * Parity status: pinned on outputs the reference printed.  The reference
+ * ships no force- or energy-per-call vectors (its tests are four chaotic full
+ * MD runs) and it cannot be built here (Fortran + FFTW + MPI, none
+ * installed), but test2 wrote restart files at three steps of its first
+ * replica and printed an energy record at each of them: the restatement,
+ * given ORAC's own topology-parameter file and those restarts, reproduces the
+ * records' bonded columns to the printed digits and the nonbonded and
+ * reciprocal-carrying columns to 1e-4 (tests/test_oracle_orac_records.py,
+ * fixtures by tests/golden/make_f0.py).  Its non-equilibrium loop reproduces
+ * the lambdas of all four of test4's work files and test4's printed work at
+ * 60 fs to 0.4% (tests/test_oracle_ne.py; ORAC's run is NPT).  Properties
+ * the algorithm must satisfy are checked as well: forces = -dE/dx by finite
+ * differences, PME against a direct Ewald k-sum, the NaCl Madelung constant,
+ * the FFT against numpy.fft, and the linked-cell list against a brute-force
+ * pair search.
  *
  * Conventions follow the Fortran arguments: every array is column-major,
  * every index stored in an array (grppt, atomp, mapnl, list entries, type

@@ -2,8 +2,9 @@
 
 ctypes front end of liborac_oracle.so (the FP64 CPU restatement of ORAC's
 nonbonded force path).  Only tests/, __graft_entry__.smoke() and bench.py's
-CPU-baseline leg import this module, as the checker.  Parity status: unpinned
-against reference outputs (see orac_oracle.h).
+CPU-baseline leg import this module, as the checker.  Parity status: pinned
+on the energy records and the NE work ORAC printed for its own test system
+(see orac_oracle.h).
 
 The Oracle class drives the restated routines in the order ORAC's r-RESPA
 driver does (src/mtsmd.f:2403-2470 for the list update, :3030/:3185/:3263 for
